@@ -1,0 +1,267 @@
+"""B200 plane-wave fast Gauss transform (2D and 3D), Python front end.
+
+Mirrors the reference's calling sequence
+``fgt2d(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal,
+dipstr, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+gradtarg, hesstarg)`` (2d/planewave/src/fgt2d.f:19-22; fgt3d identical with
+d = 3) over the C ABI in ``include/fgt_b200.h``.  Arrays use the reference's
+memory layout: ``sources`` is the Fortran ``sources(d, ns)``, i.e. a C-order
+``(ns, d)`` array; ``charge(nd, ns)`` is ``(ns, nd)``; outputs likewise.
+
+The compute path is the CUDA library ``fgt2d_b200/lib/libfgt_b200.so``; there
+is no CPU fallback: importing works without it, but every call raises if the
+library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["fgt2d", "fgt3d", "transform", "Context", "Plan", "HostTree", "lib", "FGTError",
+           "PREC_FP64", "PREC_MIXED", "PREC_AUTO"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfgt_b200.so")
+
+PREC_FP64, PREC_MIXED, PREC_AUTO = 0, 1, 2
+_PREC = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "auto": PREC_AUTO}
+STATUS = {0: "ok", 1: "bad argument", 2: "unsupported option", 3: "out of memory",
+          4: "CUDA error", 5: "no CUDA device"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class FGTError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = int(status)
+        msg = f"{where}: status {status} ({STATUS.get(int(status), 'unknown')})"
+        if status == 4 and _lib is not None:
+            msg += f", cuda error {_lib.fgt_last_cuda_error()}"
+        super().__init__(msg)
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in
+                ["dim", "nd", "ns", "nt", "npwlevel", "nlevels", "nboxes", "npw", "nexp", "nlmax",
+                 "nform", "neval", "ndirect_tasks", "nmp", "nloc"]] + \
+               [("direct_pairs", ctypes.c_longlong), ("form_sources", ctypes.c_longlong),
+                ("eval_points", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
+                ("host_tree_s", ctypes.c_double), ("host_lists_s", ctypes.c_double),
+                ("host_plan_s", ctypes.c_double), ("large_delta", ctypes.c_int),
+                ("all_direct", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FGTError(5, f"fgt2d_b200: {LIB_PATH} is missing (run __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    i, d = ctypes.c_int, ctypes.c_double
+    L.fgt_ctx_create.argtypes = [i, ctypes.POINTER(_vp)]
+    L.fgt_ctx_destroy.argtypes = [_vp]
+    L.fgt_ctx_set_precision.argtypes = [_vp, i]
+    L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
+    L.fgt_default_ctx.restype = _vp
+    L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,
+                                _dp, i, _dp, _dp, _dp]
+    L.fgt_plan_create.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, ctypes.POINTER(_vp)]
+    L.fgt_plan_execute_host.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp]
+    L.fgt_plan_execute_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.fgt_plan_profile_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]
+    L.fgt_plan_get_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
+    L.fgt_plan_destroy.argtypes = [_vp]
+    L.fgt_status_string.restype = ctypes.c_char_p
+    L.fgt_status_string.argtypes = [i]
+    L.fgt_build_info.restype = ctypes.c_char_p
+    L.fgt_host_tree_create.argtypes = [i, d, d, i, _dp, i, _dp, i, ctypes.POINTER(_vp)]
+    L.fgt_host_tree_dims.argtypes = [_vp, _ip]
+    L.fgt_host_tree_field.restype = ctypes.c_longlong
+    L.fgt_host_tree_field.argtypes = [_vp, i, _vp]
+    L.fgt_host_tree_destroy.argtypes = [_vp]
+    _lib = L
+    return L
+
+
+def _check(st, where):
+    if st != 0:
+        raise FGTError(st, where)
+
+
+def _f64(a, shape):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(shape)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+class Context:
+    """One CUDA device, its stream and the precision mode."""
+
+    def __init__(self, device=0, precision="auto", host_threads=0):
+        L = lib()
+        h = _vp()
+        _check(L.fgt_ctx_create(int(device), ctypes.byref(h)), "fgt_ctx_create")
+        self._h = h
+        self.set_precision(precision)
+        if host_threads:
+            L.fgt_ctx_set_host_threads(self._h, int(host_threads))
+
+    def set_precision(self, precision):
+        p = _PREC[precision] if isinstance(precision, str) else int(precision)
+        _check(lib().fgt_ctx_set_precision(self._h, p), "fgt_ctx_set_precision")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fgt_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _default_ctx():
+    h = lib().fgt_default_ctx()
+    if not h:
+        raise FGTError(5, "fgt_default_ctx")
+    return h
+
+
+def transform(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
+              ifcharge=1, ifdipole=0):
+    """Whole transform; returns ``(pot, pottarg)`` shaped ``(ns, nd)``, ``(nt, nd)``."""
+    L = lib()
+    src = _f64(sources, (-1, dim))
+    ns = src.shape[0]
+    q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
+    trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
+    nt = trg.shape[0]
+    pot = np.zeros((ns, nd)) if ifpgh else None
+    pt = np.zeros((nt, nd)) if ifpghtarg else None
+    h = ctx.handle if ctx is not None else _default_ctx()
+    st = L.fgt_transform(h, dim, nd, float(delta), float(eps), ns, _p(src), ifcharge, _p(q),
+                         ifdipole, None, None, ifpgh, _p(pot), None, None, nt, _p(trg), ifpghtarg,
+                         _p(pt), None, None)
+    _check(st, "fgt_transform")
+    return pot, pt
+
+
+def fgt2d(nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None):
+    """2D transform with the reference's argument meaning (fgt2d.f:19-61)."""
+    return transform(2, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, ctx)
+
+
+def fgt3d(nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None):
+    """3D transform with the reference's argument meaning (fgt3d.f:19-64)."""
+    return transform(3, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, ctx)
+
+
+class Plan:
+    """Tree, lists and device task arrays for fixed points; apply many times."""
+
+    def __init__(self, ctx, dim, nd, delta, eps, sources, targ=None, ifpgh=1, ifpghtarg=0):
+        L = lib()
+        self.ctx = ctx
+        self.dim, self.nd = dim, nd
+        src = _f64(sources, (-1, dim))
+        trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
+        self.ns, self.nt = src.shape[0], trg.shape[0]
+        self.ifpgh, self.ifpghtarg = ifpgh, ifpghtarg
+        h = _vp()
+        _check(L.fgt_plan_create(ctx.handle, dim, nd, float(delta), float(eps), self.ns, _p(src),
+                                 self.nt, _p(trg), ifpgh, ifpghtarg, ctx and ctypes.byref(h)),
+               "fgt_plan_create")
+        self._h = h
+
+    def info(self):
+        inf = PlanInfo()
+        _check(lib().fgt_plan_get_info(self._h, ctypes.byref(inf)), "fgt_plan_get_info")
+        return inf.as_dict()
+
+    def execute_host(self, sources, charge, targ=None):
+        src = _f64(sources, (self.ns, self.dim))
+        q = _f64(charge, (self.ns, self.nd))
+        trg = _f64(targ, (self.nt, self.dim)) if targ is not None else None
+        pot = np.zeros((self.ns, self.nd))
+        pt = np.zeros((self.nt, self.nd))
+        _check(lib().fgt_plan_execute_host(self._h, _p(src), _p(q), _p(trg), _p(pot), _p(pt)),
+               "fgt_plan_execute_host")
+        return pot, pt
+
+    def execute_device(self, d_src, d_chg, d_trg, d_pot, d_pottarg, stream=None):
+        """Device pointers (ints, e.g. ``tensor.data_ptr()``); asynchronous."""
+        _check(lib().fgt_plan_execute_device(self._h, d_src, d_chg, d_trg or None, d_pot or None,
+                                             d_pottarg or None, stream),
+               "fgt_plan_execute_device")
+
+    def profile_device(self, d_src, d_chg, d_trg, d_pot, d_pottarg):
+        ms = (ctypes.c_float * 8)()
+        _check(lib().fgt_plan_profile_device(self._h, d_src, d_chg, d_trg or None, d_pot or None,
+                                             d_pottarg or None, ms), "fgt_plan_profile_device")
+        names = ["gather", "form", "merge", "m2l", "split", "eval", "direct", "scatter"]
+        return dict(zip(names, list(ms)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fgt_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_TREE_INT = ["laddr", "ilevel", "iparent", "nchild", "ichild", "nnbors", "nbors", "isrc",
+             "isrcse", "itarg", "itargse"]
+
+
+def HostTree(dim, delta, eps, sources, targ, nthreads=0):
+    """The host tree of the transform in the reference's conventions (1-based)."""
+    L = lib()
+    src = _f64(sources, (-1, dim))
+    trg = _f64(targ, (-1, dim))
+    h = _vp()
+    _check(L.fgt_host_tree_create(dim, float(delta), float(eps), src.shape[0], _p(src),
+                                  trg.shape[0], _p(trg), int(nthreads), ctypes.byref(h)),
+           "fgt_host_tree_create")
+    try:
+        dims = np.zeros(4, dtype=np.int32)
+        st = L.fgt_host_tree_dims(h, dims.ctypes.data_as(_ip))
+        out = {"nlevels": int(dims[0]), "nboxes": int(dims[1]), "npwlevel": int(dims[2]),
+               "nlmax": int(dims[3])}
+        if st != 0:
+            return out
+        for k, name in enumerate(_TREE_INT):
+            n = L.fgt_host_tree_field(h, k, None)
+            a = np.zeros(n, dtype=np.int32)
+            L.fgt_host_tree_field(h, k, a.ctypes.data_as(_vp))
+            out[name] = a
+        for k, name in ((11, "centers"), (12, "boxsize")):
+            n = L.fgt_host_tree_field(h, k, None)
+            a = np.zeros(n)
+            L.fgt_host_tree_field(h, k, a.ctypes.data_as(_vp))
+            out[name] = a
+        return out
+    finally:
+        L.fgt_host_tree_destroy(h)

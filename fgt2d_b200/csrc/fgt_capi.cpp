@@ -1,0 +1,590 @@
+// C ABI of the B200 plane-wave FGT (declared in include/fgt_b200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "fgt_b200.h"
+#include "fgt_device.hpp"
+#include "fgt_plan.hpp"
+
+using namespace fgtb;
+
+struct fgt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = FGT_PREC_AUTO;
+  int nthreads = 0;
+  std::mutex mu;
+};
+
+struct fgt_plan {
+  fgt_ctx* ctx = nullptr;
+  HostPlan H;
+  DevicePlan D;
+  bool have_device = false;
+  // device copies of the caller-order arrays for the host-array entry points
+  double* d_io = nullptr;
+  size_t io_bytes = 0;
+  double* d_src = nullptr;
+  double* d_chg = nullptr;
+  double* d_trg = nullptr;
+  double* d_pot = nullptr;
+  double* d_pottarg = nullptr;
+  double* d_work = nullptr;  // large-delta local expansion
+  int last_launches = 0;
+};
+
+namespace {
+thread_local int g_last_cuda = 0;
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return FGT_OK;
+  g_last_cuda = (int)e;
+  if (e == cudaErrorMemoryAllocation) return FGT_ERR_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return FGT_ERR_NODEVICE;
+  if (e == cudaErrorNotSupported) return FGT_ERR_UNSUPPORTED;
+  return FGT_ERR_CUDA;
+}
+#define CKS(x)                                 \
+  do {                                         \
+    int s_ = cuda_status(x);                   \
+    if (s_ != FGT_OK) return s_;               \
+  } while (0)
+
+int resolve_precision(const fgt_ctx* c, double eps) {
+  if (c->precision == FGT_PREC_AUTO) return eps >= 1e-6 ? PREC_MIXED : PREC_FP64;
+  return c->precision == FGT_PREC_MIXED ? PREC_MIXED : PREC_FP64;
+}
+
+bool finite_all(const double* a, size_t n) {
+  if (!a) return n == 0;
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+int check_args(int dim, int nd, double delta, double eps, int ns, const double* sources,
+               int ifcharge, int ifdipole, int ifpgh, int nt, const double* targ, int ifpghtarg) {
+  if (dim != 2 && dim != 3) return FGT_ERR_BADARG;
+  if (nd < 1 || !(delta > 0) || !std::isfinite(delta) || !(eps > 0) || !(eps < 1)) return FGT_ERR_BADARG;
+  if (ns < 0 || nt < 0) return FGT_ERR_BADARG;
+  if (ns > 0 && !sources) return FGT_ERR_BADARG;
+  if (nt > 0 && ifpghtarg > 0 && !targ) return FGT_ERR_BADARG;
+  if (!finite_all(sources, (size_t)ns * dim)) return FGT_ERR_BADARG;
+  if (nt > 0 && targ && !finite_all(targ, (size_t)nt * dim)) return FGT_ERR_BADARG;
+  if (ifcharge != 1 || ifdipole != 0) return FGT_ERR_UNSUPPORTED;
+  if (ifpgh < 0 || ifpgh > 1 || ifpghtarg < 0 || ifpghtarg > 1) return FGT_ERR_UNSUPPORTED;
+  return FGT_OK;
+}
+
+int plan_device(fgt_plan* p) {
+  const Params& P = p->H.P;
+  size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
+  size_t n_src = ns * dim, n_chg = ns * nd, n_trg = nt * dim, n_pot = ns * nd, n_pt = nt * nd;
+  size_t n_work = 0;
+  if (P.large_delta) {
+    size_t Pn = P.nlocal0 + 1;
+    n_work = 4 + nd * (dim == 2 ? Pn * Pn : Pn * Pn * Pn);
+  }
+  auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
+  p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
+  CKS(cudaMalloc(&p->d_io, p->io_bytes));
+  double* c = p->d_io;
+  p->d_src = c; c += al(n_src);
+  p->d_chg = c; c += al(n_chg);
+  p->d_trg = c; c += al(n_trg);
+  p->d_pot = c; c += al(n_pot);
+  p->d_pottarg = c; c += al(n_pt);
+  p->d_work = c;
+  if (!P.large_delta) {
+    CKS(device_plan_create(p->H, p->D));
+    p->have_device = true;
+  }
+  return FGT_OK;
+}
+
+int run_device(fgt_plan* p, const double* s, const double* q, const double* t, double* pot,
+               double* pt, cudaStream_t st, StageTimes* times) {
+  const Params& P = p->H.P;
+  int prec = resolve_precision(p->ctx, P.eps);
+  if (P.large_delta) {
+    CKS(large_delta_execute(P, s, q, t, pot, pt, p->d_work, st));
+    p->last_launches = (P.ns > 0) + (P.ifpgh == 1) + (P.ifpghtarg == 1);
+    return FGT_OK;
+  }
+  CKS(device_plan_execute(p->D, s, q, t, pot, pt, prec, st, times));
+  p->last_launches = (int)p->D.launches;
+  return FGT_OK;
+}
+
+int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                   const double* sources, int ifcharge, const double* charge, int ifdipole,
+                   int ifpgh, double* pot, int nt, const double* targ, int ifpghtarg,
+                   double* pottarg) {
+  int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg);
+  if (st != FGT_OK) return st;
+  if (ns > 0 && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
+  if (ifpgh == 1 && ns > 0 && pot) memset(pot, 0, sizeof(double) * (size_t)ns * nd);
+  if (ifpghtarg == 1 && nt > 0 && pottarg) memset(pottarg, 0, sizeof(double) * (size_t)nt * nd);
+  if (ns == 0) return FGT_OK;
+  fgt_plan* plan = nullptr;
+  st = fgt_plan_create(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, &plan);
+  if (st != FGT_OK) return st;
+  st = fgt_plan_execute_host(plan, sources, charge, targ, pot, pottarg);
+  fgt_plan_destroy(plan);
+  return st;
+}
+
+std::once_flag g_default_once;
+fgt_ctx* g_default = nullptr;
+
+void report(const char* who, int st) {
+  if (st != FGT_OK)
+    fprintf(stderr, "%s: failed with status %d (%s), cuda error %d\n", who, st, fgt_status_string(st),
+            g_last_cuda);
+}
+}  // namespace
+
+extern "C" {
+
+const char* fgt_status_string(int s) {
+  switch (s) {
+    case FGT_OK: return "ok";
+    case FGT_ERR_BADARG: return "bad argument";
+    case FGT_ERR_UNSUPPORTED: return "unsupported option";
+    case FGT_ERR_NOMEM: return "out of memory";
+    case FGT_ERR_CUDA: return "CUDA error";
+    case FGT_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+int fgt_last_cuda_error(void) { return g_last_cuda; }
+const char* fgt_build_info(void) { return "fgt_b200 sm_100a FP64+mixed near field"; }
+
+int fgt_ctx_create(int device, fgt_ctx** out) {
+  if (!out) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return FGT_ERR_NODEVICE;
+  if (device < 0 || device >= n) return FGT_ERR_BADARG;
+  fgt_ctx* c = new (std::nothrow) fgt_ctx();
+  if (!c) return FGT_ERR_NOMEM;
+  c->device = device;
+  int s = cuda_status(cudaSetDevice(device));
+  if (s == FGT_OK) s = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  if (s != FGT_OK) {
+    delete c;
+    return s;
+  }
+  *out = c;
+  return FGT_OK;
+}
+int fgt_ctx_destroy(fgt_ctx* c) {
+  if (!c) return FGT_ERR_BADARG;
+  if (c == g_default) return FGT_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return FGT_OK;
+}
+int fgt_ctx_set_precision(fgt_ctx* c, int precision) {
+  if (!c || precision < 0 || precision > 2) return FGT_ERR_BADARG;
+  c->precision = precision;
+  return FGT_OK;
+}
+int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
+  if (!c) return FGT_ERR_BADARG;
+  c->nthreads = nthreads;
+  return FGT_OK;
+}
+fgt_ctx* fgt_default_ctx(void) {
+  std::call_once(g_default_once, [] {
+    fgt_ctx* c = nullptr;
+    if (fgt_ctx_create(0, &c) == FGT_OK) g_default = c;
+  });
+  return g_default;
+}
+
+int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                    fgt_plan** out) {
+  if (!ctx || !out) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg);
+  if (st != FGT_OK) return st;
+  if (ns == 0) return FGT_ERR_BADARG;
+  std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
+  if (!p) return FGT_ERR_NOMEM;
+  p->ctx = ctx;
+  try {
+    build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads);
+  } catch (const std::bad_alloc&) {
+    return FGT_ERR_NOMEM;
+  }
+  CKS(cudaSetDevice(ctx->device));
+  st = plan_device(p.get());
+  if (st != FGT_OK) {
+    fgt_plan_destroy(p.release());
+    return st;
+  }
+  *out = p.release();
+  return FGT_OK;
+}
+
+int fgt_plan_destroy(fgt_plan* p) {
+  if (!p) return FGT_ERR_BADARG;
+  if (p->ctx) cudaSetDevice(p->ctx->device);
+  if (p->have_device) device_plan_destroy(p->D);
+  if (p->d_io) cudaFree(p->d_io);
+  delete p;
+  return FGT_OK;
+}
+
+int fgt_plan_execute_host(fgt_plan* p, const double* sources, const double* charge,
+                          const double* targ, double* pot, double* pottarg) {
+  if (!p) return FGT_ERR_BADARG;
+  const Params& P = p->H.P;
+  cudaStream_t st = p->ctx->stream;
+  CKS(cudaSetDevice(p->ctx->device));
+  size_t ns = P.ns, nt = P.nt;
+  CKS(cudaMemcpyAsync(p->d_src, sources, ns * P.dim * 8, cudaMemcpyHostToDevice, st));
+  CKS(cudaMemcpyAsync(p->d_chg, charge, ns * P.nd * 8, cudaMemcpyHostToDevice, st));
+  if (P.ifpghtarg == 1 && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, targ, nt * P.dim * 8, cudaMemcpyHostToDevice, st));
+  int s = run_device(p, p->d_src, p->d_chg, p->d_trg, p->d_pot, p->d_pottarg, st, nullptr);
+  if (s != FGT_OK) return s;
+  if (P.ifpgh == 1 && pot) CKS(cudaMemcpyAsync(pot, p->d_pot, ns * P.nd * 8, cudaMemcpyDeviceToHost, st));
+  if (P.ifpghtarg == 1 && nt > 0 && pottarg)
+    CKS(cudaMemcpyAsync(pottarg, p->d_pottarg, nt * P.nd * 8, cudaMemcpyDeviceToHost, st));
+  CKS(cudaStreamSynchronize(st));
+  return FGT_OK;
+}
+
+int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const double* t,
+                            double* pot, double* pt, void* stream) {
+  if (!p) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  return run_device(p, s, q, t, pot, pt, st, nullptr);
+}
+
+int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const double* t,
+                            double* pot, double* pt, float* ms8) {
+  if (!p || !ms8) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  StageTimes T;
+  memset(&T, 0, sizeof(T));
+  int r = run_device(p, s, q, t, pot, pt, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
+  if (r != FGT_OK) return r;
+  CKS(cudaStreamSynchronize(p->ctx->stream));
+  for (int i = 0; i < 8; i++) ms8[i] = T.ms[i];
+  return FGT_OK;
+}
+
+int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
+  if (!p || !o) return FGT_ERR_BADARG;
+  memset(o, 0, sizeof(*o));
+  const Params& P = p->H.P;
+  o->dim = P.dim; o->nd = P.nd; o->ns = P.ns; o->nt = P.nt;
+  o->npwlevel = P.npwlevel; o->nlevels = P.nlevels; o->nboxes = p->H.tree.nboxes;
+  o->npw = P.npw; o->nexp = P.nexp; o->nlmax = P.nlmax;
+  o->nform = (int)p->H.form.size(); o->neval = (int)p->H.eval.size();
+  o->ndirect_tasks = (int)p->H.dir.size(); o->nmp = p->H.nmp; o->nloc = p->H.nloc;
+  o->direct_pairs = p->H.direct_pairs; o->form_sources = p->H.form_sources;
+  o->eval_points = p->H.eval_points;
+  o->device_bytes = (long long)(p->D.bytes + p->io_bytes);
+  o->host_tree_s = p->H.host_tree_s; o->host_lists_s = p->H.host_lists_s;
+  o->host_plan_s = p->H.host_plan_s;
+  o->large_delta = P.large_delta; o->all_direct = P.all_direct;
+  o->kernel_launches = p->last_launches;
+  return FGT_OK;
+}
+
+struct fgt_host_tree {
+  Tree t;
+  int nlmax = 0;
+  bool large = false;
+};
+
+int fgt_host_tree_create(int dim, double delta, double eps, int ns, const double* sources, int nt,
+                         const double* targ, int nthreads, fgt_host_tree** out) {
+  if (!out) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int st = check_args(dim, 1, delta, eps, ns, sources, 1, 0, 0, nt, targ, 0);
+  if (st != FGT_OK) return st;
+  if (ns == 0) return FGT_ERR_BADARG;
+  fgt_host_tree* h = new (std::nothrow) fgt_host_tree();
+  if (!h) return FGT_ERR_NOMEM;
+  try {
+    HostPlan H;
+    int lc;
+    double bs0, cen0[3] = {0, 0, 0};
+    boxsize0(dim, delta, eps, sources, ns, targ, nt, &lc, &bs0, cen0);
+    if (lc < -2) {
+      h->large = true;
+      h->t.npwlevel = lc;
+    } else {
+      int ndiv0 = dim == 2 ? 10 : 40, ndiv = dim == 2 ? 80 : 100, hcap = dim == 2 ? 18 : 15;
+      int nlmax = lc + 4, nls = lc > 0 ? lc : 0, nl0 = 0;
+      double bsize = bs0 / std::ldexp(1.0, nls);
+      for (int i = nls; i <= 100; i++) {
+        nl0 = hlterms(dim, bsize, delta, eps, nl0);
+        if (nl0 <= hcap) { nlmax = i; break; }
+        bsize /= 2;
+      }
+      build_tree(h->t, dim, sources, ns, targ, nt, ndiv, ndiv0, lc, nlmax, bs0, cen0, nthreads);
+      h->t.npwlevel = lc;
+      h->nlmax = nlmax;
+    }
+  } catch (const std::bad_alloc&) {
+    delete h;
+    return FGT_ERR_NOMEM;
+  }
+  *out = h;
+  return FGT_OK;
+}
+int fgt_host_tree_dims(const fgt_host_tree* h, int* dims) {
+  if (!h || !dims) return FGT_ERR_BADARG;
+  dims[0] = h->t.nlevels; dims[1] = h->t.nboxes; dims[2] = h->t.npwlevel; dims[3] = h->nlmax;
+  return h->large ? FGT_ERR_UNSUPPORTED : FGT_OK;
+}
+long long fgt_host_tree_field(const fgt_host_tree* h, int field, void* out) {
+  if (!h || h->large) return -1;
+  const Tree& t = h->t;
+  std::vector<int> v;
+  int nb = t.nboxes;
+  auto id = [](int b) { return b >= 0 ? b + 1 : -1; };
+  switch (field) {
+    case 0: for (int l = 0; l <= t.nlevels; l++) { v.push_back(t.lfirst[l] + 1); v.push_back(t.llast[l] + 1); } break;
+    case 1: v.assign(t.level.begin(), t.level.begin() + nb); break;
+    case 2: for (int b = 0; b < nb; b++) v.push_back(id(t.parent[b])); break;
+    case 3: v.assign(t.nchild.begin(), t.nchild.begin() + nb); break;
+    case 4: for (size_t i = 0; i < (size_t)nb * t.nch; i++) v.push_back(id(t.child[i])); break;
+    case 5: v.assign(t.ncoll.begin(), t.ncoll.begin() + nb); break;
+    case 6: for (size_t i = 0; i < (size_t)nb * t.nco; i++) v.push_back(id(t.coll[i])); break;
+    case 7: for (int x : t.isrc) v.push_back(x + 1); break;
+    case 8: for (int b = 0; b < nb; b++) { v.push_back(t.s0[b] + 1); v.push_back(t.s1[b]); } break;
+    case 9: for (int x : t.itarg) v.push_back(x + 1); break;
+    case 10: for (int b = 0; b < nb; b++) { v.push_back(t.t0[b] + 1); v.push_back(t.t1[b]); } break;
+    case 11:
+      if (out) memcpy(out, t.centers.data(), sizeof(double) * (size_t)nb * t.dim);
+      return (long long)nb * t.dim;
+    case 12:
+      if (out) memcpy(out, t.boxsize.data(), sizeof(double) * (t.nlevels + 1));
+      return t.nlevels + 1;
+    default: return -1;
+  }
+  if (out) memcpy(out, v.data(), sizeof(int) * v.size());
+  return (long long)v.size();
+}
+int fgt_host_tree_destroy(fgt_host_tree* h) {
+  delete h;
+  return FGT_OK;
+}
+
+int fgt_transform(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                  const double* sources, int ifcharge, const double* charge, int ifdipole,
+                  const double* rnormal, const double* dipstr, int ifpgh, double* pot, double* grad,
+                  double* hess, int nt, const double* targ, int ifpghtarg, double* pottarg,
+                  double* gradtarg, double* hesstarg) {
+  (void)rnormal; (void)dipstr; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  if (!ctx) return FGT_ERR_BADARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return transform_impl(ctx, dim, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh,
+                        pot, nt, targ, ifpghtarg, pottarg);
+}
+
+static int fortran_call(int dim, const int* nd, const double* delta, const double* eps, const int* ns,
+                        const double* sources, const int* ifcharge, const double* charge,
+                        const int* ifdipole, const double* rnormal, const double* dipstr,
+                        const int* ifpgh, double* pot, double* grad, double* hess, const int* nt,
+                        const double* targ, const int* ifpghtarg, double* pottarg, double* gradtarg,
+                        double* hesstarg) {
+  if (!nd || !delta || !eps || !ns || !ifcharge || !ifdipole || !ifpgh || !nt || !ifpghtarg)
+    return FGT_ERR_BADARG;
+  fgt_ctx* c = fgt_default_ctx();
+  if (!c) return FGT_ERR_NODEVICE;
+  return fgt_transform(c, dim, *nd, *delta, *eps, *ns, sources, *ifcharge, charge, *ifdipole,
+                       rnormal, dipstr, *ifpgh, pot, grad, hess, *nt, targ, *ifpghtarg, pottarg,
+                       gradtarg, hesstarg);
+}
+
+void fgt2d_(const int* nd, const double* delta, const double* eps, const int* ns,
+            const double* sources, const int* ifcharge, const double* charge, const int* ifdipole,
+            const double* rnormal, const double* dipstr, const int* iper, const int* ifpgh,
+            double* pot, double* grad, double* hess, const int* nt, const double* targ,
+            const int* ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
+  (void)iper;
+  report("fgt2d", fortran_call(2, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal,
+                               dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                               gradtarg, hesstarg));
+}
+void fgt3d_(const int* nd, const double* delta, const double* eps, const int* ns,
+            const double* sources, const int* ifcharge, const double* charge, const int* ifdipole,
+            const double* rnormal, const double* dipstr, const int* iper, const int* ifpgh,
+            double* pot, double* grad, double* hess, const int* nt, const double* targ,
+            const int* ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
+  (void)iper;
+  report("fgt3d", fortran_call(3, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal,
+                               dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                               gradtarg, hesstarg));
+}
+void fgt2d_st_(const int* nd, const double* delta, const double* eps, const int* ns,
+               const double* sources, const int* ifcharge, const double* charge,
+               const int* ifdipole, const double* rnormal, const double* dipstr, const int* iper,
+               const int* ifpgh, double* pot, double* grad, double* hess, const int* nt,
+               const double* targ, const int* ifpghtarg, double* pottarg, double* gradtarg,
+               double* hesstarg, int* ier) {
+  (void)iper;
+  int s = fortran_call(2, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr,
+                       ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg);
+  if (ier) *ier = s;
+}
+void fgt3d_st_(const int* nd, const double* delta, const double* eps, const int* ns,
+               const double* sources, const int* ifcharge, const double* charge,
+               const int* ifdipole, const double* rnormal, const double* dipstr, const int* iper,
+               const int* ifpgh, double* pot, double* grad, double* hess, const int* nt,
+               const double* targ, const int* ifpghtarg, double* pottarg, double* gradtarg,
+               double* hesstarg, int* ier) {
+  (void)iper;
+  int s = fortran_call(3, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr,
+                       ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg);
+  if (ier) *ier = s;
+}
+
+}  // extern "C"
+
+// ---- the fgt2dmain / fgt3dmain cut -----------------------------------------
+template <typename IP>
+static int main_gpu(int dim, const int* nd, const double* delta, const double* eps,
+                    const int* nsource, const double* sourcesort, const int* ifcharge,
+                    const double* chargesort, const int* ifdipole, const int* ntarget,
+                    const double* targetsort, const int* itree, const IP* iptr, const int* nlevels,
+                    const int* npwlevel, const int* nboxes, const double* boxsize,
+                    const double* centers, const int* laddr, const int* isrcse, const int* itargse,
+                    const int* nlocal, const double* pmax, const int* npw, const int* ifpgh,
+                    double* pot, const int* ifpghtarg, double* pottarg) {
+  if (!nd || !delta || !eps || !nsource || !ntarget || !itree || !iptr || !nlevels || !npwlevel ||
+      !nboxes || !boxsize || !centers || !laddr || !isrcse || !itargse || !nlocal || !pmax || !npw ||
+      !ifpgh || !ifpghtarg || !ifcharge || !ifdipole)
+    return FGT_ERR_BADARG;
+  int st = check_args(dim, *nd, *delta, *eps, *nsource, sourcesort, *ifcharge, *ifdipole, *ifpgh,
+                      *ntarget, targetsort, *ifpghtarg);
+  if (st != FGT_OK) return st;
+  fgt_ctx* c = fgt_default_ctx();
+  if (!c) return FGT_ERR_NODEVICE;
+  std::lock_guard<std::mutex> lk(c->mu);
+  std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
+  if (!p) return FGT_ERR_NOMEM;
+  p->ctx = c;
+  int nb = *nboxes, nlev = *nlevels, ns = *nsource, nt = *ntarget, D = dim;
+  int nch = 1 << dim, nco = dim == 2 ? 9 : 27;
+  Tree& t = p->H.tree;
+  t.dim = dim; t.nch = nch; t.nco = nco; t.nlevels = nlev; t.nboxes = nb; t.npwlevel = *npwlevel;
+  t.lfirst.resize(nlev + 1);
+  t.llast.resize(nlev + 1);
+  for (int l = 0; l <= nlev; l++) {
+    t.lfirst[l] = laddr[2 * l] - 1;
+    t.llast[l] = laddr[2 * l + 1] - 1;
+  }
+  auto at = [&](int k, long long off) { return itree[(long long)iptr[k] - 1 + off]; };
+  t.level.resize(nb); t.parent.resize(nb); t.nchild.resize(nb);
+  t.child.assign((size_t)nb * nch, -1); t.ncoll.resize(nb); t.coll.assign((size_t)nb * nco, -1);
+  for (int b = 0; b < nb; b++) {
+    t.level[b] = at(1, b);
+    int par = at(2, b);
+    t.parent[b] = par > 0 ? par - 1 : -1;
+    t.nchild[b] = at(3, b);
+    for (int j = 0; j < nch; j++) {
+      int cb = at(4, (long long)nch * b + j);
+      t.child[(size_t)b * nch + j] = cb > 0 ? cb - 1 : -1;
+    }
+    t.ncoll[b] = at(5, b);
+    for (int i = 0; i < t.ncoll[b] && i < nco; i++) {
+      int cb = at(6, (long long)nco * b + i);
+      t.coll[(size_t)b * nco + i] = cb > 0 ? cb - 1 : -1;
+    }
+  }
+  t.centers.assign(centers, centers + (size_t)nb * D);
+  t.boxsize.assign(boxsize, boxsize + nlev + 1);
+  t.s0.resize(nb); t.s1.resize(nb); t.t0.resize(nb); t.t1.resize(nb);
+  for (int b = 0; b < nb; b++) {
+    t.s0[b] = isrcse[2 * b] - 1; t.s1[b] = isrcse[2 * b + 1];
+    t.t0[b] = itargse[2 * b] - 1; t.t1[b] = itargse[2 * b + 1];
+  }
+  t.isrc.resize(ns); t.itarg.resize(nt);
+  for (int i = 0; i < ns; i++) t.isrc[i] = i;
+  for (int i = 0; i < nt; i++) t.itarg[i] = i;
+  Params P0;
+  P0.dim = dim; P0.nd = *nd; P0.delta = *delta; P0.eps = *eps; P0.ns = ns; P0.nt = nt;
+  P0.ifpgh = *ifpgh; P0.ifpghtarg = *ifpghtarg; P0.npwlevel = *npwlevel;
+  std::vector<int> nl(nlocal, nlocal + nlev + 1);
+  try {
+    build_host_plan_from_tree(p->H, P0, nl, *pmax, *npw);
+  } catch (const std::bad_alloc&) {
+    return FGT_ERR_NOMEM;
+  }
+  CKS(cudaSetDevice(c->device));
+  st = plan_device(p.get());
+  if (st != FGT_OK) {
+    fgt_plan_destroy(p.release());
+    return st;
+  }
+  std::vector<double> po((size_t)ns * *nd), pt((size_t)nt * *nd);
+  st = fgt_plan_execute_host(p.get(), sourcesort, chargesort, targetsort, po.data(), pt.data());
+  fgt_plan_destroy(p.release());
+  if (st != FGT_OK) return st;
+  if (*ifpgh == 1 && pot)
+    for (size_t i = 0; i < po.size(); i++) pot[i] += po[i];
+  if (*ifpghtarg == 1 && pottarg)
+    for (size_t i = 0; i < pt.size(); i++) pottarg[i] += pt[i];
+  return FGT_OK;
+}
+
+extern "C" {
+
+int fgt2dmain_gpu_(const int* nd, const double* delta, const double* eps, const int* nsource,
+                   const double* sourcesort, const int* ifcharge, const double* chargesort,
+                   const int* ifdipole, const double* rnormalsort, const double* dipstrsort,
+                   const int* ntarget, const double* targetsort, const int* iaddr,
+                   const double* rmlexp, const int* itree, const int* ltree, const int* iptr,
+                   const int* nlevels, const int* npwlevel, const int* nboxes, const int* iper,
+                   const double* boxsize, const double* centers, const int* laddr,
+                   const int* isrcse, const int* itargse, const int* ntermsh, const int* nlocal,
+                   const int* ntermmax, const double* pmax, const int* npw, const int* ifpgh,
+                   double* pot, double* grad, double* hess, const int* ifpghtarg, double* pottarg,
+                   double* gradtarg, double* hesstarg) {
+  (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
+  (void)ntermsh; (void)ntermmax; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  return main_gpu<int>(2, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
+                       ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
+                       centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, ifpghtarg,
+                       pottarg);
+}
+
+int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const int* nsource,
+                   const double* sourcesort, const int* ifcharge, const double* chargesort,
+                   const int* ifdipole, const double* rnormalsort, const double* dipstrsort,
+                   const int* ntarget, const double* targetsort, const int* iaddr,
+                   const double* rmlexp, const int* itree, const long long* ltree,
+                   const long long* iptr, const int* nlevels, const int* npwlevel, const int* ndiv,
+                   const int* nboxes, const int* iper, const double* boxsize,
+                   const double* centers, const int* laddr, const int* isrcse,
+                   const int* itargse, const int* ntermsh, const int* nlocal, const int* ntermmax,
+                   const double* pmax, const int* npw, const int* ifpgh, double* pot, double* grad,
+                   double* hess, const int* ifpghtarg, double* pottarg, double* gradtarg,
+                   double* hesstarg) {
+  (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
+  (void)ndiv; (void)ntermsh; (void)ntermmax; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  return main_gpu<long long>(3, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
+                             ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
+                             centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot,
+                             ifpghtarg, pottarg);
+}
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// Device side of a plan: task arrays and tables resident in HBM, expansion
+// pools, scratch, and the stage launcher.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <vector>
+
+#include "fgt_plan.hpp"
+
+namespace fgtb {
+
+enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+struct MergeGroup {
+  int dst, beg, cnt;
+};
+
+struct StageTimes {
+  float ms[8];  // gather, form, merge, m2l, split, eval, direct, scatter
+};
+
+struct DevicePlan {
+  Params P;
+  int nboxes = 0, nch = 4;
+  // buffers (one allocation, carved)
+  char* base = nullptr;
+  size_t bytes = 0;
+  double* centers = nullptr;
+  double* h2x = nullptr;
+  double* x2l = nullptr;
+  double2* wms = nullptr;
+  double2* wsh = nullptr;
+  int* isrc = nullptr;
+  int* itarg = nullptr;
+  FormTask* form = nullptr;
+  int nform = 0;
+  std::vector<int> merge_beg, merge_end;  // host copies of group ranges per level
+  MergeGroup* mgroups = nullptr;
+  ShiftTask* merge = nullptr;
+  ShiftTask* split = nullptr;
+  std::vector<int> split_beg, split_end;
+  M2LTask* m2l = nullptr;
+  int nm2l = 0;
+  M2LNbr* m2l_nbr = nullptr;
+  EvalTask* eval = nullptr;
+  int neval = 0;
+  DirTask* dir = nullptr;
+  int ndir = 0;
+  SrcRange* dir_src = nullptr;
+  // pools and sorted data
+  double2* mp = nullptr;
+  double2* loc = nullptr;
+  int nmp = 0, nloc = 0;
+  double* ssort = nullptr;  // sorted sources (ns, dim)
+  double* csort = nullptr;  // sorted charges (ns, nd)
+  double* tsort = nullptr;  // sorted targets (nt, dim)
+  double* psort = nullptr;  // sorted pot (ns, nd)
+  double* ptsort = nullptr; // sorted pottarg (nt, nd)
+  double* local0 = nullptr; // large-delta local expansion
+  // per-CTA scratch of the 3D separable transforms
+  double2* scratch = nullptr;
+  size_t scratch_per_cta = 0;  // in double2
+  int scratch_ctas = 0;
+  // launch shapes
+  int form_hermite_n = 0, form_pw_n = 0;
+  int eval_taylor_n = 0, eval_pw_n = 0;
+  int form_pmax = 0, eval_pmax = 0;  // largest order among Hermite form / Taylor eval tasks
+  int sm_count = 148;
+  // statistics copied from the host plan
+  long long direct_pairs = 0, form_sources = 0, eval_points = 0;
+  long long launches = 0;
+};
+
+// Uploads the host plan; returns cudaSuccess or the first error.
+cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D);
+void device_plan_destroy(DevicePlan& D);
+
+// Runs gather -> stages -> scatter on `stream`.  Inputs and outputs are
+// device pointers in the caller's (unsorted) order: sources (ns, dim),
+// charge (ns, nd), targets (nt, dim), pot (ns, nd), pottarg (nt, nd).
+// times (optional) receives per-stage milliseconds (synchronises).
+cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* chg,
+                                const double* trg, double* pot, double* pottarg, int precision,
+                                cudaStream_t stream, StageTimes* times);
+
+// Large-delta path (one Taylor local about the root centre), no tree.
+cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
+                                const double* trg, double* pot, double* pottarg, double* work,
+                                cudaStream_t stream);
+
+}  // namespace fgtb

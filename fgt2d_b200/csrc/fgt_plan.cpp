@@ -1,0 +1,352 @@
+// Host plan construction: tree, lists, expansion lengths, translation tables
+// and the flattened task arrays of the four GPU stages.
+//
+// The set-up follows the driver and the start of the main routine of the
+// reference: fgt2d.f:125-400 / fgt2dmain fgt2d.f:695-857 (2D) and
+// fgt3d.f:127-414 / fgt3dmain fgt3d.f:690-900 (3D).
+#include "fgt_plan.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+
+namespace fgtb {
+
+namespace {
+typedef std::complex<double> cplx;
+double now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+// Translation tables and 1D matrices (pw_translation_matrices,
+// merge_split_pw_matrices, g2drh2xmat, g2drx2lmat and 3D twins).
+static void build_tables(HostPlan& H) {
+  Params& P = H.P;
+  const Tree& t = H.tree;
+  int D = P.dim, npw = P.npw, n2 = npw / 2, nch = 1 << D;
+  double pi = 4.0 * std::atan(1.0);
+  // get_pwnodes: 2D +half then -half (g2drouts.f:2205); 3D ascending (g3drouts.f:2669)
+  H.ts.assign(npw, 0.0);
+  H.ws.assign(npw, 0.0);
+  double h = P.pmax / n2, w = h / (2.0 * std::sqrt(pi));
+  for (int j = 0; j < npw; j++) {
+    double tj = D == 2 ? (j < n2 ? (j + 0.5) * h : -((j - n2) + 0.5) * h) : (j - n2 + 0.5) * h;
+    H.ts[j] = tj;
+    H.ws[j] = w * std::exp(-tj * tj / 4);
+  }
+  int tm = P.ntermmax;
+  H.h2x.assign((size_t)(tm + 1) * npw, 0.0);
+  H.x2l.assign((size_t)(tm + 1) * npw, 0.0);
+  {
+    std::vector<double> fac(tm + 1), fac2(tm + 1);
+    fac[0] = fac2[0] = 1;
+    for (int i = 1; i <= tm; i++) {
+      fac[i] = fac[i - 1] / std::sqrt((double)i);
+      fac2[i] = fac2[i - 1] * i;
+    }
+    for (int j = 0; j <= tm; j++)
+      for (int k = 0; k < npw; k++) {
+        H.h2x[(size_t)j * npw + k] = H.ws[k] * __builtin_powi(-H.ts[k], j) * fac[j];
+        H.x2l[(size_t)j * npw + k] = __builtin_powi(H.ts[k], j) / fac2[j];
+      }
+  }
+  // expansion index -> (kx, ky[, kz]) node indices, reference layouts:
+  // 2D pw(npw/2, npw): kx in the first half; 3D pw(npw, npw, npw/2).
+  size_t nexp = P.nexp;
+  auto node = [&](size_t e, int d) -> int {
+    if (D == 2) return d == 0 ? (int)(e % n2) : (int)(e / n2);
+    if (d == 0) return (int)(e % npw);
+    if (d == 1) return (int)((e / npw) % npw);
+    return (int)(e / ((size_t)npw * npw));
+  };
+  cplx I(0, 1);
+  // merge factors: child slot j merged into its parent, the parent-child
+  // offset at level l being boxsize(l+1)/2; ww(k) = exp(i t xmin2)^(2^(k-1))
+  // as in merge_split_pw_matrices (g2drouts.f:2326-2332).
+  int nms = std::max(P.nlevels - std::max(P.npwlevel, 0), 1);
+  double xmin2 = t.boxsize[P.nlevels] / std::sqrt(P.delta) / 2;
+  std::vector<cplx> ww((size_t)npw * (nms + 1));
+  for (int j = 0; j < npw; j++) {
+    cplx z = std::exp(I * H.ts[j] * xmin2);
+    for (int k = 1; k <= nms; k++) {
+      ww[(size_t)j * (nms + 1) + k] = z;
+      z = z * z;
+    }
+  }
+  // row (l * nch + j) for parents at level l: klev = nlevels - l
+  int nrow = (P.nlevels + 1) * nch;
+  H.wms.assign((size_t)nrow * nexp * 2, 0.0);
+  for (int l = std::max(P.nlevstart, 0); l <= P.nlevels - 1; l++) {
+    int klev = P.nlevels - l;
+    for (int jc = 0; jc < nch; jc++) {
+      double* W = H.wms.data() + ((size_t)l * nch + jc) * nexp * 2;
+      for (size_t e = 0; e < nexp; e++) {
+        cplx f = 1.0;
+        for (int d = 0; d < D; d++) {
+          // parent - child along d is negative when the child sits on the + side
+          cplx v = ww[(size_t)node(e, d) * (nms + 1) + klev];
+          f *= ((jc >> d) & 1) ? std::conj(v) : v;
+        }
+        W[2 * e] = f.real();
+        W[2 * e + 1] = f.imag();
+      }
+    }
+  }
+  // mp->loc factors, s = (jx+1) + 3 (jy+1) [+ 9 (jz+1)], xmin = boxsize(cut)
+  int ns3 = D == 2 ? 9 : 27;
+  H.wsh.assign((size_t)ns3 * nexp * 2, 0.0);
+  double xmin = (P.npwlevel >= 0 ? t.boxsize[P.npwlevel] : 0.0) / std::sqrt(P.delta);
+  std::vector<cplx> w1(npw);
+  for (int j = 0; j < npw; j++) w1[j] = std::exp(I * H.ts[j] * xmin);
+  for (int s = 0; s < ns3; s++) {
+    int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
+    double* W = H.wsh.data() + (size_t)s * nexp * 2;
+    for (size_t e = 0; e < nexp; e++) {
+      cplx f = 1.0;
+      for (int d = 0; d < D; d++) {
+        cplx v = w1[node(e, d)];
+        f *= o[d] == 0 ? cplx(1.0) : (o[d] > 0 ? v : std::conj(v));
+      }
+      W[2 * e] = f.real();
+      W[2 * e + 1] = f.imag();
+    }
+  }
+}
+
+// Flattens the tree into the stage task arrays.
+static void build_tasks(HostPlan& H) {
+  Params& P = H.P;
+  const Tree& t = H.tree;
+  const Lists& L = H.lists;
+  int nb = t.nboxes, D = P.dim, nch = t.nch;
+  int npl = P.npwlevel, nls = P.nlevstart;
+  auto relevant = [&](int b) {
+    return (P.ifpghtarg > 0 ? t.nt(b) : 0) + (P.ifpgh > 0 ? t.ns(b) : 0);
+  };
+  H.mp_slot.assign(nb, -1);
+  H.loc_slot.assign(nb, -1);
+  H.nmp = H.nloc = 0;
+  H.form.clear(); H.merge.clear(); H.split.clear(); H.m2l.clear(); H.m2l_nbr.clear();
+  H.eval.clear(); H.dir.clear(); H.dir_src.clear();
+  H.merge_beg.assign(P.nlevels + 1, 0);
+  H.merge_end.assign(P.nlevels + 1, 0);
+  H.split_beg.assign(P.nlevels + 1, 0);
+  H.split_end.assign(P.nlevels + 1, 0);
+  H.form_sources = H.eval_points = 0;
+  if (!P.all_direct) {
+    for (int l = nls; l <= P.nlevels; l++)
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        bool leaf = t.nchild[b] == 0;
+        if (t.ns(b) > 0 && !(leaf && l == npl)) H.mp_slot[b] = H.nmp++;
+        if (relevant(b) > 0 && !(leaf && l == npl && !L.iflocal[b])) H.loc_slot[b] = H.nloc++;
+      }
+    // (a) form, levels nlevels .. max(npwlevel+1, 0) (fgt2d.f:871)
+    for (int l = P.nlevels; l >= std::max(npl + 1, 0); l--) {
+      int p = H.nlocal[l];
+      int route = ROUTE_HERMITE;
+      if (D == 3) {
+        double r1 = (p + 1.0) / P.npw, r3 = r1 * r1 * r1;
+        route = r3 >= 3 ? ROUTE_PW : ROUTE_HERMITE;  // fgt3d.f:931-940
+      }
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (t.nchild[b] != 0 || t.ns(b) <= 0) continue;
+        int r = route;
+        if (D == 3 && route == ROUTE_PW && t.ns(b) > 1000000) r = ROUTE_HERMITE;
+        // a 3D Hermite block of more than 29^3 coefficients does not fit in
+        // shared memory; the exact exponential sum replaces it there
+        if (D == 3 && r == ROUTE_HERMITE && p + 1 > 29) r = ROUTE_PW;
+        H.form.push_back({b, t.s0[b], t.ns(b), H.mp_slot[b], p, r});
+        H.form_sources += t.ns(b);
+      }
+    }
+    // (b) merge, parents at levels nlevels-1 .. nlevstart
+    for (int l = P.nlevels - 1; l >= nls; l--) {
+      H.merge_beg[l] = (int)H.merge.size();
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (H.mp_slot[b] < 0 || t.nchild[b] == 0) continue;
+        for (int j = 0; j < nch; j++) {
+          int c = t.ch(b, j);
+          if (c >= 0 && H.mp_slot[c] >= 0) H.merge.push_back({H.mp_slot[b], H.mp_slot[c], l * nch + j});
+        }
+      }
+      H.merge_end[l] = (int)H.merge.size();
+    }
+    // (b) mp -> loc at the cut level
+    double xmin = npl >= 0 ? t.boxsize[npl] : 1.0;
+    for (int b = t.lfirst[nls]; b <= t.llast[nls]; b++) {
+      if (H.loc_slot[b] < 0) continue;
+      M2LTask mt{H.loc_slot[b], H.mp_slot[b], (int)H.m2l_nbr.size(), 0};
+      for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) {
+        int j = L.pw[k];
+        if (H.mp_slot[j] < 0) continue;
+        int s = 0, mul = 1;
+        for (int d = 0; d < D; d++) {
+          int o = (int)std::lround((t.c(b, d) - t.c(j, d)) / xmin);
+          s += (o + 1) * mul;
+          mul *= 3;
+        }
+        H.m2l_nbr.push_back({H.mp_slot[j], s});
+        mt.cnt++;
+      }
+      H.m2l.push_back(mt);
+    }
+    // (b) split, parents at levels nlevstart .. nlevels-1
+    for (int l = nls; l <= P.nlevels - 1; l++) {
+      H.split_beg[l] = (int)H.split.size();
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (H.loc_slot[b] < 0 || t.nchild[b] == 0) continue;
+        for (int j = 0; j < nch; j++) {
+          int c = t.ch(b, j);
+          if (c >= 0 && H.loc_slot[c] >= 0) H.split.push_back({H.loc_slot[c], H.loc_slot[b], l * nch + j});
+        }
+      }
+      H.split_end[l] = (int)H.split.size();
+    }
+    // (c) evaluation leaves (fgt2d.f:1141-1271 / fgt3d.f:1283-1446)
+    for (int l = nls; l <= P.nlevels; l++) {
+      int p = H.nlocal[l];
+      bool pw;
+      if (D == 2) pw = p > 50;
+      else {
+        double r1 = (p + 1.0) / P.npw, r3 = r1 * r1 * r1;
+        pw = r3 >= 3;
+      }
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (t.nchild[b] != 0 || H.loc_slot[b] < 0) continue;
+        if (l == npl && !L.iflocal[b]) continue;
+        int route = pw ? ROUTE_PW : ROUTE_TAYLOR;
+        if (D == 3 && pw && t.ns(b) + t.nt(b) >= 1000000) route = ROUTE_TAYLOR;
+        if (P.ifpghtarg == 1 && t.nt(b) > 0) {
+          H.eval.push_back({b, 1, t.t0[b], t.nt(b), H.loc_slot[b], p, route});
+          H.eval_points += t.nt(b);
+        }
+        if (P.ifpgh == 1 && t.ns(b) > 0) {
+          H.eval.push_back({b, 0, t.s0[b], t.ns(b), H.loc_slot[b], p, route});
+          H.eval_points += t.ns(b);
+        }
+      }
+    }
+  }
+  // (d) near field, target-centric: for every leaf, the ifhung source boxes
+  // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
+  std::vector<std::vector<int>> into(nb);  // box A -> source boxes S with A in list1(S)
+  int nlevend = npl < P.nlevels ? npl : P.nlevels;
+  for (int l = 0; l <= nlevend; l++)
+    for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
+      if (!L.ifhung[s]) continue;
+      for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[L.l1[k]].push_back(s);
+    }
+  const int CH = 128;
+  H.direct_pairs = 0;
+  for (int b = 0; b < nb; b++) {
+    if (t.nchild[b] != 0) continue;
+    std::vector<SrcRange> rs;
+    for (int a = b; a >= 0; a = t.parent[a])
+      for (int s : into[a]) rs.push_back({t.s0[s], t.ns(s)});
+    if (rs.empty()) continue;
+    long long nsrc = 0;
+    for (auto& r : rs) nsrc += r.n;
+    for (int set = 0; set < 2; set++) {
+      if (set == 0 && !(P.ifpgh == 1)) continue;
+      if (set == 1 && !(P.ifpghtarg == 1)) continue;
+      int i0 = set == 0 ? t.s0[b] : t.t0[b];
+      int n = set == 0 ? t.ns(b) : t.nt(b);
+      if (n == 0) continue;
+      int off = (int)H.dir_src.size();
+      H.dir_src.insert(H.dir_src.end(), rs.begin(), rs.end());
+      for (int c = 0; c < n; c += CH) H.dir.push_back({set, i0 + c, std::min(CH, n - c), off, (int)rs.size()});
+      H.direct_pairs += nsrc * n;
+    }
+  }
+  (void)D;
+}
+
+static void finish_plan(HostPlan& H) {
+  Params& P = H.P;
+  Tree& t = H.tree;
+  double t0 = now();
+  t.npwlevel = P.npwlevel;
+  build_lists(t, H.lists);
+  double t1 = now();
+  H.host_lists_s = t1 - t0;
+  if (!P.all_direct) build_tables(H);
+  build_tasks(H);
+  H.box_centers = t.centers;
+  H.host_plan_s = now() - t1;
+}
+
+int build_host_plan_from_tree(HostPlan& H, const Params& P0, const std::vector<int>& nlocal,
+                              double pmax, int npw) {
+  H.P = P0;
+  Params& P = H.P;
+  H.nlocal = nlocal;
+  P.pmax = pmax;
+  P.npw = npw;
+  P.nlevels = H.tree.nlevels;
+  P.nlevstart = std::max(P.npwlevel, 0);
+  P.all_direct = P.npwlevel >= P.nlevels;
+  P.nexp = P.dim == 2 ? npw * npw / 2 : npw * npw * npw / 2;
+  P.ntermmax = 0;
+  for (int v : nlocal) P.ntermmax = std::max(P.ntermmax, v);
+  P.dsq = 1.0 / std::sqrt(P.delta);
+  P.dmax = P.dim == 2 ? std::log(1.0 / (P.eps / 90)) * P.delta : std::log(1.0 / P.eps) * P.delta;
+  finish_plan(H);
+  return 0;
+}
+
+int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
+                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                    int nthreads) {
+  Params& P = H.P;
+  P = Params();
+  P.dim = dim; P.nd = nd; P.delta = delta; P.eps = eps; P.ns = ns; P.nt = nt;
+  P.ifpgh = ifpgh; P.ifpghtarg = ifpghtarg;
+  P.dsq = 1.0 / std::sqrt(delta);
+  P.dmax = dim == 2 ? std::log(1.0 / (eps / 90)) * delta : std::log(1.0 / eps) * delta;
+  double tstart = now();
+  int npwlevel;
+  double bs0, cen0[3] = {0, 0, 0};
+  boxsize0(dim, delta, eps, sources, ns, targ, nt, &npwlevel, &bs0, cen0);
+  P.npwlevel = npwlevel;
+  for (int d = 0; d < 3; d++) P.cen0[d] = cen0[d];
+  if (npwlevel < -2) {  // fgt2d.f:133-150: one Taylor local about the box centre
+    P.large_delta = true;
+    int nl0 = hlterms(dim, bs0, delta, eps, 0);
+    P.nlocal0 = nl0 + std::max(ifpgh, ifpghtarg) - 1;
+    H.host_tree_s = now() - tstart;
+    return 0;
+  }
+  int ndiv0 = dim == 2 ? 10 : 40, ndiv = dim == 2 ? 80 : 100, hcap = dim == 2 ? 18 : 15;
+  int nlmax = npwlevel + 4, nls = std::max(npwlevel, 0);
+  double bsize = bs0 / std::ldexp(1.0, nls);
+  int nl0 = 0;
+  for (int i = nls; i <= 100; i++) {  // fgt2d.f:175-186
+    nl0 = hlterms(dim, bsize, delta, eps, nl0);
+    if (nl0 <= hcap) { nlmax = i; break; }
+    bsize /= 2;
+  }
+  P.nlmax = nlmax;
+  build_tree(H.tree, dim, sources, ns, targ, nt, ndiv, ndiv0, npwlevel, nlmax, bs0, cen0, nthreads);
+  H.host_tree_s = now() - tstart;
+  Tree& t = H.tree;
+  P.nlevels = t.nlevels;
+  P.nlevstart = nls;
+  P.all_direct = npwlevel >= t.nlevels;
+  H.nlocal.assign(t.nlevels + 1, 0);
+  int nadd = std::max(ifpgh, ifpghtarg);
+  for (int i = nls; i <= t.nlevels; i++) {
+    H.nlocal[i] = hlterms(dim, t.boxsize[i], delta, eps, 0);
+    if (ifpgh >= 2 || ifpghtarg >= 2) H.nlocal[i] += nadd;
+  }
+  P.ntermmax = 0;
+  for (int v : H.nlocal) P.ntermmax = std::max(P.ntermmax, v);
+  double pweps = nadd > 2 ? eps / 100 : eps;
+  pwterms(2 * bs0 / std::pow(2.0, nls), delta, pweps, &P.pmax, &P.npw);
+  P.nexp = dim == 2 ? P.npw * P.npw / 2 : P.npw * P.npw * P.npw / 2;
+  finish_plan(H);
+  return 0;
+}
+
+}  // namespace fgtb

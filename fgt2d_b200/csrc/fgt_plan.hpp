@@ -1,0 +1,94 @@
+// Execution plan of one plane-wave FGT on one GPU: the host tree and lists
+// flattened into task arrays that the CUDA stages consume, plus the device
+// copies of those arrays and of the expansion pools.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <vector>
+
+#include "fgt_tree.hpp"
+
+namespace fgtb {
+
+enum Route { ROUTE_HERMITE = 0, ROUTE_PW = 1, ROUTE_TAYLOR = 0 };
+
+// stage (a): one formed leaf
+struct FormTask {
+  int box, s0, n, slot, p, route;
+};
+// stage (b) merge / split: one (parent, child) shift
+struct ShiftTask {
+  int dst, src, table;  // dst slot, src slot, table row (level * nch + child slot)
+};
+// stage (b) mp->loc: one cut-level box, its sources in [off, off+cnt) of the
+// neighbour array
+struct M2LTask {
+  int loc, self_mp, off, cnt;
+};
+struct M2LNbr {
+  int mp, shift;  // neighbour mp slot, translation index (jx+1)+3(jy+1)+9(jz+1)
+};
+// stage (c): one evaluation leaf and point set
+struct EvalTask {
+  int box, set, i0, n, slot, p, route;
+};
+// stage (d): a chunk of evaluation points and its source ranges
+struct DirTask {
+  int set, i0, n, off, cnt;
+};
+struct SrcRange {
+  int s0, n;
+};
+
+struct Params {
+  int dim = 2, nd = 1;
+  double delta = 0, eps = 0;
+  int ns = 0, nt = 0, ifpgh = 0, ifpghtarg = 0;
+  int npwlevel = 0, nlevels = 0, nlevstart = 0, nlmax = 0;
+  int npw = 0, nexp = 0, ntermmax = 0;
+  double pmax = 0, dsq = 0, dmax = 0;
+  bool large_delta = false, all_direct = false;
+  int nlocal0 = 0;  // large-delta local order
+  double cen0[3] = {0, 0, 0};
+};
+
+// Host side of the plan.
+struct HostPlan {
+  Params P;
+  Tree tree;
+  Lists lists;
+  std::vector<int> nlocal;        // per level
+  std::vector<double> ts, ws;     // reference node order for the dimension
+  std::vector<double> h2x;        // [j * npw + k] = ws_k (-ts_k)^j / sqrt(j!)
+  std::vector<double> x2l;        // [j * npw + k] = ts_k^j / j!
+  std::vector<double> wms;        // merge factors [(lev*nch + j) * nexp + e] (re,im)
+  std::vector<double> wsh;        // mp->loc factors [s * nexp + e] (re,im)
+  int nmp = 0, nloc = 0;
+  std::vector<int> mp_slot, loc_slot;  // per box, -1 when absent
+  std::vector<double> box_centers;     // dim per box
+  // tasks
+  std::vector<FormTask> form;
+  // merge / split tasks of parents at level l: [beg[l], end[l])
+  std::vector<int> merge_beg, merge_end;
+  std::vector<ShiftTask> merge;
+  std::vector<int> split_beg, split_end;
+  std::vector<ShiftTask> split;
+  std::vector<M2LTask> m2l;
+  std::vector<M2LNbr> m2l_nbr;
+  std::vector<EvalTask> eval;
+  std::vector<DirTask> dir;
+  std::vector<SrcRange> dir_src;
+  // statistics
+  long long direct_pairs = 0;
+  long long form_sources = 0, eval_points = 0;
+  double host_tree_s = 0, host_lists_s = 0, host_plan_s = 0;
+};
+
+int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
+                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                    int nthreads);
+// Fills the plan from a tree that was built outside (the fgt2dmain entry).
+int build_host_plan_from_tree(HostPlan& H, const Params& P0, const std::vector<int>& nlocal,
+                              double pmax, int npw);
+
+}  // namespace fgtb

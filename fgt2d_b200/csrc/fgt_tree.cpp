@@ -1,0 +1,549 @@
+// Host-side tree and lists; see fgt_tree.hpp.
+//
+// Point work (refinement bookkeeping, final point location and the stable
+// sort into tree order) is data-parallel over points with OpenMP; box work
+// (level restriction, colleagues, lists) follows the reference routines.
+#include "fgt_tree.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace fgtb {
+
+namespace {
+// Default-real (single precision) literals of the reference.
+const double F105 = (double)1.05f;  // tree_routs4.f:195, pts_tree2d4.f:959
+const double F109 = (double)1.09f;  // g2dterms.f:54
+inline double child_sign(int j, int d) { return ((j >> d) & 1) ? 1.0 : -1.0; }
+}  // namespace
+
+// g2dhlterms, g2dterms.f:19-64 (Wan-Karniadakis error bound)
+int hlterms(int ndim, double bsize, double delta, double eps, int nterms_default) {
+  double e1 = std::exp(1.0);
+  double r = bsize / std::sqrt(2.0 * delta);
+  int p0 = (int)(e1 * r * r) + 1;
+  double rk = F109 * std::pow(8 * std::atan(1.0), -0.25);
+  for (int p = p0; p <= 300; p++) {
+    double rp = r * std::sqrt(e1 / p);
+    double err = ndim * rk * std::pow((double)p, -0.25) * __builtin_powi(rp, p) / (1 - rp);
+    if (err < eps) return p;
+  }
+  return nterms_default;
+}
+
+// g2dpwterms, g2dterms.f:71-133 (Poisson summation: h = 2pi/(rmax+sqrt(ln 1/eps)))
+void pwterms(double bsize, double delta, double eps, double* pmax, int* npw) {
+  double pi = 4.0 * std::atan(1.0);
+  double rmax = bsize / std::sqrt(delta);
+  double d = std::sqrt(std::log(1.0 / eps));
+  *pmax = 2.0 * d;
+  double h = 2 * pi / (rmax + d);
+  *npw = 2 * (int)(*pmax / h);
+}
+
+void boxsize0(int dim, double delta, double eps, const double* src, int ns, const double* trg,
+              int nt, int* levcut, double* bs0, double* cen0) {
+  double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+  const double* first = ns > 0 ? src : trg;
+  for (int d = 0; d < dim; d++) mn[d] = mx[d] = first[d];
+  auto scan = [&](const double* x, int n) {
+    for (int d = 0; d < dim; d++) {
+      double lo = mn[d], hi = mx[d];
+#pragma omp parallel for reduction(min : lo) reduction(max : hi)
+      for (int i = 0; i < n; i++) {
+        double v = x[(size_t)dim * i + d];
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+      }
+      mn[d] = lo;
+      mx[d] = hi;
+    }
+  };
+  scan(src, ns);
+  scan(trg, nt);
+  double b = mx[0] - mn[0];
+  for (int d = 1; d < dim; d++)
+    if (mx[d] - mn[d] > b) b = mx[d] - mn[d];
+  for (int d = 0; d < dim; d++) cen0[d] = (mn[d] + mx[d]) / 2;
+  double dc = std::sqrt(delta * std::log(1.0 / eps));
+  double dl = std::log(b / dc) / std::log(2.0);
+  int lc = (int)dl;
+  *bs0 = b;
+  *levcut = lc;
+  if (b < dc) return;
+  *bs0 = std::ldexp(1.0, lc + 1) * dc;
+  *levcut = lc + 1;
+}
+
+namespace {
+
+struct Builder {
+  Tree& t;
+  int D, NCH, NCO;
+  explicit Builder(Tree& tt) : t(tt), D(tt.dim), NCH(tt.nch), NCO(tt.nco) {}
+
+  double& C(int b, int d) { return t.centers[(size_t)b * D + d]; }
+  int& CH(int b, int j) { return t.child[(size_t)b * NCH + j]; }
+
+  void reserve_boxes(int n) {
+    if ((int)t.level.size() >= n) return;
+    size_t m = std::max<size_t>(n, t.level.size() * 2);
+    t.level.resize(m, 0);
+    t.parent.resize(m, -1);
+    t.nchild.resize(m, 0);
+    t.child.resize(m * NCH, -1);
+    t.centers.resize(m * D, 0.0);
+  }
+
+  // Appends the children of box b (tree_refine_boxes, tree_routs4.f:28-49).
+  void make_children(int b, int first_child, int lev, double bs) {
+    t.nchild[b] = NCH;
+    for (int j = 0; j < NCH; j++) {
+      int c = first_child + j;
+      for (int d = 0; d < D; d++) C(c, d) = C(b, d) + child_sign(j, d) * bs / 2;
+      t.parent[c] = b;
+      t.nchild[c] = 0;
+      for (int l = 0; l < NCH; l++) CH(c, l) = -1;
+      CH(b, j) = c;
+      t.level[c] = lev;
+    }
+  }
+
+  // computecoll, tree_routs4.f:100-211, levels [l0, l1]
+  void colleagues_level(int l) {
+    double lim = F105 * t.boxsize[l];
+#pragma omp parallel for schedule(static)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+      int dad = t.parent[b];
+      int n = 0;
+      for (int i = 0; i < t.ncoll[dad]; i++) {
+        int jb = t.coll[(size_t)dad * NCO + i];
+        for (int j = 0; j < NCH; j++) {
+          int kb = CH(jb, j);
+          if (kb < 0) continue;
+          bool ok = true;
+          for (int d = 0; d < D; d++)
+            if (!(std::fabs(C(kb, d) - C(b, d)) <= lim)) ok = false;
+          if (ok) t.coll[(size_t)b * NCO + n++] = kb;
+        }
+      }
+      t.ncoll[b] = n;
+    }
+  }
+  void colleagues_all() {
+    t.ncoll.assign(t.nboxes, 0);
+    t.coll.assign((size_t)t.nboxes * NCO, -1);
+    t.ncoll[0] = 1;
+    t.coll[0] = 0;
+    for (int l = 1; l <= t.nlevels; l++) colleagues_level(l);
+  }
+
+  // tree_refine_boxes_flag, tree_routs4.f:334-388, over boxes ids[]
+  void refine_flagged(std::vector<int>& iflag, int a, int b, int lev) {
+    for (int box = a; box <= b; box++) {
+      if (iflag[box] <= 0) continue;
+      int c0 = t.nboxes;
+      reserve_boxes(c0 + NCH);
+      if ((int)iflag.size() < c0 + NCH) iflag.resize((size_t)(c0 + NCH) * 2, 0);
+      make_children(box, c0, lev + 1, t.boxsize[lev + 1]);
+      for (int j = 0; j < NCH; j++) iflag[c0 + j] = iflag[box] == 1 ? 3 : 0;
+      t.nboxes += NCH;
+    }
+  }
+
+  // pts_tree_reorg, pts_tree2d4.f:1001-1150: level l >= 2 becomes
+  // [old boxes of l] ++ [tail boxes of l].
+  void reorg(const std::vector<int>& tf, const std::vector<int>& tl, std::vector<int>& iflag) {
+    int nb = t.nboxes;
+    std::vector<int> map(nb, -1);
+    std::vector<int> olevel(t.level.begin(), t.level.begin() + nb);
+    std::vector<int> oparent(t.parent.begin(), t.parent.begin() + nb);
+    std::vector<int> onchild(t.nchild.begin(), t.nchild.begin() + nb);
+    std::vector<int> ochild(t.child.begin(), t.child.begin() + (size_t)nb * NCH);
+    std::vector<double> ocent(t.centers.begin(), t.centers.begin() + (size_t)nb * D);
+    std::vector<int> oflag(iflag.begin(), iflag.begin() + nb);
+    for (int l = 0; l <= std::min(1, t.nlevels); l++)
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) map[b] = b;
+    if (t.nlevels >= 2) {
+      int cur = t.lfirst[2];
+      for (int l = 2; l <= t.nlevels; l++) {
+        int a0 = t.lfirst[l], a1 = t.llast[l];
+        t.lfirst[l] = cur;
+        for (int pass = 0; pass < 2; pass++) {
+          int a = pass ? tf[l] : a0, b = pass ? tl[l] : a1;
+          for (int box = a; box <= b; box++) {
+            t.level[cur] = olevel[box];
+            t.nchild[cur] = onchild[box];
+            for (int d = 0; d < D; d++) t.centers[(size_t)cur * D + d] = ocent[(size_t)box * D + d];
+            iflag[cur] = oflag[box];
+            map[box] = cur++;
+          }
+        }
+        t.llast[l] = cur - 1;
+      }
+    }
+    for (int box = 0; box < nb; box++) {
+      int nbx = map[box];
+      t.parent[nbx] = oparent[box] >= 0 ? map[oparent[box]] : -1;
+      for (int j = 0; j < NCH; j++) {
+        int c = ochild[(size_t)box * NCH + j];
+        CH(nbx, j) = c >= 0 ? map[c] : -1;
+      }
+    }
+  }
+
+  bool touching(int a, int b, double lim) {
+    for (int d = 0; d < D; d++)
+      if (!(std::fabs(C(a, d) - C(b, d)) <= lim)) return false;
+    return true;
+  }
+
+  // pts_tree_fix_lr, pts_tree2d4.f:693-996
+  void fix_lr() {
+    int nlev = t.nlevels;
+    std::vector<int> iflag((size_t)t.nboxes * 2, 0);
+    for (int l = nlev; l >= 2; l--) {
+      double dist = 1.05 * (t.boxsize[l - 1] + t.boxsize[l - 2]) / 2.0;
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        int dad = t.parent[b], gd = t.parent[dad];
+        for (int i = 0; i < t.ncoll[gd]; i++) {
+          int jb = t.coll[(size_t)gd * NCO + i];
+          if (t.nchild[jb] == 0 && iflag[jb] == 0 && touching(jb, dad, dist)) iflag[jb] = 1;
+        }
+      }
+    }
+    for (int l = nlev; l >= 1; l--) {
+      double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (iflag[b] != 1 && iflag[b] != 2) continue;
+        int dad = t.parent[b];
+        for (int i = 0; i < t.ncoll[dad]; i++) {
+          int jb = t.coll[(size_t)dad * NCO + i];
+          if (t.nchild[jb] == 0 && iflag[jb] == 0 && touching(jb, b, dist)) iflag[jb] = 2;
+        }
+      }
+    }
+    std::vector<int> tf(nlev + 1, 0), tl(nlev + 1, -1);
+    for (int l = 1; l <= nlev - 2; l++) {
+      tf[l + 1] = t.nboxes;
+      refine_flagged(iflag, t.lfirst[l], t.llast[l], l);
+      tl[l + 1] = t.nboxes - 1;
+    }
+    reorg(tf, tl, iflag);
+    colleagues_all();
+    for (int b = 0; b < t.nboxes; b++)
+      if (iflag[b] != 3) iflag[b] = 0;
+    std::fill(tf.begin(), tf.end(), 0);
+    std::fill(tl.begin(), tl.end(), -1);
+    for (int l = 2; l <= nlev - 2; l++) {
+      update_flags(l, t.lfirst[l], t.llast[l], iflag);
+      update_flags(l, tf[l], tl[l], iflag);
+      tf[l + 1] = t.nboxes;
+      refine_flagged(iflag, t.lfirst[l], t.llast[l], l);
+      refine_flagged(iflag, tf[l], tl[l], l);
+      tl[l + 1] = t.nboxes - 1;
+      t.ncoll.resize(t.nboxes, 0);
+      t.coll.resize((size_t)t.nboxes * NCO, -1);
+      double lim = F105 * t.boxsize[l + 1];
+      for (int b = tf[l + 1]; b <= tl[l + 1]; b++) {
+        int dad = t.parent[b];
+        int n = 0;
+        for (int i = 0; i < t.ncoll[dad]; i++) {
+          int jb = t.coll[(size_t)dad * NCO + i];
+          for (int j = 0; j < NCH; j++) {
+            int kb = CH(jb, j);
+            if (kb >= 0 && touching(kb, b, lim)) t.coll[(size_t)b * NCO + n++] = kb;
+          }
+        }
+        t.ncoll[b] = n;
+      }
+    }
+    reorg(tf, tl, iflag);
+    colleagues_all();
+  }
+
+  // updateflags, tree_routs4.f:217-326
+  void update_flags(int lev, int a, int b, std::vector<int>& iflag) {
+    double dist = 1.05 * (t.boxsize[lev] + t.boxsize[lev + 1]) / 2.0;
+    for (int box = a; box <= b; box++) {
+      if (iflag[box] != 3) continue;
+      iflag[box] = 0;
+      for (int i = 0; i < t.ncoll[box] && iflag[box] == 0; i++) {
+        int jb = t.coll[(size_t)box * NCO + i];
+        for (int j = 0; j < NCH; j++) {
+          int kb = CH(jb, j);
+          if (kb >= 0 && t.nchild[kb] > 0 && touching(kb, box, dist)) { iflag[box] = 1; break; }
+        }
+      }
+    }
+  }
+};
+
+// Child slot of point x in box centre c (sort_pts_to_children: coordinate
+// minus centre < 0 goes to the lower child).
+inline int child_slot(const double* x, const double* c, int D) {
+  int j = 0;
+  for (int d = 0; d < D; d++)
+    if (!(x[d] - c[d] < 0)) j |= 1 << d;
+  return j;
+}
+
+// Locates every point in its leaf, then stable-sorts points by the leaf's
+// depth-first rank (the order pts_tree_sort produces) and fills the per-box
+// ranges.
+void sort_points(Tree& t, const double* x, int n, std::vector<int>& perm, std::vector<int>& r0,
+                 std::vector<int>& r1, const std::vector<int>& dfs_rank, int nleafrank,
+                 const std::vector<int>& leaf_of_rank) {
+  int D = t.dim;
+  std::vector<int> key(n);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    const double* p = x + (size_t)D * i;
+    int b = 0;
+    while (t.nchild[b] > 0) b = t.child[(size_t)b * t.nch + child_slot(p, &t.centers[(size_t)b * D], D)];
+    key[i] = dfs_rank[b];
+  }
+  // stable counting sort by key (per-thread histograms keep it stable)
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  if ((size_t)nth * nleafrank > (size_t)64 << 20) nth = std::max<int>(1, (64 << 20) / std::max(nleafrank, 1));
+  std::vector<int> cnt((size_t)nth * nleafrank, 0);
+  perm.assign(n, 0);
+#pragma omp parallel num_threads(nth)
+  {
+    int tid = 0, nt = 1;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+    nt = omp_get_num_threads();
+#endif
+    int lo = (int)((long long)n * tid / nt), hi = (int)((long long)n * (tid + 1) / nt);
+    int* c = cnt.data() + (size_t)tid * nleafrank;
+    for (int i = lo; i < hi; i++) c[key[i]]++;
+#pragma omp barrier
+#pragma omp single
+    {
+      long long run = 0;
+      for (int k = 0; k < nleafrank; k++)
+        for (int th = 0; th < nt; th++) {
+          int v = cnt[(size_t)th * nleafrank + k];
+          cnt[(size_t)th * nleafrank + k] = (int)run;
+          run += v;
+        }
+    }
+    for (int i = lo; i < hi; i++) perm[c[key[i]]++] = i;
+  }
+  // leaf ranges from the per-leaf counts, then internal boxes by DFS
+  std::vector<int> leafcount(nleafrank, 0);
+  for (int i = 0; i < n; i++) leafcount[key[i]]++;
+  r0.assign(t.nboxes, 0);
+  r1.assign(t.nboxes, 0);
+  int pos = 0;
+  for (int k = 0; k < nleafrank; k++) {
+    int b = leaf_of_rank[k];
+    r0[b] = pos;
+    pos += leafcount[k];
+    r1[b] = pos;
+  }
+  for (int l = t.nlevels; l >= 0; l--)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
+      if (t.nchild[b] > 0) {
+        r0[b] = r0[t.child[(size_t)b * t.nch]];
+        r1[b] = r1[t.child[(size_t)b * t.nch + t.nch - 1]];
+      }
+}
+
+}  // namespace
+
+void compute_colleagues(Tree& t) {
+  Builder B(t);
+  B.colleagues_all();
+}
+
+void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, int nt, int ndiv,
+                int ndiv0, int levcut, int nlmax, double bs0, const double* cen0, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  t = Tree();
+  t.dim = dim;
+  t.nch = 1 << dim;
+  t.nco = dim == 2 ? 9 : 27;
+  t.bs0 = bs0;
+  for (int d = 0; d < dim; d++) t.cen0[d] = cen0[d];
+  Builder B(t);
+  int NCH = t.nch, D = dim;
+  int maxlev = std::max(nlmax, 0);
+  t.boxsize.assign(maxlev + 2, 0.0);
+  t.lfirst.assign(maxlev + 2, 0);
+  t.llast.assign(maxlev + 2, -1);
+  B.reserve_boxes(1024);
+  t.boxsize[0] = bs0;
+  for (int d = 0; d < D; d++) B.C(0, d) = cen0[d];
+  t.level[0] = 0;
+  t.parent[0] = -1;
+  t.nchild[0] = 0;
+  t.lfirst[0] = 0;
+  t.llast[0] = 0;
+  t.nboxes = 1;
+
+  // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
+  std::vector<int> pbox(ns, 0);
+  std::vector<int> count(1, ns);
+  int lev;
+  for (lev = 0; lev <= nlmax - 1; lev++) {
+    int a = t.lfirst[lev], b = t.llast[lev];
+    int thr = lev < levcut ? ndiv0 : ndiv;
+    std::vector<int> firstchild(b - a + 1, -1);
+    int nref = 0;
+    for (int box = a; box <= b; box++)
+      if (count[box] > thr) firstchild[box - a] = t.nboxes + NCH * nref++;
+    if (nref == 0) break;
+    t.boxsize[lev + 1] = t.boxsize[lev] / 2;
+    B.reserve_boxes(t.nboxes + NCH * nref);
+    t.lfirst[lev + 1] = t.nboxes;
+    for (int box = a; box <= b; box++)
+      if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, t.boxsize[lev + 1]);
+    t.nboxes += NCH * nref;
+    t.llast[lev + 1] = t.nboxes - 1;
+    count.resize(t.nboxes, 0);
+    int* cnt = count.data();
+    const int* fc = firstchild.data();
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < ns; i++) {
+      int box = pbox[i];
+      if (box < a || box > b || fc[box - a] < 0) continue;
+      int c = fc[box - a] + child_slot(src + (size_t)D * i, &t.centers[(size_t)box * D], D);
+      pbox[i] = c;
+#pragma omp atomic
+      cnt[c]++;
+    }
+  }
+  t.nlevels = lev;
+  t.boxsize.resize(t.nlevels + 1);
+  t.lfirst.resize(t.nlevels + 1);
+  t.llast.resize(t.nlevels + 1);
+  B.colleagues_all();
+  if (t.nlevels >= 2) B.fix_lr();
+  t.level.resize(t.nboxes);
+  t.parent.resize(t.nboxes);
+  t.nchild.resize(t.nboxes);
+  t.child.resize((size_t)t.nboxes * NCH);
+  t.centers.resize((size_t)t.nboxes * D);
+
+  // depth-first rank of the leaves
+  std::vector<int> dfs_rank(t.nboxes, -1), leaf_of_rank;
+  leaf_of_rank.reserve(t.nboxes);
+  {
+    std::vector<int> stack;
+    stack.push_back(0);
+    while (!stack.empty()) {
+      int b = stack.back();
+      stack.pop_back();
+      if (t.nchild[b] == 0) {
+        dfs_rank[b] = (int)leaf_of_rank.size();
+        leaf_of_rank.push_back(b);
+      } else {
+        for (int j = NCH - 1; j >= 0; j--) stack.push_back(t.child[(size_t)b * NCH + j]);
+      }
+    }
+  }
+  int nl = (int)leaf_of_rank.size();
+  sort_points(t, src, ns, t.isrc, t.s0, t.s1, dfs_rank, nl, leaf_of_rank);
+  sort_points(t, trg, nt, t.itarg, t.t0, t.t1, dfs_rank, nl, leaf_of_rank);
+}
+
+void build_lists(const Tree& t, Lists& L) {
+  int nb = t.nboxes, NCO = t.nco, NCH = t.nch, D = t.dim;
+  int npw = t.npwlevel;
+  int nlevend = npw < t.nlevels ? npw : t.nlevels;
+  L.ifhung.assign(nb, 0);
+  for (int l = 0; l <= nlevend; l++)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
+      if (t.nchild[b] == 0 && t.ns(b) > 0) L.ifhung[b] = 1;
+  // modified list1: tree_routs4.f:715-879 (2D, symmetric insertion at
+  // coarse levels) / tree_routs3d.f:511-619 (3D, coarser leaf neighbours)
+  std::vector<std::vector<int>> l1(nb);
+  if (t.nchild[0] == 0) l1[0].push_back(0);
+  auto cdist = [&](int a, int b, int d) { return std::fabs(t.c(a, d) - t.c(b, d)); };
+  for (int l = 1; l <= t.nlevels; l++) {
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+      if (t.nchild[b] != 0) continue;
+      for (int i = 0; i < t.ncoll[b]; i++) {
+        int jb = t.coll[(size_t)b * NCO + i];
+        if (l >= npw || t.nchild[jb] == 0) {
+          l1[b].push_back(jb);
+          continue;
+        }
+        double dist = 1.05 * (t.boxsize[l] + t.boxsize[l + 1]) / 2.0;
+        for (int j = 0; j < NCH; j++) {
+          int kb = t.ch(jb, j);
+          if (kb < 0) continue;
+          bool near = true;
+          for (int d = 0; d < D; d++)
+            if (!(cdist(kb, b, d) < dist)) near = false;
+          if (near) {
+            l1[b].push_back(kb);
+            if (D == 2) l1[kb].push_back(b);
+          }
+        }
+      }
+      if (D == 3) {
+        int dad = t.parent[b];
+        double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+        for (int i = 0; i < t.ncoll[dad]; i++) {
+          int jb = t.coll[(size_t)dad * NCO + i];
+          if (t.nchild[jb] != 0) continue;
+          bool near = true;
+          for (int d = 0; d < D; d++)
+            if (!(cdist(jb, b, d) < dist)) near = false;
+          if (near) l1[b].push_back(jb);
+        }
+      }
+    }
+  }
+  L.l1off.assign(nb + 1, 0);
+  for (int b = 0; b < nb; b++) L.l1off[b + 1] = L.l1off[b] + (int)l1[b].size();
+  L.l1.resize(L.l1off[nb]);
+  for (int b = 0; b < nb; b++) std::copy(l1[b].begin(), l1[b].end(), L.l1.begin() + L.l1off[b]);
+
+  // plane-wave lists
+  L.pwoff.assign(nb + 1, 0);
+  L.pw.clear();
+  std::vector<std::vector<int>> pw(nb);
+  int nls = std::max(npw, 0);
+  for (int l = nls; l <= t.nlevels; l++)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+      if (l == npw) {
+        for (int i = 0; i < t.ncoll[b]; i++) {
+          int jb = t.coll[(size_t)b * NCO + i];
+          if (jb != b && (D == 2 || t.nchild[jb] > 0)) pw[b].push_back(jb);
+        }
+      } else if (l > nls) {
+        int dad = t.parent[b];
+        for (int j = 0; j < NCH; j++) {
+          int jb = t.ch(dad, j);
+          if (jb >= 0 && jb != b) pw[b].push_back(jb);
+        }
+      }
+    }
+  for (int b = 0; b < nb; b++) L.pwoff[b + 1] = L.pwoff[b] + (int)pw[b].size();
+  L.pw.resize(L.pwoff[nb]);
+  for (int b = 0; b < nb; b++) std::copy(pw[b].begin(), pw[b].end(), L.pw.begin() + L.pwoff[b]);
+
+  // iflocal: cut-level leaves with a non-leaf colleague (fgt2d.f:790-814)
+  L.iflocal.assign(nb, 0);
+  if (npw >= 0 && npw <= t.nlevels)
+    for (int b = t.lfirst[npw]; b <= t.llast[npw]; b++)
+      if (t.nchild[b] == 0)
+        for (int i = 0; i < t.ncoll[b]; i++)
+          if (t.nchild[t.coll[(size_t)b * NCO + i]] > 0) { L.iflocal[b] = 1; break; }
+}
+
+}  // namespace fgtb

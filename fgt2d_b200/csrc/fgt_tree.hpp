@@ -1,0 +1,65 @@
+// Host-side adaptive tree and interaction lists for the plane-wave FGT.
+//
+// Same tree and list semantics as the reference's host layer
+// (2d/planewave/src/common/pts_tree2d4.f, tree_routs4.f and the 3D twins
+// pts_tree3d.f, tree_routs3d.f): level-restricted 2^d-tree refined on source
+// counts, colleagues, modified list1, plane-wave list.  Box ids here are
+// 0-based; the reference's numbering order is kept (level by level, children
+// in parent order, level-restriction boxes appended per level), so box k here
+// is box k+1 there.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace fgtb {
+
+struct Tree {
+  int dim = 2, nch = 4, nco = 9;
+  int nlevels = 0, nboxes = 0;
+  int npwlevel = 0;
+  double bs0 = 0, cen0[3] = {0, 0, 0};
+  std::vector<int> lfirst, llast;          // boxes of level l: [lfirst[l], llast[l]]
+  std::vector<int> level, parent, nchild;  // per box
+  std::vector<int> child;                  // nch per box, -1 when absent
+  std::vector<int> ncoll, coll;            // colleagues (self included), nco per box
+  std::vector<double> centers;             // dim per box
+  std::vector<double> boxsize;             // per level
+  // sorted order: position -> original index (0-based)
+  std::vector<int> isrc, itarg;
+  // per box point ranges in sorted order, [start, end)
+  std::vector<int> s0, s1, t0, t1;
+
+  int ns(int b) const { return s1[b] - s0[b]; }
+  int nt(int b) const { return t1[b] - t0[b]; }
+  int ch(int b, int j) const { return child[(size_t)b * nch + j]; }
+  double c(int b, int d) const { return centers[(size_t)b * dim + d]; }
+};
+
+// Expansion-length rules, g2dterms.f:19-133 / g3dterms.f:13-127.
+int hlterms(int ndim, double bsize, double delta, double eps, int nterms_default);
+void pwterms(double bsize, double delta, double eps, double* pmax, int* npw);
+
+// Bounding box, cut level and enlarged root size, pts_tree2d4.f:1187-1258.
+void boxsize0(int dim, double delta, double eps, const double* src, int ns, const double* trg,
+              int nt, int* levcut, double* bs0, double* cen0);
+
+// Builds the tree for sources/targets given as (n, dim) row-major arrays and
+// sorts both point sets (pts_tree_mem/build/sort).  nthreads <= 0 uses all.
+void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, int nt, int ndiv,
+                int ndiv0, int levcut, int nlmax, double bs0, const double* cen0, int nthreads);
+
+// Interaction lists used by the transform (fgt2dmain / fgt3dmain set-up).
+struct Lists {
+  // modified list1 as CSR over source boxes (compute_modified_list1)
+  std::vector<int> l1off, l1;
+  // plane-wave list at the cut level and below (gt2d_computelistpw_slow /
+  // gt3d_computelistpw), CSR
+  std::vector<int> pwoff, pw;
+  std::vector<uint8_t> ifhung, iflocal;
+};
+void build_lists(const Tree& t, Lists& L);
+
+// Recomputes colleagues (computecoll) on a tree given from outside.
+void compute_colleagues(Tree& t);
+
+}  // namespace fgtb

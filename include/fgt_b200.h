@@ -1,0 +1,179 @@
+/*
+ * fgt_b200.h -- C ABI of the B200 plane-wave fast Gauss transform.
+ *
+ * The transform is the point-case plane-wave FGT of flatironinstitute/fgt2d
+ * (2d/planewave, 3d/planewave):
+ *
+ *     pot(x_t) = sum_s charge_s exp(-|x_t - x_s|^2 / delta)
+ *
+ * at the sources (ifpgh = 1) and/or at separate targets (ifpghtarg = 1), to
+ * precision eps.  Arrays follow the reference: column-major Fortran arrays,
+ * i.e. sources(dim, ns) is ns consecutive dim-tuples, charge(nd, ns) is ns
+ * consecutive nd-tuples, pot(nd, ns) likewise.  Every argument of the
+ * Fortran-named entry points is passed by reference.
+ *
+ * Supported now: ifcharge = 1, ifdipole = 0, ifpgh and ifpghtarg in {0, 1},
+ * any nd >= 1.  Other flag values return FGT_ERR_UNSUPPORTED.
+ *
+ * All entry points return a status (FGT_OK or an error code below) except
+ * fgt2d_ / fgt3d_, which keep the reference's subroutine signature and
+ * report a failure on stderr; fgt2d_st_ / fgt3d_st_ add a trailing status.
+ */
+#ifndef FGT_B200_H
+#define FGT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FGT_OK = 0,
+  FGT_ERR_BADARG = 1,      /* nd < 1, delta <= 0, eps not in (0,1), n < 0, NaN */
+  FGT_ERR_UNSUPPORTED = 2, /* dipoles, gradients/Hessians, orders too large */
+  FGT_ERR_NOMEM = 3,       /* device or host allocation failed */
+  FGT_ERR_CUDA = 4,        /* CUDA runtime error (see fgt_last_cuda_error) */
+  FGT_ERR_NODEVICE = 5     /* no CUDA device */
+};
+
+enum {
+  FGT_PREC_FP64 = 0,  /* everything in FP64 (the plain form) */
+  FGT_PREC_MIXED = 1, /* FP32 SFU exponentials in the near field, FP64 accumulation */
+  FGT_PREC_AUTO = 2   /* MIXED when eps >= 1e-6, FP64 otherwise (default) */
+};
+
+typedef struct fgt_ctx fgt_ctx;
+typedef struct fgt_plan fgt_plan;
+
+typedef struct fgt_plan_info {
+  int dim, nd, ns, nt;
+  int npwlevel, nlevels, nboxes, npw, nexp, nlmax;
+  int nform, neval, ndirect_tasks, nmp, nloc;
+  long long direct_pairs, form_sources, eval_points;
+  long long device_bytes;
+  double host_tree_s, host_lists_s, host_plan_s;
+  int large_delta, all_direct;
+  int kernel_launches;
+} fgt_plan_info;
+
+/* ---- context: one device, its stream and default precision -------------- */
+int fgt_ctx_create(int device, fgt_ctx** out);
+int fgt_ctx_destroy(fgt_ctx* ctx);
+int fgt_ctx_set_precision(fgt_ctx* ctx, int precision);
+int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
+/* the context used by the Fortran-named entry points (device 0, created on
+ * first use) */
+fgt_ctx* fgt_default_ctx(void);
+
+/* ---- whole transform from host arrays ------------------------------------
+ * Replaces fgt2d (2d/planewave/src/fgt2d.f:19-462) and fgt3d
+ * (3d/planewave/src/fgt3d.f:19-477): argument meaning, array layouts and
+ * output semantics are the reference's (outputs are overwritten). */
+int fgt_transform(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                  const double* sources, int ifcharge, const double* charge, int ifdipole,
+                  const double* rnormal, const double* dipstr, int ifpgh, double* pot, double* grad,
+                  double* hess, int nt, const double* targ, int ifpghtarg, double* pottarg,
+                  double* gradtarg, double* hesstarg);
+
+/* gfortran-ABI drop-ins for `call fgt2d(...)` / `call fgt3d(...)`
+ * (fgt2d.f:19-22, fgt3d.f:19-22); all arguments by reference. */
+void fgt2d_(const int* nd, const double* delta, const double* eps, const int* ns,
+            const double* sources, const int* ifcharge, const double* charge, const int* ifdipole,
+            const double* rnormal, const double* dipstr, const int* iper, const int* ifpgh,
+            double* pot, double* grad, double* hess, const int* nt, const double* targ,
+            const int* ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg);
+void fgt3d_(const int* nd, const double* delta, const double* eps, const int* ns,
+            const double* sources, const int* ifcharge, const double* charge, const int* ifdipole,
+            const double* rnormal, const double* dipstr, const int* iper, const int* ifpgh,
+            double* pot, double* grad, double* hess, const int* nt, const double* targ,
+            const int* ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg);
+/* the same with a trailing status argument */
+void fgt2d_st_(const int* nd, const double* delta, const double* eps, const int* ns,
+               const double* sources, const int* ifcharge, const double* charge,
+               const int* ifdipole, const double* rnormal, const double* dipstr, const int* iper,
+               const int* ifpgh, double* pot, double* grad, double* hess, const int* nt,
+               const double* targ, const int* ifpghtarg, double* pottarg, double* gradtarg,
+               double* hesstarg, int* ier);
+void fgt3d_st_(const int* nd, const double* delta, const double* eps, const int* ns,
+               const double* sources, const int* ifcharge, const double* charge,
+               const int* ifdipole, const double* rnormal, const double* dipstr, const int* iper,
+               const int* ifpgh, double* pot, double* grad, double* hess, const int* nt,
+               const double* targ, const int* ifpghtarg, double* pottarg, double* gradtarg,
+               double* hesstarg, int* ier);
+
+/* ---- the GPU main at the reference's host/device cut ---------------------
+ * fgt2dmain (fgt2d.f:468-478) / fgt3dmain (fgt3d.f:483-493): tree-sorted
+ * arrays and the reference's own tree (itree/iptr as built by pts_tree_build,
+ * 1-based box ids).  iaddr/rmlexp are accepted and ignored: the device keeps
+ * its own expansion pool.  Outputs are incremented, as in the reference.
+ * 2D: iptr and ltree are default integers; 3D: integer*8 (fgt3d.f:643-645). */
+int fgt2dmain_gpu_(const int* nd, const double* delta, const double* eps, const int* nsource,
+                   const double* sourcesort, const int* ifcharge, const double* chargesort,
+                   const int* ifdipole, const double* rnormalsort, const double* dipstrsort,
+                   const int* ntarget, const double* targetsort, const int* iaddr,
+                   const double* rmlexp, const int* itree, const int* ltree, const int* iptr,
+                   const int* nlevels, const int* npwlevel, const int* nboxes, const int* iper,
+                   const double* boxsize, const double* centers, const int* laddr,
+                   const int* isrcse, const int* itargse, const int* ntermsh, const int* nlocal,
+                   const int* ntermmax, const double* pmax, const int* npw, const int* ifpgh,
+                   double* pot, double* grad, double* hess, const int* ifpghtarg, double* pottarg,
+                   double* gradtarg, double* hesstarg);
+int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const int* nsource,
+                   const double* sourcesort, const int* ifcharge, const double* chargesort,
+                   const int* ifdipole, const double* rnormalsort, const double* dipstrsort,
+                   const int* ntarget, const double* targetsort, const int* iaddr,
+                   const double* rmlexp, const int* itree, const long long* ltree,
+                   const long long* iptr, const int* nlevels, const int* npwlevel, const int* ndiv,
+                   const int* nboxes, const int* iper, const double* boxsize,
+                   const double* centers, const int* laddr, const int* isrcse,
+                   const int* itargse, const int* ntermsh, const int* nlocal, const int* ntermmax,
+                   const double* pmax, const int* npw, const int* ifpgh, double* pot, double* grad,
+                   double* hess, const int* ifpghtarg, double* pottarg, double* gradtarg,
+                   double* hesstarg);
+
+/* ---- plans: build the tree once, apply many times ------------------------
+ * A plan fixes the points (sources, targets), delta, eps and flags.  The
+ * execute calls take charges (and, for the device variant, the same point
+ * coordinates already resident in device memory) and write the outputs. */
+int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                    fgt_plan** out);
+/* host arrays in and out; copies inside the call */
+int fgt_plan_execute_host(fgt_plan* plan, const double* sources, const double* charge,
+                          const double* targ, double* pot, double* pottarg);
+/* device pointers in the caller's order; runs on `stream` (a cudaStream_t,
+ * NULL for the context stream) and returns without synchronising */
+int fgt_plan_execute_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
+                            const double* d_targ, double* d_pot, double* d_pottarg, void* stream);
+/* per-stage device milliseconds of one synchronous execute on device data:
+ * gather, form, merge, mp->loc, split, eval, direct, scatter */
+int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
+                            const double* d_targ, double* d_pot, double* d_pottarg, float* ms8);
+int fgt_plan_get_info(const fgt_plan* plan, fgt_plan_info* info);
+int fgt_plan_destroy(fgt_plan* plan);
+
+/* ---- host tree (no device needed) ----------------------------------------
+ * The level-restricted tree the transform builds (pts_tree_boxsize0,
+ * pts_tree_mem/build/sort: pts_tree2d4.f:34-1258, pts_tree3d.f:34-1685),
+ * exposed in the reference's conventions: 1-based box ids, laddr(2,0:nlevels),
+ * per-box ranges isrcse(2,nboxes) and the sort permutations isrc/itarg. */
+typedef struct fgt_host_tree fgt_host_tree;
+int fgt_host_tree_create(int dim, double delta, double eps, int ns, const double* sources, int nt,
+                         const double* targ, int nthreads, fgt_host_tree** out);
+/* dims[0..3] = nlevels, nboxes, npwlevel, nlmax; returns FGT_ERR_UNSUPPORTED
+ * for the large-delta case, which builds no tree */
+int fgt_host_tree_dims(const fgt_host_tree* t, int* dims);
+/* field: 0 laddr, 1 ilevel, 2 iparent, 3 nchild, 4 ichild, 5 nnbors, 6 nbors,
+ * 7 isrc, 8 isrcse, 9 itarg, 10 itargse (int); 11 centers, 12 boxsize (double).
+ * Returns the element count; copies when out != NULL. */
+long long fgt_host_tree_field(const fgt_host_tree* t, int field, void* out);
+int fgt_host_tree_destroy(fgt_host_tree* t);
+
+/* ---- status -------------------------------------------------------------- */
+const char* fgt_status_string(int status);
+int fgt_last_cuda_error(void);
+const char* fgt_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FGT_B200_H */

@@ -1,0 +1,155 @@
+"""GPU parity: the CUDA transform against the oracle (the restated reference)
+and against the FP64 direct sum, through the C ABI.
+
+Bars (relative l2, the reference test's ``derr``):
+  * FP64 plain form vs oracle: <= 1e-2 * eps  (same routes, rounding-level)
+  * mixed form vs oracle:      <= eps          (north-star parity bar)
+  * both forms vs direct sum:  <= 10 * eps     (the reference's own accuracy)
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NSAMPLE = 400
+
+
+def _cases():
+    rng = np.random.default_rng(20240601)
+    out = []
+
+    def unif(n, d):
+        return rng.random((n, d))
+
+    def circle(n):
+        th = rng.random(n) * 2 * np.pi
+        r = 0.3 + rng.normal(0, 1e-3, n)
+        pts = np.c_[0.5 + r * np.cos(th), 0.5 + r * np.sin(th)]
+        k = n // 10
+        pts[:k] = rng.random((k, 2))
+        return pts
+
+    def blobs(n):
+        c = rng.random((16, 3)) * 0.8 + 0.1
+        lab = rng.integers(0, 16, n)
+        p = c[lab] + rng.normal(0, 0.02, (n, 3))
+        m = rng.random(n) < 0.2
+        p[m] = rng.random((int(m.sum()), 3))
+        return p
+
+    # name, dim, nd, delta, eps, sources, targets, ifpgh, ifpghtarg
+    n = 60000
+    out.append(("2d_unif_d1e-4_e1e-9", 2, 1, 1e-4, 1e-9, unif(n, 2), unif(n, 2), 1, 1))
+    out.append(("2d_unif_d1e-4_e1e-6", 2, 1, 1e-4, 1e-6, unif(n, 2), unif(n, 2), 1, 1))
+    c = circle(120000)
+    out.append(("2d_circle_d1e-6_e1e-6", 2, 1, 1e-6, 1e-6, c, c.copy(), 1, 0))
+    out.append(("2d_circle_targets_only", 2, 1, 3e-6, 1e-6, circle(40000), circle(30000), 0, 1))
+    out.append(("2d_unif_nd2_e1e-3", 2, 2, 1e-3, 1e-3, unif(30000, 2), unif(20000, 2), 1, 1))
+    b = blobs(40000)
+    out.append(("3d_blobs_d1e-3_e1e-6", 3, 1, 1e-3, 1e-6, b, blobs(30000), 0, 1))
+    out.append(("3d_unif_d1e-2_e1e-3", 3, 1, 1e-2, 1e-3, unif(20000, 3), unif(20000, 3), 1, 1))
+    out.append(("3d_unif_d1e-2_e1e-6", 3, 1, 1e-2, 1e-6, unif(20000, 3), unif(10000, 3), 1, 1))
+    out.append(("3d_unif_d1e-4_e1e-9", 3, 1, 1e-4, 1e-9, unif(30000, 3), unif(10000, 3), 1, 1))
+    out.append(("3d_unif_nd2_d1e-3", 3, 2, 1e-3, 1e-6, unif(20000, 3), unif(5000, 3), 1, 1))
+    # all-direct (cut level at or below the finest level) and large delta
+    out.append(("2d_alldirect", 2, 1, 1e-6, 1e-6, unif(3000, 2), unif(2000, 2), 1, 1))
+    out.append(("3d_alldirect", 3, 1, 1e-4, 1e-6, unif(3000, 3), unif(2000, 3), 1, 1))
+    out.append(("2d_large_delta", 2, 1, 10.0, 1e-6, unif(3000, 2), unif(2000, 2), 1, 1))
+    out.append(("3d_large_delta", 3, 1, 10.0, 1e-6, unif(3000, 3), unif(2000, 3), 1, 1))
+    # root box just below the cut-off length (npwlevel in {-2,-1,0})
+    for name, d, s in (("2d_npw_m1", 2, 0.25), ("2d_npw_m2", 2, 0.12), ("3d_npw_0", 3, 0.7)):
+        dlt = 1e-2
+        pts = unif(4000, d) * s
+        out.append((name, d, 1, dlt, 1e-6, pts, unif(3000, d) * s, 1, 1))
+    return out
+
+
+CASES = _cases()
+
+
+def _charges(rng, n, nd, signed):
+    q = rng.random((n, nd))
+    return 2 * q - 1 if signed else q
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_parity(case, precision, fgt, oracle):
+    name, dim, nd, delta, eps, src, trg, ifpgh, ifpghtarg = case
+    if precision == "mixed" and eps < 1e-6:
+        pytest.skip("the mixed form applies at eps >= 1e-6")
+    rng = np.random.default_rng(hash(name) & 0xFFFF)
+    q = _charges(rng, src.shape[0], nd, signed="blob" in name)
+    ctx = fgt.Context(0, precision=precision)
+    pot, pt = fgt.transform(dim, nd, delta, eps, src, q, trg, ifpgh, ifpghtarg, ctx=ctx)
+    opot, opt, info = oracle.fgt(dim, nd, delta, eps, src, q, trg, ifpgh, ifpghtarg)
+    tol_ref = 1e-2 * eps if precision == "fp64" else eps
+    if ifpgh:
+        e_ref = oracle.derr(opot, pot)
+        idx = rng.choice(src.shape[0], min(NSAMPLE, src.shape[0]), replace=False)
+        ex = oracle.direct(dim, nd, delta, src, q, src[idx])
+        e_dir = oracle.derr(ex, pot[idx])
+        print(f"{name} {precision} src: vs oracle {e_ref:.2e} vs direct {e_dir:.2e} {info}")
+        assert e_ref <= tol_ref, (e_ref, tol_ref)
+        assert e_dir <= 10 * eps, e_dir
+    if ifpghtarg:
+        e_ref = oracle.derr(opt, pt)
+        idx = rng.choice(trg.shape[0], min(NSAMPLE, trg.shape[0]), replace=False)
+        ex = oracle.direct(dim, nd, delta, src, q, trg[idx])
+        e_dir = oracle.derr(ex, pt[idx])
+        print(f"{name} {precision} trg: vs oracle {e_ref:.2e} vs direct {e_dir:.2e}")
+        assert e_ref <= tol_ref, (e_ref, tol_ref)
+        assert e_dir <= 10 * eps, e_dir
+
+
+def test_reference_test_inputs_2d(fgt, oracle):
+    """The reference 2D driver's inputs (hkrand stream, pinned sources, delta,
+    eps = 5e-11), scaled to 20000 points, first 20 sources checked as there."""
+    src, q, trg, delta, eps = oracle.reference_test_inputs_2d(20000)
+    pot, _ = fgt.fgt2d(1, delta, eps, src, q, trg, 1, 0, ctx=fgt.Context(0, "fp64"))
+    ex = oracle.direct(2, 1, delta, src, q, src[:20])
+    assert oracle.derr(ex, pot[:20]) <= 10 * eps
+    opot, _, _ = oracle.fgt(2, 1, delta, eps, src, q, trg, 1, 0)
+    assert oracle.derr(opot, pot) <= 1e-2 * eps
+
+
+def test_reference_test_inputs_3d(fgt, oracle):
+    src, q, trg, delta, eps = oracle.reference_test_inputs_3d(20000)
+    pot, _ = fgt.fgt3d(1, delta, eps, src, q, trg, 1, 0, ctx=fgt.Context(0, "fp64"))
+    ex = oracle.direct(3, 1, delta, src, q, src[:20])
+    assert oracle.derr(ex, pot[:20]) <= 10 * eps
+    opot, _, _ = oracle.fgt(3, 1, delta, eps, src, q, trg, 1, 0)
+    assert oracle.derr(opot, pot) <= 1e-2 * eps
+
+
+def test_edge_cases(fgt, oracle):
+    ctx = fgt.Context(0, "fp64")
+    # one source, one target: a root box far below the Gaussian width takes
+    # the large-delta Taylor path (fgt2d.f:133-150), accurate to eps
+    p, t = fgt.fgt2d(1, 1e-3, 1e-6, [[0.5, 0.5]], [2.0], [[0.51, 0.5]], 1, 1, ctx=ctx)
+    assert abs(p[0, 0] - 2.0) < 2e-6
+    assert abs(t[0, 0] - 2.0 * np.exp(-1e-4 / 1e-3)) < 2e-6
+    # duplicated points and points on box centres
+    rng = np.random.default_rng(3)
+    base = rng.random((500, 2))
+    src = np.concatenate([base, base, np.full((50, 2), 0.5)])
+    q = rng.random(src.shape[0])
+    pot, _ = fgt.fgt2d(1, 1e-4, 1e-6, src, q, None, 1, 0, ctx=ctx)
+    ex = oracle.direct(2, 1, 1e-4, src, q, src)
+    assert oracle.derr(ex, pot) <= 1e-5
+    # empty source set returns zeros
+    p, t = fgt.fgt2d(1, 1e-3, 1e-6, np.zeros((0, 2)), np.zeros(0), rng.random((5, 2)), 0, 1, ctx=ctx)
+    assert np.all(t == 0)
+
+
+def test_bad_arguments(fgt):
+    ctx = fgt.Context(0)
+    with pytest.raises(fgt.FGTError) as e:
+        fgt.fgt2d(1, -1.0, 1e-6, [[0.1, 0.2]], [1.0], ctx=ctx)
+    assert e.value.status == 1
+    with pytest.raises(fgt.FGTError) as e:
+        fgt.fgt2d(1, 1e-3, 1e-6, [[np.nan, 0.2]], [1.0], ctx=ctx)
+    assert e.value.status == 1
+    with pytest.raises(fgt.FGTError) as e:
+        fgt.transform(2, 1, 1e-3, 1e-6, [[0.1, 0.2]], [1.0], ifpgh=2, ctx=ctx)
+    assert e.value.status == 2
