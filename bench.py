@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 plane-wave FGT on its headline workload.
+
+Metric: FGT points/s at eps = 1e-6 (mixed form; the FP64 plain form is timed
+beside it on the same GPU).  Workload (default): the 2D strongly clustered
+adaptive-tree case -- N = 1e7 sources = targets, 90% on a circle of radius 0.3
+about (0.5, 0.5) with Gaussian radial jitter sigma = 1e-3, 10% uniform in the
+unit square, charges N(0,1), delta = 1e-6, eps = 1e-6, potential at the
+sources (ifpgh = 1, ifpghtarg = 0); seeded synthetic data.
+
+points/s = (ns + targets evaluated) / time.  ``value`` times one execute of a
+prebuilt plan with inputs resident in HBM (gather -> form -> merge -> mp->loc
+-> split -> eval -> near field -> scatter); ``e2e`` times the drop-in call
+(host tree and lists, host->device copies from pinned memory, transform,
+device->host copy of the potentials).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--workload cfg2|cfg1|cfg3|cfg4_d1e-2_e1e-6|...]
+Multi-GPU (N > 1, torchrun): independent replicas, one per rank.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+# ------------------------------------------------------------------ workloads
+def make_workload(name: str, seed: int):
+    rng = np.random.default_rng(seed)
+    if name in ("cfg2", "cfg2_n2e6"):
+        n = 10_000_000 if name == "cfg2" else 2_000_000
+        m = int(0.9 * n)
+        th = rng.random(m) * 2 * np.pi
+        r = 0.3 + rng.normal(0.0, 1e-3, m)
+        p = np.empty((n, 2))
+        p[:m, 0] = 0.5 + r * np.cos(th)
+        p[:m, 1] = 0.5 + r * np.sin(th)
+        p[m:] = rng.random((n - m, 2))
+        q = rng.standard_normal(n)
+        return dict(name=f"2d_circle_clustered_N{n:.0e}_d1e-6_e1e-6".replace("+0", ""), dim=2, nd=1, delta=1e-6, eps=1e-6,
+                    src=p, chg=q, trg=p, ifpgh=1, ifpghtarg=0)
+    if name == "cfg1":
+        n = 100_000
+        return dict(name="2d_uniform_N1e5+1e5_d1e-4_e1e-9", dim=2, nd=1, delta=1e-4, eps=1e-9,
+                    src=rng.random((n, 2)), chg=rng.random(n), trg=rng.random((n, 2)), ifpgh=1,
+                    ifpghtarg=1)
+    if name in ("cfg3", "cfg3_n5e5"):
+        n = 4_000_000 if name == "cfg3" else 500_000
+        c = rng.random((16, 3)) * 0.8 + 0.1
+
+        def pts(k):
+            lab = rng.integers(0, 16, k)
+            x = c[lab] + rng.normal(0, 0.02, (k, 3))
+            u = rng.random(k) < 0.2
+            x[u] = rng.random((int(u.sum()), 3))
+            return x
+
+        return dict(name=f"3d_blobs_N{n:.0e}+{n:.0e}_d1e-3_e1e-6".replace("+0", ""), dim=3, nd=1, delta=1e-3, eps=1e-6,
+                    src=pts(n), chg=2 * rng.random(n) - 1, trg=pts(n), ifpgh=0, ifpghtarg=1)
+    if name.startswith("cfg4"):
+        _, d, e = name.split("_")
+        n = 2_000_000
+        x = rng.random((n, 3))
+        return dict(name=f"3d_uniform_N2e6_{d}_{e}", dim=3, nd=1, delta=float(d[1:]),
+                    eps=float(e[1:]), src=x, chg=rng.random(n), trg=x, ifpgh=1, ifpghtarg=0)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def points_of(w):
+    return w["src"].shape[0] * (1 if w["ifpgh"] else 0) + (w["trg"].shape[0] if w["ifpghtarg"] else 0)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.lines: list[str] = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_oracle(w, nthreads, sample_n=None, seed=0):
+    from oracle import oracle as O
+    O.build()
+    src, chg, trg = w["src"], w["chg"], w["trg"]
+    if sample_n is not None and sample_n < src.shape[0]:
+        rng = np.random.default_rng(seed)
+        idx = rng.choice(src.shape[0], sample_n, replace=False)
+        same = trg is src
+        src, chg = src[idx], chg[idx]
+        trg = src if same else trg[rng.choice(trg.shape[0], min(sample_n, trg.shape[0]), replace=False)]
+    t0 = time.perf_counter()
+    O.fgt(w["dim"], w["nd"], w["delta"], w["eps"], src, chg, trg, w["ifpgh"], w["ifpghtarg"],
+          nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    pts = src.shape[0] * (1 if w["ifpgh"] else 0) + (trg.shape[0] if w["ifpghtarg"] else 0)
+    return pts, dt, src.shape[0]
+
+
+# ------------------------------------------------------------------ arms
+def reference_arm(args, w, rank, world):
+    if rank != 0:
+        return 0
+    cores = cpu_cores()
+    sample = min(2_000_000, w["src"].shape[0])
+    for i in range(args.warmup):
+        run_oracle(w, cores, sample, seed=i)
+    times, pts = [], 0
+    for i in range(args.steps):
+        p, dt, _ = run_oracle(w, cores, sample, seed=100 + i)
+        times.append(dt)
+        pts = p
+    ms = 1e3 * sum(times) / len(times)
+    v = pts / (ms / 1e3)
+    line = {"impl": "reference", "metric": "FGT points/s at eps 1e-6", "value": v,
+            "unit": "points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded numpy)",
+            "config": {"workload": w["name"], "sample_points": sample, "eps": w["eps"],
+                       "delta": w["delta"]},
+            "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
+                             "sample": f"random {sample}-point subset of the workload per step, "
+                                       f"oracle (C++ restatement of the reference) on {cores} threads"},
+            "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ours_arm(args, w, rank, world, local_rank):
+    import torch
+    import fgt2d_b200 as F
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+    pts = points_of(w)
+    dim, nd = w["dim"], w["nd"]
+
+    # plan (host tree + lists + device tasks), built once per precision
+    ctx = {p: F.Context(dev, precision=p) for p in ("mixed", "fp64")}
+    t0 = time.perf_counter()
+    plan = F.Plan(ctx["mixed"], dim, nd, w["delta"], w["eps"], w["src"], w["trg"], w["ifpgh"],
+                  w["ifpghtarg"])
+    plan_s = time.perf_counter() - t0
+    info = plan.info()
+    d_src = torch.from_numpy(np.ascontiguousarray(w["src"])).to(f"cuda:{dev}")
+    d_chg = torch.from_numpy(np.ascontiguousarray(w["chg"]).reshape(-1, nd)).to(f"cuda:{dev}")
+    d_trg = d_src if w["trg"] is w["src"] else torch.from_numpy(np.ascontiguousarray(w["trg"])).to(f"cuda:{dev}")
+    d_pot = torch.zeros((w["src"].shape[0], nd), dtype=torch.float64, device=f"cuda:{dev}")
+    d_pt = torch.zeros((w["trg"].shape[0], nd), dtype=torch.float64, device=f"cuda:{dev}")
+    # a dedicated stream: the plan's kernels and the timing events share it
+    stream = torch.cuda.Stream(dev)
+    sp = stream.cuda_stream
+
+    def step(precision):
+        ctx["mixed"].set_precision(precision)
+        plan.execute_device(d_src.data_ptr(), d_chg.data_ptr(), d_trg.data_ptr(),
+                            d_pot.data_ptr(), d_pt.data_ptr(), stream=sp)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    clocks = None
+    for prec in ("fp64", "mixed"):  # mixed last: its clocks are the headline's
+        for _ in range(args.warmup):
+            step(prec)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(dev) if prec == "mixed" else None
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(prec)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        if sampler is not None:
+            clocks = sampler.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        results[prec] = max_over_ranks(ms)
+    # per-stage device times (CUDA events around each stage, on the plan's
+    # stream) over K further steps of each precision
+    stages = {}
+    for prec in ("fp64", "mixed"):
+        ctx["mixed"].set_precision(prec)
+        acc = {}
+        for _ in range(args.steps):
+            s = plan.profile_device(d_src.data_ptr(), d_chg.data_ptr(), d_trg.data_ptr(),
+                                    d_pot.data_ptr(), d_pt.data_ptr())
+            for k, v in s.items():
+                acc[k] = acc.get(k, 0.0) + v / args.steps
+        stages[prec] = acc
+    stage = stages["mixed"]
+    launches_per_step = plan.info()["kernel_launches"]
+
+    # end to end through the public API from pinned host memory
+    src_h = torch.from_numpy(np.ascontiguousarray(w["src"])).pin_memory().numpy()
+    chg_h = torch.from_numpy(np.ascontiguousarray(w["chg"]).reshape(-1, nd)).pin_memory().numpy()
+    trg_h = src_h if w["trg"] is w["src"] else torch.from_numpy(np.ascontiguousarray(w["trg"])).pin_memory().numpy()
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    ctx["mixed"].set_precision("mixed")
+    e2e_s = float("nan")
+    if e2e_steps:
+        F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"], w["ifpghtarg"],
+                    ctx=ctx["mixed"])
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"],
+                        w["ifpghtarg"], ctx=ctx["mixed"])
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+    h2d = src_h.nbytes + chg_h.nbytes + (trg_h.nbytes if w["ifpghtarg"] else 0)
+    d2h = (w["src"].shape[0] * nd * 8 if w["ifpgh"] else 0) + (w["trg"].shape[0] * nd * 8 if w["ifpghtarg"] else 0)
+
+    if rank != 0:
+        return 0
+    hbm, tf, peak_src = measured_peaks()
+    # roofline of the dominant kernel of the headline step
+    names = {"form": "form", "merge": "merge", "m2l": "m2l", "split": "split", "eval": "eval",
+             "direct": "direct", "gather": "gather", "scatter": "scatter"}
+    dom = max(stage, key=lambda k: stage[k])
+    sb = info["shift_bytes"]
+    work = {
+        "merge": ("hbm", sb[0] / 1e9, "GB/s"), "m2l": ("hbm", sb[1] / 1e9, "GB/s"),
+        "split": ("hbm", sb[2] / 1e9, "GB/s"),
+        "gather": ("hbm", (w["src"].shape[0] * (dim * 16 + nd * 16 + 4)) / 1e9, "GB/s"),
+        "scatter": ("hbm", (w["src"].shape[0] * nd * 16 + w["src"].shape[0] * 4) / 1e9, "GB/s"),
+    }
+    roof = None
+    if dom in work:
+        bound, amount, unit = work[dom]
+        ach = amount / (stage[dom] / 1e3)
+        roof = {"bound": bound, "kernel": dom, "achieved": ach, "peak": hbm, "unit": unit,
+                "frac": ach / hbm, "traffic": None, "peak_source": peak_src}
+    else:
+        # compute-bound stages are reported against the HBM roofline of their
+        # streamed bytes; the pair / flop rates are given beside it
+        if dom == "direct":
+            streamed = (info["direct_pairs"] * 0) + w["src"].shape[0] * (dim + nd + 1) * 8
+        else:
+            streamed = w["src"].shape[0] * (dim + nd) * 8 + (info["nmp"] + info["nloc"]) * info["nexp"] * 16
+        ach = streamed / 1e9 / (stage[dom] / 1e3)
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "traffic": None, "peak_source": peak_src,
+                "pairs_per_s": info["direct_pairs"] / (stage["direct"] / 1e3) if stage.get("direct") else None}
+    cpu_base = None
+    if world == 1 and not args.no_cpu_baseline:
+        cores = cpu_cores()
+        p_cpu, dt_cpu, n_cpu = run_oracle(w, cores)
+        cpu_base = {"value": p_cpu / dt_cpu, "unit": "points/s", "cores": cores, "kind": "port",
+                    "sample": f"the full workload once ({n_cpu} sources), oracle (C++ restatement "
+                              f"of the reference plane-wave FGT) on {cores} threads, {dt_cpu:.1f} s"}
+    ms_mixed, ms_fp64 = results["mixed"], results["fp64"]
+    line = {
+        "metric": "FGT points/s at eps 1e-6 (mixed form)",
+        "value": world * pts / (ms_mixed / 1e3),
+        "unit": "points/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (near-field exp in f32)", "data": "synthetic (seeded numpy)",
+        "config": {"workload": w["name"], "points_per_step": pts, "ifpgh": w["ifpgh"],
+                   "ifpghtarg": w["ifpghtarg"], "l2": "inputs 240 MB > 126 MB L2 (no flush)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64_form": {"value": world * pts / (ms_fp64 / 1e3), "ms_per_step": ms_fp64,
+                      "mixed_over_fp64": ms_fp64 / ms_mixed},
+        "stages_ms": stage,
+        "stages_ms_fp64": stages["fp64"],
+        "plan": {k: info[k] for k in ("npwlevel", "nlevels", "nboxes", "npw", "nexp", "nform",
+                                      "neval", "ndirect_tasks", "direct_pairs", "device_bytes")},
+        "host_plan_s": plan_s,
+        "e2e": {"value": world * pts / e2e_s, "unit": "points/s", "s_per_step": e2e_s,
+                "steps": e2e_steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "includes": "host tree + lists + plan upload + H2D + transform + D2H"},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu_base,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    w = make_workload(args.workload, seed=1234 + 2 + 7919 * rank)
+    if args.impl == "reference":
+        return reference_arm(args, w, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            return ours_arm(args, w, rank, world, local_rank)
+        finally:
+            dist.destroy_process_group()
+    return ours_arm(args, w, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -53,10 +53,14 @@ class PlanInfo(ctypes.Structure):
                 ("eval_points", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
                 ("host_tree_s", ctypes.c_double), ("host_lists_s", ctypes.c_double),
                 ("host_plan_s", ctypes.c_double), ("large_delta", ctypes.c_int),
-                ("all_direct", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
+                ("all_direct", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("shift_bytes", ctypes.c_longlong * 3), ("form_flops", ctypes.c_double),
+                ("eval_flops", ctypes.c_double)]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_}
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["shift_bytes"] = list(self.shift_bytes)
+        return d
 
 
 def lib():
@@ -73,6 +77,8 @@ def lib():
     L.fgt_ctx_set_precision.argtypes = [_vp, i]
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
     L.fgt_default_ctx.restype = _vp
+    L.fgt_ctx_stream.restype = _vp
+    L.fgt_ctx_stream.argtypes = [_vp]
     L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,
                                 _dp, i, _dp, _dp, _dp]
     L.fgt_plan_create.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, ctypes.POINTER(_vp)]
@@ -126,6 +132,11 @@ class Context:
     @property
     def handle(self):
         return self._h
+
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer."""
+        return lib().fgt_ctx_stream(self._h)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -188,7 +199,7 @@ class Plan:
         self.ifpgh, self.ifpghtarg = ifpgh, ifpghtarg
         h = _vp()
         _check(L.fgt_plan_create(ctx.handle, dim, nd, float(delta), float(eps), self.ns, _p(src),
-                                 self.nt, _p(trg), ifpgh, ifpghtarg, ctx and ctypes.byref(h)),
+                                 self.nt, _p(trg), ifpgh, ifpghtarg, ctypes.byref(h)),
                "fgt_plan_create")
         self._h = h
 

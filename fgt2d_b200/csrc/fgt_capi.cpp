@@ -83,7 +83,7 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
   return FGT_OK;
 }
 
-int plan_device(fgt_plan* p) {
+int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   const Params& P = p->H.P;
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
   size_t n_src = ns * dim, n_chg = ns * nd, n_trg = nt * dim, n_pot = ns * nd, n_pt = nt * nd;
@@ -102,23 +102,27 @@ int plan_device(fgt_plan* p) {
   p->d_pot = c; c += al(n_pot);
   p->d_pottarg = c; c += al(n_pt);
   p->d_work = c;
+  cudaStream_t st = p->ctx->stream;
+  if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
+  if (nt > 0 && P.ifpghtarg > 0) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
   if (!P.large_delta) {
     CKS(device_plan_create(p->H, p->D));
     p->have_device = true;
+    CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, st));
   }
   return FGT_OK;
 }
 
-int run_device(fgt_plan* p, const double* s, const double* q, const double* t, double* pot,
-               double* pt, cudaStream_t st, StageTimes* times) {
+int run_device(fgt_plan* p, const double* q, double* pot, double* pt, cudaStream_t st,
+               StageTimes* times) {
   const Params& P = p->H.P;
   int prec = resolve_precision(p->ctx, P.eps);
   if (P.large_delta) {
-    CKS(large_delta_execute(P, s, q, t, pot, pt, p->d_work, st));
+    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, pot, pt, p->d_work, st));
     p->last_launches = (P.ns > 0) + (P.ifpgh == 1) + (P.ifpghtarg == 1);
     return FGT_OK;
   }
-  CKS(device_plan_execute(p->D, s, q, t, pot, pt, prec, st, times));
+  CKS(device_plan_execute(p->D, q, pot, pt, prec, st, times));
   p->last_launches = (int)p->D.launches;
   return FGT_OK;
 }
@@ -203,6 +207,7 @@ int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
   c->nthreads = nthreads;
   return FGT_OK;
 }
+void* fgt_ctx_stream(fgt_ctx* c) { return c ? (void*)c->stream : nullptr; }
 fgt_ctx* fgt_default_ctx(void) {
   std::call_once(g_default_once, [] {
     fgt_ctx* c = nullptr;
@@ -228,7 +233,7 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
     return FGT_ERR_NOMEM;
   }
   CKS(cudaSetDevice(ctx->device));
-  st = plan_device(p.get());
+  st = plan_device(p.get(), sources, targ);
   if (st != FGT_OK) {
     fgt_plan_destroy(p.release());
     return st;
@@ -252,11 +257,10 @@ int fgt_plan_execute_host(fgt_plan* p, const double* sources, const double* char
   const Params& P = p->H.P;
   cudaStream_t st = p->ctx->stream;
   CKS(cudaSetDevice(p->ctx->device));
+  (void)sources; (void)targ;  // fixed at plan creation
   size_t ns = P.ns, nt = P.nt;
-  CKS(cudaMemcpyAsync(p->d_src, sources, ns * P.dim * 8, cudaMemcpyHostToDevice, st));
   CKS(cudaMemcpyAsync(p->d_chg, charge, ns * P.nd * 8, cudaMemcpyHostToDevice, st));
-  if (P.ifpghtarg == 1 && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, targ, nt * P.dim * 8, cudaMemcpyHostToDevice, st));
-  int s = run_device(p, p->d_src, p->d_chg, p->d_trg, p->d_pot, p->d_pottarg, st, nullptr);
+  int s = run_device(p, p->d_chg, p->d_pot, p->d_pottarg, st, nullptr);
   if (s != FGT_OK) return s;
   if (P.ifpgh == 1 && pot) CKS(cudaMemcpyAsync(pot, p->d_pot, ns * P.nd * 8, cudaMemcpyDeviceToHost, st));
   if (P.ifpghtarg == 1 && nt > 0 && pottarg)
@@ -270,7 +274,8 @@ int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const
   if (!p) return FGT_ERR_BADARG;
   CKS(cudaSetDevice(p->ctx->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
-  return run_device(p, s, q, t, pot, pt, st, nullptr);
+  (void)s; (void)t;  // the points are fixed at plan creation
+  return run_device(p, q, pot, pt, st, nullptr);
 }
 
 int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const double* t,
@@ -279,7 +284,8 @@ int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const
   CKS(cudaSetDevice(p->ctx->device));
   StageTimes T;
   memset(&T, 0, sizeof(T));
-  int r = run_device(p, s, q, t, pot, pt, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
+  (void)s; (void)t;
+  int r = run_device(p, q, pot, pt, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
   if (r != FGT_OK) return r;
   CKS(cudaStreamSynchronize(p->ctx->stream));
   for (int i = 0; i < 8; i++) ms8[i] = T.ms[i];
@@ -302,6 +308,10 @@ int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
   o->host_plan_s = p->H.host_plan_s;
   o->large_delta = P.large_delta; o->all_direct = P.all_direct;
   o->kernel_launches = p->last_launches;
+  for (int i = 0; i < 3; i++) o->shift_bytes[i] = p->H.shift_bytes[i];
+  double npwd = std::pow((double)P.npw, P.dim);
+  o->form_flops = 4.0 * (double)p->H.form_sources * npwd;
+  o->eval_flops = 4.0 * (double)p->H.eval_points * npwd;
   return FGT_OK;
 }
 
@@ -530,7 +540,7 @@ static int main_gpu(int dim, const int* nd, const double* delta, const double* e
     return FGT_ERR_NOMEM;
   }
   CKS(cudaSetDevice(c->device));
-  st = plan_device(p.get());
+  st = plan_device(p.get(), sourcesort, targetsort);
   if (st != FGT_OK) {
     fgt_plan_destroy(p.release());
     return st;

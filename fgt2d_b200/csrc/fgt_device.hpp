@@ -16,6 +16,10 @@ struct MergeGroup {
   int dst, beg, cnt;
 };
 
+struct OrderGroup {
+  int p, beg, end;  // tasks [beg, end) of expansion order p
+};
+
 struct StageTimes {
   float ms[8];  // gather, form, merge, m2l, split, eval, direct, scatter
 };
@@ -31,8 +35,12 @@ struct DevicePlan {
   double* x2l = nullptr;
   double2* wms = nullptr;
   double2* wsh = nullptr;
-  int* isrc = nullptr;
+  int* isrc = nullptr;       // sorted position -> caller index
   int* itarg = nullptr;
+  int* isrc_inv = nullptr;   // caller index -> sorted position
+  int* itarg_inv = nullptr;
+  double* isq = nullptr;     // 1/sqrt(j), j = 0..ntermmax+1
+  double* cfac = nullptr;    // 1/sqrt(j!), j < 32
   FormTask* form = nullptr;
   int nform = 0;
   std::vector<int> merge_beg, merge_end;  // host copies of group ranges per level
@@ -58,7 +66,15 @@ struct DevicePlan {
   double* psort = nullptr;  // sorted pot (ns, nd)
   double* ptsort = nullptr; // sorted pottarg (nt, nd)
   double* local0 = nullptr; // large-delta local expansion
-  // per-CTA scratch of the 3D separable transforms
+  // 3D Hermite form in two kernels: source chunks and their partial blocks
+  FormChunk* fchunks = nullptr;
+  int nfchunks = 0;
+  int* fcbeg = nullptr;      // per Hermite form task, first chunk (size n+1)
+  double* hbuf = nullptr;    // partial Hermite blocks
+  bool form3_smem = false, eval3_smem = false;
+  size_t form3_shA = 0, form3_shB = 0, eval3_sh = 0;
+  int form3_sub = 64;
+  // per-CTA scratch of the 3D separable transforms (fallback path)
   double2* scratch = nullptr;
   size_t scratch_per_cta = 0;  // in double2
   int scratch_ctas = 0;
@@ -66,6 +82,7 @@ struct DevicePlan {
   int form_hermite_n = 0, form_pw_n = 0;
   int eval_taylor_n = 0, eval_pw_n = 0;
   int form_pmax = 0, eval_pmax = 0;  // largest order among Hermite form / Taylor eval tasks
+  std::vector<OrderGroup> form_groups, eval_groups;
   int sm_count = 148;
   // statistics copied from the host plan
   long long direct_pairs = 0, form_sources = 0, eval_points = 0;
@@ -76,13 +93,15 @@ struct DevicePlan {
 cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D);
 void device_plan_destroy(DevicePlan& D);
 
-// Runs gather -> stages -> scatter on `stream`.  Inputs and outputs are
-// device pointers in the caller's (unsorted) order: sources (ns, dim),
-// charge (ns, nd), targets (nt, dim), pot (ns, nd), pottarg (nt, nd).
+// Sorts the plan's points into tree order once: device arrays in the
+// caller's order, sources (ns, dim) and targets (nt, dim).
+cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const double* trg,
+                                   cudaStream_t stream);
+// Runs charge gather -> stages -> scatter on `stream`.  Device pointers in
+// the caller's order: charge (ns, nd), pot (ns, nd), pottarg (nt, nd).
 // times (optional) receives per-stage milliseconds (synchronises).
-cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* chg,
-                                const double* trg, double* pot, double* pottarg, int precision,
-                                cudaStream_t stream, StageTimes* times);
+cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
+                                int precision, cudaStream_t stream, StageTimes* times);
 
 // Large-delta path (one Taylor local about the root centre), no tree.
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
+#include <cstdint>
 #include <cstring>
 
 #include "fgt_device.hpp"
@@ -28,7 +30,6 @@ namespace fgtb {
 namespace {
 
 constexpr int FORM_CH = 32;    // sources staged per chunk in the form kernels
-constexpr int DIR_T = 128;     // threads (targets) per near-field task
 
 struct KP {
   int dim, nd, npw, n2, nexp;
@@ -90,94 +91,120 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 // ------------------------------------------------------------ sort / unsort
-__global__ void k_gather(const double* __restrict__ in, double* __restrict__ out,
-                         const int* __restrict__ perm, long long n, int w) {
-  long long tot = n * w;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long r = i / w;
-    int c = (int)(i - r * w);
-    out[i] = in[(long long)perm[r] * w + c];
+// Tree order: out row i = in row perm[i] (dreorderf, fmmcommon2d.f:3-26);
+// coordinates and charges of a point move together.
+__global__ void k_gather_pts(const double* __restrict__ x, const double* __restrict__ q,
+                             double* __restrict__ xs, double* __restrict__ qs,
+                             const int* __restrict__ perm, int n, int dim, int nd, int vec) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long p = perm[i];
+    if (x == nullptr) {
+    } else if (dim == 2 && vec) {
+      reinterpret_cast<double2*>(xs)[i] = reinterpret_cast<const double2*>(x)[p];
+    } else {
+      for (int d = 0; d < dim; d++) xs[(long long)i * dim + d] = x[p * dim + d];
+    }
+    if (q)
+      for (int c = 0; c < nd; c++) qs[(long long)i * nd + c] = q[p * nd + c];
   }
 }
-__global__ void k_scatter(const double* __restrict__ in, double* __restrict__ out,
-                          const int* __restrict__ perm, long long n, int w) {
-  long long tot = n * w;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long r = i / w;
-    int c = (int)(i - r * w);
-    out[(long long)perm[r] * w + c] = in[i];
+// Caller order: out row j = in row iperm[j] (dreorderi, fmmcommon2d.f:29-56),
+// written as a gather so the stores stay coalesced.
+__global__ void k_unsort(const double* __restrict__ in, double* __restrict__ out,
+                         const int* __restrict__ iperm, int n, int nd) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const long long p = iperm[j];
+    for (int c = 0; c < nd; c++) out[(long long)j * nd + c] = in[p * nd + c];
   }
 }
 
 // ------------------------------------------------------------ (a) form, 2D
-// One CTA per (leaf, density).  H[j + P k] = sum_i q_i x_i^j y_i^k / sqrt(j! k!)
-// accumulated in registers (MAXE entries per thread), then the two 1D
-// Hermite -> plane-wave passes in shared memory (g2drouts.f:1276-1326).
-template <int MAXE>
-__global__ void __launch_bounds__(256) k_form2d_hermite(KP k, const FormTask* __restrict__ tasks) {
+// One CTA (256 threads) per (leaf, density).
+//   H[j + Pp k] = sum_i q_i x_i^j y_i^k / sqrt(j! k!)      (g2dformhc_vec)
+// is a small (P x n) * (n x P) product: the rows x^j/sqrt(j!) and
+// q y^k/sqrt(k!) of a chunk of sources are built in shared memory with the
+// 1/sqrt(j) table, each thread keeps a 4x4 register tile of H and the chunk's
+// sources are split over G thread groups (split-K), reduced at the end.  Then
+// the two 1D Hermite -> plane-wave passes (g2dh2pw_real_vec,
+// g2drouts.f:1276-1326) run in shared memory.
+__global__ void __launch_bounds__(256) k_form2d(KP k, const FormTask* __restrict__ tasks,
+                                                const double* __restrict__ isq, int ch) {
   const FormTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
-  const int Pn = T.p + 1, n2 = k.n2, npw = k.npw, nent = Pn * Pn;
+  const int Pn = T.p + 1, n2 = k.n2, npw = k.npw;
+  const int tpd = (Pn + 3) >> 2, Pp = tpd * 4, ntiles = tpd * tpd;
+  const int G = 256 / ntiles;
   extern __shared__ double sm[];
-  double* xs = sm;
-  double* ys = xs + FORM_CH * Pn;
-  double* H = ys + FORM_CH * Pn;
-  double2* px = reinterpret_cast<double2*>(H + ((nent + 1) & ~1));
+  double* xs = sm;                     // [ch][Pp]
+  double* ys = xs + ch * Pp;           // [ch][Pp]
+  double* part = ys + ch * Pp;         // [G][Pp*Pp]
+  double* H = part;                    // reduced H overwrites group 0
+  double2* px = reinterpret_cast<double2*>(part + G * Pp * Pp);  // [Pn][n2]
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
-  double acc[MAXE];
-  int oj[MAXE], ok[MAXE];
+  const int tid = threadIdx.x, tile = tid % ntiles, g = tid / ntiles;
+  const int jb = (tile % tpd) * 4, kb = (tile / tpd) * 4;
+  double acc[4][4];
 #pragma unroll
-  for (int s = 0; s < MAXE; s++) {
-    int e = threadIdx.x + s * 256;
-    acc[s] = 0.0;
-    oj[s] = e % Pn;
-    ok[s] = e / Pn;
-  }
-  for (int c0 = 0; c0 < T.n; c0 += FORM_CH) {
-    const int m = min(FORM_CH, T.n - c0);
-    if (threadIdx.x < m) {
-      const int i = T.s0 + c0 + threadIdx.x;
-      const double x = (k.src[2 * i] - cx) * k.dsq, y = (k.src[2 * i + 1] - cy) * k.dsq;
-      double* xr = xs + threadIdx.x * Pn;
-      double* yr = ys + threadIdx.x * Pn;
-      double xv = 1.0, yv = k.chg[(size_t)i * k.nd + ind];
-      xr[0] = xv;
-      yr[0] = yv;
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  for (int c0 = 0; c0 < T.n; c0 += ch) {
+    const int m = min(ch, T.n - c0);
+    for (int r = tid; r < 2 * m; r += 256) {
+      const int t = r >> 1, kind = r & 1;
+      const int i = T.s0 + c0 + t;
+      double v, w;
+      if (kind == 0) { v = (k.src[2 * i] - cx) * k.dsq; w = 1.0; }
+      else { v = (k.src[2 * i + 1] - cy) * k.dsq; w = k.chg[(size_t)i * k.nd + ind]; }
+      double* row = (kind ? ys : xs) + t * Pp;
+      row[0] = w;
       for (int j = 1; j < Pn; j++) {
-        double sj = sqrt((double)j);
-        xv = xv * x / sj;
-        yv = yv * y / sj;
-        xr[j] = xv;
-        yr[j] = yv;
+        w = w * v * isq[j];
+        row[j] = w;
+      }
+      for (int j = Pn; j < Pp; j++) row[j] = 0.0;
+    }
+    __syncthreads();
+    if (g < G) {
+      for (int t = g; t < m; t += G) {
+        const double2 x01 = *reinterpret_cast<const double2*>(xs + t * Pp + jb);
+        const double2 x23 = *reinterpret_cast<const double2*>(xs + t * Pp + jb + 2);
+        const double2 y01 = *reinterpret_cast<const double2*>(ys + t * Pp + kb);
+        const double2 y23 = *reinterpret_cast<const double2*>(ys + t * Pp + kb + 2);
+        const double xa[4] = {x01.x, x01.y, x23.x, x23.y};
+        const double ya[4] = {y01.x, y01.y, y23.x, y23.y};
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int a = 0; a < 4; a++) acc[a][b] = fma(ya[b], xa[a], acc[a][b]);
       }
     }
     __syncthreads();
-    for (int t = 0; t < m; t++) {
-      const double* xr = xs + t * Pn;
-      const double* yr = ys + t * Pn;
-#pragma unroll
-      for (int s = 0; s < MAXE; s++)
-        if (threadIdx.x + s * 256 < nent) acc[s] = fma(yr[ok[s]], xr[oj[s]], acc[s]);
-    }
-    __syncthreads();
   }
+  if (g < G) {
 #pragma unroll
-  for (int s = 0; s < MAXE; s++)
-    if (threadIdx.x + s * 256 < nent) H[threadIdx.x + s * 256] = acc[s];
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) part[g * Pp * Pp + (jb + a) + Pp * (kb + b)] = acc[a][b];
+  }
+  __syncthreads();
+  for (int e = tid; e < Pp * Pp; e += 256) {
+    double v = 0.0;
+    for (int q = 0; q < G; q++) v += part[q * Pp * Pp + e];
+    H[e] = v;  // element e is read and written by this thread only
+  }
   __syncthreads();
   // x pass: px[j2][k2] = sum_j1 h2x(j1,k2) i^j1 H[j1][j2], k2 over the positive half
-  for (int idx = threadIdx.x; idx < Pn * n2; idx += 256) {
+  for (int idx = tid; idx < Pn * n2; idx += 256) {
     const int j2 = idx / n2, k2 = idx - j2 * n2;
     double2 a = make_double2(0.0, 0.0);
-    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k2] * H[j1 + Pn * j2], j1);
+    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k2] * H[j1 + Pp * j2], j1);
     px[idx] = a;
   }
   __syncthreads();
   // y pass over the full node set, written to the leaf's multipole slot
   double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  for (int e = threadIdx.x; e < k.nexp; e += 256) {
+  for (int e = tid; e < k.nexp; e += 256) {
     const int k1 = e / n2, k2 = e - k1 * n2;
     double2 a = make_double2(0.0, 0.0);
     for (int j2 = 0; j2 < Pn; j2++) {
@@ -286,6 +313,415 @@ __global__ void __launch_bounds__(256) k_form3d_hermite(KP k, const FormTask* __
       out[e] = a;
     }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ (a) form, 2D on FP64 MMA
+// Same product as k_form2d, H (P x P, P <= 8 NT) = sum_t x_t^j (q_t y_t^k),
+// on the FP64 tensor cores: mma.sync.m8n8k4.f64 takes four sources per step
+// (K = 4) into NT x NT tiles of 8 x 8.  Fragment layout (PTX ISA, m8n8k4
+// .f64): A element (row = lane/4, col = lane%4), B element (row = lane%4,
+// col = lane/4), accumulator pair (row = lane/4, col = 2 (lane%4) + i).  Lane
+// (j0 = lane/4, t = lane%4) therefore needs x_t^(j0 + 8 m) / sqrt((j0+8m)!)
+// and q_t y_t^(j0 + 8 m) / sqrt(..) for m < NT, built from x, x^2, x^4, x^8.
+// Four warps split the leaf's sources; their tiles are summed in shared
+// memory, then the Hermite -> plane-wave passes run as in k_form2d.
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __restrict__ tasks,
+                                                    const double* __restrict__ cfac) {
+  constexpr int PP = 8 * NT;
+  const FormTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const int Pn = T.p + 1, n2 = k.n2, npw = k.npw;
+  __shared__ double part[4][PP * PP];
+  __shared__ double cf[PP];
+  extern __shared__ double2 px[];  // [Pn][n2]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x < PP) cf[threadIdx.x] = cfac[threadIdx.x];
+  __syncthreads();
+  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
+  const int j0 = lane >> 2, tl = lane & 3;
+  double c[NT][NT][2];
+#pragma unroll
+  for (int a = 0; a < NT; a++)
+#pragma unroll
+    for (int b = 0; b < NT; b++) c[a][b][0] = c[a][b][1] = 0.0;
+  double cj[NT];
+#pragma unroll
+  for (int m = 0; m < NT; m++) cj[m] = cf[j0 + 8 * m];
+  // each warp takes steps s = warp, warp + 4, ... of four sources
+  for (int t0 = 4 * warp; t0 < T.n; t0 += 16) {
+    const int t = t0 + tl;
+    double x = 0.0, y = 0.0, q = 0.0;
+    if (t < T.n) {
+      const int i = T.s0 + t;
+      x = (k.src[2 * i] - cx) * k.dsq;
+      y = (k.src[2 * i + 1] - cy) * k.dsq;
+      q = k.chg[(size_t)i * k.nd + ind];
+    }
+    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
+    const double y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
+    double xa = (j0 & 1) ? x : 1.0, ya = (j0 & 1) ? y : 1.0;
+    if (j0 & 2) { xa *= x2; ya *= y2; }
+    if (j0 & 4) { xa *= x4; ya *= y4; }
+    ya *= q;
+    double av[NT], bv[NT];
+#pragma unroll
+    for (int m = 0; m < NT; m++) {
+      av[m] = xa * cj[m];
+      bv[m] = ya * cj[m];
+      xa *= x8;
+      ya *= y8;
+    }
+#pragma unroll
+    for (int a = 0; a < NT; a++)
+#pragma unroll
+      for (int b = 0; b < NT; b++) dmma_884(c[a][b][0], c[a][b][1], av[a], bv[b]);
+  }
+  // tile (a, b) holds H[j = 8a + lane/4][k = 8b + 2 (lane%4) + i]
+#pragma unroll
+  for (int a = 0; a < NT; a++)
+#pragma unroll
+    for (int b = 0; b < NT; b++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) part[warp][(8 * a + j0) + PP * (8 * b + 2 * tl + i)] = c[a][b][i];
+  __syncthreads();
+  for (int e = threadIdx.x; e < PP * PP; e += 128)
+    part[0][e] = part[0][e] + part[1][e] + part[2][e] + part[3][e];
+  __syncthreads();
+  const double* H = part[0];
+  for (int idx = threadIdx.x; idx < Pn * n2; idx += 128) {
+    const int j2 = idx / n2, k2 = idx - j2 * n2;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k2] * H[j1 + PP * j2], j1);
+    px[idx] = a;
+  }
+  __syncthreads();
+  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  for (int e = threadIdx.x; e < k.nexp; e += 128) {
+    const int k1 = e / n2, k2 = e - k1 * n2;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j2 = 0; j2 < Pn; j2++) {
+      const double h = k.h2x[j2 * npw + k1];
+      const double2 z = rot(px[j2 * n2 + k2], j2);
+      a.x = fma(h, z.x, a.x);
+      a.y = fma(h, z.y, a.y);
+    }
+    out[e] = a;
+  }
+}
+
+// ------------------------------------------------------------ (a) form, 3D, two kernels
+// Kernel A: one CTA per chunk of <= FORM3_CHK sources of a leaf; the chunk's
+// Hermite block H[j + P (k + P l)] (g3dformhc_vec, g3drouts.f:109-192) is
+// accumulated in shared memory -- each thread owns (j,k) pairs and keeps the
+// P values of l in registers -- and written to its slot of the partial buffer.
+// Kernel B: one CTA per leaf sums the leaf's partial blocks in chunk order
+// (deterministic) and runs the separable Hermite -> plane-wave transform
+// (g3dh2pw_real_vec, g3drouts.f:1565-1685) in shared memory: z pass over the
+// stored half, then y and x passes over the positive half using the mirror
+// symmetry A(j, mirror k) = (-1)^j A(j, k) of the ascending node set.
+
+template <int MAXP>
+__global__ void __launch_bounds__(256) k_form3d_acc(KP k, const FormTask* __restrict__ tasks,
+                                                    const FormChunk* __restrict__ chunks,
+                                                    double* __restrict__ hbuf, const double* __restrict__ isq,
+                                                    int sub) {
+  const FormChunk C = chunks[blockIdx.x];
+  const FormTask T = tasks[C.task];
+  const int ind = blockIdx.y;
+  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
+  extern __shared__ double sm[];
+  double* H = sm;
+  double* X = H + P3;
+  double* Y = X + sub * Pn;
+  double* Z = Y + sub * Pn;
+  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
+  for (int e = threadIdx.x; e < P3; e += blockDim.x) H[e] = 0.0;
+  for (int c0 = 0; c0 < C.n; c0 += sub) {
+    const int m = min(sub, C.n - c0);
+    __syncthreads();
+    for (int r = threadIdx.x; r < 3 * m; r += blockDim.x) {
+      const int t = r / 3, d = r - 3 * t;
+      const int i = C.s0 + c0 + t;
+      const double v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
+      double w = d == 2 ? k.chg[(size_t)i * k.nd + ind] : 1.0;
+      double* row = (d == 0 ? X : d == 1 ? Y : Z) + t * Pn;
+      row[0] = w;
+      for (int j = 1; j < Pn; j++) {
+        w = w * v * isq[j];
+        row[j] = w;
+      }
+    }
+    __syncthreads();
+    for (int pr = threadIdx.x; pr < P2; pr += blockDim.x) {
+      const int j = pr % Pn, kk = pr / Pn;
+      double acc[MAXP];
+#pragma unroll
+      for (int l = 0; l < MAXP; l++) acc[l] = l < Pn ? H[pr + P2 * l] : 0.0;
+      for (int t = 0; t < m; t++) {
+        const double a = X[t * Pn + j] * Y[t * Pn + kk];
+        const double* zr = Z + t * Pn;
+#pragma unroll
+        for (int l = 0; l < MAXP; l++)
+          if (l < Pn) acc[l] = fma(a, zr[l], acc[l]);
+      }
+#pragma unroll
+      for (int l = 0; l < MAXP; l++)
+        if (l < Pn) H[pr + P2 * l] = acc[l];
+    }
+  }
+  __syncthreads();
+  double* out = hbuf + ((size_t)C.hoff * k.nd + (size_t)ind * P3);
+  for (int e = threadIdx.x; e < P3; e += blockDim.x) out[e] = H[e];
+}
+
+__global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __restrict__ tasks,
+                                                     const int* __restrict__ cbeg,
+                                                     const FormChunk* __restrict__ chunks,
+                                                     const double* __restrict__ hbuf) {
+  const int tk = blockIdx.x, ind = blockIdx.y;
+  const FormTask T = tasks[tk];
+  const int npw = k.npw, n2 = k.n2;
+  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
+  extern __shared__ double sm[];
+  // region A: H, later T2 [(j3 npw + k2) n2 + k1]; region B: T1 [(j3 + P j2) n2 + k1]
+  const size_t szA = max((size_t)P3, (size_t)2 * Pn * npw * n2);
+  double* H = sm;
+  double2* T2 = reinterpret_cast<double2*>(sm);
+  double2* T1 = reinterpret_cast<double2*>(sm + ((szA + 1) & ~size_t(1)));
+  for (int e = threadIdx.x; e < P3; e += blockDim.x) {
+    double v = 0.0;
+    for (int c = cbeg[tk]; c < cbeg[tk + 1]; c++) v += hbuf[(size_t)chunks[c].hoff * k.nd + (size_t)ind * P3 + e];
+    H[e] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < P2 * n2; idx += blockDim.x) {
+    const int k1 = idx % n2, jj = idx / n2;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k1] * H[jj + P2 * j1], j1);
+    T1[idx] = a;
+  }
+  __syncthreads();
+  // y pass over the positive half k2 = n2 + m and its mirror n2 - 1 - m
+  for (int idx = threadIdx.x; idx < Pn * n2 * n2; idx += blockDim.x) {
+    const int k1 = idx % n2, r = idx / n2, m = r % n2, j3 = r / n2;
+    const int kp = n2 + m, km = n2 - 1 - m;
+    double2 ev = make_double2(0.0, 0.0), od = make_double2(0.0, 0.0);
+    for (int j2 = 0; j2 < Pn; j2++) {
+      const double h = k.h2x[j2 * npw + kp];
+      const double2 z = rot(T1[(j3 + Pn * j2) * n2 + k1], j2);
+      double2& acc = (j2 & 1) ? od : ev;
+      acc.x = fma(h, z.x, acc.x);
+      acc.y = fma(h, z.y, acc.y);
+    }
+    T2[((size_t)j3 * npw + kp) * n2 + k1] = make_double2(ev.x + od.x, ev.y + od.y);
+    T2[((size_t)j3 * npw + km) * n2 + k1] = make_double2(ev.x - od.x, ev.y - od.y);
+  }
+  __syncthreads();
+  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  // x pass into the slot, positive half k3 = n2 + m and mirror
+  for (int idx = threadIdx.x; idx < n2 * npw * n2; idx += blockDim.x) {
+    const int m = idx % n2, r = idx / n2, k2 = r % npw, k1 = r / npw;
+    const int kp = n2 + m, km = n2 - 1 - m;
+    double2 ev = make_double2(0.0, 0.0), od = make_double2(0.0, 0.0);
+    for (int j3 = 0; j3 < Pn; j3++) {
+      const double h = k.h2x[j3 * npw + kp];
+      const double2 z = rot(T2[((size_t)j3 * npw + k2) * n2 + k1], j3);
+      double2& acc = (j3 & 1) ? od : ev;
+      acc.x = fma(h, z.x, acc.x);
+      acc.y = fma(h, z.y, acc.y);
+    }
+    const size_t base = (size_t)npw * (k2 + (size_t)npw * k1);
+    out[base + kp] = make_double2(ev.x + od.x, ev.y + od.y);
+    out[base + km] = make_double2(ev.x - od.x, ev.y - od.y);
+  }
+}
+
+// ------------------------------------------------------------ (c) eval, 2D Taylor on FP64 MMA
+// One CTA (4 warps) per chunk of an evaluation leaf.  The leaf's plane-wave
+// expansion is staged in shared memory and converted to the Taylor block
+// lo[k2 + LD k1] (g2dpw2local_real_vec); then for eight points per warp step
+//     E[t][k1] = sum_k2 x_t^k2 lo[k2][k1]      (mma.m8n8k4.f64, K = 4 per step)
+//     pot_t   += sum_k1 E[t][k1] y_t^k1         (per lane, then two shuffles)
+// The B fragments of lo stay in registers for the whole chunk.
+template <int NT>
+__global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __restrict__ tasks) {
+  constexpr int PP = 8 * NT, LD = PP + 1;
+  const EvalTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2, Pn = T.p + 1;
+  extern __shared__ double sm[];
+  double* lo = sm;                                   // [PP][LD], zero padded
+  double2* lx = reinterpret_cast<double2*>(sm + ((PP * LD + 1) & ~1));  // [Pn][npw]
+  double2* Ls = lx + Pn * npw;                       // [nexp]
+  const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  for (int e = threadIdx.x; e < k.nexp; e += 128) Ls[e] = L[e];
+  for (int e = threadIdx.x; e < PP * LD; e += 128) lo[e] = 0.0;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < Pn * npw; idx += 128) {
+    const int k2 = idx / npw, j1 = idx - k2 * npw;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j2 = 0; j2 < n2; j2++) {
+      const double h = k.x2l[k2 * npw + j2];
+      const double2 v = Ls[j2 + n2 * j1];
+      a.x = fma(h, v.x, a.x);
+      a.y = fma(h, v.y, a.y);
+    }
+    lx[idx] = rot(a, k2);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < Pn * Pn; idx += 128) {
+    const int k1 = idx / Pn, k2 = idx - k1 * Pn;
+    const double sg = (k1 & 1) ? -1.0 : 1.0;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j1 = 0; j1 < n2; j1++) {
+      const double h = k.x2l[k1 * npw + j1];
+      const double2 u = lx[k2 * npw + j1], v = lx[k2 * npw + j1 + n2];
+      a.x = fma(h, fma(sg, v.x, u.x), a.x);
+      a.y = fma(h, fma(sg, v.y, u.y), a.y);
+    }
+    lo[k2 + LD * k1] = 2.0 * rot(a, k1).x;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r4 = lane >> 2, c4 = lane & 3;
+  // B fragment (row = k2 = 4 ks + c4, col = k1 = 8 b + r4)
+  double bf[2 * NT][NT];
+#pragma unroll
+  for (int ks = 0; ks < 2 * NT; ks++)
+#pragma unroll
+    for (int b = 0; b < NT; b++) bf[ks][b] = lo[(4 * ks + c4) + LD * (8 * b + r4)];
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
+  for (int t0 = 8 * warp; t0 < T.n; t0 += 32) {
+    // A rows: target t0 + r4, powers k2 = 4 ks + c4
+    const int ta = t0 + r4;
+    double x = 0.0, y = 0.0;
+    if (ta < T.n) {
+      const int ip = T.i0 + ta;
+      x = (pts[2 * ip] - cx) * k.dsq;
+      y = (pts[2 * ip + 1] - cy) * k.dsq;
+    }
+    const double x2 = x * x, x4 = x2 * x2;
+    double xa = (c4 & 1) ? x : 1.0;
+    if (c4 & 2) xa *= x2;
+    double c[NT][2];
+#pragma unroll
+    for (int b = 0; b < NT; b++) c[b][0] = c[b][1] = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < 2 * NT; ks++) {
+#pragma unroll
+      for (int b = 0; b < NT; b++) dmma_884(c[b][0], c[b][1], xa, bf[ks][b]);
+      xa *= x4;
+    }
+    // accumulator (row = target t0 + r4, col = k1 = 8 b + 2 c4 + i)
+    const double y2 = y * y, y8 = (y2 * y2) * (y2 * y2);
+    double yb = (c4 & 1) ? y2 : 1.0;
+    if (c4 & 2) yb *= y2 * y2;
+    double r = 0.0;
+#pragma unroll
+    for (int b = 0; b < NT; b++) {
+      r = fma(c[b][0], yb, r);
+      r = fma(c[b][1], yb * y, r);
+      yb *= y8;
+    }
+    r += __shfl_xor_sync(0xffffffffu, r, 1);
+    r += __shfl_xor_sync(0xffffffffu, r, 2);
+    if (c4 == 0 && ta < T.n) out[(size_t)(T.i0 + ta) * k.nd + ind] += r;
+  }
+}
+
+// ------------------------------------------------------------ (c) eval, 3D Taylor in shared memory
+// One CTA per chunk of an evaluation leaf: plane wave -> Taylor
+// (g3dpw2local_real_vec, g3drouts.f:1774-1938) with x and y passes over the
+// positive half (mirror pre-add) and the z pass over the stored half, then
+// Horner evaluation, two points per thread.
+__global__ void __launch_bounds__(512) k_eval3d_taylor_smem(KP k, const EvalTask* __restrict__ tasks) {
+  const EvalTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2;
+  const int Pn = T.p + 1, P2 = Pn * Pn;
+  extern __shared__ double sm[];
+  const size_t szA = max((size_t)2 * Pn * npw * n2, (size_t)P2 * Pn);
+  double2* U1 = reinterpret_cast<double2*>(sm);                       // [(a npw + m2) n2 + m1]
+  double* lo = sm;                                                    // overwrites U1
+  double2* U2 = reinterpret_cast<double2*>(sm + ((szA + 1) & ~size_t(1)));  // [(a P + b) n2 + m1]
+  const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  for (int idx = threadIdx.x; idx < Pn * npw * n2; idx += blockDim.x) {
+    const int m1 = idx % n2, r = idx / n2, m2 = r % npw, a = r / npw;
+    const double2* row = L + (size_t)npw * (m2 + (size_t)npw * m1);
+    const double sg = (a & 1) ? -1.0 : 1.0;
+    double2 s = make_double2(0.0, 0.0);
+    for (int m = 0; m < n2; m++) {
+      const double h = k.x2l[a * npw + n2 + m];
+      const double2 u = row[n2 + m], v = row[n2 - 1 - m];
+      s.x = fma(h, fma(sg, v.x, u.x), s.x);
+      s.y = fma(h, fma(sg, v.y, u.y), s.y);
+    }
+    U1[idx] = rot(s, a);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < P2 * n2; idx += blockDim.x) {
+    const int m1 = idx % n2, r = idx / n2, b = r % Pn, a = r / Pn;
+    const double sg = (b & 1) ? -1.0 : 1.0;
+    double2 s = make_double2(0.0, 0.0);
+    for (int m = 0; m < n2; m++) {
+      const double h = k.x2l[b * npw + n2 + m];
+      const double2 u = U1[((size_t)a * npw + n2 + m) * n2 + m1], v = U1[((size_t)a * npw + n2 - 1 - m) * n2 + m1];
+      s.x = fma(h, fma(sg, v.x, u.x), s.x);
+      s.y = fma(h, fma(sg, v.y, u.y), s.y);
+    }
+    U2[idx] = rot(s, b);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < P2 * Pn; idx += blockDim.x) {
+    const int a = idx % Pn, r = idx / Pn, b = r % Pn, c = r / Pn;
+    double2 s = make_double2(0.0, 0.0);
+    for (int m1 = 0; m1 < n2; m1++) {
+      const double h = k.x2l[c * npw + m1];
+      const double2 v = U2[((size_t)a * Pn + b) * n2 + m1];
+      s.x = fma(h, v.x, s.x);
+      s.y = fma(h, v.y, s.y);
+    }
+    lo[idx] = 2.0 * rot(s, c).x;
+  }
+  __syncthreads();
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
+  for (int i0 = threadIdx.x; i0 < T.n; i0 += 2 * blockDim.x) {
+    const int i1 = i0 + blockDim.x;
+    const bool two = i1 < T.n;
+    const int p0 = T.i0 + i0, p1 = T.i0 + (two ? i1 : i0);
+    const double x0 = (pts[3 * p0] - cx) * k.dsq, y0 = (pts[3 * p0 + 1] - cy) * k.dsq, z0 = (pts[3 * p0 + 2] - cz) * k.dsq;
+    const double x1 = (pts[3 * p1] - cx) * k.dsq, y1 = (pts[3 * p1 + 1] - cy) * k.dsq, z1 = (pts[3 * p1 + 2] - cz) * k.dsq;
+    double rz0 = 0.0, rz1 = 0.0;
+    for (int c = Pn - 1; c >= 0; c--) {
+      double ry0 = 0.0, ry1 = 0.0;
+      for (int b = Pn - 1; b >= 0; b--) {
+        const double* row = lo + Pn * (b + Pn * c);
+        double rx0 = 0.0, rx1 = 0.0;
+        for (int a = Pn - 1; a >= 0; a--) {
+          const double cf = row[a];
+          rx0 = fma(rx0, x0, cf);
+          rx1 = fma(rx1, x1, cf);
+        }
+        ry0 = fma(ry0, y0, rx0);
+        ry1 = fma(ry1, y1, rx1);
+      }
+      rz0 = fma(rz0, z0, ry0);
+      rz1 = fma(rz1, z1, ry1);
+    }
+    out[(size_t)p0 * k.nd + ind] += rz0;
+    if (two) out[(size_t)p1 * k.nd + ind] += rz1;
   }
 }
 
@@ -444,17 +880,28 @@ __global__ void __launch_bounds__(256) k_eval2d(KP k, const EvalTask* __restrict
       lo[k2 + Pn * k1] = 2.0 * rot(a, k1).x;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
-      const int ip = T.i0 + i;
-      const double x = (pts[2 * ip] - cx) * k.dsq, y = (pts[2 * ip + 1] - cy) * k.dsq;
-      double r = 0.0;
+    // Horner in x within a row, then in y; two points per thread for two
+    // independent FMA chains
+    for (int i0 = threadIdx.x; i0 < T.n; i0 += 2 * blockDim.x) {
+      const int i1 = i0 + blockDim.x;
+      const bool two = i1 < T.n;
+      const int p0 = T.i0 + i0, p1 = T.i0 + (two ? i1 : i0);
+      const double x0 = (pts[2 * p0] - cx) * k.dsq, y0 = (pts[2 * p0 + 1] - cy) * k.dsq;
+      const double x1 = (pts[2 * p1] - cx) * k.dsq, y1 = (pts[2 * p1 + 1] - cy) * k.dsq;
+      double r0 = 0.0, r1 = 0.0;
       for (int k1 = Pn - 1; k1 >= 0; k1--) {
-        double s = 0.0;
+        double s0 = 0.0, s1 = 0.0;
         const double* row = lo + Pn * k1;
-        for (int k2 = Pn - 1; k2 >= 0; k2--) s = fma(s, x, row[k2]);
-        r = fma(r, y, s);
+        for (int k2 = Pn - 1; k2 >= 0; k2--) {
+          const double c = row[k2];
+          s0 = fma(s0, x0, c);
+          s1 = fma(s1, x1, c);
+        }
+        r0 = fma(r0, y0, s0);
+        r1 = fma(r1, y1, s1);
       }
-      out[(size_t)ip * k.nd + ind] += r;
+      out[(size_t)p0 * k.nd + ind] += r0;
+      if (two) out[(size_t)p1 * k.nd + ind] += r1;
     }
   } else {
     for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
@@ -604,54 +1051,69 @@ __global__ void __launch_bounds__(256) k_eval3d_pw(KP k, const EvalTask* __restr
 // r^2 < dmax.  MIXED computes exp in FP32 on the SFU (ex2.approx) from an
 // FP64 argument and accumulates in FP64.
 template <int DIM, bool MIXED>
-__global__ void __launch_bounds__(DIR_T) k_direct(KP k, const DirTask* __restrict__ tasks,
-                                                  const SrcRange* __restrict__ ranges) {
-  const DirTask T = tasks[blockIdx.x];
+__global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict__ tasks, int ntask,
+                                                const SrcRange* __restrict__ ranges) {
+  constexpr int CAP = 256;  // sources staged per warp and batch
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 4 + warp;
+  __shared__ double ssm[4][(DIM + 1) * CAP];
+  if (w >= ntask) return;  // whole warp leaves; no block-wide barrier below
+  const DirTask T = tasks[w];
   const int ind = blockIdx.y;
-  __shared__ double sx[DIR_T], sy[DIR_T], sz[DIM == 3 ? DIR_T : 1], sq[DIR_T];
+  double* sx = ssm[warp];
+  double* sy = sx + CAP;
+  double* sz = sy + CAP;
+  double* sq = sz + (DIM == 3 ? CAP : 0);
+  // g lanes per point (g * n <= 32) split the sources of that point
+  int g = 1;
+  while (g * 2 * T.n <= 32) g *= 2;
+  const int tt = lane / g, sub = lane - tt * g;
+  const bool act = tt < T.n;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
-  const bool act = threadIdx.x < T.n;
-  const int ip = T.i0 + threadIdx.x;
-  double tx = 0, ty = 0, tz = 0;
-  if (act) {
-    tx = pts[DIM * ip];
-    ty = pts[DIM * ip + 1];
-    if (DIM == 3) tz = pts[DIM * ip + 2];
-  }
+  const int ip = T.i0 + (act ? tt : 0);
+  const double tx = pts[DIM * ip], ty = pts[DIM * ip + 1];
+  const double tz = DIM == 3 ? pts[DIM * ip + 2] : 0.0;
   const double ninv = -1.0 / k.delta;
   const double nl2 = -1.4426950408889634 / k.delta;
   double acc = 0.0;
-  for (int r = 0; r < T.cnt; r++) {
-    const SrcRange R = ranges[T.off + r];
-    for (int c0 = 0; c0 < R.n; c0 += DIR_T) {
-      const int m = min(DIR_T, R.n - c0);
-      __syncthreads();
-      if (threadIdx.x < m) {
-        const int j = R.s0 + c0 + threadIdx.x;
-        sx[threadIdx.x] = k.src[DIM * j];
-        sy[threadIdx.x] = k.src[DIM * j + 1];
-        if (DIM == 3) sz[threadIdx.x] = k.src[DIM * j + 2];
-        sq[threadIdx.x] = k.chg[(size_t)j * k.nd + ind];
+  int r = 0, roff = 0;
+  while (r < T.cnt) {
+    int m = 0;
+    __syncwarp();
+    while (r < T.cnt && m < CAP) {
+      const SrcRange R = ranges[T.off + r];
+      const int take = min(CAP - m, R.n - roff);
+      for (int t = lane; t < take; t += 32) {
+        const int j = R.s0 + roff + t;
+        sx[m + t] = k.src[DIM * j];
+        sy[m + t] = k.src[DIM * j + 1];
+        if (DIM == 3) sz[m + t] = k.src[DIM * j + 2];
+        sq[m + t] = k.chg[(size_t)j * k.nd + ind];
       }
-      __syncthreads();
-      if (act) {
-        for (int t = 0; t < m; t++) {
-          const double dx = tx - sx[t], dy = ty - sy[t];
-          double rr = fma(dx, dx, dy * dy);
-          if (DIM == 3) {
-            const double dz = tz - sz[t];
-            rr = fma(dz, dz, rr);
-          }
-          if (rr < k.dmax) {
-            if (MIXED) acc = fma((double)ex2_approx((float)(rr * nl2)), sq[t], acc);
-            else acc = fma(exp(rr * ninv), sq[t], acc);
-          }
+      m += take;
+      roff += take;
+      if (roff == R.n) { r++; roff = 0; }
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll 4
+      for (int t = sub; t < m; t += g) {
+        const double dx = tx - sx[t], dy = ty - sy[t];
+        double rr = fma(dx, dx, dy * dy);
+        if (DIM == 3) {
+          const double dz = tz - sz[t];
+          rr = fma(dz, dz, rr);
+        }
+        if (rr < k.dmax) {
+          if (MIXED) acc = fma((double)ex2_approx((float)(rr * nl2)), sq[t], acc);
+          else acc = fma(exp(rr * ninv), sq[t], acc);
         }
       }
     }
   }
-  if (act) out[(size_t)ip * k.nd + ind] += acc;
+  for (int o = 1; o < g; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (act && sub == 0) out[(size_t)ip * k.nd + ind] += acc;
 }
 
 // ------------------------------------------------------------ large delta
@@ -751,13 +1213,6 @@ size_t bytes_of(const std::vector<T>& v) {
 }
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 
-int form2d_maxe(int pmax) {
-  int need = ((pmax + 1) * (pmax + 1) + 255) / 256;
-  if (need <= 4) return 4;
-  if (need <= 16) return 16;
-  if (need <= 40) return 40;
-  return -1;
-}
 
 }  // namespace
 
@@ -778,18 +1233,35 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   CK(cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev));
   // order form and eval tasks by route so each kernel gets a contiguous range
   std::vector<FormTask> form = H.form;
-  std::stable_sort(form.begin(), form.end(), [](const FormTask& a, const FormTask& b) { return a.route < b.route; });
+  std::stable_sort(form.begin(), form.end(), [](const FormTask& a, const FormTask& b) {
+    return a.route != b.route ? a.route < b.route : a.p < b.p;
+  });
   D.nform = (int)form.size();
   for (auto& f : form) {
     (f.route == ROUTE_PW ? D.form_pw_n : D.form_hermite_n)++;
     if (f.route == ROUTE_HERMITE) D.form_pmax = std::max(D.form_pmax, f.p);
   }
   std::vector<EvalTask> ev = H.eval;
-  std::stable_sort(ev.begin(), ev.end(), [](const EvalTask& a, const EvalTask& b) { return a.route < b.route; });
+  std::stable_sort(ev.begin(), ev.end(), [](const EvalTask& a, const EvalTask& b) {
+    return a.route != b.route ? a.route < b.route : a.p < b.p;
+  });
   D.neval = (int)ev.size();
   for (auto& e : ev) {
     (e.route == ROUTE_PW ? D.eval_pw_n : D.eval_taylor_n)++;
     if (e.route == ROUTE_TAYLOR) D.eval_pmax = std::max(D.eval_pmax, e.p);
+  }
+  // launch groups of equal order among the Hermite form / Taylor eval tasks
+  for (int t = 0; t < D.form_hermite_n;) {
+    int u = t;
+    while (u < D.form_hermite_n && form[u].p == form[t].p) u++;
+    D.form_groups.push_back({form[t].p, t, u});
+    t = u;
+  }
+  for (int t = 0; t < D.eval_taylor_n;) {
+    int u = t;
+    while (u < D.eval_taylor_n && ev[u].p == ev[t].p) u++;
+    D.eval_groups.push_back({ev[t].p, t, u});
+    t = u;
   }
   // merge groups: consecutive tasks with the same destination
   std::vector<MergeGroup> groups;
@@ -814,14 +1286,53 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   D.direct_pairs = H.direct_pairs;
   D.form_sources = H.form_sources;
   D.eval_points = H.eval_points;
-  // scratch for the 3D separable transforms
+  // 3D: shared-memory paths when the largest order fits, else the scratch path
+  std::vector<FormChunk> fchunks;
+  std::vector<int> fcbeg;
+  size_t hbuf_doubles = 0;
   if (P.dim == 3 && !P.all_direct) {
+    const size_t lim = 227 * 1024;
+    const int n2 = P.npw / 2;
+    if (D.form_hermite_n > 0) {
+      const size_t Pn = D.form_pmax + 1, P3 = Pn * Pn * Pn;
+      size_t szA = std::max(P3, 2 * Pn * P.npw * n2);
+      D.form3_shB = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
+      D.form3_sub = (P3 + 3 * 64 * Pn) * 8 <= lim ? 64 : 32;
+      D.form3_shA = (P3 + 3 * (size_t)D.form3_sub * Pn) * 8;
+      D.form3_smem = D.form3_shB <= lim && D.form3_shA <= lim;
+      if (D.form3_smem) {
+        long long hoff = 0;
+        for (int t = 0; t < D.form_hermite_n; t++) {
+          fcbeg.push_back((int)fchunks.size());
+          const FormTask& f = form[t];
+          long long p3 = (long long)(f.p + 1) * (f.p + 1) * (f.p + 1);
+          for (int c = 0; c < f.n; c += 4096) {
+            fchunks.push_back({t, f.s0 + c, std::min(4096, f.n - c), hoff});
+            hoff += p3;
+          }
+        }
+        fcbeg.push_back((int)fchunks.size());
+        hbuf_doubles = (size_t)hoff * P.nd;
+        D.nfchunks = (int)fchunks.size();
+      }
+    }
+    if (D.eval_taylor_n > 0) {
+      const size_t Pn = D.eval_pmax + 1;
+      size_t szA = std::max(2 * Pn * P.npw * n2, Pn * Pn * Pn);
+      D.eval3_sh = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
+      D.eval3_smem = D.eval3_sh <= lim;
+    }
+  }
+  // scratch for the 3D separable transforms (fallback path)
+  if (P.dim == 3 && !P.all_direct && (!D.form3_smem || !D.eval3_smem)) {
     size_t slab = 0;
     int n2 = P.npw / 2;
-    for (auto& f : form)
-      if (f.route == ROUTE_HERMITE) slab = std::max(slab, (size_t)(f.p + 1) * (f.p + 1) * n2 + (size_t)(f.p + 1) * P.npw * n2);
-    for (auto& e : ev)
-      if (e.route == ROUTE_TAYLOR) {
+    if (!D.form3_smem)
+      for (auto& f : form)
+        if (f.route == ROUTE_HERMITE) slab = std::max(slab, (size_t)(f.p + 1) * (f.p + 1) * n2 + (size_t)(f.p + 1) * P.npw * n2);
+    if (!D.eval3_smem)
+      for (auto& e : ev)
+        if (e.route == ROUTE_TAYLOR) {
         size_t Pn = e.p + 1;
         slab = std::max(slab, Pn * P.npw * n2 + Pn * Pn * n2 + (Pn * Pn * Pn + 1) / 2);
       }
@@ -830,13 +1341,15 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
   size_t total = bytes_of(H.box_centers) + bytes_of(H.h2x) + bytes_of(H.x2l) + al(H.wms.size() * 8) +
-                 al(H.wsh.size() * 8) + al(H.tree.isrc.size() * 4) + al(H.tree.itarg.size() * 4) +
+                 al(H.wsh.size() * 8) + 2 * al(H.tree.isrc.size() * 4) + 2 * al(H.tree.itarg.size() * 4) +
+                 al((size_t)(std::max(P.ntermmax, 1) + 2) * 8) + al(32 * 8) +
                  bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(H.split) +
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
                  al(nt * dim * 8) + al(ns * nd * 8) + al(nt * nd * 8) +
-                 al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + 4096;
+                 al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
+                 bytes_of(fcbeg) + al(hbuf_doubles * 8) + 4096;
   D.bytes = total;
   CK(cudaMalloc(&D.base, total));
   char* cur = D.base;
@@ -854,6 +1367,23 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   }
   CK(put(cur, D.isrc, H.tree.isrc, s));
   CK(put(cur, D.itarg, H.tree.itarg, s));
+  {
+    std::vector<int> inv(H.tree.isrc.size());
+    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.isrc[i]] = (int)i;
+    CK(put(cur, D.isrc_inv, inv, s));
+    CK(cudaStreamSynchronize(s));
+    inv.assign(H.tree.itarg.size(), 0);
+    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.itarg[i]] = (int)i;
+    CK(put(cur, D.itarg_inv, inv, s));
+    std::vector<double> isq(std::max(P.ntermmax, 1) + 2, 0.0);
+    for (size_t j = 1; j < isq.size(); j++) isq[j] = 1.0 / std::sqrt((double)j);
+    CK(put(cur, D.isq, isq, s));
+    std::vector<double> cfac(32);
+    cfac[0] = 1.0;
+    for (int j = 1; j < 32; j++) cfac[j] = cfac[j - 1] / std::sqrt((double)j);
+    CK(put(cur, D.cfac, cfac, s));
+    CK(cudaStreamSynchronize(s));
+  }
   CK(put(cur, D.form, form, s));
   CK(put(cur, D.mgroups, groups, s));
   CK(put(cur, D.merge, H.merge, s));
@@ -863,6 +1393,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   CK(put(cur, D.eval, ev, s));
   CK(put(cur, D.dir, H.dir, s));
   CK(put(cur, D.dir_src, H.dir_src, s));
+  CK(put(cur, D.fchunks, fchunks, s));
+  CK(put(cur, D.fcbeg, fcbeg, s));
+  D.hbuf = reinterpret_cast<double*>(cur); cur += al(hbuf_doubles * 8);
   D.mp = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nmp * nd * P.nexp * 16);
   D.loc = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nloc * nd * P.nexp * 16);
   D.ssort = reinterpret_cast<double*>(cur); cur += al(ns * dim * 8);
@@ -894,9 +1427,23 @@ static KP make_kp(const DevicePlan& D) {
 
 // node weights for the direct 3D form kernel live in the x2l/h2x neighbourhood:
 // ws(k) = h2x[0 * npw + k] (j = 0 row of h2x is ws_k).
-cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* chg,
-                                const double* trg, double* pot, double* pottarg, int precision,
-                                cudaStream_t st, StageTimes* times) {
+cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const double* trg,
+                                   cudaStream_t st) {
+  const Params& P = D.P;
+  const int gb = std::max(1, std::min(8 * D.sm_count, (std::max(P.ns, P.nt) + 255) / 256));
+  if (P.ns > 0) {
+    const int vec = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+    k_gather_pts<<<gb, 256, 0, st>>>(src, nullptr, D.ssort, nullptr, D.isrc, P.ns, P.dim, P.nd, vec);
+  }
+  if (P.nt > 0 && P.ifpghtarg > 0) {
+    const int vec = (reinterpret_cast<uintptr_t>(trg) & 15) == 0;
+    k_gather_pts<<<gb, 256, 0, st>>>(trg, nullptr, D.tsort, nullptr, D.itarg, P.nt, P.dim, P.nd, vec);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
+                                int precision, cudaStream_t st, StageTimes* times) {
   const Params& P = D.P;
   KP k = make_kp(D);
   k.ws = D.h2x;  // row j = 0 of h2x holds the weights
@@ -907,14 +1454,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* 
   auto mark = [&](int i) { if (times) cudaEventRecord(ev[i], st); };
   long long launches = 0;
   mark(0);
-  // gather into tree order
+  // charges into tree order (coordinates were sorted once, at plan set-up)
+  const int gb = std::max(1, std::min(8 * D.sm_count, (std::max(P.ns, P.nt) + 255) / 256));
   if (P.ns > 0) {
-    k_gather<<<std::min<long long>(4096, ((long long)P.ns * P.dim + 255) / 256), 256, 0, st>>>(src, D.ssort, D.isrc, P.ns, P.dim);
-    k_gather<<<std::min<long long>(4096, ((long long)P.ns * nd + 255) / 256), 256, 0, st>>>(chg, D.csort, D.isrc, P.ns, nd);
-    launches += 2;
-  }
-  if (P.nt > 0 && P.ifpghtarg > 0) {
-    k_gather<<<std::min<long long>(4096, ((long long)P.nt * P.dim + 255) / 256), 256, 0, st>>>(trg, D.tsort, D.itarg, P.nt, P.dim);
+    k_gather_pts<<<gb, 256, 0, st>>>(nullptr, chg, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
   if (P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * 8, st));
@@ -924,26 +1467,46 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* 
   if (!P.all_direct) {
     // (a) form
     if (P.dim == 2 && D.form_hermite_n > 0) {
-      int pm = D.form_pmax;
-      int Pn = pm + 1;
-      size_t sh = (2 * FORM_CH * Pn + ((Pn * Pn + 1) & ~1) + 2 * Pn * n2) * 8;
-      int me = form2d_maxe(pm);
-      dim3 g(D.form_hermite_n, nd);
-      if (me == 4) {
-        CK(cudaFuncSetAttribute(k_form2d_hermite<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form2d_hermite<4><<<g, 256, sh, st>>>(k, D.form);
-      } else if (me == 16) {
-        CK(cudaFuncSetAttribute(k_form2d_hermite<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form2d_hermite<16><<<g, 256, sh, st>>>(k, D.form);
-      } else if (me == 40) {
-        CK(cudaFuncSetAttribute(k_form2d_hermite<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form2d_hermite<40><<<g, 256, sh, st>>>(k, D.form);
-      } else {
-        return cudaErrorNotSupported;
+      for (const OrderGroup& G : D.form_groups) {
+        const int Pn = G.p + 1;
+        dim3 g(G.end - G.beg, nd);
+        const FormTask* tk = D.form + G.beg;
+        if (Pn <= 32) {
+          size_t sh = (size_t)Pn * n2 * 16;
+#define FORM_MMA(NT)                                                                              \
+  do {                                                                                            \
+    CK(cudaFuncSetAttribute(k_form2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_form2d_mma<NT><<<g, 128, sh, st>>>(k, tk, D.cfac);                                          \
+  } while (0)
+          if (Pn <= 8) FORM_MMA(1);
+          else if (Pn <= 16) FORM_MMA(2);
+          else if (Pn <= 24) FORM_MMA(3);
+          else FORM_MMA(4);
+#undef FORM_MMA
+        } else {
+          const int tpd = (Pn + 3) / 4, Pp = 4 * tpd;
+          if (tpd * tpd > 256) return cudaErrorNotSupported;
+          const int ch = Pp <= 32 ? 128 : 64;
+          size_t sh = ((size_t)2 * ch * Pp + 4096 + 2 * (size_t)Pn * n2) * 8;
+          CK(cudaFuncSetAttribute(k_form2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+          k_form2d<<<g, 256, sh, st>>>(k, tk, D.isq, ch);
+        }
+        launches++;
       }
-      launches++;
     }
-    if (P.dim == 3 && D.form_hermite_n > 0) {
+    if (P.dim == 3 && D.form_hermite_n > 0 && D.form3_smem) {
+      const int Pn = D.form_pmax + 1;
+      if (Pn <= 16) {
+        CK(cudaFuncSetAttribute(k_form3d_acc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shA));
+        k_form3d_acc<16><<<dim3(D.nfchunks, nd), 256, D.form3_shA, st>>>(k, D.form, D.fchunks, D.hbuf, D.isq, D.form3_sub);
+      } else {
+        CK(cudaFuncSetAttribute(k_form3d_acc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shA));
+        k_form3d_acc<32><<<dim3(D.nfchunks, nd), 256, D.form3_shA, st>>>(k, D.form, D.fchunks, D.hbuf, D.isq, D.form3_sub);
+      }
+      CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shB));
+      k_form3d_h2pw<<<dim3(D.form_hermite_n, nd), 512, D.form3_shB, st>>>(k, D.form, D.fcbeg, D.fchunks, D.hbuf);
+      launches += 2;
+    } else if (P.dim == 3 && D.form_hermite_n > 0) {
       int Pn = D.form_pmax + 1;
       size_t sh = ((size_t)Pn * Pn * Pn + 3 * FORM_CH * Pn) * 8;
       if (Pn > 32 || sh > 227 * 1024) return cudaErrorNotSupported;
@@ -987,13 +1550,39 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* 
     mark(5);
     // (c) eval
     if (P.dim == 2 && D.neval > 0) {
-      int Pn = D.eval_pmax + 1;
-      size_t sh = (2 * (size_t)Pn * P.npw + (size_t)Pn * Pn) * 8;
-      CK(cudaFuncSetAttribute(k_eval2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-      k_eval2d<<<dim3(D.neval, nd), 256, sh, st>>>(k, D.eval);
-      launches++;
+      for (const OrderGroup& G : D.eval_groups) {
+        const int Pn = G.p + 1;
+        dim3 g(G.end - G.beg, nd);
+        const EvalTask* tk = D.eval + G.beg;
+        if (Pn <= 32) {
+#define EVAL_MMA(NT)                                                                              \
+  do {                                                                                            \
+    size_t sh = ((size_t)((8 * NT * (8 * NT + 1) + 1) & ~1) + 2 * (size_t)Pn * P.npw + 2 * (size_t)P.nexp) * 8; \
+    CK(cudaFuncSetAttribute(k_eval2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_eval2d_mma<NT><<<g, 128, sh, st>>>(k, tk);                                                  \
+  } while (0)
+          if (Pn <= 8) EVAL_MMA(1);
+          else if (Pn <= 16) EVAL_MMA(2);
+          else if (Pn <= 24) EVAL_MMA(3);
+          else EVAL_MMA(4);
+#undef EVAL_MMA
+        } else {
+          size_t sh = (2 * (size_t)Pn * P.npw + (size_t)Pn * Pn) * 8;
+          CK(cudaFuncSetAttribute(k_eval2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+          k_eval2d<<<g, 256, sh, st>>>(k, tk);
+        }
+        launches++;
+      }
+      if (D.eval_pw_n > 0) {
+        k_eval2d<<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
+        launches++;
+      }
     }
-    if (P.dim == 3 && D.eval_taylor_n > 0) {
+    if (P.dim == 3 && D.eval_taylor_n > 0 && D.eval3_smem) {
+      CK(cudaFuncSetAttribute(k_eval3d_taylor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
+      k_eval3d_taylor_smem<<<dim3(D.eval_taylor_n, nd), 512, D.eval3_sh, st>>>(k, D.eval);
+      launches++;
+    } else if (P.dim == 3 && D.eval_taylor_n > 0) {
       k_eval3d_taylor<<<D.scratch_ctas, 256, 0, st>>>(k, D.eval, D.eval_taylor_n, D.scratch, D.scratch_per_cta);
       launches++;
     }
@@ -1007,24 +1596,24 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* src, const double* 
   mark(6);
   // (d) near field
   if (D.ndir > 0) {
-    dim3 g(D.ndir, nd);
+    dim3 g((D.ndir + 3) / 4, nd);
     bool mixed = precision == PREC_MIXED;
     if (P.dim == 2) {
-      if (mixed) k_direct<2, true><<<g, DIR_T, 0, st>>>(k, D.dir, D.dir_src);
-      else k_direct<2, false><<<g, DIR_T, 0, st>>>(k, D.dir, D.dir_src);
+      if (mixed) k_direct<2, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      else k_direct<2, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
     } else {
-      if (mixed) k_direct<3, true><<<g, DIR_T, 0, st>>>(k, D.dir, D.dir_src);
-      else k_direct<3, false><<<g, DIR_T, 0, st>>>(k, D.dir, D.dir_src);
+      if (mixed) k_direct<3, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      else k_direct<3, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
     }
     launches++;
   }
   mark(7);
   if (P.ifpgh > 0 && P.ns > 0) {
-    k_scatter<<<std::min<long long>(4096, ((long long)P.ns * nd + 255) / 256), 256, 0, st>>>(D.psort, pot, D.isrc, P.ns, nd);
+    k_unsort<<<gb, 256, 0, st>>>(D.psort, pot, D.isrc_inv, P.ns, nd);
     launches++;
   }
   if (P.ifpghtarg > 0 && P.nt > 0) {
-    k_scatter<<<std::min<long long>(4096, ((long long)P.nt * nd + 255) / 256), 256, 0, st>>>(D.ptsort, pottarg, D.itarg, P.nt, nd);
+    k_unsort<<<gb, 256, 0, st>>>(D.ptsort, pottarg, D.itarg_inv, P.nt, nd);
     launches++;
   }
   mark(8);

@@ -218,16 +218,42 @@ static void build_tasks(HostPlan& H) {
         if (l == npl && !L.iflocal[b]) continue;
         int route = pw ? ROUTE_PW : ROUTE_TAYLOR;
         if (D == 3 && pw && t.ns(b) + t.nt(b) >= 1000000) route = ROUTE_TAYLOR;
-        if (P.ifpghtarg == 1 && t.nt(b) > 0) {
-          H.eval.push_back({b, 1, t.t0[b], t.nt(b), H.loc_slot[b], p, route});
-          H.eval_points += t.nt(b);
-        }
-        if (P.ifpgh == 1 && t.ns(b) > 0) {
-          H.eval.push_back({b, 0, t.s0[b], t.ns(b), H.loc_slot[b], p, route});
-          H.eval_points += t.ns(b);
+        // big leaves are cut into chunks so that no CTA serialises a
+        // 10^4-point leaf; each chunk rebuilds the leaf's Taylor expansion
+        const int evch = D == 2 ? 4096 : 2048;
+        for (int set = 1; set >= 0; set--) {
+          if (set == 1 && !(P.ifpghtarg == 1 && t.nt(b) > 0)) continue;
+          if (set == 0 && !(P.ifpgh == 1 && t.ns(b) > 0)) continue;
+          int i0 = set ? t.t0[b] : t.s0[b], n = set ? t.nt(b) : t.ns(b);
+          for (int c = 0; c < n; c += evch)
+            H.eval.push_back({b, set, i0 + c, std::min(evch, n - c), H.loc_slot[b], p, route});
+          H.eval_points += n;
         }
       }
     }
+  }
+  // algorithmic bytes of the shift stages: each distinct expansion read once,
+  // each written once, 16 bytes per complex coefficient
+  {
+    long long per = 16LL * P.nexp * P.nd;
+    std::vector<char> seen;
+    auto distinct = [&](const std::vector<int>& ids, int n) {
+      seen.assign(n, 0);
+      long long c = 0;
+      for (int v : ids)
+        if (v >= 0 && !seen[v]) { seen[v] = 1; c++; }
+      return c;
+    };
+    std::vector<int> a, b;
+    for (auto& s : H.merge) { a.push_back(s.src); b.push_back(s.dst); }
+    H.shift_bytes[0] = per * (distinct(a, H.nmp) + distinct(b, H.nmp));
+    a.clear(); b.clear();
+    for (auto& m : H.m2l) { b.push_back(m.loc); a.push_back(m.self_mp); }
+    for (auto& n : H.m2l_nbr) a.push_back(n.mp);
+    H.shift_bytes[1] = per * (distinct(a, H.nmp) + distinct(b, H.nloc));
+    a.clear(); b.clear();
+    for (auto& s : H.split) { a.push_back(s.src); b.push_back(s.dst); }
+    H.shift_bytes[2] = per * (distinct(a, H.nloc) + distinct(b, H.nloc));
   }
   // (d) near field, target-centric: for every leaf, the ifhung source boxes
   // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
@@ -238,7 +264,7 @@ static void build_tasks(HostPlan& H) {
       if (!L.ifhung[s]) continue;
       for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[L.l1[k]].push_back(s);
     }
-  const int CH = 128;
+  const int CH = 32;  // one warp per task
   H.direct_pairs = 0;
   for (int b = 0; b < nb; b++) {
     if (t.nchild[b] != 0) continue;

@@ -16,6 +16,12 @@ enum Route { ROUTE_HERMITE = 0, ROUTE_PW = 1, ROUTE_TAYLOR = 0 };
 struct FormTask {
   int box, s0, n, slot, p, route;
 };
+// stage (a), 3D Hermite: a chunk of a leaf's sources and the offset (in
+// doubles, per density) of its partial Hermite block
+struct FormChunk {
+  int task, s0, n;
+  long long hoff;
+};
 // stage (b) merge / split: one (parent, child) shift
 struct ShiftTask {
   int dst, src, table;  // dst slot, src slot, table row (level * nch + child slot)
@@ -34,7 +40,7 @@ struct EvalTask {
 };
 // stage (d): a chunk of evaluation points and its source ranges
 struct DirTask {
-  int set, i0, n, off, cnt;
+  int set, i0, n, off, cnt;  // points [i0, i0+n) of set; source ranges [off, off+cnt)
 };
 struct SrcRange {
   int s0, n;
@@ -81,6 +87,7 @@ struct HostPlan {
   // statistics
   long long direct_pairs = 0;
   long long form_sources = 0, eval_points = 0;
+  long long shift_bytes[3] = {0, 0, 0};  // algorithmic bytes of merge, mp->loc, split
   double host_tree_s = 0, host_lists_s = 0, host_plan_s = 0;
 };
 

@@ -9,6 +9,9 @@
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -85,6 +88,7 @@ namespace {
 struct Builder {
   Tree& t;
   int D, NCH, NCO;
+  std::vector<int> idmap;  // box id before level restriction -> current id
   explicit Builder(Tree& tt) : t(tt), D(tt.dim), NCH(tt.nch), NCO(tt.nco) {}
 
   double& C(int b, int d) { return t.centers[(size_t)b * D + d]; }
@@ -187,6 +191,7 @@ struct Builder {
         t.llast[l] = cur - 1;
       }
     }
+    for (int& v : idmap) v = map[v];
     for (int box = 0; box < nb; box++) {
       int nbx = map[box];
       t.parent[nbx] = oparent[box] >= 0 ? map[oparent[box]] : -1;
@@ -298,13 +303,13 @@ inline int child_slot(const double* x, const double* c, int D) {
 // ranges.
 void sort_points(Tree& t, const double* x, int n, std::vector<int>& perm, std::vector<int>& r0,
                  std::vector<int>& r1, const std::vector<int>& dfs_rank, int nleafrank,
-                 const std::vector<int>& leaf_of_rank) {
+                 const std::vector<int>& leaf_of_rank, const int* start = nullptr) {
   int D = t.dim;
   std::vector<int> key(n);
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     const double* p = x + (size_t)D * i;
-    int b = 0;
+    int b = start ? start[i] : 0;
     while (t.nchild[b] > 0) b = t.child[(size_t)b * t.nch + child_slot(p, &t.centers[(size_t)b * D], D)];
     key[i] = dfs_rank[b];
   }
@@ -393,6 +398,9 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
   t.llast[0] = 0;
   t.nboxes = 1;
 
+  auto T = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
+  double tA = T();
   // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
   std::vector<int> pbox(ns, 0);
   std::vector<int> count(1, ns);
@@ -413,24 +421,37 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
     t.nboxes += NCH * nref;
     t.llast[lev + 1] = t.nboxes - 1;
     count.resize(t.nboxes, 0);
-    int* cnt = count.data();
     const int* fc = firstchild.data();
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < ns; i++) {
-      int box = pbox[i];
-      if (box < a || box > b || fc[box - a] < 0) continue;
-      int c = fc[box - a] + child_slot(src + (size_t)D * i, &t.centers[(size_t)box * D], D);
-      pbox[i] = c;
-#pragma omp atomic
-      cnt[c]++;
+    const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0;
+    // per-thread counts of the new boxes, summed afterwards (no atomics)
+#pragma omp parallel
+    {
+      std::vector<int> loc(nnew, 0);
+#pragma omp for schedule(static) nowait
+      for (int i = 0; i < ns; i++) {
+        int box = pbox[i];
+        if (box < a || box > b || fc[box - a] < 0) continue;
+        int c = fc[box - a] + child_slot(src + (size_t)D * i, &t.centers[(size_t)box * D], D);
+        pbox[i] = c;
+        loc[c - c0]++;
+      }
+#pragma omp critical
+      for (int k = 0; k < nnew; k++) count[c0 + k] += loc[k];
     }
   }
   t.nlevels = lev;
   t.boxsize.resize(t.nlevels + 1);
   t.lfirst.resize(t.nlevels + 1);
   t.llast.resize(t.nlevels + 1);
+  double tB = T();
   B.colleagues_all();
+  B.idmap.resize(t.nboxes);
+  for (int k = 0; k < t.nboxes; k++) B.idmap[k] = k;
   if (t.nlevels >= 2) B.fix_lr();
+  // each source continues its descent from its box before level restriction
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < ns; i++) pbox[i] = B.idmap[pbox[i]];
+  double tC = T();
   t.level.resize(t.nboxes);
   t.parent.resize(t.nboxes);
   t.nchild.resize(t.nboxes);
@@ -455,8 +476,18 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
     }
   }
   int nl = (int)leaf_of_rank.size();
-  sort_points(t, src, ns, t.isrc, t.s0, t.s1, dfs_rank, nl, leaf_of_rank);
-  sort_points(t, trg, nt, t.itarg, t.t0, t.t1, dfs_rank, nl, leaf_of_rank);
+  double tD = T();
+  sort_points(t, src, ns, t.isrc, t.s0, t.s1, dfs_rank, nl, leaf_of_rank, pbox.data());
+  double tE = T();
+  if (trg == src && nt == ns) {  // targets given as the same array as the sources
+    t.itarg = t.isrc;
+    t.t0 = t.s0;
+    t.t1 = t.s1;
+  } else {
+    sort_points(t, trg, nt, t.itarg, t.t0, t.t1, dfs_rank, nl, leaf_of_rank);
+  }
+  double tF = T();
+  if (dbg) fprintf(stderr, "tree: refine %.3f lr %.3f dfs %.3f sort_s %.3f sort_t %.3f\n", tB - tA, tC - tB, tD - tC, tE - tD, tF - tE);
 }
 
 void build_lists(const Tree& t, Lists& L) {

@@ -53,6 +53,11 @@ typedef struct fgt_plan_info {
   double host_tree_s, host_lists_s, host_plan_s;
   int large_delta, all_direct;
   int kernel_launches;
+  /* algorithmic work per execute: stage (b) bytes counting each distinct
+   * expansion once (merge, mp->loc, split), stage (a)/(c) flops as
+   * 4 * points * npw^dim, stage (d) source-target pairs */
+  long long shift_bytes[3];
+  double form_flops, eval_flops;
 } fgt_plan_info;
 
 /* ---- context: one device, its stream and default precision -------------- */
@@ -63,6 +68,8 @@ int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
 /* the context used by the Fortran-named entry points (device 0, created on
  * first use) */
 fgt_ctx* fgt_default_ctx(void);
+/* the context's CUDA stream (a cudaStream_t) */
+void* fgt_ctx_stream(fgt_ctx* ctx);
 
 /* ---- whole transform from host arrays ------------------------------------
  * Replaces fgt2d (2d/planewave/src/fgt2d.f:19-462) and fgt3d
@@ -131,13 +138,15 @@ int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                    double* hesstarg);
 
 /* ---- plans: build the tree once, apply many times ------------------------
- * A plan fixes the points (sources, targets), delta, eps and flags.  The
- * execute calls take charges (and, for the device variant, the same point
- * coordinates already resident in device memory) and write the outputs. */
+ * A plan fixes the points (sources, targets), delta, eps and flags: it holds
+ * the tree, the lists and the points sorted into tree order on the device.
+ * The execute calls take charges and write the outputs; their point
+ * arguments are accepted for symmetry with the reference call and ignored
+ * (they may be NULL). */
 int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                     fgt_plan** out);
-/* host arrays in and out; copies inside the call */
+/* host arrays in and out; copies the charges in and the outputs back */
 int fgt_plan_execute_host(fgt_plan* plan, const double* sources, const double* charge,
                           const double* targ, double* pot, double* pottarg);
 /* device pointers in the caller's order; runs on `stream` (a cudaStream_t,
