@@ -341,23 +341,25 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
   const int Pn = T.p + 1, n2 = k.n2, npw = k.npw;
   __shared__ double part[4][PP * PP];
   __shared__ double cf[PP];
-  extern __shared__ double2 px[];  // [Pn][n2]
+  extern __shared__ double2 px[];  // [Pn][n2], then the h2x table [Pn][npw]
+  double* hx = reinterpret_cast<double*>(px + Pn * n2);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x < PP) cf[threadIdx.x] = cfac[threadIdx.x];
+  for (int e = threadIdx.x; e < Pn * npw; e += 128) hx[e] = k.h2x[e];
   __syncthreads();
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
   const int j0 = lane >> 2, tl = lane & 3;
-  double c[NT][NT][2];
+  double c[NT][NT][2], c2[NT][NT][2];
 #pragma unroll
   for (int a = 0; a < NT; a++)
 #pragma unroll
-    for (int b = 0; b < NT; b++) c[a][b][0] = c[a][b][1] = 0.0;
+    for (int b = 0; b < NT; b++) c[a][b][0] = c[a][b][1] = c2[a][b][0] = c2[a][b][1] = 0.0;
   double cj[NT];
 #pragma unroll
   for (int m = 0; m < NT; m++) cj[m] = cf[j0 + 8 * m];
-  // each warp takes steps s = warp, warp + 4, ... of four sources
-  for (int t0 = 4 * warp; t0 < T.n; t0 += 16) {
-    const int t = t0 + tl;
+  // each warp takes steps of four sources: two steps (eight sources) per
+  // iteration as independent chains, warps interleaved
+  auto rows = [&](int t, double* av, double* bv) {
     double x = 0.0, y = 0.0, q = 0.0;
     if (t < T.n) {
       const int i = T.s0 + t;
@@ -371,7 +373,6 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
     if (j0 & 2) { xa *= x2; ya *= y2; }
     if (j0 & 4) { xa *= x4; ya *= y4; }
     ya *= q;
-    double av[NT], bv[NT];
 #pragma unroll
     for (int m = 0; m < NT; m++) {
       av[m] = xa * cj[m];
@@ -379,11 +380,26 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
       xa *= x8;
       ya *= y8;
     }
+  };
+  for (int t0 = 8 * warp; t0 < T.n; t0 += 32) {
+    double av0[NT], bv0[NT], av1[NT], bv1[NT];
+    rows(t0 + tl, av0, bv0);
+    rows(t0 + 4 + tl, av1, bv1);
 #pragma unroll
     for (int a = 0; a < NT; a++)
 #pragma unroll
-      for (int b = 0; b < NT; b++) dmma_884(c[a][b][0], c[a][b][1], av[a], bv[b]);
+      for (int b = 0; b < NT; b++) {
+        dmma_884(c[a][b][0], c[a][b][1], av0[a], bv0[b]);
+        dmma_884(c2[a][b][0], c2[a][b][1], av1[a], bv1[b]);
+      }
   }
+#pragma unroll
+  for (int a = 0; a < NT; a++)
+#pragma unroll
+    for (int b = 0; b < NT; b++) {
+      c[a][b][0] += c2[a][b][0];
+      c[a][b][1] += c2[a][b][1];
+    }
   // tile (a, b) holds H[j = 8a + lane/4][k = 8b + 2 (lane%4) + i]
 #pragma unroll
   for (int a = 0; a < NT; a++)
@@ -399,7 +415,7 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
   for (int idx = threadIdx.x; idx < Pn * n2; idx += 128) {
     const int j2 = idx / n2, k2 = idx - j2 * n2;
     double2 a = make_double2(0.0, 0.0);
-    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k2] * H[j1 + PP * j2], j1);
+    for (int j1 = 0; j1 < Pn; j1++) addrot(a, hx[j1 * npw + k2] * H[j1 + PP * j2], j1);
     px[idx] = a;
   }
   __syncthreads();
@@ -408,7 +424,7 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
     const int k1 = e / n2, k2 = e - k1 * n2;
     double2 a = make_double2(0.0, 0.0);
     for (int j2 = 0; j2 < Pn; j2++) {
-      const double h = k.h2x[j2 * npw + k1];
+      const double h = hx[j2 * npw + k1];
       const double2 z = rot(px[j2 * n2 + k2], j2);
       a.x = fma(h, z.x, a.x);
       a.y = fma(h, z.y, a.y);
@@ -561,15 +577,17 @@ __global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __rest
   double* lo = sm;                                   // [PP][LD], zero padded
   double2* lx = reinterpret_cast<double2*>(sm + ((PP * LD + 1) & ~1));  // [Pn][npw]
   double2* Ls = lx + Pn * npw;                       // [nexp]
+  double* xl = reinterpret_cast<double*>(Ls + k.nexp);  // [Pn][npw]
   const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
   for (int e = threadIdx.x; e < k.nexp; e += 128) Ls[e] = L[e];
   for (int e = threadIdx.x; e < PP * LD; e += 128) lo[e] = 0.0;
+  for (int e = threadIdx.x; e < Pn * npw; e += 128) xl[e] = k.x2l[e];
   __syncthreads();
   for (int idx = threadIdx.x; idx < Pn * npw; idx += 128) {
     const int k2 = idx / npw, j1 = idx - k2 * npw;
     double2 a = make_double2(0.0, 0.0);
     for (int j2 = 0; j2 < n2; j2++) {
-      const double h = k.x2l[k2 * npw + j2];
+      const double h = xl[k2 * npw + j2];
       const double2 v = Ls[j2 + n2 * j1];
       a.x = fma(h, v.x, a.x);
       a.y = fma(h, v.y, a.y);
@@ -582,7 +600,7 @@ __global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __rest
     const double sg = (k1 & 1) ? -1.0 : 1.0;
     double2 a = make_double2(0.0, 0.0);
     for (int j1 = 0; j1 < n2; j1++) {
-      const double h = k.x2l[k1 * npw + j1];
+      const double h = xl[k1 * npw + j1];
       const double2 u = lx[k2 * npw + j1], v = lx[k2 * npw + j1 + n2];
       a.x = fma(h, fma(sg, v.x, u.x), a.x);
       a.y = fma(h, fma(sg, v.y, u.y), a.y);
@@ -601,28 +619,17 @@ __global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __rest
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
-  for (int t0 = 8 * warp; t0 < T.n; t0 += 32) {
-    // A rows: target t0 + r4, powers k2 = 4 ks + c4
-    const int ta = t0 + r4;
-    double x = 0.0, y = 0.0;
+  // two groups of eight points per warp iteration (independent MMA chains)
+  auto point = [&](int ta, double& x, double& y) {
+    x = 0.0;
+    y = 0.0;
     if (ta < T.n) {
       const int ip = T.i0 + ta;
       x = (pts[2 * ip] - cx) * k.dsq;
       y = (pts[2 * ip + 1] - cy) * k.dsq;
     }
-    const double x2 = x * x, x4 = x2 * x2;
-    double xa = (c4 & 1) ? x : 1.0;
-    if (c4 & 2) xa *= x2;
-    double c[NT][2];
-#pragma unroll
-    for (int b = 0; b < NT; b++) c[b][0] = c[b][1] = 0.0;
-#pragma unroll
-    for (int ks = 0; ks < 2 * NT; ks++) {
-#pragma unroll
-      for (int b = 0; b < NT; b++) dmma_884(c[b][0], c[b][1], xa, bf[ks][b]);
-      xa *= x4;
-    }
-    // accumulator (row = target t0 + r4, col = k1 = 8 b + 2 c4 + i)
+  };
+  auto finish = [&](int ta, double y, double (*c)[2]) {
     const double y2 = y * y, y8 = (y2 * y2) * (y2 * y2);
     double yb = (c4 & 1) ? y2 : 1.0;
     if (c4 & 2) yb *= y2 * y2;
@@ -636,6 +643,30 @@ __global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __rest
     r += __shfl_xor_sync(0xffffffffu, r, 1);
     r += __shfl_xor_sync(0xffffffffu, r, 2);
     if (c4 == 0 && ta < T.n) out[(size_t)(T.i0 + ta) * k.nd + ind] += r;
+  };
+  for (int t0 = 16 * warp; t0 < T.n; t0 += 64) {
+    const int ta0 = t0 + r4, ta1 = t0 + 8 + r4;
+    double x0, y0, x1, y1;
+    point(ta0, x0, y0);
+    point(ta1, x1, y1);
+    const double x20 = x0 * x0, x40 = x20 * x20, x21 = x1 * x1, x41 = x21 * x21;
+    double xa0 = (c4 & 1) ? x0 : 1.0, xa1 = (c4 & 1) ? x1 : 1.0;
+    if (c4 & 2) { xa0 *= x20; xa1 *= x21; }
+    double c0[NT][2], c1[NT][2];
+#pragma unroll
+    for (int b = 0; b < NT; b++) c0[b][0] = c0[b][1] = c1[b][0] = c1[b][1] = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < 2 * NT; ks++) {
+#pragma unroll
+      for (int b = 0; b < NT; b++) {
+        dmma_884(c0[b][0], c0[b][1], xa0, bf[ks][b]);
+        dmma_884(c1[b][0], c1[b][1], xa1, bf[ks][b]);
+      }
+      xa0 *= x40;
+      xa1 *= x41;
+    }
+    finish(ta0, y0, c0);
+    finish(ta1, y1, c1);
   }
 }
 
@@ -1472,7 +1503,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         dim3 g(G.end - G.beg, nd);
         const FormTask* tk = D.form + G.beg;
         if (Pn <= 32) {
-          size_t sh = (size_t)Pn * n2 * 16;
+          size_t sh = (size_t)Pn * n2 * 16 + (size_t)Pn * P.npw * 8;
 #define FORM_MMA(NT)                                                                              \
   do {                                                                                            \
     CK(cudaFuncSetAttribute(k_form2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
@@ -1557,7 +1588,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         if (Pn <= 32) {
 #define EVAL_MMA(NT)                                                                              \
   do {                                                                                            \
-    size_t sh = ((size_t)((8 * NT * (8 * NT + 1) + 1) & ~1) + 2 * (size_t)Pn * P.npw + 2 * (size_t)P.nexp) * 8; \
+    size_t sh = ((size_t)((8 * NT * (8 * NT + 1) + 1) & ~1) + 2 * (size_t)Pn * P.npw + 2 * (size_t)P.nexp + (size_t)Pn * P.npw) * 8; \
     CK(cudaFuncSetAttribute(k_eval2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
     k_eval2d_mma<NT><<<g, 128, sh, st>>>(k, tk);                                                  \
   } while (0)

@@ -220,7 +220,7 @@ static void build_tasks(HostPlan& H) {
         if (D == 3 && pw && t.ns(b) + t.nt(b) >= 1000000) route = ROUTE_TAYLOR;
         // big leaves are cut into chunks so that no CTA serialises a
         // 10^4-point leaf; each chunk rebuilds the leaf's Taylor expansion
-        const int evch = D == 2 ? 4096 : 2048;
+        const int evch = D == 2 ? 2048 : 2048;
         for (int set = 1; set >= 0; set--) {
           if (set == 1 && !(P.ifpghtarg == 1 && t.nt(b) > 0)) continue;
           if (set == 0 && !(P.ifpgh == 1 && t.ns(b) > 0)) continue;
