@@ -200,10 +200,6 @@ def ours_arm(args, w, rank, world, local_rank):
 
     dev = local_rank
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist = dist_mod
     pts = points_of(w)
     dim, nd = w["dim"], w["nd"]
 
@@ -228,16 +224,7 @@ def ours_arm(args, w, rank, world, local_rank):
         plan.execute_device(d_src.data_ptr(), d_chg.data_ptr(), d_trg.data_ptr(),
                             d_pot.data_ptr(), d_pt.data_ptr(), stream=sp)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from fgt2d_b200.replicas import barrier, max_over_ranks
 
     results = {}
     clocks = None
@@ -298,34 +285,43 @@ def ours_arm(args, w, rank, world, local_rank):
     if rank != 0:
         return 0
     hbm, tf, peak_src = measured_peaks()
-    # roofline of the dominant kernel of the headline step
-    names = {"form": "form", "merge": "merge", "m2l": "m2l", "split": "split", "eval": "eval",
-             "direct": "direct", "gather": "gather", "scatter": "scatter"}
+    fp64_tf = ctx["mixed"].fp64_mma_tflops()
+    # roofline of the dominant stage of the headline step
     dom = max(stage, key=lambda k: stage[k])
     sb = info["shift_bytes"]
-    work = {
-        "merge": ("hbm", sb[0] / 1e9, "GB/s"), "m2l": ("hbm", sb[1] / 1e9, "GB/s"),
-        "split": ("hbm", sb[2] / 1e9, "GB/s"),
-        "gather": ("hbm", (w["src"].shape[0] * (dim * 16 + nd * 16 + 4)) / 1e9, "GB/s"),
-        "scatter": ("hbm", (w["src"].shape[0] * nd * 16 + w["src"].shape[0] * 4) / 1e9, "GB/s"),
-    }
-    roof = None
-    if dom in work:
-        bound, amount, unit = work[dom]
-        ach = amount / (stage[dom] / 1e3)
-        roof = {"bound": bound, "kernel": dom, "achieved": ach, "peak": hbm, "unit": unit,
-                "frac": ach / hbm, "traffic": None, "peak_source": peak_src}
+    kernels = {"form": "k_form2d_mma / k_form3d_acc+k_form3d_h2pw", "eval": "k_eval2d_mma / k_eval3d_taylor_smem",
+               "direct": "k_direct", "merge": "k_merge", "m2l": "k_m2l", "split": "k_split",
+               "gather": "k_gather_pts", "scatter": "k_unsort"}
+    hbm_work = {"merge": sb[0], "m2l": sb[1], "split": sb[2],
+                "gather": w["src"].shape[0] * nd * (8 + 8 + 4),
+                "scatter": w["src"].shape[0] * nd * (8 + 8) + w["src"].shape[0] * 4}
+    t_dom = stage[dom] / 1e3
+    if dom in ("form", "eval"):
+        flops = info[f"{dom}_route_flops"]
+        ach = flops / t_dom / 1e12
+        roof = {"bound": "tensor", "kernel": kernels[dom], "stage": dom, "achieved": ach,
+                "peak": tf, "unit": "TFLOP/s", "frac": ach / tf, "traffic": None,
+                "peak_source": f"{peak_src} bf16 dense (burst)",
+                "fp64_mma_peak_measured": fp64_tf, "frac_of_fp64_mma": ach / fp64_tf,
+                "work": f"{flops:.4g} route flops per step (FP64 m8n8k4 MMA + FMA)"}
+    elif dom in hbm_work:
+        ach = hbm_work[dom] / t_dom / 1e9
+        roof = {"bound": "hbm", "kernel": kernels[dom], "stage": dom, "achieved": ach, "peak": hbm,
+                "unit": "GB/s", "frac": ach / hbm, "traffic": None, "peak_source": peak_src}
     else:
-        # compute-bound stages are reported against the HBM roofline of their
-        # streamed bytes; the pair / flop rates are given beside it
-        if dom == "direct":
-            streamed = (info["direct_pairs"] * 0) + w["src"].shape[0] * (dim + nd + 1) * 8
-        else:
-            streamed = w["src"].shape[0] * (dim + nd) * 8 + (info["nmp"] + info["nloc"]) * info["nexp"] * 16
-        ach = streamed / 1e9 / (stage[dom] / 1e3)
-        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "traffic": None, "peak_source": peak_src,
-                "pairs_per_s": info["direct_pairs"] / (stage["direct"] / 1e3) if stage.get("direct") else None}
+        pairs = info["direct_pairs"]
+        roof = {"bound": "hbm", "kernel": kernels[dom], "stage": dom,
+                "achieved": w["src"].shape[0] * (dim + nd) * 8 / t_dom / 1e9, "peak": hbm,
+                "unit": "GB/s", "frac": None, "traffic": None, "peak_source": peak_src,
+                "note": f"exp-bound; {pairs / t_dom:.4g} source-target pairs/s"}
+    stage_rates = {
+        "form_tflops": info["form_route_flops"] / (stage["form"] / 1e3) / 1e12 if stage.get("form") else None,
+        "eval_tflops": info["eval_route_flops"] / (stage["eval"] / 1e3) / 1e12 if stage.get("eval") else None,
+        "direct_pairs_per_s": info["direct_pairs"] / (stage["direct"] / 1e3) if stage.get("direct") else None,
+        "shift_gbs": (sb[0] + sb[1] + sb[2]) / ((stage["merge"] + stage["m2l"] + stage["split"]) / 1e3) / 1e9
+        if stage.get("merge", 0) + stage.get("m2l", 0) + stage.get("split", 0) > 0 else None,
+        "fp64_mma_peak_measured_tflops": fp64_tf,
+    }
     cpu_base = None
     if world == 1 and not args.no_cpu_baseline:
         cores = cpu_cores()
@@ -356,6 +352,7 @@ def ours_arm(args, w, rank, world, local_rank):
                 "includes": "host tree + lists + plan upload + H2D + transform + D2H"},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roof,
+        "stage_rates": stage_rates,
         "cpu_baseline": cpu_base,
         "clocks": clocks,
     }
@@ -377,7 +374,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    w = make_workload(args.workload, seed=1234 + 2 + 7919 * rank)
+    from fgt2d_b200.replicas import replica_seed
+    w = make_workload(args.workload, seed=replica_seed(1234 + 2, rank))
     if args.impl == "reference":
         return reference_arm(args, w, rank, world)
     if world > 1:

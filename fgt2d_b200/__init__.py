@@ -55,7 +55,8 @@ class PlanInfo(ctypes.Structure):
                 ("host_plan_s", ctypes.c_double), ("large_delta", ctypes.c_int),
                 ("all_direct", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("shift_bytes", ctypes.c_longlong * 3), ("form_flops", ctypes.c_double),
-                ("eval_flops", ctypes.c_double)]
+                ("eval_flops", ctypes.c_double), ("form_route_flops", ctypes.c_double),
+                ("eval_route_flops", ctypes.c_double)]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}
@@ -79,6 +80,7 @@ def lib():
     L.fgt_default_ctx.restype = _vp
     L.fgt_ctx_stream.restype = _vp
     L.fgt_ctx_stream.argtypes = [_vp]
+    L.fgt_probe_fp64_mma_tflops.argtypes = [_vp, ctypes.POINTER(ctypes.c_double)]
     L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,
                                 _dp, i, _dp, _dp, _dp]
     L.fgt_plan_create.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, ctypes.POINTER(_vp)]
@@ -132,6 +134,12 @@ class Context:
     @property
     def handle(self):
         return self._h
+
+    def fp64_mma_tflops(self):
+        """Measured FP64 tensor-core throughput of this device (TFLOP/s)."""
+        v = ctypes.c_double()
+        _check(lib().fgt_probe_fp64_mma_tflops(self._h, ctypes.byref(v)), "fgt_probe_fp64_mma_tflops")
+        return v.value
 
     @property
     def stream(self):

@@ -207,6 +207,12 @@ int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
   c->nthreads = nthreads;
   return FGT_OK;
 }
+int fgt_probe_fp64_mma_tflops(fgt_ctx* c, double* tflops) {
+  if (!c || !tflops) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(c->device));
+  CKS(probe_fp64_mma(tflops));
+  return FGT_OK;
+}
 void* fgt_ctx_stream(fgt_ctx* c) { return c ? (void*)c->stream : nullptr; }
 fgt_ctx* fgt_default_ctx(void) {
   std::call_once(g_default_once, [] {
@@ -309,6 +315,8 @@ int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
   o->large_delta = P.large_delta; o->all_direct = P.all_direct;
   o->kernel_launches = p->last_launches;
   for (int i = 0; i < 3; i++) o->shift_bytes[i] = p->H.shift_bytes[i];
+  o->form_route_flops = p->H.form_route_flops;
+  o->eval_route_flops = p->H.eval_route_flops;
   double npwd = std::pow((double)P.npw, P.dim);
   o->form_flops = 4.0 * (double)p->H.form_sources * npwd;
   o->eval_flops = 4.0 * (double)p->H.eval_points * npwd;

@@ -103,6 +103,10 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
 cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
                                 int precision, cudaStream_t stream, StageTimes* times);
 
+// Measures the FP64 tensor-core (mma.m8n8k4.f64) throughput of the current
+// device in TFLOP/s.
+cudaError_t probe_fp64_mma(double* tflops);
+
 // Large-delta path (one Taylor local about the root centre), no tree.
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
                                 const double* trg, double* pot, double* pottarg, double* work,

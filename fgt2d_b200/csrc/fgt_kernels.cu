@@ -1229,6 +1229,25 @@ __global__ void k_ld_eval(KP k, int n, const double* __restrict__ pts, double* _
   }
 }
 
+// ------------------------------------------------------------ FP64 MMA throughput probe
+// Eight independent m8n8k4 f64 accumulator chains per warp, `iters` steps:
+// 8 * 256 * iters FMAs per warp.  Used to measure the FP64 tensor-core
+// denominator of the 2D form/eval roofline on the running GPU.
+__global__ void __launch_bounds__(128) k_probe_dmma(double* out, int iters) {
+  double c[8][2];
+  const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * blockIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; i++) c[i][0] = c[i][1] = 0.0;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) dmma_884(c[i][0], c[i][1], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += c[i][0] + c[i][1];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
 // ------------------------------------------------------------ host helpers
 template <typename T>
 cudaError_t put(char*& cur, T*& dst, const std::vector<T>& v, cudaStream_t s) {
@@ -1659,6 +1678,28 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
     for (int i = 0; i < 9; i++) cudaEventDestroy(ev[i]);
   }
   return cudaSuccess;
+}
+
+cudaError_t probe_fp64_mma(double* tflops) {
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int iters = 4096, blocks = sms * 16;
+  k_probe_dmma<<<blocks, 128>>>(nullptr, 64);  // warm-up
+  CK(cudaEventRecord(e0));
+  k_probe_dmma<<<blocks, 128>>>(nullptr, iters);
+  CK(cudaEventRecord(e1));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double fma = (double)blocks * 4 * 8 * 256 * iters;
+  *tflops = 2.0 * fma / (ms * 1e-3) / 1e12;
+  return cudaGetLastError();
 }
 
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,

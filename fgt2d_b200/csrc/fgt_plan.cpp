@@ -232,6 +232,34 @@ static void build_tasks(HostPlan& H) {
       }
     }
   }
+  // flops of the routes taken: Hermite block (2 n P^d) and its separable
+  // transform, or the direct exponential sum (8 n nexp); Taylor conversion
+  // and evaluation (2 P^d per point) or direct plane-wave evaluation
+  {
+    const double n2 = P.npw / 2, npw = P.npw, nexp = P.nexp;
+    H.form_route_flops = 0;
+    for (auto& f : H.form) {
+      const double Pn = f.p + 1;
+      if (f.route == ROUTE_HERMITE) {
+        if (D == 2) H.form_route_flops += 2 * f.n * Pn * Pn + 4 * Pn * Pn * n2 + 4 * Pn * nexp;
+        else H.form_route_flops += 2 * f.n * Pn * Pn * Pn + 4 * Pn * Pn * Pn * n2 + 4 * Pn * Pn * npw * n2 + 4 * Pn * nexp;
+      } else {
+        H.form_route_flops += 8.0 * f.n * nexp;
+      }
+    }
+    H.form_route_flops *= P.nd;
+    H.eval_route_flops = 0;
+    for (auto& e : H.eval) {
+      const double Pn = e.p + 1;
+      if (e.route == ROUTE_TAYLOR) {
+        if (D == 2) H.eval_route_flops += 4 * Pn * npw * n2 + 4 * Pn * Pn * n2 + 2 * e.n * Pn * Pn;
+        else H.eval_route_flops += 4 * Pn * npw * npw * n2 + 4 * Pn * Pn * npw * n2 + 4 * Pn * Pn * Pn * n2 + 2 * e.n * Pn * Pn * Pn;
+      } else {
+        H.eval_route_flops += 8.0 * e.n * nexp;
+      }
+    }
+    H.eval_route_flops *= P.nd;
+  }
   // algorithmic bytes of the shift stages: each distinct expansion read once,
   // each written once, 16 bytes per complex coefficient
   {

@@ -88,6 +88,7 @@ struct HostPlan {
   long long direct_pairs = 0;
   long long form_sources = 0, eval_points = 0;
   long long shift_bytes[3] = {0, 0, 0};  // algorithmic bytes of merge, mp->loc, split
+  double form_route_flops = 0, eval_route_flops = 0;
   double host_tree_s = 0, host_lists_s = 0, host_plan_s = 0;
 };
 

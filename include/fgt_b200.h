@@ -58,6 +58,9 @@ typedef struct fgt_plan_info {
    * 4 * points * npw^dim, stage (d) source-target pairs */
   long long shift_bytes[3];
   double form_flops, eval_flops;
+  /* flops of the routes actually taken (Hermite/Taylor or plane wave),
+   * counting each multiply-add as 2 and complex ones as 8 */
+  double form_route_flops, eval_route_flops;
 } fgt_plan_info;
 
 /* ---- context: one device, its stream and default precision -------------- */
@@ -70,6 +73,9 @@ int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
 fgt_ctx* fgt_default_ctx(void);
 /* the context's CUDA stream (a cudaStream_t) */
 void* fgt_ctx_stream(fgt_ctx* ctx);
+/* measured FP64 tensor-core (mma.m8n8k4.f64) throughput of the context's
+ * device, in TFLOP/s: the denominator of the FP64 form/eval roofline */
+int fgt_probe_fp64_mma_tflops(fgt_ctx* ctx, double* tflops);
 
 /* ---- whole transform from host arrays ------------------------------------
  * Replaces fgt2d (2d/planewave/src/fgt2d.f:19-462) and fgt3d

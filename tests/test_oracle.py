@@ -1,0 +1,123 @@
+"""CPU checks of the oracle: the reference's own known-answer test (FGT vs FP64
+direct sum, relative l2 ``derr``), independent restatements of the generator
+and the expansion-length formulas, and the golden fixtures."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "oracle_golden.npz")
+
+
+def test_dlaran_known_answer(oracle):
+    """DLARAN is x_{k+1} = a x_k mod 2^48, a = 33952834046453 (dlaran.f:36-40),
+    seed (0,0,0,1) -> x_0 = 1; checked with exact integers."""
+    vals = oracle.hkrand(20, reset=True)
+    a, m, x = 33952834046453, 2 ** 48, 1
+    for v in vals:
+        x = (a * x) % m
+        assert v == x / m
+
+
+def _hlterms(ndim, bsize, delta, eps):
+    # g2dterms.f:19-64, written independently (1.09 is a single-precision literal)
+    e1 = math.exp(1.0)
+    r = bsize / math.sqrt(2.0 * delta)
+    p0 = int(e1 * r * r) + 1
+    rk = float(np.float32(1.09)) * (8 * math.atan(1.0)) ** -0.25
+    for p in range(p0, 301):
+        rp = r * math.sqrt(e1 / p)
+        err = ndim * rk * p ** -0.25 * rp ** p / (1 - rp)
+        if err < eps:
+            return p
+    return -1
+
+
+def _pwterms(bsize, delta, eps):
+    rmax = bsize / math.sqrt(delta)
+    d = math.sqrt(math.log(1.0 / eps))
+    pmax = 2.0 * d
+    h = 2 * math.pi / (rmax + d)
+    return pmax, 2 * int(pmax / h)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("eps", [1e-3, 1e-6, 1e-9, 1e-12])
+def test_term_counts(oracle, ndim, eps):
+    for delta in (1e-6, 1e-4, 1e-2):
+        for bs in (0.1, 0.01, 1e-3, 5e-4):
+            assert oracle.hlterms(ndim, bs, delta, eps) == _hlterms(ndim, bs, delta, eps)
+        pm, n = oracle.pwterms(0.2, delta, eps)
+        pm2, n2 = _pwterms(0.2, delta, eps)
+        assert n == n2 and abs(pm - pm2) < 1e-12
+
+
+def test_cut_level_and_npw_of_configs(oracle):
+    """npwlevel / npw of the benchmark configurations as derived from the
+    reference formulas (2D uniform N=1e5: npwlevel 5, npw 38; 2D circle
+    delta=eps=1e-6: npwlevel 9, npw 26)."""
+    rng = np.random.default_rng(0)
+    pts = rng.random((1000, 2))
+    pts[0] = (0, 0)
+    pts[1] = (1, 1)
+    lc, bs0, _ = oracle.boxsize0(2, 1e-4, 1e-9, pts, pts)
+    assert lc == 5
+    _, npw = oracle.pwterms(2 * bs0 / 2 ** 5, 1e-4, 1e-9)
+    assert npw == 38
+    lc, bs0, _ = oracle.boxsize0(2, 1e-6, 1e-6, pts, pts)
+    assert lc == 9
+    _, npw = oracle.pwterms(2 * bs0 / 2 ** 9, 1e-6, 1e-6)
+    assert npw == 26
+
+
+def test_reference_driver_2d_known_answer(oracle):
+    """test_fgt2d.f: FGT vs direct sum on the first 20 sources (reduced N)."""
+    src, q, trg, delta, eps = oracle.reference_test_inputs_2d(5000)
+    pot, _, _ = oracle.fgt(2, 1, delta, eps, src, q, trg, 1, 0)
+    ex = oracle.direct(2, 1, delta, src, q, src[:20])
+    assert oracle.derr(ex, pot[:20]) <= 10 * eps
+
+
+def test_reference_driver_3d_known_answer(oracle):
+    src, q, trg, delta, eps = oracle.reference_test_inputs_3d(5000)
+    pot, _, _ = oracle.fgt(3, 1, delta, eps, src, q, trg, 1, 0)
+    ex = oracle.direct(3, 1, delta, src, q, src[:20])
+    assert oracle.derr(ex, pot[:20]) <= 10 * eps
+
+
+@pytest.mark.parametrize("dim,n,delta,eps", [(2, 20000, 1e-4, 1e-9), (2, 20000, 1e-4, 1e-6),
+                                             (3, 15000, 1e-2, 1e-6), (3, 8000, 1e-3, 1e-3),
+                                             (2, 3000, 10.0, 1e-6), (3, 3000, 10.0, 1e-6)])
+def test_plane_wave_path_vs_direct(oracle, dim, n, delta, eps):
+    rng = np.random.default_rng(n + dim)
+    src, trg, q = rng.random((n, dim)), rng.random((n // 2, dim)), rng.random(n)
+    pot, pt, info = oracle.fgt(dim, 1, delta, eps, src, q, trg, 1, 1)
+    idx = rng.choice(n, 200, replace=False)
+    assert oracle.derr(oracle.direct(dim, 1, delta, src, q, src[idx]), pot[idx]) <= 10 * eps
+    jdx = rng.choice(n // 2, 200, replace=False)
+    assert oracle.derr(oracle.direct(dim, 1, delta, src, q, trg[jdx]), pt[jdx]) <= 10 * eps
+
+
+def test_golden_fixtures(oracle):
+    g = np.load(GOLDEN)
+    assert np.array_equal(oracle.hkrand(64, reset=True), g["hkrand_first64"])
+    src, q, trg, delta, eps = oracle.reference_test_inputs_2d(3000)
+    pot, _, info = oracle.fgt(2, 1, delta, eps, src, q, trg, 1, 0)
+    assert np.allclose(pot[:20, 0], g["ref2d_pot_first20"], rtol=1e-13, atol=1e-16)
+    assert oracle.derr(g["ref2d_direct_first20"], pot[:20, 0]) <= 10 * eps
+    src, q, trg, delta, eps = oracle.reference_test_inputs_3d(3000)
+    pot, _, _ = oracle.fgt(3, 1, delta, eps, src, q, trg, 1, 0)
+    assert np.allclose(pot[:20, 0], g["ref3d_pot_first20"], rtol=1e-13, atol=1e-16)
+    rng = np.random.default_rng(1235)
+    s2, t2, c2 = rng.random((20000, 2)), rng.random((20000, 2)), rng.random(20000)
+    p2, pt2, _ = oracle.fgt(2, 1, 1e-4, 1e-9, s2, c2, t2, 1, 1)
+    assert np.allclose(p2[:50, 0], g["pw2d_pot_first50"], rtol=1e-12)
+    assert np.allclose(pt2[:50, 0], g["pw2d_pottarg_first50"], rtol=1e-12)
+
+
+def test_derr_switches_to_absolute(oracle):
+    """derr uses an absolute norm when the exact vector is tiny (test_fgt2d.f:216-221)."""
+    ex = np.full(10, 1e-12)
+    ap = ex + 1e-13
+    assert abs(oracle.derr(ex, ap) - np.sqrt(10 * 1e-26) / 10) < 1e-20
