@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libfgt_b200.so")
 PREC_FP64, PREC_MIXED, PREC_AUTO = 0, 1, 2
 _PREC = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "auto": PREC_AUTO}
 STATUS = {0: "ok", 1: "bad argument", 2: "unsupported option", 3: "out of memory",
-          4: "CUDA error", 5: "no CUDA device"}
+          4: "CUDA error", 5: "no CUDA device", 6: "problem exceeds the fixed scratch"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -81,6 +81,7 @@ def lib():
     L.fgt_ctx_stream.restype = _vp
     L.fgt_ctx_stream.argtypes = [_vp]
     L.fgt_probe_fp64_mma_tflops.argtypes = [_vp, ctypes.POINTER(ctypes.c_double)]
+    L.fgt_large_delta_noalloc.argtypes = [i, i, d, i, _vp, _vp, i, _dp, i, _vp, i, _vp, i, _vp, _vp]
     L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,
                                 _dp, i, _dp, _dp, _dp]
     L.fgt_plan_create.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, ctypes.POINTER(_vp)]

@@ -165,6 +165,7 @@ const char* fgt_status_string(int s) {
     case FGT_ERR_NOMEM: return "out of memory";
     case FGT_ERR_CUDA: return "CUDA error";
     case FGT_ERR_NODEVICE: return "no CUDA device";
+    case FGT_ERR_SCRATCH: return "problem exceeds the fixed scratch of the allocation-free call";
     default: return "unknown status";
   }
 }
@@ -207,6 +208,31 @@ int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
   c->nthreads = nthreads;
   return FGT_OK;
 }
+int fgt_large_delta_noalloc(int dim, int nd, double delta, int ns, const double* sources,
+                            const double* charge, int nlocal, const double* center, int ifpgh,
+                            double* pot, int nt, const double* targ, int ifpghtarg,
+                            double* pottarg, void* stream) {
+  if ((dim != 2 && dim != 3) || nd < 1 || !(delta > 0) || !std::isfinite(delta) || ns < 0 ||
+      nt < 0 || nlocal < 0 || !center)
+    return FGT_ERR_BADARG;
+  if (ifpgh < 0 || ifpgh > 1 || ifpghtarg < 0 || ifpghtarg > 1) return FGT_ERR_UNSUPPORTED;
+  if ((ns > 0 && (!sources || !charge)) || (ifpgh == 1 && ns > 0 && !pot) ||
+      (ifpghtarg == 1 && nt > 0 && (!targ || !pottarg)))
+    return FGT_ERR_BADARG;
+  for (int d = 0; d < dim; d++)
+    if (!std::isfinite(center[d])) return FGT_ERR_BADARG;
+  const size_t Pn = (size_t)nlocal + 1;
+  if ((double)nd * std::pow((double)Pn, dim) > (double)large_delta_noalloc_capacity())
+    return FGT_ERR_SCRATCH;
+  Params P;
+  P.dim = dim; P.nd = nd; P.delta = delta; P.dsq = 1.0 / std::sqrt(delta);
+  P.ns = ns; P.nt = nt; P.ifpgh = ifpgh; P.ifpghtarg = ifpghtarg;
+  P.large_delta = true; P.nlocal0 = nlocal;
+  for (int d = 0; d < dim; d++) P.cen0[d] = center[d];
+  CKS(large_delta_noalloc(P, sources, charge, targ, pot, pottarg, (cudaStream_t)stream));
+  return FGT_OK;
+}
+
 int fgt_probe_fp64_mma_tflops(fgt_ctx* c, double* tflops) {
   if (!c || !tflops) return FGT_ERR_BADARG;
   CKS(cudaSetDevice(c->device));

@@ -107,6 +107,14 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
 // device in TFLOP/s.
 cudaError_t probe_fp64_mma(double* tflops);
 
+// Large-delta path with its scratch in a fixed device array instead of
+// `work`: no allocation.  cudaErrorInvalidValue when nd (nlocal0+1)^dim
+// exceeds large_delta_noalloc_capacity() doubles.
+cudaError_t large_delta_noalloc(const Params& P, const double* src, const double* chg,
+                                const double* trg, double* pot, double* pottarg,
+                                cudaStream_t stream);
+size_t large_delta_noalloc_capacity();
+
 // Large-delta path (one Taylor local about the root centre), no tree.
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
                                 const double* trg, double* pot, double* pottarg, double* work,

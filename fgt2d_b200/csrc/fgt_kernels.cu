@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "fgt_device.hpp"
 
@@ -1731,6 +1732,57 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const double
   if (P.ifpghtarg == 1) ev(trg, P.nt, pottarg);
   if (P.ifpgh == 1) ev(src, P.ns, pot);
   return cudaGetLastError();
+}
+
+
+// ------------------------------------------------------------ allocation-free large-delta call
+// Some callers cannot let this library allocate device memory: codes that
+// hand over device arrays from their own pool and run under a fixed memory
+// budget, and latency-critical loops that must not pay for cudaMalloc, which
+// can synchronise the whole device.  For them the large-delta transform (one
+// Taylor local about a given centre, the reference's fgt2d_large_delta /
+// fgt3d_large_delta) runs with its only scratch -- the centre and the local
+// expansion -- in this fixed device array.  Every device that loads the
+// library holds it (512 KB) until the process exits; every call shares it, so
+// calls that overlap on the GPU race; each call clears what it accumulates.
+namespace {
+constexpr size_t kNoAllocScratchDoubles = 65536;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles + 8];
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};
+}  // namespace
+
+size_t large_delta_noalloc_capacity() { return kNoAllocScratchDoubles; }
+
+cudaError_t large_delta_noalloc(const Params& P, const double* src, const double* chg,
+                                const double* trg, double* pot, double* pottarg, cudaStream_t st) {
+  const size_t Pn = (size_t)P.nlocal0 + 1;
+  const size_t nent = P.dim == 2 ? Pn * Pn : Pn * Pn * Pn;
+  if (P.nlocal0 < 0 || nent * P.nd > kNoAllocScratchDoubles) return cudaErrorInvalidValue;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  double* work = nullptr;
+  {
+    // the host name of the array is not a device address: its address on
+    // this device is looked up once, with this device current
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* ptr = nullptr;
+      CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+      g_noalloc_ptr[dev] = static_cast<double*>(ptr);
+    }
+    work = g_noalloc_ptr[dev];
+  }
+  // the source staging of the local-expansion kernel grows with the order
+  const int sh = (int)(3 * FORM_CH * Pn * 8);
+  if (sh > 48 * 1024) {
+    CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
+    CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
+  }
+  // large_delta_execute copies the centre into work[0..2] and clears the
+  // local expansion in work[4..] before accumulating into it
+  return large_delta_execute(P, src, chg, trg, pot, pottarg, work, st);
 }
 
 }  // namespace fgtb

@@ -32,7 +32,8 @@ enum {
   FGT_ERR_UNSUPPORTED = 2, /* dipoles, gradients/Hessians, orders too large */
   FGT_ERR_NOMEM = 3,       /* device or host allocation failed */
   FGT_ERR_CUDA = 4,        /* CUDA runtime error (see fgt_last_cuda_error) */
-  FGT_ERR_NODEVICE = 5     /* no CUDA device */
+  FGT_ERR_NODEVICE = 5,    /* no CUDA device */
+  FGT_ERR_SCRATCH = 6      /* problem larger than the fixed scratch of fgt_large_delta_noalloc */
 };
 
 enum {
@@ -182,6 +183,34 @@ int fgt_host_tree_dims(const fgt_host_tree* t, int* dims);
  * Returns the element count; copies when out != NULL. */
 long long fgt_host_tree_field(const fgt_host_tree* t, int field, void* out);
 int fgt_host_tree_destroy(fgt_host_tree* t);
+
+/* ---- allocation-free large-delta transform ----------------------------------
+ * No counterpart in the reference.  For callers that cannot let the library
+ * allocate device memory -- codes that pass device arrays from their own
+ * memory pool under a fixed budget, or latency-critical loops that must not
+ * call cudaMalloc, which can synchronise the whole device.  It runs the
+ * large-delta transform of fgt2d_large_delta / fgt3d_large_delta
+ * (fgt2d.f:1616-1733, fgt3d.f:1783-1914): one Taylor expansion of order
+ * `nlocal` about `center` (dim doubles, host memory), formed from all sources
+ * and evaluated at the sources (ifpgh = 1) and/or targets (ifpghtarg = 1);
+ * the fgt2d/fgt3d driver takes this path when the root box is far smaller
+ * than the Gaussian (cut level < -2), with the box centre and nlocal =
+ * hlterms(dim, box size, delta, eps) + max(ifpgh, ifpghtarg) - 1.
+ * All arrays are device pointers in the caller's layout: sources (ns, dim),
+ * charge (ns, nd), targ (nt, dim), pot (ns, nd), pottarg (nt, nd); outputs
+ * are overwritten.  The work runs on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without synchronising.
+ * Scratch: the local expansion lives in one fixed device array of
+ * FGT_NOALLOC_MAX_DOUBLES doubles that every device which loads the library
+ * holds until the process exits; nd * (nlocal+1)^dim larger than that returns
+ * FGT_ERR_SCRATCH.  All calls share the array: calls that overlap on the GPU
+ * race.  The first call on a device looks up the array's device address
+ * (set-up); make that first call before any stream capture. */
+#define FGT_NOALLOC_MAX_DOUBLES 65536
+int fgt_large_delta_noalloc(int dim, int nd, double delta, int ns, const double* sources,
+                            const double* charge, int nlocal, const double* center, int ifpgh,
+                            double* pot, int nt, const double* targ, int ifpghtarg,
+                            double* pottarg, void* stream);
 
 /* ---- status -------------------------------------------------------------- */
 const char* fgt_status_string(int status);
