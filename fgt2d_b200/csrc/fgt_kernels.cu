@@ -1718,6 +1718,11 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const double
   CK(cudaMemcpyAsync(cen, P.cen0, 3 * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(local, 0, nent * P.nd * sizeof(double), st));
   size_t sh = 3 * FORM_CH * Pn * 8;
+  if (sh > 227 * 1024) return cudaErrorNotSupported;
+  if (sh > 48 * 1024) {
+    CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+  }
   int blocks = std::max(1, std::min(1024, (P.ns + 255) / 256));
   if (P.ns > 0) {
     if (P.dim == 2) k_ld_form<2><<<dim3(blocks, P.nd), 256, sh, st>>>(k, P.ns, p, cen, local);
