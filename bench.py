@@ -82,29 +82,88 @@ def points_of(w):
 
 
 # ------------------------------------------------------------------ clocks
+_REASON_BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+                0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+
 class ClockSampler:
+    """SM clock and clock-event reasons sampled through NVML every ~1 ms in a
+    background thread while the timed loop runs (the timed region of a short
+    run lasts only tens of ms, too short for nvidia-smi's 200 ms polling).
+    Falls back to nvidia-smi polling when NVML is not importable."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.lines: list[str] = []
+    def __init__(self, device: int):
+        self.sm: list[float] = []
+        self.reasons: set[str] = set()
+        self.smax = None
         self.proc = None
+        self.lines: list[str] = []
+        self.stop_ev = threading.Event()
+        self.nv = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:
+                import torch
+                pr = torch.cuda.get_device_properties(device)
+                h = nv.nvmlDeviceGetHandleByUUID("GPU-" + str(pr.uuid))
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(device)
+            self.nv, self.h = nv, h
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._sample()
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(gpu_index)],
+                 "-lms", "200", "-i", str(device)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
 
+    def _sample(self):
+        nv, h = self.nv, self.h
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        try:
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        for bit, name in _REASON_BITS.items():
+            if r & bit:
+                self.reasons.add(name)
+
+    def _loop(self):
+        while not self.stop_ev.wait(0.001):
+            try:
+                self._sample()
+            except Exception:
+                break
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=5)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                    "sm_max_mhz": self.smax, "reasons": sorted(self.reasons),
+                    "samples": len(self.sm), "source": "nvml, 1 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -127,7 +186,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(k)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------------ helpers
