@@ -17,7 +17,20 @@ struct MergeGroup {
 };
 
 struct OrderGroup {
-  int p, beg, end;  // tasks [beg, end) of expansion order p
+  int p, beg, end;     // tasks [beg, end) of expansion order p
+  long long tab = -1;  // offset of the group's operand tables in DevicePlan::tables (doubles)
+};
+
+// 2D Taylor evaluation in two kernels: one plane wave -> Taylor conversion per
+// evaluation leaf (its block of nd * P * E doubles at `off`, E = P rounded up
+// to even), then point chunks of <= 256 that read the block.
+struct ConvTask {
+  int slot, p;
+  long long off;
+};
+struct HornerTask {
+  int box, set, i0, n, p;
+  long long off;
 };
 
 struct StageTimes {
@@ -83,6 +96,13 @@ struct DevicePlan {
   int eval_taylor_n = 0, eval_pw_n = 0;
   int form_pmax = 0, eval_pmax = 0;  // largest order among Hermite form / Taylor eval tasks
   std::vector<OrderGroup> form_groups, eval_groups;
+  // 2D Taylor evaluation (conversion per leaf, then Horner per point chunk)
+  long long* form_hoff = nullptr;  // 2D MMA form: per form task, offset of its Hermite block in hbuf
+  ConvTask* conv = nullptr;
+  HornerTask* horner = nullptr;
+  double* lo = nullptr;
+  double* tables = nullptr;  // padded operand tables of the 2D MMA transforms
+  std::vector<OrderGroup> conv_groups, horner_groups;
   int sm_count = 148;
   // statistics copied from the host plan
   long long direct_pairs = 0, form_sources = 0, eval_points = 0;

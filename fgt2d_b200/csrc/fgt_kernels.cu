@@ -31,6 +31,7 @@ namespace fgtb {
 namespace {
 
 constexpr int FORM_CH = 32;    // sources staged per chunk in the form kernels
+constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct KP {
   int dim, nd, npw, n2, nexp;
@@ -70,6 +71,11 @@ __device__ __forceinline__ double2 rot(double2 z, int j) {
     case 2: return make_double2(-z.x, -z.y);
     default: return make_double2(z.y, -z.x);
   }
+}
+// z * i^j without a branch on j (lanes of a warp hold different j)
+__device__ __forceinline__ double2 rot_bf(double2 z, int j) {
+  const double a = (j & 1) ? -z.y : z.x, b = (j & 1) ? z.x : z.y;
+  return (j & 2) ? make_double2(-a, -b) : make_double2(a, b);
 }
 // a + v * i^j for real v
 __device__ __forceinline__ void addrot(double2& a, double v, int j) {
@@ -318,119 +324,268 @@ __global__ void __launch_bounds__(256) k_form3d_hermite(KP k, const FormTask* __
 }
 
 // ------------------------------------------------------------ (a) form, 2D on FP64 MMA
-// Same product as k_form2d, H (P x P, P <= 8 NT) = sum_t x_t^j (q_t y_t^k),
-// on the FP64 tensor cores: mma.sync.m8n8k4.f64 takes four sources per step
-// (K = 4) into NT x NT tiles of 8 x 8.  Fragment layout (PTX ISA, m8n8k4
-// .f64): A element (row = lane/4, col = lane%4), B element (row = lane%4,
-// col = lane/4), accumulator pair (row = lane/4, col = 2 (lane%4) + i).  Lane
-// (j0 = lane/4, t = lane%4) therefore needs x_t^(j0 + 8 m) / sqrt((j0+8m)!)
-// and q_t y_t^(j0 + 8 m) / sqrt(..) for m < NT, built from x, x^2, x^4, x^8.
-// Four warps split the leaf's sources; their tiles are summed in shared
-// memory, then the Hermite -> plane-wave passes run as in k_form2d.
+// Hermite block of a leaf, H[j][k] = sum_t q_t x_t^j y_t^k (g2dformhc_vec,
+// g2drouts.f:100-168, without the 1/sqrt(j! k!) factors, which k_h2pw2d
+// folds into its tables), on the FP64 tensor cores: mma.sync.m8n8k4.f64 takes
+// four sources per step (K = 4) into NT x NT tiles of 8 x 8 (P <= 8 NT).
+// Fragment layout (PTX ISA, m8n8k4 .f64): A element (row = lane/4, col =
+// lane%4), B element (row = lane%4, col = lane/4), accumulator pair (row =
+// lane/4, col = 2 (lane%4) + i).  The powers x^j and q y^j of a block of 32
+// sources are built once per source (one lane each) in a per-warp
+// shared-memory stage laid out [j][source] with a row stride of 36 doubles, so
+// each fragment load is two conflict-free wavefronts.  Four warps split the
+// leaf's sources; their tiles are summed in shared memory and the P x P block
+// goes to the leaf's slot of the Hermite buffer.
 __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
 
+// Leading dimensions (in doubles) of zero-padded shared-memory operands of
+// the m8n8k4 FP64 MMA: an A operand with K columns is stored with a stride of
+// 4 (mod 16) and a B operand with N columns with a stride of 8 (mod 16), so
+// the eight rows (A) or four rows (B) that a fragment load touches fall in
+// distinct bank pairs: two wavefronts per load, the minimum for 256 bytes.
+__host__ __device__ __forceinline__ int mma_lda(int K) { return K <= 4 ? 4 : ((K + 11) & ~15) + 4; }
+__host__ __device__ __forceinline__ int mma_ldb(int N) { return ((N + 7) & ~15) + 8; }
+
+// Warp-level C = A B (+ C2 = A2 B2 on the same tiles when TWO) on the FP64
+// MMA with row-major, zero-padded operands in shared memory: A is
+// (8 Mt) x (4 Ks), B is (4 Ks) x (8 Nt).  out(i, j, c0, c1 [, d0, d1])
+// receives row i, columns j and j + 1 (j even) of C (and C2).  Two
+// accumulator sets alternate over the K steps.
+template <bool TWO, class Out>
+__device__ __forceinline__ void warp_gemm(const double* A, int lda, const double* B, int ldb,
+                                          const double* A2, const double* B2, int Mt, int Nt, int Ks,
+                                          Out out) {
+  const int lane = threadIdx.x & 31, r = lane >> 2, c = lane & 3;
+  for (int mt = 0; mt < Mt; mt++)
+  for (int nt = 0; nt < Nt; nt++) {
+    const int ao = (8 * mt + r) * lda + c, bo = c * ldb + 8 * nt + r;
+    double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+    double f0 = 0.0, f1 = 0.0, g0 = 0.0, g1 = 0.0;
+    for (int ks = 0; ks < Ks; ks++) {
+      const int ak = ao + 4 * ks, bk = bo + 4 * ks * ldb;
+      if (ks & 1) {
+        dmma_884(e0, e1, A[ak], B[bk]);
+        if (TWO) dmma_884(g0, g1, A2[ak], B2[bk]);
+      } else {
+        dmma_884(d0, d1, A[ak], B[bk]);
+        if (TWO) dmma_884(f0, f1, A2[ak], B2[bk]);
+      }
+    }
+    if (TWO) out(8 * mt + r, 8 * nt + 2 * c, d0 + e0, d1 + e1, f0 + g0, f1 + g1);
+    else out(8 * mt + r, 8 * nt + 2 * c, d0 + e0, d1 + e1, 0.0, 0.0);
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __restrict__ tasks,
-                                                    const double* __restrict__ cfac) {
-  constexpr int PP = 8 * NT;
+                                                    const long long* __restrict__ hoff,
+                                                    double* __restrict__ hbuf) {
+  constexpr int PP = 8 * NT, SW = 36, WS = 2 * PP * SW;  // per-warp staging [2][PP][SW]
   const FormTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
-  const int Pn = T.p + 1, n2 = k.n2, npw = k.npw;
-  __shared__ double part[4][PP * PP];
-  __shared__ double cf[PP];
-  extern __shared__ double2 px[];  // [Pn][n2], then the h2x table [Pn][npw]
-  double* hx = reinterpret_cast<double*>(px + Pn * n2);
+  const int Pn = T.p + 1;
+  extern __shared__ double smf[];
+  double* stg = smf;                                          // [4][WS]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x < PP) cf[threadIdx.x] = cfac[threadIdx.x];
-  for (int e = threadIdx.x; e < Pn * npw; e += 128) hx[e] = k.h2x[e];
-  __syncthreads();
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
   const int j0 = lane >> 2, tl = lane & 3;
-  double c[NT][NT][2], c2[NT][NT][2];
+  double* X = stg + warp * WS;  // X[j][s] = x_s^j, Y[j][s] = q_s y_s^j
+  double* Y = X + PP * SW;
+  double c[2][NT][NT][2];
 #pragma unroll
-  for (int a = 0; a < NT; a++)
-#pragma unroll
-    for (int b = 0; b < NT; b++) c[a][b][0] = c[a][b][1] = c2[a][b][0] = c2[a][b][1] = 0.0;
-  double cj[NT];
-#pragma unroll
-  for (int m = 0; m < NT; m++) cj[m] = cf[j0 + 8 * m];
-  // each warp takes steps of four sources: two steps (eight sources) per
-  // iteration as independent chains, warps interleaved
-  auto rows = [&](int t, double* av, double* bv) {
-    double x = 0.0, y = 0.0, q = 0.0;
-    if (t < T.n) {
-      const int i = T.s0 + t;
-      x = (k.src[2 * i] - cx) * k.dsq;
-      y = (k.src[2 * i + 1] - cy) * k.dsq;
-      q = k.chg[(size_t)i * k.nd + ind];
-    }
-    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
-    const double y2 = y * y, y4 = y2 * y2, y8 = y4 * y4;
-    double xa = (j0 & 1) ? x : 1.0, ya = (j0 & 1) ? y : 1.0;
-    if (j0 & 2) { xa *= x2; ya *= y2; }
-    if (j0 & 4) { xa *= x4; ya *= y4; }
-    ya *= q;
-#pragma unroll
-    for (int m = 0; m < NT; m++) {
-      av[m] = xa * cj[m];
-      bv[m] = ya * cj[m];
-      xa *= x8;
-      ya *= y8;
-    }
-  };
-  for (int t0 = 8 * warp; t0 < T.n; t0 += 32) {
-    double av0[NT], bv0[NT], av1[NT], bv1[NT];
-    rows(t0 + tl, av0, bv0);
-    rows(t0 + 4 + tl, av1, bv1);
+  for (int h = 0; h < 2; h++)
 #pragma unroll
     for (int a = 0; a < NT; a++)
 #pragma unroll
-      for (int b = 0; b < NT; b++) {
-        dmma_884(c[a][b][0], c[a][b][1], av0[a], bv0[b]);
-        dmma_884(c2[a][b][0], c2[a][b][1], av1[a], bv1[b]);
-      }
-  }
-#pragma unroll
-  for (int a = 0; a < NT; a++)
-#pragma unroll
-    for (int b = 0; b < NT; b++) {
-      c[a][b][0] += c2[a][b][0];
-      c[a][b][1] += c2[a][b][1];
+      for (int b = 0; b < NT; b++) c[h][a][b][0] = c[h][a][b][1] = 0.0;
+  // each warp takes blocks of 32 sources in turn: every lane builds the
+  // powers of one source in shared memory, then the warp runs up to eight
+  // K = 4 steps of the FP64 MMA over the block, alternating two accumulator
+  // sets so consecutive steps are independent
+  for (int base = 32 * warp; base < T.n; base += 128) {
+    double x = 0.0, y = 0.0, q = 0.0;
+    if (base + lane < T.n) {
+      const int i = T.s0 + base + lane;
+      const double2 pt = reinterpret_cast<const double2*>(k.src)[i];
+      x = (pt.x - cx) * k.dsq;
+      y = (pt.y - cy) * k.dsq;
+      q = k.chg[(size_t)i * k.nd + ind];
     }
-  // tile (a, b) holds H[j = 8a + lane/4][k = 8b + 2 (lane%4) + i]
+    double xp = 1.0, yp = q;
+#pragma unroll
+    for (int j = 0; j < PP; j++) {
+      X[j * SW + lane] = xp;
+      Y[j * SW + lane] = yp;
+      xp *= x;
+      yp *= y;
+    }
+    __syncwarp();
+    const int nst = min(8, (T.n - base + 3) >> 2);
+    for (int st = 0; st < nst; st += 2) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (st + h < nst) {
+          const int col = 4 * (st + h) + tl;
+          double av[NT], bv[NT];
+#pragma unroll
+          for (int a = 0; a < NT; a++) {
+            av[a] = X[(8 * a + j0) * SW + col];
+            bv[a] = Y[(8 * a + j0) * SW + col];
+          }
+#pragma unroll
+          for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) dmma_884(c[h][a][b][0], c[h][a][b][1], av[a], bv[b]);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // tile (a, b) holds H'[j = 8a + lane/4][k = 8b + 2 (lane%4) + i]; each warp
+  // writes its sum into its own staging area, then the four are added and
+  // the leaf's P x P block is stored row-major (x power j, y power k)
+  double* part = X;
 #pragma unroll
   for (int a = 0; a < NT; a++)
 #pragma unroll
     for (int b = 0; b < NT; b++)
 #pragma unroll
-      for (int i = 0; i < 2; i++) part[warp][(8 * a + j0) + PP * (8 * b + 2 * tl + i)] = c[a][b][i];
+      for (int i = 0; i < 2; i++)
+        part[(8 * a + j0) + PP * (8 * b + 2 * tl + i)] = c[0][a][b][i] + c[1][a][b][i];
   __syncthreads();
-  for (int e = threadIdx.x; e < PP * PP; e += 128)
-    part[0][e] = part[0][e] + part[1][e] + part[2][e] + part[3][e];
-  __syncthreads();
-  const double* H = part[0];
-  for (int idx = threadIdx.x; idx < Pn * n2; idx += 128) {
-    const int j2 = idx / n2, k2 = idx - j2 * n2;
-    double2 a = make_double2(0.0, 0.0);
-    for (int j1 = 0; j1 < Pn; j1++) addrot(a, hx[j1 * npw + k2] * H[j1 + PP * j2], j1);
-    px[idx] = a;
+  double* hb = hbuf + hoff[blockIdx.x] + (size_t)ind * Pn * Pn;
+  for (int e = threadIdx.x; e < Pn * Pn; e += 128) {
+    const int j = e / Pn, kk = e - j * Pn, f = j + PP * kk;
+    hb[e] = stg[f] + stg[WS + f] + stg[2 * WS + f] + stg[3 * WS + f];
   }
-  __syncthreads();
-  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  for (int e = threadIdx.x; e < k.nexp; e += 128) {
-    const int k1 = e / n2, k2 = e - k1 * n2;
-    double2 a = make_double2(0.0, 0.0);
-    for (int j2 = 0; j2 < Pn; j2++) {
-      const double h = hx[j2 * npw + k1];
-      const double2 z = rot(px[j2 * n2 + k2], j2);
-      a.x = fma(h, z.x, a.x);
-      a.y = fma(h, z.y, a.y);
+}
+
+// Hermite -> plane wave (g2dh2pw_real_vec, g2drouts.f:1242-1329), one warp
+// per leaf, the two 1D passes on the leaf's P x P block H[j1][j2] as FP64 MMA
+// products:
+//   px[k2][j2]  = sum_j1 i^j1 hx[j1][k2] H[j1][j2]           (pass 1)
+//   pw[k1][k2]  = sum_j2 hx[j2][k1] (i^j2 px[k2][j2])         (pass 2)
+// with hx[j][k] = h2x[j][k] / sqrt(j!).  Pass 1 splits i^j1 by parity: the even
+// rows of H give Re px and the odd rows Im px, through the table signed by
+// (j mod 4 < 2 ? + : -), so it is two real products on the same tiles.  Pass 2
+// is one real product with B[j2][2 k2 + c] = component c of i^j2 px[k2][j2].
+// The tables are shared by the CTA's warps (all leaves of a launch have one
+// order); operands are zero padded to whole tiles.
+struct H2pwDims {
+  int Pn, Ph, Mp, Kp, Np, Kq, Nq, Mq;  // see k_h2pw2d
+  int ldS, ldH, ldP, ldU;
+  int tab, warp;  // doubles: CTA tables, per-warp area
+  __host__ __device__ H2pwDims(int P, int npw) {
+    const int n2 = npw / 2;
+    Pn = P;
+    Ph = (Pn + 1) / 2;
+    Mp = (n2 + 7) & ~7;     // pass 1 rows: k2
+    Kp = (Ph + 3) & ~3;     // pass 1 depth: j1 of one parity
+    Np = (Pn + 7) & ~7;     // pass 1 columns: j2 (also the rows of the pass 2 operand)
+    Kq = (Pn + 3) & ~3;     // pass 2 depth: j2
+    Nq = (npw + 7) & ~7;    // pass 2 columns: (k2, re/im)
+    Mq = (npw + 7) & ~7;    // pass 2 rows: k1
+    ldS = mma_lda(Kp);
+    ldH = mma_ldb(Np);
+    ldP = mma_ldb(Nq > 2 * Mp ? Nq : 2 * Mp);
+    ldU = mma_lda(Kq);
+    tab = 2 * Mp * ldS + Mq * ldU;
+    warp = Np * ldP;
+  }
+};
+
+// Tables of k_h2pw2d for order P (built on the host, copied to shared
+// memory): HSe[k2][i] = s(2i) hx[2i][k2], HSo[k2][i] = s(2i+1) hx[2i+1][k2]
+// with s(j) = (j mod 4 < 2 ? 1 : -1), and HUT[k1][j2] = hx[j2][k1].
+void build_h2pw_table(const HostPlan& H, int Pn, std::vector<double>& out) {
+  const int npw = H.P.npw, n2 = npw / 2;
+  const H2pwDims Z(Pn, npw);
+  std::vector<double> cf(Pn + 1, 1.0);
+  for (int j = 1; j <= Pn; j++) cf[j] = cf[j - 1] / std::sqrt((double)j);
+  auto hx = [&](int j, int kk) { return H.h2x[(size_t)j * npw + kk] * cf[j]; };
+  const size_t base = out.size();
+  out.resize(base + Z.tab, 0.0);
+  double* HSe = out.data() + base;
+  double* HSo = HSe + Z.Mp * Z.ldS;
+  double* HUT = HSo + Z.Mp * Z.ldS;
+  for (int k2 = 0; k2 < n2; k2++)
+    for (int i = 0; 2 * i < Pn; i++) {
+      const int je = 2 * i, jo = 2 * i + 1;
+      HSe[k2 * Z.ldS + i] = (je & 2) ? -hx(je, k2) : hx(je, k2);
+      if (jo < Pn) HSo[k2 * Z.ldS + i] = (jo & 2) ? -hx(jo, k2) : hx(jo, k2);
     }
-    out[e] = a;
+  for (int k1 = 0; k1 < npw; k1++)
+    for (int j2 = 0; j2 < Pn; j2++) HUT[k1 * Z.ldU + j2] = hx(j2, k1);
+}
+
+template <int KQ>  // pass 2 depth in steps of 4: KQ = ceil(P / 4)
+__global__ void __launch_bounds__(128) k_h2pw2d(KP k, const FormTask* __restrict__ tasks, int ntask,
+                                                const long long* __restrict__ hoff,
+                                                const double* __restrict__ hbuf,
+                                                const double* __restrict__ tab) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = blockIdx.x * 4 + warp;
+  if (t >= ntask) return;  // no CTA-wide barrier in this kernel
+  const FormTask T = tasks[t];
+  const int npw = k.npw, n2 = k.n2;
+  const H2pwDims Z(T.p + 1, npw);
+  const int Pn = Z.Pn;
+  extern __shared__ double sh2[];
+  double* PB = sh2 + warp * Z.Np * Z.ldP;    // [Np][ldP]
+  const double* HSe = tab;                   // [Mp][ldS], read through L1
+  const double* HSo = HSe + Z.Mp * Z.ldS;    // [Mp][ldS]
+  const double* HUT = HSo + Z.Mp * Z.ldS;    // [Mq][ldU]
+  const int ind = blockIdx.y;
+  const double* H = hbuf + hoff[t] + (size_t)ind * Pn * Pn;
+  const int r = lane >> 2, c = lane & 3;
+  // pass 1: (Re, Im) px[k2][j2] on the same tiles, B operands He[i][j2] =
+  // H[2i][j2] and Ho[i][j2] = H[2i+1][j2] read straight from the block;
+  // PB[j2][2 k2 + c] = i^j2 px (padded rows and columns come out zero)
+  for (int nt = 0; nt < Z.Np / 8; nt++) {
+    const int j2b = 8 * nt + r;
+    for (int mt = 0; mt < Z.Mp / 8; mt++) {
+      const double* ae = HSe + (8 * mt + r) * Z.ldS + c;
+      const double* ao = HSo + (8 * mt + r) * Z.ldS + c;
+      double re0 = 0.0, re1 = 0.0, im0 = 0.0, im1 = 0.0;
+      for (int ks = 0; ks < Z.Kp / 4; ks++) {
+        const int i = 4 * ks + c, je = 2 * i, jo = 2 * i + 1;
+        const double be = (je < Pn && j2b < Pn) ? __ldg(H + je * Pn + j2b) : 0.0;
+        const double bo = (jo < Pn && j2b < Pn) ? __ldg(H + jo * Pn + j2b) : 0.0;
+        dmma_884(re0, re1, __ldg(ae + 4 * ks), be);
+        dmma_884(im0, im1, __ldg(ao + 4 * ks), bo);
+      }
+      const int k2 = 8 * mt + r, j2 = 8 * nt + 2 * c;
+      const double2 z0 = rot_bf(make_double2(re0, im0), j2);
+      const double2 z1 = rot_bf(make_double2(re1, im1), j2 + 1);
+      PB[j2 * Z.ldP + 2 * k2] = z0.x;
+      PB[j2 * Z.ldP + 2 * k2 + 1] = z0.y;
+      PB[(j2 + 1) * Z.ldP + 2 * k2] = z1.x;
+      PB[(j2 + 1) * Z.ldP + 2 * k2 + 1] = z1.y;
+    }
+  }
+  __syncwarp();
+  // pass 2: pw[k1][k2] = sum_j2 hx[j2][k1] PB[j2][(k2, c)]
+  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  for (int mt = 0; mt < Z.Mq / 8; mt++) {
+    const double* ap = HUT + (8 * mt + r) * Z.ldU + c;
+    double a[KQ];
+#pragma unroll
+    for (int ks = 0; ks < KQ; ks++) a[ks] = __ldg(ap + 4 * ks);
+    for (int nt = 0; nt < Z.Nq / 8; nt++) {
+      const double* bp = PB + c * Z.ldP + 8 * nt + r;
+      double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < KQ; ks++) {
+        if (ks & 1) dmma_884(e0, e1, a[ks], bp[4 * ks * Z.ldP]);
+        else dmma_884(d0, d1, a[ks], bp[4 * ks * Z.ldP]);
+      }
+      const int k1 = 8 * mt + r, n = 8 * nt + 2 * c;
+      if (k1 < npw && n < npw) out[k1 * n2 + (n >> 1)] = make_double2(d0 + e0, d1 + e1);
+    }
   }
 }
 
@@ -668,6 +823,209 @@ __global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __rest
     }
     finish(ta0, y0, c0);
     finish(ta1, y1, c1);
+  }
+}
+
+// ------------------------------------------------------------ (c) eval, 2D Taylor in two kernels
+// k_pw2taylor2d: one warp per evaluation leaf converts the leaf's plane-wave
+// expansion L[j2 + n2 j1] into the real Taylor block (g2dpw2local_real_vec,
+// g2drouts.f:1417-1540)
+//     lx[k2][j1] = i^k2 sum_j2 x2l[k2][j2] L[j2 + n2 j1]                     (pass A)
+//     lo[k1][k2] = 2 Re( i^k1 sum_{j1 < n2} x2l[k1][j1] (lx[k2][j1] + (-1)^k1 lx[k2][j1 + n2]) )
+// once per leaf, as FP64 MMA products, and stores it row-major with the even
+// row length E >= P (zero padded) for k_eval2d_horner.  Pass A is one real
+// product with B[j2][2 j1 + c] = component c of L[j2 + n2 j1].  2 Re(i^k1 a)
+// keeps a.x (even k1) or a.y (odd k1), so pass B is two real products: even
+// k1 against be[j1][k2] = Re(lx[k2][j1] + lx[k2][j1+n2]), odd k1 against
+// bo[j1][k2] = Im(lx[k2][j1] - lx[k2][j1+n2]).  Operands are zero padded to
+// whole tiles; the x2l tables are shared by the CTA's warps (all leaves of a
+// launch have one order).
+struct ConvDims {
+  int Pn, E, Ph, M1, K1, N1, M2, N2;
+  int ldX, ldA2, ldB2;
+  int tab, warp;  // doubles: CTA tables, per-warp area
+  __host__ __device__ ConvDims(int P, int npw) {
+    const int n2 = npw / 2;
+    Pn = P;
+    E = (Pn + 1) & ~1;
+    Ph = (Pn + 1) / 2;
+    M1 = (Pn + 7) & ~7;        // pass A rows: k2
+    K1 = (n2 + 3) & ~3;        // pass A depth j2, pass B depth j1
+    N1 = (4 * n2 + 7) & ~7;    // pass A columns: (j1, {re, im} of j1 and of j1 + n2)
+    M2 = (Ph + 7) & ~7;        // pass B rows: k1 of one parity
+    N2 = M1;                   // pass B columns: k2
+    ldX = mma_lda(K1);
+    ldA2 = mma_lda(K1);
+    ldB2 = mma_ldb(N2);
+    tab = M1 * ldX + 2 * M2 * ldA2;
+    warp = 2 * K1 * ldB2;
+  }
+};
+constexpr int CONV_MAXKS = 12;  // largest pass A depth in steps of 4: n2 <= 48
+
+// Tables of k_pw2taylor2d for order P: XA[k2][j2] = x2l[k2][j2],
+// AE[i][j1] = x2l[2i][j1], AO[i][j1] = x2l[2i+1][j1], zero padded.
+void build_conv_table(const HostPlan& H, int Pn, std::vector<double>& out) {
+  const int npw = H.P.npw, n2 = npw / 2;
+  const ConvDims Z(Pn, npw);
+  const size_t base = out.size();
+  out.resize(base + Z.tab, 0.0);
+  double* XA = out.data() + base;
+  double* AE = XA + Z.M1 * Z.ldX;
+  double* AO = AE + Z.M2 * Z.ldA2;
+  for (int r = 0; r < Pn; r++)
+    for (int c = 0; c < n2; c++) {
+      XA[r * Z.ldX + c] = H.x2l[(size_t)r * npw + c];
+      if (r % 2 == 0) AE[(r / 2) * Z.ldA2 + c] = H.x2l[(size_t)r * npw + c];
+      else AO[(r / 2) * Z.ldA2 + c] = H.x2l[(size_t)r * npw + c];
+    }
+}
+
+template <int KS>  // pass A depth in steps of 4: KS = ceil(n2 / 4)
+__global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __restrict__ tasks, int ntask,
+                                                     double* __restrict__ lo_all,
+                                                     const double* __restrict__ tab) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int t = blockIdx.x * nw + warp;
+  if (t >= ntask) return;  // no CTA-wide barrier in this kernel
+  const ConvTask T = tasks[t];
+  const int n2 = k.n2;
+  const ConvDims Z(T.p + 1, k.npw);
+  const int Pn = Z.Pn, E = Z.E;
+  extern __shared__ double s1[];
+  const double* XA = tab;                 // [M1][ldX], read through L1
+  const double* AE = XA + Z.M1 * Z.ldX;   // [M2][ldA2]
+  const double* AO = AE + Z.M2 * Z.ldA2;  // [M2][ldA2]
+  double* BE = s1 + warp * Z.warp;        // [K1][ldB2]: be[j1][k2]
+  double* BO = BE + Z.K1 * Z.ldB2;        // [K1][ldB2]: bo[j1][k2]
+  // rows of be / bo that pass A does not write
+  for (int rr = Z.N1 / 4; rr < Z.K1; rr++)
+    for (int c = lane; c < Z.ldB2; c += 32) {
+      BE[rr * Z.ldB2 + c] = 0.0;
+      BO[rr * Z.ldB2 + c] = 0.0;
+    }
+  const int ind = blockIdx.y;
+  const double* Ld = reinterpret_cast<const double*>(k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp);
+  const int r = lane >> 2, c = lane & 3;
+  // pass A: B[j2][n], n = 4 j1 + {re, im of L[.][j1], re, im of L[.][j1 + n2]},
+  // read straight from the leaf's expansion (it stays in L1 across the tiles).
+  // The accumulator pair of lane (r, c) in tile (mt, nt) is row k2 = 8 mt + r,
+  // j1 = 2 nt + c/2: lx[k2][j1] for even c, lx[k2][j1 + n2] for odd c; the
+  // partner lane (c xor 1) holds the other, so one exchange forms be and bo.
+  for (int nt = 0; nt < Z.N1 / 8; nt++) {
+    double bk[KS];
+    {
+      const int j1 = 2 * nt + (r >> 2), q = r & 3;
+      const bool ok = j1 < n2;
+      const double* bp = Ld + 2 * (c + n2 * (j1 + (q >> 1) * n2)) + (q & 1);
+#pragma unroll
+      for (int ks = 0; ks < KS; ks++) bk[ks] = (ok && 4 * ks + c < n2) ? __ldg(bp + 8 * ks) : 0.0;
+    }
+    for (int mt = 0; mt < Z.M1 / 8; mt++) {
+      const double* ap = XA + (8 * mt + r) * Z.ldX + c;
+      double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < KS; ks++) {
+        if (ks & 1) dmma_884(e0, e1, __ldg(ap + 4 * ks), bk[ks]);
+        else dmma_884(d0, d1, __ldg(ap + 4 * ks), bk[ks]);
+      }
+      const int k2 = 8 * mt + r, j1 = 2 * nt + (c >> 1);
+      const double2 z = rot_bf(make_double2(d0 + e0, d1 + e1), k2);
+      const double px = __shfl_xor_sync(FULL_MASK, z.x, 1), py = __shfl_xor_sync(FULL_MASK, z.y, 1);
+      if ((c & 1) == 0) BE[j1 * Z.ldB2 + k2] = z.x + px;  // Re(lx[j1] + lx[j1 + n2])
+      else BO[j1 * Z.ldB2 + k2] = py - z.y;               // Im(lx[j1] - lx[j1 + n2])
+    }
+  }
+  __syncwarp();
+  // pass B: 2 Re(i^k1 ...) = 2 {x, -y, -x, y}[k1 mod 4]
+  double* out = lo_all + T.off + (size_t)ind * Pn * E;
+  warp_gemm<true>(AE, Z.ldA2, BE, Z.ldB2, AO, BO, Z.M2 / 8, Z.N2 / 8, KS,  // A through L1
+                  [&](int i, int k2, double e0, double e1, double o0, double o1) {
+                    const double se = (i & 1) ? -2.0 : 2.0, so = -se;
+                    const int ke = 2 * i, ko = 2 * i + 1;
+                    if (ke < Pn) {
+                      if (k2 < E) out[ke * E + k2] = se * e0;
+                      if (k2 + 1 < E) out[ke * E + k2 + 1] = se * e1;
+                    }
+                    if (ko < Pn) {
+                      if (k2 < E) out[ko * E + k2] = so * o0;
+                      if (k2 + 1 < E) out[ko * E + k2 + 1] = so * o1;
+                    }
+                  });
+}
+
+// k_eval2d_horner: one CTA (128 threads) per chunk of <= 256 points of an
+// evaluation leaf; the leaf's Taylor block (P rows of E = 2 NP2) is staged in
+// shared memory and each thread evaluates two points (g2dlevalp_vec,
+// g2drouts.f:847-900):
+//     pot += sum_k1 y^k1 sum_k2 lo[k1][k2] x^k2,
+// Horner in x along each row (coefficient pairs read as double2), then in y.
+// Plain FP64 FMAs: on B200 the FP64 FMA pipe and the FP64 MMA share one
+// throughput, and Horner at the exact order does P (E - 1) + P FMAs a point
+// where the 8 x 8 x 4 MMA pads P up to a multiple of 8 in both dimensions.
+template <int NP2>
+__global__ void __launch_bounds__(128) k_eval2d_horner(KP k, const HornerTask* __restrict__ tasks,
+                                                       const double* __restrict__ lo_all) {
+  const HornerTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y, Pn = T.p + 1;
+  extern __shared__ double2 lo2[];  // [Pn][NP2]
+  const double2* src = reinterpret_cast<const double2*>(lo_all + T.off + (size_t)ind * Pn * 2 * NP2);
+  for (int e = threadIdx.x; e < Pn * NP2; e += blockDim.x) lo2[e] = src[e];
+  __syncthreads();
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
+  const int ta = threadIdx.x, tb = threadIdx.x + 128;
+  if (ta >= T.n) return;
+  const bool two = tb < T.n;
+  const double2 pa = reinterpret_cast<const double2*>(pts)[T.i0 + ta];
+  const double2 pb = reinterpret_cast<const double2*>(pts)[T.i0 + (two ? tb : ta)];
+  const double x0 = (pa.x - cx) * k.dsq, y0 = (pa.y - cy) * k.dsq;
+  const double x1 = (pb.x - cx) * k.dsq, y1 = (pb.y - cy) * k.dsq;
+  double r0 = 0.0, r1 = 0.0;
+  for (int k1 = Pn - 1; k1 >= 0; k1--) {
+    const double2* rw = lo2 + k1 * NP2;
+    const double2 ct = rw[NP2 - 1];
+    double s0 = fma(ct.y, x0, ct.x), s1 = fma(ct.y, x1, ct.x);
+#pragma unroll
+    for (int m = NP2 - 2; m >= 0; m--) {
+      const double2 c = rw[m];
+      s0 = fma(s0, x0, c.y);
+      s1 = fma(s1, x1, c.y);
+      s0 = fma(s0, x0, c.x);
+      s1 = fma(s1, x1, c.x);
+    }
+    r0 = fma(r0, y0, s0);
+    r1 = fma(r1, y1, s1);
+  }
+  out[(size_t)(T.i0 + ta) * k.nd + ind] += r0;
+  if (two) out[(size_t)(T.i0 + tb) * k.nd + ind] += r1;
+}
+
+// Orders above 64 (rows longer than 64): the same evaluation with a runtime
+// row length.
+__global__ void __launch_bounds__(128) k_eval2d_horner_any(KP k, const HornerTask* __restrict__ tasks,
+                                                           const double* __restrict__ lo_all) {
+  const HornerTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y, Pn = T.p + 1, E = (Pn + 1) & ~1;
+  extern __shared__ double lo1[];  // [Pn][E]
+  const double* src = lo_all + T.off + (size_t)ind * Pn * E;
+  for (int e = threadIdx.x; e < Pn * E; e += blockDim.x) lo1[e] = src[e];
+  __syncthreads();
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
+  for (int t = threadIdx.x; t < T.n; t += blockDim.x) {
+    const double2 pa = reinterpret_cast<const double2*>(pts)[T.i0 + t];
+    const double x = (pa.x - cx) * k.dsq, y = (pa.y - cy) * k.dsq;
+    double r = 0.0;
+    for (int k1 = Pn - 1; k1 >= 0; k1--) {
+      const double* rw = lo1 + k1 * E;
+      double s = rw[Pn - 1];
+      for (int k2 = Pn - 2; k2 >= 0; k2--) s = fma(s, x, rw[k2]);
+      r = fma(r, y, s);
+    }
+    out[(size_t)(T.i0 + t) * k.nd + ind] += r;
   }
 }
 
@@ -1078,11 +1436,56 @@ __global__ void __launch_bounds__(256) k_eval3d_pw(KP k, const EvalTask* __restr
 }
 
 // ------------------------------------------------------------ (d) near field
-// One CTA per chunk of <= 128 evaluation points; every source range of the
-// chunk is staged through shared memory.  pot += q exp(-r^2/delta) when
-// r^2 < dmax.  MIXED computes exp in FP32 on the SFU (ex2.approx) from an
-// FP64 argument and accumulates in FP64.
-template <int DIM, bool MIXED>
+// Source list of a near-field task: the concatenation of its source ranges
+// (leaves of its list1).  A warp walks it in batches of at most CAP sources:
+// ranges are read 32 at a time (one per lane) and prefix-summed with
+// shuffles; for the batch starting at b0 each lane maps its slots
+// b0 + lane + 32 u to source indices by a binary search over the lanes'
+// prefixes, so all loads of a batch can be in flight together (a range at a
+// time would serialise one load round trip per range).
+struct RangeChunk {
+  int nr, excl, s0, tot;  // ranges in the chunk; this lane's exclusive prefix and start; chunk size
+};
+__device__ __forceinline__ RangeChunk load_range_chunk(const SrcRange* __restrict__ ranges, int off,
+                                                       int cnt, int rc, int lane) {
+  RangeChunk C;
+  C.nr = min(32, cnt - rc);
+  int rn = 0;
+  C.s0 = 0;
+  if (lane < C.nr) {
+    const SrcRange R = ranges[off + rc + lane];
+    rn = R.n;
+    C.s0 = R.s0;
+  }
+  int inc = rn;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL_MASK, inc, o);
+    if (lane >= o) inc += v;
+  }
+  C.excl = inc - rn;
+  C.tot = __shfl_sync(FULL_MASK, inc, 31);
+  return C;
+}
+// source index of slot s (0 <= s < C.tot) of the chunk; all lanes must call
+__device__ __forceinline__ int range_slot_source(const RangeChunk& C, int s) {
+  int lo = 0, hi = C.nr;
+#pragma unroll
+  for (int it = 0; it < 5; it++) {
+    const int mid = (lo + hi) >> 1;
+    if (__shfl_sync(FULL_MASK, C.excl, mid) <= s) lo = mid;
+    else hi = mid;
+  }
+  return __shfl_sync(FULL_MASK, C.s0, lo) + (s - __shfl_sync(FULL_MASK, C.excl, lo));
+}
+
+// ------------------------------------------------------------ (d) near field, kernels
+// One warp per chunk of <= 32 evaluation points (g2d_directcp_vec,
+// g2ddirect.f:32-76; g3d_directcp_vec, g3ddirect.f:3-49): the chunk's source
+// ranges are staged through the warp's shared memory in batches of 256, and
+// g lanes per point (g n <= 32) split the sources of that point.
+// pot += q exp(-r^2/delta) when r^2 < dmax, all in FP64.
+template <int DIM>
 __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict__ tasks, int ntask,
                                                 const SrcRange* __restrict__ ranges) {
   constexpr int CAP = 256;  // sources staged per warp and batch
@@ -1107,45 +1510,160 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
   const double tx = pts[DIM * ip], ty = pts[DIM * ip + 1];
   const double tz = DIM == 3 ? pts[DIM * ip + 2] : 0.0;
   const double ninv = -1.0 / k.delta;
-  const double nl2 = -1.4426950408889634 / k.delta;
   double acc = 0.0;
-  int r = 0, roff = 0;
-  while (r < T.cnt) {
-    int m = 0;
-    __syncwarp();
-    while (r < T.cnt && m < CAP) {
-      const SrcRange R = ranges[T.off + r];
-      const int take = min(CAP - m, R.n - roff);
-      for (int t = lane; t < take; t += 32) {
-        const int j = R.s0 + roff + t;
-        sx[m + t] = k.src[DIM * j];
-        sy[m + t] = k.src[DIM * j + 1];
-        if (DIM == 3) sz[m + t] = k.src[DIM * j + 2];
-        sq[m + t] = k.chg[(size_t)j * k.nd + ind];
-      }
-      m += take;
-      roff += take;
-      if (roff == R.n) { r++; roff = 0; }
-    }
-    __syncwarp();
-    if (act) {
-#pragma unroll 4
-      for (int t = sub; t < m; t += g) {
-        const double dx = tx - sx[t], dy = ty - sy[t];
-        double rr = fma(dx, dx, dy * dy);
-        if (DIM == 3) {
-          const double dz = tz - sz[t];
-          rr = fma(dz, dz, rr);
+  for (int rc = 0; rc < T.cnt; rc += 32) {
+    const RangeChunk C = load_range_chunk(ranges, T.off, T.cnt, rc, lane);
+    for (int b0 = 0; b0 < C.tot; b0 += CAP) {
+      const int m = min(CAP, C.tot - b0);
+      int js[CAP / 32];
+#pragma unroll
+      for (int u = 0; u < CAP / 32; u++) js[u] = range_slot_source(C, b0 + lane + 32 * u);
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < CAP / 32; u++) {
+        const int t = lane + 32 * u;
+        if (t < m) {
+          const int j = js[u];
+          sx[t] = k.src[DIM * j];
+          sy[t] = k.src[DIM * j + 1];
+          if (DIM == 3) sz[t] = k.src[DIM * j + 2];
+          sq[t] = k.chg[(size_t)j * k.nd + ind];
         }
-        if (rr < k.dmax) {
-          if (MIXED) acc = fma((double)ex2_approx((float)(rr * nl2)), sq[t], acc);
-          else acc = fma(exp(rr * ninv), sq[t], acc);
+      }
+      __syncwarp();
+      if (act) {
+#pragma unroll 4
+        for (int t = sub; t < m; t += g) {
+          const double dx = tx - sx[t], dy = ty - sy[t];
+          double rr = fma(dx, dx, dy * dy);
+          if (DIM == 3) {
+            const double dz = tz - sz[t];
+            rr = fma(dz, dz, rr);
+          }
+          if (rr < k.dmax) acc = fma(exp(rr * ninv), sq[t], acc);
         }
       }
     }
   }
   for (int o = 1; o < g; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (act && sub == 0) out[(size_t)ip * k.nd + ind] += acc;
+}
+
+// Mixed form of the near field (eps >= 1e-6): the same task structure with
+// the pair arithmetic in FP32.  Coordinates are taken relative to the task's
+// first target, scaled by sqrt(log2(e) / delta) and split into a float pair
+// (hi, lo), so dx = (t_hi - s_hi) + (t_lo - s_lo) carries about FP32 relative
+// accuracy in dx itself (not in the coordinates); the Gaussian is then
+// 2^-(dx^2 + dy^2 (+ dz^2)) by ex2.approx.  Each lane holds NTL = 4 targets,
+// so a staged source is read from shared memory once for four pairs; g lanes
+// per target group (g * groups <= 32) split the sources.  Groups of four
+// sources are summed in FP32 per target and added into FP64 accumulators.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __restrict__ tasks, int ntask,
+                                                      const SrcRange* __restrict__ ranges, double cs,
+                                                      float amax) {
+  constexpr int CAP = 256, NTL = 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 4 + warp;
+  __shared__ float fsm[4][(2 * DIM + 1) * CAP];
+  if (w >= ntask) return;  // whole warp leaves; no block-wide barrier below
+  const DirTask T = tasks[w];
+  const int ind = blockIdx.y;
+  float* sh = fsm[warp];           // [DIM][CAP] hi parts
+  float* sl = sh + DIM * CAP;      // [DIM][CAP] lo parts
+  float* sq = sl + DIM * CAP;      // [CAP] charges
+  const int ngr = (T.n + NTL - 1) / NTL;
+  int g = 1;
+  while (g * 2 * ngr <= 32) g *= 2;
+  const int tt = lane / g, sub = lane - tt * g;
+  const bool act = tt < ngr;
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  double o[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) o[d] = pts[DIM * T.i0 + d];
+  float th[NTL][DIM], tl[NTL][DIM];
+  double acc[NTL];
+#pragma unroll
+  for (int v = 0; v < NTL; v++) {
+    acc[v] = 0.0;
+    const int it = min(tt * NTL + v, T.n - 1);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double x = (pts[DIM * (T.i0 + it) + d] - o[d]) * cs;
+      th[v][d] = (float)x;
+      tl[v][d] = (float)(x - (double)th[v][d]);
+    }
+  }
+  for (int rc = 0; rc < T.cnt; rc += 32) {
+   const RangeChunk C = load_range_chunk(ranges, T.off, T.cnt, rc, lane);
+   for (int b0 = 0; b0 < C.tot; b0 += CAP) {
+    const int m = min(CAP, C.tot - b0);
+    int js[CAP / 32];
+#pragma unroll
+    for (int u = 0; u < CAP / 32; u++) js[u] = range_slot_source(C, b0 + lane + 32 * u);
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < CAP / 32; u++) {
+      const int t = lane + 32 * u;
+      if (t < m) {
+        const int j = js[u];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const double x = (k.src[DIM * j + d] - o[d]) * cs;
+          const float h = (float)x;
+          sh[d * CAP + t] = h;
+          sl[d * CAP + t] = (float)(x - (double)h);
+        }
+        sq[t] = (float)k.chg[(size_t)j * k.nd + ind];
+      }
+    }
+    __syncwarp();
+    if (act) {
+      for (int t = sub; t < m; t += 4 * g) {
+        float part[NTL];
+#pragma unroll
+        for (int v = 0; v < NTL; v++) part[v] = 0.0f;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int tu = t + u * g;
+          if (tu < m) {
+            float sH[DIM], sL[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+              sH[d] = sh[d * CAP + tu];
+              sL[d] = sl[d * CAP + tu];
+            }
+            const float q = sq[tu];
+#pragma unroll
+            for (int v = 0; v < NTL; v++) {
+              float a = 0.0f;
+#pragma unroll
+              for (int d = 0; d < DIM; d++) {
+                const float dx = (th[v][d] - sH[d]) + (tl[v][d] - sL[d]);
+                a = fmaf(dx, dx, a);
+              }
+              const float e = ex2_approx(-a);
+              part[v] = a < amax ? fmaf(e, q, part[v]) : part[v];
+            }
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < NTL; v++) acc[v] += (double)part[v];
+      }
+    }
+   }
+  }
+#pragma unroll
+  for (int v = 0; v < NTL; v++)
+    for (int o2 = 1; o2 < g; o2 <<= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o2);
+  if (act && sub == 0) {
+#pragma unroll
+    for (int v = 0; v < NTL; v++) {
+      const int it = tt * NTL + v;
+      if (it < T.n) out[(size_t)(T.i0 + it) * k.nd + ind] += acc[v];
+    }
+  }
 }
 
 // ------------------------------------------------------------ large delta
@@ -1314,6 +1832,50 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
     D.eval_groups.push_back({ev[t].p, t, u});
     t = u;
   }
+  // 2D Taylor evaluation: one conversion per leaf slot, point chunks of <= 256
+  std::vector<ConvTask> conv;
+  std::vector<HornerTask> horner;
+  size_t lo_doubles = 0;
+  if (P.dim == 2 && !P.all_direct) {
+    std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
+    for (int t = 0; t < D.eval_taylor_n; t++) {
+      const EvalTask& e = ev[t];
+      const long long Pn = e.p + 1, E = (Pn + 1) & ~1LL;
+      if (slot_off[e.slot] < 0) {
+        slot_off[e.slot] = (long long)lo_doubles;
+        conv.push_back({e.slot, e.p, (long long)lo_doubles});
+        lo_doubles += (size_t)(P.nd * Pn * E);
+      }
+      for (int c = 0; c < e.n; c += 256)
+        horner.push_back({e.box, e.set, e.i0 + c, std::min(256, e.n - c), e.p, slot_off[e.slot]});
+    }
+    // conv and horner are in order of p (the Taylor tasks are sorted by p)
+    for (size_t t = 0; t < conv.size();) {
+      size_t u = t;
+      while (u < conv.size() && conv[u].p == conv[t].p) u++;
+      D.conv_groups.push_back({conv[t].p, (int)t, (int)u});
+      t = u;
+    }
+    for (size_t t = 0; t < horner.size();) {
+      size_t u = t;
+      while (u < horner.size() && horner[u].p == horner[t].p) u++;
+      D.horner_groups.push_back({horner[t].p, (int)t, (int)u});
+      t = u;
+    }
+  }
+  // padded operand tables of the 2D MMA transforms, one per order group
+  std::vector<double> tables;
+  if (P.dim == 2 && !P.all_direct) {
+    for (OrderGroup& G : D.form_groups)
+      if (G.p + 1 <= 32) {
+        G.tab = (long long)tables.size();
+        build_h2pw_table(H, G.p + 1, tables);
+      }
+    for (OrderGroup& G : D.conv_groups) {
+      G.tab = (long long)tables.size();
+      build_conv_table(H, G.p + 1, tables);
+    }
+  }
   // merge groups: consecutive tasks with the same destination
   std::vector<MergeGroup> groups;
   D.merge_beg.assign(P.nlevels + 1, 0);
@@ -1341,6 +1903,17 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   std::vector<FormChunk> fchunks;
   std::vector<int> fcbeg;
   size_t hbuf_doubles = 0;
+  // 2D: Hermite blocks of the MMA form (orders <= 31), nd P^2 doubles per leaf
+  std::vector<long long> form_hoff;
+  if (P.dim == 2 && !P.all_direct) {
+    form_hoff.assign(form.size(), 0);
+    for (int t = 0; t < D.form_hermite_n; t++) {
+      const long long Pn = form[t].p + 1;
+      if (Pn > 32) continue;
+      form_hoff[t] = (long long)hbuf_doubles;
+      hbuf_doubles += (size_t)(P.nd * Pn * Pn);
+    }
+  }
   if (P.dim == 3 && !P.all_direct) {
     const size_t lim = 227 * 1024;
     const int n2 = P.npw / 2;
@@ -1400,7 +1973,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
                  al(nt * dim * 8) + al(ns * nd * 8) + al(nt * nd * 8) +
                  al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
-                 bytes_of(fcbeg) + al(hbuf_doubles * 8) + 4096;
+                 bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
+                 al(lo_doubles * 8) + 4096;
   D.bytes = total;
   CK(cudaMalloc(&D.base, total));
   char* cur = D.base;
@@ -1446,6 +2020,11 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   CK(put(cur, D.dir_src, H.dir_src, s));
   CK(put(cur, D.fchunks, fchunks, s));
   CK(put(cur, D.fcbeg, fcbeg, s));
+  CK(put(cur, D.form_hoff, form_hoff, s));
+  CK(put(cur, D.tables, tables, s));
+  CK(put(cur, D.conv, conv, s));
+  CK(put(cur, D.horner, horner, s));
+  D.lo = reinterpret_cast<double*>(cur); cur += al(lo_doubles * 8);
   D.hbuf = reinterpret_cast<double*>(cur); cur += al(hbuf_doubles * 8);
   D.mp = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nmp * nd * P.nexp * 16);
   D.loc = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nloc * nd * P.nexp * 16);
@@ -1523,17 +2102,34 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         dim3 g(G.end - G.beg, nd);
         const FormTask* tk = D.form + G.beg;
         if (Pn <= 32) {
-          size_t sh = (size_t)Pn * n2 * 16 + (size_t)Pn * P.npw * 8;
 #define FORM_MMA(NT)                                                                              \
   do {                                                                                            \
+    const size_t sh = (size_t)4 * 2 * (8 * NT) * 36 * 8;                                          \
     CK(cudaFuncSetAttribute(k_form2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_form2d_mma<NT><<<g, 128, sh, st>>>(k, tk, D.cfac);                                          \
+    k_form2d_mma<NT><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);                     \
   } while (0)
           if (Pn <= 8) FORM_MMA(1);
           else if (Pn <= 16) FORM_MMA(2);
           else if (Pn <= 24) FORM_MMA(3);
           else FORM_MMA(4);
 #undef FORM_MMA
+          const int nt = G.end - G.beg;
+          const H2pwDims Z(Pn, P.npw);
+          const size_t sh2 = 4 * (size_t)Z.warp * 8;
+          if (sh2 > 227 * 1024) return cudaErrorNotSupported;
+          const dim3 hg((nt + 3) / 4, nd);
+          switch (Z.Kq / 4) {
+#define H2PW_CASE(N)                                                                              \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_h2pw2d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh2)); \
+    k_h2pw2d<N><<<hg, 128, sh2, st>>>(k, tk, nt, D.form_hoff + G.beg, D.hbuf, D.tables + G.tab);  \
+    break;
+            H2PW_CASE(1) H2PW_CASE(2) H2PW_CASE(3) H2PW_CASE(4) H2PW_CASE(5) H2PW_CASE(6)
+            H2PW_CASE(7) H2PW_CASE(8)
+#undef H2PW_CASE
+            default: return cudaErrorNotSupported;
+          }
+          launches++;
         } else {
           const int tpd = (Pn + 3) / 4, Pp = 4 * tpd;
           if (tpd * tpd > 256) return cudaErrorNotSupported;
@@ -1601,26 +2197,50 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
     mark(5);
     // (c) eval
     if (P.dim == 2 && D.neval > 0) {
-      for (const OrderGroup& G : D.eval_groups) {
-        const int Pn = G.p + 1;
-        dim3 g(G.end - G.beg, nd);
-        const EvalTask* tk = D.eval + G.beg;
-        if (Pn <= 32) {
-#define EVAL_MMA(NT)                                                                              \
-  do {                                                                                            \
-    size_t sh = ((size_t)((8 * NT * (8 * NT + 1) + 1) & ~1) + 2 * (size_t)Pn * P.npw + 2 * (size_t)P.nexp + (size_t)Pn * P.npw) * 8; \
-    CK(cudaFuncSetAttribute(k_eval2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_eval2d_mma<NT><<<g, 128, sh, st>>>(k, tk);                                                  \
-  } while (0)
-          if (Pn <= 8) EVAL_MMA(1);
-          else if (Pn <= 16) EVAL_MMA(2);
-          else if (Pn <= 24) EVAL_MMA(3);
-          else EVAL_MMA(4);
-#undef EVAL_MMA
-        } else {
-          size_t sh = (2 * (size_t)Pn * P.npw + (size_t)Pn * Pn) * 8;
-          CK(cudaFuncSetAttribute(k_eval2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-          k_eval2d<<<g, 256, sh, st>>>(k, tk);
+      for (const OrderGroup& G : D.conv_groups) {
+        const int Pn = G.p + 1, nt = G.end - G.beg;
+        const ConvDims Z(Pn, P.npw);
+        if (Z.K1 / 4 > CONV_MAXKS) return cudaErrorNotSupported;
+        int nw = 4;
+        while (nw > 1 && (size_t)nw * Z.warp * 8 > 100 * 1024) nw >>= 1;
+        const size_t sh = (size_t)nw * Z.warp * 8;
+        if (sh > 227 * 1024) return cudaErrorNotSupported;
+        const dim3 cg((nt + nw - 1) / nw, nd);
+        switch (Z.K1 / 4) {
+#define CONV_CASE(N)                                                                              \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_pw2taylor2d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_pw2taylor2d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab);     \
+    break;
+          CONV_CASE(1) CONV_CASE(2) CONV_CASE(3) CONV_CASE(4) CONV_CASE(5) CONV_CASE(6)
+          CONV_CASE(7) CONV_CASE(8) CONV_CASE(9) CONV_CASE(10) CONV_CASE(11) CONV_CASE(12)
+#undef CONV_CASE
+          default: return cudaErrorNotSupported;
+        }
+        launches++;
+      }
+      for (const OrderGroup& G : D.horner_groups) {
+        const int Pn = G.p + 1, np2 = (Pn + 1) / 2;
+        const dim3 g(G.end - G.beg, nd);
+        const HornerTask* tk = D.horner + G.beg;
+        const size_t sh = (size_t)Pn * np2 * 16;
+        if (sh > 227 * 1024) return cudaErrorNotSupported;
+        switch (np2) {
+#define HORNER_CASE(N)                                                                            \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_eval2d_horner<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_eval2d_horner<N><<<g, 128, sh, st>>>(k, tk, D.lo);                                          \
+    break;
+          HORNER_CASE(1) HORNER_CASE(2) HORNER_CASE(3) HORNER_CASE(4) HORNER_CASE(5) HORNER_CASE(6)
+          HORNER_CASE(7) HORNER_CASE(8) HORNER_CASE(9) HORNER_CASE(10) HORNER_CASE(11) HORNER_CASE(12)
+          HORNER_CASE(13) HORNER_CASE(14) HORNER_CASE(15) HORNER_CASE(16) HORNER_CASE(17) HORNER_CASE(18)
+          HORNER_CASE(19) HORNER_CASE(20) HORNER_CASE(21) HORNER_CASE(22) HORNER_CASE(23) HORNER_CASE(24)
+          HORNER_CASE(25) HORNER_CASE(26) HORNER_CASE(27) HORNER_CASE(28) HORNER_CASE(29) HORNER_CASE(30)
+          HORNER_CASE(31) HORNER_CASE(32)
+#undef HORNER_CASE
+          default:
+            CK(cudaFuncSetAttribute(k_eval2d_horner_any, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+            k_eval2d_horner_any<<<g, 128, sh, st>>>(k, tk, D.lo);
         }
         launches++;
       }
@@ -1648,13 +2268,16 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
   // (d) near field
   if (D.ndir > 0) {
     dim3 g((D.ndir + 3) / 4, nd);
-    bool mixed = precision == PREC_MIXED;
+    const bool mixed = precision == PREC_MIXED;
+    const double l2e = 1.4426950408889634;
+    const double cs = std::sqrt(l2e / P.delta);
+    const float amax = (float)(P.dmax * l2e / P.delta);
     if (P.dim == 2) {
-      if (mixed) k_direct<2, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
-      else k_direct<2, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      if (mixed) k_direct_mixed<2><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
+      else k_direct<2><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
     } else {
-      if (mixed) k_direct<3, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
-      else k_direct<3, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      if (mixed) k_direct_mixed<3><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
+      else k_direct<3><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
     }
     launches++;
   }
