@@ -77,6 +77,8 @@ def lib():
     L.fgt_ctx_destroy.argtypes = [_vp]
     L.fgt_ctx_set_precision.argtypes = [_vp, i]
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
+    L.fgt_ctx_set_tree.argtypes = [_vp, i]
+    L.fgt_device_tree_create.argtypes = [_vp, i, d, d, i, _dp, i, _dp, ctypes.POINTER(_vp)]
     L.fgt_default_ctx.restype = _vp
     L.fgt_ctx_stream.restype = _vp
     L.fgt_ctx_stream.argtypes = [_vp]
@@ -119,14 +121,19 @@ def _p(a):
 class Context:
     """One CUDA device, its stream and the precision mode."""
 
-    def __init__(self, device=0, precision="auto", host_threads=0):
+    def __init__(self, device=0, precision="auto", host_threads=0, tree="device"):
         L = lib()
         h = _vp()
         _check(L.fgt_ctx_create(int(device), ctypes.byref(h)), "fgt_ctx_create")
         self._h = h
         self.set_precision(precision)
+        self.set_tree(tree)
         if host_threads:
             L.fgt_ctx_set_host_threads(self._h, int(host_threads))
+
+    def set_tree(self, where):
+        """Where plans build their tree: "device" (point work on the GPU) or "host"."""
+        _check(lib().fgt_ctx_set_tree(self._h, {"device": 0, "host": 1}[where]), "fgt_ctx_set_tree")
 
     def set_precision(self, precision):
         p = _PREC[precision] if isinstance(precision, str) else int(precision)
@@ -260,11 +267,28 @@ def HostTree(dim, delta, eps, sources, targ, nthreads=0):
     """The host tree of the transform in the reference's conventions (1-based)."""
     L = lib()
     src = _f64(sources, (-1, dim))
-    trg = _f64(targ, (-1, dim))
+    trg = src if targ is sources else _f64(targ, (-1, dim))
     h = _vp()
     _check(L.fgt_host_tree_create(dim, float(delta), float(eps), src.shape[0], _p(src),
                                   trg.shape[0], _p(trg), int(nthreads), ctypes.byref(h)),
            "fgt_host_tree_create")
+    return _tree_dict(h)
+
+
+def DeviceTree(ctx, dim, delta, eps, sources, targ):
+    """The same tree built with its point work on the context's GPU."""
+    L = lib()
+    src = _f64(sources, (-1, dim))
+    trg = src if targ is sources else _f64(targ, (-1, dim))
+    h = _vp()
+    _check(L.fgt_device_tree_create(ctx.handle, dim, float(delta), float(eps), src.shape[0], _p(src),
+                                    trg.shape[0], _p(trg), ctypes.byref(h)),
+           "fgt_device_tree_create")
+    return _tree_dict(h)
+
+
+def _tree_dict(h):
+    L = lib()
     try:
         dims = np.zeros(4, dtype=np.int32)
         st = L.fgt_host_tree_dims(h, dims.ctypes.data_as(_ip))

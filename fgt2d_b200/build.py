@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfgt_b200.so")
-SOURCES = ["fgt_kernels.cu", "fgt_tree.cpp", "fgt_plan.cpp", "fgt_capi.cpp"]
+SOURCES = ["fgt_kernels.cu", "fgt_devtree.cu", "fgt_tree.cpp", "fgt_plan.cpp", "fgt_capi.cpp"]
 HEADERS = ["fgt_tree.hpp", "fgt_plan.hpp", "fgt_device.hpp"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 

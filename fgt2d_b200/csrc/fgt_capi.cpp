@@ -19,6 +19,7 @@ struct fgt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int precision = FGT_PREC_AUTO;
+  int tree = FGT_TREE_DEVICE;
   int nthreads = 0;
   std::mutex mu;
 };
@@ -83,6 +84,36 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
   return FGT_OK;
 }
 
+// Device copies of the caller-order arrays (sources, charges, targets,
+// potentials, large-delta work) in one allocation; uploads the points.
+int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int nlocal0, const double* src_host,
+             const double* trg_host, bool upload_trg) {
+  size_t n_src = (size_t)ns * dim, n_chg = (size_t)ns * nd, n_trg = (size_t)nt * dim;
+  size_t n_pot = (size_t)ns * nd, n_pt = (size_t)nt * nd;
+  // large-delta local expansion: the order is known only after the bounding
+  // box, so reserve for the largest order the term rule gives (nlocal0 < 0:
+  // size it later in plan_device)
+  size_t n_work = 0;
+  if (nlocal0 >= 0) {
+    size_t Pn = nlocal0 + 1;
+    n_work = 4 + nd * (dim == 2 ? Pn * Pn : Pn * Pn * Pn);
+  }
+  auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
+  p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
+  CKS(cudaMalloc(&p->d_io, p->io_bytes));
+  double* c = p->d_io;
+  p->d_src = c; c += al(n_src);
+  p->d_chg = c; c += al(n_chg);
+  p->d_trg = c; c += al(n_trg);
+  p->d_pot = c; c += al(n_pot);
+  p->d_pottarg = c; c += al(n_pt);
+  p->d_work = c;
+  cudaStream_t st = p->ctx->stream;
+  if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
+  if (nt > 0 && upload_trg) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
+  return FGT_OK;
+}
+
 int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   const Params& P = p->H.P;
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
@@ -110,6 +141,48 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
     p->have_device = true;
     CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, st));
   }
+  return FGT_OK;
+}
+
+// Plan whose tree build does its point work on the GPU (fgt_devtree.cu).  The
+// largest large-delta order is not known before the bounding box, so that
+// path re-allocates its work array once the order is.
+int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double eps, int ns,
+                            const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg) {
+  const bool same = targ == sources && nt == ns;
+  int st = alloc_io(p, dim, nd, ns, nt, -1, sources, targ, !same);
+  if (st != FGT_OK) return st;
+  cudaStream_t s = p->ctx->stream;
+  const double* d_trg = same ? p->d_src : p->d_trg;
+  int* perms = nullptr;
+  CKS(cudaMalloc(&perms, sizeof(int) * ((size_t)ns + nt + 2)));
+  struct Free {
+    int* q;
+    ~Free() { cudaFree(q); }
+  } fr{perms};
+  int *d_isrc = perms, *d_itarg = perms + ns + 1;
+  try {
+    CKS(build_plan_device(p->H, dim, nd, delta, eps, ns, p->d_src, nt, d_trg, same, ifpgh, ifpghtarg,
+                          d_isrc, d_itarg, s));
+  } catch (const std::bad_alloc&) {
+    return FGT_ERR_NOMEM;
+  }
+  const Params& P = p->H.P;
+  if (P.large_delta) {
+    // same layout as plan_device, with the work array of the known order
+    std::vector<double> hs((size_t)ns * dim), ht(same ? 0 : (size_t)nt * dim);
+    CKS(cudaMemcpyAsync(hs.data(), p->d_src, hs.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!same && nt > 0) CKS(cudaMemcpyAsync(ht.data(), p->d_trg, ht.size() * 8, cudaMemcpyDeviceToHost, s));
+    CKS(cudaStreamSynchronize(s));
+    cudaFree(p->d_io);
+    p->d_io = nullptr;
+    return plan_device(p, hs.data(), same ? hs.data() : ht.data());
+  }
+  if (same && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, p->d_src, (size_t)nt * dim * 8, cudaMemcpyDeviceToDevice, s));
+  CKS(device_plan_create(p->H, p->D, d_isrc, d_itarg, s));
+  p->have_device = true;
+  CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, s));
+  CKS(cudaStreamSynchronize(s));
   return FGT_OK;
 }
 
@@ -203,6 +276,11 @@ int fgt_ctx_set_precision(fgt_ctx* c, int precision) {
   c->precision = precision;
   return FGT_OK;
 }
+int fgt_ctx_set_tree(fgt_ctx* c, int where) {
+  if (!c || (where != FGT_TREE_DEVICE && where != FGT_TREE_HOST)) return FGT_ERR_BADARG;
+  c->tree = where;
+  return FGT_OK;
+}
 int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
   if (!c) return FGT_ERR_BADARG;
   c->nthreads = nthreads;
@@ -256,16 +334,21 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
   int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg);
   if (st != FGT_OK) return st;
   if (ns == 0) return FGT_ERR_BADARG;
+  if (!targ) nt = 0;  // no target array: no targets in the tree either
   std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
   if (!p) return FGT_ERR_NOMEM;
   p->ctx = ctx;
-  try {
-    build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads);
-  } catch (const std::bad_alloc&) {
-    return FGT_ERR_NOMEM;
-  }
   CKS(cudaSetDevice(ctx->device));
-  st = plan_device(p.get(), sources, targ);
+  if (ctx->tree == FGT_TREE_DEVICE) {
+    st = plan_create_device_tree(p.get(), dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg);
+  } else {
+    try {
+      build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads);
+    } catch (const std::bad_alloc&) {
+      return FGT_ERR_NOMEM;
+    }
+    st = plan_device(p.get(), sources, targ);
+  }
   if (st != FGT_OK) {
     fgt_plan_destroy(p.release());
     return st;
@@ -390,6 +473,63 @@ int fgt_host_tree_create(int dim, double delta, double eps, int ns, const double
     return FGT_ERR_NOMEM;
   }
   *out = h;
+  return FGT_OK;
+}
+int fgt_device_tree_create(fgt_ctx* ctx, int dim, double delta, double eps, int ns, const double* sources,
+                           int nt, const double* targ, fgt_host_tree** out) {
+  if (!ctx || !out) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int st = check_args(dim, 1, delta, eps, ns, sources, 1, 0, 0, nt, targ, 0);
+  if (st != FGT_OK) return st;
+  if (ns == 0) return FGT_ERR_BADARG;
+  if (!targ) nt = 0;
+  CKS(cudaSetDevice(ctx->device));
+  std::unique_ptr<fgt_host_tree> h(new (std::nothrow) fgt_host_tree());
+  if (!h) return FGT_ERR_NOMEM;
+  cudaStream_t s = ctx->stream;
+  const bool same = targ == sources && nt == ns;
+  double *d_src = nullptr, *d_trg = nullptr;
+  int* perms = nullptr;
+  size_t nsd = (size_t)ns * dim, ntd = same ? 0 : (size_t)nt * dim;
+  CKS(cudaMalloc(&d_src, 8 * (nsd + ntd + 2)));
+  struct Free {
+    void* a;
+    void* b;
+    ~Free() { cudaFree(a); cudaFree(b); }
+  } fr{d_src, nullptr};
+  CKS(cudaMalloc(&perms, sizeof(int) * ((size_t)ns + nt + 2)));
+  fr.b = perms;
+  d_trg = same ? d_src : d_src + nsd + 1;
+  CKS(cudaMemcpyAsync(d_src, sources, nsd * 8, cudaMemcpyHostToDevice, s));
+  if (!same && nt > 0) CKS(cudaMemcpyAsync(d_trg, targ, ntd * 8, cudaMemcpyHostToDevice, s));
+  try {
+    HostPlan H;
+    double mn[3], mx[3];
+    CKS(cudaStreamSynchronize(s));
+    int lc;
+    double bs0, cen0[3] = {0, 0, 0};
+    // bounding box from the same reduction the plan uses
+    CKS(build_plan_device_bbox(d_src, ns, d_trg, same ? 0 : nt, dim, mn, mx, s));
+    boxsize0_bbox(dim, delta, eps, mn, mx, &lc, &bs0, cen0);
+    TreeSetup ts;
+    if (!plan_begin(H, dim, 1, delta, eps, ns, nt, 0, 0, lc, bs0, cen0, ts)) {
+      h->large = true;
+      h->t.npwlevel = lc;
+    } else {
+      CKS(build_tree_device(h->t, dim, d_src, ns, d_trg, nt, same, ts, perms, perms + ns + 1, s));
+      h->t.npwlevel = lc;
+      h->nlmax = ts.nlmax;
+      h->t.isrc.resize(ns);
+      h->t.itarg.resize(nt);
+      CKS(cudaMemcpyAsync(h->t.isrc.data(), perms, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+      if (nt > 0)
+        CKS(cudaMemcpyAsync(h->t.itarg.data(), perms + ns + 1, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
+      CKS(cudaStreamSynchronize(s));
+    }
+  } catch (const std::bad_alloc&) {
+    return FGT_ERR_NOMEM;
+  }
+  *out = h.release();
   return FGT_OK;
 }
 int fgt_host_tree_dims(const fgt_host_tree* h, int* dims) {

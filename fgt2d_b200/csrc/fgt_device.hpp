@@ -109,8 +109,24 @@ struct DevicePlan {
   long long launches = 0;
 };
 
-// Uploads the host plan; returns cudaSuccess or the first error.
-cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D);
+// Uploads the host plan; returns cudaSuccess or the first error.  The point
+// permutations come from H.tree (host) or, when d_isrc is given, from device
+// arrays (d_isrc: ns, d_itarg: nt) copied on stream st.
+cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_isrc = nullptr,
+                               const int* d_itarg = nullptr, cudaStream_t st = 0);
+
+// Tree and plan with the point work of the tree build on the GPU
+// (fgt_devtree.cu).  d_src (ns, dim) and d_trg (nt, dim) are device arrays in
+// the caller's order (same: targets are the sources); the permutations
+// (position -> input index) are written to d_isrc / d_itarg.
+cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
+                              bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st);
+// Bounding box (per-dimension min / max) of device point arrays.
+cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim,
+                                   double* mn, double* mx, cudaStream_t st);
+cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
+                              const double* d_src, int nt, const double* d_trg, bool same, int ifpgh,
+                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st);
 void device_plan_destroy(DevicePlan& D);
 
 // Sorts the plan's points into tree order once: device arrays in the

@@ -1,0 +1,319 @@
+// Tree build with its point work on the GPU.
+//
+// The same tree as build_tree (fgt_tree.cpp), which follows the reference's
+// pts_tree_build / pts_tree_fix_lr / pts_tree_sort (pts_tree2d4.f,
+// pts_tree3d.f): the box-level steps (which boxes refine, level restriction,
+// reorganisation, colleagues, depth-first leaf ranks) stay on the host and are
+// shared with the host build; every step that touches all points runs here:
+//   - the bounding box (pts_tree_boxsize0's min / max);
+//   - each refinement level: every point of a refined box moves to its child
+//     (coordinate minus centre < 0 goes to the lower child, as
+//     sort_pts_to_children) and the children's source counts are summed with
+//     warp-aggregated atomics; the host reads the counts back to decide the
+//     next level;
+//   - after the level restriction, every point descends to its final leaf;
+//   - the stable sort of the points by the depth-first rank of their leaf
+//     (pts_tree_sort keeps the input order inside a leaf), done as a stable
+//     LSD radix sort (CUB) of (rank, input index), and the per-leaf counts
+//     that give every box its point range.
+// The permutations stay on the device; only box-level arrays cross the bus.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "fgt_device.hpp"
+#include "fgt_plan.hpp"
+
+namespace fgtb {
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+#define CKD(x)                          \
+  do {                                  \
+    cudaError_t e_ = (x);               \
+    if (e_ != cudaSuccess) return e_;   \
+  } while (0)
+
+__device__ __forceinline__ int child_slot_d(const double* x, const double* c, int D) {
+  int j = 0;
+  for (int d = 0; d < D; d++)
+    if (!(x[d] - c[d] < 0)) j |= 1 << d;
+  return j;
+}
+
+// Per-block minimum and maximum of each coordinate (blockDim = 256);
+// part[6 block + d] = min, part[6 block + 3 + d] = max.
+__global__ void __launch_bounds__(256) k_bbox(const double* __restrict__ x, int n, int dim,
+                                              double* __restrict__ part) {
+  __shared__ double smn[3][256], smx[3][256];
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+    for (int d = 0; d < dim; d++) {
+      const double v = x[(size_t)dim * i + d];
+      mn[d] = fmin(mn[d], v);
+      mx[d] = fmax(mx[d], v);
+    }
+  for (int d = 0; d < 3; d++) {
+    smn[d][threadIdx.x] = mn[d];
+    smx[d][threadIdx.x] = mx[d];
+  }
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int d = 0; d < 3; d++) {
+        smn[d][threadIdx.x] = fmin(smn[d][threadIdx.x], smn[d][threadIdx.x + s]);
+        smx[d][threadIdx.x] = fmax(smx[d][threadIdx.x], smx[d][threadIdx.x + s]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; d++) {
+      part[6 * blockIdx.x + d] = smn[d][0];
+      part[6 * blockIdx.x + 3 + d] = smx[d][0];
+    }
+}
+
+// One refinement level: a point in a refined box [a, b] of the level moves to
+// its child; cnt[c - c0] counts the sources of each new box.
+__global__ void __launch_bounds__(256) k_refine(const double* __restrict__ x, int n, int dim,
+                                                int* __restrict__ pbox, int a, int b,
+                                                const int* __restrict__ fc, const double* __restrict__ cen,
+                                                int c0, int* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = -1;
+  if (i < n) {
+    const int box = pbox[i];
+    if (box >= a && box <= b) {
+      const int f = fc[box - a];
+      if (f >= 0) {
+        c = f + child_slot_d(x + (size_t)dim * i, cen + (size_t)(box - a) * dim, dim);
+        pbox[i] = c;
+      }
+    }
+  }
+  const unsigned m = __match_any_sync(0xffffffffu, c);
+  if (c >= 0 && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(cnt + (c - c0), __popc(m));
+}
+
+__global__ void k_remap(int* __restrict__ pbox, int n, const int* __restrict__ idmap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pbox[i] = idmap[pbox[i]];
+}
+
+// Descent to the final leaf (from start[i], or the root), its depth-first
+// rank as the sort key, and the per-leaf counts.  The descent is bounded by
+// the number of levels; a point that does not reach a leaf sets *err.
+__global__ void __launch_bounds__(256) k_locate(const double* __restrict__ x, int n, int dim,
+                                                const int* __restrict__ start, const int* __restrict__ nchild,
+                                                const int* __restrict__ child, const double* __restrict__ cen,
+                                                int nch, int maxdepth, const int* __restrict__ rank,
+                                                int* __restrict__ key, int* __restrict__ idx,
+                                                int* __restrict__ leafcnt, int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = -1;
+  if (i < n) {
+    int b = start ? start[i] : 0;
+    const double* p = x + (size_t)dim * i;
+    for (int it = 0; it <= maxdepth && nchild[b] > 0; it++) {
+      const int c = child[(size_t)b * nch + child_slot_d(p, cen + (size_t)b * dim, dim)];
+      if (c < 0) break;
+      b = c;
+    }
+    r = nchild[b] == 0 ? rank[b] : -1;
+    if (r < 0) {
+      atomicExch(err, 1);
+      r = 0;
+    }
+    key[i] = r;
+    idx[i] = i;
+  }
+  const unsigned m = __match_any_sync(0xffffffffu, i < n ? r : -1);
+  if (i < n && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(leafcnt + r, __popc(m));
+}
+
+// Device scratch that grows on demand and is freed at the end of the build.
+struct Scratch {
+  std::vector<void*> ptrs;
+  ~Scratch() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t get(T** out, size_t n) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    ptrs.push_back(p);
+    *out = static_cast<T*>(p);
+    return cudaSuccess;
+  }
+};
+
+template <typename T>
+cudaError_t upload(T* dst, const T* src, size_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+cudaError_t device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim, double* mn,
+                        double* mx, cudaStream_t st) {
+  Scratch S;
+  const int nb = 296;
+  double* part = nullptr;
+  CKD(S.get(&part, (size_t)12 * nb));
+  k_bbox<<<nb, 256, 0, st>>>(d_src, ns, dim, part);
+  k_bbox<<<nb, 256, 0, st>>>(d_trg, nt, dim, part + 6 * nb);
+  std::vector<double> h((size_t)12 * nb);
+  CKD(cudaMemcpyAsync(h.data(), part, h.size() * 8, cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  for (int d = 0; d < dim; d++) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int k = 0; k < 2 * nb; k++) {
+      lo = std::min(lo, h[6 * (size_t)k + d]);
+      hi = std::max(hi, h[6 * (size_t)k + 3 + d]);
+    }
+    mn[d] = lo;
+    mx[d] = hi;
+  }
+  return cudaGetLastError();
+}
+
+// Sorts one point set into tree order: perm (device) and per-box ranges.
+cudaError_t sort_points_device(const Tree& t, const double* d_x, int n, const int* d_start,
+                               const int* d_nchild, const int* d_child, const double* d_cen,
+                               const int* d_rank, int nleaf, const std::vector<int>& leaf_of_rank,
+                               int* d_perm, std::vector<int>& r0, std::vector<int>& r1, cudaStream_t st) {
+  Scratch S;
+  int *key = nullptr, *key2 = nullptr, *idx = nullptr, *cnt = nullptr, *err = nullptr;
+  CKD(S.get(&key, n));
+  CKD(S.get(&key2, n));
+  CKD(S.get(&idx, n));
+  CKD(S.get(&cnt, nleaf));
+  CKD(S.get(&err, 1));
+  CKD(cudaMemsetAsync(cnt, 0, sizeof(int) * nleaf, st));
+  CKD(cudaMemsetAsync(err, 0, sizeof(int), st));
+  if (n > 0)
+    k_locate<<<(n + 255) / 256, 256, 0, st>>>(d_x, n, t.dim, d_start, d_nchild, d_child, d_cen, t.nch,
+                                                t.nlevels + 1, d_rank, key, idx, cnt, err);
+  int bits = 1;
+  while ((1 << bits) < nleaf) bits++;
+  size_t tmp = 0;
+  CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, key2, idx, d_perm, n, 0, bits, st));
+  void* dtmp = nullptr;
+  CKD(S.get(reinterpret_cast<char**>(&dtmp), tmp));
+  CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, key, key2, idx, d_perm, n, 0, bits, st));
+  std::vector<int> lc(nleaf);
+  int herr = 0;
+  CKD(cudaMemcpyAsync(lc.data(), cnt, sizeof(int) * nleaf, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  if (herr) return cudaErrorLaunchFailure;
+  tree_ranges(t, lc, leaf_of_rank, r0, r1);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim,
+                                   double* mn, double* mx, cudaStream_t st) {
+  return device_bbox(d_src, ns, d_trg, nt, dim, mn, mx, st);
+}
+
+cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
+                              bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg,
+                              cudaStream_t st) {
+  tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
+  Scratch S;
+  int* pbox = nullptr;
+  CKD(S.get(&pbox, ns));
+  CKD(cudaMemsetAsync(pbox, 0, sizeof(int) * std::max(ns, 1), st));
+  // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
+  std::vector<int> count(1, ns), fc;
+  int* d_fc = nullptr;
+  double* d_cen = nullptr;
+  int* d_cnt = nullptr;
+  size_t cap_lev = 0, cap_new = 0;
+  int lev;
+  for (lev = 0; lev <= ts.nlmax - 1; lev++) {
+    const int a = t.lfirst[lev], b = t.llast[lev];
+    const int thr = lev < ts.levcut ? ts.ndiv0 : ts.ndiv;
+    if (tree_refine_level(t, lev, thr, count, fc) == 0) break;
+    const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0, nlev = b - a + 1;
+    if ((size_t)nlev > cap_lev) {
+      cap_lev = (size_t)nlev * 2;
+      CKD(S.get(&d_fc, cap_lev));
+      CKD(S.get(&d_cen, cap_lev * dim));
+    }
+    if ((size_t)nnew > cap_new) {
+      cap_new = (size_t)nnew * 2;
+      CKD(S.get(&d_cnt, cap_new));
+    }
+    CKD(upload(d_fc, fc.data(), nlev, st));
+    CKD(upload(d_cen, t.centers.data() + (size_t)a * dim, (size_t)nlev * dim, st));
+    CKD(cudaMemsetAsync(d_cnt, 0, sizeof(int) * nnew, st));
+    if (ns > 0) k_refine<<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, dim, pbox, a, b, d_fc, d_cen, c0, d_cnt);
+    count.resize(t.nboxes, 0);
+    CKD(cudaMemcpyAsync(count.data() + c0, d_cnt, sizeof(int) * nnew, cudaMemcpyDeviceToHost, st));
+    CKD(cudaStreamSynchronize(st));
+  }
+  std::vector<int> idmap;
+  tree_finish(t, lev, idmap);
+  int* d_map = nullptr;
+  CKD(S.get(&d_map, idmap.size()));
+  CKD(upload(d_map, idmap.data(), idmap.size(), st));
+  if (ns > 0) k_remap<<<(ns + 255) / 256, 256, 0, st>>>(pbox, ns, d_map);
+  std::vector<int> dfs_rank, leaf_of_rank;
+  tree_leaf_ranks(t, dfs_rank, leaf_of_rank);
+  const int nb = t.nboxes, nleaf = (int)leaf_of_rank.size();
+  int *d_nchild = nullptr, *d_child = nullptr, *d_rank = nullptr;
+  double* d_centers = nullptr;
+  CKD(S.get(&d_nchild, nb));
+  CKD(S.get(&d_child, (size_t)nb * t.nch));
+  CKD(S.get(&d_rank, nb));
+  CKD(S.get(&d_centers, (size_t)nb * dim));
+  CKD(upload(d_nchild, t.nchild.data(), nb, st));
+  CKD(upload(d_child, t.child.data(), (size_t)nb * t.nch, st));
+  CKD(upload(d_rank, dfs_rank.data(), nb, st));
+  CKD(upload(d_centers, t.centers.data(), (size_t)nb * dim, st));
+  CKD(sort_points_device(t, d_src, ns, pbox, d_nchild, d_child, d_centers, d_rank, nleaf, leaf_of_rank,
+                         d_isrc, t.s0, t.s1, st));
+  if (same) {
+    if (nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+    t.t0 = t.s0;
+    t.t1 = t.s1;
+  } else {
+    CKD(sort_points_device(t, d_trg, nt, nullptr, d_nchild, d_child, d_centers, d_rank, nleaf,
+                           leaf_of_rank, d_itarg, t.t0, t.t1, st));
+  }
+  CKD(cudaStreamSynchronize(st));
+  return cudaGetLastError();
+}
+
+cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
+                              const double* d_src, int nt, const double* d_trg, bool same, int ifpgh,
+                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st) {
+  const double tstart = now_s();
+  double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+  CKD(device_bbox(d_src, ns, d_trg, same ? 0 : nt, dim, mn, mx, st));
+  int npwlevel;
+  double bs0, cen0[3] = {0, 0, 0};
+  boxsize0_bbox(dim, delta, eps, mn, mx, &npwlevel, &bs0, cen0);
+  TreeSetup ts;
+  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts)) {
+    H.host_tree_s = now_s() - tstart;
+    return cudaSuccess;
+  }
+  CKD(build_tree_device(H.tree, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st));
+  H.host_tree_s = now_s() - tstart;
+  plan_end(H);
+  return cudaSuccess;
+}
+
+}  // namespace fgtb

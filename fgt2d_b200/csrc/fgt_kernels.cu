@@ -115,6 +115,11 @@ __global__ void k_gather_pts(const double* __restrict__ x, const double* __restr
       for (int c = 0; c < nd; c++) qs[(long long)i * nd + c] = q[p * nd + c];
   }
 }
+// inv[perm[i]] = i
+__global__ void k_invperm(const int* __restrict__ perm, int n, int* __restrict__ inv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) inv[perm[i]] = i;
+}
 // Caller order: out row j = in row iperm[j] (dreorderi, fmmcommon2d.f:29-56),
 // written as a gather so the stores stay coalesced.
 __global__ void k_unsort(const double* __restrict__ in, double* __restrict__ out,
@@ -1791,7 +1796,8 @@ size_t al(size_t b) { return (b + 255) & ~size_t(255); }
     if (e_ != cudaSuccess) return e_;       \
   } while (0)
 
-cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
+cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_isrc, const int* d_itarg,
+                               cudaStream_t pst) {
   D = DevicePlan();
   D.P = H.P;
   const Params& P = H.P;
@@ -1965,7 +1971,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
   }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
   size_t total = bytes_of(H.box_centers) + bytes_of(H.h2x) + bytes_of(H.x2l) + al(H.wms.size() * 8) +
-                 al(H.wsh.size() * 8) + 2 * al(H.tree.isrc.size() * 4) + 2 * al(H.tree.itarg.size() * 4) +
+                 al(H.wsh.size() * 8) + 2 * al((size_t)P.ns * 4) + 2 * al((size_t)P.nt * 4) +
                  al((size_t)(std::max(P.ntermmax, 1) + 2) * 8) + al(32 * 8) +
                  bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(H.split) +
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
@@ -1990,9 +1996,28 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
     CK(put(cur, D.wsh, v, s));
     CK(cudaStreamSynchronize(s));
   }
-  CK(put(cur, D.isrc, H.tree.isrc, s));
-  CK(put(cur, D.itarg, H.tree.itarg, s));
-  {
+  if (d_isrc) {
+    // permutations built on the device (fgt_devtree.cu): copy, invert there
+    auto carve = [&](int*& dst, size_t n) {
+      dst = reinterpret_cast<int*>(cur);
+      cur += al(n * 4);
+    };
+    carve(D.isrc, P.ns);
+    carve(D.itarg, P.nt);
+    carve(D.isrc_inv, P.ns);
+    carve(D.itarg_inv, P.nt);
+    if (P.ns > 0) {
+      CK(cudaMemcpyAsync(D.isrc, d_isrc, (size_t)P.ns * 4, cudaMemcpyDeviceToDevice, pst));
+      k_invperm<<<(P.ns + 255) / 256, 256, 0, pst>>>(D.isrc, P.ns, D.isrc_inv);
+    }
+    if (P.nt > 0) {
+      CK(cudaMemcpyAsync(D.itarg, d_itarg, (size_t)P.nt * 4, cudaMemcpyDeviceToDevice, pst));
+      k_invperm<<<(P.nt + 255) / 256, 256, 0, pst>>>(D.itarg, P.nt, D.itarg_inv);
+    }
+    CK(cudaStreamSynchronize(pst));
+  } else {
+    CK(put(cur, D.isrc, H.tree.isrc, s));
+    CK(put(cur, D.itarg, H.tree.itarg, s));
     std::vector<int> inv(H.tree.isrc.size());
     for (size_t i = 0; i < inv.size(); i++) inv[H.tree.isrc[i]] = (int)i;
     CK(put(cur, D.isrc_inv, inv, s));
@@ -2000,6 +2025,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D) {
     inv.assign(H.tree.itarg.size(), 0);
     for (size_t i = 0; i < inv.size(); i++) inv[H.tree.itarg[i]] = (int)i;
     CK(put(cur, D.itarg_inv, inv, s));
+  }
+  {
     std::vector<double> isq(std::max(P.ntermmax, 1) + 2, 0.0);
     for (size_t j = 1; j < isq.size(); j++) isq[j] = 1.0 / std::sqrt((double)j);
     CK(put(cur, D.isq, isq, s));

@@ -350,29 +350,25 @@ int build_host_plan_from_tree(HostPlan& H, const Params& P0, const std::vector<i
   return 0;
 }
 
-int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
-                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
-                    int nthreads) {
+bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, int nt, int ifpgh,
+                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts) {
   Params& P = H.P;
   P = Params();
   P.dim = dim; P.nd = nd; P.delta = delta; P.eps = eps; P.ns = ns; P.nt = nt;
   P.ifpgh = ifpgh; P.ifpghtarg = ifpghtarg;
   P.dsq = 1.0 / std::sqrt(delta);
   P.dmax = dim == 2 ? std::log(1.0 / (eps / 90)) * delta : std::log(1.0 / eps) * delta;
-  double tstart = now();
-  int npwlevel;
-  double bs0, cen0[3] = {0, 0, 0};
-  boxsize0(dim, delta, eps, sources, ns, targ, nt, &npwlevel, &bs0, cen0);
   P.npwlevel = npwlevel;
   for (int d = 0; d < 3; d++) P.cen0[d] = cen0[d];
   if (npwlevel < -2) {  // fgt2d.f:133-150: one Taylor local about the box centre
     P.large_delta = true;
     int nl0 = hlterms(dim, bs0, delta, eps, 0);
     P.nlocal0 = nl0 + std::max(ifpgh, ifpghtarg) - 1;
-    H.host_tree_s = now() - tstart;
-    return 0;
+    return false;
   }
-  int ndiv0 = dim == 2 ? 10 : 40, ndiv = dim == 2 ? 80 : 100, hcap = dim == 2 ? 18 : 15;
+  ts.ndiv0 = dim == 2 ? 10 : 40;
+  ts.ndiv = dim == 2 ? 80 : 100;
+  const int hcap = dim == 2 ? 18 : 15;
   int nlmax = npwlevel + 4, nls = std::max(npwlevel, 0);
   double bsize = bs0 / std::ldexp(1.0, nls);
   int nl0 = 0;
@@ -382,24 +378,51 @@ int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int 
     bsize /= 2;
   }
   P.nlmax = nlmax;
-  build_tree(H.tree, dim, sources, ns, targ, nt, ndiv, ndiv0, npwlevel, nlmax, bs0, cen0, nthreads);
-  H.host_tree_s = now() - tstart;
+  ts.levcut = npwlevel;
+  ts.nlmax = nlmax;
+  ts.bs0 = bs0;
+  for (int d = 0; d < 3; d++) ts.cen0[d] = cen0[d];
+  return true;
+}
+
+void plan_end(HostPlan& H) {
+  Params& P = H.P;
+  const int dim = P.dim;
   Tree& t = H.tree;
+  const int nls = std::max(P.npwlevel, 0);
   P.nlevels = t.nlevels;
   P.nlevstart = nls;
-  P.all_direct = npwlevel >= t.nlevels;
+  P.all_direct = P.npwlevel >= t.nlevels;
   H.nlocal.assign(t.nlevels + 1, 0);
-  int nadd = std::max(ifpgh, ifpghtarg);
+  int nadd = std::max(P.ifpgh, P.ifpghtarg);
   for (int i = nls; i <= t.nlevels; i++) {
-    H.nlocal[i] = hlterms(dim, t.boxsize[i], delta, eps, 0);
-    if (ifpgh >= 2 || ifpghtarg >= 2) H.nlocal[i] += nadd;
+    H.nlocal[i] = hlterms(dim, t.boxsize[i], P.delta, P.eps, 0);
+    if (P.ifpgh >= 2 || P.ifpghtarg >= 2) H.nlocal[i] += nadd;
   }
   P.ntermmax = 0;
   for (int v : H.nlocal) P.ntermmax = std::max(P.ntermmax, v);
-  double pweps = nadd > 2 ? eps / 100 : eps;
-  pwterms(2 * bs0 / std::pow(2.0, nls), delta, pweps, &P.pmax, &P.npw);
+  double pweps = nadd > 2 ? P.eps / 100 : P.eps;
+  pwterms(2 * t.bs0 / std::pow(2.0, nls), P.delta, pweps, &P.pmax, &P.npw);
   P.nexp = dim == 2 ? P.npw * P.npw / 2 : P.npw * P.npw * P.npw / 2;
   finish_plan(H);
+}
+
+int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
+                    const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                    int nthreads) {
+  double tstart = now();
+  int npwlevel;
+  double bs0, cen0[3] = {0, 0, 0};
+  boxsize0(dim, delta, eps, sources, ns, targ, nt, &npwlevel, &bs0, cen0);
+  TreeSetup ts;
+  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts)) {
+    H.host_tree_s = now() - tstart;
+    return 0;
+  }
+  build_tree(H.tree, dim, sources, ns, targ, nt, ts.ndiv, ts.ndiv0, ts.levcut, ts.nlmax, ts.bs0, ts.cen0,
+             nthreads);
+  H.host_tree_s = now() - tstart;
+  plan_end(H);
   return 0;
 }
 

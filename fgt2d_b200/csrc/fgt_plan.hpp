@@ -92,6 +92,19 @@ struct HostPlan {
   double host_tree_s = 0, host_lists_s = 0, host_plan_s = 0;
 };
 
+// Plan building in two halves around the tree build (shared by the host tree
+// and the tree whose point work runs on the GPU):
+//   plan_begin: parameters from the bounding-box results; false for the
+//     large-delta path (no tree).  ts receives the tree-build settings.
+//   plan_end: expansion lengths, tables and tasks once H.tree is complete.
+struct TreeSetup {
+  int ndiv = 0, ndiv0 = 0, levcut = 0, nlmax = 0;
+  double bs0 = 0, cen0[3] = {0, 0, 0};
+};
+bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, int nt, int ifpgh,
+                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts);
+void plan_end(HostPlan& H);
+
 int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                     int nthreads);

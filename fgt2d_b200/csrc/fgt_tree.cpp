@@ -69,6 +69,11 @@ void boxsize0(int dim, double delta, double eps, const double* src, int ns, cons
   };
   scan(src, ns);
   scan(trg, nt);
+  boxsize0_bbox(dim, delta, eps, mn, mx, levcut, bs0, cen0);
+}
+
+void boxsize0_bbox(int dim, double delta, double eps, const double* mn, const double* mx, int* levcut,
+                   double* bs0, double* cen0) {
   double b = mx[0] - mn[0];
   for (int d = 1; d < dim; d++)
     if (mx[d] - mn[d] > b) b = mx[d] - mn[d];
@@ -344,13 +349,20 @@ void sort_points(Tree& t, const double* x, int n, std::vector<int>& perm, std::v
     }
     for (int i = lo; i < hi; i++) perm[c[key[i]]++] = i;
   }
-  // leaf ranges from the per-leaf counts, then internal boxes by DFS
   std::vector<int> leafcount(nleafrank, 0);
   for (int i = 0; i < n; i++) leafcount[key[i]]++;
+  tree_ranges(t, leafcount, leaf_of_rank, r0, r1);
+}
+
+}  // namespace
+
+void tree_ranges(const Tree& t, const std::vector<int>& leafcount, const std::vector<int>& leaf_of_rank,
+                 std::vector<int>& r0, std::vector<int>& r1) {
+  // leaf ranges from the per-leaf counts, then internal boxes bottom-up
   r0.assign(t.nboxes, 0);
   r1.assign(t.nboxes, 0);
   int pos = 0;
-  for (int k = 0; k < nleafrank; k++) {
+  for (size_t k = 0; k < leaf_of_rank.size(); k++) {
     int b = leaf_of_rank[k];
     r0[b] = pos;
     pos += leafcount[k];
@@ -364,7 +376,84 @@ void sort_points(Tree& t, const double* x, int n, std::vector<int>& perm, std::v
       }
 }
 
-}  // namespace
+void tree_init(Tree& t, int dim, double bs0, const double* cen0, int nlmax) {
+  t = Tree();
+  t.dim = dim;
+  t.nch = 1 << dim;
+  t.nco = dim == 2 ? 9 : 27;
+  t.bs0 = bs0;
+  for (int d = 0; d < dim; d++) t.cen0[d] = cen0[d];
+  Builder B(t);
+  int maxlev = std::max(nlmax, 0);
+  t.boxsize.assign(maxlev + 2, 0.0);
+  t.lfirst.assign(maxlev + 2, 0);
+  t.llast.assign(maxlev + 2, -1);
+  B.reserve_boxes(1024);
+  t.boxsize[0] = bs0;
+  for (int d = 0; d < dim; d++) B.C(0, d) = cen0[d];
+  t.level[0] = 0;
+  t.parent[0] = -1;
+  t.nchild[0] = 0;
+  t.lfirst[0] = 0;
+  t.llast[0] = 0;
+  t.nboxes = 1;
+}
+
+int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, std::vector<int>& firstchild) {
+  Builder B(t);
+  const int a = t.lfirst[lev], b = t.llast[lev], NCH = t.nch;
+  firstchild.assign(b - a + 1, -1);
+  int nref = 0;
+  for (int box = a; box <= b; box++)
+    if (count[box] > thr) firstchild[box - a] = t.nboxes + NCH * nref++;
+  if (nref == 0) return 0;
+  t.boxsize[lev + 1] = t.boxsize[lev] / 2;
+  B.reserve_boxes(t.nboxes + NCH * nref);
+  t.lfirst[lev + 1] = t.nboxes;
+  for (int box = a; box <= b; box++)
+    if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, t.boxsize[lev + 1]);
+  t.nboxes += NCH * nref;
+  t.llast[lev + 1] = t.nboxes - 1;
+  return nref;
+}
+
+void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap) {
+  t.nlevels = nlevels;
+  t.boxsize.resize(t.nlevels + 1);
+  t.lfirst.resize(t.nlevels + 1);
+  t.llast.resize(t.nlevels + 1);
+  Builder B(t);
+  B.colleagues_all();
+  B.idmap.resize(t.nboxes);
+  for (int k = 0; k < t.nboxes; k++) B.idmap[k] = k;
+  if (t.nlevels >= 2) B.fix_lr();
+  idmap.swap(B.idmap);
+  const int NCH = t.nch, D = t.dim;
+  t.level.resize(t.nboxes);
+  t.parent.resize(t.nboxes);
+  t.nchild.resize(t.nboxes);
+  t.child.resize((size_t)t.nboxes * NCH);
+  t.centers.resize((size_t)t.nboxes * D);
+}
+
+void tree_leaf_ranks(const Tree& t, std::vector<int>& dfs_rank, std::vector<int>& leaf_of_rank) {
+  const int NCH = t.nch;
+  dfs_rank.assign(t.nboxes, -1);
+  leaf_of_rank.clear();
+  leaf_of_rank.reserve(t.nboxes);
+  std::vector<int> stack;
+  stack.push_back(0);
+  while (!stack.empty()) {
+    int b = stack.back();
+    stack.pop_back();
+    if (t.nchild[b] == 0) {
+      dfs_rank[b] = (int)leaf_of_rank.size();
+      leaf_of_rank.push_back(b);
+    } else {
+      for (int j = NCH - 1; j >= 0; j--) stack.push_back(t.child[(size_t)b * NCH + j]);
+    }
+  }
+}
 
 void compute_colleagues(Tree& t) {
   Builder B(t);
@@ -376,50 +465,19 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
-  t = Tree();
-  t.dim = dim;
-  t.nch = 1 << dim;
-  t.nco = dim == 2 ? 9 : 27;
-  t.bs0 = bs0;
-  for (int d = 0; d < dim; d++) t.cen0[d] = cen0[d];
-  Builder B(t);
-  int NCH = t.nch, D = dim;
-  int maxlev = std::max(nlmax, 0);
-  t.boxsize.assign(maxlev + 2, 0.0);
-  t.lfirst.assign(maxlev + 2, 0);
-  t.llast.assign(maxlev + 2, -1);
-  B.reserve_boxes(1024);
-  t.boxsize[0] = bs0;
-  for (int d = 0; d < D; d++) B.C(0, d) = cen0[d];
-  t.level[0] = 0;
-  t.parent[0] = -1;
-  t.nchild[0] = 0;
-  t.lfirst[0] = 0;
-  t.llast[0] = 0;
-  t.nboxes = 1;
-
+  tree_init(t, dim, bs0, cen0, nlmax);
+  const int D = dim;
   auto T = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
   bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   double tA = T();
   // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
   std::vector<int> pbox(ns, 0);
-  std::vector<int> count(1, ns);
+  std::vector<int> count(1, ns), firstchild;
   int lev;
   for (lev = 0; lev <= nlmax - 1; lev++) {
-    int a = t.lfirst[lev], b = t.llast[lev];
-    int thr = lev < levcut ? ndiv0 : ndiv;
-    std::vector<int> firstchild(b - a + 1, -1);
-    int nref = 0;
-    for (int box = a; box <= b; box++)
-      if (count[box] > thr) firstchild[box - a] = t.nboxes + NCH * nref++;
-    if (nref == 0) break;
-    t.boxsize[lev + 1] = t.boxsize[lev] / 2;
-    B.reserve_boxes(t.nboxes + NCH * nref);
-    t.lfirst[lev + 1] = t.nboxes;
-    for (int box = a; box <= b; box++)
-      if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, t.boxsize[lev + 1]);
-    t.nboxes += NCH * nref;
-    t.llast[lev + 1] = t.nboxes - 1;
+    const int a = t.lfirst[lev], b = t.llast[lev];
+    const int thr = lev < levcut ? ndiv0 : ndiv;
+    if (tree_refine_level(t, lev, thr, count, firstchild) == 0) break;
     count.resize(t.nboxes, 0);
     const int* fc = firstchild.data();
     const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0;
@@ -439,42 +497,15 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
       for (int k = 0; k < nnew; k++) count[c0 + k] += loc[k];
     }
   }
-  t.nlevels = lev;
-  t.boxsize.resize(t.nlevels + 1);
-  t.lfirst.resize(t.nlevels + 1);
-  t.llast.resize(t.nlevels + 1);
   double tB = T();
-  B.colleagues_all();
-  B.idmap.resize(t.nboxes);
-  for (int k = 0; k < t.nboxes; k++) B.idmap[k] = k;
-  if (t.nlevels >= 2) B.fix_lr();
+  std::vector<int> idmap;
+  tree_finish(t, lev, idmap);
   // each source continues its descent from its box before level restriction
 #pragma omp parallel for schedule(static)
-  for (int i = 0; i < ns; i++) pbox[i] = B.idmap[pbox[i]];
+  for (int i = 0; i < ns; i++) pbox[i] = idmap[pbox[i]];
   double tC = T();
-  t.level.resize(t.nboxes);
-  t.parent.resize(t.nboxes);
-  t.nchild.resize(t.nboxes);
-  t.child.resize((size_t)t.nboxes * NCH);
-  t.centers.resize((size_t)t.nboxes * D);
-
-  // depth-first rank of the leaves
-  std::vector<int> dfs_rank(t.nboxes, -1), leaf_of_rank;
-  leaf_of_rank.reserve(t.nboxes);
-  {
-    std::vector<int> stack;
-    stack.push_back(0);
-    while (!stack.empty()) {
-      int b = stack.back();
-      stack.pop_back();
-      if (t.nchild[b] == 0) {
-        dfs_rank[b] = (int)leaf_of_rank.size();
-        leaf_of_rank.push_back(b);
-      } else {
-        for (int j = NCH - 1; j >= 0; j--) stack.push_back(t.child[(size_t)b * NCH + j]);
-      }
-    }
-  }
+  std::vector<int> dfs_rank, leaf_of_rank;
+  tree_leaf_ranks(t, dfs_rank, leaf_of_rank);
   int nl = (int)leaf_of_rank.size();
   double tD = T();
   sort_points(t, src, ns, t.isrc, t.s0, t.s1, dfs_rank, nl, leaf_of_rank, pbox.data());

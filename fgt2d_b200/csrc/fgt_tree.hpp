@@ -42,11 +42,33 @@ void pwterms(double bsize, double delta, double eps, double* pmax, int* npw);
 // Bounding box, cut level and enlarged root size, pts_tree2d4.f:1187-1258.
 void boxsize0(int dim, double delta, double eps, const double* src, int ns, const double* trg,
               int nt, int* levcut, double* bs0, double* cen0);
+// The same from a bounding box already known (per-dimension min mn, max mx).
+void boxsize0_bbox(int dim, double delta, double eps, const double* mn, const double* mx, int* levcut,
+                   double* bs0, double* cen0);
 
 // Builds the tree for sources/targets given as (n, dim) row-major arrays and
 // sorts both point sets (pts_tree_mem/build/sort).  nthreads <= 0 uses all.
 void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, int nt, int ndiv,
                 int ndiv0, int levcut, int nlmax, double bs0, const double* cen0, int nthreads);
+
+// Box-level steps of build_tree, shared by the host build and the build whose
+// point work runs on the GPU (fgt_devtree.cu).
+//   tree_init: the root box only.
+//   tree_refine_level: refines the boxes of level lev whose source count
+//     (count[box], every box so far) exceeds thr, appending their children;
+//     firstchild[box - lfirst[lev]] receives the first child id or -1.
+//     Returns the number of refined boxes (0 ends the refinement).
+//   tree_finish: closes the refinement at nlevels, computes colleagues and
+//     applies the level restriction (pts_tree_fix_lr + reorg); idmap maps a
+//     box id of the refinement to its final id.
+//   tree_leaf_ranks: depth-first rank of the leaves (the pts_tree_sort order).
+//   tree_ranges: per-box point ranges [r0, r1) from the per-leaf counts.
+void tree_init(Tree& t, int dim, double bs0, const double* cen0, int nlmax);
+int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, std::vector<int>& firstchild);
+void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap);
+void tree_leaf_ranks(const Tree& t, std::vector<int>& dfs_rank, std::vector<int>& leaf_of_rank);
+void tree_ranges(const Tree& t, const std::vector<int>& leafcount, const std::vector<int>& leaf_of_rank,
+                 std::vector<int>& r0, std::vector<int>& r1);
 
 // Interaction lists used by the transform (fgt2dmain / fgt3dmain set-up).
 struct Lists {

@@ -42,6 +42,11 @@ enum {
   FGT_PREC_AUTO = 2   /* MIXED when eps >= 1e-6, FP64 otherwise (default) */
 };
 
+enum {
+  FGT_TREE_DEVICE = 0, /* tree build with its point work on the GPU (default) */
+  FGT_TREE_HOST = 1    /* tree build entirely on the host (OpenMP) */
+};
+
 typedef struct fgt_ctx fgt_ctx;
 typedef struct fgt_plan fgt_plan;
 
@@ -69,6 +74,10 @@ int fgt_ctx_create(int device, fgt_ctx** out);
 int fgt_ctx_destroy(fgt_ctx* ctx);
 int fgt_ctx_set_precision(fgt_ctx* ctx, int precision);
 int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
+/* where plans built with this context build their tree (FGT_TREE_DEVICE or
+ * FGT_TREE_HOST); both give the same tree.  No counterpart in the reference,
+ * whose tree is built on the host (pts_tree_build, pts_tree2d4.f:363-590). */
+int fgt_ctx_set_tree(fgt_ctx* ctx, int where);
 /* the context used by the Fortran-named entry points (device 0, created on
  * first use) */
 fgt_ctx* fgt_default_ctx(void);
@@ -175,6 +184,10 @@ int fgt_plan_destroy(fgt_plan* plan);
 typedef struct fgt_host_tree fgt_host_tree;
 int fgt_host_tree_create(int dim, double delta, double eps, int ns, const double* sources, int nt,
                          const double* targ, int nthreads, fgt_host_tree** out);
+/* The same tree built with its point work on the context's GPU (the build
+ * the plans use by default); the handle is read with the calls below. */
+int fgt_device_tree_create(fgt_ctx* ctx, int dim, double delta, double eps, int ns,
+                           const double* sources, int nt, const double* targ, fgt_host_tree** out);
 /* dims[0..3] = nlevels, nboxes, npwlevel, nlmax; returns FGT_ERR_UNSUPPORTED
  * for the large-delta case, which builds no tree */
 int fgt_host_tree_dims(const fgt_host_tree* t, int* dims);
