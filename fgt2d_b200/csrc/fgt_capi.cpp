@@ -1,8 +1,10 @@
 // C ABI of the B200 plane-wave FGT (declared in include/fgt_b200.h).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -38,11 +40,16 @@ struct fgt_plan {
   double* d_pot = nullptr;
   double* d_pottarg = nullptr;
   double* d_work = nullptr;  // large-delta local expansion
+  int* d_flag = nullptr;     // device-side argument checks
   int last_launches = 0;
 };
 
 namespace {
 thread_local int g_last_cuda = 0;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return FGT_OK;
@@ -70,15 +77,18 @@ bool finite_all(const double* a, size_t n) {
   return true;
 }
 
+// Argument checks; scan_points = false leaves the finiteness of the point
+// coordinates to a device-side check after the upload.
 int check_args(int dim, int nd, double delta, double eps, int ns, const double* sources,
-               int ifcharge, int ifdipole, int ifpgh, int nt, const double* targ, int ifpghtarg) {
+               int ifcharge, int ifdipole, int ifpgh, int nt, const double* targ, int ifpghtarg,
+               bool scan_points = true) {
   if (dim != 2 && dim != 3) return FGT_ERR_BADARG;
   if (nd < 1 || !(delta > 0) || !std::isfinite(delta) || !(eps > 0) || !(eps < 1)) return FGT_ERR_BADARG;
   if (ns < 0 || nt < 0) return FGT_ERR_BADARG;
   if (ns > 0 && !sources) return FGT_ERR_BADARG;
   if (nt > 0 && ifpghtarg > 0 && !targ) return FGT_ERR_BADARG;
-  if (!finite_all(sources, (size_t)ns * dim)) return FGT_ERR_BADARG;
-  if (nt > 0 && targ && !finite_all(targ, (size_t)nt * dim)) return FGT_ERR_BADARG;
+  if (scan_points && !finite_all(sources, (size_t)ns * dim)) return FGT_ERR_BADARG;
+  if (scan_points && nt > 0 && targ && !finite_all(targ, (size_t)nt * dim)) return FGT_ERR_BADARG;
   if (ifcharge != 1 || ifdipole != 0) return FGT_ERR_UNSUPPORTED;
   if (ifpgh < 0 || ifpgh > 1 || ifpghtarg < 0 || ifpghtarg > 1) return FGT_ERR_UNSUPPORTED;
   return FGT_OK;
@@ -107,11 +117,24 @@ int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int nlocal0, const do
   p->d_trg = c; c += al(n_trg);
   p->d_pot = c; c += al(n_pot);
   p->d_pottarg = c; c += al(n_pt);
-  p->d_work = c;
+  p->d_work = c; c += al(n_work);
+  p->d_flag = reinterpret_cast<int*>(c);
   cudaStream_t st = p->ctx->stream;
   if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
   if (nt > 0 && upload_trg) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
   return FGT_OK;
+}
+
+// Device-side finiteness check of n doubles at d (synchronises).
+int check_finite_device(fgt_plan* p, const double* d, size_t n) {
+  if (n == 0) return FGT_OK;
+  cudaStream_t st = p->ctx->stream;
+  int bad = 0;
+  CKS(cudaMemsetAsync(p->d_flag, 0, sizeof(int), st));
+  CKS(device_check_finite(d, n, p->d_flag, st));
+  CKS(cudaMemcpyAsync(&bad, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKS(cudaStreamSynchronize(st));
+  return bad ? FGT_ERR_BADARG : FGT_OK;
 }
 
 int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
@@ -132,7 +155,8 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   p->d_trg = c; c += al(n_trg);
   p->d_pot = c; c += al(n_pot);
   p->d_pottarg = c; c += al(n_pt);
-  p->d_work = c;
+  p->d_work = c; c += al(n_work);
+  p->d_flag = reinterpret_cast<int*>(c);
   cudaStream_t st = p->ctx->stream;
   if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
   if (nt > 0 && P.ifpghtarg > 0) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
@@ -152,6 +176,9 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   const bool same = targ == sources && nt == ns;
   int st = alloc_io(p, dim, nd, ns, nt, -1, sources, targ, !same);
   if (st != FGT_OK) return st;
+  st = check_finite_device(p, p->d_src, (size_t)ns * dim);
+  if (st == FGT_OK && !same) st = check_finite_device(p, p->d_trg, (size_t)nt * dim);
+  if (st != FGT_OK) return st;
   cudaStream_t s = p->ctx->stream;
   const double* d_trg = same ? p->d_src : p->d_trg;
   int* perms = nullptr;
@@ -168,6 +195,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     return FGT_ERR_NOMEM;
   }
   const Params& P = p->H.P;
+  const double tP = now_s();
   if (P.large_delta) {
     // same layout as plan_device, with the work array of the known order
     std::vector<double> hs((size_t)ns * dim), ht(same ? 0 : (size_t)nt * dim);
@@ -183,6 +211,9 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   p->have_device = true;
   CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, s));
   CKS(cudaStreamSynchronize(s));
+  if (getenv("FGT_TREE_TIMING"))
+    fprintf(stderr, "plan: tree %.4f lists %.4f tasks %.4f device plan %.4f\n", p->H.host_tree_s,
+            p->H.host_lists_s, p->H.host_plan_s, now_s() - tP);
   return FGT_OK;
 }
 
@@ -204,17 +235,28 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
                    const double* sources, int ifcharge, const double* charge, int ifdipole,
                    int ifpgh, double* pot, int nt, const double* targ, int ifpghtarg,
                    double* pottarg) {
-  int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg);
+  const bool on_device = ctx->tree == FGT_TREE_DEVICE;
+  int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg,
+                      !on_device);
   if (st != FGT_OK) return st;
-  if (ns > 0 && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
-  if (ifpgh == 1 && ns > 0 && pot) memset(pot, 0, sizeof(double) * (size_t)ns * nd);
-  if (ifpghtarg == 1 && nt > 0 && pottarg) memset(pottarg, 0, sizeof(double) * (size_t)nt * nd);
-  if (ns == 0) return FGT_OK;
+  if (!on_device && ns > 0 && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
+  // outputs are written in full on success; zero them when nothing runs or
+  // the call fails
+  auto zero = [&] {
+    if (ifpgh == 1 && ns > 0 && pot) memset(pot, 0, sizeof(double) * (size_t)ns * nd);
+    if (ifpghtarg == 1 && nt > 0 && pottarg) memset(pottarg, 0, sizeof(double) * (size_t)nt * nd);
+  };
+  if (ns == 0) {
+    zero();
+    return FGT_OK;
+  }
   fgt_plan* plan = nullptr;
   st = fgt_plan_create(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, &plan);
-  if (st != FGT_OK) return st;
-  st = fgt_plan_execute_host(plan, sources, charge, targ, pot, pottarg);
-  fgt_plan_destroy(plan);
+  if (st == FGT_OK) {
+    st = fgt_plan_execute_host(plan, sources, charge, targ, pot, pottarg);
+    fgt_plan_destroy(plan);
+  }
+  if (st != FGT_OK) zero();
   return st;
 }
 
@@ -331,7 +373,8 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
                     fgt_plan** out) {
   if (!ctx || !out) return FGT_ERR_BADARG;
   *out = nullptr;
-  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg);
+  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg,
+                      ctx->tree != FGT_TREE_DEVICE);
   if (st != FGT_OK) return st;
   if (ns == 0) return FGT_ERR_BADARG;
   if (!targ) nt = 0;  // no target array: no targets in the tree either
@@ -375,7 +418,9 @@ int fgt_plan_execute_host(fgt_plan* p, const double* sources, const double* char
   (void)sources; (void)targ;  // fixed at plan creation
   size_t ns = P.ns, nt = P.nt;
   CKS(cudaMemcpyAsync(p->d_chg, charge, ns * P.nd * 8, cudaMemcpyHostToDevice, st));
-  int s = run_device(p, p->d_chg, p->d_pot, p->d_pottarg, st, nullptr);
+  int s = check_finite_device(p, p->d_chg, ns * P.nd);
+  if (s != FGT_OK) return s;
+  s = run_device(p, p->d_chg, p->d_pot, p->d_pottarg, st, nullptr);
   if (s != FGT_OK) return s;
   if (P.ifpgh == 1 && pot) CKS(cudaMemcpyAsync(pot, p->d_pot, ns * P.nd * 8, cudaMemcpyDeviceToHost, st));
   if (P.ifpghtarg == 1 && nt > 0 && pottarg)

@@ -139,6 +139,10 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
 cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
                                 int precision, cudaStream_t stream, StageTimes* times);
 
+// Sets *d_flag (device int, not cleared here) when any of x[0, n) is not
+// finite; asynchronous on st.
+cudaError_t device_check_finite(const double* x, size_t n, int* d_flag, cudaStream_t st);
+
 // Measures the FP64 tensor-core (mma.m8n8k4.f64) throughput of the current
 // device in TFLOP/s.
 cudaError_t probe_fp64_mma(double* tflops);

@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -229,6 +231,8 @@ cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
                               bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg,
                               cudaStream_t st) {
+  const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
+  const double tA = now_s();
   tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
   Scratch S;
   int* pbox = nullptr;
@@ -263,8 +267,10 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
     CKD(cudaMemcpyAsync(count.data() + c0, d_cnt, sizeof(int) * nnew, cudaMemcpyDeviceToHost, st));
     CKD(cudaStreamSynchronize(st));
   }
+  const double tB = now_s();
   std::vector<int> idmap;
   tree_finish(t, lev, idmap);
+  const double tC = now_s();
   int* d_map = nullptr;
   CKD(S.get(&d_map, idmap.size()));
   CKD(upload(d_map, idmap.data(), idmap.size(), st));
@@ -282,8 +288,10 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
   CKD(upload(d_child, t.child.data(), (size_t)nb * t.nch, st));
   CKD(upload(d_rank, dfs_rank.data(), nb, st));
   CKD(upload(d_centers, t.centers.data(), (size_t)nb * dim, st));
+  const double tD = now_s();
   CKD(sort_points_device(t, d_src, ns, pbox, d_nchild, d_child, d_centers, d_rank, nleaf, leaf_of_rank,
                          d_isrc, t.s0, t.s1, st));
+  const double tE = now_s();
   if (same) {
     if (nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
     t.t0 = t.s0;
@@ -293,6 +301,9 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
                            leaf_of_rank, d_itarg, t.t0, t.t1, st));
   }
   CKD(cudaStreamSynchronize(st));
+  if (dbg)
+    fprintf(stderr, "device tree: refine %.4f lr %.4f ranks+upload %.4f sort_s %.4f sort_t %.4f\n", tB - tA,
+            tC - tB, tD - tC, tE - tD, now_s() - tE);
   return cudaGetLastError();
 }
 

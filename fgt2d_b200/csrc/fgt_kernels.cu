@@ -18,7 +18,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -114,6 +116,11 @@ __global__ void k_gather_pts(const double* __restrict__ x, const double* __restr
     if (q)
       for (int c = 0; c < nd; c++) qs[(long long)i * nd + c] = q[p * nd + c];
   }
+}
+// *bad = 1 when any of x[0, n) is not finite
+__global__ void k_all_finite(const double* __restrict__ x, size_t n, int* __restrict__ bad) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) *bad = 1;
 }
 // inv[perm[i]] = i
 __global__ void k_invperm(const int* __restrict__ perm, int n, int* __restrict__ inv) {
@@ -1982,7 +1989,12 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
                  al(lo_doubles * 8) + 4096;
   D.bytes = total;
+  const auto tnow = [] {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  const double tm0 = tnow();
   CK(cudaMalloc(&D.base, total));
+  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "device plan: malloc %.4f (%zu bytes)\n", tnow() - tm0, total);
   char* cur = D.base;
   cudaStream_t s = 0;
   CK(put(cur, D.centers, H.box_centers, s));
@@ -2084,6 +2096,16 @@ static KP make_kp(const DevicePlan& D) {
 
 // node weights for the direct 3D form kernel live in the x2l/h2x neighbourhood:
 // ws(k) = h2x[0 * npw + k] (j = 0 row of h2x is ws_k).
+cudaError_t device_check_finite(const double* x, size_t n, int* d_flag, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const size_t blocks = std::min<size_t>((n + 255) / 256, (size_t)sms * 8);
+  k_all_finite<<<(unsigned)blocks, 256, 0, st>>>(x, n, d_flag);
+  return cudaGetLastError();
+}
+
 cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const double* trg,
                                    cudaStream_t st) {
   const Params& P = D.P;

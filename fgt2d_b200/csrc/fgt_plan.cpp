@@ -265,40 +265,53 @@ static void build_tasks(HostPlan& H) {
   {
     long long per = 16LL * P.nexp * P.nd;
     std::vector<char> seen;
-    auto distinct = [&](const std::vector<int>& ids, int n) {
+    long long c = 0;
+    auto start = [&](int n) {
       seen.assign(n, 0);
-      long long c = 0;
-      for (int v : ids)
-        if (v >= 0 && !seen[v]) { seen[v] = 1; c++; }
-      return c;
+      c = 0;
     };
-    std::vector<int> a, b;
-    for (auto& s : H.merge) { a.push_back(s.src); b.push_back(s.dst); }
-    H.shift_bytes[0] = per * (distinct(a, H.nmp) + distinct(b, H.nmp));
-    a.clear(); b.clear();
-    for (auto& m : H.m2l) { b.push_back(m.loc); a.push_back(m.self_mp); }
-    for (auto& n : H.m2l_nbr) a.push_back(n.mp);
-    H.shift_bytes[1] = per * (distinct(a, H.nmp) + distinct(b, H.nloc));
-    a.clear(); b.clear();
-    for (auto& s : H.split) { a.push_back(s.src); b.push_back(s.dst); }
-    H.shift_bytes[2] = per * (distinct(a, H.nloc) + distinct(b, H.nloc));
+    auto see = [&](int v) {
+      if (v >= 0 && !seen[v]) { seen[v] = 1; c++; }
+    };
+    long long ra, rb;
+    start(H.nmp); for (auto& s : H.merge) see(s.src); ra = c;
+    start(H.nmp); for (auto& s : H.merge) see(s.dst); rb = c;
+    H.shift_bytes[0] = per * (ra + rb);
+    start(H.nmp); for (auto& m : H.m2l) see(m.self_mp); for (auto& n : H.m2l_nbr) see(n.mp); ra = c;
+    start(H.nloc); for (auto& m : H.m2l) see(m.loc); rb = c;
+    H.shift_bytes[1] = per * (ra + rb);
+    start(H.nloc); for (auto& s : H.split) see(s.src); ra = c;
+    start(H.nloc); for (auto& s : H.split) see(s.dst); rb = c;
+    H.shift_bytes[2] = per * (ra + rb);
   }
   // (d) near field, target-centric: for every leaf, the ifhung source boxes
   // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
-  std::vector<std::vector<int>> into(nb);  // box A -> source boxes S with A in list1(S)
+  // box A -> source boxes S with A in list1(S), as CSR in the order of S
+  std::vector<int> ioff(nb + 1, 0), into, icur;
   int nlevend = npl < P.nlevels ? npl : P.nlevels;
-  for (int l = 0; l <= nlevend; l++)
-    for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
-      if (!L.ifhung[s]) continue;
-      for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[L.l1[k]].push_back(s);
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 1) {
+      for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
+      into.assign(ioff[nb], 0);
+      icur.assign(ioff.begin(), ioff.end() - 1);
     }
+    for (int l = 0; l <= nlevend; l++)
+      for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
+        if (!L.ifhung[s]) continue;
+        for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) {
+          if (pass == 0) ioff[L.l1[k] + 1]++;
+          else into[icur[L.l1[k]]++] = s;
+        }
+      }
+  }
   const int CH = 32;  // one warp per task
   H.direct_pairs = 0;
+  std::vector<SrcRange> rs;
   for (int b = 0; b < nb; b++) {
     if (t.nchild[b] != 0) continue;
-    std::vector<SrcRange> rs;
+    rs.clear();
     for (int a = b; a >= 0; a = t.parent[a])
-      for (int s : into[a]) rs.push_back({t.s0[s], t.ns(s)});
+      for (int k = ioff[a]; k < ioff[a + 1]; k++) rs.push_back({t.s0[into[k]], t.ns(into[k])});
     if (rs.empty()) continue;
     long long nsrc = 0;
     for (auto& r : rs) nsrc += r.n;

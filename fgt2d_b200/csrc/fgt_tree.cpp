@@ -530,74 +530,92 @@ void build_lists(const Tree& t, Lists& L) {
     for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
       if (t.nchild[b] == 0 && t.ns(b) > 0) L.ifhung[b] = 1;
   // modified list1: tree_routs4.f:715-879 (2D, symmetric insertion at
-  // coarse levels) / tree_routs3d.f:511-619 (3D, coarser leaf neighbours)
-  std::vector<std::vector<int>> l1(nb);
-  if (t.nchild[0] == 0) l1[0].push_back(0);
+  // coarse levels) / tree_routs3d.f:511-619 (3D, coarser leaf neighbours).
+  // Two passes over the same sequence of insertions: the first counts per
+  // box, the second fills the CSR arrays in insertion order.
   auto cdist = [&](int a, int b, int d) { return std::fabs(t.c(a, d) - t.c(b, d)); };
-  for (int l = 1; l <= t.nlevels; l++) {
-    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-      if (t.nchild[b] != 0) continue;
-      for (int i = 0; i < t.ncoll[b]; i++) {
-        int jb = t.coll[(size_t)b * NCO + i];
-        if (l >= npw || t.nchild[jb] == 0) {
-          l1[b].push_back(jb);
-          continue;
-        }
-        double dist = 1.05 * (t.boxsize[l] + t.boxsize[l + 1]) / 2.0;
-        for (int j = 0; j < NCH; j++) {
-          int kb = t.ch(jb, j);
-          if (kb < 0) continue;
-          bool near = true;
-          for (int d = 0; d < D; d++)
-            if (!(cdist(kb, b, d) < dist)) near = false;
-          if (near) {
-            l1[b].push_back(kb);
-            if (D == 2) l1[kb].push_back(b);
+  std::vector<int> cur;
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 0) {
+      L.l1off.assign(nb + 1, 0);
+    } else {
+      for (int b = 0; b < nb; b++) L.l1off[b + 1] += L.l1off[b];
+      L.l1.assign(L.l1off[nb], 0);
+      cur.assign(L.l1off.begin(), L.l1off.end() - 1);
+    }
+    auto add = [&](int b, int v) {
+      if (pass == 0) L.l1off[b + 1]++;
+      else L.l1[cur[b]++] = v;
+    };
+    if (t.nchild[0] == 0) add(0, 0);
+    for (int l = 1; l <= t.nlevels; l++) {
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (t.nchild[b] != 0) continue;
+        for (int i = 0; i < t.ncoll[b]; i++) {
+          int jb = t.coll[(size_t)b * NCO + i];
+          if (l >= npw || t.nchild[jb] == 0) {
+            add(b, jb);
+            continue;
+          }
+          double dist = 1.05 * (t.boxsize[l] + t.boxsize[l + 1]) / 2.0;
+          for (int j = 0; j < NCH; j++) {
+            int kb = t.ch(jb, j);
+            if (kb < 0) continue;
+            bool near = true;
+            for (int d = 0; d < D; d++)
+              if (!(cdist(kb, b, d) < dist)) near = false;
+            if (near) {
+              add(b, kb);
+              if (D == 2) add(kb, b);
+            }
           }
         }
-      }
-      if (D == 3) {
-        int dad = t.parent[b];
-        double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
-        for (int i = 0; i < t.ncoll[dad]; i++) {
-          int jb = t.coll[(size_t)dad * NCO + i];
-          if (t.nchild[jb] != 0) continue;
-          bool near = true;
-          for (int d = 0; d < D; d++)
-            if (!(cdist(jb, b, d) < dist)) near = false;
-          if (near) l1[b].push_back(jb);
+        if (D == 3) {
+          int dad = t.parent[b];
+          double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+          for (int i = 0; i < t.ncoll[dad]; i++) {
+            int jb = t.coll[(size_t)dad * NCO + i];
+            if (t.nchild[jb] != 0) continue;
+            bool near = true;
+            for (int d = 0; d < D; d++)
+              if (!(cdist(jb, b, d) < dist)) near = false;
+            if (near) add(b, jb);
+          }
         }
       }
     }
   }
-  L.l1off.assign(nb + 1, 0);
-  for (int b = 0; b < nb; b++) L.l1off[b + 1] = L.l1off[b] + (int)l1[b].size();
-  L.l1.resize(L.l1off[nb]);
-  for (int b = 0; b < nb; b++) std::copy(l1[b].begin(), l1[b].end(), L.l1.begin() + L.l1off[b]);
 
-  // plane-wave lists
-  L.pwoff.assign(nb + 1, 0);
-  L.pw.clear();
-  std::vector<std::vector<int>> pw(nb);
+  // plane-wave lists, the same two passes
   int nls = std::max(npw, 0);
-  for (int l = nls; l <= t.nlevels; l++)
-    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-      if (l == npw) {
-        for (int i = 0; i < t.ncoll[b]; i++) {
-          int jb = t.coll[(size_t)b * NCO + i];
-          if (jb != b && (D == 2 || t.nchild[jb] > 0)) pw[b].push_back(jb);
-        }
-      } else if (l > nls) {
-        int dad = t.parent[b];
-        for (int j = 0; j < NCH; j++) {
-          int jb = t.ch(dad, j);
-          if (jb >= 0 && jb != b) pw[b].push_back(jb);
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 0) {
+      L.pwoff.assign(nb + 1, 0);
+    } else {
+      for (int b = 0; b < nb; b++) L.pwoff[b + 1] += L.pwoff[b];
+      L.pw.assign(L.pwoff[nb], 0);
+      cur.assign(L.pwoff.begin(), L.pwoff.end() - 1);
+    }
+    auto add = [&](int b, int v) {
+      if (pass == 0) L.pwoff[b + 1]++;
+      else L.pw[cur[b]++] = v;
+    };
+    for (int l = nls; l <= t.nlevels; l++)
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (l == npw) {
+          for (int i = 0; i < t.ncoll[b]; i++) {
+            int jb = t.coll[(size_t)b * NCO + i];
+            if (jb != b && (D == 2 || t.nchild[jb] > 0)) add(b, jb);
+          }
+        } else if (l > nls) {
+          int dad = t.parent[b];
+          for (int j = 0; j < NCH; j++) {
+            int jb = t.ch(dad, j);
+            if (jb >= 0 && jb != b) add(b, jb);
+          }
         }
       }
-    }
-  for (int b = 0; b < nb; b++) L.pwoff[b + 1] = L.pwoff[b] + (int)pw[b].size();
-  L.pw.resize(L.pwoff[nb]);
-  for (int b = 0; b < nb; b++) std::copy(pw[b].begin(), pw[b].end(), L.pw.begin() + L.pwoff[b]);
+  }
 
   // iflocal: cut-level leaves with a non-leaf colleague (fgt2d.f:790-814)
   L.iflocal.assign(nb, 0);

@@ -153,3 +153,18 @@ def test_bad_arguments(fgt):
     with pytest.raises(fgt.FGTError) as e:
         fgt.transform(2, 1, 1e-3, 1e-6, [[0.1, 0.2]], [1.0], ifpgh=2, ctx=ctx)
     assert e.value.status == 2
+    # non-finite charges and targets, checked on either tree build
+    rng = np.random.default_rng(3)
+    src, trg = rng.random((2000, 2)), rng.random((100, 2))
+    q = rng.random(2000)
+    q[1234] = np.nan
+    trg_bad = trg.copy()
+    trg_bad[7, 1] = np.inf
+    for tree in ("device", "host"):
+        c = fgt.Context(0, tree=tree)
+        with pytest.raises(fgt.FGTError) as e:
+            fgt.fgt2d(1, 1e-4, 1e-6, src, q, trg, 1, 1, ctx=c)
+        assert e.value.status == 1
+        with pytest.raises(fgt.FGTError) as e:
+            fgt.fgt2d(1, 1e-4, 1e-6, src, np.ones(2000), trg_bad, 1, 1, ctx=c)
+        assert e.value.status == 1
