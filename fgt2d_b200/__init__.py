@@ -64,6 +64,21 @@ class PlanInfo(ctypes.Structure):
         return d
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("nd", ctypes.c_int), ("delta", ctypes.c_double),
+                ("eps", ctypes.c_double), ("ns", ctypes.c_int), ("sources", _dp), ("charge", _dp),
+                ("nt", ctypes.c_int), ("targ", _dp), ("ifpgh", ctypes.c_int),
+                ("ifpghtarg", ctypes.c_int), ("pot", _dp), ("pottarg", _dp)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("points", ctypes.c_longlong),
+                ("peak_bytes", ctypes.c_longlong), ("budget_bytes", ctypes.c_longlong),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double),
+                ("max_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+
+
 def lib():
     """Loads the CUDA library; raises if it has not been built."""
     global _lib
@@ -78,6 +93,12 @@ def lib():
     L.fgt_ctx_set_precision.argtypes = [_vp, i]
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
     L.fgt_ctx_set_tree.argtypes = [_vp, i]
+    L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
+    L.fgt_server_set_precision.argtypes = [_vp, i]
+    L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
+    L.fgt_server_wait.argtypes = [_vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]
+    L.fgt_server_stats_get.argtypes = [_vp, ctypes.POINTER(ServerStats)]
+    L.fgt_server_destroy.argtypes = [_vp]
     L.fgt_device_tree_create.argtypes = [_vp, i, d, d, i, _dp, i, _dp, ctypes.POINTER(_vp)]
     L.fgt_default_ctx.restype = _vp
     L.fgt_ctx_stream.restype = _vp
@@ -309,3 +330,59 @@ def _tree_dict(h):
         return out
     finally:
         L.fgt_host_tree_destroy(h)
+
+
+class Server:
+    """Transform server on one device (continuous batching of independent
+    requests over worker streams, admission by device-memory footprint)."""
+
+    def __init__(self, device=0, max_bytes=0, workers=4, precision="auto"):
+        L = lib()
+        h = _vp()
+        _check(L.fgt_server_create(int(device), int(max_bytes), int(workers), ctypes.byref(h)),
+               "fgt_server_create")
+        self._h = h
+        p = _PREC[precision] if isinstance(precision, str) else int(precision)
+        _check(L.fgt_server_set_precision(h, p), "fgt_server_set_precision")
+        self._live = {}
+
+    def submit(self, dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0):
+        """Queues one transform; returns its id.  The arrays are kept alive here."""
+        src = _f64(sources, (-1, dim))
+        ns = src.shape[0]
+        q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
+        trg = (src if targ is sources else _f64(targ, (-1, dim))) if targ is not None else None
+        nt = trg.shape[0] if trg is not None else 0
+        pot = np.empty((ns, nd)) if ifpgh else None
+        pt = np.empty((nt, nd)) if ifpghtarg else None
+        r = Request(dim, nd, float(delta), float(eps), ns, _p(src), _p(q), nt, _p(trg), ifpgh,
+                    ifpghtarg, _p(pot), _p(pt))
+        rid = ctypes.c_longlong()
+        _check(lib().fgt_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "fgt_server_submit")
+        self._live[rid.value] = (src, q, trg, pot, pt)
+        return rid.value
+
+    def wait(self, rid):
+        """Blocks until request rid is done; returns (pot, pottarg, latency_s)."""
+        lat = ctypes.c_double()
+        st = lib().fgt_server_wait(self._h, int(rid), ctypes.byref(lat))
+        src, q, trg, pot, pt = self._live.pop(rid)
+        _check(st, "fgt_server_wait")
+        return pot, pt, lat.value
+
+    def stats(self):
+        s = ServerStats()
+        _check(lib().fgt_server_stats_get(self._h, ctypes.byref(s)), "fgt_server_stats_get")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fgt_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -6,10 +6,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <condition_variable>
+#include <functional>
+#include <thread>
+#include <unordered_map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <vector>
+
+#include <omp.h>
 
 #include "fgt_b200.h"
 #include "fgt_device.hpp"
@@ -42,6 +49,9 @@ struct fgt_plan {
   double* d_work = nullptr;  // large-delta local expansion
   int* d_flag = nullptr;     // device-side argument checks
   int last_launches = 0;
+  // recorded after every execute on the stream it used: the frees of
+  // fgt_plan_destroy (stream-ordered on the context's stream) wait for it
+  cudaEvent_t done = nullptr;
 };
 
 namespace {
@@ -95,22 +105,17 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
 }
 
 // Device copies of the caller-order arrays (sources, charges, targets,
-// potentials, large-delta work) in one allocation; uploads the points.
-int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int nlocal0, const double* src_host,
-             const double* trg_host, bool upload_trg) {
+// potentials) in one allocation; uploads the points.  The large-delta work
+// array is sized once the order is known (plan_device re-allocates then).
+int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, const double* src_host, const double* trg_host,
+             bool upload_trg) {
   size_t n_src = (size_t)ns * dim, n_chg = (size_t)ns * nd, n_trg = (size_t)nt * dim;
   size_t n_pot = (size_t)ns * nd, n_pt = (size_t)nt * nd;
-  // large-delta local expansion: the order is known only after the bounding
-  // box, so reserve for the largest order the term rule gives (nlocal0 < 0:
-  // size it later in plan_device)
-  size_t n_work = 0;
-  if (nlocal0 >= 0) {
-    size_t Pn = nlocal0 + 1;
-    n_work = 4 + nd * (dim == 2 ? Pn * Pn : Pn * Pn * Pn);
-  }
+  const size_t n_work = 0;
   auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
   p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
-  CKS(cudaMalloc(&p->d_io, p->io_bytes));
+  CKS(device_pool_setup());
+  CKS(cudaMallocAsync(reinterpret_cast<void**>(&p->d_io), p->io_bytes, p->ctx->stream));
   double* c = p->d_io;
   p->d_src = c; c += al(n_src);
   p->d_chg = c; c += al(n_chg);
@@ -142,13 +147,11 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
   size_t n_src = ns * dim, n_chg = ns * nd, n_trg = nt * dim, n_pot = ns * nd, n_pt = nt * nd;
   size_t n_work = 0;
-  if (P.large_delta) {
-    size_t Pn = P.nlocal0 + 1;
-    n_work = 4 + nd * (dim == 2 ? Pn * Pn : Pn * Pn * Pn);
-  }
+  if (P.large_delta) n_work = large_delta_work_doubles(P, true);
   auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
   p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
-  CKS(cudaMalloc(&p->d_io, p->io_bytes));
+  CKS(device_pool_setup());
+  CKS(cudaMallocAsync(reinterpret_cast<void**>(&p->d_io), p->io_bytes, p->ctx->stream));
   double* c = p->d_io;
   p->d_src = c; c += al(n_src);
   p->d_chg = c; c += al(n_chg);
@@ -171,10 +174,14 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
 // Plan whose tree build does its point work on the GPU (fgt_devtree.cu).  The
 // largest large-delta order is not known before the bounding box, so that
 // path re-allocates its work array once the order is.
+// admit (optional) is called with the device bytes of the plan proper once
+// the tree is built and before they are allocated; it may block, and a
+// status other than FGT_OK abandons the plan.
 int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double eps, int ns,
-                            const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg) {
+                            const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                            const std::function<int(size_t)>* admit = nullptr) {
   const bool same = targ == sources && nt == ns;
-  int st = alloc_io(p, dim, nd, ns, nt, -1, sources, targ, !same);
+  int st = alloc_io(p, dim, nd, ns, nt, sources, targ, !same);
   if (st != FGT_OK) return st;
   st = check_finite_device(p, p->d_src, (size_t)ns * dim);
   if (st == FGT_OK && !same) st = check_finite_device(p, p->d_trg, (size_t)nt * dim);
@@ -182,11 +189,12 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   cudaStream_t s = p->ctx->stream;
   const double* d_trg = same ? p->d_src : p->d_trg;
   int* perms = nullptr;
-  CKS(cudaMalloc(&perms, sizeof(int) * ((size_t)ns + nt + 2)));
+  CKS(cudaMallocAsync(reinterpret_cast<void**>(&perms), sizeof(int) * ((size_t)ns + nt + 2), s));
   struct Free {
     int* q;
-    ~Free() { cudaFree(q); }
-  } fr{perms};
+    cudaStream_t st;
+    ~Free() { cudaFreeAsync(q, st); }
+  } fr{perms, s};
   int *d_isrc = perms, *d_itarg = perms + ns + 1;
   try {
     CKS(build_plan_device(p->H, dim, nd, delta, eps, ns, p->d_src, nt, d_trg, same, ifpgh, ifpghtarg,
@@ -202,11 +210,18 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     CKS(cudaMemcpyAsync(hs.data(), p->d_src, hs.size() * 8, cudaMemcpyDeviceToHost, s));
     if (!same && nt > 0) CKS(cudaMemcpyAsync(ht.data(), p->d_trg, ht.size() * 8, cudaMemcpyDeviceToHost, s));
     CKS(cudaStreamSynchronize(s));
-    cudaFree(p->d_io);
+    cudaFreeAsync(p->d_io, s);
     p->d_io = nullptr;
     return plan_device(p, hs.data(), same ? hs.data() : ht.data());
   }
   if (same && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, p->d_src, (size_t)nt * dim * 8, cudaMemcpyDeviceToDevice, s));
+  if (admit) {
+    size_t bytes = 0;
+    DevicePlan probe;
+    CKS(device_plan_create(p->H, probe, d_isrc, d_itarg, s, &bytes));
+    st = (*admit)(bytes);
+    if (st != FGT_OK) return st;
+  }
   CKS(device_plan_create(p->H, p->D, d_isrc, d_itarg, s));
   p->have_device = true;
   CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, s));
@@ -221,13 +236,15 @@ int run_device(fgt_plan* p, const double* q, double* pot, double* pt, cudaStream
                StageTimes* times) {
   const Params& P = p->H.P;
   int prec = resolve_precision(p->ctx, P.eps);
+  if (!p->done) CKS(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
   if (P.large_delta) {
-    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, pot, pt, p->d_work, st));
+    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, pot, pt, p->d_work, st, true));
     p->last_launches = (P.ns > 0) + (P.ifpgh == 1) + (P.ifpghtarg == 1);
-    return FGT_OK;
+  } else {
+    CKS(device_plan_execute(p->D, q, pot, pt, prec, st, times));
+    p->last_launches = (int)p->D.launches;
   }
-  CKS(device_plan_execute(p->D, q, pot, pt, prec, st, times));
-  p->last_launches = (int)p->D.launches;
+  CKS(cudaEventRecord(p->done, st));
   return FGT_OK;
 }
 
@@ -403,8 +420,16 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
 int fgt_plan_destroy(fgt_plan* p) {
   if (!p) return FGT_ERR_BADARG;
   if (p->ctx) cudaSetDevice(p->ctx->device);
-  if (p->have_device) device_plan_destroy(p->D);
-  if (p->d_io) cudaFree(p->d_io);
+  if (p->done) {
+    // the stream-ordered frees below follow the last execute, on any stream
+    cudaStreamWaitEvent(p->ctx->stream, p->done, 0);
+    cudaEventDestroy(p->done);
+  }
+  if (p->have_device) {
+    p->D.stream = p->ctx->stream;
+    device_plan_destroy(p->D);
+  }
+  if (p->d_io) cudaFreeAsync(p->d_io, p->ctx->stream);
   delete p;
   return FGT_OK;
 }
@@ -814,6 +839,264 @@ int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                              ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
                              centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot,
                              ifpghtarg, pottarg);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- serving
+// A transform server on one device: requests of any dimension, size, delta and
+// eps are queued as they arrive; worker threads, each with its own context
+// and CUDA stream, take the smallest pending request (the oldest once it has
+// waited longer than kServerAgeS), build its plan and run it, so requests
+// that arrive while others are on the GPU overlap with them.  Device memory
+// is admitted by footprint from two pools that cannot deadlock: the point
+// arrays and tree scratch of a request (a fixed share of the budget), then
+// the exact bytes of its plan, computed before they are allocated.  A plan
+// pool holder never waits for anything else, so point-pool holders waiting
+// for plan memory always see it freed.
+
+struct fgt_server {
+  int device = 0;
+  long long budget = 0, budget_pts = 0, budget_plan = 0;
+  std::vector<fgt_ctx*> ctxs;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_q, cv_mem, cv_done;
+  struct Job {
+    fgt_request r;
+    long long id = 0;
+    double t_sub = 0, t_start = 0, t_end = 0;
+    int status = FGT_OK;
+    bool done = false;
+  };
+  std::vector<Job*> queue;
+  std::unordered_map<long long, Job*> jobs;
+  long long next_id = 1;
+  long long in_pts = 0, in_plan = 0, peak = 0;
+  bool stop = false;
+  long long submitted = 0, completed = 0, failed = 0, points = 0;
+  std::vector<double> lat;
+  double t_first = -1, t_last = 0;
+};
+
+namespace {
+constexpr double kServerAgeS = 0.05;
+
+long long request_points(const fgt_request& r) {
+  return (r.ifpgh == 1 ? r.ns : 0) + (r.ifpghtarg == 1 && r.targ ? r.nt : 0);
+}
+
+// blocks until b bytes fit in the pool (or the pool is idle), then takes them
+void server_take(fgt_server* S, long long* in_use, long long cap, long long b) {
+  std::unique_lock<std::mutex> lk(S->mu);
+  S->cv_mem.wait(lk, [&] { return *in_use + b <= cap || *in_use == 0; });
+  *in_use += b;
+  S->peak = std::max(S->peak, S->in_pts + S->in_plan);
+}
+void server_give(fgt_server* S, long long* in_use, long long b) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  *in_use -= b;
+  S->cv_mem.notify_all();
+}
+
+int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
+  const int nt = r.targ ? r.nt : 0;
+  int st = check_args(r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, 1, 0, r.ifpgh, nt, r.targ,
+                      r.ifpghtarg, false);
+  if (st != FGT_OK) return st;
+  auto zero = [&] {
+    if (r.ifpgh == 1 && r.ns > 0 && r.pot) memset(r.pot, 0, sizeof(double) * (size_t)r.ns * r.nd);
+    if (r.ifpghtarg == 1 && nt > 0 && r.pottarg) memset(r.pottarg, 0, sizeof(double) * (size_t)nt * r.nd);
+  };
+  if (r.ns == 0) {
+    zero();
+    return FGT_OK;
+  }
+  CKS(cudaSetDevice(ctx->device));
+  // point arrays (caller order, sorted copies, potentials) and tree scratch
+  const long long npts = (long long)r.ns + nt;
+  const long long est_pts = 8LL * ((long long)r.ns * (2 * r.dim + 3 * r.nd) + (long long)nt * (2 * r.dim + 3 * r.nd)) +
+                            64LL * npts + (1 << 20);
+  server_take(S, &S->in_pts, S->budget_pts, est_pts);
+  long long plan_bytes = 0;
+  std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
+  if (!p) {
+    server_give(S, &S->in_pts, est_pts);
+    return FGT_ERR_NOMEM;
+  }
+  p->ctx = ctx;
+  std::function<int(size_t)> admit = [&](size_t b) {
+    plan_bytes = (long long)b;
+    server_take(S, &S->in_plan, S->budget_plan, plan_bytes);
+    return FGT_OK;
+  };
+  st = plan_create_device_tree(p.get(), r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, nt, r.targ, r.ifpgh,
+                               r.ifpghtarg, &admit);
+  if (st == FGT_OK) st = fgt_plan_execute_host(p.get(), r.sources, r.charge, r.targ, r.pot, r.pottarg);
+  fgt_plan_destroy(p.release());
+  cudaStreamSynchronize(ctx->stream);  // the stream-ordered frees have run
+  if (plan_bytes) server_give(S, &S->in_plan, plan_bytes);
+  server_give(S, &S->in_pts, est_pts);
+  if (st != FGT_OK) zero();
+  return st;
+}
+
+void server_worker(fgt_server* S, int w) {
+  fgt_ctx* ctx = S->ctxs[w];
+  // the workers share the host cores: each builds its host-side plan parts
+  // with its share of them
+  omp_set_num_threads(std::max(1, omp_get_num_procs() / (int)S->ctxs.size()));
+  for (;;) {
+    fgt_server::Job* J = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_q.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      if (S->queue.empty()) return;  // stop requested and nothing left
+      const double t = now_s();
+      size_t pick = 0;
+      for (size_t k = 1; k < S->queue.size(); k++) {
+        const fgt_server::Job* a = S->queue[k];
+        const fgt_server::Job* b = S->queue[pick];
+        const bool a_old = t - a->t_sub > kServerAgeS, b_old = t - b->t_sub > kServerAgeS;
+        if (a_old != b_old ? a_old
+                           : (a_old ? a->t_sub < b->t_sub
+                                    : (long long)a->r.ns + a->r.nt < (long long)b->r.ns + b->r.nt))
+          pick = k;
+      }
+      J = S->queue[pick];
+      S->queue.erase(S->queue.begin() + pick);
+      J->t_start = t;
+    }
+    const int st = server_run(S, ctx, J->r);
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      J->t_end = now_s();
+      J->status = st;
+      J->done = true;
+      S->completed++;
+      if (st != FGT_OK) S->failed++;
+      else S->points += request_points(J->r);
+      S->lat.push_back(J->t_end - J->t_sub);
+      S->t_last = std::max(S->t_last, J->t_end);
+      S->cv_done.notify_all();
+    }
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_server** out) {
+  if (!out || nworkers < 1 || nworkers > 64) return FGT_ERR_BADARG;
+  *out = nullptr;
+  std::unique_ptr<fgt_server> S(new (std::nothrow) fgt_server());
+  if (!S) return FGT_ERR_NOMEM;
+  S->device = device;
+  if (max_device_bytes <= 0) {
+    size_t fr = 0, tot = 0;
+    CKS(cudaSetDevice(device));
+    CKS(cudaMemGetInfo(&fr, &tot));
+    max_device_bytes = (long long)(0.8 * fr);
+  }
+  S->budget = max_device_bytes;
+  S->budget_pts = max_device_bytes / 4;
+  S->budget_plan = max_device_bytes - S->budget_pts;
+  for (int w = 0; w < nworkers; w++) {
+    fgt_ctx* c = nullptr;
+    int st = fgt_ctx_create(device, &c);
+    if (st != FGT_OK) {
+      for (fgt_ctx* x : S->ctxs) fgt_ctx_destroy(x);
+      return st;
+    }
+    S->ctxs.push_back(c);
+  }
+  fgt_server* raw = S.release();
+  for (int w = 0; w < nworkers; w++) raw->workers.emplace_back(server_worker, raw, w);
+  *out = raw;
+  return FGT_OK;
+}
+
+int fgt_server_set_precision(fgt_server* s, int precision) {
+  if (!s) return FGT_ERR_BADARG;
+  for (fgt_ctx* c : s->ctxs) {
+    int st = fgt_ctx_set_precision(c, precision);
+    if (st != FGT_OK) return st;
+  }
+  return FGT_OK;
+}
+
+int fgt_server_submit(fgt_server* s, const fgt_request* req, long long* id) {
+  if (!s || !req || !id) return FGT_ERR_BADARG;
+  auto* J = new (std::nothrow) fgt_server::Job();
+  if (!J) return FGT_ERR_NOMEM;
+  J->r = *req;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    delete J;
+    return FGT_ERR_BADARG;
+  }
+  J->id = s->next_id++;
+  J->t_sub = now_s();
+  if (s->t_first < 0) s->t_first = J->t_sub;
+  s->jobs[J->id] = J;
+  s->queue.push_back(J);
+  s->submitted++;
+  *id = J->id;
+  s->cv_q.notify_one();
+  return FGT_OK;
+}
+
+int fgt_server_wait(fgt_server* s, long long id, double* latency_s) {
+  if (!s) return FGT_ERR_BADARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return FGT_ERR_BADARG;
+  fgt_server::Job* J = it->second;
+  s->cv_done.wait(lk, [&] { return J->done; });
+  const int st = J->status;
+  if (latency_s) *latency_s = J->t_end - J->t_sub;
+  s->jobs.erase(it);
+  delete J;
+  return st;
+}
+
+int fgt_server_stats_get(fgt_server* s, fgt_server_stats* out) {
+  if (!s || !out) return FGT_ERR_BADARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  memset(out, 0, sizeof(*out));
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->failed = s->failed;
+  out->points = s->points;
+  out->peak_bytes = s->peak;
+  out->budget_bytes = s->budget;
+  if (!s->lat.empty()) {
+    std::vector<double> v = s->lat;
+    std::sort(v.begin(), v.end());
+    auto q = [&](double f) { return v[std::min(v.size() - 1, (size_t)(f * (v.size() - 1) + 0.5))]; };
+    out->p50_s = q(0.50);
+    out->p99_s = q(0.99);
+    out->max_s = v.back();
+    double m = 0;
+    for (double x : v) m += x;
+    out->mean_s = m / v.size();
+  }
+  out->span_s = s->t_first >= 0 ? s->t_last - s->t_first : 0.0;
+  return FGT_OK;
+}
+
+int fgt_server_destroy(fgt_server* s) {
+  if (!s) return FGT_ERR_BADARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv_q.notify_all();
+  }
+  for (auto& t : s->workers) t.join();
+  for (auto& kv : s->jobs) delete kv.second;
+  for (fgt_ctx* c : s->ctxs) fgt_ctx_destroy(c);
+  delete s;
+  return FGT_OK;
 }
 
 }  // extern "C"

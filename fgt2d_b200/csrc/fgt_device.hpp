@@ -43,6 +43,7 @@ struct DevicePlan {
   // buffers (one allocation, carved)
   char* base = nullptr;
   size_t bytes = 0;
+  cudaStream_t stream = 0;  // stream of the stream-ordered allocation
   double* centers = nullptr;
   double* h2x = nullptr;
   double* x2l = nullptr;
@@ -109,11 +110,17 @@ struct DevicePlan {
   long long launches = 0;
 };
 
+// Makes freed stream-ordered allocations stay in the current device's default
+// memory pool (once per device).
+cudaError_t device_pool_setup();
+
 // Uploads the host plan; returns cudaSuccess or the first error.  The point
 // permutations come from H.tree (host) or, when d_isrc is given, from device
-// arrays (d_isrc: ns, d_itarg: nt) copied on stream st.
+// arrays (d_isrc: ns, d_itarg: nt) copied on stream st.  With size_only, only
+// the device bytes the plan needs are computed (nothing is allocated).
 cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_isrc = nullptr,
-                               const int* d_itarg = nullptr, cudaStream_t st = 0);
+                               const int* d_itarg = nullptr, cudaStream_t st = 0,
+                               size_t* size_only = nullptr);
 
 // Tree and plan with the point work of the tree build on the GPU
 // (fgt_devtree.cu).  d_src (ns, dim) and d_trg (nt, dim) are device arrays in
@@ -156,8 +163,13 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
 size_t large_delta_noalloc_capacity();
 
 // Large-delta path (one Taylor local about the root centre), no tree.
+// deterministic: the sources' contributions are summed in a fixed order
+// through per-CTA partial blocks (work must hold large_delta_work_doubles(P,
+// true) doubles); otherwise they are added atomically (nd (nlocal0+1)^dim + 4
+// doubles of work; results can differ in the last bits from call to call).
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
                                 const double* trg, double* pot, double* pottarg, double* work,
-                                cudaStream_t stream);
+                                cudaStream_t stream, bool deterministic);
+size_t large_delta_work_doubles(const Params& P, bool deterministic);
 
 }  // namespace fgtb

@@ -141,16 +141,19 @@ __global__ void __launch_bounds__(256) k_locate(const double* __restrict__ x, in
   if (i < n && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(leafcnt + r, __popc(m));
 }
 
-// Device scratch that grows on demand and is freed at the end of the build.
+// Device scratch of one build, stream-ordered on the build's stream (no
+// device-wide synchronisation) and freed at the end of the build.
 struct Scratch {
+  cudaStream_t st;
   std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : st(s) {}
   ~Scratch() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) cudaFreeAsync(p, st);
   }
   template <typename T>
   cudaError_t get(T** out, size_t n) {
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), st);
     if (e != cudaSuccess) return e;
     ptrs.push_back(p);
     *out = static_cast<T*>(p);
@@ -166,7 +169,7 @@ cudaError_t upload(T* dst, const T* src, size_t n, cudaStream_t st) {
 
 cudaError_t device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim, double* mn,
                         double* mx, cudaStream_t st) {
-  Scratch S;
+  Scratch S(st);
   const int nb = 296;
   double* part = nullptr;
   CKD(S.get(&part, (size_t)12 * nb));
@@ -192,7 +195,7 @@ cudaError_t sort_points_device(const Tree& t, const double* d_x, int n, const in
                                const int* d_nchild, const int* d_child, const double* d_cen,
                                const int* d_rank, int nleaf, const std::vector<int>& leaf_of_rank,
                                int* d_perm, std::vector<int>& r0, std::vector<int>& r1, cudaStream_t st) {
-  Scratch S;
+  Scratch S(st);
   int *key = nullptr, *key2 = nullptr, *idx = nullptr, *cnt = nullptr, *err = nullptr;
   CKD(S.get(&key, n));
   CKD(S.get(&key2, n));
@@ -234,7 +237,7 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
   const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   const double tA = now_s();
   tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
-  Scratch S;
+  Scratch S(st);
   int* pbox = nullptr;
   CKD(S.get(&pbox, ns));
   CKD(cudaMemsetAsync(pbox, 0, sizeof(int) * std::max(ns, 1), st));

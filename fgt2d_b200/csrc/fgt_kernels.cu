@@ -33,6 +33,7 @@ namespace fgtb {
 namespace {
 
 constexpr int FORM_CH = 32;    // sources staged per chunk in the form kernels
+constexpr int LD_PARTS = 256;  // CTAs (partial blocks) of the deterministic large-delta form
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 struct KP {
@@ -1684,7 +1685,7 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
 // partial sum per CTA added into the global array.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const double* __restrict__ cen,
-                                                 double* __restrict__ local) {
+                                                 double* __restrict__ local, double* __restrict__ partial) {
   const int Pn = p + 1;
   const int nent = DIM == 2 ? Pn * Pn : Pn * Pn * Pn;
   extern __shared__ double sm[];
@@ -1731,8 +1732,19 @@ __global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const doub
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       const int e = e0 + threadIdx.x + s * 256;
-      if (e < nent) atomicAdd(local + (size_t)ind * nent + e, acc[s]);
+      if (e >= nent) continue;
+      if (partial) partial[((size_t)ind * gridDim.x + blockIdx.x) * nent + e] = acc[s];
+      else atomicAdd(local + (size_t)ind * nent + e, acc[s]);
     }
+  }
+}
+// local = sum of the per-CTA partial blocks, in CTA order (deterministic)
+__global__ void k_ld_sum(int nent, int nparts, const double* __restrict__ partial, double* __restrict__ local) {
+  const int ind = blockIdx.y;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nent; e += gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int c = 0; c < nparts; c++) a += partial[((size_t)ind * nparts + c) * nent + e];
+    local[(size_t)ind * nent + e] = a;
   }
 }
 template <int DIM>
@@ -1803,8 +1815,27 @@ size_t al(size_t b) { return (b + 255) & ~size_t(255); }
     if (e_ != cudaSuccess) return e_;       \
   } while (0)
 
+cudaError_t device_pool_setup() {
+  // keep freed stream-ordered allocations in the device's default pool
+  // instead of returning them at every synchronisation (process-local
+  // runtime state, once per device)
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && !done[dev]) {
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_isrc, const int* d_itarg,
-                               cudaStream_t pst) {
+                               cudaStream_t pst, size_t* size_only) {
   D = DevicePlan();
   D.P = H.P;
   const Params& P = H.P;
@@ -1989,14 +2020,20 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
                  al(lo_doubles * 8) + 4096;
   D.bytes = total;
+  if (size_only) {
+    *size_only = total;
+    return cudaSuccess;
+  }
   const auto tnow = [] {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   };
   const double tm0 = tnow();
-  CK(cudaMalloc(&D.base, total));
+  D.stream = pst;
+  CK(device_pool_setup());
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&D.base), total, pst));
   if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "device plan: malloc %.4f (%zu bytes)\n", tnow() - tm0, total);
   char* cur = D.base;
-  cudaStream_t s = 0;
+  cudaStream_t s = pst;
   CK(put(cur, D.centers, H.box_centers, s));
   CK(put(cur, D.h2x, H.h2x, s));
   CK(put(cur, D.x2l, H.x2l, s));
@@ -2078,7 +2115,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
 }
 
 void device_plan_destroy(DevicePlan& D) {
-  if (D.base) cudaFree(D.base);
+  if (D.base) cudaFreeAsync(D.base, D.stream);
   D.base = nullptr;
 }
 
@@ -2375,9 +2412,15 @@ cudaError_t probe_fp64_mma(double* tflops) {
   return cudaGetLastError();
 }
 
+size_t large_delta_work_doubles(const Params& P, bool deterministic) {
+  const size_t Pn = P.nlocal0 + 1;
+  const size_t nent = P.dim == 2 ? Pn * Pn : Pn * Pn * Pn;
+  return 4 + (size_t)P.nd * nent * (deterministic ? 1 + LD_PARTS : 1);
+}
+
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
                                 const double* trg, double* pot, double* pottarg, double* work,
-                                cudaStream_t st) {
+                                cudaStream_t st, bool deterministic) {
   KP k;
   memset(&k, 0, sizeof(k));
   k.dim = P.dim; k.nd = P.nd; k.dsq = P.dsq; k.delta = P.delta;
@@ -2395,10 +2438,17 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const double
     CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
     CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
   }
-  int blocks = std::max(1, std::min(1024, (P.ns + 255) / 256));
+  // deterministic: per-CTA partial blocks after the local block, summed in
+  // CTA order; otherwise atomic accumulation (last-bit order dependence)
+  double* partial = deterministic ? local + nent * P.nd : nullptr;
+  int blocks = std::max(1, std::min(deterministic ? LD_PARTS : 1024, (P.ns + 255) / 256));
   if (P.ns > 0) {
-    if (P.dim == 2) k_ld_form<2><<<dim3(blocks, P.nd), 256, sh, st>>>(k, P.ns, p, cen, local);
-    else k_ld_form<3><<<dim3(blocks, P.nd), 256, sh, st>>>(k, P.ns, p, cen, local);
+    if (P.dim == 2) k_ld_form<2><<<dim3(blocks, P.nd), 256, sh, st>>>(k, P.ns, p, cen, local, partial);
+    else k_ld_form<3><<<dim3(blocks, P.nd), 256, sh, st>>>(k, P.ns, p, cen, local, partial);
+    if (deterministic) {
+      const int sb = std::max(1, std::min(1024, (int)((nent + 255) / 256)));
+      k_ld_sum<<<dim3(sb, P.nd), 256, 0, st>>>((int)nent, blocks, partial, local);
+    }
   }
   auto ev = [&](const double* pts, int n, double* out) {
     if (n <= 0) return;
@@ -2459,7 +2509,7 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
   }
   // large_delta_execute copies the centre into work[0..2] and clears the
   // local expansion in work[4..] before accumulating into it
-  return large_delta_execute(P, src, chg, trg, pot, pottarg, work, st);
+  return large_delta_execute(P, src, chg, trg, pot, pottarg, work, st, false);
 }
 
 }  // namespace fgtb

@@ -126,7 +126,7 @@ struct Builder {
   // computecoll, tree_routs4.f:100-211, levels [l0, l1]
   void colleagues_level(int l) {
     double lim = F105 * t.boxsize[l];
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
     for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
       int dad = t.parent[b];
       int n = 0;

@@ -197,6 +197,48 @@ int fgt_host_tree_dims(const fgt_host_tree* t, int* dims);
 long long fgt_host_tree_field(const fgt_host_tree* t, int field, void* out);
 int fgt_host_tree_destroy(fgt_host_tree* t);
 
+/* ---- serving ----------------------------------------------------------------
+ * No counterpart in the reference (a Fortran library call).  A server on one
+ * device accepts transforms of any dimension, size, delta and eps as they
+ * arrive and runs them on worker threads, each with its own stream, so
+ * requests that arrive while others are on the GPU overlap with them.  The
+ * smallest pending request goes first (the oldest once it has waited 50 ms).
+ * Device memory is admitted by footprint: a quarter of max_device_bytes for
+ * the requests' point arrays and tree scratch, the rest for their plans,
+ * whose exact size is known before allocation; a request that does not fit
+ * waits until memory frees up (or runs alone when nothing else is in
+ * flight).  max_device_bytes <= 0 uses 80% of the free memory.
+ * The request's host arrays must stay valid until fgt_server_wait returns;
+ * outputs have fgt_transform's meaning (zeros on failure). */
+typedef struct fgt_server fgt_server;
+typedef struct fgt_request {
+  int dim, nd;
+  double delta, eps;
+  int ns;
+  const double* sources; /* (ns, dim) */
+  const double* charge;  /* (ns, nd) */
+  int nt;
+  const double* targ;    /* (nt, dim), may be NULL */
+  int ifpgh, ifpghtarg;
+  double* pot;           /* (ns, nd) when ifpgh = 1 */
+  double* pottarg;       /* (nt, nd) when ifpghtarg = 1 */
+} fgt_request;
+typedef struct fgt_server_stats {
+  long long submitted, completed, failed;
+  long long points;            /* potentials evaluated by successful requests */
+  long long peak_bytes, budget_bytes;
+  double p50_s, p99_s, mean_s, max_s;  /* latency: submit -> result on the host */
+  double span_s;               /* first submit -> last completion */
+} fgt_server_stats;
+int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_server** out);
+int fgt_server_set_precision(fgt_server* server, int precision);
+int fgt_server_submit(fgt_server* server, const fgt_request* request, long long* id);
+/* blocks until request id completes; returns its status (and frees its id) */
+int fgt_server_wait(fgt_server* server, long long id, double* latency_s);
+int fgt_server_stats_get(fgt_server* server, fgt_server_stats* out);
+/* finishes the queued requests, then stops the workers */
+int fgt_server_destroy(fgt_server* server);
+
 /* ---- allocation-free large-delta transform ----------------------------------
  * No counterpart in the reference.  For callers that cannot let the library
  * allocate device memory -- codes that pass device arrays from their own
