@@ -419,6 +419,79 @@ def ours_arm(args, w, rank, world, local_rank):
     return 0
 
 
+def serving_arm(args):
+    """Serving stream: Poisson arrivals of transforms with mixed dimension, N,
+    delta and eps, submitted to the transform server at their arrival times;
+    latency is submit -> result on the host.  One base array of uniform
+    points (and charges) is sliced for every request, so no generation time
+    falls inside the arrival loop."""
+    import threading as th
+
+    import fgt2d_b200 as F
+
+    n_req = args.requests
+    rate = args.rate
+    rng = np.random.default_rng(1234 + 5)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    dims = rng.integers(2, 4, n_req)
+    ns = np.floor(10 ** rng.uniform(3, 6, n_req)).astype(int)
+    deltas = 10 ** rng.uniform(-6, -1, n_req)
+    epss = rng.choice([1e-3, 1e-6, 1e-9], n_req)
+    nmax = int(ns.max())
+    base = {2: rng.random((nmax, 2)), 3: rng.random((nmax, 3))}
+    chg = rng.random(nmax)
+    srv = F.Server(0, max_bytes=args.server_bytes, workers=args.workers, precision="auto")
+    # warm-up: one small request of each dimension (module load, first launches)
+    for d in (2, 3):
+        srv.wait(srv.submit(d, 1, 1e-3, 1e-6, base[d][:2000], chg[:2000]))
+    ids = [None] * n_req
+    lat = np.full(n_req, np.nan)
+    status = np.zeros(n_req, dtype=int)
+    done = th.Event()
+
+    def waiter():
+        for k in range(n_req):
+            while ids[k] is None:
+                time.sleep(1e-4)
+            try:
+                _, _, lat[k] = srv.wait(ids[k])
+            except F.FGTError as e:
+                status[k] = e.status
+        done.set()
+
+    wt = th.Thread(target=waiter, daemon=True)
+    wt.start()
+    t0 = time.perf_counter()
+    for k in range(n_req):
+        dt = arrivals[k] - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        d, n = int(dims[k]), int(ns[k])
+        ids[k] = srv.submit(d, 1, float(deltas[k]), float(epss[k]), base[d][:n], chg[:n])
+    done.wait()
+    span = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    ok = status == 0
+    small = ok & (ns <= 100_000)
+    q = lambda a, f: float(np.quantile(a, f) * 1e3) if a.size else None
+    pts = int(ns[ok].sum())
+    line = {
+        "metric": "serving p99 latency, requests with N <= 1e5", "value": q(lat[small], 0.99),
+        "unit": "ms", "higher_is_better": False, "n_gpus": 1, "impl": "ours",
+        "p50_ms_small": q(lat[small], 0.50), "p50_ms_all": q(lat[ok], 0.50), "p99_ms_all": q(lat[ok], 0.99),
+        "max_ms_all": q(lat[ok], 1.0), "requests": n_req, "completed": int(ok.sum()),
+        "failed": int((~ok).sum()), "points_per_s": pts / span, "span_s": span,
+        "arrival_rate_per_s": rate, "workers": args.workers, "peak_device_bytes": st["peak_bytes"],
+        "budget_device_bytes": st["budget_bytes"], "data": "synthetic (seeded numpy)",
+        "config": {"workload": "serving stream: Poisson arrivals, dim in {2,3}, N log-uniform [1e3,1e6] "
+                               "(sources = targets, uniform), charges U[0,1), delta log-uniform [1e-6,1e-1], "
+                               "eps in {1e-3,1e-6,1e-9}", "ifpgh": 1, "ifpghtarg": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,7 +501,13 @@ def main():
     ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--requests", type=int, default=4096, help="serving workload: number of requests")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: arrivals per second")
+    ap.add_argument("--workers", type=int, default=8, help="serving workload: server worker streams")
+    ap.add_argument("--server-bytes", type=int, default=0, help="serving workload: device budget (0: 80%% free)")
     args = ap.parse_args()
+    if args.workload == "serving":
+        return serving_arm(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

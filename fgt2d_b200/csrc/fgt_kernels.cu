@@ -118,6 +118,62 @@ __global__ void k_gather_pts(const double* __restrict__ x, const double* __restr
       for (int c = 0; c < nd; c++) qs[(long long)i * nd + c] = q[p * nd + c];
   }
 }
+// Diagonal translation tables from their 1D factors (merge_split_pw_matrices,
+// pw_translation_matrices): merge row (l nch + jc) for parents at level l,
+// entry e = prod_d (child jc on the + side along d ? conj(v) : v) with
+// v = ww[node_d(e)][nlevels - l]; mp->loc row s = (ox+1) + 3 (oy+1) [+ 9 (oz+1)],
+// entry prod_d (o_d = 0 ? 1 : o_d > 0 ? w1 : conj(w1)).  Products are formed
+// left to right without contraction, (ac - bd, ad + bc).
+__device__ __forceinline__ double2 cmul_rn(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__global__ void k_shift_tables(int dim, int npw, int nexp, int nlevels, int lstart, int nms,
+                               const double2* __restrict__ ww, const double2* __restrict__ w1,
+                               double2* __restrict__ wms, double2* __restrict__ wsh) {
+  const int nch = 1 << dim, n2 = npw / 2, ns3 = dim == 2 ? 9 : 27;
+  const long long nm = (long long)(nlevels + 1) * nch * nexp, total = nm + (long long)ns3 * nexp;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool merge = i < nm;
+    const long long r = merge ? i / nexp : (i - nm) / nexp;
+    const int e = (int)((merge ? i : i - nm) % nexp);
+    int node[3];
+    if (dim == 2) {
+      node[0] = e % n2;
+      node[1] = e / n2;
+    } else {
+      node[0] = e % npw;
+      node[1] = (e / npw) % npw;
+      node[2] = e / (npw * npw);
+    }
+    double2 f = make_double2(1.0, 0.0);
+    if (merge) {
+      const int l = (int)(r / nch), jc = (int)(r % nch);
+      if (l < lstart || l > nlevels - 1) {
+        wms[i] = make_double2(0.0, 0.0);
+        continue;
+      }
+      const int klev = nlevels - l;
+      for (int d = 0; d < dim; d++) {
+        double2 v = ww[node[d] * (nms + 1) + klev];
+        if ((jc >> d) & 1) v.y = -v.y;
+        f = cmul_rn(f, v);
+      }
+      wms[i] = f;
+    } else {
+      const int s = (int)r;
+      const int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
+      for (int d = 0; d < dim; d++) {
+        double2 v = o[d] == 0 ? make_double2(1.0, 0.0) : w1[node[d]];
+        if (o[d] < 0) v.y = -v.y;
+        f = cmul_rn(f, v);
+      }
+      wsh[i - nm] = f;
+    }
+  }
+}
+
 // *bad = 1 when any of x[0, n) is not finite
 __global__ void k_all_finite(const double* __restrict__ x, size_t n, int* __restrict__ bad) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -2008,8 +2064,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     D.scratch_ctas = D.scratch_per_cta ? D.sm_count * 2 : 0;
   }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
-  size_t total = bytes_of(H.box_centers) + bytes_of(H.h2x) + bytes_of(H.x2l) + al(H.wms.size() * 8) +
-                 al(H.wsh.size() * 8) + 2 * al((size_t)P.ns * 4) + 2 * al((size_t)P.nt * 4) +
+  // diagonal translation tables (formed on the device)
+  const size_t n_wms = P.all_direct ? 0 : (size_t)(P.nlevels + 1) * D.nch * P.nexp;
+  const size_t n_wsh = P.all_direct ? 0 : (size_t)(P.dim == 2 ? 9 : 27) * P.nexp;
+  size_t total = bytes_of(H.box_centers) + bytes_of(H.h2x) + bytes_of(H.x2l) + al(n_wms * 16) + al(n_wsh * 16) + al(H.ww.size() * 8) + al(H.w1.size() * 8) + 2 * al((size_t)P.ns * 4) + 2 * al((size_t)P.nt * 4) +
                  al((size_t)(std::max(P.ntermmax, 1) + 2) * 8) + al(32 * 8) +
                  bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(H.split) +
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
@@ -2038,11 +2096,22 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   CK(put(cur, D.h2x, H.h2x, s));
   CK(put(cur, D.x2l, H.x2l, s));
   {
-    std::vector<double2> w(H.wms.size() / 2), v(H.wsh.size() / 2);
-    memcpy(w.data(), H.wms.data(), H.wms.size() * 8);
-    memcpy(v.data(), H.wsh.data(), H.wsh.size() * 8);
-    CK(put(cur, D.wms, w, s));
-    CK(put(cur, D.wsh, v, s));
+    // translation tables formed on the device from their 1D factors
+    std::vector<double2> ww(H.ww.size() / 2), w1(H.w1.size() / 2);
+    memcpy(ww.data(), H.ww.data(), H.ww.size() * 8);
+    memcpy(w1.data(), H.w1.data(), H.w1.size() * 8);
+    double2 *d_ww = nullptr, *d_w1 = nullptr;
+    CK(put(cur, d_ww, ww, s));
+    CK(put(cur, d_w1, w1, s));
+    D.wms = reinterpret_cast<double2*>(cur); cur += al(n_wms * 16);
+    D.wsh = reinterpret_cast<double2*>(cur); cur += al(n_wsh * 16);
+    if (n_wms > 0) {
+      const long long tot = (long long)(n_wms + n_wsh);
+      const int blocks = (int)std::min<long long>((tot + 255) / 256, (long long)D.sm_count * 16);
+      k_shift_tables<<<blocks, 256, 0, s>>>(P.dim, P.npw, P.nexp, P.nlevels, std::max(P.nlevstart, 0), H.nms,
+                                            d_ww, d_w1, D.wms, D.wsh);
+      CK(cudaGetLastError());
+    }
     CK(cudaStreamSynchronize(s));
   }
   if (d_isrc) {

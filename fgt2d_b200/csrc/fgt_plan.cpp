@@ -52,67 +52,33 @@ static void build_tables(HostPlan& H) {
         H.x2l[(size_t)j * npw + k] = __builtin_powi(H.ts[k], j) / fac2[j];
       }
   }
-  // expansion index -> (kx, ky[, kz]) node indices, reference layouts:
-  // 2D pw(npw/2, npw): kx in the first half; 3D pw(npw, npw, npw/2).
-  size_t nexp = P.nexp;
-  auto node = [&](size_t e, int d) -> int {
-    if (D == 2) return d == 0 ? (int)(e % n2) : (int)(e / n2);
-    if (d == 0) return (int)(e % npw);
-    if (d == 1) return (int)((e / npw) % npw);
-    return (int)(e / ((size_t)npw * npw));
-  };
-  cplx I(0, 1);
-  // merge factors: child slot j merged into its parent, the parent-child
+  // 1D factors of the diagonal translation tables; the tables themselves
+  // (nexp entries per row) are formed on the device (device_plan_create).
+  // Merge factors: child slot j merged into its parent, the parent-child
   // offset at level l being boxsize(l+1)/2; ww(k) = exp(i t xmin2)^(2^(k-1))
   // as in merge_split_pw_matrices (g2drouts.f:2326-2332).
+  cplx I(0, 1);
   int nms = std::max(P.nlevels - std::max(P.npwlevel, 0), 1);
+  H.nms = nms;
   double xmin2 = t.boxsize[P.nlevels] / std::sqrt(P.delta) / 2;
-  std::vector<cplx> ww((size_t)npw * (nms + 1));
+  H.ww.assign((size_t)npw * (nms + 1) * 2, 0.0);
   for (int j = 0; j < npw; j++) {
     cplx z = std::exp(I * H.ts[j] * xmin2);
     for (int k = 1; k <= nms; k++) {
-      ww[(size_t)j * (nms + 1) + k] = z;
+      H.ww[2 * ((size_t)j * (nms + 1) + k)] = z.real();
+      H.ww[2 * ((size_t)j * (nms + 1) + k) + 1] = z.imag();
       z = z * z;
     }
   }
-  // row (l * nch + j) for parents at level l: klev = nlevels - l
-  int nrow = (P.nlevels + 1) * nch;
-  H.wms.assign((size_t)nrow * nexp * 2, 0.0);
-  for (int l = std::max(P.nlevstart, 0); l <= P.nlevels - 1; l++) {
-    int klev = P.nlevels - l;
-    for (int jc = 0; jc < nch; jc++) {
-      double* W = H.wms.data() + ((size_t)l * nch + jc) * nexp * 2;
-      for (size_t e = 0; e < nexp; e++) {
-        cplx f = 1.0;
-        for (int d = 0; d < D; d++) {
-          // parent - child along d is negative when the child sits on the + side
-          cplx v = ww[(size_t)node(e, d) * (nms + 1) + klev];
-          f *= ((jc >> d) & 1) ? std::conj(v) : v;
-        }
-        W[2 * e] = f.real();
-        W[2 * e + 1] = f.imag();
-      }
-    }
-  }
-  // mp->loc factors, s = (jx+1) + 3 (jy+1) [+ 9 (jz+1)], xmin = boxsize(cut)
-  int ns3 = D == 2 ? 9 : 27;
-  H.wsh.assign((size_t)ns3 * nexp * 2, 0.0);
+  // mp->loc factors (pw_translation_matrices): exp(i t xmin), xmin = boxsize(cut)
   double xmin = (P.npwlevel >= 0 ? t.boxsize[P.npwlevel] : 0.0) / std::sqrt(P.delta);
-  std::vector<cplx> w1(npw);
-  for (int j = 0; j < npw; j++) w1[j] = std::exp(I * H.ts[j] * xmin);
-  for (int s = 0; s < ns3; s++) {
-    int o[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
-    double* W = H.wsh.data() + (size_t)s * nexp * 2;
-    for (size_t e = 0; e < nexp; e++) {
-      cplx f = 1.0;
-      for (int d = 0; d < D; d++) {
-        cplx v = w1[node(e, d)];
-        f *= o[d] == 0 ? cplx(1.0) : (o[d] > 0 ? v : std::conj(v));
-      }
-      W[2 * e] = f.real();
-      W[2 * e + 1] = f.imag();
-    }
+  H.w1.assign((size_t)npw * 2, 0.0);
+  for (int j = 0; j < npw; j++) {
+    cplx v = std::exp(I * H.ts[j] * xmin);
+    H.w1[2 * j] = v.real();
+    H.w1[2 * j + 1] = v.imag();
   }
+  (void)nch;
 }
 
 // Flattens the tree into the stage task arrays.

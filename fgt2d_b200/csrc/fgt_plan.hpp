@@ -67,8 +67,11 @@ struct HostPlan {
   std::vector<double> ts, ws;     // reference node order for the dimension
   std::vector<double> h2x;        // [j * npw + k] = ws_k (-ts_k)^j / sqrt(j!)
   std::vector<double> x2l;        // [j * npw + k] = ts_k^j / j!
-  std::vector<double> wms;        // merge factors [(lev*nch + j) * nexp + e] (re,im)
-  std::vector<double> wsh;        // mp->loc factors [s * nexp + e] (re,im)
+  // 1D factors of the diagonal translation tables (re, im): ww[j][k] =
+  // exp(i t_j xmin2)^(2^(k-1)) for the merge / split rows of nms levels,
+  // w1[j] = exp(i t_j xmin) for mp->loc; the device forms the nexp-long rows
+  std::vector<double> ww, w1;
+  int nms = 1;
   int nmp = 0, nloc = 0;
   std::vector<int> mp_slot, loc_slot;  // per box, -1 when absent
   std::vector<double> box_centers;     // dim per box
