@@ -86,6 +86,7 @@ struct DevicePlan {
   int* fcbeg = nullptr;      // per Hermite form task, first chunk (size n+1)
   double* hbuf = nullptr;    // partial Hermite blocks
   bool form3_smem = false, eval3_smem = false;
+  bool eval3_split = false;  // 3D Taylor eval in two kernels (conversion, Horner)
   size_t form3_shA = 0, form3_shB = 0, eval3_sh = 0;
   int form3_sub = 64;
   // per-CTA scratch of the 3D separable transforms (fallback path)

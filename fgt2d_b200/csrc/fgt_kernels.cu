@@ -1098,6 +1098,243 @@ __global__ void __launch_bounds__(128) k_eval2d_horner_any(KP k, const HornerTas
   }
 }
 
+// ------------------------------------------------------------ (c) eval, 3D Taylor in two kernels
+// k_pw2taylor3d: one CTA per evaluation leaf converts the leaf's plane-wave
+// expansion L[(m1 npw + m2) npw + m3] (m1 over the stored half) into the real
+// Taylor block (g3dpw2local_real_vec, g3drouts.f:1774-1938)
+//   S1[m2][a]    = i^a  sum_m3 x2l[a][m3] L[m1][m2][m3]        (pass 1, per m1)
+//   U2[a][b][m1] = i^b  sum_m2 x2l[b][m2] S1[m2][a]            (pass 2, per m1)
+//   lo[c][b][a]  = 2 Re( i^c sum_{m1 < n2} x2l[c][m1] U2[a][b][m1] )   (pass 3)
+// as FP64 MMA products.  Passes 1 and 2 run slice by slice over m1 (the
+// warps take the slices in turn), so the only large intermediate is U2,
+// kept as its real and imaginary parts: pass 3 is two real products, even c
+// against Re U2 and odd c against Im U2 (2 Re(i^c z) keeps z.x or z.y).
+// Pass 1 reads L straight from the expansion pool: a fragment is four runs of
+// 64 contiguous bytes.  The real and imaginary parts of a pass-1 or pass-2
+// result sit in the lanes r and r xor 1 of the accumulator layout (rows
+// interleave re / im), so one exchange pairs them for the rotation.
+struct Conv3Dims {
+  int Pn, E, n2, npw;
+  int N1, K1, M1;       // pass 1: N1 = a (padded), K1 = m3, M1 = (m2, re/im)
+  int M2, K2;           // pass 2: M2 = (a, re/im), K2 = m2, N = N1 (b)
+  int M3, K3, N3;       // pass 3: M3 = (a, b) compact, K3 = m1, N3 = c of one parity
+  int ldT, ldA2, ldU, ldB3;
+  int tab, warp, shared;  // doubles: CTA tables, per-warp area, shared U2
+  __host__ __device__ Conv3Dims(int P, int npw_) {
+    Pn = P;
+    npw = npw_;
+    n2 = npw / 2;
+    E = (Pn + 1) & ~1;
+    N1 = (Pn + 7) & ~7;
+    K1 = (npw + 3) & ~3;
+    M1 = (2 * npw + 7) & ~7;
+    M2 = 2 * N1;
+    K2 = K1;
+    M3 = (Pn * Pn + 7) & ~7;
+    K3 = (n2 + 3) & ~3;
+    N3 = (((Pn + 1) / 2) + 7) & ~7;
+    ldT = mma_ldb(N1);
+    ldA2 = mma_lda(K2);
+    ldU = mma_lda(K3);
+    ldB3 = mma_ldb(N3);
+    tab = K1 * ldT + 2 * K3 * ldB3;
+    warp = M2 * ldA2;
+    shared = 2 * M3 * ldU;
+  }
+};
+
+size_t conv3_smem_bytes(int Pn, int npw, int nw) {
+  const Conv3Dims Z(Pn, npw);
+  return ((size_t)Z.tab + Z.shared + (size_t)nw * Z.warp) * 8;
+}
+
+// Tables of k_pw2taylor3d for order P: XT[m][n] = x2l[n][m] (m < npw, n < P),
+// B3e[m1][i] = x2l[2i][m1], B3o[m1][i] = x2l[2i+1][m1] (m1 < n2), zero padded.
+void build_conv3_table(const HostPlan& H, int Pn, std::vector<double>& out) {
+  const int npw = H.P.npw, n2 = npw / 2;
+  const Conv3Dims Z(Pn, npw);
+  const size_t base = out.size();
+  out.resize(base + Z.tab, 0.0);
+  double* XT = out.data() + base;
+  double* B3e = XT + Z.K1 * Z.ldT;
+  double* B3o = B3e + Z.K3 * Z.ldB3;
+  for (int m = 0; m < npw; m++)
+    for (int n = 0; n < Pn; n++) XT[m * Z.ldT + n] = H.x2l[(size_t)n * npw + m];
+  for (int m1 = 0; m1 < n2; m1++)
+    for (int c = 0; c < Pn; c++) {
+      double* B = (c & 1) ? B3o : B3e;
+      B[m1 * Z.ldB3 + c / 2] = H.x2l[(size_t)c * npw + m1];
+    }
+}
+
+template <int KS1>  // pass 1 depth in steps of 4: KS1 = ceil(npw / 4)
+__global__ void __launch_bounds__(256) k_pw2taylor3d(KP k, const ConvTask* __restrict__ tasks,
+                                                     double* __restrict__ lo_all,
+                                                     const double* __restrict__ tab) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int r = lane >> 2, c = lane & 3;
+  const ConvTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const Conv3Dims Z(T.p + 1, k.npw);
+  const int Pn = Z.Pn, E = Z.E, npw = Z.npw, n2 = Z.n2;
+  extern __shared__ double s3[];
+  double* XT = s3;                                 // [K1][ldT]
+  double* B3e = XT + Z.K1 * Z.ldT;                 // [K3][ldB3]
+  double* B3o = B3e + Z.K3 * Z.ldB3;
+  double* Ure = s3 + Z.tab;                        // [M3][ldU]
+  double* Uim = Ure + Z.M3 * Z.ldU;
+  double* A2 = Uim + Z.M3 * Z.ldU + warp * Z.warp; // [M2][ldA2]
+  for (int e = threadIdx.x; e < Z.tab; e += blockDim.x) s3[e] = tab[e];
+  for (int e = threadIdx.x; e < 2 * Z.M3 * Z.ldU; e += blockDim.x) Ure[e] = 0.0;
+  __syncthreads();
+  const double* Ld = reinterpret_cast<const double*>(k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp);
+  for (int m1 = warp; m1 < n2; m1 += nw) {
+    // pass 1: rows (m2, re/im) of the slice, columns a
+    for (int mt = 0; mt < Z.M1 / 8; mt++) {
+      const int row = 8 * mt + r, m2 = row >> 1, comp = row & 1;
+      const bool rok = m2 < npw;
+      const double* ap = Ld + ((size_t)(m1 * npw + m2) * npw) * 2 + comp;
+      double av[KS1];
+#pragma unroll
+      for (int ks = 0; ks < KS1; ks++) {
+        const int m3 = 4 * ks + c;
+        av[ks] = (rok && m3 < npw) ? __ldg(ap + 2 * m3) : 0.0;
+      }
+      for (int nt = 0; nt < Z.N1 / 8; nt++) {
+        const double* bp = XT + c * Z.ldT + 8 * nt + r;
+        double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS1; ks++) {
+          if (ks & 1) dmma_884(e0, e1, av[ks], bp[4 * ks * Z.ldT]);
+          else dmma_884(d0, d1, av[ks], bp[4 * ks * Z.ldT]);
+        }
+        d0 += e0;
+        d1 += e1;
+        // lane r holds comp (r & 1) of S1[m2][a0], S1[m2][a0 + 1]; r xor 1 the other
+        const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
+        const int a0 = 8 * nt + 2 * c;
+        const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), a0);
+        const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), a0 + 1);
+        if (m2 < Z.K2) {
+          if (comp == 0) {
+            A2[(2 * a0) * Z.ldA2 + m2] = z0.x;
+            A2[(2 * a0 + 1) * Z.ldA2 + m2] = z0.y;
+          } else {
+            A2[(2 * a0 + 2) * Z.ldA2 + m2] = z1.x;
+            A2[(2 * a0 + 3) * Z.ldA2 + m2] = z1.y;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // pass 2: rows (a, re/im), columns b; U2[a][b][m1] into Ure / Uim
+    for (int mt = 0; mt < Z.M2 / 8; mt++) {
+      const double* ap = A2 + (8 * mt + r) * Z.ldA2 + c;
+      for (int nt = 0; nt < Z.N1 / 8; nt++) {
+        const double* bp = XT + c * Z.ldT + 8 * nt + r;
+        double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+        for (int ks = 0; ks < Z.K2 / 4; ks += 2) {
+          dmma_884(d0, d1, ap[4 * ks], bp[4 * ks * Z.ldT]);
+          if (ks + 1 < Z.K2 / 4) dmma_884(e0, e1, ap[4 * ks + 4], bp[(4 * ks + 4) * Z.ldT]);
+        }
+        d0 += e0;
+        d1 += e1;
+        const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
+        const int row = 8 * mt + r, a = row >> 1, comp = row & 1, b0 = 8 * nt + 2 * c;
+        const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), b0);
+        const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), b0 + 1);
+        if (a < Pn) {
+          if (comp == 0 && b0 < Pn) {
+            Ure[(a * Pn + b0) * Z.ldU + m1] = z0.x;
+            Uim[(a * Pn + b0) * Z.ldU + m1] = z0.y;
+          }
+          if (comp == 1 && b0 + 1 < Pn) {
+            Ure[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.x;
+            Uim[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.y;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // pass 3: lo[c][b][a] = 2 {x, -y, -x, y}[c mod 4] of sum_m1 x2l[c][m1] U2[a][b][m1]
+  double* out = lo_all + T.off + (size_t)ind * Pn * Pn * E;
+  for (int mt = warp; mt < Z.M3 / 8; mt += nw) {
+    const double* ae = Ure + (8 * mt + r) * Z.ldU + c;
+    const double* ao = Uim + (8 * mt + r) * Z.ldU + c;
+    for (int nt = 0; nt < Z.N3 / 8; nt++) {
+      const double* be = B3e + c * Z.ldB3 + 8 * nt + r;
+      const double* bo = B3o + c * Z.ldB3 + 8 * nt + r;
+      double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+      for (int ks = 0; ks < Z.K3 / 4; ks++) {
+        dmma_884(e0, e1, ae[4 * ks], be[4 * ks * Z.ldB3]);
+        dmma_884(o0, o1, ao[4 * ks], bo[4 * ks * Z.ldB3]);
+      }
+      const int q = 8 * mt + r;
+      if (q >= Pn * Pn) continue;
+      const int a = q / Pn, b = q - a * Pn;
+      const double ev[2] = {e0, e1}, od[2] = {o0, o1};
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int ce = 2 * (8 * nt + 2 * c + i), co = ce + 1;
+        if (ce < Pn) out[((size_t)ce * Pn + b) * E + a] = ((ce & 3) == 2 ? -2.0 : 2.0) * ev[i];
+        if (co < Pn) out[((size_t)co * Pn + b) * E + a] = ((co & 3) == 1 ? -2.0 : 2.0) * od[i];
+      }
+    }
+  }
+  if (E > Pn)  // the padding column of every row
+    for (int e = threadIdx.x; e < Pn * Pn; e += blockDim.x) out[(size_t)e * E + Pn] = 0.0;
+}
+
+// k_eval3d_horner: one CTA (128 threads) per chunk of <= 256 points of an
+// evaluation leaf; the leaf's Taylor block lo[c][b][a] (rows of E = 2 NP2)
+// is staged in shared memory and each thread evaluates two points by Horner
+// in x along each row, then in y, then in z (g3dlevalp_vec,
+// g3drouts.f:1045-1107), plain FP64 FMAs at the exact order.
+template <int NP2>
+__global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* __restrict__ tasks,
+                                                       const double* __restrict__ lo_all) {
+  const HornerTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y, Pn = T.p + 1;
+  extern __shared__ double2 lo3[];  // [Pn][Pn][NP2]
+  const double2* src = reinterpret_cast<const double2*>(lo_all + T.off + (size_t)ind * Pn * Pn * 2 * NP2);
+  for (int e = threadIdx.x; e < Pn * Pn * NP2; e += blockDim.x) lo3[e] = src[e];
+  __syncthreads();
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
+  const int ta = threadIdx.x, tb = threadIdx.x + 128;
+  if (ta >= T.n) return;
+  const bool two = tb < T.n;
+  const int pa = T.i0 + ta, pb = T.i0 + (two ? tb : ta);
+  const double x0 = (pts[3 * pa] - cx) * k.dsq, y0 = (pts[3 * pa + 1] - cy) * k.dsq, z0 = (pts[3 * pa + 2] - cz) * k.dsq;
+  const double x1 = (pts[3 * pb] - cx) * k.dsq, y1 = (pts[3 * pb + 1] - cy) * k.dsq, z1 = (pts[3 * pb + 2] - cz) * k.dsq;
+  double r0 = 0.0, r1 = 0.0;
+  for (int cc = Pn - 1; cc >= 0; cc--) {
+    double q0 = 0.0, q1 = 0.0;
+    for (int b = Pn - 1; b >= 0; b--) {
+      const double2* rw = lo3 + (cc * Pn + b) * NP2;
+      const double2 ct = rw[NP2 - 1];
+      double s0 = fma(ct.y, x0, ct.x), s1 = fma(ct.y, x1, ct.x);
+#pragma unroll
+      for (int m = NP2 - 2; m >= 0; m--) {
+        const double2 cf = rw[m];
+        s0 = fma(s0, x0, cf.y);
+        s1 = fma(s1, x1, cf.y);
+        s0 = fma(s0, x0, cf.x);
+        s1 = fma(s1, x1, cf.x);
+      }
+      q0 = fma(q0, y0, s0);
+      q1 = fma(q1, y1, s1);
+    }
+    r0 = fma(r0, z0, q0);
+    r1 = fma(r1, z1, q1);
+  }
+  out[(size_t)pa * k.nd + ind] += r0;
+  if (two) out[(size_t)pb * k.nd + ind] += r1;
+}
+
 // ------------------------------------------------------------ (c) eval, 3D Taylor in shared memory
 // One CTA per chunk of an evaluation leaf: plane wave -> Taylor
 // (g3dpw2local_real_vec, g3drouts.f:1774-1938) with x and y passes over the
@@ -1936,7 +2173,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   std::vector<ConvTask> conv;
   std::vector<HornerTask> horner;
   size_t lo_doubles = 0;
-  if (P.dim == 2 && !P.all_direct) {
+  // 3D: the same two kernels where the order's shared-memory needs fit
+  D.eval3_split = P.dim == 3 && !P.all_direct && D.eval_taylor_n > 0 &&
+                  conv3_smem_bytes(D.eval_pmax + 1, P.npw, 1) <= 227 * 1024 && (P.npw + 3) / 4 <= CONV_MAXKS;
+  if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     for (int t = 0; t < D.eval_taylor_n; t++) {
       const EvalTask& e = ev[t];
@@ -1944,7 +2184,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       if (slot_off[e.slot] < 0) {
         slot_off[e.slot] = (long long)lo_doubles;
         conv.push_back({e.slot, e.p, (long long)lo_doubles});
-        lo_doubles += (size_t)(P.nd * Pn * E);
+        lo_doubles += (size_t)(P.nd * Pn * E * (P.dim == 3 ? Pn : 1));
       }
       for (int c = 0; c < e.n; c += 256)
         horner.push_back({e.box, e.set, e.i0 + c, std::min(256, e.n - c), e.p, slot_off[e.slot]});
@@ -1976,6 +2216,11 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       build_conv_table(H, G.p + 1, tables);
     }
   }
+  if (D.eval3_split)
+    for (OrderGroup& G : D.conv_groups) {
+      G.tab = (long long)tables.size();
+      build_conv3_table(H, G.p + 1, tables);
+    }
   // merge groups: consecutive tasks with the same destination
   std::vector<MergeGroup> groups;
   D.merge_beg.assign(P.nlevels + 1, 0);
@@ -2044,7 +2289,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       const size_t Pn = D.eval_pmax + 1;
       size_t szA = std::max(2 * Pn * P.npw * n2, Pn * Pn * Pn);
       D.eval3_sh = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
-      D.eval3_smem = D.eval3_sh <= lim;
+      D.eval3_smem = D.eval3_sh <= lim || D.eval3_split;  // the split path needs no scratch
     }
   }
   // scratch for the 3D separable transforms (fallback path)
@@ -2404,7 +2649,47 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         launches++;
       }
     }
-    if (P.dim == 3 && D.eval_taylor_n > 0 && D.eval3_smem) {
+    if (P.dim == 3 && D.eval3_split) {
+      for (const OrderGroup& G : D.conv_groups) {
+        const int Pn = G.p + 1, nt = G.end - G.beg;
+        int nw = 8;
+        while (nw > 1 && conv3_smem_bytes(Pn, P.npw, nw) > 200 * 1024) nw >>= 1;
+        const size_t sh = conv3_smem_bytes(Pn, P.npw, nw);
+        const dim3 cg(nt, nd);
+        switch ((P.npw + 3) / 4) {
+#define CONV3_CASE(N)                                                                             \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_pw2taylor3d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_pw2taylor3d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, D.lo, D.tables + G.tab);         \
+    break;
+          CONV3_CASE(1) CONV3_CASE(2) CONV3_CASE(3) CONV3_CASE(4) CONV3_CASE(5) CONV3_CASE(6)
+          CONV3_CASE(7) CONV3_CASE(8) CONV3_CASE(9) CONV3_CASE(10) CONV3_CASE(11) CONV3_CASE(12)
+#undef CONV3_CASE
+          default: return cudaErrorNotSupported;
+        }
+        launches++;
+      }
+      for (const OrderGroup& G : D.horner_groups) {
+        const int Pn = G.p + 1, np2 = (Pn + 1) / 2;
+        const dim3 g(G.end - G.beg, nd);
+        const HornerTask* tk = D.horner + G.beg;
+        const size_t sh = (size_t)Pn * Pn * np2 * 16;
+        if (sh > 227 * 1024) return cudaErrorNotSupported;
+        switch (np2) {
+#define HORNER3_CASE(N)                                                                           \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_eval3d_horner<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_eval3d_horner<N><<<g, 128, sh, st>>>(k, tk, D.lo);                                          \
+    break;
+          HORNER3_CASE(1) HORNER3_CASE(2) HORNER3_CASE(3) HORNER3_CASE(4) HORNER3_CASE(5)
+          HORNER3_CASE(6) HORNER3_CASE(7) HORNER3_CASE(8) HORNER3_CASE(9) HORNER3_CASE(10)
+          HORNER3_CASE(11) HORNER3_CASE(12) HORNER3_CASE(13) HORNER3_CASE(14) HORNER3_CASE(15)
+#undef HORNER3_CASE
+          default: return cudaErrorNotSupported;
+        }
+        launches++;
+      }
+    } else if (P.dim == 3 && D.eval_taylor_n > 0 && D.eval3_smem) {
       CK(cudaFuncSetAttribute(k_eval3d_taylor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
       k_eval3d_taylor_smem<<<dim3(D.eval_taylor_n, nd), 512, D.eval3_sh, st>>>(k, D.eval);
       launches++;
