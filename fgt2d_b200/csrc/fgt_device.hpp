@@ -89,6 +89,7 @@ struct DevicePlan {
   bool eval3_split = false;  // 3D Taylor eval in two kernels (conversion, Horner)
   size_t form3_shA = 0, form3_shB = 0, eval3_sh = 0;
   int form3_sub = 64;
+  std::vector<OrderGroup> fchunk_groups;  // chunk ranges of equal order
   // per-CTA scratch of the 3D separable transforms (fallback path)
   double2* scratch = nullptr;
   size_t scratch_per_cta = 0;  // in double2

@@ -723,6 +723,96 @@ __global__ void __launch_bounds__(256) k_form3d_acc(KP k, const FormTask* __rest
   for (int e = threadIdx.x; e < P3; e += blockDim.x) out[e] = H[e];
 }
 
+// The chunk's Hermite block on the FP64 tensor cores: H[j][(k, l)] =
+// sum_t x_t^j (q_t y_t^k z_t^l) (with the 1/sqrt(j!) factors, g3dformhc_vec,
+// g3drouts.f:109-192) is one product with M = j (MT tiles of 8), N = the
+// P^2 pairs (k, l) and K = the sources, four per mma.m8n8k4 step.  Sources
+// are staged 64 at a time as power rows in shared memory (row stride 68: the
+// A fragments are conflict-free); a B element is y^k q z^l, one multiply of
+// two staged powers, with (k, l) of the lane's column fixed per tile.  The
+// eight warps split the N tiles (up to four each per pass over the sources).
+// The partial block goes to the chunk's slot of the Hermite buffer, laid out
+// H[j + P (k + P l)] as k_form3d_h2pw reads it.
+template <int MT>
+__global__ void __launch_bounds__(256) k_form3d_mma(KP k, const FormTask* __restrict__ tasks,
+                                                    const FormChunk* __restrict__ chunks,
+                                                    double* __restrict__ hbuf, const double* __restrict__ isq) {
+  constexpr int SB = 64, SW = 68, NTW = 4;
+  const FormChunk C = chunks[blockIdx.x];
+  const FormTask T = tasks[C.task];
+  const int ind = blockIdx.y;
+  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn, ntiles = (P2 + 7) / 8;
+  extern __shared__ double sm[];
+  double* X = sm;                // [8 MT][SW]
+  double* Y = X + 8 * MT * SW;   // [Pn][SW]
+  double* Z = Y + Pn * SW;       // [Pn][SW], times q
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
+  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
+  for (int e = threadIdx.x; e < (8 * MT - Pn) * SW; e += blockDim.x) X[Pn * SW + e] = 0.0;
+  double* out = hbuf + ((size_t)C.hoff * k.nd + (size_t)ind * P3);
+  for (int base = 0; base < ntiles; base += 8 * NTW) {
+    double acc[MT][NTW][2];
+    int ko[NTW], lo_[NTW];
+#pragma unroll
+    for (int i = 0; i < NTW; i++) {
+      const int n = 8 * (base + warp + 8 * i) + r;
+      ko[i] = n < P2 ? (n % Pn) * SW : -1;
+      lo_[i] = n < P2 ? (n / Pn) * SW : 0;
+#pragma unroll
+      for (int mt = 0; mt < MT; mt++) acc[mt][i][0] = acc[mt][i][1] = 0.0;
+    }
+    for (int c0 = 0; c0 < C.n; c0 += SB) {
+      const int m = min(SB, C.n - c0);
+      __syncthreads();
+      for (int job = threadIdx.x; job < 3 * SB; job += blockDim.x) {
+        const int t = job / 3, d = job - 3 * t;
+        double v = 0.0, w = 0.0;
+        if (t < m) {
+          const int i = C.s0 + c0 + t;
+          v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
+          w = d == 2 ? k.chg[(size_t)i * k.nd + ind] : 1.0;
+        }
+        double* row = (d == 0 ? X : d == 1 ? Y : Z) + t;
+        row[0] = w;
+        for (int j = 1; j < Pn; j++) {
+          w = w * v * isq[j];
+          row[j * SW] = w;
+        }
+      }
+      __syncthreads();
+      const int nst = (m + 3) >> 2;
+      for (int st = 0; st < nst; st++) {
+        const int s = 4 * st + c;
+        double a[MT];
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) a[mt] = X[(8 * mt + r) * SW + s];
+#pragma unroll
+        for (int i = 0; i < NTW; i++) {
+          if (base + warp + 8 * i < ntiles) {
+            const double b = ko[i] >= 0 ? Y[ko[i] + s] * Z[lo_[i] + s] : 0.0;
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++) dmma_884(acc[mt][i][0], acc[mt][i][1], a[mt], b);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NTW; i++) {
+      const int nt = base + warp + 8 * i;
+      if (nt >= ntiles) continue;
+#pragma unroll
+      for (int mt = 0; mt < MT; mt++) {
+        const int j = 8 * mt + r;
+#pragma unroll
+        for (int ii = 0; ii < 2; ii++) {
+          const int n = 8 * nt + 2 * c + ii;
+          if (j < Pn && n < P2) out[j + Pn * n] = acc[mt][i][ii];
+        }
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __restrict__ tasks,
                                                      const int* __restrict__ cbeg,
                                                      const FormChunk* __restrict__ chunks,
@@ -2283,6 +2373,14 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
         fcbeg.push_back((int)fchunks.size());
         hbuf_doubles = (size_t)hoff * P.nd;
         D.nfchunks = (int)fchunks.size();
+        // chunk ranges of equal order (the tasks are sorted by order)
+        for (size_t t = 0; t < fchunks.size();) {
+          size_t u = t;
+          const int pt = form[fchunks[t].task].p;
+          while (u < fchunks.size() && form[fchunks[u].task].p == pt) u++;
+          D.fchunk_groups.push_back({pt, (int)t, (int)u});
+          t = u;
+        }
       }
     }
     if (D.eval_taylor_n > 0) {
@@ -2542,17 +2640,26 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
       }
     }
     if (P.dim == 3 && D.form_hermite_n > 0 && D.form3_smem) {
-      const int Pn = D.form_pmax + 1;
-      if (Pn <= 16) {
-        CK(cudaFuncSetAttribute(k_form3d_acc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shA));
-        k_form3d_acc<16><<<dim3(D.nfchunks, nd), 256, D.form3_shA, st>>>(k, D.form, D.fchunks, D.hbuf, D.isq, D.form3_sub);
-      } else {
-        CK(cudaFuncSetAttribute(k_form3d_acc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shA));
-        k_form3d_acc<32><<<dim3(D.nfchunks, nd), 256, D.form3_shA, st>>>(k, D.form, D.fchunks, D.hbuf, D.isq, D.form3_sub);
+      for (const OrderGroup& G : D.fchunk_groups) {
+        const int Pn = G.p + 1, mt = (Pn + 7) / 8;
+        const size_t sh = ((size_t)8 * mt + 2 * Pn) * 68 * 8;
+        const dim3 fg(G.end - G.beg, nd);
+        const FormChunk* ch = D.fchunks + G.beg;
+        switch (mt) {
+#define FORM3_CASE(N)                                                                             \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_form3d_mma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_form3d_mma<N><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                           \
+    break;
+          FORM3_CASE(1) FORM3_CASE(2) FORM3_CASE(3) FORM3_CASE(4)
+#undef FORM3_CASE
+          default: return cudaErrorNotSupported;
+        }
+        launches++;
       }
       CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shB));
       k_form3d_h2pw<<<dim3(D.form_hermite_n, nd), 512, D.form3_shB, st>>>(k, D.form, D.fcbeg, D.fchunks, D.hbuf);
-      launches += 2;
+      launches++;
     } else if (P.dim == 3 && D.form_hermite_n > 0) {
       int Pn = D.form_pmax + 1;
       size_t sh = ((size_t)Pn * Pn * Pn + 3 * FORM_CH * Pn) * 8;
