@@ -87,8 +87,7 @@ struct DevicePlan {
   double* hbuf = nullptr;    // partial Hermite blocks
   bool form3_smem = false, eval3_smem = false;
   bool eval3_split = false;  // 3D Taylor eval in two kernels (conversion, Horner)
-  size_t form3_shA = 0, form3_shB = 0, eval3_sh = 0;
-  int form3_sub = 64;
+  size_t form3_shB = 0, eval3_sh = 0;
   std::vector<OrderGroup> fchunk_groups;  // chunk ranges of equal order
   // per-CTA scratch of the 3D separable transforms (fallback path)
   double2* scratch = nullptr;
@@ -98,7 +97,7 @@ struct DevicePlan {
   int form_hermite_n = 0, form_pw_n = 0;
   int eval_taylor_n = 0, eval_pw_n = 0;
   int form_pmax = 0, eval_pmax = 0;  // largest order among Hermite form / Taylor eval tasks
-  std::vector<OrderGroup> form_groups, eval_groups;
+  std::vector<OrderGroup> form_groups;
   // 2D Taylor evaluation (conversion per leaf, then Horner per point chunk)
   long long* form_hoff = nullptr;  // 2D MMA form: per form task, offset of its Hermite block in hbuf
   ConvTask* conv = nullptr;

@@ -669,60 +669,6 @@ __global__ void __launch_bounds__(128) k_h2pw2d(KP k, const FormTask* __restrict
 // stored half, then y and x passes over the positive half using the mirror
 // symmetry A(j, mirror k) = (-1)^j A(j, k) of the ascending node set.
 
-template <int MAXP>
-__global__ void __launch_bounds__(256) k_form3d_acc(KP k, const FormTask* __restrict__ tasks,
-                                                    const FormChunk* __restrict__ chunks,
-                                                    double* __restrict__ hbuf, const double* __restrict__ isq,
-                                                    int sub) {
-  const FormChunk C = chunks[blockIdx.x];
-  const FormTask T = tasks[C.task];
-  const int ind = blockIdx.y;
-  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
-  extern __shared__ double sm[];
-  double* H = sm;
-  double* X = H + P3;
-  double* Y = X + sub * Pn;
-  double* Z = Y + sub * Pn;
-  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
-  for (int e = threadIdx.x; e < P3; e += blockDim.x) H[e] = 0.0;
-  for (int c0 = 0; c0 < C.n; c0 += sub) {
-    const int m = min(sub, C.n - c0);
-    __syncthreads();
-    for (int r = threadIdx.x; r < 3 * m; r += blockDim.x) {
-      const int t = r / 3, d = r - 3 * t;
-      const int i = C.s0 + c0 + t;
-      const double v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
-      double w = d == 2 ? k.chg[(size_t)i * k.nd + ind] : 1.0;
-      double* row = (d == 0 ? X : d == 1 ? Y : Z) + t * Pn;
-      row[0] = w;
-      for (int j = 1; j < Pn; j++) {
-        w = w * v * isq[j];
-        row[j] = w;
-      }
-    }
-    __syncthreads();
-    for (int pr = threadIdx.x; pr < P2; pr += blockDim.x) {
-      const int j = pr % Pn, kk = pr / Pn;
-      double acc[MAXP];
-#pragma unroll
-      for (int l = 0; l < MAXP; l++) acc[l] = l < Pn ? H[pr + P2 * l] : 0.0;
-      for (int t = 0; t < m; t++) {
-        const double a = X[t * Pn + j] * Y[t * Pn + kk];
-        const double* zr = Z + t * Pn;
-#pragma unroll
-        for (int l = 0; l < MAXP; l++)
-          if (l < Pn) acc[l] = fma(a, zr[l], acc[l]);
-      }
-#pragma unroll
-      for (int l = 0; l < MAXP; l++)
-        if (l < Pn) H[pr + P2 * l] = acc[l];
-    }
-  }
-  __syncthreads();
-  double* out = hbuf + ((size_t)C.hoff * k.nd + (size_t)ind * P3);
-  for (int e = threadIdx.x; e < P3; e += blockDim.x) out[e] = H[e];
-}
-
 // The chunk's Hermite block on the FP64 tensor cores: H[j][(k, l)] =
 // sum_t x_t^j (q_t y_t^k z_t^l) (with the 1/sqrt(j!) factors, g3dformhc_vec,
 // g3drouts.f:109-192) is one product with M = j (MT tiles of 8), N = the
@@ -872,116 +818,6 @@ __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __res
     const size_t base = (size_t)npw * (k2 + (size_t)npw * k1);
     out[base + kp] = make_double2(ev.x + od.x, ev.y + od.y);
     out[base + km] = make_double2(ev.x - od.x, ev.y - od.y);
-  }
-}
-
-// ------------------------------------------------------------ (c) eval, 2D Taylor on FP64 MMA
-// One CTA (4 warps) per chunk of an evaluation leaf.  The leaf's plane-wave
-// expansion is staged in shared memory and converted to the Taylor block
-// lo[k2 + LD k1] (g2dpw2local_real_vec); then for eight points per warp step
-//     E[t][k1] = sum_k2 x_t^k2 lo[k2][k1]      (mma.m8n8k4.f64, K = 4 per step)
-//     pot_t   += sum_k1 E[t][k1] y_t^k1         (per lane, then two shuffles)
-// The B fragments of lo stay in registers for the whole chunk.
-template <int NT>
-__global__ void __launch_bounds__(128) k_eval2d_mma(KP k, const EvalTask* __restrict__ tasks) {
-  constexpr int PP = 8 * NT, LD = PP + 1;
-  const EvalTask T = tasks[blockIdx.x];
-  const int ind = blockIdx.y;
-  const int npw = k.npw, n2 = k.n2, Pn = T.p + 1;
-  extern __shared__ double sm[];
-  double* lo = sm;                                   // [PP][LD], zero padded
-  double2* lx = reinterpret_cast<double2*>(sm + ((PP * LD + 1) & ~1));  // [Pn][npw]
-  double2* Ls = lx + Pn * npw;                       // [nexp]
-  double* xl = reinterpret_cast<double*>(Ls + k.nexp);  // [Pn][npw]
-  const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  for (int e = threadIdx.x; e < k.nexp; e += 128) Ls[e] = L[e];
-  for (int e = threadIdx.x; e < PP * LD; e += 128) lo[e] = 0.0;
-  for (int e = threadIdx.x; e < Pn * npw; e += 128) xl[e] = k.x2l[e];
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < Pn * npw; idx += 128) {
-    const int k2 = idx / npw, j1 = idx - k2 * npw;
-    double2 a = make_double2(0.0, 0.0);
-    for (int j2 = 0; j2 < n2; j2++) {
-      const double h = xl[k2 * npw + j2];
-      const double2 v = Ls[j2 + n2 * j1];
-      a.x = fma(h, v.x, a.x);
-      a.y = fma(h, v.y, a.y);
-    }
-    lx[idx] = rot(a, k2);
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < Pn * Pn; idx += 128) {
-    const int k1 = idx / Pn, k2 = idx - k1 * Pn;
-    const double sg = (k1 & 1) ? -1.0 : 1.0;
-    double2 a = make_double2(0.0, 0.0);
-    for (int j1 = 0; j1 < n2; j1++) {
-      const double h = xl[k1 * npw + j1];
-      const double2 u = lx[k2 * npw + j1], v = lx[k2 * npw + j1 + n2];
-      a.x = fma(h, fma(sg, v.x, u.x), a.x);
-      a.y = fma(h, fma(sg, v.y, u.y), a.y);
-    }
-    lo[k2 + LD * k1] = 2.0 * rot(a, k1).x;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int r4 = lane >> 2, c4 = lane & 3;
-  // B fragment (row = k2 = 4 ks + c4, col = k1 = 8 b + r4)
-  double bf[2 * NT][NT];
-#pragma unroll
-  for (int ks = 0; ks < 2 * NT; ks++)
-#pragma unroll
-    for (int b = 0; b < NT; b++) bf[ks][b] = lo[(4 * ks + c4) + LD * (8 * b + r4)];
-  const double* pts = T.set ? k.trg : k.src;
-  double* out = T.set ? k.pottarg : k.pot;
-  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
-  // two groups of eight points per warp iteration (independent MMA chains)
-  auto point = [&](int ta, double& x, double& y) {
-    x = 0.0;
-    y = 0.0;
-    if (ta < T.n) {
-      const int ip = T.i0 + ta;
-      x = (pts[2 * ip] - cx) * k.dsq;
-      y = (pts[2 * ip + 1] - cy) * k.dsq;
-    }
-  };
-  auto finish = [&](int ta, double y, double (*c)[2]) {
-    const double y2 = y * y, y8 = (y2 * y2) * (y2 * y2);
-    double yb = (c4 & 1) ? y2 : 1.0;
-    if (c4 & 2) yb *= y2 * y2;
-    double r = 0.0;
-#pragma unroll
-    for (int b = 0; b < NT; b++) {
-      r = fma(c[b][0], yb, r);
-      r = fma(c[b][1], yb * y, r);
-      yb *= y8;
-    }
-    r += __shfl_xor_sync(0xffffffffu, r, 1);
-    r += __shfl_xor_sync(0xffffffffu, r, 2);
-    if (c4 == 0 && ta < T.n) out[(size_t)(T.i0 + ta) * k.nd + ind] += r;
-  };
-  for (int t0 = 16 * warp; t0 < T.n; t0 += 64) {
-    const int ta0 = t0 + r4, ta1 = t0 + 8 + r4;
-    double x0, y0, x1, y1;
-    point(ta0, x0, y0);
-    point(ta1, x1, y1);
-    const double x20 = x0 * x0, x40 = x20 * x20, x21 = x1 * x1, x41 = x21 * x21;
-    double xa0 = (c4 & 1) ? x0 : 1.0, xa1 = (c4 & 1) ? x1 : 1.0;
-    if (c4 & 2) { xa0 *= x20; xa1 *= x21; }
-    double c0[NT][2], c1[NT][2];
-#pragma unroll
-    for (int b = 0; b < NT; b++) c0[b][0] = c0[b][1] = c1[b][0] = c1[b][1] = 0.0;
-#pragma unroll
-    for (int ks = 0; ks < 2 * NT; ks++) {
-#pragma unroll
-      for (int b = 0; b < NT; b++) {
-        dmma_884(c0[b][0], c0[b][1], xa0, bf[ks][b]);
-        dmma_884(c1[b][0], c1[b][1], xa1, bf[ks][b]);
-      }
-      xa0 *= x40;
-      xa1 *= x41;
-    }
-    finish(ta0, y0, c0);
-    finish(ta1, y1, c1);
   }
 }
 
@@ -1623,91 +1459,35 @@ __global__ void k_split(KP k, const ShiftTask* __restrict__ tasks) {
   }
 }
 
-// ------------------------------------------------------------ (c) eval, 2D
-// One CTA per (leaf, point set, density).  Taylor route: plane wave ->
-// Taylor in shared memory (g2drouts.f:1449-1535), then Horner evaluation of
-// sum_{k1,k2} L[k2 + P k1] x^k2 y^k1.  PW route: direct plane-wave sum with
-// e^{i t x} built by the recurrence of g2dpwevalp_vec.
+// ------------------------------------------------------------ (c) eval, 2D plane-wave route
+// One CTA per (leaf, point set, density): direct plane-wave sum at every point
+// with e^{i t x} built by the recurrence of g2dpwevalp_vec (g2drouts.f:1887-1966),
+// on the levels where the reference picks it (nlocal > 50, fgt2d.f:1166).
 __global__ void __launch_bounds__(256) k_eval2d(KP k, const EvalTask* __restrict__ tasks) {
   const EvalTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
-  const int npw = k.npw, n2 = k.n2;
+  const int n2 = k.n2;
   const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
-  extern __shared__ double sm[];
-  if (T.route == ROUTE_TAYLOR) {
-    const int Pn = T.p + 1;
-    double2* lx = reinterpret_cast<double2*>(sm);   // [Pn][npw]
-    double* lo = sm + 2 * Pn * npw;                  // [Pn][Pn]
-    for (int idx = threadIdx.x; idx < Pn * npw; idx += blockDim.x) {
-      const int k2 = idx / npw, j1 = idx - k2 * npw;
-      double2 a = make_double2(0.0, 0.0);
-      for (int j2 = 0; j2 < n2; j2++) {
-        const double h = k.x2l[k2 * npw + j2];
-        const double2 v = L[j2 + n2 * j1];
-        a.x = fma(h, v.x, a.x);
-        a.y = fma(h, v.y, a.y);
+  for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
+    const int ip = T.i0 + i;
+    const double x = (pts[2 * ip] - cx) * k.dsq, y = (pts[2 * ip + 1] - cy) * k.dsq;
+    const double2 ex = cexpi(k.t1 * x), ey = cexpi(k.t1 * y);
+    const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey);
+    double2 z = make_double2(0.0, 0.0), w1 = ex;
+    for (int kx = 0; kx < n2; kx++) {
+      double2 s = make_double2(0.0, 0.0), w2 = ey;
+      for (int ky = 0; ky < n2; ky++) {
+        s = cfma(L[kx + n2 * ky], w2, s);
+        s = cfmac(L[kx + n2 * (ky + n2)], w2, s);
+        w2 = cmul(w2, eyy);
       }
-      lx[idx] = rot(a, k2);
+      z = cfma(s, w1, z);
+      w1 = cmul(w1, exx);
     }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < Pn * Pn; idx += blockDim.x) {
-      const int k1 = idx / Pn, k2 = idx - k1 * Pn;
-      const double sg = (k1 & 1) ? -1.0 : 1.0;
-      double2 a = make_double2(0.0, 0.0);
-      for (int j1 = 0; j1 < n2; j1++) {
-        const double h = k.x2l[k1 * npw + j1];
-        const double2 u = lx[k2 * npw + j1], v = lx[k2 * npw + j1 + n2];
-        a.x = fma(h, fma(sg, v.x, u.x), a.x);
-        a.y = fma(h, fma(sg, v.y, u.y), a.y);
-      }
-      lo[k2 + Pn * k1] = 2.0 * rot(a, k1).x;
-    }
-    __syncthreads();
-    // Horner in x within a row, then in y; two points per thread for two
-    // independent FMA chains
-    for (int i0 = threadIdx.x; i0 < T.n; i0 += 2 * blockDim.x) {
-      const int i1 = i0 + blockDim.x;
-      const bool two = i1 < T.n;
-      const int p0 = T.i0 + i0, p1 = T.i0 + (two ? i1 : i0);
-      const double x0 = (pts[2 * p0] - cx) * k.dsq, y0 = (pts[2 * p0 + 1] - cy) * k.dsq;
-      const double x1 = (pts[2 * p1] - cx) * k.dsq, y1 = (pts[2 * p1 + 1] - cy) * k.dsq;
-      double r0 = 0.0, r1 = 0.0;
-      for (int k1 = Pn - 1; k1 >= 0; k1--) {
-        double s0 = 0.0, s1 = 0.0;
-        const double* row = lo + Pn * k1;
-        for (int k2 = Pn - 1; k2 >= 0; k2--) {
-          const double c = row[k2];
-          s0 = fma(s0, x0, c);
-          s1 = fma(s1, x1, c);
-        }
-        r0 = fma(r0, y0, s0);
-        r1 = fma(r1, y1, s1);
-      }
-      out[(size_t)p0 * k.nd + ind] += r0;
-      if (two) out[(size_t)p1 * k.nd + ind] += r1;
-    }
-  } else {
-    for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
-      const int ip = T.i0 + i;
-      const double x = (pts[2 * ip] - cx) * k.dsq, y = (pts[2 * ip + 1] - cy) * k.dsq;
-      const double2 ex = cexpi(k.t1 * x), ey = cexpi(k.t1 * y);
-      const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey);
-      double2 z = make_double2(0.0, 0.0), w1 = ex;
-      for (int kx = 0; kx < n2; kx++) {
-        double2 s = make_double2(0.0, 0.0), w2 = ey;
-        for (int ky = 0; ky < n2; ky++) {
-          s = cfma(L[kx + n2 * ky], w2, s);
-          s = cfmac(L[kx + n2 * (ky + n2)], w2, s);
-          w2 = cmul(w2, eyy);
-        }
-        z = cfma(s, w1, z);
-        w1 = cmul(w1, exx);
-      }
-      out[(size_t)ip * k.nd + ind] += 2.0 * z.x;
-    }
+    out[(size_t)ip * k.nd + ind] += 2.0 * z.x;
   }
 }
 
@@ -2253,12 +2033,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     D.form_groups.push_back({form[t].p, t, u});
     t = u;
   }
-  for (int t = 0; t < D.eval_taylor_n;) {
-    int u = t;
-    while (u < D.eval_taylor_n && ev[u].p == ev[t].p) u++;
-    D.eval_groups.push_back({ev[t].p, t, u});
-    t = u;
-  }
+
   // 2D Taylor evaluation: one conversion per leaf slot, point chunks of <= 256
   std::vector<ConvTask> conv;
   std::vector<HornerTask> horner;
@@ -2356,9 +2131,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       const size_t Pn = D.form_pmax + 1, P3 = Pn * Pn * Pn;
       size_t szA = std::max(P3, 2 * Pn * P.npw * n2);
       D.form3_shB = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
-      D.form3_sub = (P3 + 3 * 64 * Pn) * 8 <= lim ? 64 : 32;
-      D.form3_shA = (P3 + 3 * (size_t)D.form3_sub * Pn) * 8;
-      D.form3_smem = D.form3_shB <= lim && D.form3_shA <= lim;
+      // k_form3d_mma stages (8 ceil(P/8) + 2 P) power rows of 68 doubles
+      const size_t shA = ((size_t)8 * ((Pn + 7) / 8) + 2 * Pn) * 68 * 8;
+      D.form3_smem = D.form3_shB <= lim && shA <= lim && Pn <= 32;
       if (D.form3_smem) {
         long long hoff = 0;
         for (int t = 0; t < D.form_hermite_n; t++) {
