@@ -81,6 +81,14 @@ def points_of(w):
     return w["src"].shape[0] * (1 if w["ifpgh"] else 0) + (w["trg"].shape[0] if w["ifpghtarg"] else 0)
 
 
+# DRAM bytes (read + write) of one launch of the dominant kernel, from the
+# committed ncu capture named beside each figure
+PROFILED_TRAFFIC = {
+    ("2d_circle_clustered_N1e7_d1e-6_e1e-6", "k_form2d_mma<2>"):
+        (216619776 + 16602112, "profiles/form2d_mma_2d_circle_N1e7.md"),
+}
+
+
 # ------------------------------------------------------------------ clocks
 _REASON_BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
                 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
@@ -345,34 +353,33 @@ def ours_arm(args, w, rank, world, local_rank):
         return 0
     hbm, tf, peak_src = measured_peaks()
     fp64_tf = ctx["mixed"].fp64_mma_tflops()
-    # roofline of the dominant stage of the headline step
-    dom = max(stage, key=lambda k: stage[k])
-    sb = info["shift_bytes"]
-    kernels = {"form": "k_form2d_mma / k_form3d_acc+k_form3d_h2pw", "eval": "k_eval2d_mma / k_eval3d_taylor_smem",
-               "direct": "k_direct", "merge": "k_merge", "m2l": "k_m2l", "split": "k_split",
-               "gather": "k_gather_pts", "scatter": "k_unsort"}
-    hbm_work = {"merge": sb[0], "m2l": sb[1], "split": sb[2],
-                "gather": w["src"].shape[0] * nd * (8 + 8 + 4),
-                "scatter": w["src"].shape[0] * nd * (8 + 8) + w["src"].shape[0] * 4}
-    t_dom = stage[dom] / 1e3
-    if dom in ("form", "eval"):
-        flops = info[f"{dom}_route_flops"]
-        ach = flops / t_dom / 1e12
-        roof = {"bound": "tensor", "kernel": kernels[dom], "stage": dom, "achieved": ach,
-                "peak": tf, "unit": "TFLOP/s", "frac": ach / tf, "traffic": None,
-                "peak_source": f"{peak_src} bf16 dense (burst)",
+    # roofline of the dominant tensor-core launch (the Hermite-block MMA kernel
+    # of the largest form order group), timed with CUDA events around that
+    # launch alone over K further executes on the plan's stream
+    ctx["mixed"].set_precision("mixed")
+    dms, dfl, dname = [], 0.0, None
+    for _ in range(args.steps):
+        r = plan.profile_dominant(d_chg.data_ptr(), d_pot.data_ptr(), d_pt.data_ptr())
+        if r is None:
+            break
+        dms.append(r[0])
+        dfl, dname = r[1], r[2]
+    if dms:
+        t_k = sum(dms) / len(dms) / 1e3
+        ach = dfl / t_k / 1e12
+        traffic, tsrc = PROFILED_TRAFFIC.get((w["name"], dname), (None, None))
+        roof = {"bound": "tensor", "kernel": dname, "stage": "form", "achieved": ach, "peak": tf,
+                "unit": "TFLOP/s", "frac": ach / tf, "traffic": traffic,
+                "peak_source": f"{peak_src} bf16 dense (burst); the kernel runs FP64 m8n8k4 MMA",
                 "fp64_mma_peak_measured": fp64_tf, "frac_of_fp64_mma": ach / fp64_tf,
-                "work": f"{flops:.4g} route flops per step (FP64 m8n8k4 MMA + FMA)"}
-    elif dom in hbm_work:
-        ach = hbm_work[dom] / t_dom / 1e9
-        roof = {"bound": "hbm", "kernel": kernels[dom], "stage": dom, "achieved": ach, "peak": hbm,
-                "unit": "GB/s", "frac": ach / hbm, "traffic": None, "peak_source": peak_src}
+                "launch_ms": t_k * 1e3,
+                "work": f"{dfl:.4g} flops per launch = 2 n P^d over the group's sources"}
+        if tsrc:
+            roof["traffic_source"] = tsrc
     else:
-        pairs = info["direct_pairs"]
-        roof = {"bound": "hbm", "kernel": kernels[dom], "stage": dom,
-                "achieved": w["src"].shape[0] * (dim + nd) * 8 / t_dom / 1e9, "peak": hbm,
-                "unit": "GB/s", "frac": None, "traffic": None, "peak_source": peak_src,
-                "note": f"exp-bound; {pairs / t_dom:.4g} source-target pairs/s"}
+        roof = {"bound": "tensor", "kernel": None, "achieved": None, "peak": tf, "unit": "TFLOP/s",
+                "frac": None, "traffic": None, "note": "no tensor-core launch in this plan"}
+    sb = info["shift_bytes"]
     stage_rates = {
         "form_tflops": info["form_route_flops"] / (stage["form"] / 1e3) / 1e12 if stage.get("form") else None,
         "eval_tflops": info["eval_route_flops"] / (stage["eval"] / 1e3) / 1e12 if stage.get("eval") else None,
@@ -408,7 +415,7 @@ def ours_arm(args, w, rank, world, local_rank):
         "host_plan_s": plan_s,
         "e2e": {"value": world * pts / e2e_s, "unit": "points/s", "s_per_step": e2e_s,
                 "steps": e2e_steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "includes": "host tree + lists + plan upload + H2D + transform + D2H"},
+                "includes": "tree build (point work on the GPU) + lists + plan upload + H2D + transform + D2H"},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roof,
         "stage_rates": stage_rates,

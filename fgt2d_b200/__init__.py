@@ -112,6 +112,8 @@ def lib():
     L.fgt_plan_execute_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.fgt_plan_profile_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]
     L.fgt_plan_get_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
+    L.fgt_plan_profile_dominant.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, i]
     L.fgt_plan_destroy.argtypes = [_vp]
     L.fgt_status_string.restype = ctypes.c_char_p
     L.fgt_status_string.argtypes = [i]
@@ -267,6 +269,18 @@ class Plan:
                                              d_pottarg or None, ms), "fgt_plan_profile_device")
         names = ["gather", "form", "merge", "m2l", "split", "eval", "direct", "scatter"]
         return dict(zip(names, list(ms)))
+
+    def profile_dominant(self, d_chg, d_pot, d_pottarg):
+        """(ms, flops, name) of the plan's dominant tensor-core launch in one
+        execute on the context's stream; None when the plan has none."""
+        ms, fl = ctypes.c_double(), ctypes.c_double()
+        name = ctypes.create_string_buffer(64)
+        st = lib().fgt_plan_profile_dominant(self._h, d_chg, d_pot or None, d_pottarg or None,
+                                             ctypes.byref(ms), ctypes.byref(fl), name, 64)
+        if st == 2:
+            return None
+        _check(st, "fgt_plan_profile_dominant")
+        return ms.value, fl.value, name.value.decode()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -463,12 +463,28 @@ int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const
   return run_device(p, q, pot, pt, st, nullptr);
 }
 
+int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double* pt, double* ms,
+                              double* flops, char* name, int name_len) {
+  if (!p || !ms || !flops) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  StageTimes T;
+  memset(T.ms, 0, sizeof(T.ms));
+  if (p->H.P.large_delta) return FGT_ERR_UNSUPPORTED;
+  int r = run_device(p, q, pot, pt, p->ctx->stream, &T);
+  if (r != FGT_OK) return r;
+  CKS(cudaStreamSynchronize(p->ctx->stream));
+  *ms = T.dom_ms;
+  *flops = T.dom_flops;
+  if (name && name_len > 0) snprintf(name, name_len, "%s", T.dom_name);
+  return T.dom_name[0] ? FGT_OK : FGT_ERR_UNSUPPORTED;
+}
+
 int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const double* t,
                             double* pot, double* pt, float* ms8) {
   if (!p || !ms8) return FGT_ERR_BADARG;
   CKS(cudaSetDevice(p->ctx->device));
   StageTimes T;
-  memset(&T, 0, sizeof(T));
+  memset(T.ms, 0, sizeof(T.ms));
   (void)s; (void)t;
   int r = run_device(p, q, pot, pt, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
   if (r != FGT_OK) return r;

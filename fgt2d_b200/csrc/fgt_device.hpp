@@ -35,6 +35,11 @@ struct HornerTask {
 
 struct StageTimes {
   float ms[8];  // gather, form, merge, m2l, split, eval, direct, scatter
+  // the dominant tensor-core launch: the Hermite-block MMA kernel of the
+  // form group with the most sources (k_form2d_mma / k_form3d_mma)
+  float dom_ms = 0;
+  double dom_flops = 0;  // 2 n P^dim (x nd) for that group
+  char dom_name[48] = {0};
 };
 
 struct DevicePlan {
@@ -98,6 +103,9 @@ struct DevicePlan {
   int eval_taylor_n = 0, eval_pw_n = 0;
   int form_pmax = 0, eval_pmax = 0;  // largest order among Hermite form / Taylor eval tasks
   std::vector<OrderGroup> form_groups;
+  int dom_form_group = -1;        // 2D: form group with the most sources (MMA kernels)
+  int dom_fchunk_group = -1;      // 3D: chunk group with the most sources
+  std::vector<double> group_flops;  // 2 n P^dim per form group (2D) / chunk group (3D)
   // 2D Taylor evaluation (conversion per leaf, then Horner per point chunk)
   long long* form_hoff = nullptr;  // 2D MMA form: per form task, offset of its Hermite block in hbuf
   ConvTask* conv = nullptr;

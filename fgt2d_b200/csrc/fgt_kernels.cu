@@ -2034,6 +2034,18 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     t = u;
   }
 
+  // dominant form group (most sources) for the per-kernel roofline of the bench
+  if (P.dim == 2) {
+    long long best = -1;
+    for (size_t gi = 0; gi < D.form_groups.size(); gi++) {
+      const OrderGroup& G = D.form_groups[gi];
+      long long n = 0;
+      for (int t = G.beg; t < G.end; t++) n += form[t].n;
+      const double Pn = G.p + 1;
+      D.group_flops.push_back(2.0 * (double)n * Pn * Pn * P.nd);
+      if (G.p + 1 <= 32 && n > best) { best = n; D.dom_form_group = (int)gi; }
+    }
+  }
   // 2D Taylor evaluation: one conversion per leaf slot, point chunks of <= 256
   std::vector<ConvTask> conv;
   std::vector<HornerTask> horner;
@@ -2149,10 +2161,15 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
         hbuf_doubles = (size_t)hoff * P.nd;
         D.nfchunks = (int)fchunks.size();
         // chunk ranges of equal order (the tasks are sorted by order)
+        long long best = -1;
         for (size_t t = 0; t < fchunks.size();) {
           size_t u = t;
           const int pt = form[fchunks[t].task].p;
-          while (u < fchunks.size() && form[fchunks[u].task].p == pt) u++;
+          long long n = 0;
+          while (u < fchunks.size() && form[fchunks[u].task].p == pt) n += fchunks[u++].n;
+          const double Pn = pt + 1;
+          D.group_flops.push_back(2.0 * (double)n * Pn * Pn * Pn * P.nd);
+          if (n > best) { best = n; D.dom_fchunk_group = (int)D.fchunk_groups.size(); }
           D.fchunk_groups.push_back({pt, (int)t, (int)u});
           t = u;
         }
@@ -2351,9 +2368,15 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
   KP k = make_kp(D);
   k.ws = D.h2x;  // row j = 0 of h2x holds the weights
   const int nd = P.nd;
-  cudaEvent_t ev[9];
-  if (times)
+  cudaEvent_t ev[9], dev0 = nullptr, dev1 = nullptr;
+  if (times) {
     for (int i = 0; i < 9; i++) CK(cudaEventCreate(&ev[i]));
+    CK(cudaEventCreate(&dev0));
+    CK(cudaEventCreate(&dev1));
+    times->dom_ms = 0;
+    times->dom_flops = 0;
+    times->dom_name[0] = 0;
+  }
   auto mark = [&](int i) { if (times) cudaEventRecord(ev[i], st); };
   long long launches = 0;
   mark(0);
@@ -2370,10 +2393,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
   if (!P.all_direct) {
     // (a) form
     if (P.dim == 2 && D.form_hermite_n > 0) {
-      for (const OrderGroup& G : D.form_groups) {
+      for (size_t gi = 0; gi < D.form_groups.size(); gi++) {
+        const OrderGroup& G = D.form_groups[gi];
         const int Pn = G.p + 1;
         dim3 g(G.end - G.beg, nd);
         const FormTask* tk = D.form + G.beg;
+        const bool dom = times && (int)gi == D.dom_form_group;
+        if (dom) cudaEventRecord(dev0, st);
         if (Pn <= 32) {
 #define FORM_MMA(NT)                                                                              \
   do {                                                                                            \
@@ -2386,6 +2412,11 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
           else if (Pn <= 24) FORM_MMA(3);
           else FORM_MMA(4);
 #undef FORM_MMA
+          if (dom) {
+            cudaEventRecord(dev1, st);
+            snprintf(times->dom_name, sizeof(times->dom_name), "k_form2d_mma<%d>", (Pn + 7) / 8);
+            times->dom_flops = D.group_flops[gi];
+          }
           const int nt = G.end - G.beg;
           const H2pwDims Z(Pn, P.npw);
           const size_t sh2 = 4 * (size_t)Z.warp * 8;
@@ -2415,8 +2446,11 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
       }
     }
     if (P.dim == 3 && D.form_hermite_n > 0 && D.form3_smem) {
-      for (const OrderGroup& G : D.fchunk_groups) {
+      for (size_t gi = 0; gi < D.fchunk_groups.size(); gi++) {
+        const OrderGroup& G = D.fchunk_groups[gi];
         const int Pn = G.p + 1, mt = (Pn + 7) / 8;
+        const bool dom = times && (int)gi == D.dom_fchunk_group;
+        if (dom) cudaEventRecord(dev0, st);
         const size_t sh = ((size_t)8 * mt + 2 * Pn) * 68 * 8;
         const dim3 fg(G.end - G.beg, nd);
         const FormChunk* ch = D.fchunks + G.beg;
@@ -2429,6 +2463,11 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
           FORM3_CASE(1) FORM3_CASE(2) FORM3_CASE(3) FORM3_CASE(4)
 #undef FORM3_CASE
           default: return cudaErrorNotSupported;
+        }
+        if (dom) {
+          cudaEventRecord(dev1, st);
+          snprintf(times->dom_name, sizeof(times->dom_name), "k_form3d_mma<%d>", mt);
+          times->dom_flops = D.group_flops[gi];
         }
         launches++;
       }
@@ -2621,7 +2660,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
     float t[8];
     for (int i = 0; i < 8; i++) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
     for (int i = 0; i < 8; i++) times->ms[i] = t[i];
+    if (times->dom_name[0]) cudaEventElapsedTime(&times->dom_ms, dev0, dev1);
     for (int i = 0; i < 9; i++) cudaEventDestroy(ev[i]);
+    cudaEventDestroy(dev0);
+    cudaEventDestroy(dev1);
   }
   return cudaSuccess;
 }

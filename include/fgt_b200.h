@@ -174,6 +174,13 @@ int fgt_plan_execute_device(fgt_plan* plan, const double* d_sources, const doubl
 int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
                             const double* d_targ, double* d_pot, double* d_pottarg, float* ms8);
 int fgt_plan_get_info(const fgt_plan* plan, fgt_plan_info* info);
+/* One execute with CUDA events around the plan's dominant tensor-core launch
+ * (the Hermite-block MMA kernel of the form order group with the most
+ * sources) on the context's stream: its device time (ms), its algorithmic
+ * flops (2 n P^dim nd) and its name.  FGT_ERR_UNSUPPORTED when the plan has
+ * no such launch (all-direct, large-delta). */
+int fgt_plan_profile_dominant(fgt_plan* plan, const double* d_charge, double* d_pot, double* d_pottarg,
+                              double* ms, double* flops, char* name, int name_len);
 int fgt_plan_destroy(fgt_plan* plan);
 
 /* ---- host tree (no device needed) ----------------------------------------
