@@ -19,8 +19,8 @@ import os
 
 import numpy as np
 
-__all__ = ["fgt2d", "fgt3d", "transform", "Context", "Plan", "HostTree", "lib", "FGTError",
-           "PREC_FP64", "PREC_MIXED", "PREC_AUTO"]
+__all__ = ["fgt2d", "fgt3d", "transform", "transform_pgh", "Context", "Plan", "HostTree", "lib",
+           "FGTError", "PREC_FP64", "PREC_MIXED", "PREC_AUTO", "nhess"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libfgt_b200.so")
@@ -68,7 +68,8 @@ class Request(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("nd", ctypes.c_int), ("delta", ctypes.c_double),
                 ("eps", ctypes.c_double), ("ns", ctypes.c_int), ("sources", _dp), ("charge", _dp),
                 ("nt", ctypes.c_int), ("targ", _dp), ("ifpgh", ctypes.c_int),
-                ("ifpghtarg", ctypes.c_int), ("pot", _dp), ("pottarg", _dp)]
+                ("ifpghtarg", ctypes.c_int), ("pot", _dp), ("pottarg", _dp), ("grad", _dp),
+                ("hess", _dp), ("gradtarg", _dp), ("hesstarg", _dp)]
 
 
 class ServerStats(ctypes.Structure):
@@ -110,6 +111,8 @@ def lib():
     L.fgt_plan_create.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, ctypes.POINTER(_vp)]
     L.fgt_plan_execute_host.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp]
     L.fgt_plan_execute_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.fgt_plan_execute_host_pgh.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.fgt_plan_execute_device_pgh.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.fgt_plan_profile_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]
     L.fgt_plan_get_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
     L.fgt_plan_profile_dominant.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_double),
@@ -196,23 +199,57 @@ def _default_ctx():
     return h
 
 
-def transform(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
-              ifcharge=1, ifdipole=0):
-    """Whole transform; returns ``(pot, pottarg)`` shaped ``(ns, nd)``, ``(nt, nd)``."""
+def nhess(dim):
+    """Hessian components per density: 3 in 2D (xx, xy, yy), 6 in 3D
+    (xx, yy, zz, xy, xz, yz), the reference's orders."""
+    return 3 if dim == 2 else 6
+
+
+def _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg):
+    H = nhess(dim)
+    return {"pot": np.zeros((ns, nd)) if ifpgh >= 1 else None,
+            "grad": np.zeros((ns, dim, nd)) if ifpgh >= 2 else None,
+            "hess": np.zeros((ns, H, nd)) if ifpgh >= 3 else None,
+            "pottarg": np.zeros((nt, nd)) if ifpghtarg >= 1 else None,
+            "gradtarg": np.zeros((nt, dim, nd)) if ifpghtarg >= 2 else None,
+            "hesstarg": np.zeros((nt, H, nd)) if ifpghtarg >= 3 else None}
+
+
+def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
+                  ifcharge=1, ifdipole=0):
+    """Whole transform with gradients (ifpgh / ifpghtarg = 2) and Hessians (3).
+
+    Returns a dict with ``pot`` (ns, nd), ``grad`` (ns, dim, nd), ``hess``
+    (ns, H, nd) and the same for the targets (``pottarg``, ``gradtarg``,
+    ``hesstarg``), None where not requested: the reference's
+    ``grad(nd, dim, ns)`` / ``hess(nd, H, ns)`` in C order.
+    """
     L = lib()
     src = _f64(sources, (-1, dim))
     ns = src.shape[0]
     q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
     trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
     nt = trg.shape[0]
-    pot = np.zeros((ns, nd)) if ifpgh else None
-    pt = np.zeros((nt, nd)) if ifpghtarg else None
+    o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg)
     h = ctx.handle if ctx is not None else _default_ctx()
     st = L.fgt_transform(h, dim, nd, float(delta), float(eps), ns, _p(src), ifcharge, _p(q),
-                         ifdipole, None, None, ifpgh, _p(pot), None, None, nt, _p(trg), ifpghtarg,
-                         _p(pt), None, None)
+                         ifdipole, None, None, ifpgh, _p(o["pot"]), _p(o["grad"]), _p(o["hess"]),
+                         nt, _p(trg), ifpghtarg, _p(o["pottarg"]), _p(o["gradtarg"]),
+                         _p(o["hesstarg"]))
     _check(st, "fgt_transform")
-    return pot, pt
+    return o
+
+
+def transform(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
+              ifcharge=1, ifdipole=0):
+    """Whole transform; returns ``(pot, pottarg)`` shaped ``(ns, nd)``, ``(nt, nd)``.
+    With ifpgh or ifpghtarg >= 2 it returns the reference's six outputs
+    ``(pot, grad, hess, pottarg, gradtarg, hesstarg)`` (see transform_pgh)."""
+    o = transform_pgh(dim, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, ctx, ifcharge,
+                      ifdipole)
+    if max(ifpgh, ifpghtarg) >= 2:
+        return o["pot"], o["grad"], o["hess"], o["pottarg"], o["gradtarg"], o["hesstarg"]
+    return o["pot"], o["pottarg"]
 
 
 def fgt2d(nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None):
@@ -256,6 +293,23 @@ class Plan:
         _check(lib().fgt_plan_execute_host(self._h, _p(src), _p(q), _p(trg), _p(pot), _p(pt)),
                "fgt_plan_execute_host")
         return pot, pt
+
+    def execute_host_pgh(self, charge):
+        """All outputs of the plan's flags (dict as transform_pgh)."""
+        q = _f64(charge, (self.ns, self.nd))
+        o = _outputs(self.dim, self.nd, self.ns, self.nt, self.ifpgh, self.ifpghtarg)
+        _check(lib().fgt_plan_execute_host_pgh(self._h, _p(q), _p(o["pot"]), _p(o["grad"]),
+                                               _p(o["hess"]), _p(o["pottarg"]), _p(o["gradtarg"]),
+                                               _p(o["hesstarg"])), "fgt_plan_execute_host_pgh")
+        return o
+
+    def execute_device_pgh(self, d_chg, d_pot, d_grad, d_hess, d_pottarg, d_gradtarg, d_hesstarg,
+                           stream=None):
+        """Device pointers (ints; 0 skips a gradient or Hessian); asynchronous."""
+        _check(lib().fgt_plan_execute_device_pgh(self._h, d_chg, d_pot or None, d_grad or None,
+                                                 d_hess or None, d_pottarg or None,
+                                                 d_gradtarg or None, d_hesstarg or None, stream),
+               "fgt_plan_execute_device_pgh")
 
     def execute_device(self, d_src, d_chg, d_trg, d_pot, d_pottarg, stream=None):
         """Device pointers (ints, e.g. ``tensor.data_ptr()``); asynchronous."""
@@ -367,22 +421,27 @@ class Server:
         q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
         trg = (src if targ is sources else _f64(targ, (-1, dim))) if targ is not None else None
         nt = trg.shape[0] if trg is not None else 0
-        pot = np.empty((ns, nd)) if ifpgh else None
-        pt = np.empty((nt, nd)) if ifpghtarg else None
+        o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg)
         r = Request(dim, nd, float(delta), float(eps), ns, _p(src), _p(q), nt, _p(trg), ifpgh,
-                    ifpghtarg, _p(pot), _p(pt))
+                    ifpghtarg, _p(o["pot"]), _p(o["pottarg"]), _p(o["grad"]), _p(o["hess"]),
+                    _p(o["gradtarg"]), _p(o["hesstarg"]))
         rid = ctypes.c_longlong()
         _check(lib().fgt_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "fgt_server_submit")
-        self._live[rid.value] = (src, q, trg, pot, pt)
+        self._live[rid.value] = (src, q, trg, o)
         return rid.value
+
+    def wait_pgh(self, rid):
+        """Blocks until request rid is done; returns (outputs dict, latency_s)."""
+        lat = ctypes.c_double()
+        st = lib().fgt_server_wait(self._h, int(rid), ctypes.byref(lat))
+        src, q, trg, o = self._live.pop(rid)
+        _check(st, "fgt_server_wait")
+        return o, lat.value
 
     def wait(self, rid):
         """Blocks until request rid is done; returns (pot, pottarg, latency_s)."""
-        lat = ctypes.c_double()
-        st = lib().fgt_server_wait(self._h, int(rid), ctypes.byref(lat))
-        src, q, trg, pot, pt = self._live.pop(rid)
-        _check(st, "fgt_server_wait")
-        return pot, pt, lat.value
+        o, lat = self.wait_pgh(rid)
+        return o["pot"], o["pottarg"], lat
 
     def stats(self):
         s = ServerStats()

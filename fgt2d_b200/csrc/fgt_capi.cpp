@@ -46,6 +46,10 @@ struct fgt_plan {
   double* d_trg = nullptr;
   double* d_pot = nullptr;
   double* d_pottarg = nullptr;
+  double* d_grad = nullptr;      // gradients / Hessians when the flags ask for them
+  double* d_hess = nullptr;
+  double* d_gradtarg = nullptr;
+  double* d_hesstarg = nullptr;
   double* d_work = nullptr;  // large-delta local expansion
   int* d_flag = nullptr;     // device-side argument checks
   int last_launches = 0;
@@ -100,20 +104,23 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
   if (scan_points && !finite_all(sources, (size_t)ns * dim)) return FGT_ERR_BADARG;
   if (scan_points && nt > 0 && targ && !finite_all(targ, (size_t)nt * dim)) return FGT_ERR_BADARG;
   if (ifcharge != 1 || ifdipole != 0) return FGT_ERR_UNSUPPORTED;
-  if (ifpgh < 0 || ifpgh > 1 || ifpghtarg < 0 || ifpghtarg > 1) return FGT_ERR_UNSUPPORTED;
+  if (ifpgh < 0 || ifpgh > 3 || ifpghtarg < 0 || ifpghtarg > 3) return FGT_ERR_UNSUPPORTED;
   return FGT_OK;
 }
 
-// Device copies of the caller-order arrays (sources, charges, targets,
-// potentials) in one allocation; uploads the points.  The large-delta work
-// array is sized once the order is known (plan_device re-allocates then).
-int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, const double* src_host, const double* trg_host,
-             bool upload_trg) {
+// Device copies of the caller-order arrays (sources, charges, targets and
+// the outputs the flags ask for) and n_work doubles of large-delta work in one
+// allocation; uploads the points.
+int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int ifpgh, int ifpghtarg, size_t n_work,
+             const double* src_host, const double* trg_host, bool upload_trg) {
+  const size_t nh = dim == 2 ? 3 : 6;
   size_t n_src = (size_t)ns * dim, n_chg = (size_t)ns * nd, n_trg = (size_t)nt * dim;
   size_t n_pot = (size_t)ns * nd, n_pt = (size_t)nt * nd;
-  const size_t n_work = 0;
+  size_t n_g = ifpgh >= 2 ? n_pot * dim : 0, n_h = ifpgh >= 3 ? n_pot * nh : 0;
+  size_t n_gt = ifpghtarg >= 2 ? n_pt * dim : 0, n_ht = ifpghtarg >= 3 ? n_pt * nh : 0;
   auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
-  p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
+  p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_g) + al(n_h) +
+                     al(n_gt) + al(n_ht) + al(n_work) + 32);
   CKS(device_pool_setup());
   CKS(cudaMallocAsync(reinterpret_cast<void**>(&p->d_io), p->io_bytes, p->ctx->stream));
   double* c = p->d_io;
@@ -122,6 +129,10 @@ int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, const double* src_hos
   p->d_trg = c; c += al(n_trg);
   p->d_pot = c; c += al(n_pot);
   p->d_pottarg = c; c += al(n_pt);
+  p->d_grad = n_g ? c : nullptr; c += al(n_g);
+  p->d_hess = n_h ? c : nullptr; c += al(n_h);
+  p->d_gradtarg = n_gt ? c : nullptr; c += al(n_gt);
+  p->d_hesstarg = n_ht ? c : nullptr; c += al(n_ht);
   p->d_work = c; c += al(n_work);
   p->d_flag = reinterpret_cast<int*>(c);
   cudaStream_t st = p->ctx->stream;
@@ -144,25 +155,11 @@ int check_finite_device(fgt_plan* p, const double* d, size_t n) {
 
 int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   const Params& P = p->H.P;
-  size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
-  size_t n_src = ns * dim, n_chg = ns * nd, n_trg = nt * dim, n_pot = ns * nd, n_pt = nt * nd;
-  size_t n_work = 0;
-  if (P.large_delta) n_work = large_delta_work_doubles(P, true);
-  auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
-  p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_work) + 32);
-  CKS(device_pool_setup());
-  CKS(cudaMallocAsync(reinterpret_cast<void**>(&p->d_io), p->io_bytes, p->ctx->stream));
-  double* c = p->d_io;
-  p->d_src = c; c += al(n_src);
-  p->d_chg = c; c += al(n_chg);
-  p->d_trg = c; c += al(n_trg);
-  p->d_pot = c; c += al(n_pot);
-  p->d_pottarg = c; c += al(n_pt);
-  p->d_work = c; c += al(n_work);
-  p->d_flag = reinterpret_cast<int*>(c);
+  const size_t n_work = P.large_delta ? large_delta_work_doubles(P, true) : 0;
+  const int sa = alloc_io(p, P.dim, P.nd, P.ns, P.nt, P.ifpgh, P.ifpghtarg, n_work, src_host, trg_host,
+                         P.ifpghtarg > 0);
+  if (sa != FGT_OK) return sa;
   cudaStream_t st = p->ctx->stream;
-  if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
-  if (nt > 0 && P.ifpghtarg > 0) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
   if (!P.large_delta) {
     CKS(device_plan_create(p->H, p->D));
     p->have_device = true;
@@ -181,7 +178,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
                             const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                             const std::function<int(size_t)>* admit = nullptr) {
   const bool same = targ == sources && nt == ns;
-  int st = alloc_io(p, dim, nd, ns, nt, sources, targ, !same);
+  int st = alloc_io(p, dim, nd, ns, nt, ifpgh, ifpghtarg, 0, sources, targ, !same);
   if (st != FGT_OK) return st;
   st = check_finite_device(p, p->d_src, (size_t)ns * dim);
   if (st == FGT_OK && !same) st = check_finite_device(p, p->d_trg, (size_t)nt * dim);
@@ -232,26 +229,62 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   return FGT_OK;
 }
 
-int run_device(fgt_plan* p, const double* q, double* pot, double* pt, cudaStream_t st,
-               StageTimes* times) {
+// Outputs the plan's flags ask for must be non-null except gradients and
+// Hessians, which are skipped when null.
+int run_device(fgt_plan* p, const double* q, const Outputs& o, cudaStream_t st, StageTimes* times) {
   const Params& P = p->H.P;
+  if ((P.ifpgh > 0 && P.ns > 0 && !o.pot) || (P.ifpghtarg > 0 && P.nt > 0 && !o.pottarg))
+    return FGT_ERR_BADARG;
   int prec = resolve_precision(p->ctx, P.eps);
   if (!p->done) CKS(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
   if (P.large_delta) {
-    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, pot, pt, p->d_work, st, true));
-    p->last_launches = (P.ns > 0) + (P.ifpgh == 1) + (P.ifpghtarg == 1);
+    Outputs lo = o;  // the large-delta kernels write every component they compute
+    double* dg[4] = {p->d_grad, p->d_hess, p->d_gradtarg, p->d_hesstarg};
+    double** og[4] = {&lo.grad, &lo.hess, &lo.gradtarg, &lo.hesstarg};
+    for (int i = 0; i < 4; i++)
+      if (!*og[i]) *og[i] = dg[i];
+    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, lo, p->d_work, st, true));
+    p->last_launches = (P.ns > 0) + (P.ifpgh >= 1) + (P.ifpghtarg >= 1);
   } else {
-    CKS(device_plan_execute(p->D, q, pot, pt, prec, st, times));
+    CKS(device_plan_execute(p->D, q, o, prec, st, times));
     p->last_launches = (int)p->D.launches;
   }
   CKS(cudaEventRecord(p->done, st));
   return FGT_OK;
 }
 
+// Charges in from the host, every execute output the plan computes back to
+// the non-null host arrays of `host`.
+int exec_host(fgt_plan* p, const double* charge, const Outputs& host) {
+  const Params& P = p->H.P;
+  cudaStream_t st = p->ctx->stream;
+  CKS(cudaSetDevice(p->ctx->device));
+  const size_t ns = P.ns, nt = P.nt, nd = P.nd, nh = P.dim == 2 ? 3 : 6;
+  CKS(cudaMemcpyAsync(p->d_chg, charge, ns * nd * 8, cudaMemcpyHostToDevice, st));
+  int s = check_finite_device(p, p->d_chg, ns * nd);
+  if (s != FGT_OK) return s;
+  Outputs d;
+  d.pot = p->d_pot; d.grad = p->d_grad; d.hess = p->d_hess;
+  d.pottarg = p->d_pottarg; d.gradtarg = p->d_gradtarg; d.hesstarg = p->d_hesstarg;
+  s = run_device(p, p->d_chg, d, st, nullptr);
+  if (s != FGT_OK) return s;
+  auto back = [&](double* h, const double* dv, size_t n) -> cudaError_t {
+    return h && dv && n ? cudaMemcpyAsync(h, dv, n * 8, cudaMemcpyDeviceToHost, st) : cudaSuccess;
+  };
+  if (P.ifpgh >= 1) CKS(back(host.pot, d.pot, ns * nd));
+  if (P.ifpgh >= 2) CKS(back(host.grad, d.grad, ns * nd * P.dim));
+  if (P.ifpgh >= 3) CKS(back(host.hess, d.hess, ns * nd * nh));
+  if (P.ifpghtarg >= 1) CKS(back(host.pottarg, d.pottarg, nt * nd));
+  if (P.ifpghtarg >= 2) CKS(back(host.gradtarg, d.gradtarg, nt * nd * P.dim));
+  if (P.ifpghtarg >= 3) CKS(back(host.hesstarg, d.hesstarg, nt * nd * nh));
+  CKS(cudaStreamSynchronize(st));
+  return FGT_OK;
+}
+
 int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                    const double* sources, int ifcharge, const double* charge, int ifdipole,
-                   int ifpgh, double* pot, int nt, const double* targ, int ifpghtarg,
-                   double* pottarg) {
+                   int ifpgh, double* pot, double* grad, double* hess, int nt, const double* targ,
+                   int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
   const bool on_device = ctx->tree == FGT_TREE_DEVICE;
   int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg,
                       !on_device);
@@ -259,9 +292,19 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
   if (!on_device && ns > 0 && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
   // outputs are written in full on success; zero them when nothing runs or
   // the call fails
+  const size_t nh = dim == 2 ? 3 : 6;
+  if ((ifpgh >= 1 && ns > 0 && !pot) || (ifpgh >= 2 && ns > 0 && !grad) || (ifpgh >= 3 && ns > 0 && !hess) ||
+      (ifpghtarg >= 1 && nt > 0 && !pottarg) || (ifpghtarg >= 2 && nt > 0 && !gradtarg) ||
+      (ifpghtarg >= 3 && nt > 0 && !hesstarg))
+    return FGT_ERR_BADARG;
   auto zero = [&] {
-    if (ifpgh == 1 && ns > 0 && pot) memset(pot, 0, sizeof(double) * (size_t)ns * nd);
-    if (ifpghtarg == 1 && nt > 0 && pottarg) memset(pottarg, 0, sizeof(double) * (size_t)nt * nd);
+    auto z = [](double* a, size_t n) { if (a && n) memset(a, 0, sizeof(double) * n); };
+    if (ifpgh >= 1) z(pot, (size_t)ns * nd);
+    if (ifpgh >= 2) z(grad, (size_t)ns * nd * dim);
+    if (ifpgh >= 3) z(hess, (size_t)ns * nd * nh);
+    if (ifpghtarg >= 1) z(pottarg, (size_t)nt * nd);
+    if (ifpghtarg >= 2) z(gradtarg, (size_t)nt * nd * dim);
+    if (ifpghtarg >= 3) z(hesstarg, (size_t)nt * nd * nh);
   };
   if (ns == 0) {
     zero();
@@ -270,7 +313,10 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
   fgt_plan* plan = nullptr;
   st = fgt_plan_create(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, &plan);
   if (st == FGT_OK) {
-    st = fgt_plan_execute_host(plan, sources, charge, targ, pot, pottarg);
+    Outputs h;
+    h.pot = pot; h.grad = grad; h.hess = hess;
+    h.pottarg = pottarg; h.gradtarg = gradtarg; h.hesstarg = hesstarg;
+    st = exec_host(plan, charge, h);
     fgt_plan_destroy(plan);
   }
   if (st != FGT_OK) zero();
@@ -437,21 +483,20 @@ int fgt_plan_destroy(fgt_plan* p) {
 int fgt_plan_execute_host(fgt_plan* p, const double* sources, const double* charge,
                           const double* targ, double* pot, double* pottarg) {
   if (!p) return FGT_ERR_BADARG;
-  const Params& P = p->H.P;
-  cudaStream_t st = p->ctx->stream;
-  CKS(cudaSetDevice(p->ctx->device));
   (void)sources; (void)targ;  // fixed at plan creation
-  size_t ns = P.ns, nt = P.nt;
-  CKS(cudaMemcpyAsync(p->d_chg, charge, ns * P.nd * 8, cudaMemcpyHostToDevice, st));
-  int s = check_finite_device(p, p->d_chg, ns * P.nd);
-  if (s != FGT_OK) return s;
-  s = run_device(p, p->d_chg, p->d_pot, p->d_pottarg, st, nullptr);
-  if (s != FGT_OK) return s;
-  if (P.ifpgh == 1 && pot) CKS(cudaMemcpyAsync(pot, p->d_pot, ns * P.nd * 8, cudaMemcpyDeviceToHost, st));
-  if (P.ifpghtarg == 1 && nt > 0 && pottarg)
-    CKS(cudaMemcpyAsync(pottarg, p->d_pottarg, nt * P.nd * 8, cudaMemcpyDeviceToHost, st));
-  CKS(cudaStreamSynchronize(st));
-  return FGT_OK;
+  Outputs h;
+  h.pot = pot;
+  h.pottarg = pottarg;
+  return exec_host(p, charge, h);
+}
+
+int fgt_plan_execute_host_pgh(fgt_plan* p, const double* charge, double* pot, double* grad,
+                              double* hess, double* pottarg, double* gradtarg, double* hesstarg) {
+  if (!p) return FGT_ERR_BADARG;
+  Outputs h;
+  h.pot = pot; h.grad = grad; h.hess = hess;
+  h.pottarg = pottarg; h.gradtarg = gradtarg; h.hesstarg = hesstarg;
+  return exec_host(p, charge, h);
 }
 
 int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const double* t,
@@ -460,7 +505,21 @@ int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const
   CKS(cudaSetDevice(p->ctx->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
   (void)s; (void)t;  // the points are fixed at plan creation
-  return run_device(p, q, pot, pt, st, nullptr);
+  Outputs o;
+  o.pot = pot;
+  o.pottarg = pt;
+  return run_device(p, q, o, st, nullptr);
+}
+
+int fgt_plan_execute_device_pgh(fgt_plan* p, const double* q, double* pot, double* grad, double* hess,
+                                double* pottarg, double* gradtarg, double* hesstarg, void* stream) {
+  if (!p) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  Outputs o;
+  o.pot = pot; o.grad = grad; o.hess = hess;
+  o.pottarg = pottarg; o.gradtarg = gradtarg; o.hesstarg = hesstarg;
+  return run_device(p, q, o, st, nullptr);
 }
 
 int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double* pt, double* ms,
@@ -470,7 +529,10 @@ int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double*
   StageTimes T;
   memset(T.ms, 0, sizeof(T.ms));
   if (p->H.P.large_delta) return FGT_ERR_UNSUPPORTED;
-  int r = run_device(p, q, pot, pt, p->ctx->stream, &T);
+  Outputs o;
+  o.pot = pot;
+  o.pottarg = pt;
+  int r = run_device(p, q, o, p->ctx->stream, &T);
   if (r != FGT_OK) return r;
   CKS(cudaStreamSynchronize(p->ctx->stream));
   *ms = T.dom_ms;
@@ -486,7 +548,10 @@ int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const
   StageTimes T;
   memset(T.ms, 0, sizeof(T.ms));
   (void)s; (void)t;
-  int r = run_device(p, q, pot, pt, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
+  Outputs o;
+  o.pot = pot;
+  o.pottarg = pt;
+  int r = run_device(p, q, o, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
   if (r != FGT_OK) return r;
   CKS(cudaStreamSynchronize(p->ctx->stream));
   for (int i = 0; i < 8; i++) ms8[i] = T.ms[i];
@@ -662,11 +727,11 @@ int fgt_transform(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int n
                   const double* rnormal, const double* dipstr, int ifpgh, double* pot, double* grad,
                   double* hess, int nt, const double* targ, int ifpghtarg, double* pottarg,
                   double* gradtarg, double* hesstarg) {
-  (void)rnormal; (void)dipstr; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  (void)rnormal; (void)dipstr;
   if (!ctx) return FGT_ERR_BADARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   return transform_impl(ctx, dim, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh,
-                        pot, nt, targ, ifpghtarg, pottarg);
+                        pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg);
 }
 
 static int fortran_call(int dim, const int* nd, const double* delta, const double* eps, const int* ns,
@@ -738,7 +803,8 @@ static int main_gpu(int dim, const int* nd, const double* delta, const double* e
                     const int* npwlevel, const int* nboxes, const double* boxsize,
                     const double* centers, const int* laddr, const int* isrcse, const int* itargse,
                     const int* nlocal, const double* pmax, const int* npw, const int* ifpgh,
-                    double* pot, const int* ifpghtarg, double* pottarg) {
+                    double* pot, double* grad, double* hess, const int* ifpghtarg, double* pottarg,
+                    double* gradtarg, double* hesstarg) {
   if (!nd || !delta || !eps || !nsource || !ntarget || !itree || !iptr || !nlevels || !npwlevel ||
       !nboxes || !boxsize || !centers || !laddr || !isrcse || !itargse || !nlocal || !pmax || !npw ||
       !ifpgh || !ifpghtarg || !ifcharge || !ifdipole)
@@ -805,14 +871,26 @@ static int main_gpu(int dim, const int* nd, const double* delta, const double* e
     fgt_plan_destroy(p.release());
     return st;
   }
-  std::vector<double> po((size_t)ns * *nd), pt((size_t)nt * *nd);
-  st = fgt_plan_execute_host(p.get(), sourcesort, chargesort, targetsort, po.data(), pt.data());
+  // outputs are incremented (fgt2dmain adds into pot/grad/hess)
+  const size_t nh = dim == 2 ? 3 : 6, n1 = (size_t)ns * *nd, n2 = (size_t)nt * *nd;
+  std::vector<double> po(n1), go(*ifpgh >= 2 ? n1 * dim : 0), ho(*ifpgh >= 3 ? n1 * nh : 0);
+  std::vector<double> pt(n2), gt(*ifpghtarg >= 2 ? n2 * dim : 0), ht(*ifpghtarg >= 3 ? n2 * nh : 0);
+  Outputs h;
+  h.pot = po.data(); h.grad = go.data(); h.hess = ho.data();
+  h.pottarg = pt.data(); h.gradtarg = gt.data(); h.hesstarg = ht.data();
+  st = exec_host(p.get(), chargesort, h);
   fgt_plan_destroy(p.release());
   if (st != FGT_OK) return st;
-  if (*ifpgh == 1 && pot)
-    for (size_t i = 0; i < po.size(); i++) pot[i] += po[i];
-  if (*ifpghtarg == 1 && pottarg)
-    for (size_t i = 0; i < pt.size(); i++) pottarg[i] += pt[i];
+  auto add = [](double* out, const std::vector<double>& v) {
+    if (out)
+      for (size_t i = 0; i < v.size(); i++) out[i] += v[i];
+  };
+  if (*ifpgh >= 1) add(pot, po);
+  if (*ifpgh >= 2) add(grad, go);
+  if (*ifpgh >= 3) add(hess, ho);
+  if (*ifpghtarg >= 1) add(pottarg, pt);
+  if (*ifpghtarg >= 2) add(gradtarg, gt);
+  if (*ifpghtarg >= 3) add(hesstarg, ht);
   return FGT_OK;
 }
 
@@ -830,11 +908,11 @@ int fgt2dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                    double* pot, double* grad, double* hess, const int* ifpghtarg, double* pottarg,
                    double* gradtarg, double* hesstarg) {
   (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
-  (void)ntermsh; (void)ntermmax; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  (void)ntermsh; (void)ntermmax;
   return main_gpu<int>(2, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
                        ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
-                       centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, ifpghtarg,
-                       pottarg);
+                       centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, grad, hess,
+                       ifpghtarg, pottarg, gradtarg, hesstarg);
 }
 
 int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const int* nsource,
@@ -850,11 +928,11 @@ int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                    double* hess, const int* ifpghtarg, double* pottarg, double* gradtarg,
                    double* hesstarg) {
   (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
-  (void)ndiv; (void)ntermsh; (void)ntermmax; (void)grad; (void)hess; (void)gradtarg; (void)hesstarg;
+  (void)ndiv; (void)ntermsh; (void)ntermmax;
   return main_gpu<long long>(3, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
                              ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
-                             centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot,
-                             ifpghtarg, pottarg);
+                             centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, grad,
+                             hess, ifpghtarg, pottarg, gradtarg, hesstarg);
 }
 
 }  // extern "C"
@@ -899,7 +977,7 @@ namespace {
 constexpr double kServerAgeS = 0.05;
 
 long long request_points(const fgt_request& r) {
-  return (r.ifpgh == 1 ? r.ns : 0) + (r.ifpghtarg == 1 && r.targ ? r.nt : 0);
+  return (r.ifpgh >= 1 ? r.ns : 0) + (r.ifpghtarg >= 1 && r.targ ? r.nt : 0);
 }
 
 // blocks until b bytes fit in the pool (or the pool is idle), then takes them
@@ -920,9 +998,19 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
   int st = check_args(r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, 1, 0, r.ifpgh, nt, r.targ,
                       r.ifpghtarg, false);
   if (st != FGT_OK) return st;
+  const size_t nh = r.dim == 2 ? 3 : 6;
+  if ((r.ifpgh >= 1 && r.ns > 0 && !r.pot) || (r.ifpgh >= 2 && r.ns > 0 && !r.grad) ||
+      (r.ifpgh >= 3 && r.ns > 0 && !r.hess) || (r.ifpghtarg >= 1 && nt > 0 && !r.pottarg) ||
+      (r.ifpghtarg >= 2 && nt > 0 && !r.gradtarg) || (r.ifpghtarg >= 3 && nt > 0 && !r.hesstarg))
+    return FGT_ERR_BADARG;
   auto zero = [&] {
-    if (r.ifpgh == 1 && r.ns > 0 && r.pot) memset(r.pot, 0, sizeof(double) * (size_t)r.ns * r.nd);
-    if (r.ifpghtarg == 1 && nt > 0 && r.pottarg) memset(r.pottarg, 0, sizeof(double) * (size_t)nt * r.nd);
+    auto z = [](double* a, size_t n) { if (a && n) memset(a, 0, sizeof(double) * n); };
+    if (r.ifpgh >= 1) z(r.pot, (size_t)r.ns * r.nd);
+    if (r.ifpgh >= 2) z(r.grad, (size_t)r.ns * r.nd * r.dim);
+    if (r.ifpgh >= 3) z(r.hess, (size_t)r.ns * r.nd * nh);
+    if (r.ifpghtarg >= 1) z(r.pottarg, (size_t)nt * r.nd);
+    if (r.ifpghtarg >= 2) z(r.gradtarg, (size_t)nt * r.nd * r.dim);
+    if (r.ifpghtarg >= 3) z(r.hesstarg, (size_t)nt * r.nd * nh);
   };
   if (r.ns == 0) {
     zero();
@@ -931,7 +1019,8 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
   CKS(cudaSetDevice(ctx->device));
   // point arrays (caller order, sorted copies, potentials) and tree scratch
   const long long npts = (long long)r.ns + nt;
-  const long long est_pts = 8LL * ((long long)r.ns * (2 * r.dim + 3 * r.nd) + (long long)nt * (2 * r.dim + 3 * r.nd)) +
+  const long long nc = 2 + out_comps(r.dim, std::max(1, std::max(r.ifpgh, r.ifpghtarg)));
+  const long long est_pts = 8LL * ((long long)r.ns * (2 * r.dim + nc * r.nd) + (long long)nt * (2 * r.dim + nc * r.nd)) +
                             64LL * npts + (1 << 20);
   server_take(S, &S->in_pts, S->budget_pts, est_pts);
   long long plan_bytes = 0;
@@ -948,7 +1037,12 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
   };
   st = plan_create_device_tree(p.get(), r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, nt, r.targ, r.ifpgh,
                                r.ifpghtarg, &admit);
-  if (st == FGT_OK) st = fgt_plan_execute_host(p.get(), r.sources, r.charge, r.targ, r.pot, r.pottarg);
+  if (st == FGT_OK) {
+    Outputs h;
+    h.pot = r.pot; h.grad = r.grad; h.hess = r.hess;
+    h.pottarg = r.pottarg; h.gradtarg = r.gradtarg; h.hesstarg = r.hesstarg;
+    st = exec_host(p.get(), r.charge, h);
+  }
   fgt_plan_destroy(p.release());
   cudaStreamSynchronize(ctx->stream);  // the stream-ordered frees have run
   if (plan_bytes) server_give(S, &S->in_plan, plan_bytes);

@@ -12,6 +12,24 @@ namespace fgtb {
 
 enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
 
+// Outputs per point and density for ifpgh = pgh: 1 (pot), 1 + dim (+ grad),
+// 1 + dim + H (+ Hessian; H = 3 in 2D, 6 in 3D); 0 for pgh = 0.
+inline int out_comps(int dim, int pgh) {
+  return pgh <= 0 ? 0 : pgh == 1 ? 1 : pgh == 2 ? 1 + dim : 1 + dim + (dim == 2 ? 3 : 6);
+}
+
+// Caller-order device outputs of one execute: pot (nd, ns), grad (nd, dim, ns),
+// hess (nd, H, ns) and the same at the targets; the ones the flags do not ask
+// for are ignored.
+struct Outputs {
+  double* pot = nullptr;
+  double* grad = nullptr;
+  double* hess = nullptr;
+  double* pottarg = nullptr;
+  double* gradtarg = nullptr;
+  double* hesstarg = nullptr;
+};
+
 struct MergeGroup {
   int dst, beg, cnt;
 };
@@ -82,8 +100,8 @@ struct DevicePlan {
   double* ssort = nullptr;  // sorted sources (ns, dim)
   double* csort = nullptr;  // sorted charges (ns, nd)
   double* tsort = nullptr;  // sorted targets (nt, dim)
-  double* psort = nullptr;  // sorted pot (ns, nd)
-  double* ptsort = nullptr; // sorted pottarg (nt, nd)
+  double* psort = nullptr;  // sorted source outputs, per point [out_comps(dim, ifpgh)][nd]
+  double* ptsort = nullptr; // sorted target outputs, per point [out_comps(dim, ifpghtarg)][nd]
   double* local0 = nullptr; // large-delta local expansion
   // 3D Hermite form in two kernels: source chunks and their partial blocks
   FormChunk* fchunks = nullptr;
@@ -150,9 +168,9 @@ void device_plan_destroy(DevicePlan& D);
 cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const double* trg,
                                    cudaStream_t stream);
 // Runs charge gather -> stages -> scatter on `stream`.  Device pointers in
-// the caller's order: charge (ns, nd), pot (ns, nd), pottarg (nt, nd).
+// the caller's order: charge (ns, nd) and the outputs.
 // times (optional) receives per-stage milliseconds (synchronises).
-cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
+cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs& out,
                                 int precision, cudaStream_t stream, StageTimes* times);
 
 // Sets *d_flag (device int, not cleared here) when any of x[0, n) is not
@@ -177,7 +195,7 @@ size_t large_delta_noalloc_capacity();
 // true) doubles); otherwise they are added atomically (nd (nlocal0+1)^dim + 4
 // doubles of work; results can differ in the last bits from call to call).
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
-                                const double* trg, double* pot, double* pottarg, double* work,
+                                const double* trg, const Outputs& out, double* work,
                                 cudaStream_t stream, bool deterministic);
 size_t large_delta_work_doubles(const Params& P, bool deterministic);
 

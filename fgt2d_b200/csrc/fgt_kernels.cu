@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include "fgt_device.hpp"
 
@@ -50,8 +51,9 @@ struct KP {
   const double* src;
   const double* chg;
   const double* trg;
-  double* pot;
-  double* pottarg;
+  double* pot;      // sorted outputs of the sources: per point [nc_s][nd]
+  double* pottarg;  // sorted outputs of the targets: per point [nc_t][nd]
+  int nc_s, nc_t;   // components per density written: 1 (pot), 1 + dim (+ grad), + H (+ Hessian)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -98,6 +100,138 @@ __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// ------------------------------------------------------------ outputs: potential, gradient, Hessian
+// PGH = 1 potential, 2 + gradient, 3 + Hessian (the reference's ifpgh).  The
+// components of one density at one point are, in order, pot, d/dx, d/dy
+// (, d/dz), then the Hessian in the reference's order: 2D xx, xy, yy
+// (g2dlevalh_vec); 3D xx, yy, zz, xy, xz, yz (g3dlevalh_vec).  A sorted
+// output row holds the nc components of all nd densities, [nc][nd].
+template <int DIM>
+__host__ __device__ constexpr int nhess() { return DIM == 2 ? 3 : 6; }
+template <int DIM, int PGH>
+__host__ __device__ constexpr int ncomp() { return PGH >= 3 ? 1 + DIM + nhess<DIM>() : PGH == 2 ? 1 + DIM : 1; }
+
+// out row ip += v[0 .. nc) for density ind (nc <= NC: the set's own count)
+template <int NC>
+__device__ __forceinline__ void add_out(double* __restrict__ out, long long ip, int nd, int nc, int ind,
+                                        const double* v) {
+#pragma unroll
+  for (int c = 0; c < NC; c++)
+    if (c < nc) out[(ip * nc + c) * nd + ind] += v[c];
+}
+
+// Horner with derivative chains.  One step with coefficient c of a
+// polynomial in x carries s, s' and s''/2:
+//   s''/2 <- s''/2 x + s',  s' <- s' x + s,  s <- s x + c.
+template <int PGH>
+__device__ __forceinline__ void hstep(double& s, double& sx, double& sxx, double x, double c) {
+  if (PGH >= 3) sxx = fma(sxx, x, sx);
+  if (PGH >= 2) sx = fma(sx, x, s);
+  s = fma(s, x, c);
+}
+// Sums over the rows of a 2D block, r = sum_k y^k s_k(x), with the x chains
+// of the rows: r, r_x, r_y, r_xx/2, r_xy, r_yy/2.
+struct Hor2 {
+  double r = 0, rx = 0, ry = 0, rxx = 0, rxy = 0, ryy = 0;
+};
+template <int PGH>
+__device__ __forceinline__ void hrow(Hor2& a, double y, double s, double sx, double sxx) {
+  if (PGH >= 3) {
+    a.ryy = fma(a.ryy, y, a.ry);
+    a.rxy = fma(a.rxy, y, a.rx);
+    a.rxx = fma(a.rxx, y, sxx);
+  }
+  if (PGH >= 2) {
+    a.ry = fma(a.ry, y, a.r);
+    a.rx = fma(a.rx, y, sx);
+  }
+  a.r = fma(a.r, y, s);
+}
+// Sums over the planes of a 3D block with the planes' 2D chains.
+struct Hor3 {
+  double r = 0, rx = 0, ry = 0, rz = 0, rxx = 0, ryy = 0, rzz = 0, rxy = 0, rxz = 0, ryz = 0;
+};
+template <int PGH>
+__device__ __forceinline__ void hplane(Hor3& a, double z, const Hor2& q) {
+  if (PGH >= 3) {
+    a.rzz = fma(a.rzz, z, a.rz);
+    a.rxz = fma(a.rxz, z, a.rx);
+    a.ryz = fma(a.ryz, z, a.ry);
+    a.rxx = fma(a.rxx, z, q.rxx);
+    a.ryy = fma(a.ryy, z, q.ryy);
+    a.rxy = fma(a.rxy, z, q.rxy);
+  }
+  if (PGH >= 2) {
+    a.rz = fma(a.rz, z, a.r);
+    a.rx = fma(a.rx, z, q.rx);
+    a.ry = fma(a.ry, z, q.ry);
+  }
+  a.r = fma(a.r, z, q.r);
+}
+// Components in physical coordinates: the expansion variable is
+// (x - c) dsq, so each derivative carries a factor dsq.
+template <int PGH>
+__device__ __forceinline__ void hemit(const Hor2& a, double dsq, double* v) {
+  v[0] = a.r;
+  if (PGH >= 2) {
+    v[1] = a.rx * dsq;
+    v[2] = a.ry * dsq;
+  }
+  if (PGH >= 3) {
+    const double d2 = dsq * dsq;
+    v[3] = 2.0 * a.rxx * d2;
+    v[4] = a.rxy * d2;
+    v[5] = 2.0 * a.ryy * d2;
+  }
+}
+template <int PGH>
+__device__ __forceinline__ void hemit(const Hor3& a, double dsq, double* v) {
+  v[0] = a.r;
+  if (PGH >= 2) {
+    v[1] = a.rx * dsq;
+    v[2] = a.ry * dsq;
+    v[3] = a.rz * dsq;
+  }
+  if (PGH >= 3) {
+    const double d2 = dsq * dsq;
+    v[4] = 2.0 * a.rxx * d2;
+    v[5] = 2.0 * a.ryy * d2;
+    v[6] = 2.0 * a.rzz * d2;
+    v[7] = a.rxy * d2;
+    v[8] = a.rxz * d2;
+    v[9] = a.ryz * d2;
+  }
+}
+// Runtime-order evaluation of a real Taylor block: 2D lo[b ld + a],
+// 3D lo[(c Pn + b) ld + a] (a, b, c the powers of x, y, z).
+template <int PGH>
+__device__ void horner2_rt(const double* lo, int ld, int Pn, double x, double y, double dsq, double* v) {
+  Hor2 a;
+  for (int b = Pn - 1; b >= 0; b--) {
+    const double* row = lo + (size_t)b * ld;
+    double s = row[Pn - 1], sx = 0.0, sxx = 0.0;
+    for (int m = Pn - 2; m >= 0; m--) hstep<PGH>(s, sx, sxx, x, row[m]);
+    hrow<PGH>(a, y, s, sx, sxx);
+  }
+  hemit<PGH>(a, dsq, v);
+}
+template <int PGH>
+__device__ void horner3_rt(const double* lo, int ld, int Pn, double x, double y, double z, double dsq,
+                           double* v) {
+  Hor3 a;
+  for (int c = Pn - 1; c >= 0; c--) {
+    Hor2 q;
+    for (int b = Pn - 1; b >= 0; b--) {
+      const double* row = lo + ((size_t)c * Pn + b) * ld;
+      double s = row[Pn - 1], sx = 0.0, sxx = 0.0;
+      for (int m = Pn - 2; m >= 0; m--) hstep<PGH>(s, sx, sxx, x, row[m]);
+      hrow<PGH>(q, y, s, sx, sxx);
+    }
+    hplane<PGH>(a, z, q);
+  }
+  hemit<PGH>(a, dsq, v);
 }
 
 // ------------------------------------------------------------ sort / unsort
@@ -184,13 +318,14 @@ __global__ void k_invperm(const int* __restrict__ perm, int n, int* __restrict__
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) inv[perm[i]] = i;
 }
-// Caller order: out row j = in row iperm[j] (dreorderi, fmmcommon2d.f:29-56),
-// written as a gather so the stores stay coalesced.
+// Caller order: out row j = in row iperm[j] (dreorderi / dreorderiv,
+// fmmcommon2d.f:29-90), written as a gather so the stores stay coalesced.
+// A sorted row is `stride` doubles; out takes the w doubles from `off`.
 __global__ void k_unsort(const double* __restrict__ in, double* __restrict__ out,
-                         const int* __restrict__ iperm, int n, int nd) {
+                         const int* __restrict__ iperm, int n, int stride, int off, int w) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const long long p = iperm[j];
-    for (int c = 0; c < nd; c++) out[(long long)j * nd + c] = in[p * nd + c];
+    for (int c = 0; c < w; c++) out[(long long)j * w + c] = in[p * stride + off + c];
   }
 }
 
@@ -958,9 +1093,13 @@ __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __res
 // Plain FP64 FMAs: on B200 the FP64 FMA pipe and the FP64 MMA share one
 // throughput, and Horner at the exact order does P (E - 1) + P FMAs a point
 // where the 8 x 8 x 4 MMA pads P up to a multiple of 8 in both dimensions.
-template <int NP2>
+// PGH > 1 carries the derivative chains of the Horner sums (hstep, hrow),
+// the gradient and Hessian of g2dlevalg_vec / g2dlevalh_vec
+// (g2drouts.f:905-1085).
+template <int NP2, int PGH>
 __global__ void __launch_bounds__(128) k_eval2d_horner(KP k, const HornerTask* __restrict__ tasks,
                                                        const double* __restrict__ lo_all) {
+  constexpr int NC = ncomp<2, PGH>();
   const HornerTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y, Pn = T.p + 1;
   extern __shared__ double2 lo2[];  // [Pn][NP2]
@@ -969,6 +1108,7 @@ __global__ void __launch_bounds__(128) k_eval2d_horner(KP k, const HornerTask* _
   __syncthreads();
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
   const int ta = threadIdx.x, tb = threadIdx.x + 128;
   if (ta >= T.n) return;
@@ -977,30 +1117,39 @@ __global__ void __launch_bounds__(128) k_eval2d_horner(KP k, const HornerTask* _
   const double2 pb = reinterpret_cast<const double2*>(pts)[T.i0 + (two ? tb : ta)];
   const double x0 = (pa.x - cx) * k.dsq, y0 = (pa.y - cy) * k.dsq;
   const double x1 = (pb.x - cx) * k.dsq, y1 = (pb.y - cy) * k.dsq;
-  double r0 = 0.0, r1 = 0.0;
+  Hor2 a0, a1;
   for (int k1 = Pn - 1; k1 >= 0; k1--) {
     const double2* rw = lo2 + k1 * NP2;
     const double2 ct = rw[NP2 - 1];
-    double s0 = fma(ct.y, x0, ct.x), s1 = fma(ct.y, x1, ct.x);
+    double s0 = ct.y, s1 = ct.y, u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
+    hstep<PGH>(s0, u0, w0, x0, ct.x);
+    hstep<PGH>(s1, u1, w1, x1, ct.x);
 #pragma unroll
     for (int m = NP2 - 2; m >= 0; m--) {
       const double2 c = rw[m];
-      s0 = fma(s0, x0, c.y);
-      s1 = fma(s1, x1, c.y);
-      s0 = fma(s0, x0, c.x);
-      s1 = fma(s1, x1, c.x);
+      hstep<PGH>(s0, u0, w0, x0, c.y);
+      hstep<PGH>(s1, u1, w1, x1, c.y);
+      hstep<PGH>(s0, u0, w0, x0, c.x);
+      hstep<PGH>(s1, u1, w1, x1, c.x);
     }
-    r0 = fma(r0, y0, s0);
-    r1 = fma(r1, y1, s1);
+    hrow<PGH>(a0, y0, s0, u0, w0);
+    hrow<PGH>(a1, y1, s1, u1, w1);
   }
-  out[(size_t)(T.i0 + ta) * k.nd + ind] += r0;
-  if (two) out[(size_t)(T.i0 + tb) * k.nd + ind] += r1;
+  double v[NC];
+  hemit<PGH>(a0, k.dsq, v);
+  add_out<NC>(out, T.i0 + ta, k.nd, nc, ind, v);
+  if (two) {
+    hemit<PGH>(a1, k.dsq, v);
+    add_out<NC>(out, T.i0 + tb, k.nd, nc, ind, v);
+  }
 }
 
 // Orders above 64 (rows longer than 64): the same evaluation with a runtime
 // row length.
+template <int PGH>
 __global__ void __launch_bounds__(128) k_eval2d_horner_any(KP k, const HornerTask* __restrict__ tasks,
                                                            const double* __restrict__ lo_all) {
+  constexpr int NC = ncomp<2, PGH>();
   const HornerTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y, Pn = T.p + 1, E = (Pn + 1) & ~1;
   extern __shared__ double lo1[];  // [Pn][E]
@@ -1009,18 +1158,13 @@ __global__ void __launch_bounds__(128) k_eval2d_horner_any(KP k, const HornerTas
   __syncthreads();
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
   for (int t = threadIdx.x; t < T.n; t += blockDim.x) {
     const double2 pa = reinterpret_cast<const double2*>(pts)[T.i0 + t];
-    const double x = (pa.x - cx) * k.dsq, y = (pa.y - cy) * k.dsq;
-    double r = 0.0;
-    for (int k1 = Pn - 1; k1 >= 0; k1--) {
-      const double* rw = lo1 + k1 * E;
-      double s = rw[Pn - 1];
-      for (int k2 = Pn - 2; k2 >= 0; k2--) s = fma(s, x, rw[k2]);
-      r = fma(r, y, s);
-    }
-    out[(size_t)(T.i0 + t) * k.nd + ind] += r;
+    double v[NC];
+    horner2_rt<PGH>(lo1, E, Pn, (pa.x - cx) * k.dsq, (pa.y - cy) * k.dsq, k.dsq, v);
+    add_out<NC>(out, T.i0 + t, k.nd, nc, ind, v);
   }
 }
 
@@ -1218,9 +1362,10 @@ __global__ void __launch_bounds__(256) k_pw2taylor3d(KP k, const ConvTask* __res
 // is staged in shared memory and each thread evaluates two points by Horner
 // in x along each row, then in y, then in z (g3dlevalp_vec,
 // g3drouts.f:1045-1107), plain FP64 FMAs at the exact order.
-template <int NP2>
+template <int NP2, int PGH>
 __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* __restrict__ tasks,
                                                        const double* __restrict__ lo_all) {
+  constexpr int NC = ncomp<3, PGH>();
   const HornerTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y, Pn = T.p + 1;
   extern __shared__ double2 lo3[];  // [Pn][Pn][NP2]
@@ -1229,6 +1374,7 @@ __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* _
   __syncthreads();
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
   const int ta = threadIdx.x, tb = threadIdx.x + 128;
   if (ta >= T.n) return;
@@ -1236,29 +1382,36 @@ __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* _
   const int pa = T.i0 + ta, pb = T.i0 + (two ? tb : ta);
   const double x0 = (pts[3 * pa] - cx) * k.dsq, y0 = (pts[3 * pa + 1] - cy) * k.dsq, z0 = (pts[3 * pa + 2] - cz) * k.dsq;
   const double x1 = (pts[3 * pb] - cx) * k.dsq, y1 = (pts[3 * pb + 1] - cy) * k.dsq, z1 = (pts[3 * pb + 2] - cz) * k.dsq;
-  double r0 = 0.0, r1 = 0.0;
+  Hor3 a0, a1;
   for (int cc = Pn - 1; cc >= 0; cc--) {
-    double q0 = 0.0, q1 = 0.0;
+    Hor2 q0, q1;
     for (int b = Pn - 1; b >= 0; b--) {
       const double2* rw = lo3 + (cc * Pn + b) * NP2;
       const double2 ct = rw[NP2 - 1];
-      double s0 = fma(ct.y, x0, ct.x), s1 = fma(ct.y, x1, ct.x);
+      double s0 = ct.y, s1 = ct.y, u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
+      hstep<PGH>(s0, u0, w0, x0, ct.x);
+      hstep<PGH>(s1, u1, w1, x1, ct.x);
 #pragma unroll
       for (int m = NP2 - 2; m >= 0; m--) {
         const double2 cf = rw[m];
-        s0 = fma(s0, x0, cf.y);
-        s1 = fma(s1, x1, cf.y);
-        s0 = fma(s0, x0, cf.x);
-        s1 = fma(s1, x1, cf.x);
+        hstep<PGH>(s0, u0, w0, x0, cf.y);
+        hstep<PGH>(s1, u1, w1, x1, cf.y);
+        hstep<PGH>(s0, u0, w0, x0, cf.x);
+        hstep<PGH>(s1, u1, w1, x1, cf.x);
       }
-      q0 = fma(q0, y0, s0);
-      q1 = fma(q1, y1, s1);
+      hrow<PGH>(q0, y0, s0, u0, w0);
+      hrow<PGH>(q1, y1, s1, u1, w1);
     }
-    r0 = fma(r0, z0, q0);
-    r1 = fma(r1, z1, q1);
+    hplane<PGH>(a0, z0, q0);
+    hplane<PGH>(a1, z1, q1);
   }
-  out[(size_t)pa * k.nd + ind] += r0;
-  if (two) out[(size_t)pb * k.nd + ind] += r1;
+  double v[NC];
+  hemit<PGH>(a0, k.dsq, v);
+  add_out<NC>(out, pa, k.nd, nc, ind, v);
+  if (two) {
+    hemit<PGH>(a1, k.dsq, v);
+    add_out<NC>(out, pb, k.nd, nc, ind, v);
+  }
 }
 
 // ------------------------------------------------------------ (c) eval, 3D Taylor in shared memory
@@ -1266,7 +1419,9 @@ __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* _
 // (g3dpw2local_real_vec, g3drouts.f:1774-1938) with x and y passes over the
 // positive half (mirror pre-add) and the z pass over the stored half, then
 // Horner evaluation, two points per thread.
+template <int PGH>
 __global__ void __launch_bounds__(512) k_eval3d_taylor_smem(KP k, const EvalTask* __restrict__ tasks) {
+  constexpr int NC = ncomp<3, PGH>();
   const EvalTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
   const int npw = k.npw, n2 = k.n2;
@@ -1318,32 +1473,14 @@ __global__ void __launch_bounds__(512) k_eval3d_taylor_smem(KP k, const EvalTask
   __syncthreads();
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
-  for (int i0 = threadIdx.x; i0 < T.n; i0 += 2 * blockDim.x) {
-    const int i1 = i0 + blockDim.x;
-    const bool two = i1 < T.n;
-    const int p0 = T.i0 + i0, p1 = T.i0 + (two ? i1 : i0);
-    const double x0 = (pts[3 * p0] - cx) * k.dsq, y0 = (pts[3 * p0 + 1] - cy) * k.dsq, z0 = (pts[3 * p0 + 2] - cz) * k.dsq;
-    const double x1 = (pts[3 * p1] - cx) * k.dsq, y1 = (pts[3 * p1 + 1] - cy) * k.dsq, z1 = (pts[3 * p1 + 2] - cz) * k.dsq;
-    double rz0 = 0.0, rz1 = 0.0;
-    for (int c = Pn - 1; c >= 0; c--) {
-      double ry0 = 0.0, ry1 = 0.0;
-      for (int b = Pn - 1; b >= 0; b--) {
-        const double* row = lo + Pn * (b + Pn * c);
-        double rx0 = 0.0, rx1 = 0.0;
-        for (int a = Pn - 1; a >= 0; a--) {
-          const double cf = row[a];
-          rx0 = fma(rx0, x0, cf);
-          rx1 = fma(rx1, x1, cf);
-        }
-        ry0 = fma(ry0, y0, rx0);
-        ry1 = fma(ry1, y1, rx1);
-      }
-      rz0 = fma(rz0, z0, ry0);
-      rz1 = fma(rz1, z1, ry1);
-    }
-    out[(size_t)p0 * k.nd + ind] += rz0;
-    if (two) out[(size_t)p1 * k.nd + ind] += rz1;
+  for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
+    const int ip = T.i0 + i;
+    double v[NC];
+    horner3_rt<PGH>(lo, Pn, Pn, (pts[3 * ip] - cx) * k.dsq, (pts[3 * ip + 1] - cy) * k.dsq,
+                    (pts[3 * ip + 2] - cz) * k.dsq, k.dsq, v);
+    add_out<NC>(out, ip, k.nd, nc, ind, v);
   }
 }
 
@@ -1459,35 +1596,112 @@ __global__ void k_split(KP k, const ShiftTask* __restrict__ tasks) {
   }
 }
 
+// ------------------------------------------------------------ (c) eval, plane-wave route derivatives
+// A pair of nodes +t, -t with coefficients A (of e^{itx}) and B (of e^{-itx})
+// contributes A w + B conj(w), w = e^{itx}; its x derivatives are
+// i t (A w - B conj(w)) and -t^2 (A w + B conj(w)).  PwAcc keeps
+//   S0 = sum (A w + B w*),  S1 = sum t (A w - B w*),  S2 = sum t^2 (A w + B w*)
+// (the derivative orders the evaluation needs), so that d/dx = i S1 and
+// d2/dx2 = -S2 (the ww1x / ww1xx factors of g2dpwevalg_vec / g2dpwevalh_vec,
+// g2drouts.f:1973-2200, and g3dpwevalg/h_vec, g3drouts.f:2369-2660).
+template <int ORD>
+struct PwAcc {
+  double2 s[ORD + 1];
+  __device__ __forceinline__ PwAcc() {
+#pragma unroll
+    for (int i = 0; i <= ORD; i++) s[i] = make_double2(0.0, 0.0);
+  }
+  // add A w + B conj(w) at node t
+  __device__ __forceinline__ void add(double2 A, double2 B, double2 w, double t) {
+    if (ORD == 0) {  // the potential alone: two complex FMAs
+      s[0] = cfmac(B, w, cfma(A, w, s[0]));
+      return;
+    }
+    const double2 p = cmul(A, w), m = cmulc(B, w);  // A w, B conj(w)
+    const double2 sp = make_double2(p.x + m.x, p.y + m.y);
+    s[0].x += sp.x;
+    s[0].y += sp.y;
+    if (ORD >= 1) {
+      s[1].x = fma(t, p.x - m.x, s[1].x);
+      s[1].y = fma(t, p.y - m.y, s[1].y);
+    }
+    if (ORD >= 2) {
+      const double t2 = t * t;
+      s[2].x = fma(t2, sp.x, s[2].x);
+      s[2].y = fma(t2, sp.y, s[2].y);
+    }
+  }
+};
+
 // ------------------------------------------------------------ (c) eval, 2D plane-wave route
 // One CTA per (leaf, point set, density): direct plane-wave sum at every point
 // with e^{i t x} built by the recurrence of g2dpwevalp_vec (g2drouts.f:1887-1966),
 // on the levels where the reference picks it (nlocal > 50, fgt2d.f:1166).
+// The stored half is x > 0; y runs over both signs.  With z_j = sum over x
+// nodes of e^{i t_x x} t_x^a (y-sum of derivative order b), the outputs are
+//   pot = 2 Re z(0,0), g_x = -2 Im z(1,0), g_y = -2 Im z(0,1),
+//   h_xx = -2 Re z(2,0), h_xy = -2 Re z(1,1), h_yy = -2 Re z(0,2)
+// times dsq per derivative.
+template <int PGH>
 __global__ void __launch_bounds__(256) k_eval2d(KP k, const EvalTask* __restrict__ tasks) {
+  constexpr int NC = ncomp<2, PGH>(), ORD = PGH - 1;
   const EvalTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
   const int n2 = k.n2;
   const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
   for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
     const int ip = T.i0 + i;
     const double x = (pts[2 * ip] - cx) * k.dsq, y = (pts[2 * ip + 1] - cy) * k.dsq;
     const double2 ex = cexpi(k.t1 * x), ey = cexpi(k.t1 * y);
     const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey);
-    double2 z = make_double2(0.0, 0.0), w1 = ex;
+    // z[0] = (0,0), z[1] = (1,0), z[2] = (0,1), z[3] = (2,0), z[4] = (1,1), z[5] = (0,2)
+    double2 z[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) z[c] = make_double2(0.0, 0.0);
+    double2 w1 = ex;
     for (int kx = 0; kx < n2; kx++) {
-      double2 s = make_double2(0.0, 0.0), w2 = ey;
+      const double tx = (2 * kx + 1) * k.t1;
+      PwAcc<ORD> sy;
+      double2 w2 = ey;
       for (int ky = 0; ky < n2; ky++) {
-        s = cfma(L[kx + n2 * ky], w2, s);
-        s = cfmac(L[kx + n2 * (ky + n2)], w2, s);
+        sy.add(L[kx + n2 * ky], L[kx + n2 * (ky + n2)], w2, (2 * ky + 1) * k.t1);
         w2 = cmul(w2, eyy);
       }
-      z = cfma(s, w1, z);
+      const double2 a0 = cmul(sy.s[0], w1);
+      z[0].x += a0.x;
+      z[0].y += a0.y;
+      if (PGH >= 2) {
+        const double2 a1 = cmul(sy.s[ORD >= 1 ? 1 : 0], w1);
+        z[1].x = fma(tx, a0.x, z[1].x);
+        z[1].y = fma(tx, a0.y, z[1].y);
+        z[2].x += a1.x;
+        z[2].y += a1.y;
+        if (PGH >= 3) {
+          const double2 a2 = cmul(sy.s[ORD >= 2 ? 2 : 0], w1);
+          z[3].x = fma(tx * tx, a0.x, z[3].x);
+          z[4].x = fma(tx, a1.x, z[4].x);
+          z[5].x += a2.x;
+        }
+      }
       w1 = cmul(w1, exx);
     }
-    out[(size_t)ip * k.nd + ind] += 2.0 * z.x;
+    double v[NC];
+    v[0] = 2.0 * z[0].x;
+    if (PGH >= 2) {
+      v[1] = -2.0 * z[1].y * k.dsq;
+      v[2] = -2.0 * z[2].y * k.dsq;
+    }
+    if (PGH >= 3) {
+      const double d2 = k.dsq * k.dsq;
+      v[3] = -2.0 * z[3].x * d2;
+      v[4] = -2.0 * z[4].x * d2;
+      v[5] = -2.0 * z[5].x * d2;
+    }
+    add_out<NC>(out, ip, k.nd, nc, ind, v);
   }
 }
 
@@ -1495,8 +1709,10 @@ __global__ void __launch_bounds__(256) k_eval2d(KP k, const EvalTask* __restrict
 // Taylor route, persistent CTAs: plane wave -> Taylor through the scratch
 // slab (x, y passes) and a z pass into shared memory
 // (g3dpw2local_real_vec, g3drouts.f:1774-1938), then Horner evaluation.
+template <int PGH>
 __global__ void __launch_bounds__(256) k_eval3d_taylor(KP k, const EvalTask* __restrict__ tasks, int ntasks,
                                                        double2* __restrict__ scratch, size_t slab) {
+  constexpr int NC = ncomp<3, PGH>();
   const int npw = k.npw, n2 = k.n2;
   double2* U1 = scratch + slab * blockIdx.x;
   for (int w = blockIdx.x; w < ntasks * k.nd; w += gridDim.x) {
@@ -1548,36 +1764,37 @@ __global__ void __launch_bounds__(256) k_eval3d_taylor(KP k, const EvalTask* __r
     __syncthreads();
     const double* pts = T.set ? k.trg : k.src;
     double* out = T.set ? k.pottarg : k.pot;
+    const int nc = T.set ? k.nc_t : k.nc_s;
     const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
     for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
       const int ip = T.i0 + i;
-      const double x = (pts[3 * ip] - cx) * k.dsq, y = (pts[3 * ip + 1] - cy) * k.dsq,
-                   z = (pts[3 * ip + 2] - cz) * k.dsq;
-      double rz = 0.0;
-      for (int c = Pn - 1; c >= 0; c--) {
-        double ry = 0.0;
-        for (int b = Pn - 1; b >= 0; b--) {
-          const double* row = lo + Pn * (b + Pn * c);
-          double rx = 0.0;
-          for (int a = Pn - 1; a >= 0; a--) rx = fma(rx, x, row[a]);
-          ry = fma(ry, y, rx);
-        }
-        rz = fma(rz, z, ry);
-      }
-      out[(size_t)ip * k.nd + ind] += rz;
+      double v[NC];
+      horner3_rt<PGH>(lo, Pn, Pn, (pts[3 * ip] - cx) * k.dsq, (pts[3 * ip + 1] - cy) * k.dsq,
+                      (pts[3 * ip + 2] - cz) * k.dsq, k.dsq, v);
+      add_out<NC>(out, ip, k.nd, nc, ind, v);
     }
     __syncthreads();
   }
 }
 
-// PW route (g3dpwevalp_vec, g3drouts.f:2268-2362): one CTA per task.
+// PW route (g3dpwevalp_vec, g3drouts.f:2268-2362): one CTA per task.  x and y
+// run over both signs (PwAcc), z over the stored half, whose nodes are
+// negative: e^{-i t z} has z derivatives -i t and -t^2.  With Y(a,b) the x/y
+// sums of derivative orders a, b and F(a,b) = sum_z Y(a,b) e^{-itz},
+// G(a,b) = sum_z t Y(a,b) e^{-itz}, Gz2 = sum_z t^2 Y(0,0) e^{-itz}:
+//   pot = 2 Re F00, g = (-2 Im F10, -2 Im F01, 2 Im G00),
+//   h_xx, h_yy, h_zz = -2 Re F20, -2 Re F02, -2 Re Gz2,
+//   h_xy, h_xz, h_yz = -2 Re F11, 2 Re G10, 2 Re G01   (times dsq per derivative).
+template <int PGH>
 __global__ void __launch_bounds__(256) k_eval3d_pw(KP k, const EvalTask* __restrict__ tasks) {
+  constexpr int NC = ncomp<3, PGH>(), ORD = PGH - 1;
   const EvalTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
   const int npw = k.npw, n2 = k.n2;
   const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
   for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
     const int ip = T.i0 + i;
@@ -1585,29 +1802,72 @@ __global__ void __launch_bounds__(256) k_eval3d_pw(KP k, const EvalTask* __restr
                  z = (pts[3 * ip + 2] - cz) * k.dsq;
     const double2 ex = cexpi(k.t1 * x), ey = cexpi(k.t1 * y), ez = cexpi(k.t1 * z);
     const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey), ezz = cmul(ez, ez);
-    double2 acc = make_double2(0.0, 0.0), w3 = ez;
+    // acc: [0] F00, [1] F10, [2] F01, [3] G00, [4] F20, [5] F02, [6] Gz2, [7] F11, [8] G10, [9] G01
+    double2 acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] = make_double2(0.0, 0.0);
+    double2 w3 = ez;
     for (int mz = 0; mz < n2; mz++) {
       // z index n2-1-mz holds node -(2 mz + 1) t1
-      double2 sy = make_double2(0.0, 0.0), w2 = ey;
+      const double tz = (2 * mz + 1) * k.t1;
+      // Y[b][a]: y order b of the x order a sums
+      PwAcc<ORD> Y[ORD + 1];
+      double2 w2 = ey;
       for (int my = 0; my < n2; my++) {
+        const double ty = (2 * my + 1) * k.t1;
         const double2* rp = L + (size_t)npw * ((n2 + my) + (size_t)npw * (n2 - 1 - mz));
         const double2* rm = L + (size_t)npw * ((n2 - 1 - my) + (size_t)npw * (n2 - 1 - mz));
-        double2 sp = make_double2(0.0, 0.0), sn = make_double2(0.0, 0.0), w1 = ex;
+        PwAcc<ORD> sp, sn;
+        double2 w1 = ex;
         for (int mx = 0; mx < n2; mx++) {
-          sp = cfma(rp[n2 + mx], w1, sp);
-          sp = cfmac(rp[n2 - 1 - mx], w1, sp);
-          sn = cfma(rm[n2 + mx], w1, sn);
-          sn = cfmac(rm[n2 - 1 - mx], w1, sn);
+          const double tx = (2 * mx + 1) * k.t1;
+          sp.add(rp[n2 + mx], rp[n2 - 1 - mx], w1, tx);
+          sn.add(rm[n2 + mx], rm[n2 - 1 - mx], w1, tx);
           w1 = cmul(w1, exx);
         }
-        sy = cfma(sp, w2, sy);
-        sy = cfmac(sn, w2, sy);
+#pragma unroll
+        for (int a = 0; a <= ORD; a++) Y[a].add(sp.s[a], sn.s[a], w2, ty);
         w2 = cmul(w2, eyy);
       }
-      acc = cfmac(sy, w3, acc);
+      // conj(w3) factors
+      const double2 f00 = cmulc(Y[0].s[0], w3);
+      acc[0].x += f00.x;
+      acc[0].y += f00.y;
+      if (PGH >= 2) {
+        const double2 f10 = cmulc(Y[ORD >= 1 ? 1 : 0].s[0], w3), f01 = cmulc(Y[0].s[ORD >= 1 ? 1 : 0], w3);
+        acc[1].y += f10.y;
+        acc[2].y += f01.y;
+        acc[3].y = fma(tz, f00.y, acc[3].y);
+        if (PGH >= 3) {
+          const double2 f20 = cmulc(Y[ORD >= 2 ? 2 : 0].s[0], w3), f02 = cmulc(Y[0].s[ORD >= 2 ? 2 : 0], w3);
+          const double2 f11 = cmulc(Y[ORD >= 1 ? 1 : 0].s[ORD >= 1 ? 1 : 0], w3);
+          acc[4].x += f20.x;
+          acc[5].x += f02.x;
+          acc[6].x = fma(tz * tz, f00.x, acc[6].x);
+          acc[7].x += f11.x;
+          acc[8].x = fma(tz, f10.x, acc[8].x);
+          acc[9].x = fma(tz, f01.x, acc[9].x);
+        }
+      }
       w3 = cmul(w3, ezz);
     }
-    out[(size_t)ip * k.nd + ind] += 2.0 * acc.x;
+    double v[NC];
+    v[0] = 2.0 * acc[0].x;
+    if (PGH >= 2) {
+      v[1] = -2.0 * acc[1].y * k.dsq;
+      v[2] = -2.0 * acc[2].y * k.dsq;
+      v[3] = 2.0 * acc[3].y * k.dsq;
+    }
+    if (PGH >= 3) {
+      const double d2 = k.dsq * k.dsq;
+      v[4] = -2.0 * acc[4].x * d2;
+      v[5] = -2.0 * acc[5].x * d2;
+      v[6] = -2.0 * acc[6].x * d2;
+      v[7] = -2.0 * acc[7].x * d2;
+      v[8] = 2.0 * acc[8].x * d2;
+      v[9] = 2.0 * acc[9].x * d2;
+    }
+    add_out<NC>(out, ip, k.nd, nc, ind, v);
   }
 }
 
@@ -1660,10 +1920,42 @@ __device__ __forceinline__ int range_slot_source(const RangeChunk& C, int s) {
 // g2ddirect.f:32-76; g3d_directcp_vec, g3ddirect.f:3-49): the chunk's source
 // ranges are staged through the warp's shared memory in batches of 256, and
 // g lanes per point (g n <= 32) split the sources of that point.
-// pot += q exp(-r^2/delta) when r^2 < dmax, all in FP64.
-template <int DIM>
+// pot += q exp(-r^2/delta) when r^2 < dmax, all in FP64; with PGH > 1 the
+// gradient and Hessian per pair as g2d_directcg/ch_vec (g2ddirect.f:83-212)
+// and g3d_directcg/ch_vec (g3ddirect.f:56-203): with rfac = -2/delta and
+// d = target - source, grad += rfac d_i r, hess_ii += (rfac + (rfac d_i)^2) r,
+// hess_ij += (rfac d_i)(rfac d_j) r, r = q exp(-|d|^2/delta).
+template <int DIM, int PGH>
+__device__ __forceinline__ void pair_terms(double* acc, double r, const double* d, double rfac) {
+  acc[0] += r;
+  if (PGH >= 2) {
+    double g[DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; i++) {
+      g[i] = rfac * d[i];
+      acc[1 + i] = fma(g[i], r, acc[1 + i]);
+    }
+    if (PGH >= 3) {
+      double* h = acc + 1 + DIM;
+      if (DIM == 2) {
+        h[0] = fma(fma(g[0], g[0], rfac), r, h[0]);
+        h[1] = fma(g[0] * g[1], r, h[1]);
+        h[2] = fma(fma(g[1], g[1], rfac), r, h[2]);
+      } else {
+        h[0] = fma(fma(g[0], g[0], rfac), r, h[0]);
+        h[1] = fma(fma(g[1], g[1], rfac), r, h[1]);
+        h[2] = fma(fma(g[DIM - 1], g[DIM - 1], rfac), r, h[2]);
+        h[3] = fma(g[0] * g[1], r, h[3]);
+        h[4] = fma(g[0] * g[DIM - 1], r, h[4]);
+        h[5] = fma(g[1] * g[DIM - 1], r, h[5]);
+      }
+    }
+  }
+}
+template <int DIM, int PGH>
 __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict__ tasks, int ntask,
                                                 const SrcRange* __restrict__ ranges) {
+  constexpr int NC = ncomp<DIM, PGH>();
   constexpr int CAP = 256;  // sources staged per warp and batch
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * 4 + warp;
@@ -1682,11 +1974,14 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
   const bool act = tt < T.n;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   const int ip = T.i0 + (act ? tt : 0);
   const double tx = pts[DIM * ip], ty = pts[DIM * ip + 1];
   const double tz = DIM == 3 ? pts[DIM * ip + 2] : 0.0;
-  const double ninv = -1.0 / k.delta;
-  double acc = 0.0;
+  const double ninv = -1.0 / k.delta, rfac = -2.0 / k.delta;
+  double acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = 0.0;
   for (int rc = 0; rc < T.cnt; rc += 32) {
     const RangeChunk C = load_range_chunk(ranges, T.off, T.cnt, rc, lane);
     for (int b0 = 0; b0 < C.tot; b0 += CAP) {
@@ -1712,17 +2007,27 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
         for (int t = sub; t < m; t += g) {
           const double dx = tx - sx[t], dy = ty - sy[t];
           double rr = fma(dx, dx, dy * dy);
+          double dz = 0.0;
           if (DIM == 3) {
-            const double dz = tz - sz[t];
+            dz = tz - sz[t];
             rr = fma(dz, dz, rr);
           }
-          if (rr < k.dmax) acc = fma(exp(rr * ninv), sq[t], acc);
+          if (rr < k.dmax) {
+            if (PGH == 1) {
+              acc[0] = fma(exp(rr * ninv), sq[t], acc[0]);
+            } else {
+              const double d[3] = {dx, dy, dz};
+              pair_terms<DIM, PGH>(acc, exp(rr * ninv) * sq[t], d, rfac);
+            }
+          }
         }
       }
     }
   }
-  for (int o = 1; o < g; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (act && sub == 0) out[(size_t)ip * k.nd + ind] += acc;
+#pragma unroll
+  for (int c = 0; c < NC; c++)
+    for (int o = 1; o < g; o <<= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  if (act && sub == 0) add_out<NC>(out, ip, k.nd, nc, ind, acc);
 }
 
 // Mixed form of the near field (eps >= 1e-6): the same task structure with
@@ -1734,11 +2039,17 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
 // so a staged source is read from shared memory once for four pairs; g lanes
 // per target group (g * groups <= 32) split the sources.  Groups of four
 // sources are summed in FP32 per target and added into FP64 accumulators.
-template <int DIM>
+// With PGH > 1 the FP32 partials are, per target, sum e q, sum e q d_i and
+// (PGH = 3) sum e q d_i d_j in the scaled differences d = (x_t - x_s) cs;
+// they become the gradient rfac/cs sum e q d_i and the Hessian
+// rfac sum e q + (rfac/cs)^2 sum e q d_i^2 (diagonal), (rfac/cs)^2 sum e q d_i d_j
+// in FP64 (the per-pair terms of g2d_directch_vec / g3d_directch_vec).
+template <int DIM, int PGH>
 __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __restrict__ tasks, int ntask,
                                                       const SrcRange* __restrict__ ranges, double cs,
                                                       float amax) {
-  constexpr int CAP = 256, NTL = 4;
+  constexpr int CAP = 256, NTL = PGH == 1 ? 4 : PGH == 2 ? 2 : 1;
+  constexpr int NC = ncomp<DIM, PGH>();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * 4 + warp;
   __shared__ float fsm[4][(2 * DIM + 1) * CAP];
@@ -1755,14 +2066,16 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
   const bool act = tt < ngr;
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
   double o[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; d++) o[d] = pts[DIM * T.i0 + d];
   float th[NTL][DIM], tl[NTL][DIM];
-  double acc[NTL];
+  double acc[NTL][NC];
 #pragma unroll
   for (int v = 0; v < NTL; v++) {
-    acc[v] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[v][c] = 0.0;
     const int it = min(tt * NTL + v, T.n - 1);
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
@@ -1797,9 +2110,11 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
     __syncwarp();
     if (act) {
       for (int t = sub; t < m; t += 4 * g) {
-        float part[NTL];
+        float part[NTL][NC];
 #pragma unroll
-        for (int v = 0; v < NTL; v++) part[v] = 0.0f;
+        for (int v = 0; v < NTL; v++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) part[v][c] = 0.0f;
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const int tu = t + u * g;
@@ -1813,31 +2128,81 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
             const float q = sq[tu];
 #pragma unroll
             for (int v = 0; v < NTL; v++) {
-              float a = 0.0f;
+              float a = 0.0f, dd[DIM];
 #pragma unroll
               for (int d = 0; d < DIM; d++) {
-                const float dx = (th[v][d] - sH[d]) + (tl[v][d] - sL[d]);
-                a = fmaf(dx, dx, a);
+                dd[d] = (th[v][d] - sH[d]) + (tl[v][d] - sL[d]);
+                a = fmaf(dd[d], dd[d], a);
               }
               const float e = ex2_approx(-a);
-              part[v] = a < amax ? fmaf(e, q, part[v]) : part[v];
+              if (PGH == 1) {
+                part[v][0] = a < amax ? fmaf(e, q, part[v][0]) : part[v][0];
+              } else if (a < amax) {
+                const float r = e * q;
+                part[v][0] += r;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) part[v][1 + d] = fmaf(dd[d], r, part[v][1 + d]);
+                if (PGH >= 3) {
+                  float* h = part[v] + 1 + DIM;
+                  if (DIM == 2) {
+                    h[0] = fmaf(dd[0] * dd[0], r, h[0]);
+                    h[1] = fmaf(dd[0] * dd[1], r, h[1]);
+                    h[2] = fmaf(dd[1] * dd[1], r, h[2]);
+                  } else {
+                    h[0] = fmaf(dd[0] * dd[0], r, h[0]);
+                    h[1] = fmaf(dd[1] * dd[1], r, h[1]);
+                    h[2] = fmaf(dd[DIM - 1] * dd[DIM - 1], r, h[2]);
+                    h[3] = fmaf(dd[0] * dd[1], r, h[3]);
+                    h[4] = fmaf(dd[0] * dd[DIM - 1], r, h[4]);
+                    h[5] = fmaf(dd[1] * dd[DIM - 1], r, h[5]);
+                  }
+                }
+              }
             }
           }
         }
 #pragma unroll
-        for (int v = 0; v < NTL; v++) acc[v] += (double)part[v];
+        for (int v = 0; v < NTL; v++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) acc[v][c] += (double)part[v][c];
       }
     }
    }
   }
 #pragma unroll
   for (int v = 0; v < NTL; v++)
-    for (int o2 = 1; o2 < g; o2 <<= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o2);
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      for (int o2 = 1; o2 < g; o2 <<= 1) acc[v][c] += __shfl_xor_sync(0xffffffffu, acc[v][c], o2);
   if (act && sub == 0) {
+    // scaled sums -> physical: d = dx cs, rfac = -2/delta
+    const double rfac = -2.0 / k.delta, c1 = rfac / cs, c2 = c1 * c1;
 #pragma unroll
     for (int v = 0; v < NTL; v++) {
       const int it = tt * NTL + v;
-      if (it < T.n) out[(size_t)(T.i0 + it) * k.nd + ind] += acc[v];
+      if (it >= T.n) continue;
+      double w[NC];
+      w[0] = acc[v][0];
+      if (PGH >= 2)
+#pragma unroll
+        for (int d = 0; d < DIM; d++) w[1 + d] = c1 * acc[v][1 + d];
+      if (PGH >= 3) {
+        const double* h = acc[v] + 1 + DIM;
+        double* hw = w + 1 + DIM;
+        if (DIM == 2) {
+          hw[0] = fma(c2, h[0], rfac * w[0]);
+          hw[1] = c2 * h[1];
+          hw[2] = fma(c2, h[2], rfac * w[0]);
+        } else {
+          hw[0] = fma(c2, h[0], rfac * w[0]);
+          hw[1] = fma(c2, h[1], rfac * w[0]);
+          hw[2] = fma(c2, h[2], rfac * w[0]);
+          hw[3] = c2 * h[3];
+          hw[4] = c2 * h[4];
+          hw[5] = c2 * h[5];
+        }
+      }
+      add_out<NC>(out, T.i0 + it, k.nd, nc, ind, w);
     }
   }
 }
@@ -1910,28 +2275,29 @@ __global__ void k_ld_sum(int nent, int nparts, const double* __restrict__ partia
     local[(size_t)ind * nent + e] = a;
   }
 }
-template <int DIM>
-__global__ void k_ld_eval(KP k, int n, const double* __restrict__ pts, double* __restrict__ out, int p,
+// Taylor evaluation at every point (g2dlevalp/g/h_vec, g3dlevalp/g/h_vec);
+// outputs in the caller's layout: pot(nd, n), grad(nd, dim, n), hess(nd, H, n).
+template <int DIM, int PGH>
+__global__ void k_ld_eval(KP k, int n, const double* __restrict__ pts, double* __restrict__ pot,
+                          double* __restrict__ grad, double* __restrict__ hess, int p,
                           const double* __restrict__ cen, const double* __restrict__ local) {
+  constexpr int NC = ncomp<DIM, PGH>(), NH = nhess<DIM>();
   const int Pn = p + 1;
   const int nent = DIM == 2 ? Pn * Pn : Pn * Pn * Pn;
-  const int ind = blockIdx.y;
+  const int ind = blockIdx.y, nd = k.nd;
   const double* lo = local + (size_t)ind * nent;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double x = (pts[DIM * i] - cen[0]) * k.dsq, y = (pts[DIM * i + 1] - cen[1]) * k.dsq;
-    const double z = DIM == 3 ? (pts[DIM * i + 2] - cen[2]) * k.dsq : 0.0;
-    double rz = 0.0;
-    for (int c = (DIM == 3 ? Pn - 1 : 0); c >= 0; c--) {
-      double ry = 0.0;
-      for (int b = Pn - 1; b >= 0; b--) {
-        const double* row = lo + Pn * (b + Pn * c);
-        double rx = 0.0;
-        for (int a = Pn - 1; a >= 0; a--) rx = fma(rx, x, row[a]);
-        ry = fma(ry, y, rx);
-      }
-      rz = DIM == 3 ? fma(rz, z, ry) : ry;
-    }
-    out[(size_t)i * k.nd + ind] = rz;
+    double v[NC];
+    if (DIM == 2) horner2_rt<PGH>(lo, Pn, Pn, x, y, k.dsq, v);
+    else horner3_rt<PGH>(lo, Pn, Pn, x, y, (pts[DIM * i + 2] - cen[DIM - 1]) * k.dsq, k.dsq, v);
+    pot[(size_t)i * nd + ind] = v[0];
+    if (PGH >= 2)
+#pragma unroll
+      for (int d = 0; d < DIM; d++) grad[((size_t)i * DIM + d) * nd + ind] = v[1 + d];
+    if (PGH >= 3)
+#pragma unroll
+      for (int c = 0; c < NH; c++) hess[((size_t)i * NH + c) * nd + ind] = v[1 + DIM + c];
   }
 }
 
@@ -2208,7 +2574,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
-                 al(nt * dim * 8) + al(ns * nd * 8) + al(nt * nd * 8) +
+                 al(nt * dim * 8) + al(ns * nd * out_comps(dim, P.ifpgh) * 8) +
+                 al(nt * nd * out_comps(dim, P.ifpghtarg) * 8) +
                  al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
                  bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
                  al(lo_doubles * 8) + 4096;
@@ -2311,8 +2678,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.ssort = reinterpret_cast<double*>(cur); cur += al(ns * dim * 8);
   D.csort = reinterpret_cast<double*>(cur); cur += al(ns * nd * 8);
   D.tsort = reinterpret_cast<double*>(cur); cur += al(nt * dim * 8);
-  D.psort = reinterpret_cast<double*>(cur); cur += al(ns * nd * 8);
-  D.ptsort = reinterpret_cast<double*>(cur); cur += al(nt * nd * 8);
+  D.psort = reinterpret_cast<double*>(cur); cur += al(ns * nd * out_comps(dim, P.ifpgh) * 8);
+  D.ptsort = reinterpret_cast<double*>(cur); cur += al(nt * nd * out_comps(dim, P.ifpghtarg) * 8);
   D.scratch = reinterpret_cast<double2*>(cur); cur += al((size_t)D.scratch_ctas * D.scratch_per_cta * 16);
   CK(cudaStreamSynchronize(s));
   return cudaSuccess;
@@ -2332,6 +2699,8 @@ static KP make_kp(const DevicePlan& D) {
   k.centers = D.centers; k.h2x = D.h2x; k.x2l = D.x2l; k.ws = nullptr;
   k.wms = D.wms; k.wsh = D.wsh; k.mp = D.mp; k.loc = D.loc;
   k.src = D.ssort; k.chg = D.csort; k.trg = D.tsort; k.pot = D.psort; k.pottarg = D.ptsort;
+  k.nc_s = out_comps(P.dim, P.ifpgh);
+  k.nc_t = out_comps(P.dim, P.ifpghtarg);
   return k;
 }
 
@@ -2362,10 +2731,23 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
   return cudaGetLastError();
 }
 
-cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, double* pottarg,
+// Runs launch(std::integral_constant<int, G>) with G = pgh in {1, 2, 3}.
+template <class F>
+cudaError_t with_pgh(int pgh, F&& launch) {
+  switch (pgh) {
+    case 1: return launch(std::integral_constant<int, 1>());
+    case 2: return launch(std::integral_constant<int, 2>());
+    case 3: return launch(std::integral_constant<int, 3>());
+    default: return cudaErrorNotSupported;
+  }
+}
+
+cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs& outs,
                                 int precision, cudaStream_t st, StageTimes* times) {
   const Params& P = D.P;
   KP k = make_kp(D);
+  // the derivative order the kernels compute: the larger of the two sets'
+  const int pgh = std::max(1, std::max(P.ifpgh, P.ifpghtarg));
   k.ws = D.h2x;  // row j = 0 of h2x holds the weights
   const int nd = P.nd;
   cudaEvent_t ev[9], dev0 = nullptr, dev1 = nullptr;
@@ -2386,8 +2768,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
     k_gather_pts<<<gb, 256, 0, st>>>(nullptr, chg, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
-  if (P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * 8, st));
-  if (P.ifpghtarg > 0 && P.nt > 0) CK(cudaMemsetAsync(D.ptsort, 0, (size_t)P.nt * nd * 8, st));
+  if (P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * k.nc_s * 8, st));
+  if (P.ifpghtarg > 0 && P.nt > 0) CK(cudaMemsetAsync(D.ptsort, 0, (size_t)P.nt * nd * k.nc_t * 8, st));
   mark(1);
   const int n2 = P.npw / 2;
   if (!P.all_direct) {
@@ -2546,27 +2928,40 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         const HornerTask* tk = D.horner + G.beg;
         const size_t sh = (size_t)Pn * np2 * 16;
         if (sh > 227 * 1024) return cudaErrorNotSupported;
-        switch (np2) {
+        {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+          constexpr int PG = decltype(G)::value;
+          switch (np2) {
 #define HORNER_CASE(N)                                                                            \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_eval2d_horner<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_eval2d_horner<N><<<g, 128, sh, st>>>(k, tk, D.lo);                                          \
+    CK(cudaFuncSetAttribute(k_eval2d_horner<N, PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_eval2d_horner<N, PG><<<g, 128, sh, st>>>(k, tk, D.lo);                                      \
     break;
-          HORNER_CASE(1) HORNER_CASE(2) HORNER_CASE(3) HORNER_CASE(4) HORNER_CASE(5) HORNER_CASE(6)
-          HORNER_CASE(7) HORNER_CASE(8) HORNER_CASE(9) HORNER_CASE(10) HORNER_CASE(11) HORNER_CASE(12)
-          HORNER_CASE(13) HORNER_CASE(14) HORNER_CASE(15) HORNER_CASE(16) HORNER_CASE(17) HORNER_CASE(18)
-          HORNER_CASE(19) HORNER_CASE(20) HORNER_CASE(21) HORNER_CASE(22) HORNER_CASE(23) HORNER_CASE(24)
-          HORNER_CASE(25) HORNER_CASE(26) HORNER_CASE(27) HORNER_CASE(28) HORNER_CASE(29) HORNER_CASE(30)
-          HORNER_CASE(31) HORNER_CASE(32)
+            HORNER_CASE(1) HORNER_CASE(2) HORNER_CASE(3) HORNER_CASE(4) HORNER_CASE(5) HORNER_CASE(6)
+            HORNER_CASE(7) HORNER_CASE(8) HORNER_CASE(9) HORNER_CASE(10) HORNER_CASE(11) HORNER_CASE(12)
+            HORNER_CASE(13) HORNER_CASE(14) HORNER_CASE(15) HORNER_CASE(16) HORNER_CASE(17) HORNER_CASE(18)
+            HORNER_CASE(19) HORNER_CASE(20) HORNER_CASE(21) HORNER_CASE(22) HORNER_CASE(23) HORNER_CASE(24)
+            HORNER_CASE(25) HORNER_CASE(26) HORNER_CASE(27) HORNER_CASE(28) HORNER_CASE(29) HORNER_CASE(30)
+            HORNER_CASE(31) HORNER_CASE(32)
 #undef HORNER_CASE
-          default:
-            CK(cudaFuncSetAttribute(k_eval2d_horner_any, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-            k_eval2d_horner_any<<<g, 128, sh, st>>>(k, tk, D.lo);
+            default:
+              CK(cudaFuncSetAttribute(k_eval2d_horner_any<PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+              k_eval2d_horner_any<PG><<<g, 128, sh, st>>>(k, tk, D.lo);
+          }
+          return cudaSuccess;
+        });
+          CK(e_pgh);
         }
         launches++;
       }
       if (D.eval_pw_n > 0) {
-        k_eval2d<<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
+        {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+          k_eval2d<decltype(G)::value><<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
+          return cudaSuccess;
+        });
+          CK(e_pgh);
+        }
         launches++;
       }
     }
@@ -2596,30 +2991,57 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
         const HornerTask* tk = D.horner + G.beg;
         const size_t sh = (size_t)Pn * Pn * np2 * 16;
         if (sh > 227 * 1024) return cudaErrorNotSupported;
-        switch (np2) {
+        {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+          constexpr int PG = decltype(G)::value;
+          switch (np2) {
 #define HORNER3_CASE(N)                                                                           \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_eval3d_horner<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_eval3d_horner<N><<<g, 128, sh, st>>>(k, tk, D.lo);                                          \
+    CK(cudaFuncSetAttribute(k_eval3d_horner<N, PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_eval3d_horner<N, PG><<<g, 128, sh, st>>>(k, tk, D.lo);                                      \
     break;
-          HORNER3_CASE(1) HORNER3_CASE(2) HORNER3_CASE(3) HORNER3_CASE(4) HORNER3_CASE(5)
-          HORNER3_CASE(6) HORNER3_CASE(7) HORNER3_CASE(8) HORNER3_CASE(9) HORNER3_CASE(10)
-          HORNER3_CASE(11) HORNER3_CASE(12) HORNER3_CASE(13) HORNER3_CASE(14) HORNER3_CASE(15)
+            HORNER3_CASE(1) HORNER3_CASE(2) HORNER3_CASE(3) HORNER3_CASE(4) HORNER3_CASE(5)
+            HORNER3_CASE(6) HORNER3_CASE(7) HORNER3_CASE(8) HORNER3_CASE(9) HORNER3_CASE(10)
+            HORNER3_CASE(11) HORNER3_CASE(12) HORNER3_CASE(13) HORNER3_CASE(14) HORNER3_CASE(15)
 #undef HORNER3_CASE
-          default: return cudaErrorNotSupported;
+            default: return cudaErrorNotSupported;
+          }
+          return cudaSuccess;
+        });
+          CK(e_pgh);
         }
         launches++;
       }
     } else if (P.dim == 3 && D.eval_taylor_n > 0 && D.eval3_smem) {
-      CK(cudaFuncSetAttribute(k_eval3d_taylor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
-      k_eval3d_taylor_smem<<<dim3(D.eval_taylor_n, nd), 512, D.eval3_sh, st>>>(k, D.eval);
+      {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+        constexpr int PG = decltype(G)::value;
+        CK(cudaFuncSetAttribute(k_eval3d_taylor_smem<PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
+        k_eval3d_taylor_smem<PG><<<dim3(D.eval_taylor_n, nd), 512, D.eval3_sh, st>>>(k, D.eval);
+        return cudaSuccess;
+      });
+          CK(e_pgh);
+        }
       launches++;
     } else if (P.dim == 3 && D.eval_taylor_n > 0) {
-      k_eval3d_taylor<<<D.scratch_ctas, 256, 0, st>>>(k, D.eval, D.eval_taylor_n, D.scratch, D.scratch_per_cta);
+      {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+        k_eval3d_taylor<decltype(G)::value><<<D.scratch_ctas, 256, 0, st>>>(k, D.eval, D.eval_taylor_n, D.scratch,
+                                                                           D.scratch_per_cta);
+        return cudaSuccess;
+      });
+          CK(e_pgh);
+        }
       launches++;
     }
     if (P.dim == 3 && D.eval_pw_n > 0) {
-      k_eval3d_pw<<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
+      {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+        k_eval3d_pw<decltype(G)::value><<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
+        return cudaSuccess;
+      });
+          CK(e_pgh);
+        }
       launches++;
     }
   } else {
@@ -2633,24 +3055,43 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, double* pot, d
     const double l2e = 1.4426950408889634;
     const double cs = std::sqrt(l2e / P.delta);
     const float amax = (float)(P.dmax * l2e / P.delta);
-    if (P.dim == 2) {
-      if (mixed) k_direct_mixed<2><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
-      else k_direct<2><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
-    } else {
-      if (mixed) k_direct_mixed<3><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
-      else k_direct<3><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
-    }
+    {
+          const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
+      constexpr int PG = decltype(G)::value;
+      if (P.dim == 2) {
+        if (mixed) k_direct_mixed<2, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
+        else k_direct<2, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      } else {
+        if (mixed) k_direct_mixed<3, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
+        else k_direct<3, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+      }
+      return cudaSuccess;
+    });
+          CK(e_pgh);
+        }
     launches++;
   }
   mark(7);
-  if (P.ifpgh > 0 && P.ns > 0) {
-    k_unsort<<<gb, 256, 0, st>>>(D.psort, pot, D.isrc_inv, P.ns, nd);
-    launches++;
-  }
-  if (P.ifpghtarg > 0 && P.nt > 0) {
-    k_unsort<<<gb, 256, 0, st>>>(D.ptsort, pottarg, D.itarg_inv, P.nt, nd);
-    launches++;
-  }
+  // sorted rows [nc][nd] -> pot (nd, n), grad (nd, dim, n), hess (nd, H, n)
+  const int nh = P.dim == 2 ? 3 : 6;
+  auto unsort = [&](const double* in, const int* inv, int n, int nc, double* pot, double* grad,
+                    double* hess) {
+    if (pot) {
+      k_unsort<<<gb, 256, 0, st>>>(in, pot, inv, n, nc * nd, 0, nd);
+      launches++;
+    }
+    if (nc > 1 && grad) {
+      k_unsort<<<gb, 256, 0, st>>>(in, grad, inv, n, nc * nd, nd, P.dim * nd);
+      launches++;
+    }
+    if (nc > 1 + P.dim && hess) {
+      k_unsort<<<gb, 256, 0, st>>>(in, hess, inv, n, nc * nd, (1 + P.dim) * nd, nh * nd);
+      launches++;
+    }
+  };
+  if (P.ifpgh > 0 && P.ns > 0) unsort(D.psort, D.isrc_inv, P.ns, k.nc_s, outs.pot, outs.grad, outs.hess);
+  if (P.ifpghtarg > 0 && P.nt > 0)
+    unsort(D.ptsort, D.itarg_inv, P.nt, k.nc_t, outs.pottarg, outs.gradtarg, outs.hesstarg);
   mark(8);
   D.launches = launches;
   CK(cudaGetLastError());
@@ -2697,7 +3138,7 @@ size_t large_delta_work_doubles(const Params& P, bool deterministic) {
 }
 
 cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
-                                const double* trg, double* pot, double* pottarg, double* work,
+                                const double* trg, const Outputs& outs, double* work,
                                 cudaStream_t st, bool deterministic) {
   KP k;
   memset(&k, 0, sizeof(k));
@@ -2728,14 +3169,18 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const double
       k_ld_sum<<<dim3(sb, P.nd), 256, 0, st>>>((int)nent, blocks, partial, local);
     }
   }
-  auto ev = [&](const double* pts, int n, double* out) {
-    if (n <= 0) return;
+  auto ev = [&](const double* pts, int n, int pgh, double* pot, double* grad, double* hess) -> cudaError_t {
+    if (n <= 0 || pgh <= 0) return cudaSuccess;
     int b = std::max(1, std::min(4096, (n + 255) / 256));
-    if (P.dim == 2) k_ld_eval<2><<<dim3(b, P.nd), 256, 0, st>>>(k, n, pts, out, p, cen, local);
-    else k_ld_eval<3><<<dim3(b, P.nd), 256, 0, st>>>(k, n, pts, out, p, cen, local);
+    return with_pgh(pgh, [&](auto G) -> cudaError_t {
+      constexpr int PG = decltype(G)::value;
+      if (P.dim == 2) k_ld_eval<2, PG><<<dim3(b, P.nd), 256, 0, st>>>(k, n, pts, pot, grad, hess, p, cen, local);
+      else k_ld_eval<3, PG><<<dim3(b, P.nd), 256, 0, st>>>(k, n, pts, pot, grad, hess, p, cen, local);
+      return cudaSuccess;
+    });
   };
-  if (P.ifpghtarg == 1) ev(trg, P.nt, pottarg);
-  if (P.ifpgh == 1) ev(src, P.ns, pot);
+  CK(ev(trg, P.nt, P.ifpghtarg, outs.pottarg, outs.gradtarg, outs.hesstarg));
+  CK(ev(src, P.ns, P.ifpgh, outs.pot, outs.grad, outs.hess));
   return cudaGetLastError();
 }
 
@@ -2787,7 +3232,10 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
   }
   // large_delta_execute copies the centre into work[0..2] and clears the
   // local expansion in work[4..] before accumulating into it
-  return large_delta_execute(P, src, chg, trg, pot, pottarg, work, st, false);
+  Outputs o;
+  o.pot = pot;
+  o.pottarg = pottarg;
+  return large_delta_execute(P, src, chg, trg, o, work, st, false);
 }
 
 }  // namespace fgtb

@@ -188,8 +188,8 @@ static void build_tasks(HostPlan& H) {
         // 10^4-point leaf; each chunk rebuilds the leaf's Taylor expansion
         const int evch = D == 2 ? 2048 : 2048;
         for (int set = 1; set >= 0; set--) {
-          if (set == 1 && !(P.ifpghtarg == 1 && t.nt(b) > 0)) continue;
-          if (set == 0 && !(P.ifpgh == 1 && t.ns(b) > 0)) continue;
+          if (set == 1 && !(P.ifpghtarg >= 1 && t.nt(b) > 0)) continue;
+          if (set == 0 && !(P.ifpgh >= 1 && t.ns(b) > 0)) continue;
           int i0 = set ? t.t0[b] : t.s0[b], n = set ? t.nt(b) : t.ns(b);
           for (int c = 0; c < n; c += evch)
             H.eval.push_back({b, set, i0 + c, std::min(evch, n - c), H.loc_slot[b], p, route});
@@ -282,8 +282,8 @@ static void build_tasks(HostPlan& H) {
     long long nsrc = 0;
     for (auto& r : rs) nsrc += r.n;
     for (int set = 0; set < 2; set++) {
-      if (set == 0 && !(P.ifpgh == 1)) continue;
-      if (set == 1 && !(P.ifpghtarg == 1)) continue;
+      if (set == 0 && !(P.ifpgh >= 1)) continue;
+      if (set == 1 && !(P.ifpghtarg >= 1)) continue;
       int i0 = set == 0 ? t.s0[b] : t.t0[b];
       int n = set == 0 ? t.ns(b) : t.nt(b);
       if (n == 0) continue;

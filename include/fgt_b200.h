@@ -12,7 +12,11 @@
  * consecutive nd-tuples, pot(nd, ns) likewise.  Every argument of the
  * Fortran-named entry points is passed by reference.
  *
- * Supported now: ifcharge = 1, ifdipole = 0, ifpgh and ifpghtarg in {0, 1},
+ * with gradients (ifpgh / ifpghtarg = 2) and Hessians (3) in the reference's
+ * layouts: grad(nd, dim, n); hess(nd, 3, n) in 2D ordered xx, xy, yy, and
+ * hess(nd, 6, n) in 3D ordered xx, yy, zz, xy, xz, yz.
+ *
+ * Supported now: ifcharge = 1, ifdipole = 0, ifpgh and ifpghtarg in {0..3},
  * any nd >= 1.  Other flag values return FGT_ERR_UNSUPPORTED.
  *
  * All entry points return a status (FGT_OK or an error code below) except
@@ -29,7 +33,7 @@ extern "C" {
 enum {
   FGT_OK = 0,
   FGT_ERR_BADARG = 1,      /* nd < 1, delta <= 0, eps not in (0,1), n < 0, NaN */
-  FGT_ERR_UNSUPPORTED = 2, /* dipoles, gradients/Hessians, orders too large */
+  FGT_ERR_UNSUPPORTED = 2, /* dipoles, flags above 3, orders too large */
   FGT_ERR_NOMEM = 3,       /* device or host allocation failed */
   FGT_ERR_CUDA = 4,        /* CUDA runtime error (see fgt_last_cuda_error) */
   FGT_ERR_NODEVICE = 5,    /* no CUDA device */
@@ -169,6 +173,16 @@ int fgt_plan_execute_host(fgt_plan* plan, const double* sources, const double* c
  * NULL for the context stream) and returns without synchronising */
 int fgt_plan_execute_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
                             const double* d_targ, double* d_pot, double* d_pottarg, void* stream);
+/* The same two with the gradient and Hessian arrays of plans created with
+ * ifpgh or ifpghtarg >= 2 (layouts as fgt_transform).  A NULL gradient or
+ * Hessian array is skipped; the potentials of the flagged sets are required.
+ * The reference has no plan API: these split fgt2d's one call
+ * (fgt2d.f:19-462) into set-up and apply. */
+int fgt_plan_execute_host_pgh(fgt_plan* plan, const double* charge, double* pot, double* grad,
+                              double* hess, double* pottarg, double* gradtarg, double* hesstarg);
+int fgt_plan_execute_device_pgh(fgt_plan* plan, const double* d_charge, double* d_pot,
+                                double* d_grad, double* d_hess, double* d_pottarg,
+                                double* d_gradtarg, double* d_hesstarg, void* stream);
 /* per-stage device milliseconds of one synchronous execute on device data:
  * gather, form, merge, mp->loc, split, eval, direct, scatter */
 int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
@@ -227,8 +241,12 @@ typedef struct fgt_request {
   int nt;
   const double* targ;    /* (nt, dim), may be NULL */
   int ifpgh, ifpghtarg;
-  double* pot;           /* (ns, nd) when ifpgh = 1 */
-  double* pottarg;       /* (nt, nd) when ifpghtarg = 1 */
+  double* pot;           /* (ns, nd) when ifpgh >= 1 */
+  double* pottarg;       /* (nt, nd) when ifpghtarg >= 1 */
+  double* grad;          /* (ns, dim, nd) when ifpgh >= 2, else may be NULL */
+  double* hess;          /* (ns, H, nd) when ifpgh = 3 */
+  double* gradtarg;      /* (nt, dim, nd) when ifpghtarg >= 2 */
+  double* hesstarg;      /* (nt, H, nd) when ifpghtarg = 3 */
 } fgt_request;
 typedef struct fgt_server_stats {
   long long submitted, completed, failed;

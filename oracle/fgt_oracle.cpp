@@ -717,35 +717,64 @@ void g2dpw2local(int nd, int p, int npw, const double* pw2l, const cplx* pw, dou
     }
   }
 }
-// g2dlevalp_vec, g2drouts.f:847-900
-void g2dlevalp(int nd, double delta, const double* cent, int p, const double* local,
-               const double* trg, int nt, double* pot) {
+// g2dlevalp_vec / g2dlevalg_vec / g2dlevalh_vec, g2drouts.f:847-1085:
+// potential (pgh = 1), + gradient (2), + Hessian (3, order xx, xy, yy).
+// grad(nd, 2, nt) and hess(nd, 3, nt) as in the reference.
+void g2dleval(int nd, double delta, const double* cent, int p, const double* local,
+              const double* trg, int nt, int pgh, double* pot, double* grad, double* hess) {
   int P = p + 1;
   double dsq = 1.0 / std::sqrt(delta);
-  std::vector<double> xp(P), yp(P);
+  std::vector<double> xp(P + 1), yp(P + 1), xpx(P + 1), ypy(P + 1), xpxx(P + 1), ypyy(P + 1);
   for (int it = 0; it < nt; it++) {
     double x = (trg[2 * it] - cent[0]) * dsq, y = (trg[2 * it + 1] - cent[1]) * dsq;
     xp[0] = 1; yp[0] = 1;
     for (int i = 1; i <= p; i++) { xp[i] = x * xp[i - 1]; yp[i] = y * yp[i - 1]; }
+    if (pgh >= 2) {
+      xpx[0] = 0; ypy[0] = 0;
+      for (int i = 1; i <= p; i++) { xpx[i] = i * xp[i - 1] * dsq; ypy[i] = i * yp[i - 1] * dsq; }
+    }
+    if (pgh >= 3) {
+      xpxx[0] = ypyy[0] = xpxx[1] = ypyy[1] = 0;
+      for (int i = 2; i <= p; i++) {
+        xpxx[i] = (double)(i * (i - 1)) * xp[i - 2] * dsq * dsq;
+        ypyy[i] = (double)(i * (i - 1)) * yp[i - 2] * dsq * dsq;
+      }
+    }
     for (int ind = 0; ind < nd; ind++) {
       const double* Lo = local + (size_t)ind * P * P;
-      double dd = 0;
+      double dd = 0, g1 = 0, g2 = 0, h1 = 0, h2 = 0, h3 = 0;
       for (int j1 = 0; j1 <= p; j1++) {
-        double d2 = 0;
-        for (int j2 = 0; j2 <= p; j2++) d2 += Lo[j2 + P * j1] * xp[j2];
+        double d2 = 0, d2x = 0, d2xx = 0;
+        for (int j2 = 0; j2 <= p; j2++) {
+          d2 += Lo[j2 + P * j1] * xp[j2];
+          if (pgh >= 2) d2x += Lo[j2 + P * j1] * xpx[j2];
+          if (pgh >= 3) d2xx += Lo[j2 + P * j1] * xpxx[j2];
+        }
         dd += d2 * yp[j1];
+        if (pgh >= 2) { g1 += d2x * yp[j1]; g2 += d2 * ypy[j1]; }
+        if (pgh >= 3) { h1 += d2xx * yp[j1]; h2 += d2x * ypy[j1]; h3 += d2 * ypyy[j1]; }
       }
       pot[nd * it + ind] += dd;
+      if (pgh >= 2) {
+        grad[ind + nd * (0 + 2 * (size_t)it)] += g1;
+        grad[ind + nd * (1 + 2 * (size_t)it)] += g2;
+      }
+      if (pgh >= 3) {
+        hess[ind + nd * (0 + 3 * (size_t)it)] += h1;
+        hess[ind + nd * (1 + 3 * (size_t)it)] += h2;
+        hess[ind + nd * (2 + 3 * (size_t)it)] += h3;
+      }
     }
   }
 }
-// g2dpwevalp_vec, g2drouts.f:1887-1966
-void g2dpwevalp(int nd, double delta, const double* cent, int npw, const double* ts,
-                const cplx* pw, const double* trg, int nt, double* pot) {
+// g2dpwevalp_vec / g2dpwevalg_vec / g2dpwevalh_vec, g2drouts.f:1887-2200
+void g2dpweval(int nd, double delta, const double* cent, int npw, const double* ts,
+               const cplx* pw, const double* trg, int nt, int pgh, double* pot, double* grad,
+               double* hess) {
   cplx eye(0, 1);
   double dsq = 1.0 / std::sqrt(delta);
   int n2 = npw / 2;
-  std::vector<cplx> w1(npw + 1), w2(npw + 1);
+  std::vector<cplx> w1(npw + 1), w2(npw + 1), w1x(npw + 1), w2y(npw + 1), w1xx(npw + 1), w2yy(npw + 1);
   for (int it = 0; it < nt; it++) {
     double x = (trg[2 * it] - cent[0]) * dsq, y = (trg[2 * it + 1] - cent[1]) * dsq;
     cplx qqx = std::exp(eye * ts[1] * x), qqy = std::exp(eye * ts[1] * y);
@@ -753,19 +782,47 @@ void g2dpwevalp(int nd, double delta, const double* cent, int npw, const double*
     qqx = qqx * qqx; qqy = qqy * qqy;
     for (int j1 = 1; j1 <= n2; j1++) {
       w1[j1] = q1; w2[j1] = q2;
-      q1 = q1 * qqx; q2 = q2 * qqy;
       w1[j1 + n2] = std::conj(w1[j1]);
       w2[j1 + n2] = std::conj(w2[j1]);
+      if (pgh >= 2) {
+        w1x[j1] = eye * ts[j1] * dsq * w1[j1];
+        w2y[j1] = eye * ts[j1] * dsq * w2[j1];
+        w1x[j1 + n2] = std::conj(w1x[j1]);
+        w2y[j1 + n2] = std::conj(w2y[j1]);
+      }
+      if (pgh >= 3) {
+        w1xx[j1] = eye * ts[j1] * dsq * w1x[j1];
+        w2yy[j1] = eye * ts[j1] * dsq * w2y[j1];
+        w1xx[j1 + n2] = std::conj(w1xx[j1]);
+        w2yy[j1 + n2] = std::conj(w2yy[j1]);
+      }
+      q1 = q1 * qqx; q2 = q2 * qqy;
     }
     for (int ind = 0; ind < nd; ind++) {
       const cplx* W = pw + (size_t)ind * n2 * npw;
-      cplx z = 0;
+      cplx z = 0, zx = 0, zy = 0, zxx = 0, zxy = 0, zyy = 0;
       for (int j2 = 1; j2 <= npw; j2++) {
-        cplx cd = 0;
-        for (int j1 = 1; j1 <= n2; j1++) cd += W[(j1 - 1) + n2 * (j2 - 1)] * w1[j1];
-        z += cd * w2[j2];
+        cplx c = 0, cx = 0, cxx = 0;
+        for (int j1 = 1; j1 <= n2; j1++) {
+          const cplx wv = W[(j1 - 1) + n2 * (j2 - 1)];
+          c += wv * w1[j1];
+          if (pgh >= 2) cx += wv * w1x[j1];
+          if (pgh >= 3) cxx += wv * w1xx[j1];
+        }
+        z += c * w2[j2];
+        if (pgh >= 2) { zx += cx * w2[j2]; zy += c * w2y[j2]; }
+        if (pgh >= 3) { zxx += cxx * w2[j2]; zxy += cx * w2y[j2]; zyy += c * w2yy[j2]; }
       }
       pot[nd * it + ind] += z.real() * 2;
+      if (pgh >= 2) {
+        grad[ind + nd * (0 + 2 * (size_t)it)] += zx.real() * 2;
+        grad[ind + nd * (1 + 2 * (size_t)it)] += zy.real() * 2;
+      }
+      if (pgh >= 3) {
+        hess[ind + nd * (0 + 3 * (size_t)it)] += zxx.real() * 2;
+        hess[ind + nd * (1 + 3 * (size_t)it)] += zxy.real() * 2;
+        hess[ind + nd * (2 + 3 * (size_t)it)] += zyy.real() * 2;
+      }
     }
   }
 }
@@ -942,40 +999,79 @@ void g3dpw2local(int nd, int p, int npw, const double* pw2l, const cplx* pw, dou
     }
   }
 }
-// g3dlevalp_vec, g3drouts.f:1045-1107
-void g3dlevalp(int nd, double delta, const double* cent, int p, const double* local,
-               const double* trg, int nt, double* pot) {
+// g3dlevalp_vec / g3dlevalg_vec / g3dlevalh_vec, g3drouts.f:1045-1360:
+// Hessian order xx, yy, zz, xy, xz, yz.
+void g3dleval(int nd, double delta, const double* cent, int p, const double* local,
+              const double* trg, int nt, int pgh, double* pot, double* grad, double* hess) {
   int P = p + 1;
   double dsq = 1.0 / std::sqrt(delta);
-  std::vector<double> xp(P), yp(P), zp(P);
+  std::vector<double> xp(P + 1), yp(P + 1), zp(P + 1), xpx(P + 1), ypy(P + 1), zpz(P + 1),
+      xpxx(P + 1), ypyy(P + 1), zpzz(P + 1);
   for (int it = 0; it < nt; it++) {
     double x = (trg[3 * it] - cent[0]) * dsq, y = (trg[3 * it + 1] - cent[1]) * dsq,
            z = (trg[3 * it + 2] - cent[2]) * dsq;
     xp[0] = yp[0] = zp[0] = 1;
     for (int i = 1; i <= p; i++) { xp[i] = x * xp[i - 1]; yp[i] = y * yp[i - 1]; zp[i] = z * zp[i - 1]; }
+    if (pgh >= 2) {
+      xpx[0] = ypy[0] = zpz[0] = 0;
+      for (int i = 1; i <= p; i++) {
+        xpx[i] = i * xp[i - 1] * dsq; ypy[i] = i * yp[i - 1] * dsq; zpz[i] = i * zp[i - 1] * dsq;
+      }
+    }
+    if (pgh >= 3) {
+      xpxx[0] = ypyy[0] = zpzz[0] = xpxx[1] = ypyy[1] = zpzz[1] = 0;
+      for (int i = 2; i <= p; i++) {
+        const double c = (double)(i * (i - 1));
+        xpxx[i] = c * xp[i - 2] * dsq * dsq;
+        ypyy[i] = c * yp[i - 2] * dsq * dsq;
+        zpzz[i] = c * zp[i - 2] * dsq * dsq;
+      }
+    }
     for (int ind = 0; ind < nd; ind++) {
       const double* Lo = local + (size_t)ind * P * P * P;
-      double dd = 0;
+      double dd = 0, g1 = 0, g2 = 0, g3 = 0, h11 = 0, h22 = 0, h33 = 0, h12 = 0, h13 = 0, h23 = 0;
       for (int j1 = 0; j1 <= p; j1++) {
-        double d1 = 0;
+        double d1 = 0, d1x = 0, d1y = 0, d1xx = 0, d1yy = 0, d1xy = 0;
         for (int j2 = 0; j2 <= p; j2++) {
-          double d2 = 0;
-          for (int j3 = 0; j3 <= p; j3++) d2 += Lo[j3 + P * (j2 + (size_t)P * j1)] * xp[j3];
+          double d2 = 0, d2x = 0, d2xx = 0;
+          for (int j3 = 0; j3 <= p; j3++) {
+            const double l = Lo[j3 + P * (j2 + (size_t)P * j1)];
+            d2 += l * xp[j3];
+            if (pgh >= 2) d2x += l * xpx[j3];
+            if (pgh >= 3) d2xx += l * xpxx[j3];
+          }
           d1 += d2 * yp[j2];
+          if (pgh >= 2) { d1x += d2x * yp[j2]; d1y += d2 * ypy[j2]; }
+          if (pgh >= 3) { d1xx += d2xx * yp[j2]; d1xy += d2x * ypy[j2]; d1yy += d2 * ypyy[j2]; }
         }
         dd += d1 * zp[j1];
+        if (pgh >= 2) { g1 += d1x * zp[j1]; g2 += d1y * zp[j1]; g3 += d1 * zpz[j1]; }
+        if (pgh >= 3) {
+          h11 += d1xx * zp[j1]; h22 += d1yy * zp[j1]; h12 += d1xy * zp[j1];
+          h13 += d1x * zpz[j1]; h23 += d1y * zpz[j1]; h33 += d1 * zpzz[j1];
+        }
       }
       pot[nd * it + ind] += dd;
+      if (pgh >= 2) {
+        double g[3] = {g1, g2, g3};
+        for (int k = 0; k < 3; k++) grad[ind + nd * (k + 3 * (size_t)it)] += g[k];
+      }
+      if (pgh >= 3) {
+        double h[6] = {h11, h22, h33, h12, h13, h23};
+        for (int k = 0; k < 6; k++) hess[ind + nd * (k + 6 * (size_t)it)] += h[k];
+      }
     }
   }
 }
-// g3dpwevalp_vec, g3drouts.f:2268-2362
-void g3dpwevalp(int nd, double delta, const double* cent, int npw, const double* ts,
-                const cplx* pw, const double* trg, int nt, double* pot) {
+// g3dpwevalp_vec / g3dpwevalg_vec / g3dpwevalh_vec, g3drouts.f:2268-2660
+void g3dpweval(int nd, double delta, const double* cent, int npw, const double* ts,
+               const cplx* pw, const double* trg, int nt, int pgh, double* pot, double* grad,
+               double* hess) {
   cplx eye(0, 1);
   double dsq = 1.0 / std::sqrt(delta);
   int n2 = npw / 2;
-  std::vector<cplx> w1(npw + 1), w2(npw + 1), w3(npw + 1);
+  std::vector<cplx> w1(npw + 1), w2(npw + 1), w3(npw + 1), w1x(npw + 1), w2y(npw + 1),
+      w3z(npw + 1), w1xx(npw + 1), w2yy(npw + 1), w3zz(npw + 1);
   for (int it = 0; it < nt; it++) {
     double x = (trg[3 * it] - cent[0]) * dsq, y = (trg[3 * it + 1] - cent[1]) * dsq,
            z = (trg[3 * it + 2] - cent[2]) * dsq;
@@ -984,25 +1080,53 @@ void g3dpwevalp(int nd, double delta, const double* cent, int npw, const double*
     cplx q1 = qx, q2 = qy, q3 = qz;
     qx = qx * qx; qy = qy * qy; qz = qz * qz;
     for (int j1 = n2 + 1; j1 <= npw; j1++) {
+      const int m = npw - j1 + 1;
       w1[j1] = q1; w2[j1] = q2; w3[j1] = q3;
+      w1[m] = std::conj(w1[j1]); w2[m] = std::conj(w2[j1]); w3[m] = std::conj(w3[j1]);
+      const cplx zt = eye * ts[j1] * dsq;
+      if (pgh >= 2) {
+        w1x[j1] = zt * w1[j1]; w2y[j1] = zt * w2[j1]; w3z[j1] = zt * w3[j1];
+        w1x[m] = std::conj(w1x[j1]); w2y[m] = std::conj(w2y[j1]); w3z[m] = std::conj(w3z[j1]);
+      }
+      if (pgh >= 3) {
+        w1xx[j1] = zt * w1x[j1]; w2yy[j1] = zt * w2y[j1]; w3zz[j1] = zt * w3z[j1];
+        w1xx[m] = std::conj(w1xx[j1]); w2yy[m] = std::conj(w2yy[j1]); w3zz[m] = std::conj(w3zz[j1]);
+      }
       q1 = q1 * qx; q2 = q2 * qy; q3 = q3 * qz;
-      w1[npw - j1 + 1] = std::conj(w1[j1]);
-      w2[npw - j1 + 1] = std::conj(w2[j1]);
-      w3[npw - j1 + 1] = std::conj(w3[j1]);
     }
     for (int ind = 0; ind < nd; ind++) {
       const cplx* W = pw + (size_t)ind * npw * npw * n2;
-      cplx c3 = 0;
+      cplx dd = 0, g1 = 0, g2 = 0, g3 = 0, h11 = 0, h22 = 0, h33 = 0, h12 = 0, h13 = 0, h23 = 0;
       for (int j3 = 1; j3 <= n2; j3++) {
-        cplx c2 = 0;
+        cplx d1 = 0, d1x = 0, d1y = 0, d1xx = 0, d1yy = 0, d1xy = 0;
         for (int j2 = 1; j2 <= npw; j2++) {
-          cplx c1 = 0;
-          for (int j1 = 1; j1 <= npw; j1++) c1 += W[(j1 - 1) + npw * ((j2 - 1) + (size_t)npw * (j3 - 1))] * w1[j1];
-          c2 += c1 * w2[j2];
+          cplx d2 = 0, d2x = 0, d2xx = 0;
+          for (int j1 = 1; j1 <= npw; j1++) {
+            const cplx wv = W[(j1 - 1) + npw * ((j2 - 1) + (size_t)npw * (j3 - 1))];
+            d2 += wv * w1[j1];
+            if (pgh >= 2) d2x += wv * w1x[j1];
+            if (pgh >= 3) d2xx += wv * w1xx[j1];
+          }
+          d1 += d2 * w2[j2];
+          if (pgh >= 2) { d1x += d2x * w2[j2]; d1y += d2 * w2y[j2]; }
+          if (pgh >= 3) { d1xx += d2xx * w2[j2]; d1xy += d2x * w2y[j2]; d1yy += d2 * w2yy[j2]; }
         }
-        c3 += c2 * w3[j3];
+        dd += d1 * w3[j3];
+        if (pgh >= 2) { g1 += d1x * w3[j3]; g2 += d1y * w3[j3]; g3 += d1 * w3z[j3]; }
+        if (pgh >= 3) {
+          h11 += d1xx * w3[j3]; h22 += d1yy * w3[j3]; h12 += d1xy * w3[j3];
+          h13 += d1x * w3z[j3]; h23 += d1y * w3z[j3]; h33 += d1 * w3zz[j3];
+        }
       }
-      pot[nd * it + ind] += c3.real() * 2;
+      pot[nd * it + ind] += dd.real() * 2;
+      if (pgh >= 2) {
+        cplx g[3] = {g1, g2, g3};
+        for (int k = 0; k < 3; k++) grad[ind + nd * (k + 3 * (size_t)it)] += g[k].real() * 2;
+      }
+      if (pgh >= 3) {
+        cplx h[6] = {h11, h22, h33, h12, h13, h23};
+        for (int k = 0; k < 6; k++) hess[ind + nd * (k + 6 * (size_t)it)] += h[k].real() * 2;
+      }
     }
   }
 }
@@ -1039,23 +1163,48 @@ void g3dformlc(int nd, double delta, const double* src, int ns, const double* ch
   }
 }
 
-// g2d_directcp_vec (g2ddirect.f:32-76) / g3d_directcp_vec (g3ddirect.f:3-49)
+// g2d_directcp/cg/ch_vec (g2ddirect.f:32-212) / g3d_directcp/cg/ch_vec
+// (g3ddirect.f:3-203): pot (pgh = 1), + grad (2), + Hessian (3) with
+// rfac = -2/delta, d_x = rfac dx, d_xx = rfac + d_x^2, d_xy = d_x d_y.
+// Hessian order 2D xx, xy, yy; 3D xx, yy, zz, xy, xz, yz.
 template <int D>
-void directcp(int nd, double delta, double dmax, const double* src, int ns, const double* chg,
-              const double* trg, int nt, double* pot) {
+void directc(int nd, double delta, double dmax, const double* src, int ns, const double* chg,
+             const double* trg, int nt, int pgh, double* pot, double* grad, double* hess) {
+  const int NH = D == 2 ? 3 : 6;
+  const double rfac = -2.0 / delta;
   for (int it = 0; it < nt; it++)
     for (int i = 0; i < ns; i++) {
-      double rr = 0;
+      double rr = 0, df[3] = {0, 0, 0};
       for (int d = 0; d < D; d++) {
-        double df = trg[D * it + d] - src[D * i + d];
-        rr += df * df;
+        df[d] = trg[D * it + d] - src[D * i + d];
+        rr += df[d] * df[d];
       }
       if (rr < dmax) {
         double r = std::exp(-rr / delta);
+        double g[3], h[6];
+        for (int d = 0; d < D; d++) g[d] = rfac * df[d];
+        if (D == 2) {
+          h[0] = rfac + g[0] * g[0]; h[1] = g[0] * g[1]; h[2] = rfac + g[1] * g[1];
+        } else {
+          h[0] = rfac + g[0] * g[0]; h[1] = rfac + g[1] * g[1]; h[2] = rfac + g[2] * g[2];
+          h[3] = g[0] * g[1]; h[4] = g[0] * g[2]; h[5] = g[1] * g[2];
+        }
         for (int ii = 0; ii < nd; ii++) {
           double v = r * chg[nd * i + ii];
 #pragma omp atomic
           pot[nd * it + ii] += v;
+          if (pgh >= 2)
+            for (int d = 0; d < D; d++) {
+              double w = g[d] * v;
+#pragma omp atomic
+              grad[ii + nd * (d + D * (size_t)it)] += w;
+            }
+          if (pgh >= 3)
+            for (int c = 0; c < NH; c++) {
+              double w = h[c] * v;
+#pragma omp atomic
+              hess[ii + nd * (c + NH * (size_t)it)] += w;
+            }
         }
       }
     }
@@ -1072,14 +1221,21 @@ struct Result {
 // (fgt3d.f:19-477, 483-1527).  Output arrays are overwritten.
 template <int D>
 int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int ifcharge,
-            const double* charge, int ifdipole, int ifpgh, double* pot, int nt, const double* targ,
-            int ifpghtarg, double* pottarg, Result* res) {
+            const double* charge, int ifdipole, int ifpgh, double* pot, double* grad, double* hess,
+            int nt, const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+            double* hesstarg, Result* res) {
   const int NCH = Tree<D>::NCH;
+  const int NH = D == 2 ? 3 : 6;
   if (nd < 1 || !(delta > 0) || !(eps > 0) || ns < 0 || nt < 0) return ORC_BADARG;
   if (ifcharge != 1 || ifdipole != 0) return ORC_UNSUPPORTED;
-  if (ifpgh < 0 || ifpgh > 1 || ifpghtarg < 0 || ifpghtarg > 1) return ORC_UNSUPPORTED;
-  if (ifpgh == 1) std::fill(pot, pot + (size_t)nd * ns, 0.0);
-  if (ifpghtarg == 1) std::fill(pottarg, pottarg + (size_t)nd * nt, 0.0);
+  if (ifpgh < 0 || ifpgh > 3 || ifpghtarg < 0 || ifpghtarg > 3) return ORC_UNSUPPORTED;
+  // fgt2d.f:238-322: outputs zeroed per flag
+  if (ifpgh >= 1) std::fill(pot, pot + (size_t)nd * ns, 0.0);
+  if (ifpgh >= 2) std::fill(grad, grad + (size_t)nd * D * ns, 0.0);
+  if (ifpgh >= 3) std::fill(hess, hess + (size_t)nd * NH * ns, 0.0);
+  if (ifpghtarg >= 1) std::fill(pottarg, pottarg + (size_t)nd * nt, 0.0);
+  if (ifpghtarg >= 2) std::fill(gradtarg, gradtarg + (size_t)nd * D * nt, 0.0);
+  if (ifpghtarg >= 3) std::fill(hesstarg, hesstarg + (size_t)nd * NH * nt, 0.0);
   if (ns == 0) return ORC_OK;
 
   int npwlevel;
@@ -1095,12 +1251,12 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
     std::vector<double> local(LL, 0.0);
     if (D == 2) {
       g2dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
-      if (ifpghtarg == 1) g2dlevalp(nd, delta, cen0, nl0, local.data(), targ, nt, pottarg);
-      if (ifpgh == 1) g2dlevalp(nd, delta, cen0, nl0, local.data(), sources, ns, pot);
+      if (ifpghtarg >= 1) g2dleval(nd, delta, cen0, nl0, local.data(), targ, nt, ifpghtarg, pottarg, gradtarg, hesstarg);
+      if (ifpgh >= 1) g2dleval(nd, delta, cen0, nl0, local.data(), sources, ns, ifpgh, pot, grad, hess);
     } else {
       g3dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
-      if (ifpghtarg == 1) g3dlevalp(nd, delta, cen0, nl0, local.data(), targ, nt, pottarg);
-      if (ifpgh == 1) g3dlevalp(nd, delta, cen0, nl0, local.data(), sources, ns, pot);
+      if (ifpghtarg >= 1) g3dleval(nd, delta, cen0, nl0, local.data(), targ, nt, ifpghtarg, pottarg, gradtarg, hesstarg);
+      if (ifpgh >= 1) g3dleval(nd, delta, cen0, nl0, local.data(), sources, ns, ifpgh, pot, grad, hess);
     }
     return ORC_OK;
   }
@@ -1149,6 +1305,17 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
   for (int i = 0; i < nt; i++)
     for (int d = 0; d < D; d++) tsort[(size_t)D * i + d] = targ[(size_t)D * (itarg[i + 1] - 1) + d];
   std::vector<double> psort((size_t)nd * ns, 0.0), ptsort((size_t)nd * nt, 0.0);
+  std::vector<double> gsort(ifpgh >= 2 ? (size_t)nd * D * ns : 0, 0.0),
+      hsort(ifpgh >= 3 ? (size_t)nd * NH * ns : 0, 0.0),
+      gtsort(ifpghtarg >= 2 ? (size_t)nd * D * nt : 0, 0.0),
+      htsort(ifpghtarg >= 3 ? (size_t)nd * NH * nt : 0, 0.0);
+  // sorted output pointers of the points from index i of either set
+  auto PT = [&](int i) { return ptsort.data() + (size_t)nd * i; };
+  auto GT = [&](int i) { return gtsort.data() + (size_t)nd * D * i; };
+  auto HT = [&](int i) { return htsort.data() + (size_t)nd * NH * i; };
+  auto PS = [&](int i) { return psort.data() + (size_t)nd * i; };
+  auto GS = [&](int i) { return gsort.data() + (size_t)nd * D * i; };
+  auto HS = [&](int i) { return hsort.data() + (size_t)nd * NH * i; };
 
   auto NS = [&](int b) { return isrcse[2 * b + 1] - isrcse[2 * b] + 1; };
   auto NT = [&](int b) { return itargse[2 * b + 1] - itargse[2 * b] + 1; };
@@ -1382,25 +1549,27 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         const double* c = &t.centers[(size_t)D * ibox];
         bool usepw = pweval && (D == 2 || nts + nss < 1000000);
         if (usepw) {
-          if (nts > 0 && ifpghtarg == 1) {
-            if (D == 2) g2dpwevalp(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 2 * (size_t)T0(ibox), nts, ptsort.data() + (size_t)nd * T0(ibox));
-            else g3dpwevalp(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 3 * (size_t)T0(ibox), nts, ptsort.data() + (size_t)nd * T0(ibox));
+          const int i0 = T0(ibox), j0 = S0(ibox);
+          if (nts > 0 && ifpghtarg >= 1) {
+            if (D == 2) g2dpweval(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 2 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
+            else g3dpweval(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 3 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
           }
-          if (nss > 0 && ifpgh == 1) {
-            if (D == 2) g2dpwevalp(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 2 * (size_t)S0(ibox), nss, psort.data() + (size_t)nd * S0(ibox));
-            else g3dpwevalp(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 3 * (size_t)S0(ibox), nss, psort.data() + (size_t)nd * S0(ibox));
+          if (nss > 0 && ifpgh >= 1) {
+            if (D == 2) g2dpweval(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 2 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
+            else g3dpweval(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 3 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
           }
         } else {
           std::vector<double> local((size_t)nd * (D == 2 ? P * P : P * P * P));
           if (D == 2) g2dpw2local(nd, p, npw, rx2l.data(), LO(ibox), local.data());
           else g3dpw2local(nd, p, npw, rx2l.data(), LO(ibox), local.data());
-          if (nts > 0 && ifpghtarg == 1) {
-            if (D == 2) g2dlevalp(nd, delta, c, p, local.data(), tsort.data() + 2 * (size_t)T0(ibox), nts, ptsort.data() + (size_t)nd * T0(ibox));
-            else g3dlevalp(nd, delta, c, p, local.data(), tsort.data() + 3 * (size_t)T0(ibox), nts, ptsort.data() + (size_t)nd * T0(ibox));
+          const int i0 = T0(ibox), j0 = S0(ibox);
+          if (nts > 0 && ifpghtarg >= 1) {
+            if (D == 2) g2dleval(nd, delta, c, p, local.data(), tsort.data() + 2 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
+            else g3dleval(nd, delta, c, p, local.data(), tsort.data() + 3 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
           }
-          if (nss > 0 && ifpgh == 1) {
-            if (D == 2) g2dlevalp(nd, delta, c, p, local.data(), ssort.data() + 2 * (size_t)S0(ibox), nss, psort.data() + (size_t)nd * S0(ibox));
-            else g3dlevalp(nd, delta, c, p, local.data(), ssort.data() + 3 * (size_t)S0(ibox), nss, psort.data() + (size_t)nd * S0(ibox));
+          if (nss > 0 && ifpgh >= 1) {
+            if (D == 2) g2dleval(nd, delta, c, p, local.data(), ssort.data() + 2 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
+            else g3dleval(nd, delta, c, p, local.data(), ssort.data() + 3 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
           }
         }
       }
@@ -1419,22 +1588,28 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         const double* q = csort.data() + (size_t)nd * S0(jbox);
         int nsj = NS(jbox);
         for (int ibox : list1[jbox]) {
-          if (NT(ibox) > 0 && ifpghtarg == 1)
-            directcp<D>(nd, delta, dmax, s, nsj, q, tsort.data() + (size_t)D * T0(ibox), NT(ibox), ptsort.data() + (size_t)nd * T0(ibox));
-          if (NS(ibox) > 0 && ifpgh == 1)
-            directcp<D>(nd, delta, dmax, s, nsj, q, ssort.data() + (size_t)D * S0(ibox), NS(ibox), psort.data() + (size_t)nd * S0(ibox));
+          const int i0 = T0(ibox), j0 = S0(ibox);
+          if (NT(ibox) > 0 && ifpghtarg >= 1)
+            directc<D>(nd, delta, dmax, s, nsj, q, tsort.data() + (size_t)D * i0, NT(ibox), ifpghtarg, PT(i0), GT(i0), HT(i0));
+          if (NS(ibox) > 0 && ifpgh >= 1)
+            directc<D>(nd, delta, dmax, s, nsj, q, ssort.data() + (size_t)D * j0, NS(ibox), ifpgh, PS(j0), GS(j0), HS(j0));
         }
       }
     }
     if (res) res->nleaf_direct = nhung;
   }
   // dreorderi: un-permute outputs
-  if (ifpgh == 1)
-    for (int i = 0; i < ns; i++)
-      for (int k = 0; k < nd; k++) pot[(size_t)nd * (isrc[i + 1] - 1) + k] = psort[(size_t)nd * i + k];
-  if (ifpghtarg == 1)
-    for (int i = 0; i < nt; i++)
-      for (int k = 0; k < nd; k++) pottarg[(size_t)nd * (itarg[i + 1] - 1) + k] = ptsort[(size_t)nd * i + k];
+  // (dreorderi / dreorderiv, fgt2d.f:430-458)
+  auto unsort = [&](int n, const std::vector<int>& perm, int w, const std::vector<double>& in, double* out) {
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < w; k++) out[(size_t)w * (perm[i + 1] - 1) + k] = in[(size_t)w * i + k];
+  };
+  if (ifpgh >= 1) unsort(ns, isrc, nd, psort, pot);
+  if (ifpgh >= 2) unsort(ns, isrc, nd * D, gsort, grad);
+  if (ifpgh >= 3) unsort(ns, isrc, nd * NH, hsort, hess);
+  if (ifpghtarg >= 1) unsort(nt, itarg, nd, ptsort, pottarg);
+  if (ifpghtarg >= 2) unsort(nt, itarg, nd * D, gtsort, gradtarg);
+  if (ifpghtarg >= 3) unsort(nt, itarg, nd * NH, htsort, hesstarg);
   return ORC_OK;
 }
 
@@ -1501,15 +1676,30 @@ void orc_boxsize0(int dim, double delta, double eps, int ns, const double* src, 
 
 // Full transform, the reference's calling sequence minus the dipole/grad/hess
 // arrays.  info (optional, int[8]): npwlevel, nlevels, nboxes, npw, nlmax, ndirect leaves.
+int orc_fgt_pgh(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                int ifcharge, const double* charge, int ifdipole, int ifpgh, double* pot,
+                double* grad, double* hess, int nt, const double* targ, int ifpghtarg,
+                double* pottarg, double* gradtarg, double* hesstarg, int* info, int nthreads);
 int orc_fgt(int dim, int nd, double delta, double eps, int ns, const double* sources,
             int ifcharge, const double* charge, int ifdipole, int ifpgh, double* pot, int nt,
             const double* targ, int ifpghtarg, double* pottarg, int* info, int nthreads) {
+  if (ifpgh > 1 || ifpghtarg > 1) return ORC_UNSUPPORTED;  // no gradient/Hessian arrays here
+  return orc_fgt_pgh(dim, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, nullptr,
+                     nullptr, nt, targ, ifpghtarg, pottarg, nullptr, nullptr, info, nthreads);
+}
+
+// The same with the gradient and Hessian arrays (ifpgh, ifpghtarg up to 3):
+// grad(nd, dim, ns), hess(nd, 3 or 6, ns) as in fgt2d / fgt3d.
+int orc_fgt_pgh(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                int ifcharge, const double* charge, int ifdipole, int ifpgh, double* pot,
+                double* grad, double* hess, int nt, const double* targ, int ifpghtarg,
+                double* pottarg, double* gradtarg, double* hesstarg, int* info, int nthreads) {
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
   Result r;
-  int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, nt, targ, ifpghtarg, pottarg, &r)
-                    : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, nt, targ, ifpghtarg, pottarg, &r);
+  int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r)
+                    : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r);
   if (info) {
     info[0] = r.npwlevel; info[1] = r.nlevels; info[2] = r.nboxes; info[3] = r.npw;
     info[4] = r.nlmax; info[5] = (int)r.nleaf_direct; info[6] = 0; info[7] = 0;
@@ -1537,6 +1727,49 @@ void orc_direct(int dim, int nd, double delta, int ns, const double* src, const 
         acc += std::exp(-rr / delta) * chg[(size_t)nd * i + k];
       }
       pot[(size_t)nd * it + k] = acc;
+    }
+  }
+}
+
+// The same direct sum with gradients and Hessians (pgh = 2, 3): the
+// derivatives of exp(-r^2/delta) with respect to the target, per
+// g2d_directch_vec / g3d_directch_vec without the cutoff.
+void orc_direct_pgh(int dim, int nd, double delta, int ns, const double* src, const double* chg,
+                    int nt, const double* trg, int pgh, double* pot, double* grad, double* hess,
+                    int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const int NH = dim == 2 ? 3 : 6;
+  const double rfac = -2.0 / delta;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int it = 0; it < nt; it++) {
+    for (int k = 0; k < nd; k++) {
+      double a[10] = {0};
+      for (int i = 0; i < ns; i++) {
+        double rr = 0, g[3] = {0, 0, 0};
+        for (int d = 0; d < dim; d++) {
+          double df = trg[(size_t)dim * it + d] - src[(size_t)dim * i + d];
+          rr += df * df;
+          g[d] = rfac * df;
+        }
+        const double v = std::exp(-rr / delta) * chg[(size_t)nd * i + k];
+        a[0] += v;
+        for (int d = 0; d < dim; d++) a[1 + d] += g[d] * v;
+        double* h = a + 1 + dim;
+        if (dim == 2) {
+          h[0] += (rfac + g[0] * g[0]) * v; h[1] += g[0] * g[1] * v; h[2] += (rfac + g[1] * g[1]) * v;
+        } else {
+          h[0] += (rfac + g[0] * g[0]) * v; h[1] += (rfac + g[1] * g[1]) * v;
+          h[2] += (rfac + g[2] * g[2]) * v; h[3] += g[0] * g[1] * v;
+          h[4] += g[0] * g[2] * v; h[5] += g[1] * g[2] * v;
+        }
+      }
+      pot[(size_t)nd * it + k] = a[0];
+      if (pgh >= 2)
+        for (int d = 0; d < dim; d++) grad[k + nd * (d + (size_t)dim * it)] = a[1 + d];
+      if (pgh >= 3)
+        for (int c = 0; c < NH; c++) hess[k + nd * (c + (size_t)NH * it)] = a[1 + dim + c];
     }
   }
 }

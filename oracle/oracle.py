@@ -46,6 +46,15 @@ def lib():
         L.orc_fgt.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                               ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                               _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _ip, ctypes.c_int]
+        L.orc_fgt_pgh.restype = ctypes.c_int
+        L.orc_fgt_pgh.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                  _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
+                                  _ip, ctypes.c_int]
+        L.orc_direct_pgh.restype = None
+        L.orc_direct_pgh.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                     _dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
+                                     ctypes.c_int]
         L.orc_direct.restype = None
         L.orc_direct.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
                                  _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
@@ -101,6 +110,53 @@ def fgt(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, n
         raise RuntimeError(f"oracle fgt returned status {rc}")
     keys = ["npwlevel", "nlevels", "nboxes", "npw", "nlmax", "ndirect_leaves"]
     return pot[:ns], pt[:nt], {k: int(info[i]) for i, k in enumerate(keys)}
+
+
+def nhess(dim):
+    return 3 if dim == 2 else 6
+
+
+def fgt_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, nthreads=0):
+    """The restated transform with gradients (ifpgh = 2) and Hessians (3).
+
+    Returns a dict of pot (ns, nd), grad (ns, dim, nd), hess (ns, H, nd) and
+    the same for the targets (H = 3 in 2D: xx, xy, yy; 6 in 3D: xx, yy, zz,
+    xy, xz, yz), each None when not requested, plus ``info``.
+    """
+    src = _f64(sources)
+    ns = src.shape[0]
+    q = _f64(charge).reshape(ns, nd) if ns else np.zeros((0, nd))
+    trg = _f64(targ) if targ is not None else np.zeros((0, dim))
+    nt = trg.shape[0]
+    H = nhess(dim)
+    pot, grad, hess = np.zeros((max(ns, 1), nd)), np.zeros((max(ns, 1), dim, nd)), np.zeros((max(ns, 1), H, nd))
+    pt, gt, ht = np.zeros((max(nt, 1), nd)), np.zeros((max(nt, 1), dim, nd)), np.zeros((max(nt, 1), H, nd))
+    info = np.zeros(8, dtype=np.int32)
+    rc = lib().orc_fgt_pgh(dim, nd, float(delta), float(eps), ns, _d(src), 1, _d(q), 0, ifpgh,
+                           _d(pot), _d(grad), _d(hess), nt, _d(trg), ifpghtarg, _d(pt), _d(gt),
+                           _d(ht), info.ctypes.data_as(_ip), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle fgt returned status {rc}")
+    keys = ["npwlevel", "nlevels", "nboxes", "npw", "nlmax", "ndirect_leaves"]
+    return {"pot": pot[:ns] if ifpgh >= 1 else None, "grad": grad[:ns] if ifpgh >= 2 else None,
+            "hess": hess[:ns] if ifpgh >= 3 else None,
+            "pottarg": pt[:nt] if ifpghtarg >= 1 else None,
+            "gradtarg": gt[:nt] if ifpghtarg >= 2 else None,
+            "hesstarg": ht[:nt] if ifpghtarg >= 3 else None,
+            "info": {k: int(info[i]) for i, k in enumerate(keys)}}
+
+
+def direct_pgh(dim, nd, delta, sources, charge, targ, pgh=3, nthreads=0):
+    """FP64 direct sum without cutoff with gradients and Hessians:
+    (pot (nt, nd), grad (nt, dim, nd), hess (nt, H, nd))."""
+    src = _f64(sources)
+    trg = _f64(targ)
+    q = _f64(charge).reshape(src.shape[0], nd)
+    nt = trg.shape[0]
+    pot, grad, hess = np.zeros((nt, nd)), np.zeros((nt, dim, nd)), np.zeros((nt, nhess(dim), nd))
+    lib().orc_direct_pgh(dim, nd, float(delta), src.shape[0], _d(src), _d(q), nt, _d(trg), pgh,
+                         _d(pot), _d(grad), _d(hess), nthreads)
+    return pot, grad, hess
 
 
 def direct(dim, nd, delta, sources, charge, targ, nthreads=0):

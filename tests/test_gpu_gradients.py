@@ -1,0 +1,140 @@
+"""GPU parity of gradients and Hessians (ifpgh / ifpghtarg = 2, 3) against the
+oracle's restatement of g2dlevalg/h_vec, g2dpwevalg/h_vec, g2d_directcg/ch_vec
+(2d/planewave/src/g2drouts.f:905-1085, 1973-2200; g2ddirect.f:83-212) and the
+3D twins, through the C ABI.
+
+Bars (relative l2 per output array, the reference test's ``derr``):
+  * FP64 vs oracle: <= 1e-2 * eps for pot and grad, <= 0.1 * eps for the
+    Hessian (same routes and orders; differentiation amplifies rounding)
+  * mixed vs oracle: <= eps (pot), 10 * eps (grad, Hessian)
+  * vs the exact direct sum: no worse than twice the oracle's own error
+    (or 10 * eps), i.e. the reference's accuracy for derivatives
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NSAMPLE = 300
+
+
+def _cases():
+    rng = np.random.default_rng(7)
+
+    def unif(n, d):
+        return rng.random((n, d))
+
+    def circle(n):
+        th = rng.random(n) * 2 * np.pi
+        r = 0.3 + rng.normal(0, 1e-3, n)
+        pts = np.c_[0.5 + r * np.cos(th), 0.5 + r * np.sin(th)]
+        pts[: n // 10] = rng.random((n // 10, 2))
+        return pts
+
+    out = []
+    # name, dim, nd, delta, eps, sources, targets, ifpgh, ifpghtarg
+    out.append(("2d_unif_h", 2, 1, 1e-4, 1e-6, unif(40000, 2), unif(30000, 2), 3, 3))
+    out.append(("2d_unif_g", 2, 1, 1e-4, 1e-6, unif(40000, 2), unif(30000, 2), 2, 2))
+    out.append(("2d_unif_e9_h", 2, 1, 1e-4, 1e-9, unif(30000, 2), unif(20000, 2), 3, 3))
+    out.append(("2d_circle_h", 2, 1, 1e-6, 1e-6, circle(60000), circle(20000), 3, 1))
+    out.append(("2d_mixed_flags", 2, 2, 1e-3, 1e-3, unif(20000, 2), unif(10000, 2), 2, 3))
+    out.append(("2d_targets_only", 2, 1, 3e-5, 1e-6, unif(20000, 2), unif(20000, 2), 0, 3))
+    out.append(("3d_unif_h", 3, 1, 1e-3, 1e-6, unif(20000, 3), unif(10000, 3), 3, 3))
+    out.append(("3d_unif_g", 3, 1, 1e-3, 1e-6, unif(20000, 3), unif(10000, 3), 2, 2))
+    out.append(("3d_e3_h", 3, 1, 1e-2, 1e-3, unif(20000, 3), unif(10000, 3), 3, 3))
+    out.append(("3d_e3_g", 3, 1, 1e-2, 1e-3, unif(20000, 3), unif(10000, 3), 2, 2))
+    out.append(("3d_e9_h", 3, 1, 1e-4, 1e-9, unif(20000, 3), unif(5000, 3), 3, 3))
+    # the cut level evaluates by plane waves: ((p + 1) / npw)^3 >= 3 (fgt3d.f:1302-1311)
+    out.append(("3d_pw_route_h", 3, 1, 1e-3, 1e-5, unif(20000, 3), unif(10000, 3), 3, 3))
+    out.append(("3d_nd2_flags", 3, 2, 1e-3, 1e-6, unif(10000, 3), unif(5000, 3), 3, 2))
+    out.append(("2d_alldirect_h", 2, 1, 1e-6, 1e-6, unif(3000, 2), unif(2000, 2), 3, 3))
+    out.append(("3d_alldirect_h", 3, 1, 1e-4, 1e-6, unif(3000, 3), unif(2000, 3), 3, 3))
+    out.append(("2d_large_delta_h", 2, 1, 10.0, 1e-6, unif(3000, 2), unif(2000, 2), 3, 3))
+    out.append(("3d_large_delta_g", 3, 1, 10.0, 1e-6, unif(3000, 3), unif(2000, 3), 2, 2))
+    out.append(("3d_large_delta_h", 3, 1, 10.0, 1e-6, unif(3000, 3), unif(2000, 3), 3, 3))
+    return out
+
+
+CASES = _cases()
+KEYS = (("pot", "grad", "hess"), ("pottarg", "gradtarg", "hesstarg"))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gradients(case, precision, fgt, oracle):
+    name, dim, nd, delta, eps, src, trg, ifpgh, ifpghtarg = case
+    if precision == "mixed" and eps < 1e-6:
+        pytest.skip("the mixed form applies at eps >= 1e-6")
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    q = 2 * rng.random((src.shape[0], nd)) - 1
+    ctx = fgt.Context(0, precision=precision)
+    got = fgt.transform_pgh(dim, nd, delta, eps, src, q, trg, ifpgh, ifpghtarg, ctx=ctx)
+    ref = oracle.fgt_pgh(dim, nd, delta, eps, src, q, trg, ifpgh, ifpghtarg)
+    for flag, pts, keys in ((ifpgh, src, KEYS[0]), (ifpghtarg, trg, KEYS[1])):
+        if flag == 0:
+            for k in keys:
+                assert got[k] is None
+            continue
+        idx = rng.choice(pts.shape[0], min(NSAMPLE, pts.shape[0]), replace=False)
+        exact = oracle.direct_pgh(dim, nd, delta, src, q, pts[idx], pgh=flag)
+        for order, k in enumerate(keys[:flag]):
+            e_ref = oracle.derr(ref[k], got[k])
+            e_dir = oracle.derr(exact[order], got[k][idx])
+            e_orc = oracle.derr(exact[order], ref[k][idx])
+            if precision == "fp64":
+                tol = (1e-2 if order < 2 else 1e-1) * eps
+            else:
+                tol = eps if order == 0 else 10 * eps
+            print(f"{name} {precision} {k}: vs oracle {e_ref:.2e} (tol {tol:.0e}) vs direct "
+                  f"{e_dir:.2e} (oracle {e_orc:.2e})")
+            assert e_ref <= tol, (k, e_ref, tol)
+            assert e_dir <= max(10 * eps, 2 * e_orc), (k, e_dir, e_orc)
+
+
+def test_gradients_plan_api(fgt, oracle):
+    """Plan create once, apply twice with host and device arrays: the same
+    outputs as the one-shot call, bitwise."""
+    import torch
+    rng = np.random.default_rng(11)
+    dim, nd, delta, eps = 2, 1, 1e-4, 1e-6
+    src, trg = rng.random((30000, 2)), rng.random((20000, 2))
+    q = rng.random((30000, nd))
+    ctx = fgt.Context(0, precision="fp64")
+    one = fgt.transform_pgh(dim, nd, delta, eps, src, q, trg, 3, 2, ctx=ctx)
+    plan = fgt.Plan(ctx, dim, nd, delta, eps, src, trg, 3, 2)
+    for _ in range(2):
+        o = plan.execute_host_pgh(q)
+        for k in ("pot", "grad", "hess", "pottarg", "gradtarg"):
+            assert np.array_equal(o[k], one[k]), k
+    dev = torch.device("cuda", 0)
+    dq = torch.from_numpy(q).to(dev)
+    out = {k: torch.zeros(one[k].shape, dtype=torch.float64, device=dev)
+           for k in ("pot", "grad", "hess", "pottarg", "gradtarg")}
+    torch.cuda.synchronize()
+    plan.execute_device_pgh(dq.data_ptr(), out["pot"].data_ptr(), out["grad"].data_ptr(),
+                            out["hess"].data_ptr(), out["pottarg"].data_ptr(),
+                            out["gradtarg"].data_ptr(), 0, stream=ctx.stream)
+    torch.cuda.synchronize()
+    for k, v in out.items():
+        assert np.array_equal(v.cpu().numpy(), one[k]), k
+    # a NULL gradient array is skipped; the potential still comes back
+    pot_only = torch.zeros_like(out["pot"])
+    plan.execute_device_pgh(dq.data_ptr(), pot_only.data_ptr(), 0, 0, out["pottarg"].data_ptr(), 0,
+                            0, stream=ctx.stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(pot_only.cpu().numpy(), one["pot"])
+    plan.close()
+
+
+def test_gradients_reference_tuple(fgt, oracle):
+    """fgt2d / fgt3d return the reference's six outputs when a flag is >= 2."""
+    rng = np.random.default_rng(5)
+    src, trg, q = rng.random((5000, 3)), rng.random((3000, 3)), rng.random(5000)
+    pot, grad, hess, pt, gt, ht = fgt.fgt3d(1, 1e-3, 1e-6, src, q, trg, 2, 3,
+                                             ctx=fgt.Context(0, "fp64"))
+    assert pot.shape == (5000, 1) and grad.shape == (5000, 3, 1) and hess is None
+    assert pt.shape == (3000, 1) and gt.shape == (3000, 3, 1) and ht.shape == (3000, 6, 1)
+    ref = oracle.fgt_pgh(3, 1, 1e-3, 1e-6, src, q, trg, 2, 3)
+    assert oracle.derr(ref["hesstarg"], ht) <= 1e-7

@@ -73,3 +73,28 @@ def test_failed_request_does_not_stop_the_others(fgt):
         assert e.value.status == 1
     assert srv.stats()["failed"] == 2
     srv.close()
+
+
+def test_gradient_requests_mixed_in(fgt):
+    """Requests with gradients and Hessians among plain ones: each equals the
+    same request run alone, bitwise."""
+    rng = np.random.default_rng(13)
+    reqs = []
+    for k in range(10):
+        dim = 2 + k % 2
+        n = int(10 ** rng.uniform(3, 4.3))
+        src, trg, q = rng.random((n, dim)), rng.random((n // 2 + 1, dim)), rng.random(n)
+        reqs.append((dim, 1e-3 if dim == 3 else 1e-4, 1e-6, src, q, trg, k % 4, (k + 1) % 4))
+    ctx = fgt.Context(0, precision="auto")
+    alone = [fgt.transform_pgh(d, 1, de, ep, s, q, t, a, b, ctx=ctx) for d, de, ep, s, q, t, a, b in reqs]
+    srv = fgt.Server(0, workers=3, precision="auto")
+    ids = [srv.submit(d, 1, de, ep, s, q, t, a, b) for d, de, ep, s, q, t, a, b in reqs]
+    for ref, rid in zip(alone, ids):
+        got, lat = srv.wait_pgh(rid)
+        for k, v in ref.items():
+            if v is None:
+                assert got[k] is None
+            else:
+                assert np.array_equal(v, got[k]), k
+    assert srv.stats()["failed"] == 0
+    srv.close()

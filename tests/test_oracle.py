@@ -121,3 +121,55 @@ def test_derr_switches_to_absolute(oracle):
     ex = np.full(10, 1e-12)
     ap = ex + 1e-13
     assert abs(oracle.derr(ex, ap) - np.sqrt(10 * 1e-26) / 10) < 1e-20
+
+
+def test_direct_derivatives_by_finite_differences(oracle):
+    """The exact-sum gradient and Hessian (the checker of the gradient tests)
+    against central differences of the exact potential."""
+    rng = np.random.default_rng(3)
+    for dim in (2, 3):
+        delta = 1e-2
+        src, q = rng.random((200, dim)), rng.random((200, 1))
+        x = rng.random((5, dim))
+        p, g, h = oracle.direct_pgh(dim, 1, delta, src, q, x)
+        assert np.allclose(p, oracle.direct(dim, 1, delta, src, q, x), rtol=1e-14)
+        step = 1e-5
+        pairs = [(0, 0), (0, 1), (1, 1)] if dim == 2 else \
+            [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+        for d in range(dim):
+            e = np.zeros(dim)
+            e[d] = step
+            fd = (oracle.direct(dim, 1, delta, src, q, x + e) - oracle.direct(dim, 1, delta, src, q, x - e)) / (2 * step)
+            assert np.allclose(g[:, d], fd, rtol=1e-6, atol=1e-8)
+        for c, (a, b) in enumerate(pairs):
+            ea, eb = np.zeros(dim), np.zeros(dim)
+            ea[a] = step
+            eb[b] = step
+            fd = (oracle.direct_pgh(dim, 1, delta, src, q, x + eb)[1][:, a] -
+                  oracle.direct_pgh(dim, 1, delta, src, q, x - eb)[1][:, a]) / (2 * step)
+            assert np.allclose(h[:, c], fd, rtol=1e-5, atol=1e-6), (dim, c)
+
+
+@pytest.mark.parametrize("dim,n,delta,eps", [(2, 20000, 1e-4, 1e-6), (2, 10000, 1e-4, 1e-9),
+                                             (3, 10000, 1e-3, 1e-6), (3, 8000, 1e-2, 1e-3),
+                                             (2, 3000, 10.0, 1e-6), (3, 3000, 10.0, 1e-6)])
+def test_oracle_derivatives_vs_direct(oracle, dim, n, delta, eps):
+    """Gradients and Hessians of the restated transform (g2dlevalg/h_vec,
+    g2dpwevalg/h_vec, g2d_directcg/ch_vec and the 3D twins) against the exact
+    derivatives.  The reference raises the orders by the derivative order
+    and divides the plane-wave eps by 100 for Hessians (fgt2d.f:340-356);
+    its derivative error grows with the derivative order, so the bars are
+    10, 100 and 1000 eps."""
+    rng = np.random.default_rng(n + 7 * dim)
+    src, trg, q = rng.random((n, dim)), rng.random((n // 2, dim)), rng.random(n)
+    r = oracle.fgt_pgh(dim, 1, delta, eps, src, q, trg, 3, 3)
+    for pts, keys in ((src, ("pot", "grad", "hess")), (trg, ("pottarg", "gradtarg", "hesstarg"))):
+        idx = rng.choice(pts.shape[0], 150, replace=False)
+        exact = oracle.direct_pgh(dim, 1, delta, src, q, pts[idx])
+        for order, k in enumerate(keys):
+            assert oracle.derr(exact[order], r[k][idx]) <= 10 ** (order + 1) * eps, (k, order)
+    # pot-only requests through the gradient entry are the plain transform
+    # (up to the order of the near field's threaded accumulation)
+    r1 = oracle.fgt_pgh(dim, 1, delta, eps, src, q, trg, 1, 1)
+    pot, pt, _ = oracle.fgt(dim, 1, delta, eps, src, q, trg, 1, 1)
+    assert oracle.derr(pot, r1["pot"]) <= 1e-14 and oracle.derr(pt, r1["pottarg"]) <= 1e-14
