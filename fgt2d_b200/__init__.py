@@ -69,7 +69,8 @@ class Request(ctypes.Structure):
                 ("eps", ctypes.c_double), ("ns", ctypes.c_int), ("sources", _dp), ("charge", _dp),
                 ("nt", ctypes.c_int), ("targ", _dp), ("ifpgh", ctypes.c_int),
                 ("ifpghtarg", ctypes.c_int), ("pot", _dp), ("pottarg", _dp), ("grad", _dp),
-                ("hess", _dp), ("gradtarg", _dp), ("hesstarg", _dp)]
+                ("hess", _dp), ("gradtarg", _dp), ("hesstarg", _dp), ("ifdipole", ctypes.c_int),
+                ("rnormal", _dp), ("dipstr", _dp)]
 
 
 class ServerStats(ctypes.Structure):
@@ -112,6 +113,9 @@ def lib():
     L.fgt_plan_execute_host.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp]
     L.fgt_plan_execute_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.fgt_plan_execute_host_pgh.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.fgt_plan_create_cd.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, i, i, ctypes.POINTER(_vp)]
+    L.fgt_plan_execute_host_full.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.fgt_plan_execute_device_full.argtypes = [_vp] + [_vp] * 10
     L.fgt_plan_execute_device_pgh.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.fgt_plan_profile_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]
     L.fgt_plan_get_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
@@ -216,24 +220,28 @@ def _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg):
 
 
 def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
-                  ifcharge=1, ifdipole=0):
+                  ifcharge=1, ifdipole=0, rnormal=None, dipstr=None):
     """Whole transform with gradients (ifpgh / ifpghtarg = 2) and Hessians (3).
 
     Returns a dict with ``pot`` (ns, nd), ``grad`` (ns, dim, nd), ``hess``
     (ns, H, nd) and the same for the targets (``pottarg``, ``gradtarg``,
     ``hesstarg``), None where not requested: the reference's
-    ``grad(nd, dim, ns)`` / ``hess(nd, H, ns)`` in C order.
+    ``grad(nd, dim, ns)`` / ``hess(nd, H, ns)`` in C order.  Dipoles
+    (ifdipole = 1) take ``rnormal`` (ns, dim) and ``dipstr`` (ns, nd);
+    ifcharge = 0 ignores ``charge``.
     """
     L = lib()
     src = _f64(sources, (-1, dim))
     ns = src.shape[0]
-    q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
+    q = _f64(charge, (ns, nd)) if ns and ifcharge else None
+    rn = _f64(rnormal, (ns, dim)) if ifdipole else None
+    ds = _f64(dipstr, (ns, nd)) if ifdipole else None
     trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
     nt = trg.shape[0]
     o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg)
     h = ctx.handle if ctx is not None else _default_ctx()
     st = L.fgt_transform(h, dim, nd, float(delta), float(eps), ns, _p(src), ifcharge, _p(q),
-                         ifdipole, None, None, ifpgh, _p(o["pot"]), _p(o["grad"]), _p(o["hess"]),
+                         ifdipole, _p(rn), _p(ds), ifpgh, _p(o["pot"]), _p(o["grad"]), _p(o["hess"]),
                          nt, _p(trg), ifpghtarg, _p(o["pottarg"]), _p(o["gradtarg"]),
                          _p(o["hesstarg"]))
     _check(st, "fgt_transform")
@@ -241,12 +249,12 @@ def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpg
 
 
 def transform(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
-              ifcharge=1, ifdipole=0):
+              ifcharge=1, ifdipole=0, rnormal=None, dipstr=None):
     """Whole transform; returns ``(pot, pottarg)`` shaped ``(ns, nd)``, ``(nt, nd)``.
     With ifpgh or ifpghtarg >= 2 it returns the reference's six outputs
     ``(pot, grad, hess, pottarg, gradtarg, hesstarg)`` (see transform_pgh)."""
     o = transform_pgh(dim, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, ctx, ifcharge,
-                      ifdipole)
+                      ifdipole, rnormal, dipstr)
     if max(ifpgh, ifpghtarg) >= 2:
         return o["pot"], o["grad"], o["hess"], o["pottarg"], o["gradtarg"], o["hesstarg"]
     return o["pot"], o["pottarg"]
@@ -265,7 +273,8 @@ def fgt3d(nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=
 class Plan:
     """Tree, lists and device task arrays for fixed points; apply many times."""
 
-    def __init__(self, ctx, dim, nd, delta, eps, sources, targ=None, ifpgh=1, ifpghtarg=0):
+    def __init__(self, ctx, dim, nd, delta, eps, sources, targ=None, ifpgh=1, ifpghtarg=0,
+                 ifcharge=1, ifdipole=0):
         L = lib()
         self.ctx = ctx
         self.dim, self.nd = dim, nd
@@ -273,11 +282,24 @@ class Plan:
         trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
         self.ns, self.nt = src.shape[0], trg.shape[0]
         self.ifpgh, self.ifpghtarg = ifpgh, ifpghtarg
+        self.ifcharge, self.ifdipole = ifcharge, ifdipole
         h = _vp()
-        _check(L.fgt_plan_create(ctx.handle, dim, nd, float(delta), float(eps), self.ns, _p(src),
-                                 self.nt, _p(trg), ifpgh, ifpghtarg, ctypes.byref(h)),
-               "fgt_plan_create")
+        _check(L.fgt_plan_create_cd(ctx.handle, dim, nd, float(delta), float(eps), self.ns, _p(src),
+                                    self.nt, _p(trg), ifcharge, ifdipole, ifpgh, ifpghtarg,
+                                    ctypes.byref(h)), "fgt_plan_create_cd")
         self._h = h
+
+    def execute_host_full(self, charge=None, rnormal=None, dipstr=None):
+        """All outputs for the plan's source kinds and flags (dict as transform_pgh)."""
+        q = _f64(charge, (self.ns, self.nd)) if self.ifcharge else None
+        rn = _f64(rnormal, (self.ns, self.dim)) if self.ifdipole else None
+        ds = _f64(dipstr, (self.ns, self.nd)) if self.ifdipole else None
+        o = _outputs(self.dim, self.nd, self.ns, self.nt, self.ifpgh, self.ifpghtarg)
+        _check(lib().fgt_plan_execute_host_full(self._h, _p(q), _p(rn), _p(ds), _p(o["pot"]),
+                                                _p(o["grad"]), _p(o["hess"]), _p(o["pottarg"]),
+                                                _p(o["gradtarg"]), _p(o["hesstarg"])),
+               "fgt_plan_execute_host_full")
+        return o
 
     def info(self):
         inf = PlanInfo()
@@ -414,27 +436,32 @@ class Server:
         _check(L.fgt_server_set_precision(h, p), "fgt_server_set_precision")
         self._live = {}
 
-    def submit(self, dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0):
-        """Queues one transform; returns its id.  The arrays are kept alive here."""
+    def submit(self, dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0,
+               rnormal=None, dipstr=None):
+        """Queues one transform; returns its id.  The arrays are kept alive here.
+        ``charge`` None: no charges; ``dipstr`` given: dipoles with ``rnormal``."""
         src = _f64(sources, (-1, dim))
         ns = src.shape[0]
-        q = _f64(charge, (ns, nd)) if ns else np.zeros((0, nd))
+        q = None if charge is None else (_f64(charge, (ns, nd)) if ns else np.zeros((0, nd)))
+        ifd = int(dipstr is not None)
+        rn = _f64(rnormal, (ns, dim)) if ifd else None
+        ds = _f64(dipstr, (ns, nd)) if ifd else None
         trg = (src if targ is sources else _f64(targ, (-1, dim))) if targ is not None else None
         nt = trg.shape[0] if trg is not None else 0
         o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg)
         r = Request(dim, nd, float(delta), float(eps), ns, _p(src), _p(q), nt, _p(trg), ifpgh,
                     ifpghtarg, _p(o["pot"]), _p(o["pottarg"]), _p(o["grad"]), _p(o["hess"]),
-                    _p(o["gradtarg"]), _p(o["hesstarg"]))
+                    _p(o["gradtarg"]), _p(o["hesstarg"]), ifd, _p(rn), _p(ds))
         rid = ctypes.c_longlong()
         _check(lib().fgt_server_submit(self._h, ctypes.byref(r), ctypes.byref(rid)), "fgt_server_submit")
-        self._live[rid.value] = (src, q, trg, o)
+        self._live[rid.value] = (src, q, trg, o, rn, ds)
         return rid.value
 
     def wait_pgh(self, rid):
         """Blocks until request rid is done; returns (outputs dict, latency_s)."""
         lat = ctypes.c_double()
         st = lib().fgt_server_wait(self._h, int(rid), ctypes.byref(lat))
-        src, q, trg, o = self._live.pop(rid)
+        o = self._live.pop(rid)[3]
         _check(st, "fgt_server_wait")
         return o, lat.value
 

@@ -46,6 +46,8 @@ struct fgt_plan {
   double* d_trg = nullptr;
   double* d_pot = nullptr;
   double* d_pottarg = nullptr;
+  double* d_rn = nullptr;        // dipole directions and strengths (dipole plans)
+  double* d_ds = nullptr;
   double* d_grad = nullptr;      // gradients / Hessians when the flags ask for them
   double* d_hess = nullptr;
   double* d_gradtarg = nullptr;
@@ -103,7 +105,7 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
   if (nt > 0 && ifpghtarg > 0 && !targ) return FGT_ERR_BADARG;
   if (scan_points && !finite_all(sources, (size_t)ns * dim)) return FGT_ERR_BADARG;
   if (scan_points && nt > 0 && targ && !finite_all(targ, (size_t)nt * dim)) return FGT_ERR_BADARG;
-  if (ifcharge != 1 || ifdipole != 0) return FGT_ERR_UNSUPPORTED;
+  if (ifcharge < 0 || ifcharge > 1 || ifdipole < 0 || ifdipole > 1) return FGT_ERR_UNSUPPORTED;
   if (ifpgh < 0 || ifpgh > 3 || ifpghtarg < 0 || ifpghtarg > 3) return FGT_ERR_UNSUPPORTED;
   return FGT_OK;
 }
@@ -112,15 +114,16 @@ int check_args(int dim, int nd, double delta, double eps, int ns, const double* 
 // the outputs the flags ask for) and n_work doubles of large-delta work in one
 // allocation; uploads the points.
 int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int ifpgh, int ifpghtarg, size_t n_work,
-             const double* src_host, const double* trg_host, bool upload_trg) {
+             const double* src_host, const double* trg_host, bool upload_trg, int ifdipole = 0) {
   const size_t nh = dim == 2 ? 3 : 6;
   size_t n_src = (size_t)ns * dim, n_chg = (size_t)ns * nd, n_trg = (size_t)nt * dim;
+  size_t n_rn = ifdipole ? (size_t)ns * dim : 0, n_ds = ifdipole ? (size_t)ns * nd : 0;
   size_t n_pot = (size_t)ns * nd, n_pt = (size_t)nt * nd;
   size_t n_g = ifpgh >= 2 ? n_pot * dim : 0, n_h = ifpgh >= 3 ? n_pot * nh : 0;
   size_t n_gt = ifpghtarg >= 2 ? n_pt * dim : 0, n_ht = ifpghtarg >= 3 ? n_pt * nh : 0;
   auto al = [](size_t n) { return (n + 31) & ~size_t(31); };
   p->io_bytes = 8 * (al(n_src) + al(n_chg) + al(n_trg) + al(n_pot) + al(n_pt) + al(n_g) + al(n_h) +
-                     al(n_gt) + al(n_ht) + al(n_work) + 32);
+                     al(n_gt) + al(n_ht) + al(n_rn) + al(n_ds) + al(n_work) + 32);
   CKS(device_pool_setup());
   CKS(cudaMallocAsync(reinterpret_cast<void**>(&p->d_io), p->io_bytes, p->ctx->stream));
   double* c = p->d_io;
@@ -133,6 +136,8 @@ int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int ifpgh, int ifpght
   p->d_hess = n_h ? c : nullptr; c += al(n_h);
   p->d_gradtarg = n_gt ? c : nullptr; c += al(n_gt);
   p->d_hesstarg = n_ht ? c : nullptr; c += al(n_ht);
+  p->d_rn = n_rn ? c : nullptr; c += al(n_rn);
+  p->d_ds = n_ds ? c : nullptr; c += al(n_ds);
   p->d_work = c; c += al(n_work);
   p->d_flag = reinterpret_cast<int*>(c);
   cudaStream_t st = p->ctx->stream;
@@ -157,7 +162,7 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   const Params& P = p->H.P;
   const size_t n_work = P.large_delta ? large_delta_work_doubles(P, true) : 0;
   const int sa = alloc_io(p, P.dim, P.nd, P.ns, P.nt, P.ifpgh, P.ifpghtarg, n_work, src_host, trg_host,
-                         P.ifpghtarg > 0);
+                         P.ifpghtarg > 0, P.ifdipole);
   if (sa != FGT_OK) return sa;
   cudaStream_t st = p->ctx->stream;
   if (!P.large_delta) {
@@ -176,9 +181,10 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
 // status other than FGT_OK abandons the plan.
 int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double eps, int ns,
                             const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
-                            const std::function<int(size_t)>* admit = nullptr) {
+                            const std::function<int(size_t)>* admit = nullptr, int ifcharge = 1,
+                            int ifdipole = 0) {
   const bool same = targ == sources && nt == ns;
-  int st = alloc_io(p, dim, nd, ns, nt, ifpgh, ifpghtarg, 0, sources, targ, !same);
+  int st = alloc_io(p, dim, nd, ns, nt, ifpgh, ifpghtarg, 0, sources, targ, !same, ifdipole);
   if (st != FGT_OK) return st;
   st = check_finite_device(p, p->d_src, (size_t)ns * dim);
   if (st == FGT_OK && !same) st = check_finite_device(p, p->d_trg, (size_t)nt * dim);
@@ -195,7 +201,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   int *d_isrc = perms, *d_itarg = perms + ns + 1;
   try {
     CKS(build_plan_device(p->H, dim, nd, delta, eps, ns, p->d_src, nt, d_trg, same, ifpgh, ifpghtarg,
-                          d_isrc, d_itarg, s));
+                          d_isrc, d_itarg, s, ifcharge, ifdipole));
   } catch (const std::bad_alloc&) {
     return FGT_ERR_NOMEM;
   }
@@ -231,42 +237,73 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
 
 // Outputs the plan's flags ask for must be non-null except gradients and
 // Hessians, which are skipped when null.
-int run_device(fgt_plan* p, const double* q, const Outputs& o, cudaStream_t st, StageTimes* times) {
+int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st, StageTimes* times) {
   const Params& P = p->H.P;
   if ((P.ifpgh > 0 && P.ns > 0 && !o.pot) || (P.ifpghtarg > 0 && P.nt > 0 && !o.pottarg))
     return FGT_ERR_BADARG;
+  if ((P.ifcharge && !in.charge) || (P.ifdipole && (!in.rnormal || !in.dipstr))) return FGT_ERR_BADARG;
   int prec = resolve_precision(p->ctx, P.eps);
   if (!p->done) CKS(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
+  if (!P.ifcharge && !P.ifdipole) {  // no sources of either kind: zero fields
+    const size_t nd = P.nd, nh = P.dim == 2 ? 3 : 6;
+    auto z = [&](double* a, size_t n) { return a && n ? cudaMemsetAsync(a, 0, n * 8, st) : cudaSuccess; };
+    if (P.ifpgh >= 1) CKS(z(o.pot, P.ns * nd));
+    if (P.ifpgh >= 2) CKS(z(o.grad, P.ns * nd * P.dim));
+    if (P.ifpgh >= 3) CKS(z(o.hess, P.ns * nd * nh));
+    if (P.ifpghtarg >= 1) CKS(z(o.pottarg, P.nt * nd));
+    if (P.ifpghtarg >= 2) CKS(z(o.gradtarg, P.nt * nd * P.dim));
+    if (P.ifpghtarg >= 3) CKS(z(o.hesstarg, P.nt * nd * nh));
+    p->last_launches = 0;
+    CKS(cudaEventRecord(p->done, st));
+    return FGT_OK;
+  }
   if (P.large_delta) {
     Outputs lo = o;  // the large-delta kernels write every component they compute
     double* dg[4] = {p->d_grad, p->d_hess, p->d_gradtarg, p->d_hesstarg};
     double** og[4] = {&lo.grad, &lo.hess, &lo.gradtarg, &lo.hesstarg};
     for (int i = 0; i < 4; i++)
       if (!*og[i]) *og[i] = dg[i];
-    CKS(large_delta_execute(P, p->d_src, q, p->d_trg, lo, p->d_work, st, true));
+    CKS(large_delta_execute(P, p->d_src, in, p->d_trg, lo, p->d_work, st, true));
     p->last_launches = (P.ns > 0) + (P.ifpgh >= 1) + (P.ifpghtarg >= 1);
   } else {
-    CKS(device_plan_execute(p->D, q, o, prec, st, times));
+    CKS(device_plan_execute(p->D, in, o, prec, st, times));
     p->last_launches = (int)p->D.launches;
   }
   CKS(cudaEventRecord(p->done, st));
   return FGT_OK;
 }
 
-// Charges in from the host, every execute output the plan computes back to
-// the non-null host arrays of `host`.
-int exec_host(fgt_plan* p, const double* charge, const Outputs& host) {
+// Source strengths in from the host (charges and/or dipole directions and
+// strengths, as the plan's flags say), every execute output the plan
+// computes back to the non-null host arrays of `host`.
+int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const double* rnormal = nullptr,
+              const double* dipstr = nullptr) {
   const Params& P = p->H.P;
   cudaStream_t st = p->ctx->stream;
   CKS(cudaSetDevice(p->ctx->device));
   const size_t ns = P.ns, nt = P.nt, nd = P.nd, nh = P.dim == 2 ? 3 : 6;
-  CKS(cudaMemcpyAsync(p->d_chg, charge, ns * nd * 8, cudaMemcpyHostToDevice, st));
-  int s = check_finite_device(p, p->d_chg, ns * nd);
-  if (s != FGT_OK) return s;
+  Inputs in;
+  if (P.ifcharge) {
+    if (!charge && ns) return FGT_ERR_BADARG;
+    CKS(cudaMemcpyAsync(p->d_chg, charge, ns * nd * 8, cudaMemcpyHostToDevice, st));
+    int s = check_finite_device(p, p->d_chg, ns * nd);
+    if (s != FGT_OK) return s;
+    in.charge = p->d_chg;
+  }
+  if (P.ifdipole) {
+    if ((!rnormal || !dipstr) && ns) return FGT_ERR_BADARG;
+    CKS(cudaMemcpyAsync(p->d_rn, rnormal, ns * P.dim * 8, cudaMemcpyHostToDevice, st));
+    CKS(cudaMemcpyAsync(p->d_ds, dipstr, ns * nd * 8, cudaMemcpyHostToDevice, st));
+    int s = check_finite_device(p, p->d_rn, ns * P.dim);
+    if (s == FGT_OK) s = check_finite_device(p, p->d_ds, ns * nd);
+    if (s != FGT_OK) return s;
+    in.rnormal = p->d_rn;
+    in.dipstr = p->d_ds;
+  }
   Outputs d;
   d.pot = p->d_pot; d.grad = p->d_grad; d.hess = p->d_hess;
   d.pottarg = p->d_pottarg; d.gradtarg = p->d_gradtarg; d.hesstarg = p->d_hesstarg;
-  s = run_device(p, p->d_chg, d, st, nullptr);
+  int s = run_device(p, in, d, st, nullptr);
   if (s != FGT_OK) return s;
   auto back = [&](double* h, const double* dv, size_t n) -> cudaError_t {
     return h && dv && n ? cudaMemcpyAsync(h, dv, n * 8, cudaMemcpyDeviceToHost, st) : cudaSuccess;
@@ -281,15 +318,21 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host) {
   return FGT_OK;
 }
 
+int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                     const double* sources, int nt, const double* targ, int ifcharge, int ifdipole,
+                     int ifpgh, int ifpghtarg, fgt_plan** out);
+
 int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                    const double* sources, int ifcharge, const double* charge, int ifdipole,
+                   const double* rnormal, const double* dipstr,
                    int ifpgh, double* pot, double* grad, double* hess, int nt, const double* targ,
                    int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg) {
   const bool on_device = ctx->tree == FGT_TREE_DEVICE;
   int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg,
                       !on_device);
   if (st != FGT_OK) return st;
-  if (!on_device && ns > 0 && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
+  if (ns > 0 && ((ifcharge && !charge) || (ifdipole && (!rnormal || !dipstr)))) return FGT_ERR_BADARG;
+  if (!on_device && ns > 0 && ifcharge && !finite_all(charge, (size_t)ns * nd)) return FGT_ERR_BADARG;
   // outputs are written in full on success; zero them when nothing runs or
   // the call fails
   const size_t nh = dim == 2 ? 3 : 6;
@@ -311,12 +354,13 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
     return FGT_OK;
   }
   fgt_plan* plan = nullptr;
-  st = fgt_plan_create(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, &plan);
+  st = plan_create_impl(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifcharge, ifdipole, ifpgh,
+                        ifpghtarg, &plan);
   if (st == FGT_OK) {
     Outputs h;
     h.pot = pot; h.grad = grad; h.hess = hess;
     h.pottarg = pottarg; h.gradtarg = gradtarg; h.hesstarg = hesstarg;
-    st = exec_host(plan, charge, h);
+    st = exec_host(plan, charge, h, rnormal, dipstr);
     fgt_plan_destroy(plan);
   }
   if (st != FGT_OK) zero();
@@ -434,9 +478,25 @@ fgt_ctx* fgt_default_ctx(void) {
 int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                     fgt_plan** out) {
+  return plan_create_impl(ctx, dim, nd, delta, eps, ns, sources, nt, targ, 1, 0, ifpgh, ifpghtarg, out);
+}
+
+int fgt_plan_create_cd(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                       const double* sources, int nt, const double* targ, int ifcharge, int ifdipole,
+                       int ifpgh, int ifpghtarg, fgt_plan** out) {
+  return plan_create_impl(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifcharge, ifdipole, ifpgh,
+                          ifpghtarg, out);
+}
+
+}  // extern "C"
+
+namespace {
+int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                     const double* sources, int nt, const double* targ, int ifcharge, int ifdipole,
+                     int ifpgh, int ifpghtarg, fgt_plan** out) {
   if (!ctx || !out) return FGT_ERR_BADARG;
   *out = nullptr;
-  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg,
+  int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg,
                       ctx->tree != FGT_TREE_DEVICE);
   if (st != FGT_OK) return st;
   if (ns == 0) return FGT_ERR_BADARG;
@@ -446,10 +506,12 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
   p->ctx = ctx;
   CKS(cudaSetDevice(ctx->device));
   if (ctx->tree == FGT_TREE_DEVICE) {
-    st = plan_create_device_tree(p.get(), dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg);
+    st = plan_create_device_tree(p.get(), dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg,
+                                 nullptr, ifcharge, ifdipole);
   } else {
     try {
-      build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads);
+      build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads,
+                      ifcharge, ifdipole);
     } catch (const std::bad_alloc&) {
       return FGT_ERR_NOMEM;
     }
@@ -462,6 +524,9 @@ int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int
   *out = p.release();
   return FGT_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int fgt_plan_destroy(fgt_plan* p) {
   if (!p) return FGT_ERR_BADARG;
@@ -508,7 +573,9 @@ int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const
   Outputs o;
   o.pot = pot;
   o.pottarg = pt;
-  return run_device(p, q, o, st, nullptr);
+  Inputs in;
+  in.charge = q;
+  return run_device(p, in, o, st, nullptr);
 }
 
 int fgt_plan_execute_device_pgh(fgt_plan* p, const double* q, double* pot, double* grad, double* hess,
@@ -519,7 +586,35 @@ int fgt_plan_execute_device_pgh(fgt_plan* p, const double* q, double* pot, doubl
   Outputs o;
   o.pot = pot; o.grad = grad; o.hess = hess;
   o.pottarg = pottarg; o.gradtarg = gradtarg; o.hesstarg = hesstarg;
-  return run_device(p, q, o, st, nullptr);
+  Inputs in;
+  in.charge = q;
+  return run_device(p, in, o, st, nullptr);
+}
+
+int fgt_plan_execute_host_full(fgt_plan* p, const double* charge, const double* rnormal,
+                               const double* dipstr, double* pot, double* grad, double* hess,
+                               double* pottarg, double* gradtarg, double* hesstarg) {
+  if (!p) return FGT_ERR_BADARG;
+  Outputs h;
+  h.pot = pot; h.grad = grad; h.hess = hess;
+  h.pottarg = pottarg; h.gradtarg = gradtarg; h.hesstarg = hesstarg;
+  return exec_host(p, charge, h, rnormal, dipstr);
+}
+
+int fgt_plan_execute_device_full(fgt_plan* p, const double* q, const double* rnormal,
+                                 const double* dipstr, double* pot, double* grad, double* hess,
+                                 double* pottarg, double* gradtarg, double* hesstarg, void* stream) {
+  if (!p) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  Outputs o;
+  o.pot = pot; o.grad = grad; o.hess = hess;
+  o.pottarg = pottarg; o.gradtarg = gradtarg; o.hesstarg = hesstarg;
+  Inputs in;
+  in.charge = q;
+  in.rnormal = rnormal;
+  in.dipstr = dipstr;
+  return run_device(p, in, o, st, nullptr);
 }
 
 int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double* pt, double* ms,
@@ -532,7 +627,9 @@ int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double*
   Outputs o;
   o.pot = pot;
   o.pottarg = pt;
-  int r = run_device(p, q, o, p->ctx->stream, &T);
+  Inputs in;
+  in.charge = q;
+  int r = run_device(p, in, o, p->ctx->stream, &T);
   if (r != FGT_OK) return r;
   CKS(cudaStreamSynchronize(p->ctx->stream));
   *ms = T.dom_ms;
@@ -551,7 +648,9 @@ int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const
   Outputs o;
   o.pot = pot;
   o.pottarg = pt;
-  int r = run_device(p, q, o, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
+  Inputs in;
+  in.charge = q;
+  int r = run_device(p, in, o, p->ctx->stream, p->H.P.large_delta ? nullptr : &T);
   if (r != FGT_OK) return r;
   CKS(cudaStreamSynchronize(p->ctx->stream));
   for (int i = 0; i < 8; i++) ms8[i] = T.ms[i];
@@ -730,7 +829,8 @@ int fgt_transform(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int n
   (void)rnormal; (void)dipstr;
   if (!ctx) return FGT_ERR_BADARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  return transform_impl(ctx, dim, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh,
+  return transform_impl(ctx, dim, nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal,
+                        dipstr, ifpgh,
                         pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg);
 }
 
@@ -798,7 +898,8 @@ void fgt3d_st_(const int* nd, const double* delta, const double* eps, const int*
 template <typename IP>
 static int main_gpu(int dim, const int* nd, const double* delta, const double* eps,
                     const int* nsource, const double* sourcesort, const int* ifcharge,
-                    const double* chargesort, const int* ifdipole, const int* ntarget,
+                    const double* chargesort, const int* ifdipole, const double* rnormalsort,
+                    const double* dipstrsort, const int* ntarget,
                     const double* targetsort, const int* itree, const IP* iptr, const int* nlevels,
                     const int* npwlevel, const int* nboxes, const double* boxsize,
                     const double* centers, const int* laddr, const int* isrcse, const int* itargse,
@@ -859,6 +960,7 @@ static int main_gpu(int dim, const int* nd, const double* delta, const double* e
   Params P0;
   P0.dim = dim; P0.nd = *nd; P0.delta = *delta; P0.eps = *eps; P0.ns = ns; P0.nt = nt;
   P0.ifpgh = *ifpgh; P0.ifpghtarg = *ifpghtarg; P0.npwlevel = *npwlevel;
+  P0.ifcharge = *ifcharge; P0.ifdipole = *ifdipole;
   std::vector<int> nl(nlocal, nlocal + nlev + 1);
   try {
     build_host_plan_from_tree(p->H, P0, nl, *pmax, *npw);
@@ -878,7 +980,7 @@ static int main_gpu(int dim, const int* nd, const double* delta, const double* e
   Outputs h;
   h.pot = po.data(); h.grad = go.data(); h.hess = ho.data();
   h.pottarg = pt.data(); h.gradtarg = gt.data(); h.hesstarg = ht.data();
-  st = exec_host(p.get(), chargesort, h);
+  st = exec_host(p.get(), chargesort, h, rnormalsort, dipstrsort);
   fgt_plan_destroy(p.release());
   if (st != FGT_OK) return st;
   auto add = [](double* out, const std::vector<double>& v) {
@@ -907,10 +1009,10 @@ int fgt2dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                    const int* ntermmax, const double* pmax, const int* npw, const int* ifpgh,
                    double* pot, double* grad, double* hess, const int* ifpghtarg, double* pottarg,
                    double* gradtarg, double* hesstarg) {
-  (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
+  (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
   (void)ntermsh; (void)ntermmax;
   return main_gpu<int>(2, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
-                       ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
+                       rnormalsort, dipstrsort, ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
                        centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, grad, hess,
                        ifpghtarg, pottarg, gradtarg, hesstarg);
 }
@@ -927,10 +1029,10 @@ int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
                    const double* pmax, const int* npw, const int* ifpgh, double* pot, double* grad,
                    double* hess, const int* ifpghtarg, double* pottarg, double* gradtarg,
                    double* hesstarg) {
-  (void)rnormalsort; (void)dipstrsort; (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
+  (void)iaddr; (void)rmlexp; (void)ltree; (void)iper;
   (void)ndiv; (void)ntermsh; (void)ntermmax;
   return main_gpu<long long>(3, nd, delta, eps, nsource, sourcesort, ifcharge, chargesort, ifdipole,
-                             ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
+                             rnormalsort, dipstrsort, ntarget, targetsort, itree, iptr, nlevels, npwlevel, nboxes, boxsize,
                              centers, laddr, isrcse, itargse, nlocal, pmax, npw, ifpgh, pot, grad,
                              hess, ifpghtarg, pottarg, gradtarg, hesstarg);
 }
@@ -995,9 +1097,11 @@ void server_give(fgt_server* S, long long* in_use, long long b) {
 
 int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
   const int nt = r.targ ? r.nt : 0;
-  int st = check_args(r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, 1, 0, r.ifpgh, nt, r.targ,
-                      r.ifpghtarg, false);
+  const int ifcharge = r.charge != nullptr, ifdipole = r.ifdipole;
+  int st = check_args(r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, ifcharge, ifdipole, r.ifpgh, nt,
+                      r.targ, r.ifpghtarg, false);
   if (st != FGT_OK) return st;
+  if (ifdipole && r.ns > 0 && (!r.rnormal || !r.dipstr)) return FGT_ERR_BADARG;
   const size_t nh = r.dim == 2 ? 3 : 6;
   if ((r.ifpgh >= 1 && r.ns > 0 && !r.pot) || (r.ifpgh >= 2 && r.ns > 0 && !r.grad) ||
       (r.ifpgh >= 3 && r.ns > 0 && !r.hess) || (r.ifpghtarg >= 1 && nt > 0 && !r.pottarg) ||
@@ -1036,12 +1140,12 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
     return FGT_OK;
   };
   st = plan_create_device_tree(p.get(), r.dim, r.nd, r.delta, r.eps, r.ns, r.sources, nt, r.targ, r.ifpgh,
-                               r.ifpghtarg, &admit);
+                               r.ifpghtarg, &admit, ifcharge, ifdipole);
   if (st == FGT_OK) {
     Outputs h;
     h.pot = r.pot; h.grad = r.grad; h.hess = r.hess;
     h.pottarg = r.pottarg; h.gradtarg = r.gradtarg; h.hesstarg = r.hesstarg;
-    st = exec_host(p.get(), r.charge, h);
+    st = exec_host(p.get(), r.charge, h, r.rnormal, r.dipstr);
   }
   fgt_plan_destroy(p.release());
   cudaStreamSynchronize(ctx->stream);  // the stream-ordered frees have run

@@ -18,6 +18,14 @@ inline int out_comps(int dim, int pgh) {
   return pgh <= 0 ? 0 : pgh == 1 ? 1 : pgh == 2 ? 1 + dim : 1 + dim + (dim == 2 ? 3 : 6);
 }
 
+// Caller-order device inputs of one execute: charge (nd, ns) when the plan
+// has charges, rnormal (dim, ns) and dipstr (nd, ns) when it has dipoles.
+struct Inputs {
+  const double* charge = nullptr;
+  const double* rnormal = nullptr;
+  const double* dipstr = nullptr;
+};
+
 // Caller-order device outputs of one execute: pot (nd, ns), grad (nd, dim, ns),
 // hess (nd, H, ns) and the same at the targets; the ones the flags do not ask
 // for are ignored.
@@ -99,6 +107,8 @@ struct DevicePlan {
   int nmp = 0, nloc = 0;
   double* ssort = nullptr;  // sorted sources (ns, dim)
   double* csort = nullptr;  // sorted charges (ns, nd)
+  double* nsort = nullptr;  // sorted dipole directions (ns, dim), dipole plans only
+  double* dsort = nullptr;  // sorted dipole strengths (ns, nd), dipole plans only
   double* tsort = nullptr;  // sorted targets (nt, dim)
   double* psort = nullptr;  // sorted source outputs, per point [out_comps(dim, ifpgh)][nd]
   double* ptsort = nullptr; // sorted target outputs, per point [out_comps(dim, ifpghtarg)][nd]
@@ -160,7 +170,8 @@ cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_
                                    double* mn, double* mx, cudaStream_t st);
 cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                               const double* d_src, int nt, const double* d_trg, bool same, int ifpgh,
-                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st);
+                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st,
+                              int ifcharge = 1, int ifdipole = 0);
 void device_plan_destroy(DevicePlan& D);
 
 // Sorts the plan's points into tree order once: device arrays in the
@@ -170,7 +181,7 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
 // Runs charge gather -> stages -> scatter on `stream`.  Device pointers in
 // the caller's order: charge (ns, nd) and the outputs.
 // times (optional) receives per-stage milliseconds (synchronises).
-cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs& out,
+cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& out,
                                 int precision, cudaStream_t stream, StageTimes* times);
 
 // Sets *d_flag (device int, not cleared here) when any of x[0, n) is not
@@ -194,7 +205,7 @@ size_t large_delta_noalloc_capacity();
 // through per-CTA partial blocks (work must hold large_delta_work_doubles(P,
 // true) doubles); otherwise they are added atomically (nd (nlocal0+1)^dim + 4
 // doubles of work; results can differ in the last bits from call to call).
-cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
+cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs& in,
                                 const double* trg, const Outputs& out, double* work,
                                 cudaStream_t stream, bool deterministic);
 size_t large_delta_work_doubles(const Params& P, bool deterministic);

@@ -312,7 +312,8 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
 
 cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                               const double* d_src, int nt, const double* d_trg, bool same, int ifpgh,
-                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st) {
+                              int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st,
+                              int ifcharge, int ifdipole) {
   const double tstart = now_s();
   double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
   CKD(device_bbox(d_src, ns, d_trg, same ? 0 : nt, dim, mn, mx, st));
@@ -320,7 +321,8 @@ cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double
   double bs0, cen0[3] = {0, 0, 0};
   boxsize0_bbox(dim, delta, eps, mn, mx, &npwlevel, &bs0, cen0);
   TreeSetup ts;
-  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts)) {
+  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts, ifcharge,
+                  ifdipole)) {
     H.host_tree_s = now_s() - tstart;
     return cudaSuccess;
   }

@@ -54,7 +54,22 @@ struct KP {
   double* pot;      // sorted outputs of the sources: per point [nc_s][nd]
   double* pottarg;  // sorted outputs of the targets: per point [nc_t][nd]
   int nc_s, nc_t;   // components per density written: 1 (pot), 1 + dim (+ grad), + H (+ Hessian)
+  int ifcharge, ifdipole;
+  const double* dnrm;  // sorted dipole directions (ns, dim)
+  const double* dstr;  // sorted dipole strengths (ns, nd)
 };
+
+// Source weights of density ind at sorted source i: the charge (0 without
+// charges) and the dipole vector dipstr * n (zeros without dipoles).
+__device__ __forceinline__ double src_charge(const KP& k, long long i, int ind) {
+  return k.ifcharge ? k.chg[i * k.nd + ind] : 0.0;
+}
+template <int DIM>
+__device__ __forceinline__ void src_dipole(const KP& k, long long i, int ind, double* v) {
+  const double s = k.dstr[i * k.nd + ind];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) v[d] = s * k.dnrm[i * DIM + d];
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -100,6 +115,34 @@ __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// A staged factor row of a dipole source column: a h_j + b dh_j for j < Pn
+// at stride `st`, with h_j = v^j / sqrt(j!) and dh_j = sqrt(j) dsq h_(j-1)
+// (the source-coordinate derivative, g3dformhd_vec's dxhx).
+__device__ __forceinline__ void dip_row(double* row, int st, int Pn, double v, double a, double b,
+                                        double dsq, const double* __restrict__ isq) {
+  double h = 1.0;
+  row[0] = a;
+  for (int j = 1; j < Pn; j++) {
+    const double dh = j * isq[j] * dsq * h;
+    h = h * v * isq[j];
+    row[j * st] = fma(a, h, b * dh);
+  }
+}
+// The three columns of a 3D dipole source (g3dformhd_vec / g3dformhcd_vec,
+// g3drouts.f:197-405): H += hx hy (q hz + v3 dhz) + hx dhy (v2 hz) + dhx hy (v1 hz).
+// Coefficients (a, b) of the factor along d (0 x, 1 y, 2 z) in column c.
+__device__ __forceinline__ void dip3_coef(int c, int d, double q, const double* v, double& a,
+                                          double& b) {
+  if (d == 2) {
+    a = c == 0 ? q : c == 1 ? v[1] : v[0];
+    b = c == 0 ? v[2] : 0.0;
+  } else {
+    const bool deriv = (d == 1 && c == 1) || (d == 0 && c == 2);
+    a = deriv ? 0.0 : 1.0;
+    b = deriv ? 1.0 : 0.0;
+  }
 }
 
 // ------------------------------------------------------------ outputs: potential, gradient, Hessian
@@ -338,6 +381,8 @@ __global__ void k_unsort(const double* __restrict__ in, double* __restrict__ out
 // sources are split over G thread groups (split-K), reduced at the end.  Then
 // the two 1D Hermite -> plane-wave passes (g2dh2pw_real_vec,
 // g2drouts.f:1276-1326) run in shared memory.
+// With dipoles each source contributes two columns (as k_form2d_mma):
+// (hx, q hy + v2 dhy) and (v1 dhx, hy), dh_j = sqrt(j) dsq h_(j-1).
 __global__ void __launch_bounds__(256) k_form2d(KP k, const FormTask* __restrict__ tasks,
                                                 const double* __restrict__ isq, int ch) {
   const FormTask T = tasks[blockIdx.x];
@@ -359,19 +404,37 @@ __global__ void __launch_bounds__(256) k_form2d(KP k, const FormTask* __restrict
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-  for (int c0 = 0; c0 < T.n; c0 += ch) {
-    const int m = min(ch, T.n - c0);
+  const int vc = k.ifdipole ? 2 : 1;     // columns per source
+  const int chs = k.ifdipole ? ch / 2 : ch;  // sources per chunk
+  for (int s0c = 0; s0c < T.n; s0c += chs) {
+    const int ms = min(chs, T.n - s0c), m = vc * ms;
     for (int r = tid; r < 2 * m; r += 256) {
       const int t = r >> 1, kind = r & 1;
-      const int i = T.s0 + c0 + t;
-      double v, w;
-      if (kind == 0) { v = (k.src[2 * i] - cx) * k.dsq; w = 1.0; }
-      else { v = (k.src[2 * i + 1] - cy) * k.dsq; w = k.chg[(size_t)i * k.nd + ind]; }
+      const int i = T.s0 + s0c + t / vc;
+      const double v = kind == 0 ? (k.src[2 * i] - cx) * k.dsq : (k.src[2 * i + 1] - cy) * k.dsq;
       double* row = (kind ? ys : xs) + t * Pp;
-      row[0] = w;
-      for (int j = 1; j < Pn; j++) {
-        w = w * v * isq[j];
-        row[j] = w;
+      if (!k.ifdipole) {
+        double w = kind == 0 ? 1.0 : k.chg[(size_t)i * k.nd + ind];
+        row[0] = w;
+        for (int j = 1; j < Pn; j++) {
+          w = w * v * isq[j];
+          row[j] = w;
+        }
+      } else {
+        // a h_j + b dh_j for the column's factor
+        double dv[2];
+        src_dipole<2>(k, i, ind, dv);
+        const bool c1 = t & 1;
+        double a, b;
+        if (kind == 0) { a = c1 ? 0.0 : 1.0; b = c1 ? dv[0] : 0.0; }
+        else { a = c1 ? 1.0 : src_charge(k, i, ind); b = c1 ? 0.0 : dv[1]; }
+        double h = 1.0;
+        row[0] = a;
+        for (int j = 1; j < Pn; j++) {
+          const double dh = j * isq[j] * k.dsq * h;
+          h = h * v * isq[j];
+          row[j] = fma(a, h, b * dh);
+        }
       }
       for (int j = Pn; j < Pp; j++) row[j] = 0.0;
     }
@@ -435,7 +498,7 @@ __global__ void __launch_bounds__(256) k_form2d(KP k, const FormTask* __restrict
 template <int MAXP>
 __global__ void __launch_bounds__(256) k_form3d_hermite(KP k, const FormTask* __restrict__ tasks,
                                                         int ntasks, double2* __restrict__ scratch,
-                                                        size_t slab) {
+                                                        size_t slab, const double* __restrict__ isq) {
   extern __shared__ double sm[];
   const int npw = k.npw, n2 = k.n2;
   double2* T1 = scratch + slab * blockIdx.x;
@@ -451,21 +514,34 @@ __global__ void __launch_bounds__(256) k_form3d_hermite(KP k, const FormTask* __
                  cz = k.centers[3 * T.box + 2];
     for (int e = threadIdx.x; e < P3; e += blockDim.x) H[e] = 0.0;
     __syncthreads();
-    for (int c0 = 0; c0 < T.n; c0 += FORM_CH) {
-      const int m = min(FORM_CH, T.n - c0);
+    // dipoles: three columns per source (dip3_coef), 10 sources per chunk
+    const int vc = k.ifdipole ? 3 : 1, chs = FORM_CH / vc;
+    for (int c0 = 0; c0 < T.n; c0 += chs) {
+      const int m = vc * min(chs, T.n - c0);
       if (threadIdx.x < m) {
-        const int i = T.s0 + c0 + threadIdx.x;
+        const int i = T.s0 + c0 + threadIdx.x / vc;
         const double x = (k.src[3 * i] - cx) * k.dsq, y = (k.src[3 * i + 1] - cy) * k.dsq,
                      z = (k.src[3 * i + 2] - cz) * k.dsq;
         double* xr = X + threadIdx.x * Pn;
         double* yr = Y + threadIdx.x * Pn;
         double* zr = Z + threadIdx.x * Pn;
-        double xv = 1.0, yv = 1.0, zv = k.chg[(size_t)i * k.nd + ind];
-        xr[0] = xv; yr[0] = yv; zr[0] = zv;
-        for (int j = 1; j < Pn; j++) {
-          double sj = sqrt((double)j);
-          xv = xv * x / sj; yv = yv * y / sj; zv = zv * z / sj;
-          xr[j] = xv; yr[j] = yv; zr[j] = zv;
+        if (!k.ifdipole) {
+          double xv = 1.0, yv = 1.0, zv = k.chg[(size_t)i * k.nd + ind];
+          xr[0] = xv; yr[0] = yv; zr[0] = zv;
+          for (int j = 1; j < Pn; j++) {
+            double sj = sqrt((double)j);
+            xv = xv * x / sj; yv = yv * y / sj; zv = zv * z / sj;
+            xr[j] = xv; yr[j] = yv; zr[j] = zv;
+          }
+        } else {
+          double dv[3], a, b;
+          src_dipole<3>(k, i, ind, dv);
+          const double q = src_charge(k, i, ind), cv[3] = {x, y, z};
+          double* rows[3] = {xr, yr, zr};
+          for (int d = 0; d < 3; d++) {
+            dip3_coef(threadIdx.x % vc, d, q, dv, a, b);
+            dip_row(rows[d], 1, Pn, cv[d], a, b, k.dsq, isq);
+          }
         }
       }
       __syncthreads();
@@ -584,7 +660,13 @@ __device__ __forceinline__ void warp_gemm(const double* A, int lda, const double
   }
 }
 
-template <int NT>
+// With dipoles (DIP) the source derivative enters as a second column per
+// source (g2dformhd_vec / g2dformhcd_vec, g2drouts.f:173-338; in the
+// unnormalised powers here d/dX x^j = j dsq x^(j-1)):
+//   column 0: X = x^j,               Y = q y^k + v2 k dsq y^(k-1)
+//   column 1: X = v1 j dsq x^(j-1),  Y = y^k
+// (v = dipstr * n), so a block of 32 columns holds 16 sources.
+template <int NT, bool DIP>
 __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __restrict__ tasks,
                                                     const long long* __restrict__ hoff,
                                                     double* __restrict__ hbuf) {
@@ -610,25 +692,50 @@ __global__ void __launch_bounds__(128) k_form2d_mma(KP k, const FormTask* __rest
   // powers of one source in shared memory, then the warp runs up to eight
   // K = 4 steps of the FP64 MMA over the block, alternating two accumulator
   // sets so consecutive steps are independent
-  for (int base = 32 * warp; base < T.n; base += 128) {
-    double x = 0.0, y = 0.0, q = 0.0;
-    if (base + lane < T.n) {
-      const int i = T.s0 + base + lane;
+  constexpr int SPB = DIP ? 16 : 32;  // sources per 32-column block
+  for (int base = SPB * warp; base < T.n; base += 4 * SPB) {
+    const int sl = DIP ? lane >> 1 : lane;
+    double x = 0.0, y = 0.0, q = 0.0, v[2] = {0.0, 0.0};
+    if (base + sl < T.n) {
+      const int i = T.s0 + base + sl;
       const double2 pt = reinterpret_cast<const double2*>(k.src)[i];
       x = (pt.x - cx) * k.dsq;
       y = (pt.y - cy) * k.dsq;
-      q = k.chg[(size_t)i * k.nd + ind];
+      if (DIP) {
+        q = src_charge(k, i, ind);
+        src_dipole<2>(k, i, ind, v);
+      } else {
+        q = k.chg[(size_t)i * k.nd + ind];
+      }
     }
-    double xp = 1.0, yp = q;
+    if (!DIP) {
+      double xp = 1.0, yp = q;
 #pragma unroll
-    for (int j = 0; j < PP; j++) {
-      X[j * SW + lane] = xp;
-      Y[j * SW + lane] = yp;
-      xp *= x;
-      yp *= y;
+      for (int j = 0; j < PP; j++) {
+        X[j * SW + lane] = xp;
+        Y[j * SW + lane] = yp;
+        xp *= x;
+        yp *= y;
+      }
+    } else {
+      // column (lane & 1): powers and their derivatives, one pass
+      const bool c1 = lane & 1;
+      const double ax = c1 ? 0.0 : 1.0, bx = c1 ? v[0] * k.dsq : 0.0;
+      const double ay = c1 ? 1.0 : q, by = c1 ? 0.0 : v[1] * k.dsq;
+      double xp = 1.0, yp = 1.0, xm = 0.0, ym = 0.0;  // x^j, j x^(j-1)
+#pragma unroll
+      for (int j = 0; j < PP; j++) {
+        X[j * SW + lane] = fma(ax, xp, bx * xm);
+        Y[j * SW + lane] = fma(ay, yp, by * ym);
+        xm = fma(xm, x, xp);  // (j+1) x^j = j x^(j-1) x + x^j
+        ym = fma(ym, y, yp);
+        xp *= x;
+        yp *= y;
+      }
     }
     __syncwarp();
-    const int nst = min(8, (T.n - base + 3) >> 2);
+    const int ncol = DIP ? 2 * min(SPB, T.n - base) : T.n - base;
+    const int nst = min(8, (ncol + 3) >> 2);
     for (int st = 0; st < nst; st += 2) {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
@@ -814,11 +921,14 @@ __global__ void __launch_bounds__(128) k_h2pw2d(KP k, const FormTask* __restrict
 // eight warps split the N tiles (up to four each per pass over the sources).
 // The partial block goes to the chunk's slot of the Hermite buffer, laid out
 // H[j + P (k + P l)] as k_form3d_h2pw reads it.
-template <int MT>
+// With dipoles (DIP) every source stages three columns (dip3_coef), 21
+// sources (63 columns) per batch.
+template <int MT, bool DIP>
 __global__ void __launch_bounds__(256) k_form3d_mma(KP k, const FormTask* __restrict__ tasks,
                                                     const FormChunk* __restrict__ chunks,
                                                     double* __restrict__ hbuf, const double* __restrict__ isq) {
   constexpr int SB = 64, SW = 68, NTW = 4;
+  constexpr int VC = DIP ? 3 : 1, SBS = SB / VC;  // columns per source, sources per batch
   const FormChunk C = chunks[blockIdx.x];
   const FormTask T = tasks[C.task];
   const int ind = blockIdx.y;
@@ -842,22 +952,34 @@ __global__ void __launch_bounds__(256) k_form3d_mma(KP k, const FormTask* __rest
 #pragma unroll
       for (int mt = 0; mt < MT; mt++) acc[mt][i][0] = acc[mt][i][1] = 0.0;
     }
-    for (int c0 = 0; c0 < C.n; c0 += SB) {
-      const int m = min(SB, C.n - c0);
+    for (int c0 = 0; c0 < C.n; c0 += SBS) {
+      const int m = VC * min(SBS, C.n - c0);
       __syncthreads();
       for (int job = threadIdx.x; job < 3 * SB; job += blockDim.x) {
         const int t = job / 3, d = job - 3 * t;
-        double v = 0.0, w = 0.0;
-        if (t < m) {
-          const int i = C.s0 + c0 + t;
-          v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
-          w = d == 2 ? k.chg[(size_t)i * k.nd + ind] : 1.0;
-        }
         double* row = (d == 0 ? X : d == 1 ? Y : Z) + t;
-        row[0] = w;
-        for (int j = 1; j < Pn; j++) {
-          w = w * v * isq[j];
-          row[j * SW] = w;
+        if (!DIP) {
+          double v = 0.0, w = 0.0;
+          if (t < m) {
+            const int i = C.s0 + c0 + t;
+            v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
+            w = d == 2 ? k.chg[(size_t)i * k.nd + ind] : 1.0;
+          }
+          row[0] = w;
+          for (int j = 1; j < Pn; j++) {
+            w = w * v * isq[j];
+            row[j * SW] = w;
+          }
+        } else {
+          double v = 0.0, a = 0.0, b = 0.0;
+          if (t < m) {
+            const int i = C.s0 + c0 + t / VC;
+            v = (k.src[3 * i + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
+            double dv[3];
+            src_dipole<3>(k, i, ind, dv);
+            dip3_coef(t % VC, d, src_charge(k, i, ind), dv, a, b);
+          }
+          dip_row(row, SW, Pn, v, a, b, k.dsq, isq);
         }
       }
       __syncthreads();
@@ -1510,14 +1632,21 @@ __global__ void __launch_bounds__(256) k_form3d_pw(KP k, const FormTask* __restr
       i2[s] = (e / npw) % npw;
       i1[s] = e / (npw * npw);
     }
-    for (int c0 = 0; c0 < T.n; c0 += FORM_CH) {
-      const int m = min(FORM_CH, T.n - c0);
+    // dipoles (g3dformpwd_vec / g3dformpwcd_vec, g3drouts.f:2042-2262): three
+    // columns per source, the factor of one dimension times v_d (-i t dsq)
+    // in each (as dip3_coef), 10 sources per chunk
+    const int vc = k.ifdipole ? 3 : 1, chs = FORM_CH / vc;
+    for (int c0 = 0; c0 < T.n; c0 += chs) {
+      const int m = vc * min(chs, T.n - c0);
       __syncthreads();
       if (threadIdx.x < m) {
-        const int i = T.s0 + c0 + threadIdx.x;
+        const int i = T.s0 + c0 + threadIdx.x / vc, col = threadIdx.x % vc;
         const double x = (k.src[3 * i] - cx) * k.dsq, y = (k.src[3 * i + 1] - cy) * k.dsq,
                      z = (k.src[3 * i + 2] - cz) * k.dsq;
-        const double q = k.chg[(size_t)i * k.nd + ind];
+        double dv[3] = {0.0, 0.0, 0.0}, ca[3], cb[3];
+        if (k.ifdipole) src_dipole<3>(k, i, ind, dv);
+        const double q = k.ifdipole ? src_charge(k, i, ind) : k.chg[(size_t)i * k.nd + ind];
+        for (int d = 0; d < 3; d++) dip3_coef(col, d, q, dv, ca[d], cb[d]);
         // positive node m: t = (2m+1) t1 at index n2+m; its mirror n2-1-m
         double2 ex = cexpi(-k.t1 * x), ey = cexpi(-k.t1 * y), ez = cexpi(-k.t1 * z);
         const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey), ezz = cmul(ez, ez);
@@ -1528,6 +1657,16 @@ __global__ void __launch_bounds__(256) k_form3d_pw(KP k, const FormTask* __restr
           const double w = k.ws[n2 + mm];
           double2 a = make_double2(ex.x * w, ex.y * w), b = make_double2(ey.x * w, ey.y * w),
                   c = make_double2(ez.x * w * q, ez.y * w * q);
+          if (k.ifdipole) {
+            // ca f + cb f (-i t dsq) per dimension, f = w e^{-i t x}
+            const double td = (2 * mm + 1) * k.t1 * k.dsq;
+            auto mix = [td](double2 f, double p0, double p1) {
+              return make_double2(fma(p0, f.x, p1 * td * f.y), fma(p0, f.y, -p1 * td * f.x));
+            };
+            a = mix(a, ca[0], cb[0]);
+            b = mix(b, ca[1], cb[1]);
+            c = mix(make_double2(ez.x * w, ez.y * w), ca[2], cb[2]);
+          }
           f1[n2 + mm] = a; f1[n2 - 1 - mm] = make_double2(a.x, -a.y);
           f2[n2 + mm] = b; f2[n2 - 1 - mm] = make_double2(b.x, -b.y);
           f3[n2 - 1 - mm] = make_double2(c.x, -c.y);
@@ -1952,14 +2091,58 @@ __device__ __forceinline__ void pair_terms(double* acc, double r, const double* 
     }
   }
 }
+// Dipole terms per pair (g2d_directd{p,g,h}_vec, g2ddirect.f:217-420, and
+// g3d_directd*_vec, g3ddirect.f:207-435), v = dipstr n, e = exp(-r^2/delta):
+// with R = 2/delta, u = R (t - s), rinc = u.v,
+//   pot += rinc e,  grad_a += g_a e with g_a = R v_a - rinc u_a,
+//   hess_aa += (-R (u_a v_a + rinc) - g_a u_a) e,  hess_ab += (-R u_a v_b - g_a u_b) e.
 template <int DIM, int PGH>
+__device__ __forceinline__ void dip_terms(double* acc, double e, const double* d, const double* v,
+                                          double R) {
+  double u[DIM], rinc = 0.0;
+#pragma unroll
+  for (int a = 0; a < DIM; a++) {
+    u[a] = R * d[a];
+    rinc = fma(u[a], v[a], rinc);
+  }
+  acc[0] = fma(rinc, e, acc[0]);
+  if (PGH >= 2) {
+    double g[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; a++) {
+      g[a] = fma(R, v[a], -rinc * u[a]);
+      acc[1 + a] = fma(g[a], e, acc[1 + a]);
+    }
+    if (PGH >= 3) {
+      double* h = acc + 1 + DIM;
+      auto hd = [&](int a) { return -R * (u[a] * v[a] + rinc) - g[a] * u[a]; };
+      auto ho = [&](int a, int b) { return -R * u[a] * v[b] - g[a] * u[b]; };
+      if (DIM == 2) {
+        h[0] = fma(hd(0), e, h[0]);
+        h[1] = fma(ho(0, 1), e, h[1]);
+        h[2] = fma(hd(1), e, h[2]);
+      } else {
+        h[0] = fma(hd(0), e, h[0]);
+        h[1] = fma(hd(1), e, h[1]);
+        h[2] = fma(hd(DIM - 1), e, h[2]);
+        h[3] = fma(ho(0, 1), e, h[3]);
+        h[4] = fma(ho(0, DIM - 1), e, h[4]);
+        h[5] = fma(ho(1, DIM - 1), e, h[5]);
+      }
+    }
+  }
+}
+// DIP: charges (when present) and dipoles, staged with the dipole vectors;
+// 128 sources per batch so the staging stays within static shared memory.
+template <int DIM, int PGH, bool DIP>
 __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict__ tasks, int ntask,
                                                 const SrcRange* __restrict__ ranges) {
   constexpr int NC = ncomp<DIM, PGH>();
-  constexpr int CAP = 256;  // sources staged per warp and batch
+  constexpr int CAP = DIP ? 128 : 256;  // sources staged per warp and batch
+  constexpr int ROWS = DIP ? 2 * DIM + 1 : DIM + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * 4 + warp;
-  __shared__ double ssm[4][(DIM + 1) * CAP];
+  __shared__ double ssm[4][ROWS * CAP];
   if (w >= ntask) return;  // whole warp leaves; no block-wide barrier below
   const DirTask T = tasks[w];
   const int ind = blockIdx.y;
@@ -1967,6 +2150,7 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
   double* sy = sx + CAP;
   double* sz = sy + CAP;
   double* sq = sz + (DIM == 3 ? CAP : 0);
+  double* sv = sq + CAP;  // [DIM][CAP] dipole vectors (DIP)
   // g lanes per point (g * n <= 32) split the sources of that point
   int g = 1;
   while (g * 2 * T.n <= 32) g *= 2;
@@ -1998,7 +2182,15 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
           sx[t] = k.src[DIM * j];
           sy[t] = k.src[DIM * j + 1];
           if (DIM == 3) sz[t] = k.src[DIM * j + 2];
-          sq[t] = k.chg[(size_t)j * k.nd + ind];
+          if (DIP) {
+            sq[t] = src_charge(k, j, ind);
+            double v[DIM];
+            src_dipole<DIM>(k, j, ind, v);
+#pragma unroll
+            for (int a = 0; a < DIM; a++) sv[a * CAP + t] = v[a];
+          } else {
+            sq[t] = k.chg[(size_t)j * k.nd + ind];
+          }
         }
       }
       __syncwarp();
@@ -2013,7 +2205,15 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
             rr = fma(dz, dz, rr);
           }
           if (rr < k.dmax) {
-            if (PGH == 1) {
+            if (DIP) {
+              const double e = exp(rr * ninv), d[3] = {dx, dy, dz};
+              double v[DIM];
+#pragma unroll
+              for (int a = 0; a < DIM; a++) v[a] = sv[a * CAP + t];
+              if (PGH == 1) acc[0] = fma(e, sq[t], acc[0]);
+              else pair_terms<DIM, PGH>(acc, e * sq[t], d, rfac);
+              dip_terms<DIM, PGH>(acc, e, d, v, -rfac);
+            } else if (PGH == 1) {
               acc[0] = fma(exp(rr * ninv), sq[t], acc[0]);
             } else {
               const double d[3] = {dx, dy, dz};
@@ -2211,6 +2411,10 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
 // local[j + P k (+ P^2 l)] = sum_i q h_j(x) h_k(y) (h_l(z)) with
 // h_j(x) = H_j(x) e^{-x^2} / j! (g2dformlc_vec, g2drouts.f:621-681), one
 // partial sum per CTA added into the global array.
+// Dipoles (g2dformld_vec / g3dformld_vec, g2drouts.f:685-840,
+// g3drouts.f:857-1040) add columns with the source derivative of one
+// factor, dh_j = -(j+1) dsq h_(j+1): 2D (hx, q hy + v2 dhy), (v1 dhx, hy);
+// 3D as dip3_coef with these h and dh.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const double* __restrict__ cen,
                                                  double* __restrict__ local, double* __restrict__ partial) {
@@ -2223,25 +2427,50 @@ __global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const doub
   const int ind = blockIdx.y;
   const int per = (ns + gridDim.x - 1) / gridDim.x;
   const int i0 = blockIdx.x * per, i1 = min(ns, i0 + per);
+  const int vc = k.ifdipole ? DIM : 1, chs = FORM_CH / vc;
   for (int e0 = 0; e0 < nent; e0 += 256 * 4) {
     double acc[4] = {0, 0, 0, 0};
-    for (int c0 = i0; c0 < i1; c0 += FORM_CH) {
-      const int m = min(FORM_CH, i1 - c0);
+    for (int c0 = i0; c0 < i1; c0 += chs) {
+      const int m = vc * min(chs, i1 - c0);
       __syncthreads();
       if (threadIdx.x < m) {
-        const int i = c0 + threadIdx.x;
+        const int i = c0 + threadIdx.x / vc, col = threadIdx.x % vc;
         double v[3];
         for (int d = 0; d < DIM; d++) v[d] = (k.src[DIM * i + d] - cen[d]) * k.dsq;
-        for (int d = 0; d < DIM; d++) {
-          double* h = (d == 0 ? hx : d == 1 ? hy : hz) + threadIdx.x * Pn;
-          const double f = exp(-v[d] * v[d]);
-          h[0] = f;
-          if (Pn > 1) h[1] = 2.0 * v[d] * f;
-          for (int j = 1; j < Pn - 1; j++) h[j + 1] = 2.0 * (v[d] * h[j] - h[j - 1]) / (j + 1);
+        if (!k.ifdipole) {
+          for (int d = 0; d < DIM; d++) {
+            double* h = (d == 0 ? hx : d == 1 ? hy : hz) + threadIdx.x * Pn;
+            const double f = exp(-v[d] * v[d]);
+            h[0] = f;
+            if (Pn > 1) h[1] = 2.0 * v[d] * f;
+            for (int j = 1; j < Pn - 1; j++) h[j + 1] = 2.0 * (v[d] * h[j] - h[j - 1]) / (j + 1);
+          }
+          double* hl = (DIM == 2 ? hy : hz) + threadIdx.x * Pn;
+          const double q = k.chg[(size_t)i * k.nd + ind];
+          for (int j = 0; j < Pn; j++) hl[j] *= q;
+        } else {
+          double dv[3] = {0.0, 0.0, 0.0}, a, b;
+          src_dipole<DIM>(k, i, ind, dv);
+          const double q = src_charge(k, i, ind);
+          for (int d = 0; d < DIM; d++) {
+            if (DIM == 2) {  // columns (hx, q hy + v2 dhy) and (v1 dhx, hy)
+              a = d == 0 ? (col ? 0.0 : 1.0) : (col ? 1.0 : q);
+              b = d == 0 ? (col ? dv[0] : 0.0) : (col ? 0.0 : dv[1]);
+            } else {
+              dip3_coef(col, d, q, dv, a, b);
+            }
+            // h_0 .. h_Pn by the recurrence, row_j = a h_j - b (j+1) dsq h_(j+1)
+            double* row = (d == 0 ? hx : d == 1 ? hy : hz) + threadIdx.x * Pn;
+            const double f = exp(-v[d] * v[d]);
+            double hm = f, hc = 2.0 * v[d] * f;  // h_j, h_(j+1)
+            for (int j = 0; j < Pn; j++) {
+              row[j] = fma(a, hm, -b * (j + 1.0) * k.dsq * hc);
+              const double hn = 2.0 * (v[d] * hc - hm) / (j + 2);
+              hm = hc;
+              hc = hn;
+            }
+          }
         }
-        double* hl = (DIM == 2 ? hy : hz) + threadIdx.x * Pn;
-        const double q = k.chg[(size_t)i * k.nd + ind];
-        for (int j = 0; j < Pn; j++) hl[j] *= q;
       }
       __syncthreads();
       for (int t = 0; t < m; t++) {
@@ -2575,6 +2804,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
                  al(nt * dim * 8) + al(ns * nd * out_comps(dim, P.ifpgh) * 8) +
+                 al(P.ifdipole ? ns * dim * 8 : 0) + al(P.ifdipole ? ns * nd * 8 : 0) +
                  al(nt * nd * out_comps(dim, P.ifpghtarg) * 8) +
                  al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
                  bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
@@ -2677,6 +2907,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.loc = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nloc * nd * P.nexp * 16);
   D.ssort = reinterpret_cast<double*>(cur); cur += al(ns * dim * 8);
   D.csort = reinterpret_cast<double*>(cur); cur += al(ns * nd * 8);
+  D.nsort = reinterpret_cast<double*>(cur); cur += al(P.ifdipole ? ns * dim * 8 : 0);
+  D.dsort = reinterpret_cast<double*>(cur); cur += al(P.ifdipole ? ns * nd * 8 : 0);
   D.tsort = reinterpret_cast<double*>(cur); cur += al(nt * dim * 8);
   D.psort = reinterpret_cast<double*>(cur); cur += al(ns * nd * out_comps(dim, P.ifpgh) * 8);
   D.ptsort = reinterpret_cast<double*>(cur); cur += al(nt * nd * out_comps(dim, P.ifpghtarg) * 8);
@@ -2701,6 +2933,10 @@ static KP make_kp(const DevicePlan& D) {
   k.src = D.ssort; k.chg = D.csort; k.trg = D.tsort; k.pot = D.psort; k.pottarg = D.ptsort;
   k.nc_s = out_comps(P.dim, P.ifpgh);
   k.nc_t = out_comps(P.dim, P.ifpghtarg);
+  k.ifcharge = P.ifcharge;
+  k.ifdipole = P.ifdipole;
+  k.dnrm = D.nsort;
+  k.dstr = D.dsort;
   return k;
 }
 
@@ -2742,7 +2978,7 @@ cudaError_t with_pgh(int pgh, F&& launch) {
   }
 }
 
-cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs& outs,
+cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& outs,
                                 int precision, cudaStream_t st, StageTimes* times) {
   const Params& P = D.P;
   KP k = make_kp(D);
@@ -2764,8 +3000,12 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
   mark(0);
   // charges into tree order (coordinates were sorted once, at plan set-up)
   const int gb = std::max(1, std::min(8 * D.sm_count, (std::max(P.ns, P.nt) + 255) / 256));
-  if (P.ns > 0) {
-    k_gather_pts<<<gb, 256, 0, st>>>(nullptr, chg, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
+  if (P.ns > 0 && P.ifcharge) {
+    k_gather_pts<<<gb, 256, 0, st>>>(nullptr, in.charge, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
+    launches++;
+  }
+  if (P.ns > 0 && P.ifdipole) {  // directions and strengths of the dipoles
+    k_gather_pts<<<gb, 256, 0, st>>>(in.rnormal, in.dipstr, D.nsort, D.dsort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
   if (P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * k.nc_s * 8, st));
@@ -2786,8 +3026,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
 #define FORM_MMA(NT)                                                                              \
   do {                                                                                            \
     const size_t sh = (size_t)4 * 2 * (8 * NT) * 36 * 8;                                          \
-    CK(cudaFuncSetAttribute(k_form2d_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_form2d_mma<NT><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);                     \
+    if (P.ifdipole) {                                                                             \
+      CK(cudaFuncSetAttribute(k_form2d_mma<NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      k_form2d_mma<NT, true><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);             \
+    } else {                                                                                      \
+      CK(cudaFuncSetAttribute(k_form2d_mma<NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      k_form2d_mma<NT, false><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);            \
+    }                                                                                             \
   } while (0)
           if (Pn <= 8) FORM_MMA(1);
           else if (Pn <= 16) FORM_MMA(2);
@@ -2839,8 +3084,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
         switch (mt) {
 #define FORM3_CASE(N)                                                                             \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_form3d_mma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_form3d_mma<N><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                           \
+    if (P.ifdipole) {                                                                             \
+      CK(cudaFuncSetAttribute(k_form3d_mma<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      k_form3d_mma<N, true><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                   \
+    } else {                                                                                      \
+      CK(cudaFuncSetAttribute(k_form3d_mma<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      k_form3d_mma<N, false><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                  \
+    }                                                                                             \
     break;
           FORM3_CASE(1) FORM3_CASE(2) FORM3_CASE(3) FORM3_CASE(4)
 #undef FORM3_CASE
@@ -2863,10 +3113,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
       int grid = D.scratch_ctas;
       if (Pn <= 16) {
         CK(cudaFuncSetAttribute(k_form3d_hermite<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta);
+        k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta, D.isq);
       } else {
         CK(cudaFuncSetAttribute(k_form3d_hermite<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form3d_hermite<32><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta);
+        k_form3d_hermite<32><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta, D.isq);
       }
       launches++;
     }
@@ -3051,7 +3301,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
   // (d) near field
   if (D.ndir > 0) {
     dim3 g((D.ndir + 3) / 4, nd);
-    const bool mixed = precision == PREC_MIXED;
+    // dipoles take the FP64 near field (the mixed form is charges only)
+    const bool mixed = precision == PREC_MIXED && !P.ifdipole;
     const double l2e = 1.4426950408889634;
     const double cs = std::sqrt(l2e / P.delta);
     const float amax = (float)(P.dmax * l2e / P.delta);
@@ -3060,10 +3311,12 @@ cudaError_t device_plan_execute(DevicePlan& D, const double* chg, const Outputs&
       constexpr int PG = decltype(G)::value;
       if (P.dim == 2) {
         if (mixed) k_direct_mixed<2, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
-        else k_direct<2, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+        else if (P.ifdipole) k_direct<2, PG, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+        else k_direct<2, PG, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
       } else {
         if (mixed) k_direct_mixed<3, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src, cs, amax);
-        else k_direct<3, PG><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+        else if (P.ifdipole) k_direct<3, PG, true><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
+        else k_direct<3, PG, false><<<g, 128, 0, st>>>(k, D.dir, D.ndir, D.dir_src);
       }
       return cudaSuccess;
     });
@@ -3137,13 +3390,15 @@ size_t large_delta_work_doubles(const Params& P, bool deterministic) {
   return 4 + (size_t)P.nd * nent * (deterministic ? 1 + LD_PARTS : 1);
 }
 
-cudaError_t large_delta_execute(const Params& P, const double* src, const double* chg,
+cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs& in,
                                 const double* trg, const Outputs& outs, double* work,
                                 cudaStream_t st, bool deterministic) {
   KP k;
   memset(&k, 0, sizeof(k));
   k.dim = P.dim; k.nd = P.nd; k.dsq = P.dsq; k.delta = P.delta;
-  k.src = src; k.chg = chg;
+  k.src = src; k.chg = in.charge;
+  k.ifcharge = P.ifcharge; k.ifdipole = P.ifdipole;
+  k.dnrm = in.rnormal; k.dstr = in.dipstr;  // caller order: this path sorts nothing
   int p = P.nlocal0;
   int Pn = p + 1;
   size_t nent = P.dim == 2 ? (size_t)Pn * Pn : (size_t)Pn * Pn * Pn;
@@ -3235,7 +3490,9 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
   Outputs o;
   o.pot = pot;
   o.pottarg = pottarg;
-  return large_delta_execute(P, src, chg, trg, o, work, st, false);
+  Inputs in;
+  in.charge = chg;
+  return large_delta_execute(P, src, in, trg, o, work, st, false);
 }
 
 }  // namespace fgtb

@@ -330,11 +330,13 @@ int build_host_plan_from_tree(HostPlan& H, const Params& P0, const std::vector<i
 }
 
 bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, int nt, int ifpgh,
-                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts) {
+                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts,
+                int ifcharge, int ifdipole) {
   Params& P = H.P;
   P = Params();
   P.dim = dim; P.nd = nd; P.delta = delta; P.eps = eps; P.ns = ns; P.nt = nt;
   P.ifpgh = ifpgh; P.ifpghtarg = ifpghtarg;
+  P.ifcharge = ifcharge; P.ifdipole = ifdipole;
   P.dsq = 1.0 / std::sqrt(delta);
   P.dmax = dim == 2 ? std::log(1.0 / (eps / 90)) * delta : std::log(1.0 / eps) * delta;
   P.npwlevel = npwlevel;
@@ -373,10 +375,11 @@ void plan_end(HostPlan& H) {
   P.nlevstart = nls;
   P.all_direct = P.npwlevel >= t.nlevels;
   H.nlocal.assign(t.nlevels + 1, 0);
-  int nadd = std::max(P.ifpgh, P.ifpghtarg);
+  // fgt2d.f:339-347: orders raised by the dipole and derivative orders
+  int nadd = P.ifdipole + std::max(P.ifpgh, P.ifpghtarg);
   for (int i = nls; i <= t.nlevels; i++) {
     H.nlocal[i] = hlterms(dim, t.boxsize[i], P.delta, P.eps, 0);
-    if (P.ifpgh >= 2 || P.ifpghtarg >= 2) H.nlocal[i] += nadd;
+    if (P.ifdipole == 1 || P.ifpgh >= 2 || P.ifpghtarg >= 2) H.nlocal[i] += nadd;
   }
   P.ntermmax = 0;
   for (int v : H.nlocal) P.ntermmax = std::max(P.ntermmax, v);
@@ -388,13 +391,14 @@ void plan_end(HostPlan& H) {
 
 int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
-                    int nthreads) {
+                    int nthreads, int ifcharge, int ifdipole) {
   double tstart = now();
   int npwlevel;
   double bs0, cen0[3] = {0, 0, 0};
   boxsize0(dim, delta, eps, sources, ns, targ, nt, &npwlevel, &bs0, cen0);
   TreeSetup ts;
-  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts)) {
+  if (!plan_begin(H, dim, nd, delta, eps, ns, nt, ifpgh, ifpghtarg, npwlevel, bs0, cen0, ts, ifcharge,
+                  ifdipole)) {
     H.host_tree_s = now() - tstart;
     return 0;
   }

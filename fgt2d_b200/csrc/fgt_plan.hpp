@@ -50,6 +50,7 @@ struct Params {
   int dim = 2, nd = 1;
   double delta = 0, eps = 0;
   int ns = 0, nt = 0, ifpgh = 0, ifpghtarg = 0;
+  int ifcharge = 1, ifdipole = 0;  // source kinds (fgt2d.f:23-40)
   int npwlevel = 0, nlevels = 0, nlevstart = 0, nlmax = 0;
   int npw = 0, nexp = 0, ntermmax = 0;
   double pmax = 0, dsq = 0, dmax = 0;
@@ -105,12 +106,13 @@ struct TreeSetup {
   double bs0 = 0, cen0[3] = {0, 0, 0};
 };
 bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, int nt, int ifpgh,
-                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts);
+                int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts,
+                int ifcharge = 1, int ifdipole = 0);
 void plan_end(HostPlan& H);
 
 int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
-                    int nthreads);
+                    int nthreads, int ifcharge = 1, int ifdipole = 0);
 // Fills the plan from a tree that was built outside (the fgt2dmain entry).
 int build_host_plan_from_tree(HostPlan& H, const Params& P0, const std::vector<int>& nlocal,
                               double pmax, int npw);

@@ -16,8 +16,11 @@
  * layouts: grad(nd, dim, n); hess(nd, 3, n) in 2D ordered xx, xy, yy, and
  * hess(nd, 6, n) in 3D ordered xx, yy, zz, xy, xz, yz.
  *
- * Supported now: ifcharge = 1, ifdipole = 0, ifpgh and ifpghtarg in {0..3},
- * any nd >= 1.  Other flag values return FGT_ERR_UNSUPPORTED.
+ * Sources are charges (ifcharge = 1) and/or dipoles (ifdipole = 1: directions
+ * rnormal(dim, ns), strengths dipstr(nd, ns), field dipstr n . grad_s of the
+ * Gaussian, g2d_directdp_vec).  Supported: ifcharge, ifdipole in {0, 1},
+ * ifpgh and ifpghtarg in {0..3}, any nd >= 1.  Other flag values return
+ * FGT_ERR_UNSUPPORTED.
  *
  * All entry points return a status (FGT_OK or an error code below) except
  * fgt2d_ / fgt3d_, which keep the reference's subroutine signature and
@@ -33,7 +36,7 @@ extern "C" {
 enum {
   FGT_OK = 0,
   FGT_ERR_BADARG = 1,      /* nd < 1, delta <= 0, eps not in (0,1), n < 0, NaN */
-  FGT_ERR_UNSUPPORTED = 2, /* dipoles, flags above 3, orders too large */
+  FGT_ERR_UNSUPPORTED = 2, /* flags out of range, orders too large */
   FGT_ERR_NOMEM = 3,       /* device or host allocation failed */
   FGT_ERR_CUDA = 4,        /* CUDA runtime error (see fgt_last_cuda_error) */
   FGT_ERR_NODEVICE = 5,    /* no CUDA device */
@@ -166,6 +169,11 @@ int fgt3dmain_gpu_(const int* nd, const double* delta, const double* eps, const 
 int fgt_plan_create(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                     fgt_plan** out);
+/* The same for charges and/or dipoles (the orders grow by ifdipole as in
+ * fgt2d.f:339-347); execute such plans with the _full calls below. */
+int fgt_plan_create_cd(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                       const double* sources, int nt, const double* targ, int ifcharge,
+                       int ifdipole, int ifpgh, int ifpghtarg, fgt_plan** out);
 /* host arrays in and out; copies the charges in and the outputs back */
 int fgt_plan_execute_host(fgt_plan* plan, const double* sources, const double* charge,
                           const double* targ, double* pot, double* pottarg);
@@ -183,6 +191,15 @@ int fgt_plan_execute_host_pgh(fgt_plan* plan, const double* charge, double* pot,
 int fgt_plan_execute_device_pgh(fgt_plan* plan, const double* d_charge, double* d_pot,
                                 double* d_grad, double* d_hess, double* d_pottarg,
                                 double* d_gradtarg, double* d_hesstarg, void* stream);
+/* Every input and output: charge (nd, ns) for plans with charges, rnormal
+ * (dim, ns) and dipstr (nd, ns) for plans with dipoles (NULL otherwise). */
+int fgt_plan_execute_host_full(fgt_plan* plan, const double* charge, const double* rnormal,
+                               const double* dipstr, double* pot, double* grad, double* hess,
+                               double* pottarg, double* gradtarg, double* hesstarg);
+int fgt_plan_execute_device_full(fgt_plan* plan, const double* d_charge, const double* d_rnormal,
+                                 const double* d_dipstr, double* d_pot, double* d_grad,
+                                 double* d_hess, double* d_pottarg, double* d_gradtarg,
+                                 double* d_hesstarg, void* stream);
 /* per-stage device milliseconds of one synchronous execute on device data:
  * gather, form, merge, mp->loc, split, eval, direct, scatter */
 int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
@@ -247,6 +264,9 @@ typedef struct fgt_request {
   double* hess;          /* (ns, H, nd) when ifpgh = 3 */
   double* gradtarg;      /* (nt, dim, nd) when ifpghtarg >= 2 */
   double* hesstarg;      /* (nt, H, nd) when ifpghtarg = 3 */
+  int ifdipole;          /* 1: dipoles rnormal (ns, dim), dipstr (ns, nd); charge NULL: none */
+  const double* rnormal;
+  const double* dipstr;
 } fgt_request;
 typedef struct fgt_server_stats {
   long long submitted, completed, failed;

@@ -15,9 +15,9 @@
 //
 // Conventions: arrays that mirror Fortran arrays keep 1-based box ids and
 // column-major layouts so that each loop can be read beside the Fortran line
-// it follows.  Only charge sources with potential outputs (ifcharge=1,
-// ifdipole=0, ifpgh/ifpghtarg in {0,1}) are restated; other flag values
-// return ORC_UNSUPPORTED.
+// it follows.  Charges and/or dipoles (ifcharge, ifdipole in {0,1}) with
+// potentials, gradients and Hessians (ifpgh, ifpghtarg in {0..3}) are
+// restated; other flag values return ORC_UNSUPPORTED.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -664,6 +664,34 @@ void g2dformhc(int nd, double delta, const double* src, int ns, const double* ch
     }
   }
 }
+// Dipole terms of g2dformhd_vec / g2dformhcd_vec (g2drouts.f:173-338), added
+// to ff: with hx_j = x^j/sqrt(j!) and dxhx_j = j dsq hx_{j-1}/sqrt(j) (the
+// derivative in the source coordinate),
+//   ff(j,k) += dipstr (n1 dxhx_j hy_k + n2 hx_j dyhy_k).
+void g2dformhd_add(int nd, double delta, const double* src, int ns, const double* rn,
+                   const double* ds, const double* cent, int p, double* ff) {
+  int P = p + 1;
+  std::vector<double> hx(P), hy(P), dxhx(P), dyhy(P);
+  double dsq = 1.0 / std::sqrt(delta);
+  for (int i = 0; i < ns; i++) {
+    double x = (src[2 * i] - cent[0]) * dsq, y = (src[2 * i + 1] - cent[1]) * dsq;
+    hx[0] = 1.0; hy[0] = 1.0; dxhx[0] = 0.0; dyhy[0] = 0.0;
+    for (int j1 = 1; j1 <= p; j1++) {
+      double tmp = std::sqrt((double)j1);
+      hy[j1] = hy[j1 - 1] * y / tmp;
+      hx[j1] = hx[j1 - 1] * x / tmp;
+      dxhx[j1] = j1 * dsq * hx[j1 - 1] / tmp;
+      dyhy[j1] = j1 * dsq * hy[j1 - 1] / tmp;
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      for (int k = 0; k <= p; k++) {
+        double d1 = hy[k] * rn[2 * i] * ds[nd * i + ind];
+        double d2 = dyhy[k] * rn[2 * i + 1] * ds[nd * i + ind];
+        for (int j = 0; j <= p; j++) ff[(size_t)ind * P * P + j + P * k] += dxhx[j] * d1 + hx[j] * d2;
+      }
+    }
+  }
+}
 // g2dh2pw_real_vec, g2drouts.f:1242-1329.  h2x(npw,0:p), pw(npw/2,npw,nd) +=
 void g2dh2pw(int nd, int p, int npw, const double* h2x, const double* hexp, cplx* pw) {
   int P = p + 1, n2 = npw / 2;
@@ -849,6 +877,34 @@ void g2dformlc(int nd, double delta, const double* src, int ns, const double* ch
     }
   }
 }
+// Dipole terms of g2dformld_vec / g2dformlcd_vec (g2drouts.f:685-840): the
+// Hermite functions h_j = H_j(x) e^{-x^2}/j! and dh_j = -(j+1) dsq h_{j+1}.
+void g2dformld_add(int nd, double delta, const double* src, int ns, const double* rn,
+                   const double* ds, const double* cent, int p, double* local) {
+  int P = p + 1;
+  double dsq = 1.0 / std::sqrt(delta);
+  std::vector<double> hx(P + 1), hy(P + 1), dhx(P), dhy(P);
+  for (int i = 0; i < ns; i++) {
+    double x = (src[2 * i] - cent[0]) * dsq, y = (src[2 * i + 1] - cent[1]) * dsq;
+    double fx = std::exp(-x * x), fy = std::exp(-y * y);
+    hx[0] = fx; hy[0] = fy; hx[1] = 2.0 * x * fx; hy[1] = 2.0 * y * fy;
+    for (int j = 1; j <= p; j++) {
+      hx[j + 1] = 2.0 * (x * hx[j] - hx[j - 1]) / (j + 1);
+      hy[j + 1] = 2.0 * (y * hy[j] - hy[j - 1]) / (j + 1);
+    }
+    for (int j = 0; j <= p; j++) {
+      dhx[j] = -hx[j + 1] * dsq * (j + 1.0);
+      dhy[j] = -hy[j + 1] * dsq * (j + 1.0);
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      double r1 = rn[2 * i] * ds[nd * i + ind], r2 = rn[2 * i + 1] * ds[nd * i + ind];
+      for (int j1 = 0; j1 <= p; j1++) {
+        double ry1 = hy[j1] * r1, ry2 = dhy[j1] * r2;
+        for (int j2 = 0; j2 <= p; j2++) local[(size_t)ind * P * P + j2 + P * j1] += dhx[j2] * ry1 + hx[j2] * ry2;
+      }
+    }
+  }
+}
 
 // ---------------------------------------------------------------- 3D expansions
 // g3dformhc_vec, g3drouts.f:109-192.  ffexp(0:p,0:p,0:p,nd)
@@ -950,6 +1006,83 @@ void g3dformpwc(int nd, double delta, const double* src, int ns, const double* c
         for (int j2 = 1; j2 <= npw; j2++) {
           cplx yt = zt * w2[j2];
           for (int j1 = 1; j1 <= npw; j1++) out[(j1 - 1) + npw * ((j2 - 1) + (size_t)npw * (j3 - 1))] += yt * w1[j1];
+        }
+      }
+    }
+  }
+}
+// Dipole terms of g3dformhd_vec / g3dformhcd_vec (g3drouts.f:197-405)
+void g3dformhd_add(int nd, double delta, const double* src, int ns, const double* rn,
+                   const double* ds, const double* cent, int p, double* ff) {
+  int P = p + 1;
+  size_t PP = (size_t)P * P * P;
+  std::vector<double> hx(P), hy(P), hz(P), dxhx(P), dyhy(P), dzhz(P), sqk(P);
+  double dsq = 1.0 / std::sqrt(delta);
+  for (int k = 1; k <= p; k++) sqk[k] = std::sqrt((double)k);
+  for (int i = 0; i < ns; i++) {
+    double x = (src[3 * i] - cent[0]) * dsq, y = (src[3 * i + 1] - cent[1]) * dsq,
+           z = (src[3 * i + 2] - cent[2]) * dsq;
+    hx[0] = hy[0] = hz[0] = 1.0;
+    dxhx[0] = dyhy[0] = dzhz[0] = 0.0;
+    for (int j1 = 1; j1 <= p; j1++) {
+      hy[j1] = hy[j1 - 1] * y / sqk[j1];
+      hx[j1] = hx[j1 - 1] * x / sqk[j1];
+      hz[j1] = hz[j1 - 1] * z / sqk[j1];
+      dxhx[j1] = j1 * dsq * hx[j1 - 1] / sqk[j1];
+      dyhy[j1] = j1 * dsq * hy[j1 - 1] / sqk[j1];
+      dzhz[j1] = j1 * dsq * hz[j1 - 1] / sqk[j1];
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      double r1 = rn[3 * i] * ds[nd * i + ind], r2 = rn[3 * i + 1] * ds[nd * i + ind],
+             r3 = rn[3 * i + 2] * ds[nd * i + ind];
+      double* F = ff + PP * ind;
+      for (int l = 0; l <= p; l++) {
+        double d1 = hz[l] * r1, d2 = hz[l] * r2, d3 = dzhz[l] * r3;
+        for (int k = 0; k <= p; k++) {
+          double c1 = hy[k] * d1, c2 = dyhy[k] * d2 + hy[k] * d3;
+          for (int j = 0; j <= p; j++) F[j + P * (k + (size_t)P * l)] += dxhx[j] * c1 + hx[j] * c2;
+        }
+      }
+    }
+  }
+}
+// Dipole terms of g3dformpwd_vec / g3dformpwcd_vec (g3drouts.f:2042-2262):
+// the node factors times -i t dsq (the source-coordinate derivative).
+void g3dformpwd_add(int nd, double delta, const double* src, int ns, const double* rn,
+                    const double* ds, const double* cent, int npw, const double* ws,
+                    const double* ts, cplx* pw) {
+  cplx eye(0, 1);
+  double dsq = 1.0 / std::sqrt(delta);
+  int n2 = npw / 2;
+  std::vector<cplx> w1(npw + 1), w2(npw + 1), w3(npw + 1), w1x(npw + 1), w2y(npw + 1), w3z(npw + 1);
+  for (int i = 0; i < ns; i++) {
+    double x = (src[3 * i] - cent[0]) * dsq, y = (src[3 * i + 1] - cent[1]) * dsq,
+           z = (src[3 * i + 2] - cent[2]) * dsq;
+    cplx qx = std::exp(-eye * ts[n2 + 1] * x), qy = std::exp(-eye * ts[n2 + 1] * y),
+         qz = std::exp(-eye * ts[n2 + 1] * z);
+    cplx q1 = qx, q2 = qy, q3 = qz;
+    qx = qx * qx; qy = qy * qy; qz = qz * qz;
+    for (int j1 = n2 + 1; j1 <= npw; j1++) {
+      w1[j1] = q1 * ws[j1]; w2[j1] = q2 * ws[j1]; w3[j1] = q3 * ws[j1];
+      q1 = q1 * qx; q2 = q2 * qy; q3 = q3 * qz;
+      w1[npw - j1 + 1] = std::conj(w1[j1]);
+      w2[npw - j1 + 1] = std::conj(w2[j1]);
+      w3[npw - j1 + 1] = std::conj(w3[j1]);
+    }
+    for (int j1 = 1; j1 <= npw; j1++) {
+      cplx zt = -eye * ts[j1] * dsq;
+      w1x[j1] = w1[j1] * zt; w2y[j1] = w2[j1] * zt; w3z[j1] = w3[j1] * zt;
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      double r1 = rn[3 * i] * ds[nd * i + ind], r2 = rn[3 * i + 1] * ds[nd * i + ind],
+             r3 = rn[3 * i + 2] * ds[nd * i + ind];
+      cplx* out = pw + (size_t)ind * npw * npw * n2;
+      for (int j3 = 1; j3 <= n2; j3++) {
+        cplx rz1 = w3[j3] * r1, rz2 = w3[j3] * r2, rz3 = w3z[j3] * r3;
+        for (int j2 = 1; j2 <= npw; j2++) {
+          cplx ry1 = rz1 * w2[j2], ry2 = rz2 * w2y[j2] + rz3 * w2[j2];
+          for (int j1 = 1; j1 <= npw; j1++)
+            out[(j1 - 1) + npw * ((j2 - 1) + (size_t)npw * (j3 - 1))] += w1x[j1] * ry1 + w1[j1] * ry2;
         }
       }
     }
@@ -1162,6 +1295,35 @@ void g3dformlc(int nd, double delta, const double* src, int ns, const double* ch
     }
   }
 }
+// Dipole terms of g3dformld_vec / g3dformlcd_vec (g3drouts.f:857-1040)
+void g3dformld_add(int nd, double delta, const double* src, int ns, const double* rn,
+                   const double* ds, const double* cent, int p, double* local) {
+  int P = p + 1;
+  double dsq = 1.0 / std::sqrt(delta);
+  std::vector<double> h[3], dh[3];
+  for (int d = 0; d < 3; d++) { h[d].resize(P + 1); dh[d].resize(P); }
+  for (int i = 0; i < ns; i++) {
+    for (int d = 0; d < 3; d++) {
+      double v = (src[3 * i + d] - cent[d]) * dsq, f = std::exp(-v * v);
+      h[d][0] = f;
+      h[d][1] = 2.0 * v * f;
+      for (int j = 1; j <= p; j++) h[d][j + 1] = 2.0 * (v * h[d][j] - h[d][j - 1]) / (j + 1);
+      for (int j = 0; j <= p; j++) dh[d][j] = -h[d][j + 1] * dsq * (j + 1.0);
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      double r1 = rn[3 * i] * ds[nd * i + ind], r2 = rn[3 * i + 1] * ds[nd * i + ind],
+             r3 = rn[3 * i + 2] * ds[nd * i + ind];
+      double* Lo = local + (size_t)ind * P * P * P;
+      for (int j1 = 0; j1 <= p; j1++) {
+        double z1 = h[2][j1] * r1, z2 = h[2][j1] * r2, z3 = dh[2][j1] * r3;
+        for (int j2 = 0; j2 <= p; j2++) {
+          double c1 = h[1][j2] * z1, c2 = dh[1][j2] * z2 + h[1][j2] * z3;
+          for (int j3 = 0; j3 <= p; j3++) Lo[j3 + P * (j2 + (size_t)P * j1)] += dh[0][j3] * c1 + h[0][j3] * c2;
+        }
+      }
+    }
+  }
+}
 
 // g2d_directcp/cg/ch_vec (g2ddirect.f:32-212) / g3d_directcp/cg/ch_vec
 // (g3ddirect.f:3-203): pot (pgh = 1), + grad (2), + Hessian (3) with
@@ -1210,6 +1372,62 @@ void directc(int nd, double delta, double dmax, const double* src, int ns, const
     }
 }
 
+// Dipole terms of g2d_directd{p,g,h}_vec / g2d_directcd{p,g,h}_vec
+// (g2ddirect.f:217-658) and g3d_directd*/cd*_vec (g3ddirect.f:207-708):
+// with R = 2/delta, u = R (t - s), rinc = u.n,
+//   pot  += rinc e dipstr,  grad_a += (R n_a - rinc u_a) e dipstr,
+//   hess_aa += (-R (u_a n_a + rinc) - g_a u_a) e dipstr,
+//   hess_ab += (-R u_a n_b - g_a u_b) e dipstr   (g_a the grad factor).
+template <int D>
+void directd(int nd, double delta, double dmax, const double* src, int ns, const double* rn,
+             const double* ds, const double* trg, int nt, int pgh, double* pot, double* grad,
+             double* hess) {
+  const int NH = D == 2 ? 3 : 6;
+  const double R = 2.0 / delta;
+  for (int it = 0; it < nt; it++)
+    for (int i = 0; i < ns; i++) {
+      double rr = 0, df[3] = {0, 0, 0};
+      for (int d = 0; d < D; d++) {
+        df[d] = trg[D * it + d] - src[D * i + d];
+        rr += df[d] * df[d];
+      }
+      if (!(rr < dmax)) continue;
+      double e = std::exp(-rr / delta), u[3], n[3], g[3], h[6];
+      double rinc = 0;
+      for (int d = 0; d < D; d++) {
+        u[d] = R * df[d];
+        n[d] = rn[D * i + d];
+        rinc += u[d] * n[d];
+      }
+      for (int d = 0; d < D; d++) g[d] = n[d] * R - rinc * u[d];
+      auto hd = [&](int a) { return -R * (u[a] * n[a] + rinc) - g[a] * u[a]; };
+      auto ho = [&](int a, int b) { return -R * u[a] * n[b] - g[a] * u[b]; };
+      if (D == 2) {
+        h[0] = hd(0); h[1] = ho(0, 1); h[2] = hd(1);
+      } else {
+        h[0] = hd(0); h[1] = hd(1); h[2] = hd(2); h[3] = ho(0, 1); h[4] = ho(0, 2); h[5] = ho(1, 2);
+      }
+      for (int ii = 0; ii < nd; ii++) {
+        double v = e * ds[nd * i + ii];
+        double w = rinc * v;
+#pragma omp atomic
+        pot[nd * it + ii] += w;
+        if (pgh >= 2)
+          for (int d = 0; d < D; d++) {
+            double gv = g[d] * v;
+#pragma omp atomic
+            grad[ii + nd * (d + D * (size_t)it)] += gv;
+          }
+        if (pgh >= 3)
+          for (int c = 0; c < NH; c++) {
+            double hv = h[c] * v;
+#pragma omp atomic
+            hess[ii + nd * (c + NH * (size_t)it)] += hv;
+          }
+      }
+    }
+}
+
 // ---------------------------------------------------------------- drivers
 struct Result {
   int npwlevel = 0, nlevels = 0, nboxes = 0, npw = 0, nlmax = 0;
@@ -1221,13 +1439,14 @@ struct Result {
 // (fgt3d.f:19-477, 483-1527).  Output arrays are overwritten.
 template <int D>
 int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int ifcharge,
-            const double* charge, int ifdipole, int ifpgh, double* pot, double* grad, double* hess,
+            const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
+            int ifpgh, double* pot, double* grad, double* hess,
             int nt, const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
             double* hesstarg, Result* res) {
   const int NCH = Tree<D>::NCH;
   const int NH = D == 2 ? 3 : 6;
   if (nd < 1 || !(delta > 0) || !(eps > 0) || ns < 0 || nt < 0) return ORC_BADARG;
-  if (ifcharge != 1 || ifdipole != 0) return ORC_UNSUPPORTED;
+  if (ifcharge < 0 || ifcharge > 1 || ifdipole < 0 || ifdipole > 1) return ORC_UNSUPPORTED;
   if (ifpgh < 0 || ifpgh > 3 || ifpghtarg < 0 || ifpghtarg > 3) return ORC_UNSUPPORTED;
   // fgt2d.f:238-322: outputs zeroed per flag
   if (ifpgh >= 1) std::fill(pot, pot + (size_t)nd * ns, 0.0);
@@ -1250,11 +1469,13 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
     size_t LL = (size_t)nd * (D == 2 ? P * P : P * P * P);
     std::vector<double> local(LL, 0.0);
     if (D == 2) {
-      g2dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
+      if (ifcharge) g2dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
+      if (ifdipole) g2dformld_add(nd, delta, sources, ns, rnormal, dipstr, cen0, nl0, local.data());
       if (ifpghtarg >= 1) g2dleval(nd, delta, cen0, nl0, local.data(), targ, nt, ifpghtarg, pottarg, gradtarg, hesstarg);
       if (ifpgh >= 1) g2dleval(nd, delta, cen0, nl0, local.data(), sources, ns, ifpgh, pot, grad, hess);
     } else {
-      g3dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
+      if (ifcharge) g3dformlc(nd, delta, sources, ns, charge, cen0, nl0, local.data());
+      if (ifdipole) g3dformld_add(nd, delta, sources, ns, rnormal, dipstr, cen0, nl0, local.data());
       if (ifpghtarg >= 1) g3dleval(nd, delta, cen0, nl0, local.data(), targ, nt, ifpghtarg, pottarg, gradtarg, hesstarg);
       if (ifpgh >= 1) g3dleval(nd, delta, cen0, nl0, local.data(), sources, ns, ifpgh, pot, grad, hess);
     }
@@ -1298,9 +1519,16 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
 
   // dreorderf
   std::vector<double> ssort((size_t)D * ns), csort((size_t)nd * ns), tsort((size_t)D * nt);
+  std::vector<double> rsort(ifdipole ? (size_t)D * ns : 0), dsort(ifdipole ? (size_t)nd * ns : 0);
   for (int i = 0; i < ns; i++) {
-    for (int d = 0; d < D; d++) ssort[(size_t)D * i + d] = sources[(size_t)D * (isrc[i + 1] - 1) + d];
-    for (int k = 0; k < nd; k++) csort[(size_t)nd * i + k] = charge[(size_t)nd * (isrc[i + 1] - 1) + k];
+    const size_t o = isrc[i + 1] - 1;
+    for (int d = 0; d < D; d++) ssort[(size_t)D * i + d] = sources[(size_t)D * o + d];
+    if (ifcharge)
+      for (int k = 0; k < nd; k++) csort[(size_t)nd * i + k] = charge[(size_t)nd * o + k];
+    if (ifdipole) {
+      for (int d = 0; d < D; d++) rsort[(size_t)D * i + d] = rnormal[(size_t)D * o + d];
+      for (int k = 0; k < nd; k++) dsort[(size_t)nd * i + k] = dipstr[(size_t)nd * o + k];
+    }
   }
   for (int i = 0; i < nt; i++)
     for (int d = 0; d < D; d++) tsort[(size_t)D * i + d] = targ[(size_t)D * (itarg[i + 1] - 1) + d];
@@ -1449,17 +1677,23 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         if (t.nchild[ibox] != 0 || npts <= 0) continue;
         const double* s = ssort.data() + (size_t)D * S0(ibox);
         const double* q = csort.data() + (size_t)nd * S0(ibox);
+        const double* rn = rsort.data() + (size_t)D * S0(ibox);
+        const double* dp = dsort.data() + (size_t)nd * S0(ibox);
         const double* c = &t.centers[(size_t)D * ibox];
+        // g2dformhc/hd/hcd_vec by ifcharge/ifdipole (fgt2d.f:882-954)
         if (D == 2) {
-          std::vector<double> hexp((size_t)P * P * nd);
-          g2dformhc(nd, delta, s, npts, q, c, p, hexp.data());
+          std::vector<double> hexp((size_t)P * P * nd, 0.0);
+          if (ifcharge) g2dformhc(nd, delta, s, npts, q, c, p, hexp.data());
+          if (ifdipole) g2dformhd_add(nd, delta, s, npts, rn, dp, c, p, hexp.data());
           g2dh2pw(nd, p, npw, rh2x.data(), hexp.data(), MP(ibox));
         } else if (npts > nptsswitch) {
-          std::vector<double> hexp((size_t)P * P * P * nd);
-          g3dformhc(nd, delta, s, npts, q, c, p, hexp.data());
+          std::vector<double> hexp((size_t)P * P * P * nd, 0.0);
+          if (ifcharge) g3dformhc(nd, delta, s, npts, q, c, p, hexp.data());
+          if (ifdipole) g3dformhd_add(nd, delta, s, npts, rn, dp, c, p, hexp.data());
           g3dh2pw(nd, p, npw, rh2xt.data(), hexp.data(), MP(ibox));
         } else {
-          g3dformpwc(nd, delta, s, npts, q, c, npw, ws.data(), ts.data(), MP(ibox));
+          if (ifcharge) g3dformpwc(nd, delta, s, npts, q, c, npw, ws.data(), ts.data(), MP(ibox));
+          if (ifdipole) g3dformpwd_add(nd, delta, s, npts, rn, dp, c, npw, ws.data(), ts.data(), MP(ibox));
         }
       }
     }
@@ -1586,13 +1820,22 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         nhung++;
         const double* s = ssort.data() + (size_t)D * S0(jbox);
         const double* q = csort.data() + (size_t)nd * S0(jbox);
+        const double* rn = rsort.data() + (size_t)D * S0(jbox);
+        const double* dp = dsort.data() + (size_t)nd * S0(jbox);
         int nsj = NS(jbox);
+        // fgt2dpart_direct_vec: charge and dipole terms (fgt2d.f:1354-1512)
         for (int ibox : list1[jbox]) {
           const int i0 = T0(ibox), j0 = S0(ibox);
-          if (NT(ibox) > 0 && ifpghtarg >= 1)
-            directc<D>(nd, delta, dmax, s, nsj, q, tsort.data() + (size_t)D * i0, NT(ibox), ifpghtarg, PT(i0), GT(i0), HT(i0));
-          if (NS(ibox) > 0 && ifpgh >= 1)
-            directc<D>(nd, delta, dmax, s, nsj, q, ssort.data() + (size_t)D * j0, NS(ibox), ifpgh, PS(j0), GS(j0), HS(j0));
+          if (NT(ibox) > 0 && ifpghtarg >= 1) {
+            const double* tp = tsort.data() + (size_t)D * i0;
+            if (ifcharge) directc<D>(nd, delta, dmax, s, nsj, q, tp, NT(ibox), ifpghtarg, PT(i0), GT(i0), HT(i0));
+            if (ifdipole) directd<D>(nd, delta, dmax, s, nsj, rn, dp, tp, NT(ibox), ifpghtarg, PT(i0), GT(i0), HT(i0));
+          }
+          if (NS(ibox) > 0 && ifpgh >= 1) {
+            const double* sp = ssort.data() + (size_t)D * j0;
+            if (ifcharge) directc<D>(nd, delta, dmax, s, nsj, q, sp, NS(ibox), ifpgh, PS(j0), GS(j0), HS(j0));
+            if (ifdipole) directd<D>(nd, delta, dmax, s, nsj, rn, dp, sp, NS(ibox), ifpgh, PS(j0), GS(j0), HS(j0));
+          }
         }
       }
     }
@@ -1680,6 +1923,11 @@ int orc_fgt_pgh(int dim, int nd, double delta, double eps, int ns, const double*
                 int ifcharge, const double* charge, int ifdipole, int ifpgh, double* pot,
                 double* grad, double* hess, int nt, const double* targ, int ifpghtarg,
                 double* pottarg, double* gradtarg, double* hesstarg, int* info, int nthreads);
+int orc_fgt_full(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                 int ifcharge, const double* charge, int ifdipole, const double* rnormal,
+                 const double* dipstr, int ifpgh, double* pot, double* grad, double* hess, int nt,
+                 const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                 double* hesstarg, int* info, int nthreads);
 int orc_fgt(int dim, int nd, double delta, double eps, int ns, const double* sources,
             int ifcharge, const double* charge, int ifdipole, int ifpgh, double* pot, int nt,
             const double* targ, int ifpghtarg, double* pottarg, int* info, int nthreads) {
@@ -1697,9 +1945,24 @@ int orc_fgt_pgh(int dim, int nd, double delta, double eps, int ns, const double*
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
+  if (ifdipole) return ORC_UNSUPPORTED;  // no dipole arrays here
+  return orc_fgt_full(dim, nd, delta, eps, ns, sources, ifcharge, charge, 0, nullptr, nullptr, ifpgh,
+                      pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, info, nthreads);
+}
+
+// The reference's full argument list (fgt2d.f:19-22, less iper): charges
+// and/or dipoles with rnormal(dim, ns), dipstr(nd, ns).
+int orc_fgt_full(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                 int ifcharge, const double* charge, int ifdipole, const double* rnormal,
+                 const double* dipstr, int ifpgh, double* pot, double* grad, double* hess, int nt,
+                 const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                 double* hesstarg, int* info, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
   Result r;
-  int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r)
-                    : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r);
+  int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r)
+                    : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r);
   if (info) {
     info[0] = r.npwlevel; info[1] = r.nlevels; info[2] = r.nboxes; info[3] = r.npw;
     info[4] = r.nlmax; info[5] = (int)r.nleaf_direct; info[6] = 0; info[7] = 0;
@@ -1770,6 +2033,36 @@ void orc_direct_pgh(int dim, int nd, double delta, int ns, const double* src, co
         for (int d = 0; d < dim; d++) grad[k + nd * (d + (size_t)dim * it)] = a[1 + d];
       if (pgh >= 3)
         for (int c = 0; c < NH; c++) hess[k + nd * (c + (size_t)NH * it)] = a[1 + dim + c];
+    }
+  }
+}
+
+// Exact sums (no cutoff) with charges and/or dipoles, pot/grad/hess by pgh:
+// the per-pair terms of g2d_directc*/d*_vec and the 3D twins.
+void orc_direct_full(int dim, int nd, double delta, int ns, const double* src, int ifcharge,
+                     const double* chg, int ifdipole, const double* rn, const double* ds, int nt,
+                     const double* trg, int pgh, double* pot, double* grad, double* hess,
+                     int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const int NH = dim == 2 ? 3 : 6;
+  const double inf = HUGE_VAL;
+  std::fill(pot, pot + (size_t)nd * nt, 0.0);
+  if (pgh >= 2) std::fill(grad, grad + (size_t)nd * dim * nt, 0.0);
+  if (pgh >= 3) std::fill(hess, hess + (size_t)nd * NH * nt, 0.0);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int it = 0; it < nt; it++) {
+    double* p = pot + (size_t)nd * it;
+    double* g = pgh >= 2 ? grad + (size_t)nd * dim * it : nullptr;
+    double* h = pgh >= 3 ? hess + (size_t)nd * NH * it : nullptr;
+    const double* t = trg + (size_t)dim * it;
+    if (dim == 2) {
+      if (ifcharge) directc<2>(nd, delta, inf, src, ns, chg, t, 1, pgh, p, g, h);
+      if (ifdipole) directd<2>(nd, delta, inf, src, ns, rn, ds, t, 1, pgh, p, g, h);
+    } else {
+      if (ifcharge) directc<3>(nd, delta, inf, src, ns, chg, t, 1, pgh, p, g, h);
+      if (ifdipole) directd<3>(nd, delta, inf, src, ns, rn, ds, t, 1, pgh, p, g, h);
     }
   }
 }

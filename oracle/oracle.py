@@ -51,6 +51,15 @@ def lib():
                                   ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                                   _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
                                   _ip, ctypes.c_int]
+        L.orc_fgt_full.restype = ctypes.c_int
+        L.orc_fgt_full.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
+                                   ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int,
+                                   _dp, _dp, _dp, _ip, ctypes.c_int]
+        L.orc_direct_full.restype = None
+        L.orc_direct_full.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                      _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
+                                      ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
         L.orc_direct_pgh.restype = None
         L.orc_direct_pgh.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                      _dp, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp,
@@ -144,6 +153,54 @@ def fgt_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=
             "gradtarg": gt[:nt] if ifpghtarg >= 2 else None,
             "hesstarg": ht[:nt] if ifpghtarg >= 3 else None,
             "info": {k: int(info[i]) for i, k in enumerate(keys)}}
+
+
+def fgt_full(dim, nd, delta, eps, sources, charge=None, targ=None, ifpgh=1, ifpghtarg=0,
+             rnormal=None, dipstr=None, nthreads=0):
+    """The restated transform with charges and/or dipoles (``charge`` or
+    ``dipstr`` None switches that source kind off): rnormal (ns, dim),
+    dipstr (ns, nd).  Returns the dict of fgt_pgh."""
+    src = _f64(sources)
+    ns = src.shape[0]
+    ifc, ifd = int(charge is not None), int(dipstr is not None)
+    q = _f64(charge).reshape(ns, nd) if ifc else np.zeros((1, nd))
+    rn = _f64(rnormal).reshape(ns, dim) if ifd else np.zeros((1, dim))
+    ds = _f64(dipstr).reshape(ns, nd) if ifd else np.zeros((1, nd))
+    trg = _f64(targ) if targ is not None else np.zeros((0, dim))
+    nt = trg.shape[0]
+    H = nhess(dim)
+    pot, grad, hess = np.zeros((max(ns, 1), nd)), np.zeros((max(ns, 1), dim, nd)), np.zeros((max(ns, 1), H, nd))
+    pt, gt, ht = np.zeros((max(nt, 1), nd)), np.zeros((max(nt, 1), dim, nd)), np.zeros((max(nt, 1), H, nd))
+    info = np.zeros(8, dtype=np.int32)
+    rc = lib().orc_fgt_full(dim, nd, float(delta), float(eps), ns, _d(src), ifc, _d(q), ifd, _d(rn),
+                            _d(ds), ifpgh, _d(pot), _d(grad), _d(hess), nt, _d(trg), ifpghtarg,
+                            _d(pt), _d(gt), _d(ht), info.ctypes.data_as(_ip), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle fgt returned status {rc}")
+    keys = ["npwlevel", "nlevels", "nboxes", "npw", "nlmax", "ndirect_leaves"]
+    return {"pot": pot[:ns] if ifpgh >= 1 else None, "grad": grad[:ns] if ifpgh >= 2 else None,
+            "hess": hess[:ns] if ifpgh >= 3 else None,
+            "pottarg": pt[:nt] if ifpghtarg >= 1 else None,
+            "gradtarg": gt[:nt] if ifpghtarg >= 2 else None,
+            "hesstarg": ht[:nt] if ifpghtarg >= 3 else None,
+            "info": {k: int(info[i]) for i, k in enumerate(keys)}}
+
+
+def direct_full(dim, nd, delta, sources, targ, charge=None, rnormal=None, dipstr=None, pgh=3,
+                nthreads=0):
+    """Exact sums with charges and/or dipoles: (pot, grad, hess) at targ."""
+    src = _f64(sources)
+    ns = src.shape[0]
+    trg = _f64(targ)
+    nt = trg.shape[0]
+    ifc, ifd = int(charge is not None), int(dipstr is not None)
+    q = _f64(charge).reshape(ns, nd) if ifc else np.zeros((1, nd))
+    rn = _f64(rnormal).reshape(ns, dim) if ifd else np.zeros((1, dim))
+    ds = _f64(dipstr).reshape(ns, nd) if ifd else np.zeros((1, nd))
+    pot, grad, hess = np.zeros((nt, nd)), np.zeros((nt, dim, nd)), np.zeros((nt, nhess(dim), nd))
+    lib().orc_direct_full(dim, nd, float(delta), ns, _d(src), ifc, _d(q), ifd, _d(rn), _d(ds), nt,
+                          _d(trg), pgh, _d(pot), _d(grad), _d(hess), nthreads)
+    return pot, grad, hess
 
 
 def direct_pgh(dim, nd, delta, sources, charge, targ, pgh=3, nthreads=0):

@@ -98,3 +98,28 @@ def test_gradient_requests_mixed_in(fgt):
                 assert np.array_equal(v, got[k]), k
     assert srv.stats()["failed"] == 0
     srv.close()
+
+
+def test_dipole_requests(fgt):
+    """Dipole requests (with and without charges) through the server equal
+    the same transforms run alone, bitwise."""
+    rng = np.random.default_rng(29)
+    ctx = fgt.Context(0, precision="auto")
+    srv = fgt.Server(0, workers=2, precision="auto")
+    reqs, ids = [], []
+    for k in range(6):
+        dim = 2 + k % 2
+        n = int(10 ** rng.uniform(3, 4))
+        src, trg = rng.random((n, dim)), rng.random((n // 3 + 1, dim))
+        q = rng.random(n) if k % 3 else None
+        rn, ds = rng.normal(size=(n, dim)), rng.random(n)
+        delta = 1e-3 if dim == 3 else 1e-4
+        reqs.append(fgt.transform_pgh(dim, 1, delta, 1e-6, src, q, trg, 1 + k % 3, 1, ctx=ctx,
+                                      ifcharge=int(q is not None), ifdipole=1, rnormal=rn, dipstr=ds))
+        ids.append(srv.submit(dim, 1, delta, 1e-6, src, q, trg, 1 + k % 3, 1, rnormal=rn, dipstr=ds))
+    for ref, rid in zip(reqs, ids):
+        got, _ = srv.wait_pgh(rid)
+        for key, v in ref.items():
+            if v is not None:
+                assert np.array_equal(v, got[key]), key
+    srv.close()

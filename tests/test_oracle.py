@@ -173,3 +173,47 @@ def test_oracle_derivatives_vs_direct(oracle, dim, n, delta, eps):
     r1 = oracle.fgt_pgh(dim, 1, delta, eps, src, q, trg, 1, 1)
     pot, pt, _ = oracle.fgt(dim, 1, delta, eps, src, q, trg, 1, 1)
     assert oracle.derr(pot, r1["pot"]) <= 1e-14 and oracle.derr(pt, r1["pottarg"]) <= 1e-14
+
+
+def test_direct_dipoles_are_source_derivatives(oracle):
+    """The exact dipole field (the checker of the dipole tests) is the
+    derivative of the charge field along n at the source, times dipstr
+    (g2d_directdp_vec: grad_s exp(-r^2/delta) . n)."""
+    rng = np.random.default_rng(4)
+    for dim in (2, 3):
+        delta, step = 1e-2, 1e-6
+        src, x = rng.random((50, dim)), rng.random((6, dim))
+        n = rng.normal(size=(50, dim))
+        n /= np.linalg.norm(n, axis=1)[:, None]
+        ds = rng.random((50, 1))
+        p, g, h = oracle.direct_full(dim, 1, delta, src, x, None, n, ds, pgh=3)
+        fd = (oracle.direct_full(dim, 1, delta, src + step * n, x, ds, pgh=3)[0] -
+              oracle.direct_full(dim, 1, delta, src - step * n, x, ds, pgh=3)[0]) / (2 * step)
+        assert np.allclose(p, fd, rtol=1e-6, atol=1e-8)
+        fdg = (oracle.direct_full(dim, 1, delta, src + step * n, x, ds, pgh=3)[1] -
+               oracle.direct_full(dim, 1, delta, src - step * n, x, ds, pgh=3)[1]) / (2 * step)
+        assert np.allclose(g, fdg, rtol=1e-5, atol=1e-6)
+        fdh = (oracle.direct_full(dim, 1, delta, src + step * n, x, ds, pgh=3)[2] -
+               oracle.direct_full(dim, 1, delta, src - step * n, x, ds, pgh=3)[2]) / (2 * step)
+        assert np.allclose(h, fdh, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("dim,n,delta,eps", [(2, 20000, 1e-4, 1e-6), (3, 10000, 1e-3, 1e-6),
+                                             (3, 8000, 1e-2, 1e-3), (2, 3000, 10.0, 1e-6),
+                                             (3, 3000, 10.0, 1e-6)])
+def test_oracle_dipoles_vs_direct(oracle, dim, n, delta, eps):
+    """Dipoles (g2dformhd/hcd_vec, g3dformpwd_vec, g2dformld_vec,
+    g2d_directd*/cd*_vec and the 3D twins) with and without charges.  The
+    dipole field is one derivative rougher than the charge field, so the
+    bars are twice the charge ones (20, 200, 2000 eps)."""
+    rng = np.random.default_rng(n + 11 * dim)
+    src, trg = rng.random((n, dim)), rng.random((n // 2, dim))
+    q, ds = rng.random(n), rng.random(n)
+    rn = rng.normal(size=(n, dim))
+    rn /= np.linalg.norm(rn, axis=1)[:, None]
+    for charge in (None, q):
+        r = oracle.fgt_full(dim, 1, delta, eps, src, charge, trg, 3, 3, rn, ds)
+        idx = rng.choice(n // 2, 150, replace=False)
+        exact = oracle.direct_full(dim, 1, delta, src, trg[idx], charge, rn, ds, pgh=3)
+        for order, k in enumerate(("pottarg", "gradtarg", "hesstarg")):
+            assert oracle.derr(exact[order], r[k][idx]) <= 2 * 10 ** (order + 1) * eps, (k, order)
