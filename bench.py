@@ -334,17 +334,23 @@ def ours_arm(args, w, rank, world, local_rank):
     src_h = torch.from_numpy(np.ascontiguousarray(w["src"])).pin_memory().numpy()
     chg_h = torch.from_numpy(np.ascontiguousarray(w["chg"]).reshape(-1, nd)).pin_memory().numpy()
     trg_h = src_h if w["trg"] is w["src"] else torch.from_numpy(np.ascontiguousarray(w["trg"])).pin_memory().numpy()
+    # the results land in pinned host buffers (allocated once, outside the timing)
+    out_h = {}
+    if w["ifpgh"]:
+        out_h["pot"] = torch.zeros((w["src"].shape[0], nd), dtype=torch.float64).pin_memory().numpy()
+    if w["ifpghtarg"]:
+        out_h["pottarg"] = torch.zeros((w["trg"].shape[0], nd), dtype=torch.float64).pin_memory().numpy()
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
     ctx["mixed"].set_precision("mixed")
     e2e_s = float("nan")
     if e2e_steps:
         F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"], w["ifpghtarg"],
-                    ctx=ctx["mixed"])
+                    ctx=ctx["mixed"], out=out_h)
         barrier()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"],
-                        w["ifpghtarg"], ctx=ctx["mixed"])
+                        w["ifpghtarg"], ctx=ctx["mixed"], out=out_h)
         e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
     h2d = src_h.nbytes + chg_h.nbytes + (trg_h.nbytes if w["ifpghtarg"] else 0)
     d2h = (w["src"].shape[0] * nd * 8 if w["ifpgh"] else 0) + (w["trg"].shape[0] * nd * 8 if w["ifpghtarg"] else 0)
@@ -415,7 +421,7 @@ def ours_arm(args, w, rank, world, local_rank):
         "host_plan_s": plan_s,
         "e2e": {"value": world * pts / e2e_s, "unit": "points/s", "s_per_step": e2e_s,
                 "steps": e2e_steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "includes": "tree build (point work on the GPU) + lists + plan upload + H2D + transform + D2H"},
+                "includes": "tree build (point work on the GPU) + lists + plan upload + H2D from pinned inputs + transform + D2H into pinned outputs"},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roof,
         "stage_rates": stage_rates,

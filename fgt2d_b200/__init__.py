@@ -209,18 +209,29 @@ def nhess(dim):
     return 3 if dim == 2 else 6
 
 
-def _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg):
+def _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg, out=None):
+    """Output arrays of the flags; ``out`` (optional dict) supplies caller
+    arrays (e.g. pinned host memory) of the right shapes, C-contiguous f64."""
     H = nhess(dim)
-    return {"pot": np.zeros((ns, nd)) if ifpgh >= 1 else None,
-            "grad": np.zeros((ns, dim, nd)) if ifpgh >= 2 else None,
-            "hess": np.zeros((ns, H, nd)) if ifpgh >= 3 else None,
-            "pottarg": np.zeros((nt, nd)) if ifpghtarg >= 1 else None,
-            "gradtarg": np.zeros((nt, dim, nd)) if ifpghtarg >= 2 else None,
-            "hesstarg": np.zeros((nt, H, nd)) if ifpghtarg >= 3 else None}
+    shapes = {"pot": ((ns, nd), ifpgh >= 1), "grad": ((ns, dim, nd), ifpgh >= 2),
+              "hess": ((ns, H, nd), ifpgh >= 3), "pottarg": ((nt, nd), ifpghtarg >= 1),
+              "gradtarg": ((nt, dim, nd), ifpghtarg >= 2), "hesstarg": ((nt, H, nd), ifpghtarg >= 3)}
+    o = {}
+    for k, (shape, want) in shapes.items():
+        a = out.get(k) if out else None
+        if not want:
+            o[k] = None
+        elif a is not None:
+            if a.shape != shape or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out[{k!r}] must be a C-contiguous float64 array of shape {shape}")
+            o[k] = a
+        else:
+            o[k] = np.zeros(shape)
+    return o
 
 
 def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
-                  ifcharge=1, ifdipole=0, rnormal=None, dipstr=None):
+                  ifcharge=1, ifdipole=0, rnormal=None, dipstr=None, out=None):
     """Whole transform with gradients (ifpgh / ifpghtarg = 2) and Hessians (3).
 
     Returns a dict with ``pot`` (ns, nd), ``grad`` (ns, dim, nd), ``hess``
@@ -228,7 +239,9 @@ def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpg
     ``hesstarg``), None where not requested: the reference's
     ``grad(nd, dim, ns)`` / ``hess(nd, H, ns)`` in C order.  Dipoles
     (ifdipole = 1) take ``rnormal`` (ns, dim) and ``dipstr`` (ns, nd);
-    ifcharge = 0 ignores ``charge``.
+    ifcharge = 0 ignores ``charge``.  ``out`` (optional) maps output names to
+    caller arrays that receive the results (pinned host memory avoids a
+    staged copy).
     """
     L = lib()
     src = _f64(sources, (-1, dim))
@@ -238,7 +251,7 @@ def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpg
     ds = _f64(dipstr, (ns, nd)) if ifdipole else None
     trg = _f64(targ, (-1, dim)) if targ is not None else np.zeros((0, dim))
     nt = trg.shape[0]
-    o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg)
+    o = _outputs(dim, nd, ns, nt, ifpgh, ifpghtarg, out)
     h = ctx.handle if ctx is not None else _default_ctx()
     st = L.fgt_transform(h, dim, nd, float(delta), float(eps), ns, _p(src), ifcharge, _p(q),
                          ifdipole, _p(rn), _p(ds), ifpgh, _p(o["pot"]), _p(o["grad"]), _p(o["hess"]),
@@ -249,12 +262,12 @@ def transform_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpg
 
 
 def transform(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0, ctx=None,
-              ifcharge=1, ifdipole=0, rnormal=None, dipstr=None):
+              ifcharge=1, ifdipole=0, rnormal=None, dipstr=None, out=None):
     """Whole transform; returns ``(pot, pottarg)`` shaped ``(ns, nd)``, ``(nt, nd)``.
     With ifpgh or ifpghtarg >= 2 it returns the reference's six outputs
     ``(pot, grad, hess, pottarg, gradtarg, hesstarg)`` (see transform_pgh)."""
     o = transform_pgh(dim, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, ctx, ifcharge,
-                      ifdipole, rnormal, dipstr)
+                      ifdipole, rnormal, dipstr, out)
     if max(ifpgh, ifpghtarg) >= 2:
         return o["pot"], o["grad"], o["hess"], o["pottarg"], o["gradtarg"], o["hesstarg"]
     return o["pot"], o["pottarg"]

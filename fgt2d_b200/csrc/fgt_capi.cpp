@@ -16,6 +16,7 @@
 #include <new>
 #include <vector>
 
+#include <malloc.h>
 #include <omp.h>
 
 #include "fgt_b200.h"
@@ -303,7 +304,13 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const doub
   Outputs d;
   d.pot = p->d_pot; d.grad = p->d_grad; d.hess = p->d_hess;
   d.pottarg = p->d_pottarg; d.gradtarg = p->d_gradtarg; d.hesstarg = p->d_hesstarg;
+  const double tx0 = now_s();
+  if (getenv("FGT_TREE_TIMING")) cudaStreamSynchronize(st);
+  const double tx1 = now_s();
   int s = run_device(p, in, d, st, nullptr);
+  if (getenv("FGT_TREE_TIMING")) cudaStreamSynchronize(st);
+  const double tx2 = now_s();
+  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "exec_host: inputs %.4f run %.4f\n", tx1 - tx0, tx2 - tx1);
   if (s != FGT_OK) return s;
   auto back = [&](double* h, const double* dv, size_t n) -> cudaError_t {
     return h && dv && n ? cudaMemcpyAsync(h, dv, n * 8, cudaMemcpyDeviceToHost, st) : cudaSuccess;
@@ -397,6 +404,21 @@ const char* fgt_build_info(void) { return "fgt_b200 sm_100a FP64+mixed near fiel
 int fgt_ctx_create(int device, fgt_ctx** out) {
   if (!out) return FGT_ERR_BADARG;
   *out = nullptr;
+  // The plan build's host arrays (tree, lists, task arrays: tens of MB for
+  // 1e7 points) are allocated afresh per plan; glibc serves blocks that size
+  // with mmap and returns them on free, so every plan paid a page fault per
+  // 4 KB touched (about half of the host build time measured).  Keeping them
+  // in the heap (mmap threshold at its 32 MB maximum, no trimming below
+  // 1 GB) lets later plans reuse faulted pages.  Process-wide, set once;
+  // FGT_KEEP_MALLOC=1 leaves glibc's defaults alone.
+  static std::once_flag malloc_once;
+  std::call_once(malloc_once, [] {
+    const char* e = getenv("FGT_KEEP_MALLOC");
+    if (!(e && e[0] == '1')) {
+      mallopt(M_MMAP_THRESHOLD, 32 << 20);
+      mallopt(M_TRIM_THRESHOLD, 1 << 30);
+    }
+  });
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return FGT_ERR_NODEVICE;
   if (device < 0 || device >= n) return FGT_ERR_BADARG;

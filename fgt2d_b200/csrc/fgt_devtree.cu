@@ -105,6 +105,37 @@ __global__ void __launch_bounds__(256) k_refine(const double* __restrict__ x, in
   if (c >= 0 && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(cnt + (c - c0), __popc(m));
 }
 
+// Working order of the refinement: a Morton key of depth L (x the lowest
+// bit of each level's digit, as the child numbering) per point, so that the
+// points of a box are contiguous and warps aggregate their count atomics.
+__global__ void k_morton(const double* __restrict__ x, int n, int dim, double lx, double ly, double lz,
+                         double scale, int L, unsigned long long* __restrict__ key, int* __restrict__ id) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double lo[3] = {lx, ly, lz};
+  const long long top = (1LL << L) - 1;
+  unsigned long long k = 0;
+  for (int d = 0; d < dim; d++) {
+    const double v = floor((x[(size_t)dim * i + d] - lo[d]) * scale);
+    const long long c = v < 0 ? 0 : v > (double)top ? top : (long long)v;
+    for (int b = 0; b < L; b++) k |= (unsigned long long)((c >> b) & 1) << (dim * b + d);
+  }
+  key[i] = k;
+  id[i] = i;
+}
+__global__ void k_gather_x(const double* __restrict__ x, const int* __restrict__ id, int n, int dim,
+                           double* __restrict__ xs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long j = id[i];
+  for (int d = 0; d < dim; d++) xs[(size_t)dim * i + d] = x[dim * j + d];
+}
+__global__ void k_scatter_box(const int* __restrict__ pw, const int* __restrict__ id, int n,
+                              int* __restrict__ pbox) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pbox[id[i]] = pw[i];
+}
+
 __global__ void k_remap(int* __restrict__ pbox, int n, const int* __restrict__ idmap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) pbox[i] = idmap[pbox[i]];
@@ -240,7 +271,31 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
   Scratch S(st);
   int* pbox = nullptr;
   CKD(S.get(&pbox, ns));
-  CKD(cudaMemsetAsync(pbox, 0, sizeof(int) * std::max(ns, 1), st));
+  // the refinement runs on a copy of the sources in Morton order (pw[i] is
+  // the box of working point i, wid[i] its input index); the child choice
+  // is the centre comparison either way, so the tree does not depend on it
+  int *pw = nullptr, *wid = nullptr, *wid0 = nullptr;
+  unsigned long long *mk = nullptr, *mk2 = nullptr;
+  double* xs = nullptr;
+  CKD(S.get(&pw, ns));
+  CKD(S.get(&wid, ns));
+  CKD(S.get(&wid0, ns));
+  CKD(S.get(&mk, ns));
+  CKD(S.get(&mk2, ns));
+  CKD(S.get(&xs, (size_t)ns * dim));
+  CKD(cudaMemsetAsync(pw, 0, sizeof(int) * std::max(ns, 1), st));
+  if (ns > 0) {
+    const int L = std::max(1, std::min(ts.nlmax, dim == 2 ? 31 : 21));
+    const double lo[3] = {ts.cen0[0] - ts.bs0 / 2, ts.cen0[1] - ts.bs0 / 2, ts.cen0[2] - ts.bs0 / 2};
+    k_morton<<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, dim, lo[0], lo[1], lo[2],
+                                                std::ldexp(1.0, L) / ts.bs0, L, mk, wid0);
+    size_t tmp = 0;
+    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, mk, mk2, wid0, wid, ns, 0, dim * L, st));
+    char* dtmp = nullptr;
+    CKD(S.get(&dtmp, tmp));
+    CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, mk, mk2, wid0, wid, ns, 0, dim * L, st));
+    k_gather_x<<<(ns + 255) / 256, 256, 0, st>>>(d_src, wid, ns, dim, xs);
+  }
   // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
   std::vector<int> count(1, ns), fc;
   int* d_fc = nullptr;
@@ -248,10 +303,13 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
   int* d_cnt = nullptr;
   size_t cap_lev = 0, cap_new = 0;
   int lev;
+  double th = 0, tw = 0;
   for (lev = 0; lev <= ts.nlmax - 1; lev++) {
     const int a = t.lfirst[lev], b = t.llast[lev];
     const int thr = lev < ts.levcut ? ts.ndiv0 : ts.ndiv;
+    const double th0 = now_s();
     if (tree_refine_level(t, lev, thr, count, fc) == 0) break;
+    th += now_s() - th0;
     const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0, nlev = b - a + 1;
     if ((size_t)nlev > cap_lev) {
       cap_lev = (size_t)nlev * 2;
@@ -265,11 +323,15 @@ cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, con
     CKD(upload(d_fc, fc.data(), nlev, st));
     CKD(upload(d_cen, t.centers.data() + (size_t)a * dim, (size_t)nlev * dim, st));
     CKD(cudaMemsetAsync(d_cnt, 0, sizeof(int) * nnew, st));
-    if (ns > 0) k_refine<<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, dim, pbox, a, b, d_fc, d_cen, c0, d_cnt);
+    if (ns > 0) k_refine<<<(ns + 255) / 256, 256, 0, st>>>(xs, ns, dim, pw, a, b, d_fc, d_cen, c0, d_cnt);
     count.resize(t.nboxes, 0);
     CKD(cudaMemcpyAsync(count.data() + c0, d_cnt, sizeof(int) * nnew, cudaMemcpyDeviceToHost, st));
+    const double tw0 = now_s();
     CKD(cudaStreamSynchronize(st));
+    tw += now_s() - tw0;
   }
+  if (dbg) fprintf(stderr, "refine levels %d host %.4f wait %.4f\n", lev, th, tw);
+  if (ns > 0) k_scatter_box<<<(ns + 255) / 256, 256, 0, st>>>(pw, wid, ns, pbox);
   const double tB = now_s();
   std::vector<int> idmap;
   tree_finish(t, lev, idmap);

@@ -252,47 +252,96 @@ static void build_tasks(HostPlan& H) {
   }
   // (d) near field, target-centric: for every leaf, the ifhung source boxes
   // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
-  // box A -> source boxes S with A in list1(S), as CSR in the order of S
-  std::vector<int> ioff(nb + 1, 0), into, icur;
+  // box A -> source boxes S with A in list1(S), as CSR in increasing S (the
+  // order of the reference's loop over S): counted with atomics, filled in
+  // any order, each short segment then sorted
+  std::vector<int> ioff(nb + 1, 0), into;
   int nlevend = npl < P.nlevels ? npl : P.nlevels;
-  for (int pass = 0; pass < 2; pass++) {
-    if (pass == 1) {
-      for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
-      into.assign(ioff[nb], 0);
-      icur.assign(ioff.begin(), ioff.end() - 1);
+  const int s_lo = nlevend >= 0 ? t.lfirst[0] : 0, s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;
+#pragma omp parallel for schedule(static)
+  for (int sb = s_lo; sb <= s_hi; sb++) {
+    if (!L.ifhung[sb]) continue;
+    for (int k = L.l1off[sb]; k < L.l1off[sb + 1]; k++) {
+#pragma omp atomic
+      ioff[L.l1[k] + 1]++;
     }
-    for (int l = 0; l <= nlevend; l++)
-      for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
-        if (!L.ifhung[s]) continue;
-        for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) {
-          if (pass == 0) ioff[L.l1[k] + 1]++;
-          else into[icur[L.l1[k]]++] = s;
-        }
+  }
+  for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
+  into.assign(ioff[nb], 0);
+  {
+    std::vector<int> icur(ioff.begin(), ioff.end() - 1);
+#pragma omp parallel for schedule(static)
+    for (int sb = s_lo; sb <= s_hi; sb++) {
+      if (!L.ifhung[sb]) continue;
+      for (int k = L.l1off[sb]; k < L.l1off[sb + 1]; k++) {
+        int pos;
+#pragma omp atomic capture
+        pos = icur[L.l1[k]]++;
+        into[pos] = sb;
       }
-  }
-  const int CH = 32;  // one warp per task
-  H.direct_pairs = 0;
-  std::vector<SrcRange> rs;
-  for (int b = 0; b < nb; b++) {
-    if (t.nchild[b] != 0) continue;
-    rs.clear();
-    for (int a = b; a >= 0; a = t.parent[a])
-      for (int k = ioff[a]; k < ioff[a + 1]; k++) rs.push_back({t.s0[into[k]], t.ns(into[k])});
-    if (rs.empty()) continue;
-    long long nsrc = 0;
-    for (auto& r : rs) nsrc += r.n;
-    for (int set = 0; set < 2; set++) {
-      if (set == 0 && !(P.ifpgh >= 1)) continue;
-      if (set == 1 && !(P.ifpghtarg >= 1)) continue;
-      int i0 = set == 0 ? t.s0[b] : t.t0[b];
-      int n = set == 0 ? t.ns(b) : t.nt(b);
-      if (n == 0) continue;
-      int off = (int)H.dir_src.size();
-      H.dir_src.insert(H.dir_src.end(), rs.begin(), rs.end());
-      for (int c = 0; c < n; c += CH) H.dir.push_back({set, i0 + c, std::min(CH, n - c), off, (int)rs.size()});
-      H.direct_pairs += nsrc * n;
     }
   }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; b++) std::sort(into.begin() + ioff[b], into.begin() + ioff[b + 1]);
+  // per leaf: its source ranges (ancestors' segments, leaf first) once per
+  // evaluated point set, and its tasks of <= CH points; counted per leaf,
+  // placed by prefix sums in box order, filled in parallel
+  const int CH = 32;  // one warp per task
+  const bool sets[2] = {P.ifpgh >= 1, P.ifpghtarg >= 1};
+  // ranges and sources summed down the ancestor chains, level by level
+  std::vector<long long> cum_ns(nb, 0);
+  std::vector<int> cum_r(nb, 0);
+  for (int l = 0; l <= P.nlevels; l++) {
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+      int r = ioff[b + 1] - ioff[b];
+      long long ns_ = 0;
+      for (int k = ioff[b]; k < ioff[b + 1]; k++) ns_ += t.ns(into[k]);
+      const int a = t.parent[b];
+      cum_r[b] = r + (a >= 0 ? cum_r[a] : 0);
+      cum_ns[b] = ns_ + (a >= 0 ? cum_ns[a] : 0);
+    }
+  }
+  std::vector<int> nr(nb, 0);
+  std::vector<long long> roff(nb + 1, 0), toff(nb + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; b++) {
+    if (t.nchild[b] != 0 || cum_r[b] == 0) continue;
+    const int r = cum_r[b];
+    nr[b] = r;
+    int nset = 0, nt_ = 0;
+    for (int set = 0; set < 2; set++) {
+      const int n = set == 0 ? t.ns(b) : t.nt(b);
+      if (!sets[set] || n == 0) continue;
+      nset++;
+      nt_ += (n + CH - 1) / CH;
+    }
+    roff[b + 1] = (long long)r * nset;
+    toff[b + 1] = nt_;
+  }
+  for (int b = 0; b < nb; b++) {
+    roff[b + 1] += roff[b];
+    toff[b + 1] += toff[b];
+  }
+  H.dir_src.resize(roff[nb]);
+  H.dir.resize(toff[nb]);
+  long long pairs = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs)
+  for (int b = 0; b < nb; b++) {
+    if (nr[b] == 0) continue;
+    long long ro = roff[b], to = toff[b];
+    for (int set = 0; set < 2; set++) {
+      const int n = set == 0 ? t.ns(b) : t.nt(b);
+      if (!sets[set] || n == 0) continue;
+      const int i0 = set == 0 ? t.s0[b] : t.t0[b];
+      const int off = (int)ro;
+      for (int a = b; a >= 0; a = t.parent[a])
+        for (int k = ioff[a]; k < ioff[a + 1]; k++) H.dir_src[ro++] = {t.s0[into[k]], t.ns(into[k])};
+      for (int c = 0; c < n; c += CH) H.dir[to++] = {set, i0 + c, std::min(CH, n - c), off, nr[b]};
+      pairs += cum_ns[b] * n;
+    }
+  }
+  H.direct_pairs = pairs;
   (void)D;
 }
 
