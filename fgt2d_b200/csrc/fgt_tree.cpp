@@ -124,25 +124,68 @@ struct Builder {
   }
 
   // computecoll, tree_routs4.f:100-211, levels [l0, l1]
+  // colleagues of box b at level l from its parent's list, into (nc, co)
+  void colleagues_box(int b, double lim, std::vector<int>& nc, std::vector<int>& co) {
+    int dad = t.parent[b];
+    int n = 0;
+    for (int i = 0; i < nc[dad]; i++) {
+      int jb = co[(size_t)dad * NCO + i];
+      for (int j = 0; j < NCH; j++) {
+        int kb = CH(jb, j);
+        if (kb < 0) continue;
+        bool ok = true;
+        for (int d = 0; d < D; d++)
+          if (!(std::fabs(C(kb, d) - C(b, d)) <= lim)) ok = false;
+        if (ok) co[(size_t)b * NCO + n++] = kb;
+      }
+    }
+    nc[b] = n;
+  }
   void colleagues_level(int l) {
     double lim = F105 * t.boxsize[l];
 #pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
-    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-      int dad = t.parent[b];
-      int n = 0;
-      for (int i = 0; i < t.ncoll[dad]; i++) {
-        int jb = t.coll[(size_t)dad * NCO + i];
-        for (int j = 0; j < NCH; j++) {
-          int kb = CH(jb, j);
-          if (kb < 0) continue;
-          bool ok = true;
-          for (int d = 0; d < D; d++)
-            if (!(std::fabs(C(kb, d) - C(b, d)) <= lim)) ok = false;
-          if (ok) t.coll[(size_t)b * NCO + n++] = kb;
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) colleagues_box(b, lim, t.ncoll, t.coll);
+  }
+  // After a refinement pass and its reorg (map: id before -> id after; the
+  // boxes that existed before the pass have ids < nold before it): the
+  // lists of those boxes are carried over through map, and only the new
+  // boxes and the old boxes next to them (children of a colleague of a box
+  // refined in the pass) are computed again, level by level.  computecoll's
+  // order is kept, so the result equals colleagues_all().
+  std::vector<int> refined_ids;  // ids (before reorg) of the boxes refined in the pass
+  std::vector<int> last_map;     // reorg's map
+  void colleagues_after_pass(int nold) {
+    const int nb = t.nboxes;
+    const std::vector<int>& map = last_map;
+    std::vector<int> nc(nb, 0), co((size_t)nb * NCO, -1);
+    std::vector<char> fresh(nb, 1), mark(nb, 0), refd(nb, 0);
+#pragma omp parallel for schedule(static) if (nold > 16384)
+    for (int o = 0; o < nold; o++) {
+      const int b = map[o];
+      fresh[b] = 0;
+      nc[b] = t.ncoll[o];
+      for (int i = 0; i < t.ncoll[o]; i++) co[(size_t)b * NCO + i] = map[t.coll[(size_t)o * NCO + i]];
+    }
+    for (int r : refined_ids) refd[map[r]] = 1;
+    for (int l = 1; l <= t.nlevels; l++) {
+      const double lim = F105 * t.boxsize[l];
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
+        if (fresh[b] || mark[b]) colleagues_box(b, lim, nc, co);
+      // old boxes of level l + 1 whose parent has a refined colleague
+      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+        if (!refd[b]) continue;
+        for (int i = 0; i < nc[b]; i++) {
+          const int c = co[(size_t)b * NCO + i];
+          for (int j = 0; j < NCH; j++) {
+            const int e = CH(c, j);
+            if (e >= 0 && !fresh[e]) mark[e] = 1;
+          }
         }
       }
-      t.ncoll[b] = n;
     }
+    t.ncoll.swap(nc);
+    t.coll.swap(co);
   }
   void colleagues_all() {
     t.ncoll.assign(t.nboxes, 0);
@@ -160,6 +203,7 @@ struct Builder {
       reserve_boxes(c0 + NCH);
       if ((int)iflag.size() < c0 + NCH) iflag.resize((size_t)(c0 + NCH) * 2, 0);
       make_children(box, c0, lev + 1, t.boxsize[lev + 1]);
+      refined_ids.push_back(box);
       for (int j = 0; j < NCH; j++) iflag[c0 + j] = iflag[box] == 1 ? 3 : 0;
       t.nboxes += NCH;
     }
@@ -169,7 +213,8 @@ struct Builder {
   // [old boxes of l] ++ [tail boxes of l].
   void reorg(const std::vector<int>& tf, const std::vector<int>& tl, std::vector<int>& iflag) {
     int nb = t.nboxes;
-    std::vector<int> map(nb, -1);
+    std::vector<int>& map = last_map;
+    map.assign(nb, -1);
     std::vector<int> olevel(t.level.begin(), t.level.begin() + nb);
     std::vector<int> oparent(t.parent.begin(), t.parent.begin() + nb);
     std::vector<int> onchild(t.nchild.begin(), t.nchild.begin() + nb);
@@ -239,17 +284,21 @@ struct Builder {
       }
     }
     std::vector<int> tf(nlev + 1, 0), tl(nlev + 1, -1);
+    int nold = t.nboxes;
+    refined_ids.clear();
     for (int l = 1; l <= nlev - 2; l++) {
       tf[l + 1] = t.nboxes;
       refine_flagged(iflag, t.lfirst[l], t.llast[l], l);
       tl[l + 1] = t.nboxes - 1;
     }
     reorg(tf, tl, iflag);
-    colleagues_all();
+    colleagues_after_pass(nold);
     for (int b = 0; b < t.nboxes; b++)
       if (iflag[b] != 3) iflag[b] = 0;
     std::fill(tf.begin(), tf.end(), 0);
     std::fill(tl.begin(), tl.end(), -1);
+    nold = t.nboxes;
+    refined_ids.clear();
     for (int l = 2; l <= nlev - 2; l++) {
       update_flags(l, t.lfirst[l], t.llast[l], iflag);
       update_flags(l, tf[l], tl[l], iflag);
@@ -274,7 +323,7 @@ struct Builder {
       }
     }
     reorg(tf, tl, iflag);
-    colleagues_all();
+    colleagues_after_pass(nold);
   }
 
   // updateflags, tree_routs4.f:217-326
@@ -531,60 +580,83 @@ void build_lists(const Tree& t, Lists& L) {
       if (t.nchild[b] == 0 && t.ns(b) > 0) L.ifhung[b] = 1;
   // modified list1: tree_routs4.f:715-879 (2D, symmetric insertion at
   // coarse levels) / tree_routs3d.f:511-619 (3D, coarser leaf neighbours).
-  // Two passes over the same sequence of insertions: the first counts per
-  // box, the second fills the CSR arrays in insertion order.
+  // The serial construction appends to list(X) first the symmetric entries
+  // b (boxes of the level above, in increasing id), then X's own entries in
+  // its loop order.  Here both are counted in parallel, the list is laid out
+  // as [symmetric | own], own entries are written by X's iteration and
+  // symmetric ones through atomic cursors, each symmetric block then sorted.
+  // Only the lists of boxes at levels <= the cut are read (the near-field
+  // sources are the leaves there); they receive entries from boxes of their
+  // own level and, in 2D, of the level above, so the loops stop at the cut.
   auto cdist = [&](int a, int b, int d) { return std::fabs(t.c(a, d) - t.c(b, d)); };
-  std::vector<int> cur;
-  for (int pass = 0; pass < 2; pass++) {
-    if (pass == 0) {
-      L.l1off.assign(nb + 1, 0);
-    } else {
-      for (int b = 0; b < nb; b++) L.l1off[b + 1] += L.l1off[b];
-      L.l1.assign(L.l1off[nb], 0);
-      cur.assign(L.l1off.begin(), L.l1off.end() - 1);
-    }
-    auto add = [&](int b, int v) {
-      if (pass == 0) L.l1off[b + 1]++;
-      else L.l1[cur[b]++] = v;
-    };
-    if (t.nchild[0] == 0) add(0, 0);
-    for (int l = 1; l <= t.nlevels; l++) {
-      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-        if (t.nchild[b] != 0) continue;
-        for (int i = 0; i < t.ncoll[b]; i++) {
-          int jb = t.coll[(size_t)b * NCO + i];
-          if (l >= npw || t.nchild[jb] == 0) {
-            add(b, jb);
-            continue;
-          }
-          double dist = 1.05 * (t.boxsize[l] + t.boxsize[l + 1]) / 2.0;
-          for (int j = 0; j < NCH; j++) {
-            int kb = t.ch(jb, j);
-            if (kb < 0) continue;
-            bool near = true;
-            for (int d = 0; d < D; d++)
-              if (!(cdist(kb, b, d) < dist)) near = false;
-            if (near) {
-              add(b, kb);
-              if (D == 2) add(kb, b);
-            }
-          }
-        }
-        if (D == 3) {
-          int dad = t.parent[b];
-          double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
-          for (int i = 0; i < t.ncoll[dad]; i++) {
-            int jb = t.coll[(size_t)dad * NCO + i];
-            if (t.nchild[jb] != 0) continue;
-            bool near = true;
-            for (int d = 0; d < D; d++)
-              if (!(cdist(jb, b, d) < dist)) near = false;
-            if (near) add(b, jb);
-          }
+  const int lmax = std::min(t.nlevels, nlevend);
+  const int b_hi = lmax >= 1 ? t.llast[lmax] : -1, b_lo = t.nlevels >= 1 ? t.lfirst[1] : 1;
+  // visit(b, own, sym): X's own entries in order, and (kb, b) symmetric pairs
+  auto visit = [&](int b, auto&& own, auto&& sym) {
+    const int l = t.level[b];
+    if (t.nchild[b] != 0) return;
+    for (int i = 0; i < t.ncoll[b]; i++) {
+      int jb = t.coll[(size_t)b * NCO + i];
+      if (l >= npw || t.nchild[jb] == 0) {
+        own(jb);
+        continue;
+      }
+      double dist = 1.05 * (t.boxsize[l] + t.boxsize[l + 1]) / 2.0;
+      for (int j = 0; j < NCH; j++) {
+        int kb = t.ch(jb, j);
+        if (kb < 0) continue;
+        bool near = true;
+        for (int d = 0; d < D; d++)
+          if (!(cdist(kb, b, d) < dist)) near = false;
+        if (near) {
+          own(kb);
+          if (D == 2) sym(kb);
         }
       }
     }
+    if (D == 3) {
+      int dad = t.parent[b];
+      double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+      for (int i = 0; i < t.ncoll[dad]; i++) {
+        int jb = t.coll[(size_t)dad * NCO + i];
+        if (t.nchild[jb] != 0) continue;
+        bool near = true;
+        for (int d = 0; d < D; d++)
+          if (!(cdist(jb, b, d) < dist)) near = false;
+        if (near) own(jb);
+      }
+    }
+  };
+  std::vector<int> nown(nb, 0), nsym(nb, 0);
+  if (t.nchild[0] == 0) nown[0] = 1;  // the root leaf holds itself
+#pragma omp parallel for schedule(dynamic, 512)
+  for (int b = b_lo; b <= b_hi; b++) {
+    int n = 0;
+    visit(b, [&](int) { n++; }, [&](int kb) {
+#pragma omp atomic
+      nsym[kb]++;
+    });
+    nown[b] = n;
   }
+  L.l1off.assign(nb + 1, 0);
+  for (int b = 0; b < nb; b++) L.l1off[b + 1] = L.l1off[b] + nsym[b] + nown[b];
+  L.l1.assign(L.l1off[nb], 0);
+  std::vector<int> scur(L.l1off.begin(), L.l1off.end() - 1);
+  if (t.nchild[0] == 0) L.l1[L.l1off[0] + nsym[0]] = 0;
+#pragma omp parallel for schedule(dynamic, 512)
+  for (int b = b_lo; b <= b_hi; b++) {
+    int pos = L.l1off[b] + nsym[b];
+    visit(b, [&](int v) { L.l1[pos++] = v; }, [&](int kb) {
+      int q;
+#pragma omp atomic capture
+      q = scur[kb]++;
+      L.l1[q] = b;
+    });
+  }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; b++)
+    if (nsym[b] > 1) std::sort(L.l1.begin() + L.l1off[b], L.l1.begin() + L.l1off[b] + nsym[b]);
+  std::vector<int> cur;
 
   // plane-wave lists, the same two passes
   int nls = std::max(npw, 0);
@@ -600,7 +672,10 @@ void build_lists(const Tree& t, Lists& L) {
       if (pass == 0) L.pwoff[b + 1]++;
       else L.pw[cur[b]++] = v;
     };
-    for (int l = nls; l <= t.nlevels; l++)
+    // the plan reads the cut level's lists (mp -> loc); the merge and split
+    // steps take the children from the tree, so the sibling lists of the
+    // finer levels are not built
+    for (int l = nls; l <= std::min(t.nlevels, nls); l++)
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
         if (l == npw) {
           for (int i = 0; i < t.ncoll[b]; i++) {

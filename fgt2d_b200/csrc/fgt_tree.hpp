@@ -72,10 +72,11 @@ void tree_ranges(const Tree& t, const std::vector<int>& leafcount, const std::ve
 
 // Interaction lists used by the transform (fgt2dmain / fgt3dmain set-up).
 struct Lists {
-  // modified list1 as CSR over source boxes (compute_modified_list1)
+  // modified list1 as CSR over boxes (compute_modified_list1); filled for
+  // the boxes at levels <= the cut, the only ones whose lists are read
   std::vector<int> l1off, l1;
-  // plane-wave list at the cut level and below (gt2d_computelistpw_slow /
-  // gt3d_computelistpw), CSR
+  // plane-wave list (gt2d_computelistpw_slow / gt3d_computelistpw), CSR;
+  // filled at the cut level, the only level the plan reads
   std::vector<int> pwoff, pw;
   std::vector<uint8_t> ifhung, iflocal;
 };
