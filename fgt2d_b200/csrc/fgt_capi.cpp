@@ -56,6 +56,11 @@ struct fgt_plan {
   double* d_work = nullptr;  // large-delta local expansion
   int* d_flag = nullptr;     // device-side argument checks
   int last_launches = 0;
+  // host strengths of a one-shot call, uploaded with the points so the copy
+  // overlaps the host part of the plan build (exec_host then skips it)
+  const double* pre_q = nullptr;
+  const double* pre_rn = nullptr;
+  const double* pre_ds = nullptr;
   // recorded after every execute on the stream it used: the frees of
   // fgt_plan_destroy (stream-ordered on the context's stream) wait for it
   cudaEvent_t done = nullptr;
@@ -144,6 +149,9 @@ int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int ifpgh, int ifpght
   cudaStream_t st = p->ctx->stream;
   if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
   if (nt > 0 && upload_trg) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
+  if (ns > 0 && p->pre_q) CKS(cudaMemcpyAsync(p->d_chg, p->pre_q, n_chg * 8, cudaMemcpyHostToDevice, st));
+  if (ns > 0 && p->pre_rn && p->d_rn) CKS(cudaMemcpyAsync(p->d_rn, p->pre_rn, n_rn * 8, cudaMemcpyHostToDevice, st));
+  if (ns > 0 && p->pre_ds && p->d_ds) CKS(cudaMemcpyAsync(p->d_ds, p->pre_ds, n_ds * 8, cudaMemcpyHostToDevice, st));
   return FGT_OK;
 }
 
@@ -286,15 +294,15 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const doub
   Inputs in;
   if (P.ifcharge) {
     if (!charge && ns) return FGT_ERR_BADARG;
-    CKS(cudaMemcpyAsync(p->d_chg, charge, ns * nd * 8, cudaMemcpyHostToDevice, st));
+    if (charge != p->pre_q) CKS(cudaMemcpyAsync(p->d_chg, charge, ns * nd * 8, cudaMemcpyHostToDevice, st));
     int s = check_finite_device(p, p->d_chg, ns * nd);
     if (s != FGT_OK) return s;
     in.charge = p->d_chg;
   }
   if (P.ifdipole) {
     if ((!rnormal || !dipstr) && ns) return FGT_ERR_BADARG;
-    CKS(cudaMemcpyAsync(p->d_rn, rnormal, ns * P.dim * 8, cudaMemcpyHostToDevice, st));
-    CKS(cudaMemcpyAsync(p->d_ds, dipstr, ns * nd * 8, cudaMemcpyHostToDevice, st));
+    if (rnormal != p->pre_rn) CKS(cudaMemcpyAsync(p->d_rn, rnormal, ns * P.dim * 8, cudaMemcpyHostToDevice, st));
+    if (dipstr != p->pre_ds) CKS(cudaMemcpyAsync(p->d_ds, dipstr, ns * nd * 8, cudaMemcpyHostToDevice, st));
     int s = check_finite_device(p, p->d_rn, ns * P.dim);
     if (s == FGT_OK) s = check_finite_device(p, p->d_ds, ns * nd);
     if (s != FGT_OK) return s;
@@ -327,7 +335,8 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const doub
 
 int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                      const double* sources, int nt, const double* targ, int ifcharge, int ifdipole,
-                     int ifpgh, int ifpghtarg, fgt_plan** out);
+                     int ifpgh, int ifpghtarg, fgt_plan** out, const double* pre_q = nullptr,
+                     const double* pre_rn = nullptr, const double* pre_ds = nullptr);
 
 int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                    const double* sources, int ifcharge, const double* charge, int ifdipole,
@@ -362,7 +371,8 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
   }
   fgt_plan* plan = nullptr;
   st = plan_create_impl(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifcharge, ifdipole, ifpgh,
-                        ifpghtarg, &plan);
+                        ifpghtarg, &plan, ifcharge ? charge : nullptr, ifdipole ? rnormal : nullptr,
+                        ifdipole ? dipstr : nullptr);
   if (st == FGT_OK) {
     Outputs h;
     h.pot = pot; h.grad = grad; h.hess = hess;
@@ -515,7 +525,8 @@ int fgt_plan_create_cd(fgt_ctx* ctx, int dim, int nd, double delta, double eps, 
 namespace {
 int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
                      const double* sources, int nt, const double* targ, int ifcharge, int ifdipole,
-                     int ifpgh, int ifpghtarg, fgt_plan** out) {
+                     int ifpgh, int ifpghtarg, fgt_plan** out, const double* pre_q,
+                     const double* pre_rn, const double* pre_ds) {
   if (!ctx || !out) return FGT_ERR_BADARG;
   *out = nullptr;
   int st = check_args(dim, nd, delta, eps, ns, sources, ifcharge, ifdipole, ifpgh, nt, targ, ifpghtarg,
@@ -526,6 +537,9 @@ int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, in
   std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
   if (!p) return FGT_ERR_NOMEM;
   p->ctx = ctx;
+  p->pre_q = pre_q;
+  p->pre_rn = pre_rn;
+  p->pre_ds = pre_ds;
   CKS(cudaSetDevice(ctx->device));
   if (ctx->tree == FGT_TREE_DEVICE) {
     st = plan_create_device_tree(p.get(), dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg,
@@ -1156,6 +1170,9 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
     return FGT_ERR_NOMEM;
   }
   p->ctx = ctx;
+  p->pre_q = ifcharge ? r.charge : nullptr;
+  p->pre_rn = ifdipole ? r.rnormal : nullptr;
+  p->pre_ds = ifdipole ? r.dipstr : nullptr;
   std::function<int(size_t)> admit = [&](size_t b) {
     plan_bytes = (long long)b;
     server_take(S, &S->in_plan, S->budget_plan, plan_bytes);

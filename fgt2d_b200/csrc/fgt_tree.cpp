@@ -223,33 +223,36 @@ struct Builder {
     std::vector<int> oflag(iflag.begin(), iflag.begin() + nb);
     for (int l = 0; l <= std::min(1, t.nlevels); l++)
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) map[b] = b;
+    // the new position of every box: per level the old boxes, then the tail
     if (t.nlevels >= 2) {
       int cur = t.lfirst[2];
       for (int l = 2; l <= t.nlevels; l++) {
-        int a0 = t.lfirst[l], a1 = t.llast[l];
+        const int a0 = t.lfirst[l], a1 = t.llast[l];
         t.lfirst[l] = cur;
         for (int pass = 0; pass < 2; pass++) {
-          int a = pass ? tf[l] : a0, b = pass ? tl[l] : a1;
-          for (int box = a; box <= b; box++) {
-            t.level[cur] = olevel[box];
-            t.nchild[cur] = onchild[box];
-            for (int d = 0; d < D; d++) t.centers[(size_t)cur * D + d] = ocent[(size_t)box * D + d];
-            iflag[cur] = oflag[box];
-            map[box] = cur++;
-          }
+          const int a = pass ? tf[l] : a0, b = pass ? tl[l] : a1, base = cur;
+#pragma omp parallel for schedule(static) if (b - a > 16384)
+          for (int box = a; box <= b; box++) map[box] = base + (box - a);
+          cur += std::max(0, b - a + 1);
         }
         t.llast[l] = cur - 1;
       }
     }
-    for (int& v : idmap) v = map[v];
+#pragma omp parallel for schedule(static) if (nb > 16384)
     for (int box = 0; box < nb; box++) {
-      int nbx = map[box];
+      const int nbx = map[box];
+      t.level[nbx] = olevel[box];
+      t.nchild[nbx] = onchild[box];
+      for (int d = 0; d < D; d++) t.centers[(size_t)nbx * D + d] = ocent[(size_t)box * D + d];
+      iflag[nbx] = oflag[box];
       t.parent[nbx] = oparent[box] >= 0 ? map[oparent[box]] : -1;
       for (int j = 0; j < NCH; j++) {
         int c = ochild[(size_t)box * NCH + j];
         CH(nbx, j) = c >= 0 ? map[c] : -1;
       }
     }
+#pragma omp parallel for schedule(static) if (idmap.size() > 16384)
+    for (size_t k = 0; k < idmap.size(); k++) idmap[k] = map[idmap[k]];
   }
 
   bool touching(int a, int b, double lim) {
