@@ -252,37 +252,24 @@ static void build_tasks(HostPlan& H) {
   }
   // (d) near field, target-centric: for every leaf, the ifhung source boxes
   // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
-  // box A -> source boxes S with A in list1(S), as CSR in increasing S (the
-  // order of the reference's loop over S): counted with atomics, filled in
-  // any order, each short segment then sorted
-  std::vector<int> ioff(nb + 1, 0), into;
+  // box A -> source boxes S with A in list1(S), as CSR in the order of S
+  std::vector<int> ioff(nb + 1, 0), into, icur;
   int nlevend = npl < P.nlevels ? npl : P.nlevels;
-  const int s_lo = nlevend >= 0 ? t.lfirst[0] : 0, s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;
-#pragma omp parallel for schedule(static)
-  for (int sb = s_lo; sb <= s_hi; sb++) {
-    if (!L.ifhung[sb]) continue;
-    for (int k = L.l1off[sb]; k < L.l1off[sb + 1]; k++) {
-#pragma omp atomic
-      ioff[L.l1[k] + 1]++;
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 1) {
+      for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
+      into.assign(ioff[nb], 0);
+      icur.assign(ioff.begin(), ioff.end() - 1);
     }
-  }
-  for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
-  into.assign(ioff[nb], 0);
-  {
-    std::vector<int> icur(ioff.begin(), ioff.end() - 1);
-#pragma omp parallel for schedule(static)
-    for (int sb = s_lo; sb <= s_hi; sb++) {
-      if (!L.ifhung[sb]) continue;
-      for (int k = L.l1off[sb]; k < L.l1off[sb + 1]; k++) {
-        int pos;
-#pragma omp atomic capture
-        pos = icur[L.l1[k]]++;
-        into[pos] = sb;
+    for (int l = 0; l <= nlevend; l++)
+      for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
+        if (!L.ifhung[s]) continue;
+        for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) {
+          if (pass == 0) ioff[L.l1[k] + 1]++;
+          else into[icur[L.l1[k]]++] = s;
+        }
       }
-    }
   }
-#pragma omp parallel for schedule(static)
-  for (int b = 0; b < nb; b++) std::sort(into.begin() + ioff[b], into.begin() + ioff[b + 1]);
   // per leaf: its source ranges (ancestors' segments, leaf first) once per
   // evaluated point set, and its tasks of <= CH points; counted per leaf,
   // placed by prefix sums in box order, filled in parallel
