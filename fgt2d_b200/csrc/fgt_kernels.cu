@@ -1025,38 +1025,62 @@ __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __res
   const int npw = k.npw, n2 = k.n2;
   const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
   extern __shared__ double sm[];
-  // region A: H, later T2 [(j3 npw + k2) n2 + k1]; region B: T1 [(j3 + P j2) n2 + k1]
+  // region A: H, later T2 [(j3 npw + k2) n2 + k1]; region B: T1 [(j3 + P j2) n2 + k1];
+  // then the signed table hs[j][k] = h2x[j][k] (j mod 4 < 2 ? 1 : -1).  The
+  // factor i^j of each pass is then a sign (in hs) times 1 (even j) or i
+  // (odd j): even and odd j are summed apart, E + i O, and the mirror node
+  // of k (A(j, mirror k) = (-1)^j A(j, k)) gets E - i O.
   const size_t szA = max((size_t)P3, (size_t)2 * Pn * npw * n2);
   double* H = sm;
   double2* T2 = reinterpret_cast<double2*>(sm);
   double2* T1 = reinterpret_cast<double2*>(sm + ((szA + 1) & ~size_t(1)));
+  double* hs = reinterpret_cast<double*>(T1 + (size_t)P2 * n2);
+  for (int e = threadIdx.x; e < Pn * npw; e += blockDim.x) {
+    const int j = e / npw;
+    hs[e] = (j & 2) ? -k.h2x[e] : k.h2x[e];
+  }
   for (int e = threadIdx.x; e < P3; e += blockDim.x) {
     double v = 0.0;
     for (int c = cbeg[tk]; c < cbeg[tk + 1]; c++) v += hbuf[(size_t)chunks[c].hoff * k.nd + (size_t)ind * P3 + e];
     H[e] = v;
   }
   __syncthreads();
+  // z pass over the stored half (the first n2 ascending nodes)
   for (int idx = threadIdx.x; idx < P2 * n2; idx += blockDim.x) {
     const int k1 = idx % n2, jj = idx / n2;
-    double2 a = make_double2(0.0, 0.0);
-    for (int j1 = 0; j1 < Pn; j1++) addrot(a, k.h2x[j1 * npw + k1] * H[jj + P2 * j1], j1);
-    T1[idx] = a;
+    double ev = 0.0, od = 0.0;
+    int j1 = 0;
+    for (; j1 + 1 < Pn; j1 += 2) {
+      ev = fma(hs[j1 * npw + k1], H[jj + P2 * j1], ev);
+      od = fma(hs[(j1 + 1) * npw + k1], H[jj + P2 * (j1 + 1)], od);
+    }
+    if (j1 < Pn) ev = fma(hs[j1 * npw + k1], H[jj + P2 * j1], ev);
+    T1[idx] = make_double2(ev, od);
   }
   __syncthreads();
   // y pass over the positive half k2 = n2 + m and its mirror n2 - 1 - m
   for (int idx = threadIdx.x; idx < Pn * n2 * n2; idx += blockDim.x) {
     const int k1 = idx % n2, r = idx / n2, m = r % n2, j3 = r / n2;
     const int kp = n2 + m, km = n2 - 1 - m;
-    double2 ev = make_double2(0.0, 0.0), od = make_double2(0.0, 0.0);
-    for (int j2 = 0; j2 < Pn; j2++) {
-      const double h = k.h2x[j2 * npw + kp];
-      const double2 z = rot(T1[(j3 + Pn * j2) * n2 + k1], j2);
-      double2& acc = (j2 & 1) ? od : ev;
-      acc.x = fma(h, z.x, acc.x);
-      acc.y = fma(h, z.y, acc.y);
+    double2 E = make_double2(0.0, 0.0), O = make_double2(0.0, 0.0);
+    const double2* zc = T1 + (size_t)j3 * n2 + k1;
+    int j2 = 0;
+    for (; j2 + 1 < Pn; j2 += 2) {
+      const double he = hs[j2 * npw + kp], ho = hs[(j2 + 1) * npw + kp];
+      const double2 ze = zc[(size_t)Pn * j2 * n2], zo = zc[(size_t)Pn * (j2 + 1) * n2];
+      E.x = fma(he, ze.x, E.x);
+      E.y = fma(he, ze.y, E.y);
+      O.x = fma(ho, zo.x, O.x);
+      O.y = fma(ho, zo.y, O.y);
     }
-    T2[((size_t)j3 * npw + kp) * n2 + k1] = make_double2(ev.x + od.x, ev.y + od.y);
-    T2[((size_t)j3 * npw + km) * n2 + k1] = make_double2(ev.x - od.x, ev.y - od.y);
+    if (j2 < Pn) {
+      const double he = hs[j2 * npw + kp];
+      const double2 ze = zc[(size_t)Pn * j2 * n2];
+      E.x = fma(he, ze.x, E.x);
+      E.y = fma(he, ze.y, E.y);
+    }
+    T2[((size_t)j3 * npw + kp) * n2 + k1] = make_double2(E.x - O.y, E.y + O.x);
+    T2[((size_t)j3 * npw + km) * n2 + k1] = make_double2(E.x + O.y, E.y - O.x);
   }
   __syncthreads();
   double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
@@ -1064,17 +1088,27 @@ __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __res
   for (int idx = threadIdx.x; idx < n2 * npw * n2; idx += blockDim.x) {
     const int m = idx % n2, r = idx / n2, k2 = r % npw, k1 = r / npw;
     const int kp = n2 + m, km = n2 - 1 - m;
-    double2 ev = make_double2(0.0, 0.0), od = make_double2(0.0, 0.0);
-    for (int j3 = 0; j3 < Pn; j3++) {
-      const double h = k.h2x[j3 * npw + kp];
-      const double2 z = rot(T2[((size_t)j3 * npw + k2) * n2 + k1], j3);
-      double2& acc = (j3 & 1) ? od : ev;
-      acc.x = fma(h, z.x, acc.x);
-      acc.y = fma(h, z.y, acc.y);
+    double2 E = make_double2(0.0, 0.0), O = make_double2(0.0, 0.0);
+    const double2* zc = T2 + (size_t)k2 * n2 + k1;
+    const size_t zs = (size_t)npw * n2;
+    int j3 = 0;
+    for (; j3 + 1 < Pn; j3 += 2) {
+      const double he = hs[j3 * npw + kp], ho = hs[(j3 + 1) * npw + kp];
+      const double2 ze = zc[zs * j3], zo = zc[zs * (j3 + 1)];
+      E.x = fma(he, ze.x, E.x);
+      E.y = fma(he, ze.y, E.y);
+      O.x = fma(ho, zo.x, O.x);
+      O.y = fma(ho, zo.y, O.y);
+    }
+    if (j3 < Pn) {
+      const double he = hs[j3 * npw + kp];
+      const double2 ze = zc[zs * j3];
+      E.x = fma(he, ze.x, E.x);
+      E.y = fma(he, ze.y, E.y);
     }
     const size_t base = (size_t)npw * (k2 + (size_t)npw * k1);
-    out[base + kp] = make_double2(ev.x + od.x, ev.y + od.y);
-    out[base + km] = make_double2(ev.x - od.x, ev.y - od.y);
+    out[base + kp] = make_double2(E.x - O.y, E.y + O.x);
+    out[base + km] = make_double2(E.x + O.y, E.y - O.x);
   }
 }
 
@@ -2737,7 +2771,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     if (D.form_hermite_n > 0) {
       const size_t Pn = D.form_pmax + 1, P3 = Pn * Pn * Pn;
       size_t szA = std::max(P3, 2 * Pn * P.npw * n2);
-      D.form3_shB = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
+      D.form3_shB = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2 + Pn * P.npw) * 8;
       // k_form3d_mma stages (8 ceil(P/8) + 2 P) power rows of 68 doubles
       const size_t shA = ((size_t)8 * ((Pn + 7) / 8) + 2 * Pn) * 68 * 8;
       D.form3_smem = D.form3_shB <= lim && shA <= lim && Pn <= 32;
