@@ -126,6 +126,11 @@ struct DevicePlan {
   double2* scratch = nullptr;
   size_t scratch_per_cta = 0;  // in double2
   int scratch_ctas = 0;
+  // U2 scratch of the persistent 3D PW -> Taylor conversion: conv3_ctas CTAs
+  // per density, uscr_per_cta doubles each
+  double* uscr = nullptr;
+  size_t uscr_per_cta = 0;
+  int conv3_ctas = 0;
   // launch shapes
   int form_hermite_n = 0, form_pw_n = 0;
   int eval_taylor_n = 0, eval_pw_n = 0;

@@ -1369,9 +1369,16 @@ struct Conv3Dims {
   }
 };
 
+// Shared memory of k_pw2taylor3d with nw warps (the tables and one pass-2
+// operand per warp; U2 lives in the CTA's global scratch, conv3_scratch).
 size_t conv3_smem_bytes(int Pn, int npw, int nw) {
   const Conv3Dims Z(Pn, npw);
-  return ((size_t)Z.tab + Z.shared + (size_t)nw * Z.warp) * 8;
+  return ((size_t)Z.tab + (size_t)nw * Z.warp) * 8;
+}
+// Doubles of U2 (real and imaginary parts) per CTA.
+size_t conv3_scratch(int Pn, int npw) {
+  const Conv3Dims Z(Pn, npw);
+  return (size_t)Z.shared;
 }
 
 // Tables of k_pw2taylor3d for order P: XT[m][n] = x2l[n][m] (m < npw, n < P),
@@ -1393,124 +1400,133 @@ void build_conv3_table(const HostPlan& H, int Pn, std::vector<double>& out) {
     }
 }
 
+// Persistent CTAs: the launch's tasks (one order) are taken in turn; U2
+// (the pass-3 operand, 2 P^2 n2 doubles) lives in the CTA's slice of uscr
+// (global memory, L2-resident), so shared memory holds only the tables and
+// one pass-2 operand per warp and several CTAs fit on an SM.
 template <int KS1>  // pass 1 depth in steps of 4: KS1 = ceil(npw / 4)
-__global__ void __launch_bounds__(256) k_pw2taylor3d(KP k, const ConvTask* __restrict__ tasks,
+__global__ void __launch_bounds__(128) k_pw2taylor3d(KP k, const ConvTask* __restrict__ tasks, int ntask,
                                                      double* __restrict__ lo_all,
-                                                     const double* __restrict__ tab) {
+                                                     const double* __restrict__ tab,
+                                                     double* __restrict__ uscr, size_t uper) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int r = lane >> 2, c = lane & 3;
-  const ConvTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
-  const Conv3Dims Z(T.p + 1, k.npw);
+  const Conv3Dims Z(tasks[0].p + 1, k.npw);
   const int Pn = Z.Pn, E = Z.E, npw = Z.npw, n2 = Z.n2;
   extern __shared__ double s3[];
   double* XT = s3;                                 // [K1][ldT]
   double* B3e = XT + Z.K1 * Z.ldT;                 // [K3][ldB3]
   double* B3o = B3e + Z.K3 * Z.ldB3;
-  double* Ure = s3 + Z.tab;                        // [M3][ldU]
+  double* A2 = s3 + Z.tab + warp * Z.warp;         // [M2][ldA2]
+  double* Ure = uscr + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * uper;  // [M3][ldU]
   double* Uim = Ure + Z.M3 * Z.ldU;
-  double* A2 = Uim + Z.M3 * Z.ldU + warp * Z.warp; // [M2][ldA2]
   for (int e = threadIdx.x; e < Z.tab; e += blockDim.x) s3[e] = tab[e];
+  // every task writes the same entries of U2; the rest (padding) stays zero
   for (int e = threadIdx.x; e < 2 * Z.M3 * Z.ldU; e += blockDim.x) Ure[e] = 0.0;
   __syncthreads();
-  const double* Ld = reinterpret_cast<const double*>(k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp);
-  for (int m1 = warp; m1 < n2; m1 += nw) {
-    // pass 1: rows (m2, re/im) of the slice, columns a
-    for (int mt = 0; mt < Z.M1 / 8; mt++) {
-      const int row = 8 * mt + r, m2 = row >> 1, comp = row & 1;
-      const bool rok = m2 < npw;
-      const double* ap = Ld + ((size_t)(m1 * npw + m2) * npw) * 2 + comp;
-      double av[KS1];
-#pragma unroll
-      for (int ks = 0; ks < KS1; ks++) {
-        const int m3 = 4 * ks + c;
-        av[ks] = (rok && m3 < npw) ? __ldg(ap + 2 * m3) : 0.0;
-      }
-      for (int nt = 0; nt < Z.N1 / 8; nt++) {
-        const double* bp = XT + c * Z.ldT + 8 * nt + r;
-        double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+  for (int task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const ConvTask T = tasks[task];
+    const double* Ld = reinterpret_cast<const double*>(k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp);
+    for (int m1 = warp; m1 < n2; m1 += nw) {
+      // pass 1: rows (m2, re/im) of the slice, columns a
+      for (int mt = 0; mt < Z.M1 / 8; mt++) {
+        const int row = 8 * mt + r, m2 = row >> 1, comp = row & 1;
+        const bool rok = m2 < npw;
+        const double* ap = Ld + ((size_t)(m1 * npw + m2) * npw) * 2 + comp;
+        double av[KS1];
 #pragma unroll
         for (int ks = 0; ks < KS1; ks++) {
-          if (ks & 1) dmma_884(e0, e1, av[ks], bp[4 * ks * Z.ldT]);
-          else dmma_884(d0, d1, av[ks], bp[4 * ks * Z.ldT]);
+          const int m3 = 4 * ks + c;
+          av[ks] = (rok && m3 < npw) ? __ldg(ap + 2 * m3) : 0.0;
         }
-        d0 += e0;
-        d1 += e1;
-        // lane r holds comp (r & 1) of S1[m2][a0], S1[m2][a0 + 1]; r xor 1 the other
-        const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
-        const int a0 = 8 * nt + 2 * c;
-        const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), a0);
-        const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), a0 + 1);
-        if (m2 < Z.K2) {
-          if (comp == 0) {
-            A2[(2 * a0) * Z.ldA2 + m2] = z0.x;
-            A2[(2 * a0 + 1) * Z.ldA2 + m2] = z0.y;
-          } else {
-            A2[(2 * a0 + 2) * Z.ldA2 + m2] = z1.x;
-            A2[(2 * a0 + 3) * Z.ldA2 + m2] = z1.y;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    // pass 2: rows (a, re/im), columns b; U2[a][b][m1] into Ure / Uim
-    for (int mt = 0; mt < Z.M2 / 8; mt++) {
-      const double* ap = A2 + (8 * mt + r) * Z.ldA2 + c;
-      for (int nt = 0; nt < Z.N1 / 8; nt++) {
-        const double* bp = XT + c * Z.ldT + 8 * nt + r;
-        double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
-        for (int ks = 0; ks < Z.K2 / 4; ks += 2) {
-          dmma_884(d0, d1, ap[4 * ks], bp[4 * ks * Z.ldT]);
-          if (ks + 1 < Z.K2 / 4) dmma_884(e0, e1, ap[4 * ks + 4], bp[(4 * ks + 4) * Z.ldT]);
-        }
-        d0 += e0;
-        d1 += e1;
-        const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
-        const int row = 8 * mt + r, a = row >> 1, comp = row & 1, b0 = 8 * nt + 2 * c;
-        const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), b0);
-        const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), b0 + 1);
-        if (a < Pn) {
-          if (comp == 0 && b0 < Pn) {
-            Ure[(a * Pn + b0) * Z.ldU + m1] = z0.x;
-            Uim[(a * Pn + b0) * Z.ldU + m1] = z0.y;
-          }
-          if (comp == 1 && b0 + 1 < Pn) {
-            Ure[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.x;
-            Uim[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.y;
-          }
-        }
-      }
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  // pass 3: lo[c][b][a] = 2 {x, -y, -x, y}[c mod 4] of sum_m1 x2l[c][m1] U2[a][b][m1]
-  double* out = lo_all + T.off + (size_t)ind * Pn * Pn * E;
-  for (int mt = warp; mt < Z.M3 / 8; mt += nw) {
-    const double* ae = Ure + (8 * mt + r) * Z.ldU + c;
-    const double* ao = Uim + (8 * mt + r) * Z.ldU + c;
-    for (int nt = 0; nt < Z.N3 / 8; nt++) {
-      const double* be = B3e + c * Z.ldB3 + 8 * nt + r;
-      const double* bo = B3o + c * Z.ldB3 + 8 * nt + r;
-      double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
-      for (int ks = 0; ks < Z.K3 / 4; ks++) {
-        dmma_884(e0, e1, ae[4 * ks], be[4 * ks * Z.ldB3]);
-        dmma_884(o0, o1, ao[4 * ks], bo[4 * ks * Z.ldB3]);
-      }
-      const int q = 8 * mt + r;
-      if (q >= Pn * Pn) continue;
-      const int a = q / Pn, b = q - a * Pn;
-      const double ev[2] = {e0, e1}, od[2] = {o0, o1};
+        for (int nt = 0; nt < Z.N1 / 8; nt++) {
+          const double* bp = XT + c * Z.ldT + 8 * nt + r;
+          double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
 #pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const int ce = 2 * (8 * nt + 2 * c + i), co = ce + 1;
-        if (ce < Pn) out[((size_t)ce * Pn + b) * E + a] = ((ce & 3) == 2 ? -2.0 : 2.0) * ev[i];
-        if (co < Pn) out[((size_t)co * Pn + b) * E + a] = ((co & 3) == 1 ? -2.0 : 2.0) * od[i];
+          for (int ks = 0; ks < KS1; ks++) {
+            if (ks & 1) dmma_884(e0, e1, av[ks], bp[4 * ks * Z.ldT]);
+            else dmma_884(d0, d1, av[ks], bp[4 * ks * Z.ldT]);
+          }
+          d0 += e0;
+          d1 += e1;
+          // lane r holds comp (r & 1) of S1[m2][a0], S1[m2][a0 + 1]; r xor 1 the other
+          const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
+          const int a0 = 8 * nt + 2 * c;
+          const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), a0);
+          const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), a0 + 1);
+          if (m2 < Z.K2) {
+            if (comp == 0) {
+              A2[(2 * a0) * Z.ldA2 + m2] = z0.x;
+              A2[(2 * a0 + 1) * Z.ldA2 + m2] = z0.y;
+            } else {
+              A2[(2 * a0 + 2) * Z.ldA2 + m2] = z1.x;
+              A2[(2 * a0 + 3) * Z.ldA2 + m2] = z1.y;
+            }
+          }
+        }
+      }
+      __syncwarp();
+      // pass 2: rows (a, re/im), columns b; U2[a][b][m1] into Ure / Uim
+      for (int mt = 0; mt < Z.M2 / 8; mt++) {
+        const double* ap = A2 + (8 * mt + r) * Z.ldA2 + c;
+        for (int nt = 0; nt < Z.N1 / 8; nt++) {
+          const double* bp = XT + c * Z.ldT + 8 * nt + r;
+          double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+          for (int ks = 0; ks < Z.K2 / 4; ks += 2) {
+            dmma_884(d0, d1, ap[4 * ks], bp[4 * ks * Z.ldT]);
+            if (ks + 1 < Z.K2 / 4) dmma_884(e0, e1, ap[4 * ks + 4], bp[(4 * ks + 4) * Z.ldT]);
+          }
+          d0 += e0;
+          d1 += e1;
+          const double o0 = __shfl_xor_sync(FULL_MASK, d0, 4), o1 = __shfl_xor_sync(FULL_MASK, d1, 4);
+          const int row = 8 * mt + r, a = row >> 1, comp = row & 1, b0 = 8 * nt + 2 * c;
+          const double2 z0 = rot_bf(comp ? make_double2(o0, d0) : make_double2(d0, o0), b0);
+          const double2 z1 = rot_bf(comp ? make_double2(o1, d1) : make_double2(d1, o1), b0 + 1);
+          if (a < Pn) {
+            if (comp == 0 && b0 < Pn) {
+              Ure[(a * Pn + b0) * Z.ldU + m1] = z0.x;
+              Uim[(a * Pn + b0) * Z.ldU + m1] = z0.y;
+            }
+            if (comp == 1 && b0 + 1 < Pn) {
+              Ure[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.x;
+              Uim[(a * Pn + b0 + 1) * Z.ldU + m1] = z1.y;
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    // pass 3: lo[c][b][a] = 2 {x, -y, -x, y}[c mod 4] of sum_m1 x2l[c][m1] U2[a][b][m1]
+    double* out = lo_all + T.off + (size_t)ind * Pn * Pn * E;
+    for (int mt = warp; mt < Z.M3 / 8; mt += nw) {
+      const double* ae = Ure + (8 * mt + r) * Z.ldU + c;
+      const double* ao = Uim + (8 * mt + r) * Z.ldU + c;
+      for (int nt = 0; nt < Z.N3 / 8; nt++) {
+        const double* be = B3e + c * Z.ldB3 + 8 * nt + r;
+        const double* bo = B3o + c * Z.ldB3 + 8 * nt + r;
+        double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+        for (int ks = 0; ks < Z.K3 / 4; ks++) {
+          dmma_884(e0, e1, ae[4 * ks], be[4 * ks * Z.ldB3]);
+          dmma_884(o0, o1, ao[4 * ks], bo[4 * ks * Z.ldB3]);
+        }
+        const int q = 8 * mt + r;
+        if (q >= Pn * Pn) continue;
+        const int a = q / Pn, b = q - a * Pn;
+        const double ev[2] = {e0, e1}, od[2] = {o0, o1};
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const int ce = 2 * (8 * nt + 2 * c + i), co = ce + 1;
+          if (ce < Pn) out[((size_t)ce * Pn + b) * E + a] = ((ce & 3) == 2 ? -2.0 : 2.0) * ev[i];
+          if (co < Pn) out[((size_t)co * Pn + b) * E + a] = ((co & 3) == 1 ? -2.0 : 2.0) * od[i];
+        }
       }
     }
+    if (E > Pn)  // the padding column of every row
+      for (int e = threadIdx.x; e < Pn * Pn; e += blockDim.x) out[(size_t)e * E + Pn] = 0.0;
+    __syncthreads();  // U2 of this task is read until here
   }
-  if (E > Pn)  // the padding column of every row
-    for (int e = threadIdx.x; e < Pn * Pn; e += blockDim.x) out[(size_t)e * E + Pn] = 0.0;
 }
 
 // k_eval3d_horner: one CTA (128 threads) per chunk of <= 256 points of an
@@ -2680,8 +2696,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   std::vector<HornerTask> horner;
   size_t lo_doubles = 0;
   // 3D: the same two kernels where the order's shared-memory needs fit
-  D.eval3_split = P.dim == 3 && !P.all_direct && D.eval_taylor_n > 0 &&
-                  conv3_smem_bytes(D.eval_pmax + 1, P.npw, 1) <= 227 * 1024 && (P.npw + 3) / 4 <= CONV_MAXKS;
+  // (k_eval3d_horner is instantiated for rows of up to 30 coefficients)
+  D.eval3_split = P.dim == 3 && !P.all_direct && D.eval_taylor_n > 0 && D.eval_pmax + 1 <= 30 &&
+                  conv3_smem_bytes(D.eval_pmax + 1, P.npw, 4) <= 200 * 1024 && (P.npw + 3) / 4 <= CONV_MAXKS;
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     for (int t = 0; t < D.eval_taylor_n; t++) {
@@ -2827,6 +2844,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     D.scratch_per_cta = (slab + 15) & ~size_t(15);
     D.scratch_ctas = D.scratch_per_cta ? D.sm_count * 2 : 0;
   }
+  if (D.eval3_split) {
+    D.uscr_per_cta = (conv3_scratch(D.eval_pmax + 1, P.npw) + 31) & ~size_t(31);
+    D.conv3_ctas = D.sm_count * 4;
+  }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
   // diagonal translation tables (formed on the device)
   const size_t n_wms = P.all_direct ? 0 : (size_t)(P.nlevels + 1) * D.nch * P.nexp;
@@ -2841,6 +2862,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  al(P.ifdipole ? ns * dim * 8 : 0) + al(P.ifdipole ? ns * nd * 8 : 0) +
                  al(nt * nd * out_comps(dim, P.ifpghtarg) * 8) +
                  al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
+                 al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8) +
                  bytes_of(fcbeg) + al(hbuf_doubles * 8) + bytes_of(form_hoff) + bytes_of(tables) + bytes_of(conv) + bytes_of(horner) +
                  al(lo_doubles * 8) + 4096;
   D.bytes = total;
@@ -2947,6 +2969,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.psort = reinterpret_cast<double*>(cur); cur += al(ns * nd * out_comps(dim, P.ifpgh) * 8);
   D.ptsort = reinterpret_cast<double*>(cur); cur += al(nt * nd * out_comps(dim, P.ifpghtarg) * 8);
   D.scratch = reinterpret_cast<double2*>(cur); cur += al((size_t)D.scratch_ctas * D.scratch_per_cta * 16);
+  D.uscr = reinterpret_cast<double*>(cur); cur += al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8);
   CK(cudaStreamSynchronize(s));
   return cudaSuccess;
 }
@@ -3252,15 +3275,15 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     if (P.dim == 3 && D.eval3_split) {
       for (const OrderGroup& G : D.conv_groups) {
         const int Pn = G.p + 1, nt = G.end - G.beg;
-        int nw = 8;
-        while (nw > 1 && conv3_smem_bytes(Pn, P.npw, nw) > 200 * 1024) nw >>= 1;
+        const int nw = 4;
         const size_t sh = conv3_smem_bytes(Pn, P.npw, nw);
-        const dim3 cg(nt, nd);
+        const dim3 cg(std::min(nt, D.conv3_ctas), nd);
         switch ((P.npw + 3) / 4) {
 #define CONV3_CASE(N)                                                                             \
   case N:                                                                                         \
     CK(cudaFuncSetAttribute(k_pw2taylor3d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_pw2taylor3d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, D.lo, D.tables + G.tab);         \
+    k_pw2taylor3d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab,      \
+                                              D.uscr, D.uscr_per_cta);                            \
     break;
           CONV3_CASE(1) CONV3_CASE(2) CONV3_CASE(3) CONV3_CASE(4) CONV3_CASE(5) CONV3_CASE(6)
           CONV3_CASE(7) CONV3_CASE(8) CONV3_CASE(9) CONV3_CASE(10) CONV3_CASE(11) CONV3_CASE(12)
