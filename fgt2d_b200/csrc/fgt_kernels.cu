@@ -1112,6 +1112,195 @@ __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __res
   }
 }
 
+// k_form3d_h2pw_mma: the transform of k_form3d_h2pw with its three passes on
+// the FP64 tensor cores.  Each pass is a real product against the signed node
+// table hs, the even and odd j in separate k-steps so that i^j becomes E + i O
+// and the mirror node gets E - i O from the same accumulators (K = j, KS
+// k-steps of 4 per parity):
+//   z pass  E/O[m][kz]   = sum_l  H[m][l] hs[l][kz],        m = jx + P jy, kz < n2
+//           -> T1[jy][(jx, kz)] = E + i O                    (M = P^2, N = n2)
+//   y pass  E/O[m][col]  = sum_jy hs[jy][n2 + m] T1[jy][col], col = (jx, kz, re/im)
+//           -> T2[jx][(ky, kz)], ky = n2 + m and n2 - 1 - m  (M = n2, N = 2 P n2)
+//   x pass  E/O[m][col]  = sum_jx hs[jx][n2 + m] T2[jx][col], col = (ky, kz, re/im)
+//           -> the slot, kx = n2 + m and n2 - 1 - m          (M = n2, N = 2 npw n2)
+// The y and x passes run per 8-row tile t of the node half: the y pass of tile
+// t fills T2 with its 16 ky and the x pass of tile t drains it, so T2 holds 16
+// ky instead of npw and the Hermite block H shares its space.  The node tables
+// are register fragments; rows j >= P are zero fragments, not loads.  Row
+// strides are 4 (mod 8) doubles, so the rows two apart that one fragment reads
+// fall in opposite halves of the banks.  One CTA of 8 warps per leaf and
+// density; two CTAs per SM at the orders of eps >= 1e-6.
+struct H3Dims {
+  int ldh, ld1, ld2;
+  size_t t2, total;  // doubles
+  __host__ __device__ H3Dims(int Pn, int n2) {
+    ldh = ((Pn * Pn + 3) & ~7) + 4;
+    ld1 = 8 * ((2 * Pn * n2 + 7) / 8) + 4;
+    ld2 = 32 * n2 + 4;
+    t2 = (size_t)Pn * ld2 > (size_t)Pn * ldh + 8 ? (size_t)Pn * ld2 : (size_t)Pn * ldh + 8;
+    total = (size_t)Pn * ld1 + t2;
+  }
+};
+
+template <int KS, int MT>
+__global__ void __launch_bounds__(256, (KS * MT <= 4) ? 2 : 1)
+    k_form3d_h2pw_mma(KP k, const FormTask* __restrict__ tasks, const int* __restrict__ cbeg,
+                      const FormChunk* __restrict__ chunks, const double* __restrict__ hbuf) {
+  const int tk = blockIdx.x, ind = blockIdx.y;
+  const FormTask T = tasks[tk];
+  const int npw = k.npw, n2 = k.n2;
+  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
+  const H3Dims Z(Pn, n2);
+  extern __shared__ double sm[];
+  double* T1 = sm;                       // [Pn][ld1]: (jx, kz, re/im)
+  double* T2 = sm + (size_t)Pn * Z.ld1;  // [Pn][ld2]: (kyl, kz, re/im); H [Pn][ldh] until the y pass
+  double* H = T2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
+  const int cb0 = cbeg[tk], cb1 = cbeg[tk + 1];
+  if (cb1 - cb0 == 1) {
+    // one partial block (leaves of <= 4096 sources): asynchronous copies, all in flight at once
+    const double* src = hbuf + (size_t)chunks[cb0].hoff * k.nd + (size_t)ind * P3;
+    for (int e = threadIdx.x; e < P3; e += blockDim.x) {
+      const int l = e / P2;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(H + e + l * (Z.ldh - P2));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + e) : "memory");
+    }
+  } else {
+    for (int e = threadIdx.x; e < P3; e += blockDim.x) {
+      double v = 0.0;
+      for (int ch = cb0; ch < cb1; ch++) v += hbuf[(size_t)chunks[ch].hoff * k.nd + (size_t)ind * P3 + e];
+      const int l = e / P2;
+      H[e + l * (Z.ldh - P2)] = v;
+    }
+  }
+  // z pass: B fragments of the stored-half table, B[k = j][n = kz]
+  {
+    double hz[MT][2][KS];
+#pragma unroll
+    for (int t = 0; t < MT; t++)
+#pragma unroll
+      for (int par = 0; par < 2; par++)
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int j = 8 * s + 2 * c + par, kz = 8 * t + r;
+          hz[t][par][s] = (j < Pn && kz < n2) ? ((j & 2) ? -k.h2x[j * npw + kz] : k.h2x[j * npw + kz]) : 0.0;
+        }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    const int mtiles = (P2 + 7) / 8;
+    for (int mt = warp; mt < mtiles; mt += 8) {
+      const int m = 8 * mt + r;
+      double a[2][KS];
+#pragma unroll
+      for (int par = 0; par < 2; par++)
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int j = 8 * s + 2 * c + par;
+          a[par][s] = j < Pn ? H[m + j * Z.ldh] : 0.0;
+        }
+      const int jy = m / Pn, jx = m - jy * Pn;
+#pragma unroll
+      for (int t = 0; t < MT; t++) {
+        double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          dmma_884(e0, e1, a[0][s], hz[t][0][s]);
+          dmma_884(o0, o1, a[1][s], hz[t][1][s]);
+        }
+        const int kz = 8 * t + 2 * c;  // the lane's accumulator columns kz, kz + 1
+        if (m < P2) {
+          double* row = T1 + jy * Z.ld1 + 2 * (jx * n2 + kz);
+          if (kz < n2) *reinterpret_cast<double2*>(row) = make_double2(e0, o0);
+          if (kz + 1 < n2) *reinterpret_cast<double2*>(row + 2) = make_double2(e1, o1);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // y and x passes: A fragments of the positive-half table, A[m][k = j]
+  double hn[MT][2][KS];
+#pragma unroll
+  for (int t = 0; t < MT; t++)
+#pragma unroll
+    for (int par = 0; par < 2; par++)
+#pragma unroll
+      for (int s = 0; s < KS; s++) {
+        const int j = 8 * s + 2 * c + par, m = 8 * t + r;
+        hn[t][par][s] =
+            (j < Pn && m < n2) ? ((j & 2) ? -k.h2x[j * npw + n2 + m] : k.h2x[j * npw + n2 + m]) : 0.0;
+      }
+  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  const int nt1 = (2 * Pn * n2 + 7) / 8;
+#pragma unroll
+  for (int t = 0; t < MT; t++) {
+    const int nv = min(8, n2 - 8 * t);  // node rows of tile t
+    // y pass of tile t into T2[jx][(kyl n2 + kz)], kyl = 2 i (ky = n2 + 8t + i) or 2 i + 1 (ky = n2 - 1 - 8t - i)
+    for (int nt = warp; nt < nt1; nt += 8) {
+      const int col = 8 * nt + r;
+      double b[2][KS];
+#pragma unroll
+      for (int par = 0; par < 2; par++)
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int j = 8 * s + 2 * c + par;
+          b[par][s] = j < Pn ? T1[j * Z.ld1 + col] : 0.0;
+        }
+      double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+#pragma unroll
+      for (int s = 0; s < KS; s++) {
+        dmma_884(e0, e1, hn[t][0][s], b[0][s]);
+        dmma_884(o0, o1, hn[t][1][s], b[1][s]);
+      }
+      const int q = 4 * nt + c;  // the lane's complex column (jx, kz)
+      if (r < nv && q < Pn * n2) {
+        const int jx = q / n2, kz = q - jx * n2;
+        double* row = T2 + jx * Z.ld2 + 2 * kz;
+        *reinterpret_cast<double2*>(row + 4 * n2 * r) = make_double2(e0 - o1, e1 + o0);
+        *reinterpret_cast<double2*>(row + 4 * n2 * r + 2 * n2) = make_double2(e0 + o1, e1 - o0);
+      }
+    }
+    __syncthreads();
+    // x pass of tile t: all node rows of kx against T2's columns (kyl, kz)
+    const int nq = 2 * nv * n2, nt2 = (2 * nq + 7) / 8;
+    for (int nt = warp; nt < nt2; nt += 8) {
+      const int col = 8 * nt + r;
+      double b[2][KS];
+#pragma unroll
+      for (int par = 0; par < 2; par++)
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int j = 8 * s + 2 * c + par;
+          b[par][s] = j < Pn ? T2[j * Z.ld2 + col] : 0.0;
+        }
+      double acc[MT][4];
+#pragma unroll
+      for (int u = 0; u < MT; u++) {
+        acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          dmma_884(acc[u][0], acc[u][1], hn[u][0][s], b[0][s]);
+          dmma_884(acc[u][2], acc[u][3], hn[u][1][s], b[1][s]);
+        }
+      }
+      const int q = 4 * nt + c;  // the lane's complex column (kyl, kz)
+      if (q < nq) {
+        const int kyl = q / n2, kz = q - kyl * n2, i = kyl >> 1;
+        const int ky = (kyl & 1) ? n2 - 1 - 8 * t - i : n2 + 8 * t + i;
+        double2* o = out + (size_t)npw * (ky + (size_t)npw * kz);
+#pragma unroll
+        for (int u = 0; u < MT; u++) {
+          const int mx = 8 * u + r;
+          if (mx < n2) {
+            o[n2 + mx] = make_double2(acc[u][0] - acc[u][3], acc[u][1] + acc[u][2]);
+            o[n2 - 1 - mx] = make_double2(acc[u][0] + acc[u][3], acc[u][1] - acc[u][2]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ (c) eval, 2D Taylor in two kernels
 // k_pw2taylor2d: one warp per evaluation leaf converts the leaf's plane-wave
 // expansion L[j2 + n2 j1] into the real Taylor block (g2dpw2local_real_vec,
@@ -3160,9 +3349,34 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         }
         launches++;
       }
-      CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shB));
-      k_form3d_h2pw<<<dim3(D.form_hermite_n, nd), 512, D.form3_shB, st>>>(k, D.form, D.fcbeg, D.fchunks, D.hbuf);
-      launches++;
+      // Hermite -> plane wave per order group: tensor-core passes where the
+      // order and node count fit their fragments and shared memory
+      for (const OrderGroup& G : D.form_groups) {
+        const int Pn = G.p + 1, ks = (Pn + 7) / 8, mt = (P.npw / 2 + 7) / 8;
+        const size_t sh = H3Dims(Pn, P.npw / 2).total * 8;
+        const dim3 hg(G.end - G.beg, nd);
+        const FormTask* ft = D.form + G.beg;
+        const int* cb = D.fcbeg + G.beg;
+        if (ks <= 4 && mt <= 4 && sh <= 227 * 1024) {
+          switch (4 * (ks - 1) + mt - 1) {
+#define H2PW_CASE(KS_, MT_)                                                                        \
+  case 4 * (KS_ - 1) + MT_ - 1:                                                                    \
+    CK(cudaFuncSetAttribute(k_form3d_h2pw_mma<KS_, MT_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    k_form3d_h2pw_mma<KS_, MT_><<<hg, 256, sh, st>>>(k, ft, cb, D.fchunks, D.hbuf);                \
+    break;
+            H2PW_CASE(1, 1) H2PW_CASE(1, 2) H2PW_CASE(1, 3) H2PW_CASE(1, 4)
+            H2PW_CASE(2, 1) H2PW_CASE(2, 2) H2PW_CASE(2, 3) H2PW_CASE(2, 4)
+            H2PW_CASE(3, 1) H2PW_CASE(3, 2) H2PW_CASE(3, 3) H2PW_CASE(3, 4)
+            H2PW_CASE(4, 1) H2PW_CASE(4, 2) H2PW_CASE(4, 3) H2PW_CASE(4, 4)
+#undef H2PW_CASE
+            default: return cudaErrorNotSupported;
+          }
+        } else {
+          CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shB));
+          k_form3d_h2pw<<<hg, 512, D.form3_shB, st>>>(k, ft, cb, D.fchunks, D.hbuf);
+        }
+        launches++;
+      }
     } else if (P.dim == 3 && D.form_hermite_n > 0) {
       int Pn = D.form_pmax + 1;
       size_t sh = ((size_t)Pn * Pn * Pn + 3 * FORM_CH * Pn) * 8;
