@@ -1125,69 +1125,116 @@ __global__ void __launch_bounds__(512) k_form3d_h2pw(KP k, const FormTask* __res
 //           -> the slot, kx = n2 + m and n2 - 1 - m          (M = n2, N = 2 npw n2)
 // The y and x passes run per 8-row tile t of the node half: the y pass of tile
 // t fills T2 with its 16 ky and the x pass of tile t drains it, so T2 holds 16
-// ky instead of npw and the Hermite block H shares its space.  The node tables
-// are register fragments; rows j >= P are zero fragments, not loads.  Row
-// strides are 4 (mod 8) doubles, so the rows two apart that one fragment reads
-// fall in opposite halves of the banks.  One CTA of 8 warps per leaf and
-// density; two CTAs per SM at the orders of eps >= 1e-6.
+// ky instead of npw.  The node tables are register fragments, loaded once per
+// CTA (a launch covers one order); rows j >= P are zero fragments, not loads.
+// Row strides are 4 (mod 8) doubles, so the rows two apart that one fragment
+// reads fall in opposite halves of the banks.  Persistent CTAs of 8 warps, two
+// per SM at the orders of eps >= 1e-6, stride over the leaves of the order
+// group; where shared memory allows, the next leaf's Hermite block is copied
+// into its own buffer with cp.async while the y and x passes of the current
+// leaf run (else it is staged over T2 at the leaf's start).  Each warp takes
+// two N tiles per step (independent accumulator chains in flight).
 struct H3Dims {
   int ldh, ld1, ld2;
-  size_t t2, total;  // doubles
+  size_t total_pf, total_ov;  // doubles: H in its own buffer (prefetched) / H over T2
   __host__ __device__ H3Dims(int Pn, int n2) {
     ldh = ((Pn * Pn + 3) & ~7) + 4;
     ld1 = 8 * ((2 * Pn * n2 + 7) / 8) + 4;
     ld2 = 32 * n2 + 4;
-    t2 = (size_t)Pn * ld2 > (size_t)Pn * ldh + 8 ? (size_t)Pn * ld2 : (size_t)Pn * ldh + 8;
-    total = (size_t)Pn * ld1 + t2;
+    total_pf = (size_t)Pn * (ld1 + ld2 + ldh) + 8;
+    const size_t t2 = (size_t)Pn * ld2, hb = (size_t)Pn * ldh + 8;
+    total_ov = (size_t)Pn * ld1 + (t2 > hb ? t2 : hb);
   }
 };
 
+// Stage the Hermite block of task tk (the sum of its chunk partials) into H
+// with row stride ldh, row l of P^2 doubles per warp: a single partial block
+// by asynchronous copies (16 bytes where the rows allow; waited for by the
+// caller), several by plain loads in chunk order.
+// The task's chunk range [cb0, cb1) and its first chunk's offset hoff0 are
+// loaded by the caller ahead of time.
+__device__ __forceinline__ void h2pw_stage(const KP& k, int ind, int Pn, int ldh, int cb0, int cb1, long long hoff0,
+                                           const FormChunk* __restrict__ chunks, const double* __restrict__ hbuf,
+                                           double* H) {
+  const int P2 = Pn * Pn, P3 = P2 * Pn, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (cb1 - cb0 == 1) {
+    const double* src = hbuf + (size_t)hoff0 * k.nd + (size_t)ind * P3;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(H);
+    if (((P2 | (int)(reinterpret_cast<size_t>(src) >> 3)) & 1) == 0) {
+      for (int l = threadIdx.x >> 5; l < Pn; l += nw)
+        for (int m = 2 * lane; m < P2; m += 64)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 8u * (unsigned)(l * ldh + m)),
+                       "l"(src + l * P2 + m) : "memory");
+    } else {
+      for (int l = threadIdx.x >> 5; l < Pn; l += nw)
+        for (int m = lane; m < P2; m += 32)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst + 8u * (unsigned)(l * ldh + m)),
+                       "l"(src + l * P2 + m) : "memory");
+    }
+  } else {
+    for (int l = threadIdx.x >> 5; l < Pn; l += nw)
+      for (int m = lane; m < P2; m += 32) {
+        double v = 0.0;
+        for (int ch = cb0; ch < cb1; ch++) v += hbuf[(size_t)chunks[ch].hoff * k.nd + (size_t)ind * P3 + l * P2 + m];
+        H[l * ldh + m] = v;
+      }
+  }
+}
+
+// q / d for 0 <= q < 1115 and 1 <= d <= 64, with mg = ceil(2^16 / d)
+__device__ __forceinline__ int div16(int q, int mg) { return (q * mg) >> 16; }
+
 template <int KS, int MT>
 __global__ void __launch_bounds__(256, (KS * MT <= 4) ? 2 : 1)
-    k_form3d_h2pw_mma(KP k, const FormTask* __restrict__ tasks, const int* __restrict__ cbeg,
-                      const FormChunk* __restrict__ chunks, const double* __restrict__ hbuf) {
-  const int tk = blockIdx.x, ind = blockIdx.y;
-  const FormTask T = tasks[tk];
+    k_form3d_h2pw_mma(KP k, const FormTask* __restrict__ tasks, int ntask, const int* __restrict__ cbeg,
+                      const FormChunk* __restrict__ chunks, const double* __restrict__ hbuf, bool pf) {
+  const int ind = blockIdx.y;
   const int npw = k.npw, n2 = k.n2;
-  const int Pn = T.p + 1, P2 = Pn * Pn, P3 = P2 * Pn;
+  const int Pn = tasks[0].p + 1, P2 = Pn * Pn;
+  const int mgP = (65536 + Pn - 1) / Pn, mgN = (65536 + n2 - 1) / n2;  // div16 factors
   const H3Dims Z(Pn, n2);
   extern __shared__ double sm[];
   double* T1 = sm;                       // [Pn][ld1]: (jx, kz, re/im)
-  double* T2 = sm + (size_t)Pn * Z.ld1;  // [Pn][ld2]: (kyl, kz, re/im); H [Pn][ldh] until the y pass
-  double* H = T2;
+  double* T2 = T1 + (size_t)Pn * Z.ld1;  // [Pn][ld2]: (kyl, kz, re/im)
+  // H [Pn][ldh] (+ 8: the last M tile's rows past P^2): its own buffer when
+  // pf (the next leaf's block is prefetched), else over T2 (staged per leaf)
+  double* H = pf ? T2 + (size_t)Pn * Z.ld2 : T2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
-  const int cb0 = cbeg[tk], cb1 = cbeg[tk + 1];
-  if (cb1 - cb0 == 1) {
-    // one partial block (leaves of <= 4096 sources): asynchronous copies, all in flight at once
-    const double* src = hbuf + (size_t)chunks[cb0].hoff * k.nd + (size_t)ind * P3;
-    for (int e = threadIdx.x; e < P3; e += blockDim.x) {
-      const int l = e / P2;
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(H + e + l * (Z.ldh - P2));
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + e) : "memory");
+  int tk = blockIdx.x;
+  if (tk >= ntask) return;
+  // chunk range and first partial block of the current task
+  int cb0 = cbeg[tk], cb1 = cbeg[tk + 1];
+  long long hoff0 = chunks[cb0].hoff;
+  if (pf) h2pw_stage(k, ind, Pn, Z.ldh, cb0, cb1, hoff0, chunks, hbuf, H);
+  // B fragments of the stored-half table for the z pass (B[k = j][n = kz]) and
+  // A fragments of the positive-half table for the y and x passes (A[m][k = j])
+  double hz[MT][2][KS], hn[MT][2][KS];
+#pragma unroll
+  for (int t = 0; t < MT; t++)
+#pragma unroll
+    for (int par = 0; par < 2; par++)
+#pragma unroll
+      for (int s = 0; s < KS; s++) {
+        const int j = 8 * s + 2 * c + par, m = 8 * t + r;
+        const bool ok = j < Pn && m < n2;
+        const double sg = (j & 2) ? -1.0 : 1.0;
+        hz[t][par][s] = ok ? sg * k.h2x[j * npw + m] : 0.0;
+        hn[t][par][s] = ok ? sg * k.h2x[j * npw + n2 + m] : 0.0;
+      }
+  const int mtiles = (P2 + 7) / 8, nt1 = (2 * Pn * n2 + 7) / 8;
+  for (; tk < ntask; tk += gridDim.x) {
+    if (!pf) h2pw_stage(k, ind, Pn, Z.ldh, cb0, cb1, hoff0, chunks, hbuf, H);  // T2 is free: the last pass ended in a barrier
+    // the next task's chunk range and first block offset, loaded while this one runs
+    const int tn = tk + gridDim.x;
+    if (tn < ntask) {
+      cb0 = cbeg[tn];
+      cb1 = cbeg[tn + 1];
+      hoff0 = chunks[cb0].hoff;
     }
-  } else {
-    for (int e = threadIdx.x; e < P3; e += blockDim.x) {
-      double v = 0.0;
-      for (int ch = cb0; ch < cb1; ch++) v += hbuf[(size_t)chunks[ch].hoff * k.nd + (size_t)ind * P3 + e];
-      const int l = e / P2;
-      H[e + l * (Z.ldh - P2)] = v;
-    }
-  }
-  // z pass: B fragments of the stored-half table, B[k = j][n = kz]
-  {
-    double hz[MT][2][KS];
-#pragma unroll
-    for (int t = 0; t < MT; t++)
-#pragma unroll
-      for (int par = 0; par < 2; par++)
-#pragma unroll
-        for (int s = 0; s < KS; s++) {
-          const int j = 8 * s + 2 * c + par, kz = 8 * t + r;
-          hz[t][par][s] = (j < Pn && kz < n2) ? ((j & 2) ? -k.h2x[j * npw + kz] : k.h2x[j * npw + kz]) : 0.0;
-        }
+    const int slot = tasks[tk].slot;
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
-    const int mtiles = (P2 + 7) / 8;
+    // z pass: H -> T1
     for (int mt = warp; mt < mtiles; mt += 8) {
       const int m = 8 * mt + r;
       double a[2][KS];
@@ -1198,7 +1245,7 @@ __global__ void __launch_bounds__(256, (KS * MT <= 4) ? 2 : 1)
           const int j = 8 * s + 2 * c + par;
           a[par][s] = j < Pn ? H[m + j * Z.ldh] : 0.0;
         }
-      const int jy = m / Pn, jx = m - jy * Pn;
+      const int jy = div16(m, mgP), jx = m - jy * Pn;
 #pragma unroll
       for (int t = 0; t < MT; t++) {
         double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
@@ -1215,89 +1262,95 @@ __global__ void __launch_bounds__(256, (KS * MT <= 4) ? 2 : 1)
         }
       }
     }
-  }
-  __syncthreads();
-  // y and x passes: A fragments of the positive-half table, A[m][k = j]
-  double hn[MT][2][KS];
-#pragma unroll
-  for (int t = 0; t < MT; t++)
-#pragma unroll
-    for (int par = 0; par < 2; par++)
-#pragma unroll
-      for (int s = 0; s < KS; s++) {
-        const int j = 8 * s + 2 * c + par, m = 8 * t + r;
-        hn[t][par][s] =
-            (j < Pn && m < n2) ? ((j & 2) ? -k.h2x[j * npw + n2 + m] : k.h2x[j * npw + n2 + m]) : 0.0;
-      }
-  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  const int nt1 = (2 * Pn * n2 + 7) / 8;
-#pragma unroll
-  for (int t = 0; t < MT; t++) {
-    const int nv = min(8, n2 - 8 * t);  // node rows of tile t
-    // y pass of tile t into T2[jx][(kyl n2 + kz)], kyl = 2 i (ky = n2 + 8t + i) or 2 i + 1 (ky = n2 - 1 - 8t - i)
-    for (int nt = warp; nt < nt1; nt += 8) {
-      const int col = 8 * nt + r;
-      double b[2][KS];
-#pragma unroll
-      for (int par = 0; par < 2; par++)
-#pragma unroll
-        for (int s = 0; s < KS; s++) {
-          const int j = 8 * s + 2 * c + par;
-          b[par][s] = j < Pn ? T1[j * Z.ld1 + col] : 0.0;
-        }
-      double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
-#pragma unroll
-      for (int s = 0; s < KS; s++) {
-        dmma_884(e0, e1, hn[t][0][s], b[0][s]);
-        dmma_884(o0, o1, hn[t][1][s], b[1][s]);
-      }
-      const int q = 4 * nt + c;  // the lane's complex column (jx, kz)
-      if (r < nv && q < Pn * n2) {
-        const int jx = q / n2, kz = q - jx * n2;
-        double* row = T2 + jx * Z.ld2 + 2 * kz;
-        *reinterpret_cast<double2*>(row + 4 * n2 * r) = make_double2(e0 - o1, e1 + o0);
-        *reinterpret_cast<double2*>(row + 4 * n2 * r + 2 * n2) = make_double2(e0 + o1, e1 - o0);
-      }
-    }
     __syncthreads();
-    // x pass of tile t: all node rows of kx against T2's columns (kyl, kz)
-    const int nq = 2 * nv * n2, nt2 = (2 * nq + 7) / 8;
-    for (int nt = warp; nt < nt2; nt += 8) {
-      const int col = 8 * nt + r;
-      double b[2][KS];
+    // the next leaf's Hermite block lands while this leaf's y and x passes run
+    if (pf && tn < ntask) h2pw_stage(k, ind, Pn, Z.ldh, cb0, cb1, hoff0, chunks, hbuf, H);
+    double2* out = k.mp + ((size_t)slot * k.nd + ind) * k.nexp;
 #pragma unroll
-      for (int par = 0; par < 2; par++)
+    for (int t = 0; t < MT; t++) {
+      const int nv = min(8, n2 - 8 * t);  // node rows of tile t
+      // y pass of tile t into T2[jx][(kyl n2 + kz)], kyl = 2 i (ky = n2 + 8t + i) or 2 i + 1 (ky = n2 - 1 - 8t - i)
+      for (int nt0 = warp; nt0 < nt1; nt0 += 16) {
+        double b[2][2][KS], acc[2][4];
 #pragma unroll
-        for (int s = 0; s < KS; s++) {
-          const int j = 8 * s + 2 * c + par;
-          b[par][s] = j < Pn ? T2[j * Z.ld2 + col] : 0.0;
+        for (int h = 0; h < 2; h++) {
+          const int col = 8 * (nt0 + 8 * h) + r;
+          const bool ok = nt0 + 8 * h < nt1;
+#pragma unroll
+          for (int par = 0; par < 2; par++)
+#pragma unroll
+            for (int s = 0; s < KS; s++) {
+              const int j = 8 * s + 2 * c + par;
+              b[h][par][s] = (ok && j < Pn) ? T1[j * Z.ld1 + col] : 0.0;
+            }
+          acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0;
         }
-      double acc[MT][4];
 #pragma unroll
-      for (int u = 0; u < MT; u++) {
-        acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+        for (int s = 0; s < KS; s++)
 #pragma unroll
-        for (int s = 0; s < KS; s++) {
-          dmma_884(acc[u][0], acc[u][1], hn[u][0][s], b[0][s]);
-          dmma_884(acc[u][2], acc[u][3], hn[u][1][s], b[1][s]);
-        }
-      }
-      const int q = 4 * nt + c;  // the lane's complex column (kyl, kz)
-      if (q < nq) {
-        const int kyl = q / n2, kz = q - kyl * n2, i = kyl >> 1;
-        const int ky = (kyl & 1) ? n2 - 1 - 8 * t - i : n2 + 8 * t + i;
-        double2* o = out + (size_t)npw * (ky + (size_t)npw * kz);
+          for (int h = 0; h < 2; h++) {
+            dmma_884(acc[h][0], acc[h][1], hn[t][0][s], b[h][0][s]);
+            dmma_884(acc[h][2], acc[h][3], hn[t][1][s], b[h][1][s]);
+          }
 #pragma unroll
-        for (int u = 0; u < MT; u++) {
-          const int mx = 8 * u + r;
-          if (mx < n2) {
-            o[n2 + mx] = make_double2(acc[u][0] - acc[u][3], acc[u][1] + acc[u][2]);
-            o[n2 - 1 - mx] = make_double2(acc[u][0] + acc[u][3], acc[u][1] - acc[u][2]);
+        for (int h = 0; h < 2; h++) {
+          const int q = 4 * (nt0 + 8 * h) + c;  // the lane's complex column (jx, kz)
+          if (r < nv && q < Pn * n2) {
+            const int jx = div16(q, mgN), kz = q - jx * n2;
+            double* row = T2 + jx * Z.ld2 + 2 * kz + 4 * n2 * r;
+            *reinterpret_cast<double2*>(row) = make_double2(acc[h][0] - acc[h][3], acc[h][1] + acc[h][2]);
+            *reinterpret_cast<double2*>(row + 2 * n2) = make_double2(acc[h][0] + acc[h][3], acc[h][1] - acc[h][2]);
           }
         }
       }
+      __syncthreads();
+      // x pass of tile t: all node rows of kx against T2's columns (kyl, kz)
+      const int nq = 2 * nv * n2, nt2 = (2 * nq + 7) / 8;
+      for (int nt0 = warp; nt0 < nt2; nt0 += 16) {
+        double b[2][2][KS], acc[2][MT][4];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int col = 8 * (nt0 + 8 * h) + r;
+          const bool ok = nt0 + 8 * h < nt2;
+#pragma unroll
+          for (int par = 0; par < 2; par++)
+#pragma unroll
+            for (int s = 0; s < KS; s++) {
+              const int j = 8 * s + 2 * c + par;
+              b[h][par][s] = (ok && j < Pn) ? T2[j * Z.ld2 + col] : 0.0;
+            }
+#pragma unroll
+          for (int u = 0; u < MT; u++) acc[h][u][0] = acc[h][u][1] = acc[h][u][2] = acc[h][u][3] = 0.0;
+        }
+#pragma unroll
+        for (int s = 0; s < KS; s++)
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int u = 0; u < MT; u++) {
+              dmma_884(acc[h][u][0], acc[h][u][1], hn[u][0][s], b[h][0][s]);
+              dmma_884(acc[h][u][2], acc[h][u][3], hn[u][1][s], b[h][1][s]);
+            }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int q = 4 * (nt0 + 8 * h) + c;  // the lane's complex column (kyl, kz)
+          if (q < nq) {
+            const int kyl = div16(q, mgN), kz = q - kyl * n2, i = kyl >> 1;
+            const int ky = (kyl & 1) ? n2 - 1 - 8 * t - i : n2 + 8 * t + i;
+            double2* o = out + npw * (ky + npw * kz);
+#pragma unroll
+            for (int u = 0; u < MT; u++) {
+              const int mx = 8 * u + r;
+              if (mx < n2) {
+                o[n2 + mx] = make_double2(acc[h][u][0] - acc[h][u][3], acc[h][u][1] + acc[h][u][2]);
+                o[n2 - 1 - mx] = make_double2(acc[h][u][0] + acc[h][u][3], acc[h][u][1] - acc[h][u][2]);
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -3353,16 +3406,21 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       // order and node count fit their fragments and shared memory
       for (const OrderGroup& G : D.form_groups) {
         const int Pn = G.p + 1, ks = (Pn + 7) / 8, mt = (P.npw / 2 + 7) / 8;
-        const size_t sh = H3Dims(Pn, P.npw / 2).total * 8;
-        const dim3 hg(G.end - G.beg, nd);
+        const H3Dims Z3(Pn, P.npw / 2);
+        const bool pf = Z3.total_pf * 8 <= 227 * 1024;
+        const size_t sh = (pf ? Z3.total_pf : Z3.total_ov) * 8;
+        const int ntk = G.end - G.beg;
+        const dim3 hg(ntk, nd);
         const FormTask* ft = D.form + G.beg;
         const int* cb = D.fcbeg + G.beg;
+        // persistent CTAs: as many as fit on the SMs at once
+        const dim3 pg(std::min(ntk, D.sm_count * (ks * mt <= 4 && 2 * (sh + 1024) <= 228 * 1024 ? 2 : 1)), nd);
         if (ks <= 4 && mt <= 4 && sh <= 227 * 1024) {
           switch (4 * (ks - 1) + mt - 1) {
 #define H2PW_CASE(KS_, MT_)                                                                        \
   case 4 * (KS_ - 1) + MT_ - 1:                                                                    \
     CK(cudaFuncSetAttribute(k_form3d_h2pw_mma<KS_, MT_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_form3d_h2pw_mma<KS_, MT_><<<hg, 256, sh, st>>>(k, ft, cb, D.fchunks, D.hbuf);                \
+    k_form3d_h2pw_mma<KS_, MT_><<<pg, 256, sh, st>>>(k, ft, ntk, cb, D.fchunks, D.hbuf, pf);       \
     break;
             H2PW_CASE(1, 1) H2PW_CASE(1, 2) H2PW_CASE(1, 3) H2PW_CASE(1, 4)
             H2PW_CASE(2, 1) H2PW_CASE(2, 2) H2PW_CASE(2, 3) H2PW_CASE(2, 4)
