@@ -1771,6 +1771,188 @@ __global__ void __launch_bounds__(128) k_pw2taylor3d(KP k, const ConvTask* __res
   }
 }
 
+// k_pw2taylor3d_mma: the conversion of k_pw2taylor3d for orders P <= 16 with
+// the mirror symmetry of the node set used in both full dimensions and the
+// node tables as register fragments.  With the signed table
+// tx[a][m] = x2l[a][m] (-1)^(a/2) over the first half m < n2 and mirror node
+// mb = npw - 1 - m (x2l[a][mb] = (-1)^a x2l[a][m]), a sum over all nodes is
+//   i^a sum_m x2l[a][m] L[m] = tx[a][.] (L[m] + L[mb])        (a even)
+//                            = i tx[a][.] (L[m] - L[mb])      (a odd),
+// so every pass is two real products of depth n2 (KS k-steps of 4):
+//   x pass  S1[m1][m2][a] from the staged slices of L     (M = a, N = (m1, m2, re/im))
+//   y pass  S2[m1][b][a]  from S1, same table in b         (M = b, N = (m1, a, re/im))
+//   z pass  lo[c][b][a] += 2 Re(i^c tx[c][m1] S2[m1][b][a]): even c against
+//           Re S2, odd c against -Im S2, K = the four slices m1 of a group
+// The leaf is taken four z slices (one z k-step) at a time: the slices are
+// copied into shared memory with cp.async (the next group's copy overlaps
+// the y and z passes of this one), and the z accumulators stay in registers
+// across the groups (each warp owns up to four of the ceil(P^2 / 8) column
+// tiles).  Row strides: staged slices 8 (mod 16) doubles (the fragment's
+// re/im pairs of four rows are conflict-free), S1 and S2 4 (mod 8).
+// Persistent CTAs of 8 warps, two per SM, over the leaves of one order.
+struct C3Dims {
+  int ldL, ld1, ld2;
+  size_t total;  // doubles
+  __host__ __device__ C3Dims(int Pn, int npw) {
+    ldL = ((2 * npw + 7) & ~15) + 8;
+    ld1 = 8 * Pn + 4;
+    ld2 = 8 * ((Pn * Pn + 7) / 8) + 4;
+    total = (size_t)4 * npw * ldL + (size_t)npw * ld1 + (size_t)8 * ld2;
+  }
+};
+
+template <int KS>
+__global__ void __launch_bounds__(256, 2) k_pw2taylor3d_mma(KP k, const ConvTask* __restrict__ tasks, int ntask,
+                                                            double* __restrict__ lo_all) {
+  constexpr int NTW = 4;  // z-pass column tiles per warp (ceil(16^2 / 8) / 8)
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2;
+  const int Pn = tasks[0].p + 1, E = (Pn + 1) & ~1, P2 = Pn * Pn;
+  const int mgN = (65536 + npw - 1) / npw, mgP = (65536 + Pn - 1) / Pn;  // div16 factors
+  const C3Dims Z(Pn, npw);
+  extern __shared__ double sm[];
+  double* Lb = sm;                                  // [4 m1][npw m2][ldL]: (m3, re/im)
+  double* S1 = Lb + (size_t)4 * npw * Z.ldL;        // [npw m2][ld1]: (m1, a, re/im)
+  double* S2r = S1 + (size_t)npw * Z.ld1;           // [4 m1][ld2]: (b, a)
+  double* S2i = S2r + 4 * Z.ld2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
+  int tk = blockIdx.x;
+  if (tk >= ntask) return;
+  // A fragments: tx[par][s] = table row 2 r + par, node 4 s + c
+  double tx[2][KS];
+#pragma unroll
+  for (int par = 0; par < 2; par++)
+#pragma unroll
+    for (int s = 0; s < KS; s++) {
+      const int a = 2 * r + par, m = 4 * s + c;
+      tx[par][s] = (a < Pn && m < n2) ? (((a >> 1) & 1) ? -k.x2l[a * npw + m] : k.x2l[a * npw + m]) : 0.0;
+    }
+  // copy the slices 4 g .. 4 g + 3 of the expansion in the given slot (rows of npw complex)
+  auto stage = [&](int slot, int g) {
+    const double* L = reinterpret_cast<const double*>(k.loc + ((size_t)slot * k.nd + ind) * k.nexp) +
+                      (size_t)8 * g * npw * npw;
+    const int rows = min(4, n2 - 4 * g) * npw;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(Lb);
+    for (int row = warp; row < rows; row += 8)
+      for (int u = lane; u < npw; u += 32)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 8u * (unsigned)(row * Z.ldL + 2 * u)),
+                     "l"(L + (size_t)row * 2 * npw + 2 * u) : "memory");
+  };
+  int slot = tasks[tk].slot;
+  stage(slot, 0);
+  double acc[NTW][2][2];
+#pragma unroll
+  for (int i = 0; i < NTW; i++) acc[i][0][0] = acc[i][0][1] = acc[i][1][0] = acc[i][1][1] = 0.0;
+  const int ntZ = (P2 + 7) / 8;
+  for (; tk < ntask; tk += gridDim.x) {
+    const int tn = tk + gridDim.x;
+    const int nslot = tn < ntask ? tasks[tn].slot : 0;
+    const long long off = tasks[tk].off;
+    for (int g = 0; g < KS; g++) {
+      const int ns = min(4, n2 - 4 * g);
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      __syncthreads();
+      // x pass: columns (m1, m2, re/im) of the staged slices
+      const int ntX = (ns * npw * 2 + 7) / 8;
+      for (int nt = warp; nt < ntX; nt += 8) {
+        const int col = 8 * nt + r;
+        const double* bp = Lb + (col >> 1) * Z.ldL + (col & 1);
+        double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int m = 4 * s + c;
+          double v1 = 0.0, v2 = 0.0;
+          if (m < n2) {
+            v1 = bp[2 * m];
+            v2 = bp[2 * (npw - 1 - m)];
+          }
+          dmma_884(e0, e1, tx[0][s], v1 + v2);
+          dmma_884(o0, o1, tx[1][s], v1 - v2);
+        }
+        const int q = 4 * nt + c;  // the lane's complex column (m1, m2)
+        if (q < ns * npw) {
+          const int m1 = div16(q, mgN), m2 = q - m1 * npw;
+          double* o = S1 + m2 * Z.ld1 + 2 * (m1 * Pn + 2 * r);
+          if (2 * r < Pn) *reinterpret_cast<double2*>(o) = make_double2(e0, e1);
+          if (2 * r + 1 < Pn) *reinterpret_cast<double2*>(o + 2) = make_double2(-o1, o0);
+        }
+      }
+      __syncthreads();
+      // the slices are consumed: copy the next group's (or the next leaf's first)
+      if (g + 1 < KS) stage(slot, g + 1);
+      else if (tn < ntask) stage(nslot, 0);
+      // y pass: columns (m1, a, re/im)
+      const int ntY = (ns * Pn * 2 + 7) / 8;
+      for (int nt = warp; nt < ntY; nt += 8) {
+        const int col = 8 * nt + r;
+        double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int m = 4 * s + c;
+          double v1 = 0.0, v2 = 0.0;
+          if (m < n2) {
+            v1 = S1[m * Z.ld1 + col];
+            v2 = S1[(npw - 1 - m) * Z.ld1 + col];
+          }
+          dmma_884(e0, e1, tx[0][s], v1 + v2);
+          dmma_884(o0, o1, tx[1][s], v1 - v2);
+        }
+        const int q = 4 * nt + c;  // the lane's complex column (m1, a)
+        if (q < ns * Pn) {
+          const int m1 = div16(q, mgP), a = q - m1 * Pn;
+          const int o = m1 * Z.ld2 + 2 * r * Pn + a;
+          if (2 * r < Pn) {
+            S2r[o] = e0;
+            S2i[o] = e1;
+          }
+          if (2 * r + 1 < Pn) {
+            S2r[o + Pn] = -o1;
+            S2i[o + Pn] = o0;
+          }
+        }
+      }
+      __syncthreads();
+      // z pass: k-step g of the accumulators, rows c = 2 r + par, columns (b, a)
+      double te = tx[0][0], to = tx[1][0];
+#pragma unroll
+      for (int s = 1; s < KS; s++)
+        if (s == g) {
+          te = tx[0][s];
+          to = tx[1][s];
+        }
+#pragma unroll
+      for (int i = 0; i < NTW; i++) {
+        const int nt = warp + 8 * i;
+        if (nt < ntZ) {
+          const double br = c < ns ? S2r[c * Z.ld2 + 8 * nt + r] : 0.0;
+          const double bi = c < ns ? S2i[c * Z.ld2 + 8 * nt + r] : 0.0;
+          dmma_884(acc[i][0][0], acc[i][0][1], te, br);
+          dmma_884(acc[i][1][0], acc[i][1][1], to, bi);
+        }
+      }
+    }
+    // lo[c][b][a] = 2 acc (even c), -2 acc (odd c); rows of E doubles
+    double* out = lo_all + off + (size_t)ind * P2 * E;
+#pragma unroll
+    for (int i = 0; i < NTW; i++) {
+      const int nt = warp + 8 * i;
+#pragma unroll
+      for (int ii = 0; ii < 2; ii++) {
+        const int q = 8 * nt + 2 * c + ii;
+        if (nt < ntZ && q < P2) {
+          const int b = div16(q, mgP), a = q - b * Pn;
+          if (2 * r < Pn) out[((2 * r) * Pn + b) * E + a] = 2.0 * acc[i][0][ii];
+          if (2 * r + 1 < Pn) out[((2 * r + 1) * Pn + b) * E + a] = -2.0 * acc[i][1][ii];
+        }
+        acc[i][0][ii] = acc[i][1][ii] = 0.0;
+      }
+    }
+    if (E > Pn)  // the padding column of every row
+      for (int e = threadIdx.x; e < P2; e += blockDim.x) out[(size_t)e * E + Pn] = 0.0;
+    slot = nslot;
+  }
+}
+
 // k_eval3d_horner: one CTA (128 threads) per chunk of <= 256 points of an
 // evaluation leaf; the leaf's Taylor block lo[c][b][a] (rows of E = 2 NP2)
 // is staged in shared memory and each thread evaluates two points by Horner
@@ -3550,6 +3732,24 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const int nw = 4;
         const size_t sh = conv3_smem_bytes(Pn, P.npw, nw);
         const dim3 cg(std::min(nt, D.conv3_ctas), nd);
+        const int n2 = P.npw / 2, ksm = (n2 + 3) / 4;
+        const size_t shm = C3Dims(Pn, P.npw).total * 8;
+        if (Pn <= 16 && ksm <= 8 && shm <= 227 * 1024) {
+          const dim3 pg(std::min(nt, D.sm_count * (2 * (shm + 1024) <= 228 * 1024 ? 2 : 1)), nd);
+          switch (ksm) {
+#define CONV3M_CASE(N)                                                                            \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_pw2taylor3d_mma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm)); \
+    k_pw2taylor3d_mma<N><<<pg, 256, shm, st>>>(k, D.conv + G.beg, nt, D.lo);                      \
+    break;
+            CONV3M_CASE(1) CONV3M_CASE(2) CONV3M_CASE(3) CONV3M_CASE(4)
+            CONV3M_CASE(5) CONV3M_CASE(6) CONV3M_CASE(7) CONV3M_CASE(8)
+#undef CONV3M_CASE
+            default: return cudaErrorNotSupported;
+          }
+          launches++;
+          continue;
+        }
         switch ((P.npw + 3) / 4) {
 #define CONV3_CASE(N)                                                                             \
   case N:                                                                                         \
