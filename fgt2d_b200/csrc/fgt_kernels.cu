@@ -2199,13 +2199,33 @@ __global__ void k_m2l(KP k, const M2LTask* __restrict__ tasks, const M2LNbr* __r
     k.loc[(size_t)T.loc * per + e] = a;
   }
 }
+// One CTA per (task, block of SHU * 256 coefficients), every density in
+// turn; a thread's SHU loads of the parent and of the table are issued
+// before the first product.
+constexpr int SHU = 4;
 // split: child = parent * conj(W), W the merge factor of that child
-__global__ void k_split(KP k, const ShiftTask* __restrict__ tasks) {
+__global__ void __launch_bounds__(256) k_split(KP k, const ShiftTask* __restrict__ tasks) {
   const ShiftTask S = tasks[blockIdx.x];
   const size_t per = (size_t)k.nd * k.nexp;
-  for (size_t e = (size_t)blockIdx.y * blockDim.x + threadIdx.x; e < per; e += (size_t)gridDim.y * blockDim.x) {
-    const int ee = (int)(e % k.nexp);
-    k.loc[(size_t)S.dst * per + e] = cmulc(k.loc[(size_t)S.src * per + e], k.wms[(size_t)S.table * k.nexp + ee]);
+  const int e0 = blockIdx.y * 256 * SHU + threadIdx.x;
+  const double2* w = k.wms + (size_t)S.table * k.nexp;
+  for (int ind = 0; ind < k.nd; ind++) {
+    const double2* src = k.loc + (size_t)S.src * per + (size_t)ind * k.nexp;
+    double2* dst = k.loc + (size_t)S.dst * per + (size_t)ind * k.nexp;
+    double2 a[SHU], b[SHU];
+#pragma unroll
+    for (int u = 0; u < SHU; u++) {
+      const int e = e0 + 256 * u;
+      if (e < k.nexp) {
+        a[u] = src[e];
+        b[u] = __ldg(w + e);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SHU; u++) {
+      const int e = e0 + 256 * u;
+      if (e < k.nexp) dst[e] = cmulc(a[u], b[u]);
+    }
   }
 }
 
@@ -3639,7 +3659,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     }
     mark(2);
     // (b) merge, bottom-up
-    int echunks = (int)std::min<long long>(65535, ((long long)nd * P.nexp + 255) / 256);
+    const int echunks = (int)std::min<long long>(65535, ((long long)nd * P.nexp + 255) / 256);
+    const int schunks = (P.nexp + 256 * SHU - 1) / (256 * SHU);  // k_split: every density per block
     for (int l = P.nlevels - 1; l >= P.nlevstart; l--) {
       int ng = D.merge_end[l] - D.merge_beg[l];
       if (ng <= 0) continue;
@@ -3655,7 +3676,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     for (int l = P.nlevstart; l <= P.nlevels - 1; l++) {
       int nsp = D.split_end[l] - D.split_beg[l];
       if (nsp <= 0) continue;
-      k_split<<<dim3(nsp, echunks), 256, 0, st>>>(k, D.split + D.split_beg[l]);
+      k_split<<<dim3(nsp, schunks), 256, 0, st>>>(k, D.split + D.split_beg[l]);
       launches++;
     }
     mark(5);
