@@ -140,23 +140,45 @@ static void build_tasks(HostPlan& H) {
       H.merge_end[l] = (int)H.merge.size();
     }
     // (b) mp -> loc at the cut level
+    // in box order, the list's boxes with a multipole in list order; tasks
+    // and neighbours counted per box, placed by prefix sums, filled in parallel
     double xmin = npl >= 0 ? t.boxsize[npl] : 1.0;
-    for (int b = t.lfirst[nls]; b <= t.llast[nls]; b++) {
-      if (H.loc_slot[b] < 0) continue;
-      M2LTask mt{H.loc_slot[b], H.mp_slot[b], (int)H.m2l_nbr.size(), 0};
-      for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) {
-        int j = L.pw[k];
-        if (H.mp_slot[j] < 0) continue;
-        int s = 0, mul = 1;
-        for (int d = 0; d < D; d++) {
-          int o = (int)std::lround((t.c(b, d) - t.c(j, d)) / xmin);
-          s += (o + 1) * mul;
-          mul *= 3;
-        }
-        H.m2l_nbr.push_back({H.mp_slot[j], s});
-        mt.cnt++;
+    {
+      const int a = t.lfirst[nls], z = t.llast[nls], nc = z - a + 1;
+      std::vector<int> tix(nc + 1, 0), nix(nc + 1, 0);
+#pragma omp parallel for schedule(static) if (nc > 4096)
+      for (int b = a; b <= z; b++) {
+        if (H.loc_slot[b] < 0) continue;
+        int n = 0;
+        for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) n += H.mp_slot[L.pw[k]] >= 0;
+        tix[b - a + 1] = 1;
+        nix[b - a + 1] = n;
       }
-      H.m2l.push_back(mt);
+      for (int i = 0; i < nc; i++) {
+        tix[i + 1] += tix[i];
+        nix[i + 1] += nix[i];
+      }
+      H.m2l.resize(tix[nc]);
+      H.m2l_nbr.resize(nix[nc]);
+#pragma omp parallel for schedule(static) if (nc > 4096)
+      for (int b = a; b <= z; b++) {
+        if (H.loc_slot[b] < 0) continue;
+        int q = nix[b - a];
+        M2LTask mt{H.loc_slot[b], H.mp_slot[b], q, 0};
+        for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) {
+          int j = L.pw[k];
+          if (H.mp_slot[j] < 0) continue;
+          int s = 0, mul = 1;
+          for (int d = 0; d < D; d++) {
+            int o = (int)std::lround((t.c(b, d) - t.c(j, d)) / xmin);
+            s += (o + 1) * mul;
+            mul *= 3;
+          }
+          H.m2l_nbr[q++] = {H.mp_slot[j], s};
+          mt.cnt++;
+        }
+        H.m2l[tix[b - a]] = mt;
+      }
     }
     // (b) split, parents at levels nlevstart .. nlevels-1
     for (int l = nls; l <= P.nlevels - 1; l++) {

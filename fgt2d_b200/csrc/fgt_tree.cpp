@@ -659,40 +659,34 @@ void build_lists(const Tree& t, Lists& L) {
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++)
     if (nsym[b] > 1) std::sort(L.l1.begin() + L.l1off[b], L.l1.begin() + L.l1off[b] + nsym[b]);
-  std::vector<int> cur;
 
-  // plane-wave lists, the same two passes
-  int nls = std::max(npw, 0);
-  for (int pass = 0; pass < 2; pass++) {
-    if (pass == 0) {
-      L.pwoff.assign(nb + 1, 0);
-    } else {
-      for (int b = 0; b < nb; b++) L.pwoff[b + 1] += L.pwoff[b];
-      L.pw.assign(L.pwoff[nb], 0);
-      cur.assign(L.pwoff.begin(), L.pwoff.end() - 1);
+  // plane-wave lists: the plan reads only the cut level's lists (mp -> loc;
+  // merge and split take the children from the tree), so only those are
+  // built: the colleagues other than the box itself (3D: the non-leaf ones),
+  // counted and filled in parallel in colleague order
+  L.pwoff.assign(nb + 1, 0);
+  if (npw >= 0 && npw <= t.nlevels) {
+    const int a = t.lfirst[npw], z = t.llast[npw];
+    auto keep = [&](int b, int jb) { return jb != b && (D == 2 || t.nchild[jb] > 0); };
+#pragma omp parallel for schedule(static) if (z - a > 4096)
+    for (int b = a; b <= z; b++) {
+      int n = 0;
+      for (int i = 0; i < t.ncoll[b]; i++) n += keep(b, t.coll[(size_t)b * NCO + i]);
+      L.pwoff[b + 1] = n;
     }
-    auto add = [&](int b, int v) {
-      if (pass == 0) L.pwoff[b + 1]++;
-      else L.pw[cur[b]++] = v;
-    };
-    // the plan reads the cut level's lists (mp -> loc); the merge and split
-    // steps take the children from the tree, so the sibling lists of the
-    // finer levels are not built
-    for (int l = nls; l <= std::min(t.nlevels, nls); l++)
-      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-        if (l == npw) {
-          for (int i = 0; i < t.ncoll[b]; i++) {
-            int jb = t.coll[(size_t)b * NCO + i];
-            if (jb != b && (D == 2 || t.nchild[jb] > 0)) add(b, jb);
-          }
-        } else if (l > nls) {
-          int dad = t.parent[b];
-          for (int j = 0; j < NCH; j++) {
-            int jb = t.ch(dad, j);
-            if (jb >= 0 && jb != b) add(b, jb);
-          }
-        }
+    for (int b = a; b <= z; b++) L.pwoff[b + 1] += L.pwoff[b];
+    for (int b = z + 1; b < nb; b++) L.pwoff[b + 1] = L.pwoff[z + 1];
+    L.pw.assign(L.pwoff[nb], 0);
+#pragma omp parallel for schedule(static) if (z - a > 4096)
+    for (int b = a; b <= z; b++) {
+      int q = L.pwoff[b];
+      for (int i = 0; i < t.ncoll[b]; i++) {
+        const int jb = t.coll[(size_t)b * NCO + i];
+        if (keep(b, jb)) L.pw[q++] = jb;
       }
+    }
+  } else {
+    L.pw.clear();
   }
 
   // iflocal: cut-level leaves with a non-leaf colleague (fgt2d.f:790-814)
