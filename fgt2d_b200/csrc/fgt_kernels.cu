@@ -1953,6 +1953,191 @@ __global__ void __launch_bounds__(256, 2) k_pw2taylor3d_mma(KP k, const ConvTask
   }
 }
 
+// k_pw2taylor3d_mma2: the same conversion for orders 17..32 (two 8-row tiles
+// of each parity).  The z accumulators of these orders do not fit in
+// registers, so S2 keeps every z slice (Re and Im, n2 rows of P^2) and the z
+// pass runs once per leaf after the x and y passes of all its slice groups;
+// a group is gs slices (4, 2 or 1, the largest whose shared memory fits).
+// One CTA of 8 warps per SM, persistent over the leaves of one order.
+struct C3Dims2 {
+  int gs, ldL, ld1, ld2;
+  size_t total;  // doubles
+  __host__ __device__ C3Dims2(int Pn, int npw, int gs_) {
+    const int n2 = npw / 2;
+    gs = gs_;
+    ldL = ((2 * npw + 7) & ~15) + 8;
+    ld1 = 8 * ((2 * gs * Pn + 7) / 8) + 4;
+    ld2 = 8 * ((Pn * Pn + 7) / 8) + 4;
+    total = (size_t)gs * npw * ldL + (size_t)npw * ld1 + (size_t)2 * n2 * ld2;
+  }
+};
+
+template <int KS>
+__global__ void __launch_bounds__(256, 1) k_pw2taylor3d_mma2(KP k, const ConvTask* __restrict__ tasks, int ntask,
+                                                             double* __restrict__ lo_all, int gs) {
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2;
+  const int Pn = tasks[0].p + 1, E = (Pn + 1) & ~1, P2 = Pn * Pn;
+  const int mgN = (65536 + npw - 1) / npw, mgP = (65536 + Pn - 1) / Pn;  // div16 factors
+  const C3Dims2 Z(Pn, npw, gs);
+  extern __shared__ double sm[];
+  double* Lb = sm;                                  // [gs m1][npw m2][ldL]: (m3, re/im)
+  double* S1 = Lb + (size_t)gs * npw * Z.ldL;       // [npw m2][ld1]: (m1, a, re/im)
+  double* S2r = S1 + (size_t)npw * Z.ld1;           // [n2 m1][ld2]: (b, a)
+  double* S2i = S2r + (size_t)n2 * Z.ld2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
+  int tk = blockIdx.x;
+  if (tk >= ntask) return;
+  // A fragments: tx[u][par][s] = table row 2 (8 u + r) + par, node 4 s + c
+  double tx[2][2][KS];
+#pragma unroll
+  for (int u = 0; u < 2; u++)
+#pragma unroll
+    for (int par = 0; par < 2; par++)
+#pragma unroll
+      for (int s = 0; s < KS; s++) {
+        const int a = 2 * (8 * u + r) + par, m = 4 * s + c;
+        tx[u][par][s] =
+            (a < Pn && m < n2) ? (((a >> 1) & 1) ? -k.x2l[a * npw + m] : k.x2l[a * npw + m]) : 0.0;
+      }
+  const int ng = (n2 + gs - 1) / gs;
+  auto stage = [&](int slot, int g) {
+    const double* L = reinterpret_cast<const double*>(k.loc + ((size_t)slot * k.nd + ind) * k.nexp) +
+                      (size_t)2 * gs * g * npw * npw;
+    const int rows = min(gs, n2 - gs * g) * npw;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(Lb);
+    for (int row = warp; row < rows; row += 8)
+      for (int u = lane; u < npw; u += 32)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 8u * (unsigned)(row * Z.ldL + 2 * u)),
+                     "l"(L + (size_t)row * 2 * npw + 2 * u) : "memory");
+  };
+  int slot = tasks[tk].slot;
+  stage(slot, 0);
+  const int ntZ = (P2 + 7) / 8;
+  for (; tk < ntask; tk += gridDim.x) {
+    const int tn = tk + gridDim.x;
+    const int nslot = tn < ntask ? tasks[tn].slot : 0;
+    const long long off = tasks[tk].off;
+    for (int g = 0; g < ng; g++) {
+      const int ns = min(gs, n2 - gs * g);
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      __syncthreads();
+      // x pass: columns (m1, m2, re/im) of the staged slices
+      const int ntX = (ns * npw * 2 + 7) / 8;
+      for (int nt = warp; nt < ntX; nt += 8) {
+        const int col = 8 * nt + r;
+        const double* bp = Lb + (col >> 1) * Z.ldL + (col & 1);
+        double acc[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int m = 4 * s + c;
+          double v1 = 0.0, v2 = 0.0;
+          if (m < n2) {
+            v1 = bp[2 * m];
+            v2 = bp[2 * (npw - 1 - m)];
+          }
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            dmma_884(acc[u][0], acc[u][1], tx[u][0][s], v1 + v2);
+            dmma_884(acc[u][2], acc[u][3], tx[u][1][s], v1 - v2);
+          }
+        }
+        const int q = 4 * nt + c;  // the lane's complex column (m1, m2)
+        if (q < ns * npw) {
+          const int m1 = div16(q, mgN), m2 = q - m1 * npw;
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const int a = 2 * (8 * u + r);
+            double* o = S1 + m2 * Z.ld1 + 2 * (m1 * Pn + a);
+            if (a < Pn) *reinterpret_cast<double2*>(o) = make_double2(acc[u][0], acc[u][1]);
+            if (a + 1 < Pn) *reinterpret_cast<double2*>(o + 2) = make_double2(-acc[u][3], acc[u][2]);
+          }
+        }
+      }
+      __syncthreads();
+      // the slices are consumed: copy the next group's (or the next leaf's first)
+      if (g + 1 < ng) stage(slot, g + 1);
+      else if (tn < ntask) stage(nslot, 0);
+      // y pass: columns (m1, a, re/im) into the z slices gs g + m1 of S2
+      const int ntY = (ns * Pn * 2 + 7) / 8;
+      for (int nt = warp; nt < ntY; nt += 8) {
+        const int col = 8 * nt + r;
+        double acc[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; s++) {
+          const int m = 4 * s + c;
+          double v1 = 0.0, v2 = 0.0;
+          if (m < n2) {
+            v1 = S1[m * Z.ld1 + col];
+            v2 = S1[(npw - 1 - m) * Z.ld1 + col];
+          }
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            dmma_884(acc[u][0], acc[u][1], tx[u][0][s], v1 + v2);
+            dmma_884(acc[u][2], acc[u][3], tx[u][1][s], v1 - v2);
+          }
+        }
+        const int q = 4 * nt + c;  // the lane's complex column (m1, a)
+        if (q < ns * Pn) {
+          const int m1 = div16(q, mgP), a = q - m1 * Pn;
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const int b = 2 * (8 * u + r);
+            const int o = (gs * g + m1) * Z.ld2 + b * Pn + a;
+            if (b < Pn) {
+              S2r[o] = acc[u][0];
+              S2i[o] = acc[u][1];
+            }
+            if (b + 1 < Pn) {
+              S2r[o + Pn] = -acc[u][3];
+              S2i[o + Pn] = acc[u][2];
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // z pass over all slices: rows c = 2 (8 u + r) + par, columns (b, a)
+    double* out = lo_all + off + (size_t)ind * P2 * E;
+    for (int nt = warp; nt < ntZ; nt += 8) {
+      double acc[2][2][2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) acc[u][0][0] = acc[u][0][1] = acc[u][1][0] = acc[u][1][1] = 0.0;
+#pragma unroll
+      for (int s = 0; s < KS; s++) {
+        const int m1 = 4 * s + c;
+        const double br = m1 < n2 ? S2r[m1 * Z.ld2 + 8 * nt + r] : 0.0;
+        const double bi = m1 < n2 ? S2i[m1 * Z.ld2 + 8 * nt + r] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          dmma_884(acc[u][0][0], acc[u][0][1], tx[u][0][s], br);
+          dmma_884(acc[u][1][0], acc[u][1][1], tx[u][1][s], bi);
+        }
+      }
+#pragma unroll
+      for (int ii = 0; ii < 2; ii++) {
+        const int q = 8 * nt + 2 * c + ii;
+        if (q < P2) {
+          const int b = div16(q, mgP), a = q - b * Pn;
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const int ce = 2 * (8 * u + r);
+            if (ce < Pn) out[(ce * Pn + b) * E + a] = 2.0 * acc[u][0][ii];
+            if (ce + 1 < Pn) out[((ce + 1) * Pn + b) * E + a] = -2.0 * acc[u][1][ii];
+          }
+        }
+      }
+    }
+    if (E > Pn)  // the padding column of every row
+      for (int e = threadIdx.x; e < P2; e += blockDim.x) out[(size_t)e * E + Pn] = 0.0;
+    slot = nslot;
+  }
+}
+
 // k_eval3d_horner: one CTA (128 threads) per chunk of <= 256 points of an
 // evaluation leaf; the leaf's Taylor block lo[c][b][a] (rows of E = 2 NP2)
 // is staged in shared memory and each thread evaluates two points by Horner
@@ -3088,6 +3273,10 @@ cudaError_t device_pool_setup() {
 
 cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_isrc, const int* d_itarg,
                                cudaStream_t pst, size_t* size_only) {
+  const auto tnow = [] {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  const double tin = tnow();
   D = DevicePlan();
   D.P = H.P;
   const Params& P = H.P;
@@ -3314,14 +3503,11 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     *size_only = total;
     return cudaSuccess;
   }
-  const auto tnow = [] {
-    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-  };
   const double tm0 = tnow();
   D.stream = pst;
   CK(device_pool_setup());
   CK(cudaMallocAsync(reinterpret_cast<void**>(&D.base), total, pst));
-  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "device plan: malloc %.4f (%zu bytes)\n", tnow() - tm0, total);
+  const double tm1 = tnow();
   char* cur = D.base;
   cudaStream_t s = pst;
   CK(put(cur, D.centers, H.box_centers, s));
@@ -3415,6 +3601,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.scratch = reinterpret_cast<double2*>(cur); cur += al((size_t)D.scratch_ctas * D.scratch_per_cta * 16);
   D.uscr = reinterpret_cast<double*>(cur); cur += al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8);
   CK(cudaStreamSynchronize(s));
+  if (getenv("FGT_TREE_TIMING"))
+    fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes)\n", tm0 - tin, tm1 - tm0,
+            tnow() - tm1, total);
   return cudaSuccess;
 }
 
@@ -3766,6 +3955,25 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
             CONV3M_CASE(1) CONV3M_CASE(2) CONV3M_CASE(3) CONV3M_CASE(4)
             CONV3M_CASE(5) CONV3M_CASE(6) CONV3M_CASE(7) CONV3M_CASE(8)
 #undef CONV3M_CASE
+            default: return cudaErrorNotSupported;
+          }
+          launches++;
+          continue;
+        }
+        int gs2 = 4;
+        while (gs2 > 1 && C3Dims2(Pn, P.npw, gs2).total * 8 > 227 * 1024) gs2 >>= 1;
+        const size_t shm2 = C3Dims2(Pn, P.npw, gs2).total * 8;
+        if (Pn > 16 && Pn <= 32 && ksm <= 8 && shm2 <= 227 * 1024) {
+          const dim3 pg(std::min(nt, D.sm_count), nd);
+          switch (ksm) {
+#define CONV3M2_CASE(N)                                                                           \
+  case N:                                                                                         \
+    CK(cudaFuncSetAttribute(k_pw2taylor3d_mma2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm2)); \
+    k_pw2taylor3d_mma2<N><<<pg, 256, shm2, st>>>(k, D.conv + G.beg, nt, D.lo, gs2);               \
+    break;
+            CONV3M2_CASE(1) CONV3M2_CASE(2) CONV3M2_CASE(3) CONV3M2_CASE(4)
+            CONV3M2_CASE(5) CONV3M2_CASE(6) CONV3M2_CASE(7) CONV3M2_CASE(8)
+#undef CONV3M2_CASE
             default: return cudaErrorNotSupported;
           }
           launches++;
