@@ -494,7 +494,10 @@ def serving_arm(args):
         "unit": "ms", "higher_is_better": False, "n_gpus": 1, "impl": "ours",
         "p50_ms_small": q(lat[small], 0.50), "p50_ms_all": q(lat[ok], 0.50), "p99_ms_all": q(lat[ok], 0.99),
         "max_ms_all": q(lat[ok], 1.0), "requests": n_req, "completed": int(ok.sum()),
-        "failed": int((~ok).sum()), "points_per_s": pts / span, "span_s": span,
+        "failed": int((~ok).sum()),
+        "failures": [[int(k), int(status[k]), int(dims[k]), int(ns[k]), float(deltas[k]), float(epss[k])]
+                     for k in np.flatnonzero(~ok)[:8]],
+        "points_per_s": pts / span, "span_s": span,
         "arrival_rate_per_s": rate, "workers": args.workers, "peak_device_bytes": st["peak_bytes"],
         "budget_device_bytes": st["budget_bytes"], "data": "synthetic (seeded numpy)",
         "config": {"workload": "serving stream: Poisson arrivals, dim in {2,3}, N log-uniform [1e3,1e6] "

@@ -1107,6 +1107,7 @@ struct fgt_server {
   long long in_pts = 0, in_plan = 0, peak = 0;
   bool stop = false;
   long long submitted = 0, completed = 0, failed = 0, points = 0;
+  int running = 0;  // requests taken by a worker and not yet done
   std::vector<double> lat;
   double t_first = -1, t_last = 0;
 };
@@ -1219,10 +1220,25 @@ void server_worker(fgt_server* S, int w) {
       J = S->queue[pick];
       S->queue.erase(S->queue.begin() + pick);
       J->t_start = t;
+      S->running++;
     }
-    const int st = server_run(S, ctx, J->r);
+    int st = server_run(S, ctx, J->r);
+    for (int retry = 0; st == FGT_ERR_NOMEM && retry < 50; retry++) {
+      // the device memory is held (or fragmented) by requests in flight:
+      // retry when one of them has finished (or after 0.1 s, so that workers
+      // that all wait cannot block one another); alone, the failure stands
+      (void)cudaGetLastError();
+      {
+        std::unique_lock<std::mutex> lk(S->mu);
+        if (S->running <= 1) break;
+        const long long c0 = S->completed;
+        S->cv_done.wait_for(lk, std::chrono::milliseconds(100), [&] { return S->completed != c0; });
+      }
+      st = server_run(S, ctx, J->r);
+    }
     {
       std::lock_guard<std::mutex> lk(S->mu);
+      S->running--;
       J->t_end = now_s();
       J->status = st;
       J->done = true;
@@ -1262,6 +1278,22 @@ int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_
       return st;
     }
     S->ctxs.push_back(c);
+  }
+  {
+    // reserve the budget in the device's stream-ordered pool once (it keeps
+    // freed memory), so that a request's plan is carved from memory the pool
+    // already holds instead of growing it (mapping tens of GB) inside the
+    // request's latency; without the reservation the pool grows on demand
+    CKS(cudaSetDevice(device));
+    CKS(device_pool_setup());
+    cudaStream_t s = S->ctxs[0]->stream;
+    void* blk = nullptr;
+    if (cudaMallocAsync(&blk, (size_t)max_device_bytes, s) == cudaSuccess) {
+      CKS(cudaFreeAsync(blk, s));
+      CKS(cudaStreamSynchronize(s));
+    } else {
+      (void)cudaGetLastError();
+    }
   }
   fgt_server* raw = S.release();
   for (int w = 0; w < nworkers; w++) raw->workers.emplace_back(server_worker, raw, w);

@@ -2138,6 +2138,110 @@ __global__ void __launch_bounds__(256, 1) k_pw2taylor3d_mma2(KP k, const ConvTas
   }
 }
 
+// k_eval3d_sep: potential at a leaf's points straight from its plane-wave
+// local expansion, for the plane-wave route (g3dpwevalp_vec,
+// g3drouts.f:2268-2362) and for Taylor-route leaves whose order exceeds the
+// conversion kernels (g3dpw2local_real_vec + g3dlevalp_vec).  Both are
+//   pot = 2 Re sum_{m1 < n2} Z[m1](z) sum_{m2} Y[m2](y) sum_{m3} X[m3](x) L[m1][m2][m3]
+// with X[m](x) = exp(i t_m x) on the plane-wave route and, on the Taylor
+// route, its series truncated at the order, sum_{a<P} x2l[a][m] (i x)^a: the
+// Taylor block lo[c][b][a] of the conversion contracted with x^a y^b z^c is
+// exactly this sum, evaluated without forming the P^3 block.  One CTA per
+// task; points in blocks of 32 whose phase tables sit in shared memory; a
+// thread takes rows (m1, m2) of the expansion for four points (L read once
+// per block, through the read-only cache), and the partial sums are reduced
+// in a fixed order.  Potentials only (the derivative variants keep their own
+// kernels).
+constexpr int SEP_NPB = 32;
+__device__ __forceinline__ double2 sep_phase(const KP& k, bool taylor, int m, double u, int Pn) {
+  const double t = (2 * (m - k.n2) + 1) * k.t1;
+  if (!taylor) return cexpi(t * u);
+  // sum_{a<P} x2l[a][m] (i u)^a by Horner in (i u)
+  double re = k.x2l[(Pn - 1) * k.npw + m], im = 0.0;
+  for (int a = Pn - 2; a >= 0; a--) {
+    const double nr = fma(-im, u, k.x2l[a * k.npw + m]);
+    im = re * u;
+    re = nr;
+  }
+  return make_double2(re, im);
+}
+template <bool TAYLOR>
+__global__ void __launch_bounds__(256) k_eval3d_sep(KP k, const EvalTask* __restrict__ tasks) {
+  const EvalTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2, Pn = T.p + 1, tid = threadIdx.x;
+  const double2* L = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
+  const double* pts = T.set ? k.trg : k.src;
+  double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
+  const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
+  extern __shared__ double2 sep_sh[];
+  double2* X = sep_sh;                      // [npw][SEP_NPB]
+  double2* Y = X + npw * SEP_NPB;           // [npw][SEP_NPB]
+  double2* Zt = Y + npw * SEP_NPB;          // [n2][SEP_NPB]
+  double2* part = Zt + n2 * SEP_NPB;        // [256][4] partial sums
+  const int nrow = n2 * npw;
+  for (int p0 = 0; p0 < T.n; p0 += SEP_NPB) {
+    const int np = min(SEP_NPB, T.n - p0);
+    for (int e = tid; e < (2 * npw + n2) * SEP_NPB; e += blockDim.x) {
+      const int m = e / SEP_NPB, pt = e % SEP_NPB;
+      const int d = m < npw ? 0 : m < 2 * npw ? 1 : 2, node = d == 0 ? m : d == 1 ? m - npw : m - 2 * npw;
+      double2 v = make_double2(0.0, 0.0);
+      if (pt < np) {
+        const double u = (pts[3 * (T.i0 + p0 + pt) + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
+        v = sep_phase(k, TAYLOR, node, u, Pn);
+      }
+      X[m * SEP_NPB + pt] = v;  // X, Y and Zt are consecutive
+    }
+    __syncthreads();
+    const int npg = (np + 3) / 4, rstep = blockDim.x / npg;
+    const int pg = tid % npg, rs = tid / npg;
+    double2 acc[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[j] = make_double2(0.0, 0.0);
+    if (rs < rstep) {
+      int m1 = 0, m2 = rs;
+      while (m2 >= npw) {
+        m2 -= npw;
+        m1++;
+      }
+      for (int row = rs; row < nrow; row += rstep) {
+        const double2* Lr = L + (size_t)row * npw;
+        double2 s[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) s[j] = make_double2(0.0, 0.0);
+        for (int m3 = 0; m3 < npw; m3++) {
+          const double2 l = __ldg(Lr + m3);
+          const double2* xp = X + m3 * SEP_NPB + 4 * pg;
+#pragma unroll
+          for (int j = 0; j < 4; j++) s[j] = cfma(l, xp[j], s[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double2 yz = cmul(Y[m2 * SEP_NPB + 4 * pg + j], Zt[m1 * SEP_NPB + 4 * pg + j]);
+          acc[j] = cfma(s[j], yz, acc[j]);
+        }
+        m2 += rstep;
+        while (m2 >= npw) {
+          m2 -= npw;
+          m1++;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) part[tid * 4 + j] = acc[j];
+    __syncthreads();
+    if (tid < np) {
+      const int g = tid >> 2, j = tid & 3;
+      double re = 0.0;
+      for (int r = 0; r < rstep; r++) re += part[(r * npg + g) * 4 + j].x;
+      const double v = 2.0 * re;
+      add_out<1>(out, T.i0 + p0 + tid, k.nd, nc, ind, &v);
+    }
+    __syncthreads();
+  }
+}
+
 // k_eval3d_horner: one CTA (128 threads) per chunk of <= 256 points of an
 // evaluation leaf; the leaf's Taylor block lo[c][b][a] (rows of E = 2 NP2)
 // is staged in shared memory and each thread evaluates two points by Horner
@@ -3328,13 +3432,24 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   std::vector<ConvTask> conv;
   std::vector<HornerTask> horner;
   size_t lo_doubles = 0;
-  // 3D: the same two kernels where the order's shared-memory needs fit
-  // (k_eval3d_horner is instantiated for rows of up to 30 coefficients)
-  D.eval3_split = P.dim == 3 && !P.all_direct && D.eval_taylor_n > 0 && D.eval_pmax + 1 <= 30 &&
-                  conv3_smem_bytes(D.eval_pmax + 1, P.npw, 4) <= 200 * 1024 && (P.npw + 3) / 4 <= CONV_MAXKS;
+  // 3D: the same two kernels for the Taylor tasks whose order's shared-memory
+  // needs fit (k_eval3d_horner is instantiated for rows of up to 30
+  // coefficients); the tasks are sorted by order, so these are a prefix and
+  // the higher orders take the direct separable evaluation (k_eval3d_sep) or,
+  // with derivatives, the fallback kernels
+  if (P.dim == 3 && !P.all_direct) {
+    int t = 0;
+    while (t < D.eval_taylor_n && ev[t].p + 1 <= 30 && conv3_smem_bytes(ev[t].p + 1, P.npw, 4) <= 200 * 1024 &&
+           (P.npw + 3) / 4 <= CONV_MAXKS)
+      t++;
+    D.eval3_nsplit = t;
+  }
+  D.eval3_split = D.eval3_nsplit > 0;
+  const int split_pmax = D.eval3_split ? ev[D.eval3_nsplit - 1].p : -1;
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
-    for (int t = 0; t < D.eval_taylor_n; t++) {
+    const int ntay = P.dim == 2 ? D.eval_taylor_n : D.eval3_nsplit;
+    for (int t = 0; t < ntay; t++) {
       const EvalTask& e = ev[t];
       const long long Pn = e.p + 1, E = (Pn + 1) & ~1LL;
       if (slot_off[e.slot] < 0) {
@@ -3458,7 +3573,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       const size_t Pn = D.eval_pmax + 1;
       size_t szA = std::max(2 * Pn * P.npw * n2, Pn * Pn * Pn);
       D.eval3_sh = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2) * 8;
-      D.eval3_smem = D.eval3_sh <= lim || D.eval3_split;  // the split path needs no scratch
+      // the fallback kernels run only on the Taylor tasks beyond the split
+      // kernels' orders, and only with derivatives
+      const bool fallback = D.eval3_nsplit < D.eval_taylor_n && std::max(P.ifpgh, P.ifpghtarg) >= 2;
+      D.eval3_smem = D.eval3_sh <= lim || !fallback;
     }
   }
   // scratch for the 3D separable transforms (fallback path)
@@ -3478,7 +3596,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     D.scratch_ctas = D.scratch_per_cta ? D.sm_count * 2 : 0;
   }
   if (D.eval3_split) {
-    D.uscr_per_cta = (conv3_scratch(D.eval_pmax + 1, P.npw) + 31) & ~size_t(31);
+    D.uscr_per_cta = (conv3_scratch(split_pmax + 1, P.npw) + 31) & ~size_t(31);
     D.conv3_ctas = D.sm_count * 4;
   }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
@@ -3602,8 +3720,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.uscr = reinterpret_cast<double*>(cur); cur += al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8);
   CK(cudaStreamSynchronize(s));
   if (getenv("FGT_TREE_TIMING"))
-    fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes)\n", tm0 - tin, tm1 - tm0,
-            tnow() - tm1, total);
+    fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes); eval tasks: taylor %d "
+            "(conversion %d, max order %d) pw %d\n", tm0 - tin, tm1 - tm0, tnow() - tm1, total, D.eval_taylor_n,
+            P.dim == 3 ? D.eval3_nsplit : D.eval_taylor_n, D.eval_pmax + 1, D.eval_pw_n);
   return cudaSuccess;
 }
 
@@ -4020,29 +4139,42 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         }
         launches++;
       }
-    } else if (P.dim == 3 && D.eval_taylor_n > 0 && D.eval3_smem) {
+    }
+    // 3D Taylor tasks beyond the conversion kernels' orders, and the
+    // plane-wave route: the direct separable evaluation for potentials
+    const int nbig = P.dim == 3 ? D.eval_taylor_n - D.eval3_nsplit : 0;
+    const size_t sh_sep = ((size_t)(2 * P.npw + P.npw / 2) * SEP_NPB + 256 * 4) * 16;
+    if (nbig > 0 && pgh == 1) {
+      CK(cudaFuncSetAttribute(k_eval3d_sep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh_sep));
+      k_eval3d_sep<true><<<dim3(nbig, nd), 256, sh_sep, st>>>(k, D.eval + D.eval3_nsplit);
+      launches++;
+    } else if (nbig > 0 && D.eval3_smem) {
       {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
         constexpr int PG = decltype(G)::value;
         CK(cudaFuncSetAttribute(k_eval3d_taylor_smem<PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
-        k_eval3d_taylor_smem<PG><<<dim3(D.eval_taylor_n, nd), 512, D.eval3_sh, st>>>(k, D.eval);
+        k_eval3d_taylor_smem<PG><<<dim3(nbig, nd), 512, D.eval3_sh, st>>>(k, D.eval + D.eval3_nsplit);
         return cudaSuccess;
       });
           CK(e_pgh);
         }
       launches++;
-    } else if (P.dim == 3 && D.eval_taylor_n > 0) {
+    } else if (nbig > 0) {
       {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
-        k_eval3d_taylor<decltype(G)::value><<<D.scratch_ctas, 256, 0, st>>>(k, D.eval, D.eval_taylor_n, D.scratch,
-                                                                           D.scratch_per_cta);
+        k_eval3d_taylor<decltype(G)::value><<<D.scratch_ctas, 256, 0, st>>>(k, D.eval + D.eval3_nsplit, nbig,
+                                                                           D.scratch, D.scratch_per_cta);
         return cudaSuccess;
       });
           CK(e_pgh);
         }
       launches++;
     }
-    if (P.dim == 3 && D.eval_pw_n > 0) {
+    if (P.dim == 3 && D.eval_pw_n > 0 && pgh == 1) {
+      CK(cudaFuncSetAttribute(k_eval3d_sep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh_sep));
+      k_eval3d_sep<false><<<dim3(D.eval_pw_n, nd), 256, sh_sep, st>>>(k, D.eval + D.eval_taylor_n);
+      launches++;
+    } else if (P.dim == 3 && D.eval_pw_n > 0) {
       {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
         k_eval3d_pw<decltype(G)::value><<<dim3(D.eval_pw_n, nd), 256, 0, st>>>(k, D.eval + D.eval_taylor_n);
