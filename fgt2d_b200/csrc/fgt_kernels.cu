@@ -2372,85 +2372,104 @@ __global__ void __launch_bounds__(512) k_eval3d_taylor_smem(KP k, const EvalTask
 // ------------------------------------------------------------ (a) form, 3D direct
 // pw[k3,k2,k1] = sum_i q_i w(k3) e^{-i t x} w(k2) e^{-i t y} w(k1) e^{-i t z}
 // (g3dformpwc_vec, g3drouts.f:1950-2038).  One CTA per (leaf, density);
-// entries in passes of 4 per thread, sources staged with their factor rows.
+// sources in chunks of FORM_CH, each with its three factor rows built once
+// in shared memory; a thread owns expansion rows (k1, k2) for one block of 8
+// consecutive k3 (its block fixed, its rows strided), so each source costs
+// one row product and 8 complex FMAs per item, and the chunks' sums are added
+// to the slot in chunk order.
 __global__ void __launch_bounds__(256) k_form3d_pw(KP k, const FormTask* __restrict__ tasks) {
   const FormTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
   const int npw = k.npw, n2 = k.n2;
   extern __shared__ double sm[];
-  double2* F1 = reinterpret_cast<double2*>(sm);      // [FORM_CH][npw]
-  double2* F2 = F1 + FORM_CH * npw;                    // [FORM_CH][npw]
+  double2* F1 = reinterpret_cast<double2*>(sm);      // [FORM_CH][npw] (+ 8 padding)
+  double2* F2 = F1 + FORM_CH * npw + 8;                // [FORM_CH][npw]
   double2* F3 = F2 + FORM_CH * npw;                    // [FORM_CH][n2], charge folded in
   const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
   double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  for (int e0 = 0; e0 < k.nexp; e0 += 4 * 256) {
-    double2 acc[4];
-    int i3[4], i2[4], i1[4];
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-      acc[s] = make_double2(0.0, 0.0);
-      int e = e0 + threadIdx.x + s * 256;
-      if (e >= k.nexp) e = 0;
-      i3[s] = e % npw;
-      i2[s] = (e / npw) % npw;
-      i1[s] = e / (npw * npw);
-    }
-    // dipoles (g3dformpwd_vec / g3dformpwcd_vec, g3drouts.f:2042-2262): three
-    // columns per source, the factor of one dimension times v_d (-i t dsq)
-    // in each (as dip3_coef), 10 sources per chunk
-    const int vc = k.ifdipole ? 3 : 1, chs = FORM_CH / vc;
-    for (int c0 = 0; c0 < T.n; c0 += chs) {
-      const int m = vc * min(chs, T.n - c0);
-      __syncthreads();
-      if (threadIdx.x < m) {
-        const int i = T.s0 + c0 + threadIdx.x / vc, col = threadIdx.x % vc;
-        const double x = (k.src[3 * i] - cx) * k.dsq, y = (k.src[3 * i + 1] - cy) * k.dsq,
-                     z = (k.src[3 * i + 2] - cz) * k.dsq;
-        double dv[3] = {0.0, 0.0, 0.0}, ca[3], cb[3];
-        if (k.ifdipole) src_dipole<3>(k, i, ind, dv);
-        const double q = k.ifdipole ? src_charge(k, i, ind) : k.chg[(size_t)i * k.nd + ind];
-        for (int d = 0; d < 3; d++) dip3_coef(col, d, q, dv, ca[d], cb[d]);
-        // positive node m: t = (2m+1) t1 at index n2+m; its mirror n2-1-m
-        double2 ex = cexpi(-k.t1 * x), ey = cexpi(-k.t1 * y), ez = cexpi(-k.t1 * z);
-        const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey), ezz = cmul(ez, ez);
-        double2* f1 = F1 + threadIdx.x * npw;
-        double2* f2 = F2 + threadIdx.x * npw;
-        double2* f3 = F3 + threadIdx.x * n2;
-        for (int mm = 0; mm < n2; mm++) {
-          const double w = k.ws[n2 + mm];
-          double2 a = make_double2(ex.x * w, ex.y * w), b = make_double2(ey.x * w, ey.y * w),
-                  c = make_double2(ez.x * w * q, ez.y * w * q);
-          if (k.ifdipole) {
-            // ca f + cb f (-i t dsq) per dimension, f = w e^{-i t x}
-            const double td = (2 * mm + 1) * k.t1 * k.dsq;
-            auto mix = [td](double2 f, double p0, double p1) {
-              return make_double2(fma(p0, f.x, p1 * td * f.y), fma(p0, f.y, -p1 * td * f.x));
-            };
-            a = mix(a, ca[0], cb[0]);
-            b = mix(b, ca[1], cb[1]);
-            c = mix(make_double2(ez.x * w, ez.y * w), ca[2], cb[2]);
-          }
-          f1[n2 + mm] = a; f1[n2 - 1 - mm] = make_double2(a.x, -a.y);
-          f2[n2 + mm] = b; f2[n2 - 1 - mm] = make_double2(b.x, -b.y);
-          f3[n2 - 1 - mm] = make_double2(c.x, -c.y);
-          ex = cmul(ex, exx); ey = cmul(ey, eyy); ez = cmul(ez, ezz);
+  // this thread's k3 block and first row; rows advance by rstep.  The block
+  // is the slow index, so a warp's lanes share it (the k3 factors are
+  // broadcast loads) and take consecutive rows
+  const int nmb = (npw + 7) / 8, rstep = blockDim.x / nmb, mb = threadIdx.x / rstep;
+  const int row0 = threadIdx.x - mb * rstep, nrow = n2 * npw;
+  // dipoles (g3dformpwd_vec / g3dformpwcd_vec, g3drouts.f:2042-2262): three
+  // columns per source, the factor of one dimension times v_d (-i t dsq)
+  // in each (as dip3_coef), 10 sources per chunk
+  const int vc = k.ifdipole ? 3 : 1, chs = FORM_CH / vc;
+  for (int c0 = 0; c0 < T.n; c0 += chs) {
+    const int m = vc * min(chs, T.n - c0);
+    __syncthreads();
+    if (threadIdx.x < m) {
+      const int i = T.s0 + c0 + threadIdx.x / vc, col = threadIdx.x % vc;
+      const double x = (k.src[3 * i] - cx) * k.dsq, y = (k.src[3 * i + 1] - cy) * k.dsq,
+                   z = (k.src[3 * i + 2] - cz) * k.dsq;
+      double dv[3] = {0.0, 0.0, 0.0}, ca[3], cb[3];
+      if (k.ifdipole) src_dipole<3>(k, i, ind, dv);
+      const double q = k.ifdipole ? src_charge(k, i, ind) : k.chg[(size_t)i * k.nd + ind];
+      for (int d = 0; d < 3; d++) dip3_coef(col, d, q, dv, ca[d], cb[d]);
+      // positive node m: t = (2m+1) t1 at index n2+m; its mirror n2-1-m
+      double2 ex = cexpi(-k.t1 * x), ey = cexpi(-k.t1 * y), ez = cexpi(-k.t1 * z);
+      const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey), ezz = cmul(ez, ez);
+      double2* f1 = F1 + threadIdx.x * npw;
+      double2* f2 = F2 + threadIdx.x * npw;
+      double2* f3 = F3 + threadIdx.x * n2;
+      for (int mm = 0; mm < n2; mm++) {
+        const double w = k.ws[n2 + mm];
+        double2 a = make_double2(ex.x * w, ex.y * w), b = make_double2(ey.x * w, ey.y * w),
+                c = make_double2(ez.x * w * q, ez.y * w * q);
+        if (k.ifdipole) {
+          // ca f + cb f (-i t dsq) per dimension, f = w e^{-i t x}
+          const double td = (2 * mm + 1) * k.t1 * k.dsq;
+          auto mix = [td](double2 f, double p0, double p1) {
+            return make_double2(fma(p0, f.x, p1 * td * f.y), fma(p0, f.y, -p1 * td * f.x));
+          };
+          a = mix(a, ca[0], cb[0]);
+          b = mix(b, ca[1], cb[1]);
+          c = mix(make_double2(ez.x * w, ez.y * w), ca[2], cb[2]);
         }
+        f1[n2 + mm] = a; f1[n2 - 1 - mm] = make_double2(a.x, -a.y);
+        f2[n2 + mm] = b; f2[n2 - 1 - mm] = make_double2(b.x, -b.y);
+        f3[n2 - 1 - mm] = make_double2(c.x, -c.y);
+        ex = cmul(ex, exx); ey = cmul(ey, eyy); ez = cmul(ez, ezz);
       }
-      __syncthreads();
+    }
+    __syncthreads();
+    if (mb >= nmb) continue;
+    int i1 = 0, i2 = row0;
+    while (i2 >= npw) {
+      i2 -= npw;
+      i1++;
+    }
+    for (int row = row0; row < nrow; row += rstep) {
+      double2 acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[j] = make_double2(0.0, 0.0);
       for (int t = 0; t < m; t++) {
+        const double2 yz = cmul(F2[t * npw + i2], F3[t * n2 + i1]);
+        const double2* f1 = F1 + t * npw + 8 * mb;
 #pragma unroll
-        for (int s = 0; s < 4; s++) {
-          const double2 yz = cmul(F2[t * npw + i2[s]], F3[t * n2 + i1[s]]);
-          acc[s] = cfma(F1[t * npw + i3[s]], yz, acc[s]);
-        }
+        for (int j = 0; j < 8; j++) acc[j] = cfma(f1[j], yz, acc[j]);
       }
-    }
+      double2* o = out + (size_t)row * npw + 8 * mb;
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      int e = e0 + threadIdx.x + s * 256;
-      if (e < k.nexp) out[e] = acc[s];
+      for (int j = 0; j < 8; j++)
+        if (8 * mb + j < npw) {
+          if (c0 == 0) {
+            o[j] = acc[j];
+          } else {
+            const double2 p = o[j];
+            o[j] = make_double2(p.x + acc[j].x, p.y + acc[j].y);
+          }
+        }
+      i2 += rstep;
+      while (i2 >= npw) {
+        i2 -= npw;
+        i1++;
+      }
     }
   }
+  if (T.n == 0)  // no sources: a zero expansion
+    for (int e = threadIdx.x; e < k.nexp; e += blockDim.x) out[e] = make_double2(0.0, 0.0);
 }
 
 // ------------------------------------------------------------ (b) shifts
@@ -3960,7 +3979,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       launches++;
     }
     if (P.dim == 3 && D.form_pw_n > 0) {
-      size_t sh = (size_t)FORM_CH * (2 * P.npw + n2) * 16;
+      size_t sh = ((size_t)FORM_CH * (2 * P.npw + n2) + 8) * 16;
       CK(cudaFuncSetAttribute(k_form3d_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
       k_form3d_pw<<<dim3(D.form_pw_n, nd), 256, sh, st>>>(k, D.form + D.form_hermite_n);
       launches++;
