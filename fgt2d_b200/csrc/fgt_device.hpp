@@ -121,6 +121,7 @@ struct DevicePlan {
   bool form3_smem = false, eval3_smem = false;
   bool eval3_split = false;  // 3D Taylor eval in two kernels (conversion, Horner)
   int eval3_nsplit = 0;      // 3D Taylor tasks [0, eval3_nsplit) take the two kernels
+  int form3_nsplit = 0;      // 3D Hermite form tasks [0, form3_nsplit) take the shared-memory kernels
   size_t form3_shB = 0, eval3_sh = 0;
   std::vector<OrderGroup> fchunk_groups;  // chunk ranges of equal order
   // per-CTA scratch of the 3D separable transforms (fallback path)

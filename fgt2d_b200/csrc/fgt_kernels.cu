@@ -3375,6 +3375,24 @@ size_t al(size_t b) { return (b + 255) & ~size_t(255); }
     if (e_ != cudaSuccess) return e_;       \
   } while (0)
 
+// Shared memory of k_form3d_h2pw (the SIMT passes) at order Pn.
+size_t form3_simt_smem(int Pn_, int npw) {
+  const size_t Pn = Pn_, n2 = npw / 2, P3 = Pn * Pn * Pn;
+  const size_t szA = std::max(P3, 2 * Pn * npw * n2);
+  return (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2 + Pn * npw) * 8;
+}
+// Whether the 3D Hermite form of order Pn runs on the shared-memory kernels:
+// k_form3d_mma's staging ((8 ceil(P/8) + 2 P) power rows of 68 doubles) and
+// one of the Hermite -> PW kernels (tensor-core or SIMT passes).
+bool form3_fits(int Pn, int npw) {
+  const size_t lim = 227 * 1024;
+  const size_t shA = ((size_t)8 * ((Pn + 7) / 8) + 2 * Pn) * 68 * 8;
+  if (Pn > 32 || shA > lim) return false;
+  const H3Dims Z(Pn, npw / 2);
+  const bool mma = (Pn + 7) / 8 <= 4 && (npw / 2 + 7) / 8 <= 4 && std::min(Z.total_pf, Z.total_ov) * 8 <= lim;
+  return mma || form3_simt_smem(Pn, npw) <= lim;
+}
+
 cudaError_t device_pool_setup() {
   // keep freed stream-ordered allocations in the device's default pool
   // instead of returning them at every synchronisation (process-local
@@ -3553,15 +3571,16 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     const size_t lim = 227 * 1024;
     const int n2 = P.npw / 2;
     if (D.form_hermite_n > 0) {
-      const size_t Pn = D.form_pmax + 1, P3 = Pn * Pn * Pn;
-      size_t szA = std::max(P3, 2 * Pn * P.npw * n2);
-      D.form3_shB = (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2 + Pn * P.npw) * 8;
-      // k_form3d_mma stages (8 ceil(P/8) + 2 P) power rows of 68 doubles
-      const size_t shA = ((size_t)8 * ((Pn + 7) / 8) + 2 * Pn) * 68 * 8;
-      D.form3_smem = D.form3_shB <= lim && shA <= lim && Pn <= 32;
+      // the Hermite block kernel and one of the two Hermite -> PW kernels
+      // take the tasks whose order fits their shared memory (a prefix: the
+      // tasks are sorted by order); the rest take the scratch fallback
+      int t = 0;
+      while (t < D.form_hermite_n && form3_fits(form[t].p + 1, P.npw)) t++;
+      D.form3_nsplit = t;
+      D.form3_smem = t > 0;
       if (D.form3_smem) {
         long long hoff = 0;
-        for (int t = 0; t < D.form_hermite_n; t++) {
+        for (int t = 0; t < D.form3_nsplit; t++) {
           fcbeg.push_back((int)fchunks.size());
           const FormTask& f = form[t];
           long long p3 = (long long)(f.p + 1) * (f.p + 1) * (f.p + 1);
@@ -3599,10 +3618,11 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     }
   }
   // scratch for the 3D separable transforms (fallback path)
-  if (P.dim == 3 && !P.all_direct && (!D.form3_smem || !D.eval3_smem)) {
+  const bool form3_fallback = P.dim == 3 && D.form3_nsplit < D.form_hermite_n;
+  if (P.dim == 3 && !P.all_direct && (form3_fallback || !D.eval3_smem)) {
     size_t slab = 0;
     int n2 = P.npw / 2;
-    if (!D.form3_smem)
+    if (form3_fallback)
       for (auto& f : form)
         if (f.route == ROUTE_HERMITE) slab = std::max(slab, (size_t)(f.p + 1) * (f.p + 1) * n2 + (size_t)(f.p + 1) * P.npw * n2);
     if (!D.eval3_smem)
@@ -3740,8 +3760,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   CK(cudaStreamSynchronize(s));
   if (getenv("FGT_TREE_TIMING"))
     fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes); eval tasks: taylor %d "
-            "(conversion %d, max order %d) pw %d\n", tm0 - tin, tm1 - tm0, tnow() - tm1, total, D.eval_taylor_n,
-            P.dim == 3 ? D.eval3_nsplit : D.eval_taylor_n, D.eval_pmax + 1, D.eval_pw_n);
+            "(conversion %d, max order %d) pw %d; form tasks: hermite %d (shared memory %d, max order %d) pw %d\n",
+            tm0 - tin, tm1 - tm0, tnow() - tm1, total, D.eval_taylor_n,
+            P.dim == 3 ? D.eval3_nsplit : D.eval_taylor_n, D.eval_pmax + 1, D.eval_pw_n, D.form_hermite_n,
+            P.dim == 3 ? D.form3_nsplit : D.form_hermite_n, D.form_pmax + 1, D.form_pw_n);
   return cudaSuccess;
 }
 
@@ -3934,6 +3956,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       // Hermite -> plane wave per order group: tensor-core passes where the
       // order and node count fit their fragments and shared memory
       for (const OrderGroup& G : D.form_groups) {
+        if (G.beg >= D.form3_nsplit) break;  // the scratch fallback's orders
         const int Pn = G.p + 1, ks = (Pn + 7) / 8, mt = (P.npw / 2 + 7) / 8;
         const H3Dims Z3(Pn, P.npw / 2);
         const bool pf = Z3.total_pf * 8 <= 227 * 1024;
@@ -3959,22 +3982,27 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
             default: return cudaErrorNotSupported;
           }
         } else {
-          CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.form3_shB));
-          k_form3d_h2pw<<<hg, 512, D.form3_shB, st>>>(k, ft, cb, D.fchunks, D.hbuf);
+          const size_t shb = form3_simt_smem(Pn, P.npw);
+          CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
+          k_form3d_h2pw<<<hg, 512, shb, st>>>(k, ft, cb, D.fchunks, D.hbuf);
         }
         launches++;
       }
-    } else if (P.dim == 3 && D.form_hermite_n > 0) {
+    }
+    if (P.dim == 3 && D.form3_nsplit < D.form_hermite_n) {
+      // scratch fallback for the orders above the shared-memory kernels
+      const FormTask* ft = D.form + D.form3_nsplit;
+      const int nft = D.form_hermite_n - D.form3_nsplit;
       int Pn = D.form_pmax + 1;
       size_t sh = ((size_t)Pn * Pn * Pn + 3 * FORM_CH * Pn) * 8;
       if (Pn > 32 || sh > 227 * 1024) return cudaErrorNotSupported;
       int grid = D.scratch_ctas;
       if (Pn <= 16) {
         CK(cudaFuncSetAttribute(k_form3d_hermite<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta, D.isq);
+        k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, ft, nft, D.scratch, D.scratch_per_cta, D.isq);
       } else {
         CK(cudaFuncSetAttribute(k_form3d_hermite<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-        k_form3d_hermite<32><<<grid, 256, sh, st>>>(k, D.form, D.form_hermite_n, D.scratch, D.scratch_per_cta, D.isq);
+        k_form3d_hermite<32><<<grid, 256, sh, st>>>(k, ft, nft, D.scratch, D.scratch_per_cta, D.isq);
       }
       launches++;
     }
