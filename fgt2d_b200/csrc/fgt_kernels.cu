@@ -2166,7 +2166,7 @@ __device__ __forceinline__ double2 sep_phase(const KP& k, bool taylor, int m, do
   return make_double2(re, im);
 }
 template <bool TAYLOR>
-__global__ void __launch_bounds__(256) k_eval3d_sep(KP k, const EvalTask* __restrict__ tasks) {
+__global__ void __launch_bounds__(256, 2) k_eval3d_sep(KP k, const EvalTask* __restrict__ tasks) {
   const EvalTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y;
   const int npw = k.npw, n2 = k.n2, Pn = T.p + 1, tid = threadIdx.x;
@@ -2210,7 +2210,20 @@ __global__ void __launch_bounds__(256) k_eval3d_sep(KP k, const EvalTask* __rest
         double2 s[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) s[j] = make_double2(0.0, 0.0);
-        for (int m3 = 0; m3 < npw; m3++) {
+        // eight coefficients loaded before their products (loads in flight)
+        int m3 = 0;
+        for (; m3 + 8 <= npw; m3 += 8) {
+          double2 l[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) l[u] = __ldg(Lr + m3 + u);
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const double2* xp = X + (m3 + u) * SEP_NPB + 4 * pg;
+#pragma unroll
+            for (int j = 0; j < 4; j++) s[j] = cfma(l[u], xp[j], s[j]);
+          }
+        }
+        for (; m3 < npw; m3++) {
           const double2 l = __ldg(Lr + m3);
           const double2* xp = X + m3 * SEP_NPB + 4 * pg;
 #pragma unroll
