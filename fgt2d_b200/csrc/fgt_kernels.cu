@@ -2153,13 +2153,15 @@ __global__ void __launch_bounds__(256, 1) k_pw2taylor3d_mma2(KP k, const ConvTas
 // in a fixed order.  Potentials only (the derivative variants keep their own
 // kernels).
 constexpr int SEP_NPB = 32;
-__device__ __forceinline__ double2 sep_phase(const KP& k, bool taylor, int m, double u, int Pn) {
+// xt: the x2l table of the order, staged in shared memory ([a][m], npw per row)
+__device__ __forceinline__ double2 sep_phase(const KP& k, bool taylor, int m, double u, int Pn,
+                                             const double* xt) {
   const double t = (2 * (m - k.n2) + 1) * k.t1;
   if (!taylor) return cexpi(t * u);
   // sum_{a<P} x2l[a][m] (i u)^a by Horner in (i u)
-  double re = k.x2l[(Pn - 1) * k.npw + m], im = 0.0;
+  double re = xt[(Pn - 1) * k.npw + m], im = 0.0;
   for (int a = Pn - 2; a >= 0; a--) {
-    const double nr = fma(-im, u, k.x2l[a * k.npw + m]);
+    const double nr = fma(-im, u, xt[a * k.npw + m]);
     im = re * u;
     re = nr;
   }
@@ -2180,7 +2182,11 @@ __global__ void __launch_bounds__(256, 2) k_eval3d_sep(KP k, const EvalTask* __r
   double2* Y = X + npw * SEP_NPB;           // [npw][SEP_NPB]
   double2* Zt = Y + npw * SEP_NPB;          // [n2][SEP_NPB]
   double2* part = Zt + n2 * SEP_NPB;        // [256][4] partial sums
+  double* xt = reinterpret_cast<double*>(part + 256 * 4);  // Taylor route: x2l rows a < P
+  if (TAYLOR)
+    for (int e = tid; e < Pn * npw; e += blockDim.x) xt[e] = k.x2l[e];
   const int nrow = n2 * npw;
+  __syncthreads();
   for (int p0 = 0; p0 < T.n; p0 += SEP_NPB) {
     const int np = min(SEP_NPB, T.n - p0);
     for (int e = tid; e < (2 * npw + n2) * SEP_NPB; e += blockDim.x) {
@@ -2189,9 +2195,11 @@ __global__ void __launch_bounds__(256, 2) k_eval3d_sep(KP k, const EvalTask* __r
       double2 v = make_double2(0.0, 0.0);
       if (pt < np) {
         const double u = (pts[3 * (T.i0 + p0 + pt) + d] - (d == 0 ? cx : d == 1 ? cy : cz)) * k.dsq;
-        v = sep_phase(k, TAYLOR, node, u, Pn);
+        v = sep_phase(k, TAYLOR, node, u, Pn, xt);
       }
-      X[m * SEP_NPB + pt] = v;  // X, Y and Zt are consecutive
+      // X, Y and Zt are consecutive; point 4 g + j sits at j * 8 + g of its
+      // row, so the eight point groups of one j are one 128-byte line
+      X[m * SEP_NPB + (pt & 3) * 8 + (pt >> 2)] = v;
     }
     __syncthreads();
     const int npg = (np + 3) / 4, rstep = blockDim.x / npg;
@@ -2218,20 +2226,20 @@ __global__ void __launch_bounds__(256, 2) k_eval3d_sep(KP k, const EvalTask* __r
           for (int u = 0; u < 8; u++) l[u] = __ldg(Lr + m3 + u);
 #pragma unroll
           for (int u = 0; u < 8; u++) {
-            const double2* xp = X + (m3 + u) * SEP_NPB + 4 * pg;
+            const double2* xp = X + (m3 + u) * SEP_NPB + pg;
 #pragma unroll
-            for (int j = 0; j < 4; j++) s[j] = cfma(l[u], xp[j], s[j]);
+            for (int j = 0; j < 4; j++) s[j] = cfma(l[u], xp[8 * j], s[j]);
           }
         }
         for (; m3 < npw; m3++) {
           const double2 l = __ldg(Lr + m3);
-          const double2* xp = X + m3 * SEP_NPB + 4 * pg;
+          const double2* xp = X + m3 * SEP_NPB + pg;
 #pragma unroll
-          for (int j = 0; j < 4; j++) s[j] = cfma(l, xp[j], s[j]);
+          for (int j = 0; j < 4; j++) s[j] = cfma(l, xp[8 * j], s[j]);
         }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-          const double2 yz = cmul(Y[m2 * SEP_NPB + 4 * pg + j], Zt[m1 * SEP_NPB + 4 * pg + j]);
+          const double2 yz = cmul(Y[m2 * SEP_NPB + 8 * j + pg], Zt[m1 * SEP_NPB + 8 * j + pg]);
           acc[j] = cfma(s[j], yz, acc[j]);
         }
         m2 += rstep;
@@ -4203,7 +4211,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     // 3D Taylor tasks beyond the conversion kernels' orders, and the
     // plane-wave route: the direct separable evaluation for potentials
     const int nbig = P.dim == 3 ? D.eval_taylor_n - D.eval3_nsplit : 0;
-    const size_t sh_sep = ((size_t)(2 * P.npw + P.npw / 2) * SEP_NPB + 256 * 4) * 16;
+    const size_t sh_sep = ((size_t)(2 * P.npw + P.npw / 2) * SEP_NPB + 256 * 4) * 16 +
+                          (size_t)(D.eval_pmax + 1) * P.npw * 8;
     if (nbig > 0 && pgh == 1) {
       CK(cudaFuncSetAttribute(k_eval3d_sep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh_sep));
       k_eval3d_sep<true><<<dim3(nbig, nd), 256, sh_sep, st>>>(k, D.eval + D.eval3_nsplit);
