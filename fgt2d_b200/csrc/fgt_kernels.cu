@@ -2268,6 +2268,52 @@ __global__ void __launch_bounds__(256, 2) k_eval3d_sep(KP k, const EvalTask* __r
 // is staged in shared memory and each thread evaluates two points by Horner
 // in x along each row, then in y, then in z (g3dlevalp_vec,
 // g3drouts.f:1045-1107), plain FP64 FMAs at the exact order.
+// Horner over the planes and rows of a staged block for NPT points at once,
+// NR rows of a plane in flight (independent x chains: instruction-level
+// parallelism for leaves of few points), the rows then folded into the y
+// chain in row order: the same operations in the same order per point as
+// one row at a time.
+template <int NP2, int PGH, int NPT, int NR>
+__device__ __forceinline__ void horner3_block(const double2* lo3, int Pn, const double* x, const double* y,
+                                              const double* z, Hor3* a) {
+  for (int cc = Pn - 1; cc >= 0; cc--) {
+    Hor2 q[NPT];
+    for (int b = Pn - 1; b >= 0; b -= NR) {
+      double s[NR][NPT], u[NR][NPT], w[NR][NPT];
+      const double2* rw[NR];
+#pragma unroll
+      for (int r = 0; r < NR; r++) {
+        rw[r] = lo3 + (cc * Pn + (b - r >= 0 ? b - r : b)) * NP2;  // past row 0: a copy, not folded
+        const double2 ct = rw[r][NP2 - 1];
+#pragma unroll
+        for (int p = 0; p < NPT; p++) {
+          s[r][p] = ct.y;
+          u[r][p] = w[r][p] = 0.0;
+          hstep<PGH>(s[r][p], u[r][p], w[r][p], x[p], ct.x);
+        }
+      }
+#pragma unroll
+      for (int m = NP2 - 2; m >= 0; m--) {
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+          const double2 cf = rw[r][m];
+#pragma unroll
+          for (int p = 0; p < NPT; p++) hstep<PGH>(s[r][p], u[r][p], w[r][p], x[p], cf.y);
+#pragma unroll
+          for (int p = 0; p < NPT; p++) hstep<PGH>(s[r][p], u[r][p], w[r][p], x[p], cf.x);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < NR; r++)
+        if (b - r >= 0)
+#pragma unroll
+          for (int p = 0; p < NPT; p++) hrow<PGH>(q[p], y[p], s[r][p], u[r][p], w[r][p]);
+    }
+#pragma unroll
+    for (int p = 0; p < NPT; p++) hplane<PGH>(a[p], z[p], q[p]);
+  }
+}
+
 template <int NP2, int PGH>
 __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* __restrict__ tasks,
                                                        const double* __restrict__ lo_all) {
@@ -2284,38 +2330,29 @@ __global__ void __launch_bounds__(128) k_eval3d_horner(KP k, const HornerTask* _
   const double cx = k.centers[3 * T.box], cy = k.centers[3 * T.box + 1], cz = k.centers[3 * T.box + 2];
   const int ta = threadIdx.x, tb = threadIdx.x + 128;
   if (ta >= T.n) return;
-  const bool two = tb < T.n;
-  const int pa = T.i0 + ta, pb = T.i0 + (two ? tb : ta);
-  const double x0 = (pts[3 * pa] - cx) * k.dsq, y0 = (pts[3 * pa + 1] - cy) * k.dsq, z0 = (pts[3 * pa + 2] - cz) * k.dsq;
-  const double x1 = (pts[3 * pb] - cx) * k.dsq, y1 = (pts[3 * pb + 1] - cy) * k.dsq, z1 = (pts[3 * pb + 2] - cz) * k.dsq;
-  Hor3 a0, a1;
-  for (int cc = Pn - 1; cc >= 0; cc--) {
-    Hor2 q0, q1;
-    for (int b = Pn - 1; b >= 0; b--) {
-      const double2* rw = lo3 + (cc * Pn + b) * NP2;
-      const double2 ct = rw[NP2 - 1];
-      double s0 = ct.y, s1 = ct.y, u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
-      hstep<PGH>(s0, u0, w0, x0, ct.x);
-      hstep<PGH>(s1, u1, w1, x1, ct.x);
-#pragma unroll
-      for (int m = NP2 - 2; m >= 0; m--) {
-        const double2 cf = rw[m];
-        hstep<PGH>(s0, u0, w0, x0, cf.y);
-        hstep<PGH>(s1, u1, w1, x1, cf.y);
-        hstep<PGH>(s0, u0, w0, x0, cf.x);
-        hstep<PGH>(s1, u1, w1, x1, cf.x);
-      }
-      hrow<PGH>(q0, y0, s0, u0, w0);
-      hrow<PGH>(q1, y1, s1, u1, w1);
-    }
-    hplane<PGH>(a0, z0, q0);
-    hplane<PGH>(a1, z1, q1);
-  }
+  const int pa = T.i0 + ta;
   double v[NC];
-  hemit<PGH>(a0, k.dsq, v);
+  if (T.n <= 128) {
+    // one point per thread, four rows in flight
+    const double x = (pts[3 * pa] - cx) * k.dsq, y = (pts[3 * pa + 1] - cy) * k.dsq, z = (pts[3 * pa + 2] - cz) * k.dsq;
+    Hor3 a[1];
+    horner3_block<NP2, PGH, 1, 4>(lo3, Pn, &x, &y, &z, a);
+    hemit<PGH>(a[0], k.dsq, v);
+    add_out<NC>(out, pa, k.nd, nc, ind, v);
+    return;
+  }
+  // two points per thread, two rows in flight
+  const bool two = tb < T.n;
+  const int pb = T.i0 + (two ? tb : ta);
+  const double x[2] = {(pts[3 * pa] - cx) * k.dsq, (pts[3 * pb] - cx) * k.dsq};
+  const double y[2] = {(pts[3 * pa + 1] - cy) * k.dsq, (pts[3 * pb + 1] - cy) * k.dsq};
+  const double z[2] = {(pts[3 * pa + 2] - cz) * k.dsq, (pts[3 * pb + 2] - cz) * k.dsq};
+  Hor3 a[2];
+  horner3_block<NP2, PGH, 2, 2>(lo3, Pn, x, y, z, a);
+  hemit<PGH>(a[0], k.dsq, v);
   add_out<NC>(out, pa, k.nd, nc, ind, v);
   if (two) {
-    hemit<PGH>(a1, k.dsq, v);
+    hemit<PGH>(a[1], k.dsq, v);
     add_out<NC>(out, pb, k.nd, nc, ind, v);
   }
 }
