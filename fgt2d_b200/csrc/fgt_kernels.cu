@@ -3424,6 +3424,70 @@ size_t bytes_of(const std::vector<T>& v) {
 }
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Arrays placed one after another in the device arena (as put() does) and
+// copied up together: the host data is gathered, by the host threads, into
+// a pinned mirror of the arena range, which goes up in one asynchronous copy.
+// The mirror belongs to the calling thread and is reused; the caller
+// synchronises the stream before the thread stages again.
+struct Staged {
+  struct Item {
+    size_t off, bytes;
+    const void* src;
+  };
+  std::vector<Item> items;
+  size_t span = 0;
+  template <typename T>
+  void add(char*& cur, T*& dst, const std::vector<T>& v) {
+    dst = reinterpret_cast<T*>(cur);
+    const size_t b = v.size() * sizeof(T);
+    if (b) items.push_back({span, b, v.data()});
+    span += (b + 255) & ~size_t(255);
+    cur += (b + 255) & ~size_t(255);
+  }
+  cudaError_t upload(char* dev, cudaStream_t s) {
+    if (span == 0) return cudaSuccess;
+    struct Mirror {
+      char* p = nullptr;
+      size_t cap = 0;
+      ~Mirror() {
+        if (p) cudaFreeHost(p);
+      }
+    };
+    thread_local Mirror m;
+    if (m.cap < span) {
+      if (m.p) cudaFreeHost(m.p);
+      m.p = nullptr;
+      m.cap = 0;
+      const size_t want = span + span / 4;
+      cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&m.p), want, cudaHostAllocPortable);
+      if (e != cudaSuccess) {
+        m.p = nullptr;
+        (void)cudaGetLastError();
+        // no pinned memory: the arrays go up one by one from where they are
+        for (const Item& it : items) {
+          e = cudaMemcpyAsync(dev + it.off, it.src, it.bytes, cudaMemcpyHostToDevice, s);
+          if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+      }
+      m.cap = want;
+    }
+    // copy in 1 MB pieces so that large arrays are split over the threads
+    // (the mirror's address is taken here: m is the calling thread's own)
+    char* const mirror = m.p;
+    std::vector<std::pair<size_t, size_t>> pieces;  // (item, piece offset)
+    for (size_t i = 0; i < items.size(); i++)
+      for (size_t o = 0; o < items[i].bytes; o += (1 << 20)) pieces.push_back({i, o});
+#pragma omp parallel for schedule(dynamic, 1) if (span > (4u << 20))
+    for (long long q = 0; q < (long long)pieces.size(); q++) {
+      const Item& it = items[pieces[q].first];
+      const size_t o = pieces[q].second, n = std::min<size_t>(1 << 20, it.bytes - o);
+      memcpy(mirror + it.off + o, static_cast<const char*>(it.src) + o, n);
+    }
+    return cudaMemcpyAsync(dev, mirror, span, cudaMemcpyHostToDevice, s);
+  }
+};
+
 
 }  // namespace
 
@@ -3438,6 +3502,19 @@ size_t form3_simt_smem(int Pn_, int npw) {
   const size_t Pn = Pn_, n2 = npw / 2, P3 = Pn * Pn * Pn;
   const size_t szA = std::max(P3, 2 * Pn * npw * n2);
   return (((szA + 1) & ~size_t(1)) + 2 * Pn * Pn * n2 + Pn * npw) * 8;
+}
+// Stable sort of tasks by (route, order): a counting sort (the keys are few
+// small integers), linear in the number of tasks.
+template <typename Task>
+std::vector<Task> route_order_sort(const std::vector<Task>& in) {
+  int kmax = 0;
+  for (const Task& t : in) kmax = std::max(kmax, 4096 * t.route + t.p);
+  std::vector<int> cnt((size_t)kmax + 2, 0);
+  for (const Task& t : in) cnt[4096 * t.route + t.p + 1]++;
+  for (size_t i = 1; i < cnt.size(); i++) cnt[i] += cnt[i - 1];
+  std::vector<Task> out(in.size());
+  for (const Task& t : in) out[cnt[4096 * t.route + t.p]++] = t;
+  return out;
 }
 // Whether the 3D Hermite form of order Pn runs on the shared-memory kernels:
 // k_form3d_mma's staging ((8 ceil(P/8) + 2 P) power rows of 68 doubles) and
@@ -3485,19 +3562,14 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev));
   // order form and eval tasks by route so each kernel gets a contiguous range
-  std::vector<FormTask> form = H.form;
-  std::stable_sort(form.begin(), form.end(), [](const FormTask& a, const FormTask& b) {
-    return a.route != b.route ? a.route < b.route : a.p < b.p;
-  });
+  // (then by order; stable)
+  const std::vector<FormTask> form = route_order_sort(H.form);
   D.nform = (int)form.size();
   for (auto& f : form) {
     (f.route == ROUTE_PW ? D.form_pw_n : D.form_hermite_n)++;
     if (f.route == ROUTE_HERMITE) D.form_pmax = std::max(D.form_pmax, f.p);
   }
-  std::vector<EvalTask> ev = H.eval;
-  std::stable_sort(ev.begin(), ev.end(), [](const EvalTask& a, const EvalTask& b) {
-    return a.route != b.route ? a.route < b.route : a.p < b.p;
-  });
+  const std::vector<EvalTask> ev = route_order_sort(H.eval);
   D.neval = (int)ev.size();
   for (auto& e : ev) {
     (e.route == ROUTE_PW ? D.eval_pw_n : D.eval_taylor_n)++;
@@ -3787,21 +3859,28 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     CK(put(cur, D.cfac, cfac, s));
     CK(cudaStreamSynchronize(s));
   }
-  CK(put(cur, D.form, form, s));
-  CK(put(cur, D.mgroups, groups, s));
-  CK(put(cur, D.merge, H.merge, s));
-  CK(put(cur, D.split, H.split, s));
-  CK(put(cur, D.m2l, H.m2l, s));
-  CK(put(cur, D.m2l_nbr, H.m2l_nbr, s));
-  CK(put(cur, D.eval, ev, s));
-  CK(put(cur, D.dir, H.dir, s));
-  CK(put(cur, D.dir_src, H.dir_src, s));
-  CK(put(cur, D.fchunks, fchunks, s));
-  CK(put(cur, D.fcbeg, fcbeg, s));
-  CK(put(cur, D.form_hoff, form_hoff, s));
-  CK(put(cur, D.tables, tables, s));
-  CK(put(cur, D.conv, conv, s));
-  CK(put(cur, D.horner, horner, s));
+  {
+    // the task arrays, laid out in the arena as they come, go up in one copy
+    // from a pinned mirror of that range (filled by the host threads)
+    char* const b0 = cur;
+    Staged st;
+    st.add(cur, D.form, form);
+    st.add(cur, D.mgroups, groups);
+    st.add(cur, D.merge, H.merge);
+    st.add(cur, D.split, H.split);
+    st.add(cur, D.m2l, H.m2l);
+    st.add(cur, D.m2l_nbr, H.m2l_nbr);
+    st.add(cur, D.eval, ev);
+    st.add(cur, D.dir, H.dir);
+    st.add(cur, D.dir_src, H.dir_src);
+    st.add(cur, D.fchunks, fchunks);
+    st.add(cur, D.fcbeg, fcbeg);
+    st.add(cur, D.form_hoff, form_hoff);
+    st.add(cur, D.tables, tables);
+    st.add(cur, D.conv, conv);
+    st.add(cur, D.horner, horner);
+    CK(st.upload(b0, s));
+  }
   D.lo = reinterpret_cast<double*>(cur); cur += al(lo_doubles * 8);
   D.hbuf = reinterpret_cast<double*>(cur); cur += al(hbuf_doubles * 8);
   D.mp = reinterpret_cast<double2*>(cur); cur += al((size_t)H.nmp * nd * P.nexp * 16);
