@@ -110,6 +110,11 @@ struct DevicePlan {
   double* nsort = nullptr;  // sorted dipole directions (ns, dim), dipole plans only
   double* dsort = nullptr;  // sorted dipole strengths (ns, nd), dipole plans only
   double* tsort = nullptr;  // sorted targets (nt, dim)
+  // the mixed near field's coordinates: (x - cen0) sqrt(log2 e / delta) split
+  // into FP32 (hi, lo) pairs, per point [dim][2], sorted order (plans with a
+  // near field and no dipoles; null otherwise)
+  float* fsrc = nullptr;
+  float* ftrg = nullptr;
   double* psort = nullptr;  // sorted source outputs, per point [out_comps(dim, ifpgh)][nd]
   double* ptsort = nullptr; // sorted target outputs, per point [out_comps(dim, ifpghtarg)][nd]
   double* local0 = nullptr; // large-delta local expansion

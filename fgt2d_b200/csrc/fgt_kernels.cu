@@ -57,6 +57,8 @@ struct KP {
   int ifcharge, ifdipole;
   const double* dnrm;  // sorted dipole directions (ns, dim)
   const double* dstr;  // sorted dipole strengths (ns, nd)
+  const float* fsrc;   // mixed near field: scaled coordinates as FP32 (hi, lo), [dim][2] per point
+  const float* ftrg;
 };
 
 // Source weights of density ind at sorted source i: the charge (0 without
@@ -3090,11 +3092,26 @@ __global__ void __launch_bounds__(128) k_direct(KP k, const DirTask* __restrict_
   if (act && sub == 0) add_out<NC>(out, ip, k.nd, nc, ind, acc);
 }
 
+// Scaled coordinates of the mixed near field, once per plan: (x - c) cs with
+// c the root box's centre, as an FP32 pair (hi, lo) per dimension.
+__global__ void k_mixed_coords(const double* __restrict__ x, int n, int dim, double c0, double c1, double c2,
+                               double cs, float* __restrict__ f) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int d = 0; d < dim; d++) {
+      const double v = (x[(size_t)dim * i + d] - (d == 0 ? c0 : d == 1 ? c1 : c2)) * cs;
+      const float h = (float)v;
+      f[(size_t)2 * dim * i + 2 * d] = h;
+      f[(size_t)2 * dim * i + 2 * d + 1] = (float)(v - (double)h);
+    }
+}
+
 // Mixed form of the near field (eps >= 1e-6): the same task structure with
-// the pair arithmetic in FP32.  Coordinates are taken relative to the task's
-// first target, scaled by sqrt(log2(e) / delta) and split into a float pair
-// (hi, lo), so dx = (t_hi - s_hi) + (t_lo - s_lo) carries about FP32 relative
-// accuracy in dx itself (not in the coordinates); the Gaussian is then
+// the pair arithmetic in FP32.  Coordinates are taken relative to the root
+// box's centre, scaled by sqrt(log2(e) / delta) and split into a float pair
+// (hi, lo) once per plan (k_mixed_coords), so dx = (t_hi - s_hi) + (t_lo -
+// s_lo) carries about FP32 relative accuracy in dx itself (the hi parts of
+// nearby points subtract exactly; the lo parts hold the rest to 2^-48 of the
+// coordinate); the Gaussian is then
 // 2^-(dx^2 + dy^2 (+ dz^2)) by ex2.approx.  Each lane holds NTL = 4 targets,
 // so a staged source is read from shared memory once for four pairs; g lanes
 // per target group (g * groups <= 32) split the sources.  Groups of four
@@ -3124,12 +3141,9 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
   while (g * 2 * ngr <= 32) g *= 2;
   const int tt = lane / g, sub = lane - tt * g;
   const bool act = tt < ngr;
-  const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
   const int nc = T.set ? k.nc_t : k.nc_s;
-  double o[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; d++) o[d] = pts[DIM * T.i0 + d];
+  const float* fp = T.set ? k.ftrg : k.fsrc;  // the points' FP32 (hi, lo) coordinates
   float th[NTL][DIM], tl[NTL][DIM];
   double acc[NTL][NC];
 #pragma unroll
@@ -3139,9 +3153,8 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
     const int it = min(tt * NTL + v, T.n - 1);
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      const double x = (pts[DIM * (T.i0 + it) + d] - o[d]) * cs;
-      th[v][d] = (float)x;
-      tl[v][d] = (float)(x - (double)th[v][d]);
+      th[v][d] = fp[(size_t)2 * DIM * (T.i0 + it) + 2 * d];
+      tl[v][d] = fp[(size_t)2 * DIM * (T.i0 + it) + 2 * d + 1];
     }
   }
   for (int rc = 0; rc < T.cnt; rc += 32) {
@@ -3159,10 +3172,9 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
         const int j = js[u];
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          const double x = (k.src[DIM * j + d] - o[d]) * cs;
-          const float h = (float)x;
-          sh[d * CAP + t] = h;
-          sl[d * CAP + t] = (float)(x - (double)h);
+          const float2 hl = reinterpret_cast<const float2*>(k.fsrc)[(size_t)DIM * j + d];
+          sh[d * CAP + t] = hl.x;
+          sl[d * CAP + t] = hl.y;
         }
         sq[t] = (float)k.chg[(size_t)j * k.nd + ind];
       }
@@ -3769,6 +3781,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     D.conv3_ctas = D.sm_count * 4;
   }
   size_t ns = P.ns, nt = P.nt, nd = P.nd, dim = P.dim;
+  // FP32 coordinates of the mixed near field (charges only)
+  const bool fmix = D.ndir > 0 && !P.ifdipole;
   // diagonal translation tables (formed on the device)
   const size_t n_wms = P.all_direct ? 0 : (size_t)(P.nlevels + 1) * D.nch * P.nexp;
   const size_t n_wsh = P.all_direct ? 0 : (size_t)(P.dim == 2 ? 9 : 27) * P.nexp;
@@ -3779,6 +3793,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
                  al(nt * dim * 8) + al(ns * nd * out_comps(dim, P.ifpgh) * 8) +
+                 (fmix ? al(ns * dim * 8) + al((P.ifpghtarg > 0 ? nt : 0) * dim * 8) : 0) +
                  al(P.ifdipole ? ns * dim * 8 : 0) + al(P.ifdipole ? ns * nd * 8 : 0) +
                  al(nt * nd * out_comps(dim, P.ifpghtarg) * 8) +
                  al((size_t)D.scratch_ctas * D.scratch_per_cta * 16) + bytes_of(fchunks) +
@@ -3890,6 +3905,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.nsort = reinterpret_cast<double*>(cur); cur += al(P.ifdipole ? ns * dim * 8 : 0);
   D.dsort = reinterpret_cast<double*>(cur); cur += al(P.ifdipole ? ns * nd * 8 : 0);
   D.tsort = reinterpret_cast<double*>(cur); cur += al(nt * dim * 8);
+  if (fmix) {
+    D.fsrc = reinterpret_cast<float*>(cur); cur += al(ns * dim * 8);
+    D.ftrg = reinterpret_cast<float*>(cur); cur += al((P.ifpghtarg > 0 ? nt : 0) * dim * 8);
+  }
   D.psort = reinterpret_cast<double*>(cur); cur += al(ns * nd * out_comps(dim, P.ifpgh) * 8);
   D.ptsort = reinterpret_cast<double*>(cur); cur += al(nt * nd * out_comps(dim, P.ifpghtarg) * 8);
   D.scratch = reinterpret_cast<double2*>(cur); cur += al((size_t)D.scratch_ctas * D.scratch_per_cta * 16);
@@ -3924,6 +3943,8 @@ static KP make_kp(const DevicePlan& D) {
   k.ifdipole = P.ifdipole;
   k.dnrm = D.nsort;
   k.dstr = D.dsort;
+  k.fsrc = D.fsrc;
+  k.ftrg = D.ftrg;
   return k;
 }
 
@@ -3950,6 +3971,13 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
   if (P.nt > 0 && P.ifpghtarg > 0) {
     const int vec = (reinterpret_cast<uintptr_t>(trg) & 15) == 0;
     k_gather_pts<<<gb, 256, 0, st>>>(trg, nullptr, D.tsort, nullptr, D.itarg, P.nt, P.dim, P.nd, vec);
+  }
+  if (D.fsrc) {
+    const double cs = std::sqrt(1.4426950408889634 / P.delta);
+    if (P.ns > 0)
+      k_mixed_coords<<<gb, 256, 0, st>>>(D.ssort, P.ns, P.dim, P.cen0[0], P.cen0[1], P.cen0[2], cs, D.fsrc);
+    if (P.nt > 0 && P.ifpghtarg > 0)
+      k_mixed_coords<<<gb, 256, 0, st>>>(D.tsort, P.nt, P.dim, P.cen0[0], P.cen0[1], P.cen0[2], cs, D.ftrg);
   }
   return cudaGetLastError();
 }
