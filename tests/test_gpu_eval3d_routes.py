@@ -49,3 +49,18 @@ def test_eval3d_routes(case, pgh, fgt, oracle):
             print(f"{name} pgh={pgh} {k}: vs oracle {e_ref:.2e} vs direct {e_dir:.2e} (oracle {e_orc:.2e})")
             assert e_ref <= 1e-2 * eps, (k, e_ref)
             assert e_dir <= max(10 * eps, 2 * e_orc), (k, e_dir, e_orc)
+
+
+def test_eval3d_routes_two_densities(fgt, oracle):
+    """Two densities through the same routes (the kernels' density index)."""
+    rng = np.random.default_rng(41)
+    box = lambda n, s, o=0.0: o + rng.random((n, 3)) * s
+    src = np.r_[box(6000, 0.2), box(3000, 0.05, 0.05)]
+    q = rng.random((src.shape[0], 2)) - 0.5
+    trg = rng.random((2000, 3)) * 0.2
+    got = fgt.transform_pgh(3, 2, 1.41e-4, 1e-9, src, q, trg, 1, 1, ctx=fgt.Context(0, precision="fp64"))
+    ref = oracle.fgt_pgh(3, 2, 1.41e-4, 1e-9, src, q, trg, 1, 1)
+    for k in ("pot", "pottarg"):
+        e = oracle.derr(ref[k], got[k])
+        print(k, e)
+        assert e <= 1e-11, (k, e)
