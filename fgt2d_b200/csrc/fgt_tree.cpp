@@ -125,11 +125,30 @@ struct Builder {
 
   // computecoll, tree_routs4.f:100-211, levels [l0, l1]
   // colleagues of box b at level l from its parent's list, into (nc, co)
+  // The children of a refined box share their coordinate along d with every
+  // sibling on the same side of d, so the test is made once per side and
+  // dimension (child 0 and child 2^d) and a child passes when its sides do;
+  // a box with a missing child takes the test child by child.
   void colleagues_box(int b, double lim, std::vector<int>& nc, std::vector<int>& co) {
     int dad = t.parent[b];
     int n = 0;
     for (int i = 0; i < nc[dad]; i++) {
       int jb = co[(size_t)dad * NCO + i];
+      if (CH(jb, 0) < 0 && t.nchild[jb] == 0) continue;
+      bool all = true;
+      for (int j = 0; j < NCH; j++) all = all && CH(jb, j) >= 0;
+      if (all) {
+        unsigned pass[2] = {0u, 0u};  // bit d: side 0 / side 1 of dimension d is near
+        for (int d = 0; d < D; d++) {
+          if (std::fabs(C(CH(jb, 0), d) - C(b, d)) <= lim) pass[0] |= 1u << d;
+          if (std::fabs(C(CH(jb, 1 << d), d) - C(b, d)) <= lim) pass[1] |= 1u << d;
+        }
+        for (int j = 0; j < NCH; j++) {
+          const unsigned ok = (pass[1] & (unsigned)j) | (pass[0] & ~(unsigned)j);
+          if ((ok & ((1u << D) - 1)) == (1u << D) - 1) co[(size_t)b * NCO + n++] = CH(jb, j);
+        }
+        continue;
+      }
       for (int j = 0; j < NCH; j++) {
         int kb = CH(jb, j);
         if (kb < 0) continue;
@@ -143,7 +162,7 @@ struct Builder {
   }
   void colleagues_level(int l) {
     double lim = F105 * t.boxsize[l];
-#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 512)
     for (int b = t.lfirst[l]; b <= t.llast[l]; b++) colleagues_box(b, lim, t.ncoll, t.coll);
   }
   // After a refinement pass and its reorg (map: id before -> id after; the
@@ -169,7 +188,7 @@ struct Builder {
     for (int r : refined_ids) refd[map[r]] = 1;
     for (int l = 1; l <= t.nlevels; l++) {
       const double lim = F105 * t.boxsize[l];
-#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 512)
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
         if (fresh[b] || mark[b]) colleagues_box(b, lim, nc, co);
       // old boxes of level l + 1 whose parent has a refined colleague
