@@ -3458,19 +3458,24 @@ struct Staged {
   }
   cudaError_t upload(char* dev, cudaStream_t s) {
     if (span == 0) return cudaSuccess;
+    // A mirror that grows keeps its old buffers until the thread exits:
+    // cudaFreeHost waits for the whole device, which would stall this
+    // request behind every other stream's work (the server's workers).
     struct Mirror {
       char* p = nullptr;
       size_t cap = 0;
+      std::vector<char*> old;
       ~Mirror() {
         if (p) cudaFreeHost(p);
+        for (char* q : old) cudaFreeHost(q);
       }
     };
     thread_local Mirror m;
     if (m.cap < span) {
-      if (m.p) cudaFreeHost(m.p);
+      if (m.p) m.old.push_back(m.p);
       m.p = nullptr;
+      const size_t want = std::max(std::max(span + span / 4, 2 * m.cap), (size_t)16 << 20);
       m.cap = 0;
-      const size_t want = span + span / 4;
       cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&m.p), want, cudaHostAllocPortable);
       if (e != cudaSuccess) {
         m.p = nullptr;
