@@ -1091,6 +1091,9 @@ struct fgt_server {
   int device = 0;
   long long budget = 0, budget_pts = 0, budget_plan = 0;
   std::vector<fgt_ctx*> ctxs;
+  // per worker, a stream of the device's highest priority for small requests
+  // (their blocks are dispatched ahead of large requests' when SMs free up)
+  std::vector<cudaStream_t> hi;
   std::vector<std::thread> workers;
   std::mutex mu;
   std::condition_variable cv_q, cv_mem, cv_done;
@@ -1114,6 +1117,7 @@ struct fgt_server {
 
 namespace {
 constexpr double kServerAgeS = 0.05;
+constexpr long long kServerSmall = 100000;  // points of a request on the high-priority stream
 
 long long request_points(const fgt_request& r) {
   return (r.ifpgh >= 1 ? r.ns : 0) + (r.ifpghtarg >= 1 && r.targ ? r.nt : 0);
@@ -1222,6 +1226,9 @@ void server_worker(fgt_server* S, int w) {
       J->t_start = t;
       S->running++;
     }
+    // small requests run on the worker's high-priority stream
+    const cudaStream_t base = ctx->stream;
+    if ((long long)J->r.ns + (J->r.targ ? J->r.nt : 0) <= kServerSmall && S->hi[w]) ctx->stream = S->hi[w];
     int st = server_run(S, ctx, J->r);
     for (int retry = 0; st == FGT_ERR_NOMEM && retry < 50; retry++) {
       // the device memory is held (or fragmented) by requests in flight:
@@ -1236,6 +1243,7 @@ void server_worker(fgt_server* S, int w) {
       }
       st = server_run(S, ctx, J->r);
     }
+    ctx->stream = base;
     {
       std::lock_guard<std::mutex> lk(S->mu);
       S->running--;
@@ -1293,6 +1301,19 @@ int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_
       CKS(cudaStreamSynchronize(s));
     } else {
       (void)cudaGetLastError();
+    }
+  }
+  {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) greatest = least = 0;
+    for (int w = 0; w < nworkers; w++) {
+      cudaStream_t h = nullptr;
+      if (greatest == least ||
+          cudaStreamCreateWithPriority(&h, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+        (void)cudaGetLastError();
+        h = nullptr;  // no priorities: small requests share the worker's stream
+      }
+      S->hi.push_back(h);
     }
   }
   fgt_server* raw = S.release();
@@ -1379,6 +1400,8 @@ int fgt_server_destroy(fgt_server* s) {
   }
   for (auto& t : s->workers) t.join();
   for (auto& kv : s->jobs) delete kv.second;
+  for (cudaStream_t h : s->hi)
+    if (h) cudaStreamDestroy(h);
   for (fgt_ctx* c : s->ctxs) fgt_ctx_destroy(c);
   delete s;
   return FGT_OK;
