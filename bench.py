@@ -1,8 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the B200 plane-wave FGT on its headline workload.
 
-Metric: FGT points/s at eps = 1e-6 (mixed form; the FP64 plain form is timed
-beside it on the same GPU).  Workload (default): the 2D strongly clustered
+Metric: FGT points/s at eps = 1e-6 (the mixed form; the FP64 plain form is
+timed beside it on the same GPU, key ``fp64_form``).  Workload (default): the 2D strongly clustered
 adaptive-tree case -- N = 1e7 sources = targets, 90% on a circle of radius 0.3
 about (0.5, 0.5) with Gaussian radial jitter sigma = 1e-3, 10% uniform in the
 unit square, charges N(0,1), delta = 1e-6, eps = 1e-6, potential at the
@@ -12,7 +12,9 @@ points/s = (ns + targets evaluated) / time.  ``value`` times one execute of a
 prebuilt plan with inputs resident in HBM (gather -> form -> merge -> mp->loc
 -> split -> eval -> near field -> scatter); ``e2e`` times the drop-in call
 (host tree and lists, host->device copies from pinned memory, transform,
-device->host copy of the potentials).
+device->host copy of the potentials).  ``errors`` gives the relative l2 error
+(the reference driver's ``derr``) of the timed outputs against an FP64 direct
+sum at 1e4 sampled points and against the oracle on the whole workload.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--workload cfg2|cfg1|cfg3|cfg4_d1e-2_e1e-6|...]
@@ -214,51 +216,106 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
-def run_oracle(w, nthreads, sample_n=None, seed=0):
+METRIC = "FGT points/s at eps 1e-6"
+N_ERR_SAMPLE = 10_000  # targets of the sampled-target error against the FP64 direct sum
+
+
+def config_of(w):
+    """The workload's config object, identical in both arms."""
+    return {"workload": w["name"], "dim": w["dim"], "points_per_step": points_of(w),
+            "ns": int(w["src"].shape[0]), "nt": int(w["trg"].shape[0]), "delta": w["delta"],
+            "eps": w["eps"], "ifpgh": w["ifpgh"], "ifpghtarg": w["ifpghtarg"],
+            "l2": "inputs larger than the 126 MB L2 (no flush)"}
+
+
+def slab_sample(w, frac=1.0 / 16):
+    """The points with x below the `frac` quantile of the sources' x: a
+    spatially contiguous piece of the workload.  Unlike a random subset it
+    keeps the local density (near-field pairs per point, leaf sizes) and the
+    root box size (set by the largest extent), so its per-point cost stands
+    for the whole workload's."""
+    xs = w["src"][:, 0]
+    a = float(np.quantile(xs, frac))
+    si = xs < a
+    out = dict(w)
+    out["src"], out["chg"] = w["src"][si], w["chg"][si]
+    out["trg"] = out["src"] if w["trg"] is w["src"] else w["trg"][w["trg"][:, 0] < a]
+    out["slab_x"] = a
+    return out
+
+
+def run_oracle(w, nthreads):
+    """One oracle transform of workload `w`: (points, seconds, pot, pottarg)."""
     from oracle import oracle as O
     O.build()
-    src, chg, trg = w["src"], w["chg"], w["trg"]
-    if sample_n is not None and sample_n < src.shape[0]:
-        rng = np.random.default_rng(seed)
-        idx = rng.choice(src.shape[0], sample_n, replace=False)
-        same = trg is src
-        src, chg = src[idx], chg[idx]
-        trg = src if same else trg[rng.choice(trg.shape[0], min(sample_n, trg.shape[0]), replace=False)]
     t0 = time.perf_counter()
-    O.fgt(w["dim"], w["nd"], w["delta"], w["eps"], src, chg, trg, w["ifpgh"], w["ifpghtarg"],
-          nthreads=nthreads)
+    pot, pt, _ = O.fgt(w["dim"], w["nd"], w["delta"], w["eps"], w["src"], w["chg"], w["trg"],
+                       w["ifpgh"], w["ifpghtarg"], nthreads=nthreads)
     dt = time.perf_counter() - t0
-    pts = src.shape[0] * (1 if w["ifpgh"] else 0) + (trg.shape[0] if w["ifpghtarg"] else 0)
-    return pts, dt, src.shape[0]
+    return points_of(w), dt, pot, pt
+
+
+def error_sample(w, seed=99):
+    """Sampled evaluation points (1e4, or all when fewer) with the FP64
+    direct sum at them: (which, idx, exact), which = "pot" or "pottarg"."""
+    from oracle import oracle as O
+    O.build()
+    rng = np.random.default_rng(seed)
+    if w["ifpghtarg"]:
+        which, pts = "pottarg", w["trg"]
+    else:
+        which, pts = "pot", w["src"]
+    idx = np.sort(rng.choice(pts.shape[0], min(N_ERR_SAMPLE, pts.shape[0]), replace=False))
+    exact = O.direct_cut(w["dim"], w["nd"], w["delta"], w["src"], w["chg"].reshape(-1, w["nd"]),
+                         pts[idx])
+    return which, idx, exact
+
+
+def derr(a, b):
+    from oracle import oracle as O
+    return float(O.derr(a, b))
 
 
 # ------------------------------------------------------------------ arms
 def reference_arm(args, w, rank, world):
+    """The reference's CPU path (the oracle port: no Fortran compiler exists on
+    either machine, so the reference itself cannot be built) on the full
+    workload, all host threads, one transform per step."""
     if rank != 0:
         return 0
     cores = cpu_cores()
-    sample = min(2_000_000, w["src"].shape[0])
     for i in range(args.warmup):
-        run_oracle(w, cores, sample, seed=i)
+        run_oracle(w, cores)
     times, pts = [], 0
     for i in range(args.steps):
-        p, dt, _ = run_oracle(w, cores, sample, seed=100 + i)
+        p, dt, _, _ = run_oracle(w, cores)
         times.append(dt)
         pts = p
     ms = 1e3 * sum(times) / len(times)
     v = pts / (ms / 1e3)
-    line = {"impl": "reference", "metric": "FGT points/s at eps 1e-6", "value": v,
+    one = single_thread_baseline(w) if not args.no_cpu_baseline else None
+    line = {"impl": "reference", "metric": METRIC, "value": v,
             "unit": "points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded numpy)",
-            "config": {"workload": w["name"], "sample_points": sample, "eps": w["eps"],
-                       "delta": w["delta"]},
+            "config": config_of(w),
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
-                             "sample": f"random {sample}-point subset of the workload per step, "
-                                       f"oracle (C++ restatement of the reference) on {cores} threads"},
+                             "sample": f"the full workload each step ({w['src'].shape[0]} sources), "
+                                       f"oracle (C++ restatement of the reference) on {cores} threads",
+                             "single_thread": one},
             "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def single_thread_baseline(w):
+    """The oracle on one thread (the reference's default build, OMP=OFF) over
+    a contiguous slab holding 1/16 of the points, so the run takes seconds."""
+    sw = slab_sample(w)
+    p, dt, _, _ = run_oracle(sw, 1)
+    return {"value": p / dt, "unit": "points/s", "cores": 1, "kind": "port", "seconds": dt,
+            "sample": f"slab x < {sw['slab_x']:.4f} of the workload ({sw['src'].shape[0]} sources, "
+                      f"{p} points evaluated): same local density and root box as the full run"}
 
 
 def ours_arm(args, w, rank, world, local_rank):
@@ -270,10 +327,11 @@ def ours_arm(args, w, rank, world, local_rank):
     pts = points_of(w)
     dim, nd = w["dim"], w["nd"]
 
-    # plan (host tree + lists + device tasks), built once per precision
-    ctx = {p: F.Context(dev, precision=p) for p in ("mixed", "fp64")}
+    # plan (tree + lists + device tasks), built once; the context's precision
+    # selects the form at each execute
+    ctx = F.Context(dev, precision="mixed")
     t0 = time.perf_counter()
-    plan = F.Plan(ctx["mixed"], dim, nd, w["delta"], w["eps"], w["src"], w["trg"], w["ifpgh"],
+    plan = F.Plan(ctx, dim, nd, w["delta"], w["eps"], w["src"], w["trg"], w["ifpgh"],
                   w["ifpghtarg"])
     plan_s = time.perf_counter() - t0
     info = plan.info()
@@ -287,13 +345,13 @@ def ours_arm(args, w, rank, world, local_rank):
     sp = stream.cuda_stream
 
     def step(precision):
-        ctx["mixed"].set_precision(precision)
+        ctx.set_precision(precision)
         plan.execute_device(d_src.data_ptr(), d_chg.data_ptr(), d_trg.data_ptr(),
                             d_pot.data_ptr(), d_pt.data_ptr(), stream=sp)
 
     from fgt2d_b200.replicas import barrier, max_over_ranks
 
-    results = {}
+    results, outputs = {}, {}
     clocks = None
     for prec in ("fp64", "mixed"):  # mixed last: its clocks are the headline's
         for _ in range(args.warmup):
@@ -315,11 +373,14 @@ def ours_arm(args, w, rank, world, local_rank):
             clocks = sampler.stop()
         ms = e0.elapsed_time(e1) / args.steps
         results[prec] = max_over_ranks(ms)
+        # the last timed step's outputs, for the errors below
+        outputs[prec] = (d_pot.cpu().numpy().copy() if w["ifpgh"] else None,
+                         d_pt.cpu().numpy().copy() if w["ifpghtarg"] else None)
     # per-stage device times (CUDA events around each stage, on the plan's
     # stream) over K further steps of each precision
     stages = {}
     for prec in ("fp64", "mixed"):
-        ctx["mixed"].set_precision(prec)
+        ctx.set_precision(prec)
         acc = {}
         for _ in range(args.steps):
             s = plan.profile_device(d_src.data_ptr(), d_chg.data_ptr(), d_trg.data_ptr(),
@@ -341,16 +402,16 @@ def ours_arm(args, w, rank, world, local_rank):
     if w["ifpghtarg"]:
         out_h["pottarg"] = torch.zeros((w["trg"].shape[0], nd), dtype=torch.float64).pin_memory().numpy()
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
-    ctx["mixed"].set_precision("mixed")
+    ctx.set_precision("mixed")
     e2e_s = float("nan")
     if e2e_steps:
         F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"], w["ifpghtarg"],
-                    ctx=ctx["mixed"], out=out_h)
+                    ctx=ctx, out=out_h)
         barrier()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             F.transform(dim, nd, w["delta"], w["eps"], src_h, chg_h, trg_h, w["ifpgh"],
-                        w["ifpghtarg"], ctx=ctx["mixed"], out=out_h)
+                        w["ifpghtarg"], ctx=ctx, out=out_h)
         e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
     h2d = src_h.nbytes + chg_h.nbytes + (trg_h.nbytes if w["ifpghtarg"] else 0)
     d2h = (w["src"].shape[0] * nd * 8 if w["ifpgh"] else 0) + (w["trg"].shape[0] * nd * 8 if w["ifpghtarg"] else 0)
@@ -358,62 +419,94 @@ def ours_arm(args, w, rank, world, local_rank):
     if rank != 0:
         return 0
     hbm, tf, peak_src = measured_peaks()
-    fp64_tf = ctx["mixed"].fp64_mma_tflops()
-    # roofline of the dominant tensor-core launch (the Hermite-block MMA kernel
-    # of the largest form order group), timed with CUDA events around that
-    # launch alone over K further executes on the plan's stream
-    ctx["mixed"].set_precision("mixed")
-    dms, dfl, dname = [], 0.0, None
+    fp64_tf = ctx.fp64_mma_tflops()
+    # roofline of the dominant tensor-core launch (the Hermite-block kernel of
+    # the form order group with the most sources), timed with CUDA events
+    # around that launch alone over K further executes on the plan's stream
+    ctx.set_precision("mixed")
+    dms, dfl, dalg, dname = [], 0.0, 0.0, None
     for _ in range(args.steps):
         r = plan.profile_dominant(d_chg.data_ptr(), d_pot.data_ptr(), d_pt.data_ptr())
         if r is None:
             break
         dms.append(r[0])
-        dfl, dname = r[1], r[2]
+        dfl, dname, dalg = r[1], r[2], r[3]
     if dms:
         t_k = sum(dms) / len(dms) / 1e3
-        ach = dfl / t_k / 1e12
+        ach = dalg / t_k / 1e12
         traffic, tsrc = PROFILED_TRAFFIC.get((w["name"], dname), (None, None))
         roof = {"bound": "tensor", "kernel": dname, "stage": "form", "achieved": ach, "peak": tf,
                 "unit": "TFLOP/s", "frac": ach / tf, "traffic": traffic,
-                "peak_source": f"{peak_src} bf16 dense (burst); the kernel runs FP64 m8n8k4 MMA",
-                "fp64_mma_peak_measured": fp64_tf, "frac_of_fp64_mma": ach / fp64_tf,
+                "peak_source": f"{peak_src} bf16 dense (burst), MEASURED_PEAKS.json",
+                "work": f"{dalg:.4g} algorithmic flops per launch = 4 n npw^d nd over the "
+                        f"launch's n sources (plane-wave form count)",
                 "launch_ms": t_k * 1e3,
-                "work": f"{dfl:.4g} flops per launch = 2 n P^d over the group's sources"}
+                "executed_flops": dfl, "executed_tflops": dfl / t_k / 1e12,
+                "fp64_mma_peak_probe_tflops": fp64_tf,
+                "executed_frac_of_fp64_mma": dfl / t_k / 1e12 / fp64_tf}
         if tsrc:
             roof["traffic_source"] = tsrc
     else:
         roof = {"bound": "tensor", "kernel": None, "achieved": None, "peak": tf, "unit": "TFLOP/s",
                 "frac": None, "traffic": None, "note": "no tensor-core launch in this plan"}
     sb = info["shift_bytes"]
+    t_b = (stage.get("merge", 0) + stage.get("m2l", 0) + stage.get("split", 0)) / 1e3
+    roof_b = None
+    if t_b > 0:
+        gbs = (sb[0] + sb[1] + sb[2]) / t_b / 1e9
+        roof_b = {"bound": "hbm", "stage": "shifts (merge + mp->loc + split)", "achieved": gbs,
+                  "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                  "work": f"{sb[0] + sb[1] + sb[2]:.4g} bytes per step: 16 B per complex "
+                          f"coefficient, each distinct expansion read or written once per stage",
+                  "stage_ms": t_b * 1e3}
     stage_rates = {
-        "form_tflops": info["form_route_flops"] / (stage["form"] / 1e3) / 1e12 if stage.get("form") else None,
-        "eval_tflops": info["eval_route_flops"] / (stage["eval"] / 1e3) / 1e12 if stage.get("eval") else None,
+        "form_tflops_algorithmic": info["form_flops"] / (stage["form"] / 1e3) / 1e12 if stage.get("form") else None,
+        "eval_tflops_algorithmic": info["eval_flops"] / (stage["eval"] / 1e3) / 1e12 if stage.get("eval") else None,
+        "form_tflops_executed": info["form_route_flops"] / (stage["form"] / 1e3) / 1e12 if stage.get("form") else None,
+        "eval_tflops_executed": info["eval_route_flops"] / (stage["eval"] / 1e3) / 1e12 if stage.get("eval") else None,
         "direct_pairs_per_s": info["direct_pairs"] / (stage["direct"] / 1e3) if stage.get("direct") else None,
-        "shift_gbs": (sb[0] + sb[1] + sb[2]) / ((stage["merge"] + stage["m2l"] + stage["split"]) / 1e3) / 1e9
-        if stage.get("merge", 0) + stage.get("m2l", 0) + stage.get("split", 0) > 0 else None,
-        "fp64_mma_peak_measured_tflops": fp64_tf,
+        "fp64_mma_peak_probe_tflops": fp64_tf,
     }
+    # errors of the timed outputs: FP64 direct sum at 1e4 sampled points, and
+    # the oracle (restated reference) on the whole workload
+    errors = None
     cpu_base = None
+    if not args.no_errors:
+        which, idx, exact = error_sample(w)
+        k = 0 if which == "pot" else 1
+        errors = {"metric": "derr (relative l2, test_fgt2d.f:204-225)",
+                  "direct_sample": f"FP64 direct sum (pairs within sqrt(delta ln 1e30)) at {idx.size} "
+                                   f"sampled {'sources' if k == 0 else 'targets'}",
+                  "err_vs_direct": derr(exact, outputs["mixed"][k][idx]),
+                  "err_vs_direct_fp64": derr(exact, outputs["fp64"][k][idx])}
     if world == 1 and not args.no_cpu_baseline:
         cores = cpu_cores()
-        p_cpu, dt_cpu, n_cpu = run_oracle(w, cores)
+        p_cpu, dt_cpu, opot, opt = run_oracle(w, cores)
         cpu_base = {"value": p_cpu / dt_cpu, "unit": "points/s", "cores": cores, "kind": "port",
-                    "sample": f"the full workload once ({n_cpu} sources), oracle (C++ restatement "
-                              f"of the reference plane-wave FGT) on {cores} threads, {dt_cpu:.1f} s"}
+                    "sample": f"the full workload once ({w['src'].shape[0]} sources), oracle (C++ "
+                              f"restatement of the reference plane-wave FGT) on {cores} threads, "
+                              f"{dt_cpu:.1f} s",
+                    "single_thread": single_thread_baseline(w)}
+        if errors is not None:
+            o = (opot, opt)
+            k = 0 if w["ifpgh"] else 1
+            errors["err_vs_oracle"] = derr(o[k], outputs["mixed"][k])
+            errors["err_vs_oracle_fp64"] = derr(o[k], outputs["fp64"][k])
+            errors["oracle_vs_direct"] = derr(exact, o[0 if which == "pot" else 1][idx])
     ms_mixed, ms_fp64 = results["mixed"], results["fp64"]
     line = {
-        "metric": "FGT points/s at eps 1e-6 (mixed form)",
+        "metric": METRIC,
         "value": world * pts / (ms_mixed / 1e3),
         "unit": "points/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (near-field exp in f32)", "data": "synthetic (seeded numpy)",
-        "config": {"workload": w["name"], "points_per_step": pts, "ifpgh": w["ifpgh"],
-                   "ifpghtarg": w["ifpghtarg"], "l2": "inputs 240 MB > 126 MB L2 (no flush)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "vs_baseline": None, "dtype": "f64 + f32 (mixed form)", "form": "mixed",
+        "data": "synthetic (seeded numpy)",
+        "config": config_of(w),
+        "parallelism": "replicas" if world > 1 else "single GPU",
         "fp64_form": {"value": world * pts / (ms_fp64 / 1e3), "ms_per_step": ms_fp64,
                       "mixed_over_fp64": ms_fp64 / ms_mixed},
+        "errors": errors,
         "stages_ms": stage,
         "stages_ms_fp64": stages["fp64"],
         "plan": {k: info[k] for k in ("npwlevel", "nlevels", "nboxes", "npw", "nexp", "nform",
@@ -424,6 +517,7 @@ def ours_arm(args, w, rank, world, local_rank):
                 "includes": "tree build (point work on the GPU) + lists + plan upload + H2D from pinned inputs + transform + D2H into pinned outputs"},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roof,
+        "roofline_shifts": roof_b,
         "stage_rates": stage_rates,
         "cpu_baseline": cpu_base,
         "clocks": clocks,
@@ -517,6 +611,7 @@ def main():
     ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-errors", action="store_true", help="skip the sampled direct-sum errors")
     ap.add_argument("--requests", type=int, default=4096, help="serving workload: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: arrivals per second")
     ap.add_argument("--workers", type=int, default=8, help="serving workload: server worker streams")

@@ -78,7 +78,8 @@ class ServerStats(ctypes.Structure):
                 ("failed", ctypes.c_longlong), ("points", ctypes.c_longlong),
                 ("peak_bytes", ctypes.c_longlong), ("budget_bytes", ctypes.c_longlong),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double),
-                ("max_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+                ("max_s", ctypes.c_double), ("span_s", ctypes.c_double),
+                ("hi_priority", ctypes.c_longlong)]
 
 
 def lib():
@@ -120,6 +121,7 @@ def lib():
     L.fgt_plan_profile_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]
     L.fgt_plan_get_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
     L.fgt_plan_profile_dominant.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, i]
     L.fgt_plan_destroy.argtypes = [_vp]
     L.fgt_status_string.restype = ctypes.c_char_p
@@ -360,16 +362,18 @@ class Plan:
         return dict(zip(names, list(ms)))
 
     def profile_dominant(self, d_chg, d_pot, d_pottarg):
-        """(ms, flops, name) of the plan's dominant tensor-core launch in one
-        execute on the context's stream; None when the plan has none."""
-        ms, fl = ctypes.c_double(), ctypes.c_double()
+        """(ms, executed flops, name, algorithmic flops) of the plan's dominant
+        tensor-core launch in one execute on the context's stream; None when
+        the plan has none."""
+        ms, fl, al = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         name = ctypes.create_string_buffer(64)
         st = lib().fgt_plan_profile_dominant(self._h, d_chg, d_pot or None, d_pottarg or None,
-                                             ctypes.byref(ms), ctypes.byref(fl), name, 64)
+                                             ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(al),
+                                             name, 64)
         if st == 2:
             return None
         _check(st, "fgt_plan_profile_dominant")
-        return ms.value, fl.value, name.value.decode()
+        return ms.value, fl.value, name.value.decode(), al.value
 
     def close(self):
         if getattr(self, "_h", None):

@@ -654,7 +654,7 @@ int fgt_plan_execute_device_full(fgt_plan* p, const double* q, const double* rno
 }
 
 int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double* pt, double* ms,
-                              double* flops, char* name, int name_len) {
+                              double* flops, double* alg_flops, char* name, int name_len) {
   if (!p || !ms || !flops) return FGT_ERR_BADARG;
   CKS(cudaSetDevice(p->ctx->device));
   StageTimes T;
@@ -670,6 +670,7 @@ int fgt_plan_profile_dominant(fgt_plan* p, const double* q, double* pot, double*
   CKS(cudaStreamSynchronize(p->ctx->stream));
   *ms = T.dom_ms;
   *flops = T.dom_flops;
+  if (alg_flops) *alg_flops = T.dom_alg_flops;
   if (name && name_len > 0) snprintf(name, name_len, "%s", T.dom_name);
   return T.dom_name[0] ? FGT_OK : FGT_ERR_UNSUPPORTED;
 }
@@ -1109,7 +1110,7 @@ struct fgt_server {
   long long next_id = 1;
   long long in_pts = 0, in_plan = 0, peak = 0;
   bool stop = false;
-  long long submitted = 0, completed = 0, failed = 0, points = 0;
+  long long submitted = 0, completed = 0, failed = 0, points = 0, hi_priority = 0;
   int running = 0;  // requests taken by a worker and not yet done
   std::vector<double> lat;
   double t_first = -1, t_last = 0;
@@ -1228,7 +1229,8 @@ void server_worker(fgt_server* S, int w) {
     }
     // small requests run on the worker's high-priority stream
     const cudaStream_t base = ctx->stream;
-    if ((long long)J->r.ns + (J->r.targ ? J->r.nt : 0) <= kServerSmall && S->hi[w]) ctx->stream = S->hi[w];
+    const bool on_hi = (long long)J->r.ns + (J->r.targ ? J->r.nt : 0) <= kServerSmall && S->hi[w];
+    if (on_hi) ctx->stream = S->hi[w];
     int st = server_run(S, ctx, J->r);
     for (int retry = 0; st == FGT_ERR_NOMEM && retry < 50; retry++) {
       // the device memory is held (or fragmented) by requests in flight:
@@ -1251,6 +1253,7 @@ void server_worker(fgt_server* S, int w) {
       J->status = st;
       J->done = true;
       S->completed++;
+      if (on_hi) S->hi_priority++;
       if (st != FGT_OK) S->failed++;
       else S->points += request_points(J->r);
       S->lat.push_back(J->t_end - J->t_sub);
@@ -1388,6 +1391,7 @@ int fgt_server_stats_get(fgt_server* s, fgt_server_stats* out) {
     out->mean_s = m / v.size();
   }
   out->span_s = s->t_first >= 0 ? s->t_last - s->t_first : 0.0;
+  out->hi_priority = s->hi_priority;
   return FGT_OK;
 }
 

@@ -64,7 +64,8 @@ struct StageTimes {
   // the dominant tensor-core launch: the Hermite-block MMA kernel of the
   // form group with the most sources (k_form2d_mma / k_form3d_mma)
   float dom_ms = 0;
-  double dom_flops = 0;  // 2 n P^dim (x nd) for that group
+  double dom_flops = 0;      // executed: 2 n P^dim (x nd) for that group
+  double dom_alg_flops = 0;  // algorithmic: 4 n npw^dim (x nd), n = the group's sources
   char dom_name[48] = {0};
 };
 
@@ -145,7 +146,8 @@ struct DevicePlan {
   std::vector<OrderGroup> form_groups;
   int dom_form_group = -1;        // 2D: form group with the most sources (MMA kernels)
   int dom_fchunk_group = -1;      // 3D: chunk group with the most sources
-  std::vector<double> group_flops;  // 2 n P^dim per form group (2D) / chunk group (3D)
+  std::vector<double> group_flops;      // 2 n P^dim per form group (2D) / chunk group (3D)
+  std::vector<double> group_alg_flops;  // 4 n npw^dim per form group (2D) / chunk group (3D)
   // 2D Taylor evaluation (conversion per leaf, then Horner per point chunk)
   long long* form_hoff = nullptr;  // 2D MMA form: per form task, offset of its Hermite block in hbuf
   ConvTask* conv = nullptr;
@@ -215,7 +217,7 @@ size_t large_delta_noalloc_capacity();
 // Large-delta path (one Taylor local about the root centre), no tree.
 // deterministic: the sources' contributions are summed in a fixed order
 // through per-CTA partial blocks (work must hold large_delta_work_doubles(P,
-// true) doubles); otherwise they are added atomically (nd (nlocal0+1)^dim + 4
+// true) doubles); otherwise they are added atomically (nd (nlocal0+1)^dim
 // doubles of work; results can differ in the last bits from call to call).
 cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs& in,
                                 const double* trg, const Outputs& out, double* work,

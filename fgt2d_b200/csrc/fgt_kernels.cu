@@ -28,256 +28,11 @@
 #include <type_traits>
 
 #include "fgt_device.hpp"
+#include "fgt_kcommon.cuh"
 
 namespace fgtb {
 
 namespace {
-
-constexpr int FORM_CH = 32;    // sources staged per chunk in the form kernels
-constexpr int LD_PARTS = 256;  // CTAs (partial blocks) of the deterministic large-delta form
-constexpr unsigned FULL_MASK = 0xffffffffu;
-
-struct KP {
-  int dim, nd, npw, n2, nexp;
-  double dsq, delta, dmax, t1;
-  const double* centers;
-  const double* h2x;
-  const double* x2l;
-  const double* ws;
-  const double2* wms;
-  const double2* wsh;
-  double2* mp;
-  double2* loc;
-  const double* src;
-  const double* chg;
-  const double* trg;
-  double* pot;      // sorted outputs of the sources: per point [nc_s][nd]
-  double* pottarg;  // sorted outputs of the targets: per point [nc_t][nd]
-  int nc_s, nc_t;   // components per density written: 1 (pot), 1 + dim (+ grad), + H (+ Hessian)
-  int ifcharge, ifdipole;
-  const double* dnrm;  // sorted dipole directions (ns, dim)
-  const double* dstr;  // sorted dipole strengths (ns, nd)
-  const float* fsrc;   // mixed near field: scaled coordinates as FP32 (hi, lo), [dim][2] per point
-  const float* ftrg;
-};
-
-// Source weights of density ind at sorted source i: the charge (0 without
-// charges) and the dipole vector dipstr * n (zeros without dipoles).
-__device__ __forceinline__ double src_charge(const KP& k, long long i, int ind) {
-  return k.ifcharge ? k.chg[i * k.nd + ind] : 0.0;
-}
-template <int DIM>
-__device__ __forceinline__ void src_dipole(const KP& k, long long i, int ind, double* v) {
-  const double s = k.dstr[i * k.nd + ind];
-#pragma unroll
-  for (int d = 0; d < DIM; d++) v[d] = s * k.dnrm[i * DIM + d];
-}
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
-  return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
-}
-__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // c + a b
-  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
-}
-__device__ __forceinline__ double2 cfmac(double2 a, double2 b, double2 c) {  // c + a conj(b)
-  return make_double2(fma(a.x, b.x, fma(a.y, b.y, c.x)), fma(a.y, b.x, fma(-a.x, b.y, c.y)));
-}
-// z * i^j
-__device__ __forceinline__ double2 rot(double2 z, int j) {
-  switch (j & 3) {
-    case 0: return z;
-    case 1: return make_double2(-z.y, z.x);
-    case 2: return make_double2(-z.x, -z.y);
-    default: return make_double2(z.y, -z.x);
-  }
-}
-// z * i^j without a branch on j (lanes of a warp hold different j)
-__device__ __forceinline__ double2 rot_bf(double2 z, int j) {
-  const double a = (j & 1) ? -z.y : z.x, b = (j & 1) ? z.x : z.y;
-  return (j & 2) ? make_double2(-a, -b) : make_double2(a, b);
-}
-// a + v * i^j for real v
-__device__ __forceinline__ void addrot(double2& a, double v, int j) {
-  switch (j & 3) {
-    case 0: a.x += v; break;
-    case 1: a.y += v; break;
-    case 2: a.x -= v; break;
-    default: a.y -= v; break;
-  }
-}
-__device__ __forceinline__ double2 cexpi(double th) {
-  double s, c;
-  sincos(th, &s, &c);
-  return make_double2(c, s);
-}
-__device__ __forceinline__ float ex2_approx(float x) {
-  float y;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// A staged factor row of a dipole source column: a h_j + b dh_j for j < Pn
-// at stride `st`, with h_j = v^j / sqrt(j!) and dh_j = sqrt(j) dsq h_(j-1)
-// (the source-coordinate derivative, g3dformhd_vec's dxhx).
-__device__ __forceinline__ void dip_row(double* row, int st, int Pn, double v, double a, double b,
-                                        double dsq, const double* __restrict__ isq) {
-  double h = 1.0;
-  row[0] = a;
-  for (int j = 1; j < Pn; j++) {
-    const double dh = j * isq[j] * dsq * h;
-    h = h * v * isq[j];
-    row[j * st] = fma(a, h, b * dh);
-  }
-}
-// The three columns of a 3D dipole source (g3dformhd_vec / g3dformhcd_vec,
-// g3drouts.f:197-405): H += hx hy (q hz + v3 dhz) + hx dhy (v2 hz) + dhx hy (v1 hz).
-// Coefficients (a, b) of the factor along d (0 x, 1 y, 2 z) in column c.
-__device__ __forceinline__ void dip3_coef(int c, int d, double q, const double* v, double& a,
-                                          double& b) {
-  if (d == 2) {
-    a = c == 0 ? q : c == 1 ? v[1] : v[0];
-    b = c == 0 ? v[2] : 0.0;
-  } else {
-    const bool deriv = (d == 1 && c == 1) || (d == 0 && c == 2);
-    a = deriv ? 0.0 : 1.0;
-    b = deriv ? 1.0 : 0.0;
-  }
-}
-
-// ------------------------------------------------------------ outputs: potential, gradient, Hessian
-// PGH = 1 potential, 2 + gradient, 3 + Hessian (the reference's ifpgh).  The
-// components of one density at one point are, in order, pot, d/dx, d/dy
-// (, d/dz), then the Hessian in the reference's order: 2D xx, xy, yy
-// (g2dlevalh_vec); 3D xx, yy, zz, xy, xz, yz (g3dlevalh_vec).  A sorted
-// output row holds the nc components of all nd densities, [nc][nd].
-template <int DIM>
-__host__ __device__ constexpr int nhess() { return DIM == 2 ? 3 : 6; }
-template <int DIM, int PGH>
-__host__ __device__ constexpr int ncomp() { return PGH >= 3 ? 1 + DIM + nhess<DIM>() : PGH == 2 ? 1 + DIM : 1; }
-
-// out row ip += v[0 .. nc) for density ind (nc <= NC: the set's own count)
-template <int NC>
-__device__ __forceinline__ void add_out(double* __restrict__ out, long long ip, int nd, int nc, int ind,
-                                        const double* v) {
-#pragma unroll
-  for (int c = 0; c < NC; c++)
-    if (c < nc) out[(ip * nc + c) * nd + ind] += v[c];
-}
-
-// Horner with derivative chains.  One step with coefficient c of a
-// polynomial in x carries s, s' and s''/2:
-//   s''/2 <- s''/2 x + s',  s' <- s' x + s,  s <- s x + c.
-template <int PGH>
-__device__ __forceinline__ void hstep(double& s, double& sx, double& sxx, double x, double c) {
-  if (PGH >= 3) sxx = fma(sxx, x, sx);
-  if (PGH >= 2) sx = fma(sx, x, s);
-  s = fma(s, x, c);
-}
-// Sums over the rows of a 2D block, r = sum_k y^k s_k(x), with the x chains
-// of the rows: r, r_x, r_y, r_xx/2, r_xy, r_yy/2.
-struct Hor2 {
-  double r = 0, rx = 0, ry = 0, rxx = 0, rxy = 0, ryy = 0;
-};
-template <int PGH>
-__device__ __forceinline__ void hrow(Hor2& a, double y, double s, double sx, double sxx) {
-  if (PGH >= 3) {
-    a.ryy = fma(a.ryy, y, a.ry);
-    a.rxy = fma(a.rxy, y, a.rx);
-    a.rxx = fma(a.rxx, y, sxx);
-  }
-  if (PGH >= 2) {
-    a.ry = fma(a.ry, y, a.r);
-    a.rx = fma(a.rx, y, sx);
-  }
-  a.r = fma(a.r, y, s);
-}
-// Sums over the planes of a 3D block with the planes' 2D chains.
-struct Hor3 {
-  double r = 0, rx = 0, ry = 0, rz = 0, rxx = 0, ryy = 0, rzz = 0, rxy = 0, rxz = 0, ryz = 0;
-};
-template <int PGH>
-__device__ __forceinline__ void hplane(Hor3& a, double z, const Hor2& q) {
-  if (PGH >= 3) {
-    a.rzz = fma(a.rzz, z, a.rz);
-    a.rxz = fma(a.rxz, z, a.rx);
-    a.ryz = fma(a.ryz, z, a.ry);
-    a.rxx = fma(a.rxx, z, q.rxx);
-    a.ryy = fma(a.ryy, z, q.ryy);
-    a.rxy = fma(a.rxy, z, q.rxy);
-  }
-  if (PGH >= 2) {
-    a.rz = fma(a.rz, z, a.r);
-    a.rx = fma(a.rx, z, q.rx);
-    a.ry = fma(a.ry, z, q.ry);
-  }
-  a.r = fma(a.r, z, q.r);
-}
-// Components in physical coordinates: the expansion variable is
-// (x - c) dsq, so each derivative carries a factor dsq.
-template <int PGH>
-__device__ __forceinline__ void hemit(const Hor2& a, double dsq, double* v) {
-  v[0] = a.r;
-  if (PGH >= 2) {
-    v[1] = a.rx * dsq;
-    v[2] = a.ry * dsq;
-  }
-  if (PGH >= 3) {
-    const double d2 = dsq * dsq;
-    v[3] = 2.0 * a.rxx * d2;
-    v[4] = a.rxy * d2;
-    v[5] = 2.0 * a.ryy * d2;
-  }
-}
-template <int PGH>
-__device__ __forceinline__ void hemit(const Hor3& a, double dsq, double* v) {
-  v[0] = a.r;
-  if (PGH >= 2) {
-    v[1] = a.rx * dsq;
-    v[2] = a.ry * dsq;
-    v[3] = a.rz * dsq;
-  }
-  if (PGH >= 3) {
-    const double d2 = dsq * dsq;
-    v[4] = 2.0 * a.rxx * d2;
-    v[5] = 2.0 * a.ryy * d2;
-    v[6] = 2.0 * a.rzz * d2;
-    v[7] = a.rxy * d2;
-    v[8] = a.rxz * d2;
-    v[9] = a.ryz * d2;
-  }
-}
-// Runtime-order evaluation of a real Taylor block: 2D lo[b ld + a],
-// 3D lo[(c Pn + b) ld + a] (a, b, c the powers of x, y, z).
-template <int PGH>
-__device__ void horner2_rt(const double* lo, int ld, int Pn, double x, double y, double dsq, double* v) {
-  Hor2 a;
-  for (int b = Pn - 1; b >= 0; b--) {
-    const double* row = lo + (size_t)b * ld;
-    double s = row[Pn - 1], sx = 0.0, sxx = 0.0;
-    for (int m = Pn - 2; m >= 0; m--) hstep<PGH>(s, sx, sxx, x, row[m]);
-    hrow<PGH>(a, y, s, sx, sxx);
-  }
-  hemit<PGH>(a, dsq, v);
-}
-template <int PGH>
-__device__ void horner3_rt(const double* lo, int ld, int Pn, double x, double y, double z, double dsq,
-                           double* v) {
-  Hor3 a;
-  for (int c = Pn - 1; c >= 0; c--) {
-    Hor2 q;
-    for (int b = Pn - 1; b >= 0; b--) {
-      const double* row = lo + ((size_t)c * Pn + b) * ld;
-      double s = row[Pn - 1], sx = 0.0, sxx = 0.0;
-      for (int m = Pn - 2; m >= 0; m--) hstep<PGH>(s, sx, sxx, x, row[m]);
-      hrow<PGH>(q, y, s, sx, sxx);
-    }
-    hplane<PGH>(a, z, q);
-  }
-  hemit<PGH>(a, dsq, v);
-}
 
 // ------------------------------------------------------------ sort / unsort
 // Tree order: out row i = in row perm[i] (dreorderf, fmmcommon2d.f:3-26);
@@ -3288,8 +3043,9 @@ __global__ void __launch_bounds__(128) k_direct_mixed(KP k, const DirTask* __res
 // factor, dh_j = -(j+1) dsq h_(j+1): 2D (hx, q hy + v2 dhy), (v1 dhx, hy);
 // 3D as dip3_coef with these h and dh.
 template <int DIM>
-__global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const double* __restrict__ cen,
+__global__ void __launch_bounds__(256) k_ld_form(KP k, int ns, int p, const double3 c3,
                                                  double* __restrict__ local, double* __restrict__ partial) {
+  const double cen[3] = {c3.x, c3.y, c3.z};
   const int Pn = p + 1;
   const int nent = DIM == 2 ? Pn * Pn : Pn * Pn * Pn;
   extern __shared__ double sm[];
@@ -3381,7 +3137,8 @@ __global__ void k_ld_sum(int nent, int nparts, const double* __restrict__ partia
 template <int DIM, int PGH>
 __global__ void k_ld_eval(KP k, int n, const double* __restrict__ pts, double* __restrict__ pot,
                           double* __restrict__ grad, double* __restrict__ hess, int p,
-                          const double* __restrict__ cen, const double* __restrict__ local) {
+                          const double3 c3, const double* __restrict__ local) {
+  const double cen[3] = {c3.x, c3.y, c3.z};
   constexpr int NC = ncomp<DIM, PGH>(), NH = nhess<DIM>();
   const int Pn = p + 1;
   const int nent = DIM == 2 ? Pn * Pn : Pn * Pn * Pn;
@@ -3609,6 +3366,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       for (int t = G.beg; t < G.end; t++) n += form[t].n;
       const double Pn = G.p + 1;
       D.group_flops.push_back(2.0 * (double)n * Pn * Pn * P.nd);
+      D.group_alg_flops.push_back(4.0 * (double)n * P.npw * P.npw * P.nd);
       if (G.p + 1 <= 32 && n > best) { best = n; D.dom_form_group = (int)gi; }
     }
   }
@@ -3748,6 +3506,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
           while (u < fchunks.size() && form[fchunks[u].task].p == pt) n += fchunks[u++].n;
           const double Pn = pt + 1;
           D.group_flops.push_back(2.0 * (double)n * Pn * Pn * Pn * P.nd);
+          D.group_alg_flops.push_back(4.0 * (double)n * P.npw * P.npw * P.npw * P.nd);
           if (n > best) { best = n; D.dom_fchunk_group = (int)D.fchunk_groups.size(); }
           D.fchunk_groups.push_back({pt, (int)t, (int)u});
           t = u;
@@ -4004,6 +3763,9 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
   KP k = make_kp(D);
   // the derivative order the kernels compute: the larger of the two sets'
   const int pgh = std::max(1, std::max(P.ifpgh, P.ifpghtarg));
+  // mixed form of stages (a) and (c): FP32 arithmetic with FP64 accumulation
+  // in the 2D Hermite block and Taylor evaluation (charges, potentials)
+  const bool mixed_ac = precision == PREC_MIXED && !P.ifdipole;
   k.ws = D.h2x;  // row j = 0 of h2x holds the weights
   const int nd = P.nd;
   cudaEvent_t ev[9], dev0 = nullptr, dev1 = nullptr;
@@ -4013,6 +3775,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     CK(cudaEventCreate(&dev1));
     times->dom_ms = 0;
     times->dom_flops = 0;
+    times->dom_alg_flops = 0;
     times->dom_name[0] = 0;
   }
   auto mark = [&](int i) { if (times) cudaEventRecord(ev[i], st); };
@@ -4054,15 +3817,18 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       k_form2d_mma<NT, false><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);            \
     }                                                                                             \
   } while (0)
-          if (Pn <= 8) FORM_MMA(1);
+          if (mixed_ac && Pn <= 16) CK(launch_form2d_f32(k, tk, G.end - G.beg, nd, D.form_hoff + G.beg, D.hbuf, Pn, st));
+          else if (Pn <= 8) FORM_MMA(1);
           else if (Pn <= 16) FORM_MMA(2);
           else if (Pn <= 24) FORM_MMA(3);
           else FORM_MMA(4);
 #undef FORM_MMA
           if (dom) {
             cudaEventRecord(dev1, st);
-            snprintf(times->dom_name, sizeof(times->dom_name), "k_form2d_mma<%d>", (Pn + 7) / 8);
+            if (mixed_ac && Pn <= 16) snprintf(times->dom_name, sizeof(times->dom_name), "k_form2d_f32");
+            else snprintf(times->dom_name, sizeof(times->dom_name), "k_form2d_mma<%d>", (Pn + 7) / 8);
             times->dom_flops = D.group_flops[gi];
+            times->dom_alg_flops = D.group_alg_flops[gi];
           }
           const int nt = G.end - G.beg;
           const H2pwDims Z(Pn, P.npw);
@@ -4120,6 +3886,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           cudaEventRecord(dev1, st);
           snprintf(times->dom_name, sizeof(times->dom_name), "k_form3d_mma<%d>", mt);
           times->dom_flops = D.group_flops[gi];
+          times->dom_alg_flops = D.group_alg_flops[gi];
         }
         launches++;
       }
@@ -4235,6 +4002,11 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const HornerTask* tk = D.horner + G.beg;
         const size_t sh = (size_t)Pn * np2 * 16;
         if (sh > 227 * 1024) return cudaErrorNotSupported;
+        if (mixed_ac && pgh == 1 && np2 <= 16) {
+          CK(launch_eval2d_horner_f32(k, tk, G.end - G.beg, nd, Pn, D.lo, st));
+          launches++;
+          continue;
+        }
         {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
           constexpr int PG = decltype(G)::value;
@@ -4495,7 +4267,7 @@ cudaError_t probe_fp64_mma(double* tflops) {
 size_t large_delta_work_doubles(const Params& P, bool deterministic) {
   const size_t Pn = P.nlocal0 + 1;
   const size_t nent = P.dim == 2 ? Pn * Pn : Pn * Pn * Pn;
-  return 4 + (size_t)P.nd * nent * (deterministic ? 1 + LD_PARTS : 1);
+  return (size_t)P.nd * nent * (deterministic ? 1 + LD_PARTS : 1);
 }
 
 cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs& in,
@@ -4510,9 +4282,9 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs
   int p = P.nlocal0;
   int Pn = p + 1;
   size_t nent = P.dim == 2 ? (size_t)Pn * Pn : (size_t)Pn * Pn * Pn;
-  double* cen = work;
-  double* local = work + 4;
-  CK(cudaMemcpyAsync(cen, P.cen0, 3 * sizeof(double), cudaMemcpyHostToDevice, st));
+  // the centre travels by value in the kernel arguments (no host->device copy)
+  const double3 cen = make_double3(P.cen0[0], P.cen0[1], P.dim == 3 ? P.cen0[2] : 0.0);
+  double* local = work;
   CK(cudaMemsetAsync(local, 0, nent * P.nd * sizeof(double), st));
   size_t sh = 3 * FORM_CH * Pn * 8;
   if (sh > 227 * 1024) return cudaErrorNotSupported;
@@ -4554,8 +4326,8 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs
 // budget, and latency-critical loops that must not pay for cudaMalloc, which
 // can synchronise the whole device.  For them the large-delta transform (one
 // Taylor local about a given centre, the reference's fgt2d_large_delta /
-// fgt3d_large_delta) runs with its only scratch -- the centre and the local
-// expansion -- in this fixed device array.  Every device that loads the
+// fgt3d_large_delta) runs with its only scratch -- the local expansion -- in
+// this fixed device array.  Every device that loads the
 // library holds it (512 KB) until the process exits; every call shares it, so
 // calls that overlap on the GPU race; each call clears what it accumulates.
 namespace {
@@ -4593,8 +4365,9 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
     CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
     CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
   }
-  // large_delta_execute copies the centre into work[0..2] and clears the
-  // local expansion in work[4..] before accumulating into it
+  // large_delta_execute clears the local expansion (work[0..nd*nent)) on the
+  // stream before accumulating into it; the centre goes by value in the
+  // kernel arguments, so the call makes no host->device copy
   Outputs o;
   o.pot = pot;
   o.pottarg = pottarg;

@@ -207,11 +207,13 @@ int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const doubl
 int fgt_plan_get_info(const fgt_plan* plan, fgt_plan_info* info);
 /* One execute with CUDA events around the plan's dominant tensor-core launch
  * (the Hermite-block MMA kernel of the form order group with the most
- * sources) on the context's stream: its device time (ms), its algorithmic
- * flops (2 n P^dim nd) and its name.  FGT_ERR_UNSUPPORTED when the plan has
- * no such launch (all-direct, large-delta). */
+ * sources) on the context's stream: its device time (ms), the flops it
+ * executes (2 n P^dim nd over the group's n sources), the plane-wave
+ * algorithmic count of the same sources (4 n npw^dim nd; NULL to skip) and its
+ * name.  FGT_ERR_UNSUPPORTED when the plan has no such launch (all-direct,
+ * large-delta). */
 int fgt_plan_profile_dominant(fgt_plan* plan, const double* d_charge, double* d_pot, double* d_pottarg,
-                              double* ms, double* flops, char* name, int name_len);
+                              double* ms, double* flops, double* alg_flops, char* name, int name_len);
 int fgt_plan_destroy(fgt_plan* plan);
 
 /* ---- host tree (no device needed) ----------------------------------------
@@ -274,6 +276,8 @@ typedef struct fgt_server_stats {
   long long peak_bytes, budget_bytes;
   double p50_s, p99_s, mean_s, max_s;  /* latency: submit -> result on the host */
   double span_s;               /* first submit -> last completion */
+  long long hi_priority;       /* requests run on a worker's highest-priority stream
+                                  (those of <= 1e5 points, when the device has priorities) */
 } fgt_server_stats;
 int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_server** out);
 int fgt_server_set_precision(fgt_server* server, int precision);

@@ -1994,6 +1994,84 @@ void orc_direct(int dim, int nd, double delta, int ns, const double* src, const 
   }
 }
 
+// The FP64 direct sum at sampled targets for large N: sources binned on a
+// uniform grid whose cells are at least `rcut` wide, each target summing the
+// 3^d cells around its own.  Pairs farther apart than rcut are dropped; with
+// rcut^2 = delta * ln(1e30) every dropped term is below 1e-30 of its charge,
+// so the sum equals the plain one (orc_direct) to rounding for any workload
+// whose potentials are not themselves below ~1e-25 of the charges.
+void orc_direct_cut(int dim, int nd, double delta, double rcut, int ns, const double* src,
+                    const double* chg, int nt, const double* trg, double* pot, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  if (ns <= 0) {
+    for (size_t i = 0; i < (size_t)nt * nd; i++) pot[i] = 0;
+    return;
+  }
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  for (int d = 0; d < dim; d++) lo[d] = hi[d] = src[d];
+  for (int i = 0; i < ns; i++)
+    for (int d = 0; d < dim; d++) {
+      lo[d] = std::min(lo[d], src[(size_t)dim * i + d]);
+      hi[d] = std::max(hi[d], src[(size_t)dim * i + d]);
+    }
+  double ext = 0;
+  for (int d = 0; d < dim; d++) ext = std::max(ext, hi[d] - lo[d]);
+  const double maxcells = dim == 2 ? 4096.0 : 256.0;  // per dimension
+  const double h = std::max(rcut, ext / maxcells) * (1 + 1e-12) + 1e-300;
+  int nc[3] = {1, 1, 1};
+  for (int d = 0; d < dim; d++) nc[d] = std::max(1, (int)std::floor((hi[d] - lo[d]) / h) + 1);
+  const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+  auto cell_of = [&](const double* x, int* c) {
+    for (int d = 0; d < 3; d++) c[d] = 0;
+    for (int d = 0; d < dim; d++) c[d] = (int)std::floor((x[d] - lo[d]) / h);
+  };
+  std::vector<size_t> start(ncell + 1, 0);
+  std::vector<int> order(ns);
+  std::vector<size_t> cid(ns);
+  for (int i = 0; i < ns; i++) {
+    int c[3];
+    cell_of(src + (size_t)dim * i, c);
+    for (int d = 0; d < dim; d++) c[d] = std::min(std::max(c[d], 0), nc[d] - 1);
+    cid[i] = ((size_t)c[2] * nc[1] + c[1]) * nc[0] + c[0];
+    start[cid[i] + 1]++;
+  }
+  for (size_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+  {
+    std::vector<size_t> fill(start.begin(), start.end() - 1);
+    for (int i = 0; i < ns; i++) order[fill[cid[i]]++] = i;
+  }
+  const double r2 = rcut * rcut;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int it = 0; it < nt; it++) {
+    const double* t = trg + (size_t)dim * it;
+    int c[3];
+    cell_of(t, c);
+    std::vector<double> acc(nd, 0.0);
+    const int zr = dim == 3 ? 1 : 0;
+    for (int dz = -zr; dz <= zr; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+          if (cx < 0 || cy < 0 || cz < 0 || cx >= nc[0] || cy >= nc[1] || cz >= nc[2]) continue;
+          const size_t cc = ((size_t)cz * nc[1] + cy) * nc[0] + cx;
+          for (size_t k = start[cc]; k < start[cc + 1]; k++) {
+            const int i = order[k];
+            double rr = 0;
+            for (int d = 0; d < dim; d++) {
+              const double df = t[d] - src[(size_t)dim * i + d];
+              rr += df * df;
+            }
+            if (rr > r2) continue;
+            const double e = std::exp(-rr / delta);
+            for (int m = 0; m < nd; m++) acc[m] += e * chg[(size_t)nd * i + m];
+          }
+        }
+    for (int m = 0; m < nd; m++) pot[(size_t)nd * it + m] = acc[m];
+  }
+}
+
 // The same direct sum with gradients and Hessians (pgh = 2, 3): the
 // derivatives of exp(-r^2/delta) with respect to the target, per
 // g2d_directch_vec / g3d_directch_vec without the cutoff.

@@ -56,6 +56,9 @@ def lib():
                                    ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
                                    ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                    _dp, _dp, _dp, _ip, ctypes.c_int]
+        L.orc_direct_cut.restype = None
+        L.orc_direct_cut.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_direct_full.restype = None
         L.orc_direct_full.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                       _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
@@ -224,6 +227,21 @@ def direct(dim, nd, delta, sources, charge, targ, nthreads=0):
     out = np.zeros((trg.shape[0], nd))
     lib().orc_direct(dim, nd, float(delta), src.shape[0], _d(src), _d(q), trg.shape[0], _d(trg),
                      _d(out), nthreads)
+    return out
+
+
+def direct_cut(dim, nd, delta, sources, charge, targ, nthreads=0):
+    """FP64 direct sum at ``targ`` over sources binned on a grid, dropping
+    pairs farther apart than sqrt(delta ln 1e30) (terms below 1e-30 of their
+    charge): the plain direct sum to rounding, at a cost that does not grow
+    with N for a fixed density.  Used for sampled-target errors at full size."""
+    src = _f64(sources)
+    trg = _f64(targ)
+    q = _f64(charge).reshape(src.shape[0], nd)
+    out = np.zeros((trg.shape[0], nd))
+    rcut = float(np.sqrt(delta * np.log(1e30)))
+    lib().orc_direct_cut(dim, nd, float(delta), rcut, src.shape[0], _d(src), _d(q), trg.shape[0],
+                         _d(trg), _d(out), nthreads)
     return out
 
 

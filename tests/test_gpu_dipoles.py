@@ -5,8 +5,8 @@ g2d_directd*/cd*_vec, g3d_directd*/cd*_vec (2d/planewave/src/g2drouts.f:173-338,
 685-840; g2ddirect.f:217-658; 3d/planewave/src/g3drouts.f:197-405, 857-1040,
 2042-2262; g3ddirect.f:207-708), through the C ABI.
 
-Bars as the gradient tests: FP64 vs oracle <= 1e-2 eps (pot, grad) and
-0.1 eps (Hessian); vs the exact sums no worse than twice the oracle's own
+Bars as the gradient tests: FP64 vs oracle <= 1e-12 (pot), 1e-11 (grad) and
+1e-10 (Hessian); vs the exact sums no worse than twice the oracle's own
 error (or 20 eps).  Dipole plans run the FP64 near field in either precision
 mode, so both modes meet the FP64 bar.
 """
@@ -71,7 +71,7 @@ def test_dipoles(case, precision, fgt, oracle):
             e_ref = oracle.derr(ref[k], got[k])
             e_dir = oracle.derr(exact[order], got[k][idx])
             e_orc = oracle.derr(exact[order], ref[k][idx])
-            tol = (1e-2 if order < 2 else 1e-1) * eps
+            tol = (1e-12, 1e-11, 1e-10)[order]
             print(f"{name} {precision} {k}: vs oracle {e_ref:.2e} (tol {tol:.0e}) vs direct "
                   f"{e_dir:.2e} (oracle {e_orc:.2e}) {ref['info']}")
             assert e_ref <= tol, (k, e_ref, tol)

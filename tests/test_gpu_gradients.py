@@ -4,8 +4,8 @@ oracle's restatement of g2dlevalg/h_vec, g2dpwevalg/h_vec, g2d_directcg/ch_vec
 3D twins, through the C ABI.
 
 Bars (relative l2 per output array, the reference test's ``derr``):
-  * FP64 vs oracle: <= 1e-2 * eps for pot and grad, <= 0.1 * eps for the
-    Hessian (same routes and orders; differentiation amplifies rounding)
+  * FP64 vs oracle: <= 1e-12 for pot, 1e-11 for grad, 1e-10 for the Hessian
+    (same routes and orders: rounding-level; differentiation amplifies it)
   * mixed vs oracle: <= eps (pot), 10 * eps (grad, Hessian)
   * vs the exact direct sum: no worse than twice the oracle's own error
     (or 10 * eps), i.e. the reference's accuracy for derivatives
@@ -84,7 +84,7 @@ def test_gradients(case, precision, fgt, oracle):
             e_dir = oracle.derr(exact[order], got[k][idx])
             e_orc = oracle.derr(exact[order], ref[k][idx])
             if precision == "fp64":
-                tol = (1e-2 if order < 2 else 1e-1) * eps
+                tol = (1e-12, 1e-11, 1e-10)[order]
             else:
                 tol = eps if order == 0 else 10 * eps
             print(f"{name} {precision} {k}: vs oracle {e_ref:.2e} (tol {tol:.0e}) vs direct "

@@ -42,6 +42,9 @@ def test_mix_equals_alone(fgt):
     st = srv.stats()
     assert st["completed"] == st["submitted"] == len(reqs) and st["failed"] == 0
     assert 0 < st["p50_s"] <= st["p99_s"] <= st["max_s"]
+    # every request of this mix has <= 1e5 points: each ran on a worker's
+    # highest-priority stream (B200 exposes stream priorities)
+    assert st["hi_priority"] == len(reqs), st["hi_priority"]
     srv.close()
 
 
