@@ -107,6 +107,8 @@ def lib():
     L.fgt_ctx_stream.restype = _vp
     L.fgt_ctx_stream.argtypes = [_vp]
     L.fgt_probe_fp64_mma_tflops.argtypes = [_vp, ctypes.POINTER(ctypes.c_double)]
+    L.fgt_tc_selftest.argtypes = [i, i, ctypes.POINTER(ctypes.c_double)]
+    L.fgt_tc_error.argtypes = [i, i, ctypes.POINTER(ctypes.c_int)]
     L.fgt_large_delta_noalloc.argtypes = [i, i, d, i, _vp, _vp, i, _dp, i, _vp, i, _vp, i, _vp, _vp]
     L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,
                                 _dp, i, _dp, _dp, _dp]

@@ -492,6 +492,19 @@ int fgt_large_delta_noalloc(int dim, int nd, double delta, int ns, const double*
   return FGT_OK;
 }
 
+int fgt_tc_selftest(int device, int n, double* max_rel_err) {
+  if (!max_rel_err || n < 16 || n > 256 || n % 16) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(device));
+  CKS(tc_selftest(n, max_rel_err));
+  return FGT_OK;
+}
+int fgt_tc_error(int device, int clear, int* flag) {
+  if (!flag) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(device));
+  CKS(tc_error_flag(flag, clear != 0));
+  return FGT_OK;
+}
+
 int fgt_probe_fp64_mma_tflops(fgt_ctx* c, double* tflops) {
   if (!c || !tflops) return FGT_ERR_BADARG;
   CKS(cudaSetDevice(c->device));

@@ -206,6 +206,14 @@ cudaError_t device_check_finite(const double* x, size_t n, int* d_flag, cudaStre
 // device in TFLOP/s.
 cudaError_t probe_fp64_mma(double* tflops);
 
+// The tensor-core kernels' device error flag on the current device (set when
+// a wait on an MMA completion gave up); cleared on request.
+cudaError_t tc_error_flag(int* flag, bool clear);
+// One BF16 x 3 tcgen05 tile (M = 128, K = 16, N) on the current device
+// against an FP64 product on the host: the largest error relative to the
+// largest entry.
+cudaError_t tc_selftest(int N, double* max_rel_err);
+
 // Large-delta path with its scratch in a fixed device array instead of
 // `work`: no allocation.  cudaErrorInvalidValue when nd (nlocal0+1)^dim
 // exceeds large_delta_noalloc_capacity() doubles.

@@ -88,6 +88,45 @@ __device__ __forceinline__ double2 cexpi(double th) {
   sincos(th, &s, &c);
   return make_double2(c, s);
 }
+// Packed FP32 pairs on the sm_100 f32x2 pipe: one instruction computes both
+// lanes of a float2 (d.x = a.x b.x + c.x, d.y = a.y b.y + c.y), each rounded
+// as the scalar FP32 operation.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -254,14 +293,67 @@ __device__ void horner3_rt(const double* lo, int ld, int Pn, double x, double y,
   hemit<PGH>(a, dsq, v);
 }
 
+// ------------------------------------------------------------ (d) near field: source ranges
+// A near-field task's sources are a list of ranges; a warp reads up to 32
+// ranges at a time and maps slots of their concatenation to source indices.
+struct RangeChunk {
+  int nr, excl, s0, tot;  // ranges in the chunk; this lane's exclusive prefix and start; chunk size
+};
+__device__ __forceinline__ RangeChunk load_range_chunk(const SrcRange* __restrict__ ranges, int off,
+                                                       int cnt, int rc, int lane) {
+  RangeChunk C;
+  C.nr = min(32, cnt - rc);
+  int rn = 0;
+  C.s0 = 0;
+  if (lane < C.nr) {
+    const SrcRange R = ranges[off + rc + lane];
+    rn = R.n;
+    C.s0 = R.s0;
+  }
+  int inc = rn;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL_MASK, inc, o);
+    if (lane >= o) inc += v;
+  }
+  C.excl = inc - rn;
+  C.tot = __shfl_sync(FULL_MASK, inc, 31);
+  return C;
+}
+// source index of slot s (0 <= s < C.tot) of the chunk; all lanes must call
+__device__ __forceinline__ int range_slot_source(const RangeChunk& C, int s) {
+  int lo = 0, hi = C.nr;
+#pragma unroll
+  for (int it = 0; it < 5; it++) {
+    const int mid = (lo + hi) >> 1;
+    if (__shfl_sync(FULL_MASK, C.excl, mid) <= s) lo = mid;
+    else hi = mid;
+  }
+  return __shfl_sync(FULL_MASK, C.s0, lo) + (s - __shfl_sync(FULL_MASK, C.excl, lo));
+}
+
 // Mixed-form kernels (fgt_mixed.cu).  2D Hermite block in FP32 for the
 // leaves of one order group (Pn <= 16), written as the plain form's FP64
 // block at hbuf + hoff[task].
 cudaError_t launch_form2d_f32(const KP& k, const FormTask* tasks, int ntask, int nd,
                               const long long* hoff, double* hbuf, int Pn, cudaStream_t st);
+// Mixed near field of potentials (charges) on the packed FP32 pipe.
+cudaError_t launch_direct_mixed_x2(const KP& k, const DirTask* tasks, int ntask, int nd,
+                                   const SrcRange* ranges, float amax, cudaStream_t st);
 // 2D Taylor evaluation of potentials in FP32 (Pn <= 32) for the point chunks
 // of one order group, added into the sorted outputs.
 cudaError_t launch_eval2d_horner_f32(const KP& k, const HornerTask* tasks, int ntask, int nd, int Pn,
                                      const double* lo, cudaStream_t st);
+
+// Tensor-core kernels (fgt_tc.cu).  3D Taylor evaluation of potentials as
+// BF16 x 3 tcgen05 products for the point chunks of one order group.
+bool eval3d_tc_supported(int Pn);
+cudaError_t launch_eval3d_tc(const KP& k, const HornerTask* tasks, int ntask, int nd, int Pn,
+                             const double* lo, cudaStream_t st);
+// 3D Hermite partial blocks of the source chunks of one order group as BF16 x 3
+// tcgen05 products (the plain form's k_form3d_mma output layout).
+bool form3d_tc_supported(int Pn);
+cudaError_t launch_form3d_tc(const KP& k, const FormTask* tasks, const FormChunk* chunks, int nchunk,
+                             int nd, int Pn, double* hbuf, const double* isq, cudaStream_t st);
 
 }  // namespace fgtb

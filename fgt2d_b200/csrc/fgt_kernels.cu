@@ -2635,42 +2635,6 @@ __global__ void __launch_bounds__(256) k_eval3d_pw(KP k, const EvalTask* __restr
 // b0 + lane + 32 u to source indices by a binary search over the lanes'
 // prefixes, so all loads of a batch can be in flight together (a range at a
 // time would serialise one load round trip per range).
-struct RangeChunk {
-  int nr, excl, s0, tot;  // ranges in the chunk; this lane's exclusive prefix and start; chunk size
-};
-__device__ __forceinline__ RangeChunk load_range_chunk(const SrcRange* __restrict__ ranges, int off,
-                                                       int cnt, int rc, int lane) {
-  RangeChunk C;
-  C.nr = min(32, cnt - rc);
-  int rn = 0;
-  C.s0 = 0;
-  if (lane < C.nr) {
-    const SrcRange R = ranges[off + rc + lane];
-    rn = R.n;
-    C.s0 = R.s0;
-  }
-  int inc = rn;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(FULL_MASK, inc, o);
-    if (lane >= o) inc += v;
-  }
-  C.excl = inc - rn;
-  C.tot = __shfl_sync(FULL_MASK, inc, 31);
-  return C;
-}
-// source index of slot s (0 <= s < C.tot) of the chunk; all lanes must call
-__device__ __forceinline__ int range_slot_source(const RangeChunk& C, int s) {
-  int lo = 0, hi = C.nr;
-#pragma unroll
-  for (int it = 0; it < 5; it++) {
-    const int mid = (lo + hi) >> 1;
-    if (__shfl_sync(FULL_MASK, C.excl, mid) <= s) lo = mid;
-    else hi = mid;
-  }
-  return __shfl_sync(FULL_MASK, C.s0, lo) + (s - __shfl_sync(FULL_MASK, C.excl, lo));
-}
-
 // ------------------------------------------------------------ (d) near field, kernels
 // One warp per chunk of <= 32 evaluation points (g2d_directcp_vec,
 // g2ddirect.f:32-76; g3d_directcp_vec, g3ddirect.f:3-49): the chunk's source
@@ -3867,6 +3831,18 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const size_t sh = ((size_t)8 * mt + 2 * Pn) * 68 * 8;
         const dim3 fg(G.end - G.beg, nd);
         const FormChunk* ch = D.fchunks + G.beg;
+        if (mixed_ac && form3d_tc_supported(Pn)) {
+          // mixed form: the Hermite blocks as BF16 x 3 tensor-core products
+          CK(launch_form3d_tc(k, D.form, ch, G.end - G.beg, nd, Pn, D.hbuf, D.isq, st));
+          if (dom) {
+            cudaEventRecord(dev1, st);
+            snprintf(times->dom_name, sizeof(times->dom_name), "k_form3d_tc<%d>", Pn);
+            times->dom_flops = D.group_flops[gi];
+            times->dom_alg_flops = D.group_alg_flops[gi];
+          }
+          launches++;
+          continue;
+        }
         switch (mt) {
 #define FORM3_CASE(N)                                                                             \
   case N:                                                                                         \
@@ -4107,6 +4083,12 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const HornerTask* tk = D.horner + G.beg;
         const size_t sh = (size_t)Pn * Pn * np2 * 16;
         if (sh > 227 * 1024) return cudaErrorNotSupported;
+        if (mixed_ac && pgh == 1 && eval3d_tc_supported(Pn)) {
+          // mixed form: the Taylor evaluation as BF16 x 3 tensor-core products
+          CK(launch_eval3d_tc(k, tk, G.end - G.beg, nd, Pn, D.lo, st));
+          launches++;
+          continue;
+        }
         {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
           constexpr int PG = decltype(G)::value;
@@ -4186,7 +4168,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     const double l2e = 1.4426950408889634;
     const double cs = std::sqrt(l2e / P.delta);
     const float amax = (float)(P.dmax * l2e / P.delta);
-    {
+    if (mixed && pgh == 1) {
+      // potentials only: the packed-FP32 kernel
+      CK(launch_direct_mixed_x2(k, D.dir, D.ndir, nd, D.dir_src, amax, st));
+    } else {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
       constexpr int PG = decltype(G)::value;
       if (P.dim == 2) {

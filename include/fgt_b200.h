@@ -93,6 +93,14 @@ void* fgt_ctx_stream(fgt_ctx* ctx);
 /* measured FP64 tensor-core (mma.m8n8k4.f64) throughput of the context's
  * device, in TFLOP/s: the denominator of the FP64 form/eval roofline */
 int fgt_probe_fp64_mma_tflops(fgt_ctx* ctx, double* tflops);
+/* Diagnostics of the tcgen05 tensor-core path (no counterpart in the
+ * reference).  fgt_tc_selftest runs one BF16 x 3 compensated tile (M = 128,
+ * K = 16, N = n, n a multiple of 16 up to 256) on `device` and returns its
+ * largest error relative to the largest entry of an FP64 product;
+ * fgt_tc_error reads (and with clear != 0 resets) the flag the tensor-core
+ * kernels set when a bounded wait on an MMA completion gave up. */
+int fgt_tc_selftest(int device, int n, double* max_rel_err);
+int fgt_tc_error(int device, int clear, int* flag);
 
 /* ---- whole transform from host arrays ------------------------------------
  * Replaces fgt2d (2d/planewave/src/fgt2d.f:19-462) and fgt3d
