@@ -108,6 +108,18 @@ def lib():
     L.fgt_ctx_stream.argtypes = [_vp]
     L.fgt_probe_fp64_mma_tflops.argtypes = [_vp, ctypes.POINTER(ctypes.c_double)]
     L.fgt_tc_selftest.argtypes = [i, i, ctypes.POINTER(ctypes.c_double)]
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    L.fgt_plan_create_shard.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, i, i, i, ctypes.POINTER(_vp)]
+    L.fgt_plan_shard_counts.argtypes = [_vp, i, llp, llp, llp]
+    L.fgt_plan_shard_owned.argtypes = [_vp, llp, llp]
+    L.fgt_plan_execute_device_phase.argtypes = [_vp, i, _vp, _vp, _vp, _vp]
+    L.fgt_plan_mp_pack.argtypes = [_vp, i, _vp, _vp]
+    L.fgt_plan_mp_unpack.argtypes = [_vp, i, _vp, _vp]
+    L.fgt_host_shard_create.argtypes = [i, i, d, d, i, _dp, i, _dp, i, i, i, i, ctypes.POINTER(_vp)]
+    L.fgt_host_shard_counts.argtypes = [_vp, i, llp, llp]
+    L.fgt_host_shard_slots.argtypes = [_vp, i, i, ctypes.POINTER(ctypes.c_int)]
+    L.fgt_host_shard_stats.argtypes = [_vp, llp]
+    L.fgt_host_shard_destroy.argtypes = [_vp]
     L.fgt_tc_error.argtypes = [i, i, ctypes.POINTER(ctypes.c_int)]
     L.fgt_large_delta_noalloc.argtypes = [i, i, d, i, _vp, _vp, i, _dp, i, _vp, i, _vp, i, _vp, _vp]
     L.fgt_transform.argtypes = [_vp, i, i, d, d, i, _dp, i, _dp, i, _dp, _dp, i, _dp, _dp, _dp, i,

@@ -18,8 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfgt_b200.so")
 OBJDIR = os.path.join(LIBDIR, "obj")
-SOURCES = ["fgt_kernels.cu", "fgt_mixed.cu", "fgt_tc.cu", "fgt_devtree.cu", "fgt_tree.cpp", "fgt_plan.cpp", "fgt_capi.cpp"]
-HEADERS = ["fgt_tree.hpp", "fgt_plan.hpp", "fgt_device.hpp", "fgt_kcommon.cuh", "fgt_tc.cuh"]
+SOURCES = ["fgt_kernels.cu", "fgt_mixed.cu", "fgt_tc.cu", "fgt_shard.cu", "fgt_devtree.cu", "fgt_tree.cpp", "fgt_plan.cpp", "fgt_capi.cpp"]
+HEADERS = ["fgt_tree.hpp", "fgt_plan.hpp", "fgt_device.hpp", "fgt_kcommon.cuh", "fgt_tc.cuh", "fgt_shard.hpp"]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

@@ -22,6 +22,7 @@
 #include "fgt_b200.h"
 #include "fgt_device.hpp"
 #include "fgt_plan.hpp"
+#include "fgt_shard.hpp"
 
 using namespace fgtb;
 
@@ -64,6 +65,13 @@ struct fgt_plan {
   // recorded after every execute on the stream it used: the frees of
   // fgt_plan_destroy (stream-ordered on the context's stream) wait for it
   cudaEvent_t done = nullptr;
+  // spatial shard (fgt_plan_create_shard): this rank's part of the tasks and
+  // the cut-level mp slots it exchanges; d_xslots holds every peer's send
+  // list, then every peer's receive list
+  int shard_n = 1, shard_r = 0;
+  ShardInfo shard;
+  int* d_xslots = nullptr;
+  std::vector<long long> xsend_off, xrecv_off;
 };
 
 namespace {
@@ -174,6 +182,7 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
                          P.ifpghtarg > 0, P.ifdipole);
   if (sa != FGT_OK) return sa;
   cudaStream_t st = p->ctx->stream;
+  if (shard_filter(p->H, p->shard_n, p->shard_r, p->shard) != 0) return FGT_ERR_BADARG;
   if (!P.large_delta) {
     CKS(device_plan_create(p->H, p->D));
     p->have_device = true;
@@ -227,6 +236,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     return plan_device(p, hs.data(), same ? hs.data() : ht.data());
   }
   if (same && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, p->d_src, (size_t)nt * dim * 8, cudaMemcpyDeviceToDevice, s));
+  if (shard_filter(p->H, p->shard_n, p->shard_r, p->shard) != 0) return FGT_ERR_BADARG;
   if (admit) {
     size_t bytes = 0;
     DevicePlan probe;
@@ -246,7 +256,8 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
 
 // Outputs the plan's flags ask for must be non-null except gradients and
 // Hessians, which are skipped when null.
-int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st, StageTimes* times) {
+int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st, StageTimes* times,
+               int phase = 0) {
   const Params& P = p->H.P;
   if ((P.ifpgh > 0 && P.ns > 0 && !o.pot) || (P.ifpghtarg > 0 && P.nt > 0 && !o.pottarg))
     return FGT_ERR_BADARG;
@@ -266,7 +277,18 @@ int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st,
     CKS(cudaEventRecord(p->done, st));
     return FGT_OK;
   }
-  if (P.large_delta) {
+  if (P.large_delta && p->shard.large_delta_idle) {
+    // a shard rank other than 0 of a large-delta plan: its part is zero
+    const size_t nd = P.nd, nh = P.dim == 2 ? 3 : 6;
+    auto z = [&](double* a, size_t n) { return a && n ? cudaMemsetAsync(a, 0, n * 8, st) : cudaSuccess; };
+    if (P.ifpgh >= 1) CKS(z(o.pot, P.ns * nd));
+    if (P.ifpgh >= 2) CKS(z(o.grad, P.ns * nd * P.dim));
+    if (P.ifpgh >= 3) CKS(z(o.hess, P.ns * nd * nh));
+    if (P.ifpghtarg >= 1) CKS(z(o.pottarg, P.nt * nd));
+    if (P.ifpghtarg >= 2) CKS(z(o.gradtarg, P.nt * nd * P.dim));
+    if (P.ifpghtarg >= 3) CKS(z(o.hesstarg, P.nt * nd * nh));
+    p->last_launches = 0;
+  } else if (P.large_delta) {
     Outputs lo = o;  // the large-delta kernels write every component they compute
     double* dg[4] = {p->d_grad, p->d_hess, p->d_gradtarg, p->d_hesstarg};
     double** og[4] = {&lo.grad, &lo.hess, &lo.gradtarg, &lo.hesstarg};
@@ -275,7 +297,7 @@ int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st,
     CKS(large_delta_execute(P, p->d_src, in, p->d_trg, lo, p->d_work, st, true));
     p->last_launches = (P.ns > 0) + (P.ifpgh >= 1) + (P.ifpghtarg >= 1);
   } else {
-    CKS(device_plan_execute(p->D, in, o, prec, st, times));
+    CKS(device_plan_execute(p->D, in, o, prec, st, times, phase));
     p->last_launches = (int)p->D.launches;
   }
   CKS(cudaEventRecord(p->done, st));
@@ -590,6 +612,7 @@ int fgt_plan_destroy(fgt_plan* p) {
     device_plan_destroy(p->D);
   }
   if (p->d_io) cudaFreeAsync(p->d_io, p->ctx->stream);
+  if (p->d_xslots) cudaFreeAsync(p->d_xslots, p->ctx->stream);
   delete p;
   return FGT_OK;
 }
@@ -625,6 +648,179 @@ int fgt_plan_execute_device(fgt_plan* p, const double* s, const double* q, const
   Inputs in;
   in.charge = q;
   return run_device(p, in, o, st, nullptr);
+}
+
+int fgt_plan_create_shard(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                          const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                          int nranks, int rank, fgt_plan** out) {
+  if (!ctx || !out || nranks < 1 || rank < 0 || rank >= nranks) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg,
+                      ctx->tree != FGT_TREE_DEVICE);
+  if (st != FGT_OK) return st;
+  if (ns == 0) return FGT_ERR_BADARG;
+  if (!targ) nt = 0;
+  std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
+  if (!p) return FGT_ERR_NOMEM;
+  p->ctx = ctx;
+  p->shard_n = nranks;
+  p->shard_r = rank;
+  CKS(cudaSetDevice(ctx->device));
+  if (ctx->tree == FGT_TREE_DEVICE) {
+    st = plan_create_device_tree(p.get(), dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg);
+  } else {
+    try {
+      build_host_plan(p->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, ctx->nthreads);
+    } catch (const std::bad_alloc&) {
+      return FGT_ERR_NOMEM;
+    }
+    st = plan_device(p.get(), sources, targ);
+  }
+  if (st == FGT_OK && nranks > 1) {
+    // the exchange lists on the device: every peer's send list, then every peer's receive list
+    std::vector<int> all;
+    p->xsend_off.assign(nranks + 1, 0);
+    p->xrecv_off.assign(nranks + 1, 0);
+    for (int r = 0; r < nranks; r++) {
+      all.insert(all.end(), p->shard.send[r].begin(), p->shard.send[r].end());
+      p->xsend_off[r + 1] = (long long)all.size();
+    }
+    for (int r = 0; r < nranks; r++) {
+      p->xrecv_off[r] = (long long)all.size();
+      all.insert(all.end(), p->shard.recv[r].begin(), p->shard.recv[r].end());
+    }
+    p->xrecv_off[nranks] = (long long)all.size();
+    if (!all.empty()) {
+      cudaStream_t s = ctx->stream;
+      if (cudaMallocAsync(reinterpret_cast<void**>(&p->d_xslots), all.size() * sizeof(int), s) != cudaSuccess ||
+          cudaMemcpyAsync(p->d_xslots, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, s) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        st = FGT_ERR_CUDA;
+    }
+  }
+  if (st != FGT_OK) {
+    fgt_plan_destroy(p.release());
+    return st;
+  }
+  *out = p.release();
+  return FGT_OK;
+}
+
+int fgt_plan_shard_counts(fgt_plan* p, int peer, long long* nsend, long long* nrecv, long long* slot_doubles) {
+  if (!p || peer < 0 || peer >= p->shard_n) return FGT_ERR_BADARG;
+  if (nsend) *nsend = (long long)p->shard.send[peer].size();
+  if (nrecv) *nrecv = (long long)p->shard.recv[peer].size();
+  if (slot_doubles) *slot_doubles = 2LL * p->H.P.nd * p->H.P.nexp;
+  return FGT_OK;
+}
+
+int fgt_plan_shard_owned(fgt_plan* p, long long* owned_sources, long long* owned_targets) {
+  if (!p) return FGT_ERR_BADARG;
+  const bool all = p->shard_n <= 1;
+  if (owned_sources) *owned_sources = all ? p->H.P.ns : p->shard.owned_src;
+  if (owned_targets) *owned_targets = all ? p->H.P.nt : p->shard.owned_trg;
+  return FGT_OK;
+}
+
+int fgt_plan_execute_device_phase(fgt_plan* p, int phase, const double* q, double* pot, double* pt,
+                                  void* stream) {
+  if (!p || phase < 0 || phase > 2) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  Outputs o;
+  o.pot = pot;
+  o.pottarg = pt;
+  Inputs in;
+  in.charge = q;
+  if (p->H.P.large_delta && phase == 1) return FGT_OK;  // one phase: all of it runs in phase 2
+  return run_device(p, in, o, st, nullptr, p->H.P.large_delta ? 0 : phase);
+}
+
+int fgt_plan_mp_pack(fgt_plan* p, int peer, double* d_buf, void* stream) {
+  if (!p || peer < 0 || peer >= p->shard_n) return FGT_ERR_BADARG;
+  if (p->shard_n <= 1 || !p->have_device) return FGT_OK;
+  const long long n = p->xsend_off[peer + 1] - p->xsend_off[peer];
+  if (n > 0 && !d_buf) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  CKS(shard_mp_copy(p->D, p->d_xslots + p->xsend_off[peer], (int)n, d_buf, true, st));
+  return FGT_OK;
+}
+
+int fgt_plan_mp_unpack(fgt_plan* p, int peer, const double* d_buf, void* stream) {
+  if (!p || peer < 0 || peer >= p->shard_n) return FGT_ERR_BADARG;
+  if (p->shard_n <= 1 || !p->have_device) return FGT_OK;
+  const long long n = p->xrecv_off[peer + 1] - p->xrecv_off[peer];
+  if (n > 0 && !d_buf) return FGT_ERR_BADARG;
+  CKS(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  CKS(shard_mp_copy(p->D, p->d_xslots + p->xrecv_off[peer], (int)n, const_cast<double*>(d_buf), false, st));
+  return FGT_OK;
+}
+
+// Host-only view of a shard (no GPU): the host tree and plan, filtered.
+struct fgt_host_shard {
+  HostPlan H;
+  ShardInfo S;
+  long long nform = 0, neval = 0, ndir = 0, nm2l = 0, nmerge = 0, nsplit = 0;
+  int nmp = 0;
+};
+
+int fgt_host_shard_create(int dim, int nd, double delta, double eps, int ns, const double* sources, int nt,
+                          const double* targ, int ifpgh, int ifpghtarg, int nranks, int rank,
+                          fgt_host_shard** out) {
+  if (!out || nranks < 1 || rank < 0 || rank >= nranks) return FGT_ERR_BADARG;
+  *out = nullptr;
+  int st = check_args(dim, nd, delta, eps, ns, sources, 1, 0, ifpgh, nt, targ, ifpghtarg, true);
+  if (st != FGT_OK) return st;
+  if (!targ) nt = 0;
+  std::unique_ptr<fgt_host_shard> h(new (std::nothrow) fgt_host_shard());
+  if (!h) return FGT_ERR_NOMEM;
+  try {
+    build_host_plan(h->H, dim, nd, delta, eps, ns, sources, nt, targ, ifpgh, ifpghtarg, 0);
+  } catch (const std::bad_alloc&) {
+    return FGT_ERR_NOMEM;
+  }
+  if (shard_filter(h->H, nranks, rank, h->S) != 0) return FGT_ERR_BADARG;
+  h->nform = (long long)h->H.form.size();
+  h->neval = (long long)h->H.eval.size();
+  h->ndir = (long long)h->H.dir.size();
+  h->nm2l = (long long)h->H.m2l.size();
+  h->nmerge = (long long)h->H.merge.size();
+  h->nsplit = (long long)h->H.split.size();
+  h->nmp = h->H.nmp;
+  *out = h.release();
+  return FGT_OK;
+}
+int fgt_host_shard_counts(fgt_host_shard* h, int peer, long long* nsend, long long* nrecv) {
+  if (!h || peer < 0 || peer >= h->S.nranks) return FGT_ERR_BADARG;
+  if (nsend) *nsend = (long long)h->S.send[peer].size();
+  if (nrecv) *nrecv = (long long)h->S.recv[peer].size();
+  return FGT_OK;
+}
+int fgt_host_shard_slots(fgt_host_shard* h, int peer, int which, int* out) {
+  if (!h || !out || peer < 0 || peer >= h->S.nranks || which < 0 || which > 1) return FGT_ERR_BADARG;
+  const std::vector<int>& v = which == 0 ? h->S.send[peer] : h->S.recv[peer];
+  std::copy(v.begin(), v.end(), out);
+  return FGT_OK;
+}
+int fgt_host_shard_stats(fgt_host_shard* h, long long* out8) {
+  if (!h || !out8) return FGT_ERR_BADARG;
+  const bool all = h->S.nranks <= 1;
+  out8[0] = all ? h->H.P.ns : h->S.owned_src;
+  out8[1] = all ? h->H.P.nt : h->S.owned_trg;
+  out8[2] = h->nform;
+  out8[3] = h->neval;
+  out8[4] = h->ndir;
+  out8[5] = h->nm2l;
+  out8[6] = h->nmerge + h->nsplit;
+  out8[7] = h->nmp;
+  return FGT_OK;
+}
+int fgt_host_shard_destroy(fgt_host_shard* h) {
+  delete h;
+  return FGT_OK;
 }
 
 int fgt_plan_execute_device_pgh(fgt_plan* p, const double* q, double* pot, double* grad, double* hess,

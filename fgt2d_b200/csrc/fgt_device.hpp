@@ -195,8 +195,11 @@ cudaError_t device_plan_set_points(DevicePlan& D, const double* src, const doubl
 // Runs charge gather -> stages -> scatter on `stream`.  Device pointers in
 // the caller's order: charge (ns, nd) and the outputs.
 // times (optional) receives per-stage milliseconds (synchronises).
+// phase: 0 everything; 1 through the merge (every mp expansion up to the
+// cut level), 2 from mp -> loc on (the caller may replace mp expansions of
+// the cut level between the two).
 cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& out,
-                                int precision, cudaStream_t stream, StageTimes* times);
+                                int precision, cudaStream_t stream, StageTimes* times, int phase = 0);
 
 // Sets *d_flag (device int, not cleared here) when any of x[0, n) is not
 // finite; asynchronous on st.

@@ -3722,8 +3722,11 @@ cudaError_t with_pgh(int pgh, F&& launch) {
 }
 
 cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& outs,
-                                int precision, cudaStream_t st, StageTimes* times) {
+                                int precision, cudaStream_t st, StageTimes* times, int phase) {
   const Params& P = D.P;
+  // phase 1: gather, form, merge (every mp expansion up to the cut level);
+  // phase 2: mp -> loc, split, eval, near field, scatter; 0: both
+  const bool ph1 = phase != 2, ph2 = phase != 1;
   KP k = make_kp(D);
   // the derivative order the kernels compute: the larger of the two sets'
   const int pgh = std::max(1, std::max(P.ifpgh, P.ifpghtarg));
@@ -3747,19 +3750,22 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
   mark(0);
   // charges into tree order (coordinates were sorted once, at plan set-up)
   const int gb = std::max(1, std::min(8 * D.sm_count, (std::max(P.ns, P.nt) + 255) / 256));
-  if (P.ns > 0 && P.ifcharge) {
+  if (ph1 && P.ns > 0 && P.ifcharge) {
     k_gather_pts<<<gb, 256, 0, st>>>(nullptr, in.charge, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
-  if (P.ns > 0 && P.ifdipole) {  // directions and strengths of the dipoles
+  if (ph1 && P.ns > 0 && P.ifdipole) {  // directions and strengths of the dipoles
     k_gather_pts<<<gb, 256, 0, st>>>(in.rnormal, in.dipstr, D.nsort, D.dsort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
-  if (P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * k.nc_s * 8, st));
-  if (P.ifpghtarg > 0 && P.nt > 0) CK(cudaMemsetAsync(D.ptsort, 0, (size_t)P.nt * nd * k.nc_t * 8, st));
+  if (ph1 && P.ifpgh > 0 && P.ns > 0) CK(cudaMemsetAsync(D.psort, 0, (size_t)P.ns * nd * k.nc_s * 8, st));
+  if (ph1 && P.ifpghtarg > 0 && P.nt > 0) CK(cudaMemsetAsync(D.ptsort, 0, (size_t)P.nt * nd * k.nc_t * 8, st));
   mark(1);
   const int n2 = P.npw / 2;
+  const int echunks = (int)std::min<long long>(65535, ((long long)nd * P.nexp + 255) / 256);
+  const int schunks = (P.nexp + 256 * SHU - 1) / (256 * SHU);  // k_split: every density per block
   if (!P.all_direct) {
+   if (ph1) {
     // (a) form
     if (P.dim == 2 && D.form_hermite_n > 0) {
       for (size_t gi = 0; gi < D.form_groups.size(); gi++) {
@@ -3927,15 +3933,15 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     }
     mark(2);
     // (b) merge, bottom-up
-    const int echunks = (int)std::min<long long>(65535, ((long long)nd * P.nexp + 255) / 256);
-    const int schunks = (P.nexp + 256 * SHU - 1) / (256 * SHU);  // k_split: every density per block
     for (int l = P.nlevels - 1; l >= P.nlevstart; l--) {
       int ng = D.merge_end[l] - D.merge_beg[l];
       if (ng <= 0) continue;
       k_merge<<<dim3(ng, echunks), 256, 0, st>>>(k, D.mgroups + D.merge_beg[l], D.merge);
       launches++;
     }
+   }  // phase 1
     mark(3);
+   if (ph2) {
     if (D.nm2l > 0) {
       k_m2l<<<dim3(D.nm2l, echunks), 256, 0, st>>>(k, D.m2l, D.m2l_nbr);
       launches++;
@@ -4156,12 +4162,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         }
       launches++;
     }
+   }  // phase 2
   } else {
     mark(2); mark(3); mark(4); mark(5);
   }
   mark(6);
   // (d) near field
-  if (D.ndir > 0) {
+  if (ph2 && D.ndir > 0) {
     dim3 g((D.ndir + 3) / 4, nd);
     // dipoles take the FP64 near field (the mixed form is charges only)
     const bool mixed = precision == PREC_MIXED && !P.ifdipole;
@@ -4207,8 +4214,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       launches++;
     }
   };
-  if (P.ifpgh > 0 && P.ns > 0) unsort(D.psort, D.isrc_inv, P.ns, k.nc_s, outs.pot, outs.grad, outs.hess);
-  if (P.ifpghtarg > 0 && P.nt > 0)
+  if (ph2 && P.ifpgh > 0 && P.ns > 0) unsort(D.psort, D.isrc_inv, P.ns, k.nc_s, outs.pot, outs.grad, outs.hess);
+  if (ph2 && P.ifpghtarg > 0 && P.nt > 0)
     unsort(D.ptsort, D.itarg_inv, P.nt, k.nc_t, outs.pottarg, outs.gradtarg, outs.hesstarg);
   mark(8);
   D.launches = launches;

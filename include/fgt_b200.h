@@ -224,6 +224,48 @@ int fgt_plan_profile_dominant(fgt_plan* plan, const double* d_charge, double* d_
                               double* ms, double* flops, double* alg_flops, char* name, int name_len);
 int fgt_plan_destroy(fgt_plan* plan);
 
+/* ---- spatial shard of one transform over several GPUs ----------------------
+ * No counterpart in the reference (which runs on one node).  The cut-level
+ * boxes are cut into `nranks` Morton ranges of nearly equal point counts;
+ * rank `rank` computes the boxes of its range: their formation, merge,
+ * mp -> loc, split, evaluation and near field.  The one exchange is the
+ * cut-level multipole expansions that mp -> loc reads across a range
+ * boundary (the coupling of fgt2d.f:1026-1064 / fgt3d.f:1172-1209); the
+ * points are replicated on every rank.  Use:
+ *   fgt_plan_create_shard(...)                  same arguments on every rank
+ *   fgt_plan_execute_device_phase(plan, 1, ...)  form + merge
+ *   for every peer: fgt_plan_mp_pack(plan, peer, sendbuf[peer]) and send it;
+ *     receive recvbuf[peer], then fgt_plan_mp_unpack(plan, peer, recvbuf[peer])
+ *   fgt_plan_execute_device_phase(plan, 2, ...)  mp -> loc .. scatter
+ * Each rank's outputs hold its owned points and zeros elsewhere; their sum
+ * is the one-GPU result bit for bit.  Buffers hold nsend (nrecv) expansions
+ * of slot_doubles doubles each (fgt_plan_shard_counts).  A large-delta plan
+ * runs whole on rank 0. */
+int fgt_plan_create_shard(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int ns,
+                          const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
+                          int nranks, int rank, fgt_plan** out);
+int fgt_plan_shard_counts(fgt_plan* plan, int peer, long long* nsend, long long* nrecv,
+                          long long* slot_doubles);
+int fgt_plan_shard_owned(fgt_plan* plan, long long* owned_sources, long long* owned_targets);
+/* phase 0: the whole execute; 1: through the merge; 2: from mp -> loc on */
+int fgt_plan_execute_device_phase(fgt_plan* plan, int phase, const double* d_charge, double* d_pot,
+                                  double* d_pottarg, void* stream);
+int fgt_plan_mp_pack(fgt_plan* plan, int peer, double* d_buf, void* stream);
+int fgt_plan_mp_unpack(fgt_plan* plan, int peer, const double* d_buf, void* stream);
+/* Host-only view of a shard (no GPU needed): the host tree and plan of the
+ * same points, filtered for (nranks, rank); the exchange lists as mp slot
+ * numbers (which = 0: send to peer, 1: receive from peer) and statistics
+ * out8 = {owned sources, owned targets, form tasks, eval tasks, near-field
+ * tasks, mp -> loc tasks, merge + split tasks, mp slots}. */
+typedef struct fgt_host_shard fgt_host_shard;
+int fgt_host_shard_create(int dim, int nd, double delta, double eps, int ns, const double* sources, int nt,
+                          const double* targ, int ifpgh, int ifpghtarg, int nranks, int rank,
+                          fgt_host_shard** out);
+int fgt_host_shard_counts(fgt_host_shard* h, int peer, long long* nsend, long long* nrecv);
+int fgt_host_shard_slots(fgt_host_shard* h, int peer, int which, int* out);
+int fgt_host_shard_stats(fgt_host_shard* h, long long* out8);
+int fgt_host_shard_destroy(fgt_host_shard* h);
+
 /* ---- host tree (no device needed) ----------------------------------------
  * The level-restricted tree the transform builds (pts_tree_boxsize0,
  * pts_tree_mem/build/sort: pts_tree2d4.f:34-1258, pts_tree3d.f:34-1685),
