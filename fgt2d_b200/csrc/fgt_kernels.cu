@@ -1554,9 +1554,31 @@ struct C3Dims {
     ldL = ((2 * npw + 7) & ~15) + 8;
     ld1 = 8 * Pn + 4;
     ld2 = 8 * ((Pn * Pn + 7) / 8) + 4;
-    total = (size_t)4 * npw * ldL + (size_t)npw * ld1 + (size_t)8 * ld2;
+    total = (size_t)4 * npw * ldL + (size_t)npw * ld1 + (size_t)8 * ld2 + (size_t)2 * (2 * npw + npw / 2);
   }
 };
+// The fused split's phase tables of one task (x and y over all npw nodes, z
+// over the stored half) into ph (double2 [2 npw + n2]); node t_m = x2l[1][m].
+__device__ __forceinline__ void conv_phases(const KP& k, const ConvTask& T, double2* ph) {
+  const int npw = k.npw, n2 = k.n2;
+  for (int e = threadIdx.x; e < 2 * npw + n2; e += blockDim.x) {
+    const int d = e < npw ? 0 : e < 2 * npw ? 1 : 2, m = e - d * npw;
+    double sn, cs;
+    sincos(k.x2l[npw + m] * T.sh[d], &sn, &cs);
+    ph[e] = make_double2(cs, sn);
+  }
+}
+// Multiplies staged slices (rows (m1, m2) of npw complex m3, row stride ldL
+// doubles, slices m1 = m1_0 .. m1_0 + ns - 1) by the task's phases.
+__device__ __forceinline__ void conv_apply_phases(double* Lb, int ldL, int npw, int m1_0, int ns,
+                                                  const double2* ph) {
+  const int n = ns * npw * npw;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int row = e / npw, m3 = e - row * npw, m1 = m1_0 + row / npw, m2 = row - (row / npw) * npw;
+    double2* z = reinterpret_cast<double2*>(Lb + (size_t)row * ldL + 2 * m3);
+    *z = cmul(*z, cmul(ph[m3], cmul(ph[npw + m2], ph[2 * npw + m1])));
+  }
+}
 
 template <int KS>
 __global__ void __launch_bounds__(256, 2) k_pw2taylor3d_mma(KP k, const ConvTask* __restrict__ tasks, int ntask,
@@ -1572,6 +1594,7 @@ __global__ void __launch_bounds__(256, 2) k_pw2taylor3d_mma(KP k, const ConvTask
   double* S1 = Lb + (size_t)4 * npw * Z.ldL;        // [npw m2][ld1]: (m1, a, re/im)
   double* S2r = S1 + (size_t)npw * Z.ld1;           // [4 m1][ld2]: (b, a)
   double* S2i = S2r + 4 * Z.ld2;
+  double2* PH = reinterpret_cast<double2*>(S2i + 4 * Z.ld2);  // fused split: [2 npw + n2] phases
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
   int tk = blockIdx.x;
   if (tk >= ntask) return;
@@ -1605,10 +1628,16 @@ __global__ void __launch_bounds__(256, 2) k_pw2taylor3d_mma(KP k, const ConvTask
     const int tn = tk + gridDim.x;
     const int nslot = tn < ntask ? tasks[tn].slot : 0;
     const long long off = tasks[tk].off;
+    const bool fused = tasks[tk].fused;
+    if (fused) conv_phases(k, tasks[tk], PH);
     for (int g = 0; g < KS; g++) {
       const int ns = min(4, n2 - 4 * g);
       asm volatile("cp.async.wait_all;" ::: "memory");
       __syncthreads();
+      if (fused) {  // the ancestor's slices become the leaf's: the split, fused
+        conv_apply_phases(Lb, Z.ldL, npw, 4 * g, ns, PH);
+        __syncthreads();
+      }
       // x pass: columns (m1, m2, re/im) of the staged slices
       const int ntX = (ns * npw * 2 + 7) / 8;
       for (int nt = warp; nt < ntX; nt += 8) {
@@ -1725,7 +1754,7 @@ struct C3Dims2 {
     ldL = ((2 * npw + 7) & ~15) + 8;
     ld1 = 8 * ((2 * gs * Pn + 7) / 8) + 4;
     ld2 = 8 * ((Pn * Pn + 7) / 8) + 4;
-    total = (size_t)gs * npw * ldL + (size_t)npw * ld1 + (size_t)2 * n2 * ld2;
+    total = (size_t)gs * npw * ldL + (size_t)npw * ld1 + (size_t)2 * n2 * ld2 + (size_t)2 * (2 * npw + n2);
   }
 };
 
@@ -1742,6 +1771,7 @@ __global__ void __launch_bounds__(256, 1) k_pw2taylor3d_mma2(KP k, const ConvTas
   double* S1 = Lb + (size_t)gs * npw * Z.ldL;       // [npw m2][ld1]: (m1, a, re/im)
   double* S2r = S1 + (size_t)npw * Z.ld1;           // [n2 m1][ld2]: (b, a)
   double* S2i = S2r + (size_t)n2 * Z.ld2;
+  double2* PH = reinterpret_cast<double2*>(S2i + (size_t)n2 * Z.ld2);  // fused split: [2 npw + n2] phases
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, r = lane >> 2, c = lane & 3;
   int tk = blockIdx.x;
   if (tk >= ntask) return;
@@ -1775,10 +1805,16 @@ __global__ void __launch_bounds__(256, 1) k_pw2taylor3d_mma2(KP k, const ConvTas
     const int tn = tk + gridDim.x;
     const int nslot = tn < ntask ? tasks[tn].slot : 0;
     const long long off = tasks[tk].off;
+    const bool fused = tasks[tk].fused;
+    if (fused) conv_phases(k, tasks[tk], PH);
     for (int g = 0; g < ng; g++) {
       const int ns = min(gs, n2 - gs * g);
       asm volatile("cp.async.wait_all;" ::: "memory");
       __syncthreads();
+      if (fused) {  // the ancestor's slices become the leaf's: the split, fused
+        conv_apply_phases(Lb, Z.ldL, npw, gs * g, ns, PH);
+        __syncthreads();
+      }
       // x pass: columns (m1, m2, re/im) of the staged slices
       const int ntX = (ns * npw * 2 + 7) / 8;
       for (int nt = warp; nt < ntX; nt += 8) {
@@ -3352,6 +3388,20 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   }
   D.eval3_split = D.eval3_nsplit > 0;
   const int split_pmax = D.eval3_split ? ev[D.eval3_nsplit - 1].p : -1;
+  // 3D: the split is fused into the conversion kernels that stage the
+  // expansion in shared memory (orders <= 32): they read the cut-level
+  // ancestor's local expansion and apply the leaf's phases (ConvTask.sh)
+  auto conv3_fusable = [&](int Pn) {
+    const int ksm = (P.npw / 2 + 3) / 4;
+    if (P.dim != 3 || ksm > 8) return false;
+    if (Pn <= 16) return C3Dims(Pn, P.npw).total * 8 <= 227 * 1024;
+    if (Pn > 32) return false;
+    int gs2 = 4;
+    while (gs2 > 1 && C3Dims2(Pn, P.npw, gs2).total * 8 > 227 * 1024) gs2 >>= 1;
+    return C3Dims2(Pn, P.npw, gs2).total * 8 <= 227 * 1024;
+  };
+  const int lcut = std::max(P.npwlevel, 0);
+  std::vector<uint8_t> fused_leaf(H.tree.nboxes, 0);
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     const int ntay = P.dim == 2 ? D.eval_taylor_n : D.eval3_nsplit;
@@ -3360,7 +3410,18 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       const long long Pn = e.p + 1, E = (Pn + 1) & ~1LL;
       if (slot_off[e.slot] < 0) {
         slot_off[e.slot] = (long long)lo_doubles;
-        conv.push_back({e.slot, e.p, (long long)lo_doubles});
+        ConvTask ct{e.slot, e.p, (long long)lo_doubles};
+        if (conv3_fusable((int)Pn) && H.tree.level[e.box] > lcut) {
+          int a = e.box;
+          while (H.tree.level[a] > lcut) a = H.tree.parent[a];
+          if (a >= 0 && H.loc_slot[a] >= 0) {
+            ct.slot = H.loc_slot[a];
+            ct.fused = 1;
+            for (int d = 0; d < P.dim; d++) ct.sh[d] = (H.tree.c(e.box, d) - H.tree.c(a, d)) * P.dsq;
+            fused_leaf[e.box] = 1;
+          }
+        }
+        conv.push_back(ct);
         lo_doubles += (size_t)(P.nd * Pn * E * (P.dim == 3 ? Pn : 1));
       }
       for (int c = 0; c < e.n; c += 256)
@@ -3412,8 +3473,32 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     }
     D.merge_end[l] = (int)groups.size();
   }
-  D.split_beg = H.split_beg;
-  D.split_end = H.split_end;
+  // the split tasks still needed: the boxes on the path from the cut level
+  // to every evaluation leaf whose conversion does not fuse the split
+  std::vector<ShiftTask> split_kept;
+  {
+    const Tree& tr = H.tree;
+    std::vector<uint8_t> need(tr.nboxes, 0);
+    for (int t = 0; t < (int)H.eval.size(); t++) {
+      int b = H.eval[t].box;
+      if (fused_leaf[b]) continue;
+      while (b >= 0 && tr.level[b] > lcut && !need[b]) {
+        need[b] = 1;
+        b = tr.parent[b];
+      }
+    }
+    std::vector<int> loc_box(std::max(H.nloc, 1), -1);
+    for (int b = 0; b < tr.nboxes; b++)
+      if (H.loc_slot[b] >= 0) loc_box[H.loc_slot[b]] = b;
+    D.split_beg.assign(H.split_beg.size(), 0);
+    D.split_end.assign(H.split_end.size(), 0);
+    for (size_t l = 0; l < H.split_beg.size(); l++) {
+      D.split_beg[l] = (int)split_kept.size();
+      for (int i = H.split_beg[l]; i < H.split_end[l]; i++)
+        if (need[loc_box[H.split[i].dst]]) split_kept.push_back(H.split[i]);
+      D.split_end[l] = (int)split_kept.size();
+    }
+  }
   D.nm2l = (int)H.m2l.size();
   D.ndir = (int)H.dir.size();
   D.nmp = H.nmp;
@@ -3516,7 +3601,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   const size_t n_wsh = P.all_direct ? 0 : (size_t)(P.dim == 2 ? 9 : 27) * P.nexp;
   size_t total = bytes_of(H.box_centers) + bytes_of(H.h2x) + bytes_of(H.x2l) + al(n_wms * 16) + al(n_wsh * 16) + al(H.ww.size() * 8) + al(H.w1.size() * 8) + 2 * al((size_t)P.ns * 4) + 2 * al((size_t)P.nt * 4) +
                  al((size_t)(std::max(P.ntermmax, 1) + 2) * 8) + al(32 * 8) +
-                 bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(H.split) +
+                 bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(split_kept) +
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
@@ -3610,7 +3695,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     st.add(cur, D.form, form);
     st.add(cur, D.mgroups, groups);
     st.add(cur, D.merge, H.merge);
-    st.add(cur, D.split, H.split);
+    st.add(cur, D.split, split_kept);
     st.add(cur, D.m2l, H.m2l);
     st.add(cur, D.m2l_nbr, H.m2l_nbr);
     st.add(cur, D.eval, ev);
