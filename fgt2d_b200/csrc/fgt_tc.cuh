@@ -116,6 +116,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// The same without the wait, for several loads in flight: the registers are
+// valid only after tmem_wait_ld(); tmem_fix() then ties each register to a
+// point after the wait, so that no use of it is scheduled before.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fix(uint32_t* r) {
+#pragma unroll
+  for (int i = 0; i < 16; i++) asm volatile("" : "+r"(r[i])::"memory");
+}
+
 // ---- exact three-piece BF16 split: v = f0 + f1 + f2 with each fi a BF16 value ----
 // f0 keeps the top 8 significant bits of v (truncation), f1 the next 8 of the
 // exact remainder, f2 the rest (at most 8 significant bits), so no rounding
