@@ -96,6 +96,7 @@ def lib():
     L.fgt_ctx_set_precision.argtypes = [_vp, i]
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
     L.fgt_ctx_set_tree.argtypes = [_vp, i]
+    L.fgt_ctx_set_sm_budget.argtypes = [_vp, i]
     L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
     L.fgt_server_set_precision.argtypes = [_vp, i]
     L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
@@ -180,6 +181,10 @@ class Context:
     def set_tree(self, where):
         """Where plans build their tree: "device" (point work on the GPU) or "host"."""
         _check(lib().fgt_ctx_set_tree(self._h, {"device": 0, "host": 1}[where]), "fgt_ctx_set_tree")
+
+    def set_sm_budget(self, sms):
+        """SMs the persistent kernels of plans created afterwards size their grids for (0: all)."""
+        _check(lib().fgt_ctx_set_sm_budget(self._h, int(sms)), "fgt_ctx_set_sm_budget")
 
     def set_precision(self, precision):
         p = _PREC[precision] if isinstance(precision, str) else int(precision)

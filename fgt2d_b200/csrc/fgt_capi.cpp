@@ -32,6 +32,7 @@ struct fgt_ctx {
   int precision = FGT_PREC_AUTO;
   int tree = FGT_TREE_DEVICE;
   int nthreads = 0;
+  int sm_budget = 0;  // SMs the persistent kernels of this context's plans size their grids for (0: all)
   std::mutex mu;
 };
 
@@ -186,6 +187,7 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
   if (!P.large_delta) {
     CKS(device_plan_create(p->H, p->D));
     p->have_device = true;
+    p->D.persist_sms = p->ctx->sm_budget;
     CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, st));
   }
   return FGT_OK;
@@ -246,6 +248,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   }
   CKS(device_plan_create(p->H, p->D, d_isrc, d_itarg, s));
   p->have_device = true;
+  p->D.persist_sms = p->ctx->sm_budget;
   CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, s));
   CKS(cudaStreamSynchronize(s));
   if (getenv("FGT_TREE_TIMING"))
@@ -482,6 +485,11 @@ int fgt_ctx_set_precision(fgt_ctx* c, int precision) {
 int fgt_ctx_set_tree(fgt_ctx* c, int where) {
   if (!c || (where != FGT_TREE_DEVICE && where != FGT_TREE_HOST)) return FGT_ERR_BADARG;
   c->tree = where;
+  return FGT_OK;
+}
+int fgt_ctx_set_sm_budget(fgt_ctx* c, int sms) {
+  if (!c || sms < 0) return FGT_ERR_BADARG;
+  c->sm_budget = sms;
   return FGT_OK;
 }
 int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
@@ -1498,6 +1506,13 @@ int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_
       return st;
     }
     S->ctxs.push_back(c);
+  }
+  {
+    // a request's persistent kernels use at most half of the SMs, so that
+    // the requests arriving meanwhile find SMs free at once
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess)
+      for (fgt_ctx* c : S->ctxs) c->sm_budget = std::max(1, sms / 2);
   }
   {
     // reserve the budget in the device's stream-ordered pool once (it keeps

@@ -163,6 +163,11 @@ struct DevicePlan {
   double* tables = nullptr;  // padded operand tables of the 2D MMA transforms
   std::vector<OrderGroup> conv_groups, horner_groups;
   int sm_count = 148;
+  // SMs the persistent kernels of this plan size their grids for (0: all);
+  // a server caps it so that a large request's persistent kernels leave SMs
+  // to the requests that arrive while they run
+  int persist_sms = 0;
+  int psm() const { return persist_sms > 0 && persist_sms < sm_count ? persist_sms : sm_count; }
   // statistics copied from the host plan
   long long direct_pairs = 0, form_sources = 0, eval_points = 0;
   long long launches = 0;

@@ -172,6 +172,97 @@ __global__ void __launch_bounds__(256) k_locate(const double* __restrict__ x, in
   if (i < n && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(leafcnt + r, __popc(m));
 }
 
+// Exact child digits of every point: the descent from the root for L levels
+// with the tree's own centre arithmetic (a child's centre is its parent's
+// plus or minus a quarter of the parent's size, the test is coordinate minus
+// centre < 0 as sort_pts_to_children), packed most significant level first.
+// Every box the refinement can create is a contiguous range of these keys in
+// sorted order, and sorted order is the depth-first order of the leaves.
+__global__ void __launch_bounds__(256) k_exact_key(const double* __restrict__ x, int n, int dim, double cx,
+                                                   double cy, double cz, double bs0, int L,
+                                                   unsigned long long* __restrict__ key, int* __restrict__ id) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[3] = {0, 0, 0}, c[3] = {cx, cy, cz};
+  for (int d = 0; d < dim; d++) p[d] = x[(size_t)dim * i + d];
+  double bs = bs0;
+  unsigned long long k = 0;
+  for (int l = 0; l < L; l++) {
+    int j = 0;
+    for (int d = 0; d < dim; d++)
+      if (!(p[d] - c[d] < 0)) j |= 1 << d;
+    k = (k << dim) | (unsigned long long)j;
+    bs = bs / 2;  // size of the child level
+    const double h = bs / 2;
+    for (int d = 0; d < dim; d++) c[d] = c[d] + (((j >> d) & 1) ? h : -h);
+  }
+  key[i] = k;
+  id[i] = i;
+}
+
+// First position in [lo, hi) whose digit (key >> shift) & (nch - 1) is >= v;
+// the digits are nondecreasing there (the range is one box of the level
+// above the digit).
+__device__ __forceinline__ int digit_lower_bound(const unsigned long long* __restrict__ key, int lo, int hi,
+                                                 int shift, int nch, int v) {
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if ((int)((key[m] >> shift) & (unsigned long long)(nch - 1)) < v) lo = m + 1;
+    else hi = m;
+  }
+  return lo;
+}
+
+// Ranges of the children of the boxes [a, a + nlev) of one level, from the
+// parents' ranges: one thread per (box, child).  With fc (refinement), the
+// children of box a + i are fc[i] + j (fc[i] < 0: not refined) and their
+// source counts go to cnt[child - c0]; with child (the finished tree), they
+// are child[box * nch + j].
+__global__ void __launch_bounds__(256) k_child_ranges(const unsigned long long* __restrict__ key, int shift,
+                                                      int nch, int a, int nlev, const int* __restrict__ fc,
+                                                      const int* __restrict__ child, int* __restrict__ r0,
+                                                      int* __restrict__ r1, int c0, int* __restrict__ cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nlev * nch) return;
+  const int i = t / nch, j = t - i * nch, box = a + i;
+  const int c = fc ? (fc[i] >= 0 ? fc[i] + j : -1) : child[(size_t)box * nch + j];
+  if (c < 0) return;
+  const int lo = r0[box], hi = r1[box];
+  const int s = digit_lower_bound(key, lo, hi, shift, nch, j);
+  const int e = j == nch - 1 ? hi : digit_lower_bound(key, s, hi, shift, nch, j + 1);
+  r0[c] = s;
+  r1[c] = e;
+  if (cnt) cnt[c - c0] = e - s;
+}
+
+// Sort key of the final point order: the depth-first rank of the leaf that
+// holds sorted position k (leaf ranges start at lstart[rank], ascending),
+// scattered to the point's input index, with the input index as the value
+// (a stable sort on the rank keeps the input order inside a leaf).
+__global__ void __launch_bounds__(256) k_position_rank(const int* __restrict__ lstart, int nleaf,
+                                                       const int* __restrict__ wid, int n, int* __restrict__ rk,
+                                                       int* __restrict__ idx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int lo = 0, hi = nleaf;  // last leaf whose start is <= k
+  while (hi - lo > 1) {
+    const int m = (lo + hi) >> 1;
+    if (lstart[m] <= k) lo = m;
+    else hi = m;
+  }
+  rk[wid[k]] = lo;
+  idx[k] = k;
+}
+__global__ void k_leaf_starts(const int* __restrict__ r0, const int* __restrict__ leaf_of_rank, int nleaf,
+                              int* __restrict__ lstart) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nleaf) lstart[r] = r0[leaf_of_rank[r]];
+}
+__global__ void k_root_range(int* r0, int* r1, int n) {
+  r0[0] = 0;
+  r1[0] = n;
+}
+
 // Device scratch of one build, stream-ordered on the build's stream (no
 // device-wide synchronisation) and freed at the end of the build.
 struct Scratch {
@@ -262,9 +353,157 @@ cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_
   return device_bbox(d_src, ns, d_trg, nt, dim, mn, mx, st);
 }
 
+// The tree from the exact child digits of the sources (k_exact_key), for
+// trees whose depth fits a 64-bit key (31 levels in 2D, 21 in 3D): one sort
+// of the keys, after which every refinement level is a binary search per
+// (refined box, child) inside the parent's range, and the final point order
+// is the key order with the input order restored inside each leaf.  No pass
+// over the points per level, and the same tree, ranges and permutations as
+// the per-level refinement below.
+cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
+                                   bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st) {
+  const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
+  const double tA = now_s();
+  tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
+  Scratch S(st);
+  const int L = ts.nlmax, nch = 1 << dim;
+  unsigned long long *key = nullptr, *skey = nullptr;
+  int *wid0 = nullptr, *wid = nullptr;
+  CKD(S.get(&key, ns));
+  CKD(S.get(&skey, ns));
+  CKD(S.get(&wid0, ns));
+  CKD(S.get(&wid, ns));
+  k_exact_key<<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, dim, ts.cen0[0], ts.cen0[1], ts.cen0[2], ts.bs0, L, key,
+                                                wid0);
+  {
+    size_t tmp = 0;
+    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, wid0, wid, ns, 0, dim * L, st));
+    char* dtmp = nullptr;
+    CKD(S.get(&dtmp, tmp));
+    CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, key, skey, wid0, wid, ns, 0, dim * L, st));
+  }
+  // per-box ranges in key order, grown with the box count
+  int *r0 = nullptr, *r1 = nullptr;
+  size_t cap = 0;
+  auto grow = [&](size_t need) -> cudaError_t {
+    if (need <= cap) return cudaSuccess;
+    const size_t nc = std::max<size_t>({need, 2 * cap, 4096});
+    int *n0 = nullptr, *n1 = nullptr;
+    CKD(S.get(&n0, nc));
+    CKD(S.get(&n1, nc));
+    if (cap) {
+      CKD(cudaMemcpyAsync(n0, r0, cap * 4, cudaMemcpyDeviceToDevice, st));
+      CKD(cudaMemcpyAsync(n1, r1, cap * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    r0 = n0;
+    r1 = n1;
+    cap = nc;
+    return cudaSuccess;
+  };
+  CKD(grow(1));
+  k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
+  // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
+  std::vector<int> count(1, ns), fc;
+  int *d_fc = nullptr, *d_cnt = nullptr;
+  size_t cap_lev = 0, cap_new = 0;
+  int lev;
+  double th = 0;
+  for (lev = 0; lev <= ts.nlmax - 1; lev++) {
+    const int a = t.lfirst[lev], b = t.llast[lev];
+    const int thr = lev < ts.levcut ? ts.ndiv0 : ts.ndiv;
+    const double th0 = now_s();
+    if (tree_refine_level(t, lev, thr, count, fc) == 0) break;
+    th += now_s() - th0;
+    const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0, nlev = b - a + 1;
+    CKD(grow(t.nboxes));
+    if ((size_t)nlev > cap_lev) {
+      cap_lev = (size_t)nlev * 2;
+      CKD(S.get(&d_fc, cap_lev));
+    }
+    if ((size_t)nnew > cap_new) {
+      cap_new = (size_t)nnew * 2;
+      CKD(S.get(&d_cnt, cap_new));
+    }
+    CKD(upload(d_fc, fc.data(), nlev, st));
+    k_child_ranges<<<(nlev * nch + 255) / 256, 256, 0, st>>>(skey, dim * (L - 1 - lev), nch, a, nlev, d_fc,
+                                                              nullptr, r0, r1, c0, d_cnt);
+    count.resize(t.nboxes, 0);
+    CKD(cudaMemcpyAsync(count.data() + c0, d_cnt, sizeof(int) * nnew, cudaMemcpyDeviceToHost, st));
+    CKD(cudaStreamSynchronize(st));
+  }
+  const double tB = now_s();
+  std::vector<int> idmap;
+  tree_finish(t, lev, idmap);
+  const double tC = now_s();
+  std::vector<int> dfs_rank, leaf_of_rank;
+  tree_leaf_ranks(t, dfs_rank, leaf_of_rank);
+  const int nb = t.nboxes, nleaf = (int)leaf_of_rank.size();
+  int *d_nchild = nullptr, *d_child = nullptr, *d_lor = nullptr;
+  CKD(S.get(&d_nchild, nb));
+  CKD(S.get(&d_child, (size_t)nb * nch));
+  CKD(S.get(&d_lor, nleaf));
+  CKD(upload(d_nchild, t.nchild.data(), nb, st));
+  CKD(upload(d_child, t.child.data(), (size_t)nb * nch, st));
+  CKD(upload(d_lor, leaf_of_rank.data(), nleaf, st));
+  // ranges of the finished tree (the level restriction added boxes and
+  // renumbered), level by level from the root
+  CKD(grow(nb));
+  k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
+  for (int l = 0; l < t.nlevels; l++) {
+    const int a = t.lfirst[l], n = t.llast[l] - a + 1;
+    if (n > 0)
+      k_child_ranges<<<(n * nch + 255) / 256, 256, 0, st>>>(skey, dim * (L - 1 - l), nch, a, n, nullptr, d_child,
+                                                            r0, r1, 0, nullptr);
+  }
+  t.s0.assign(nb, 0);
+  t.s1.assign(nb, 0);
+  CKD(cudaMemcpyAsync(t.s0.data(), r0, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.s1.data(), r1, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+  // final order: leaf rank of each sorted position, to input order, stable sort
+  {
+    int *lstart = nullptr, *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
+    CKD(S.get(&lstart, nleaf));
+    CKD(S.get(&rk, ns));
+    CKD(S.get(&rk2, ns));
+    CKD(S.get(&idx, ns));
+    k_leaf_starts<<<(nleaf + 255) / 256, 256, 0, st>>>(r0, d_lor, nleaf, lstart);
+    k_position_rank<<<(ns + 255) / 256, 256, 0, st>>>(lstart, nleaf, wid, ns, rk, idx);
+    int bits = 1;
+    while ((1 << bits) < nleaf) bits++;
+    size_t tmp = 0;
+    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
+    char* dtmp = nullptr;
+    CKD(S.get(&dtmp, tmp));
+    CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
+  }
+  const double tD = now_s();
+  if (same) {
+    if (nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+    CKD(cudaStreamSynchronize(st));
+    t.t0 = t.s0;
+    t.t1 = t.s1;
+  } else {
+    int* d_rank = nullptr;
+    double* d_centers = nullptr;
+    CKD(S.get(&d_rank, nb));
+    CKD(S.get(&d_centers, (size_t)nb * dim));
+    CKD(upload(d_rank, dfs_rank.data(), nb, st));
+    CKD(upload(d_centers, t.centers.data(), (size_t)nb * dim, st));
+    CKD(sort_points_device(t, d_trg, nt, nullptr, d_nchild, d_child, d_centers, d_rank, nleaf, leaf_of_rank,
+                           d_itarg, t.t0, t.t1, st));
+  }
+  CKD(cudaStreamSynchronize(st));
+  if (dbg)
+    fprintf(stderr, "device tree (keys): refine %.4f (host %.4f, %d levels) lr %.4f ranks+sort_s %.4f sort_t %.4f\n",
+            tB - tA, th, lev, tC - tB, tD - tC, now_s() - tD);
+  return cudaGetLastError();
+}
+
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
                               bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg,
                               cudaStream_t st) {
+  if (ns > 0 && ts.nlmax >= 1 && ts.nlmax <= (dim == 2 ? 31 : 21) && !getenv("FGT_TREE_LEVELWISE"))
+    return build_tree_device_keys(t, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st);
   const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   const double tA = now_s();
   tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);

@@ -3970,7 +3970,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const FormTask* ft = D.form + G.beg;
         const int* cb = D.fcbeg + G.beg;
         // persistent CTAs: as many as fit on the SMs at once
-        const dim3 pg(std::min(ntk, D.sm_count * (ks * mt <= 4 && 2 * (sh + 1024) <= 228 * 1024 ? 2 : 1)), nd);
+        const dim3 pg(std::min(ntk, D.psm() * (ks * mt <= 4 && 2 * (sh + 1024) <= 228 * 1024 ? 2 : 1)), nd);
         if (ks <= 4 && mt <= 4 && sh <= 227 * 1024) {
           switch (4 * (ks - 1) + mt - 1) {
 #define H2PW_CASE(KS_, MT_)                                                                        \
@@ -4000,7 +4000,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       int Pn = D.form_pmax + 1;
       size_t sh = ((size_t)Pn * Pn * Pn + 3 * FORM_CH * Pn) * 8;
       if (Pn > 32 || sh > 227 * 1024) return cudaErrorNotSupported;
-      int grid = D.scratch_ctas;
+      int grid = std::min(D.scratch_ctas, 2 * D.psm());
       if (Pn <= 16) {
         CK(cudaFuncSetAttribute(k_form3d_hermite<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
         k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, ft, nft, D.scratch, D.scratch_per_cta, D.isq);
@@ -4116,11 +4116,11 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const int Pn = G.p + 1, nt = G.end - G.beg;
         const int nw = 4;
         const size_t sh = conv3_smem_bytes(Pn, P.npw, nw);
-        const dim3 cg(std::min(nt, D.conv3_ctas), nd);
+        const dim3 cg(std::min(nt, std::min(D.conv3_ctas, 4 * D.psm())), nd);
         const int n2 = P.npw / 2, ksm = (n2 + 3) / 4;
         const size_t shm = C3Dims(Pn, P.npw).total * 8;
         if (Pn <= 16 && ksm <= 8 && shm <= 227 * 1024) {
-          const dim3 pg(std::min(nt, D.sm_count * (2 * (shm + 1024) <= 228 * 1024 ? 2 : 1)), nd);
+          const dim3 pg(std::min(nt, D.psm() * (2 * (shm + 1024) <= 228 * 1024 ? 2 : 1)), nd);
           switch (ksm) {
 #define CONV3M_CASE(N)                                                                            \
   case N:                                                                                         \
@@ -4139,7 +4139,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         while (gs2 > 1 && C3Dims2(Pn, P.npw, gs2).total * 8 > 227 * 1024) gs2 >>= 1;
         const size_t shm2 = C3Dims2(Pn, P.npw, gs2).total * 8;
         if (Pn > 16 && Pn <= 32 && ksm <= 8 && shm2 <= 227 * 1024) {
-          const dim3 pg(std::min(nt, D.sm_count), nd);
+          const dim3 pg(std::min(nt, D.psm()), nd);
           switch (ksm) {
 #define CONV3M2_CASE(N)                                                                           \
   case N:                                                                                         \
@@ -4225,7 +4225,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     } else if (nbig > 0) {
       {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
-        k_eval3d_taylor<decltype(G)::value><<<D.scratch_ctas, 256, 0, st>>>(k, D.eval + D.eval3_nsplit, nbig,
+        k_eval3d_taylor<decltype(G)::value><<<std::min(D.scratch_ctas, 2 * D.psm()), 256, 0, st>>>(k, D.eval + D.eval3_nsplit, nbig,
                                                                            D.scratch, D.scratch_per_cta);
         return cudaSuccess;
       });

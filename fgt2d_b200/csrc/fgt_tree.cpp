@@ -282,6 +282,9 @@ struct Builder {
 
   // pts_tree_fix_lr, pts_tree2d4.f:693-996
   void fix_lr() {
+    auto T = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    double tt[8];
+    tt[0] = T();
     int nlev = t.nlevels;
     std::vector<int> iflag((size_t)t.nboxes * 2, 0);
     for (int l = nlev; l >= 2; l--) {
@@ -305,6 +308,8 @@ struct Builder {
         }
       }
     }
+    tt[1] = T();
+    const int nb0_ = t.nboxes;
     std::vector<int> tf(nlev + 1, 0), tl(nlev + 1, -1);
     int nold = t.nboxes;
     refined_ids.clear();
@@ -313,8 +318,12 @@ struct Builder {
       refine_flagged(iflag, t.lfirst[l], t.llast[l], l);
       tl[l + 1] = t.nboxes - 1;
     }
+    tt[2] = T();
+    const int nb1_ = t.nboxes;
     reorg(tf, tl, iflag);
+    tt[3] = T();
     colleagues_after_pass(nold);
+    tt[4] = T();
     for (int b = 0; b < t.nboxes; b++)
       if (iflag[b] != 3) iflag[b] = 0;
     std::fill(tf.begin(), tf.end(), 0);
@@ -344,8 +353,14 @@ struct Builder {
         t.ncoll[b] = n;
       }
     }
+    tt[5] = T();
     reorg(tf, tl, iflag);
+    tt[6] = T();
     colleagues_after_pass(nold);
+    tt[7] = T();
+    if (getenv("FGT_TREE_TIMING"))
+      fprintf(stderr, "fix_lr: flags %.4f refine1 %.4f reorg1 %.4f coll1 %.4f pass2 %.4f reorg2 %.4f coll2 %.4f nb %d nb0 %d nb1 %d\n",
+              tt[1] - tt[0], tt[2] - tt[1], tt[3] - tt[2], tt[4] - tt[3], tt[5] - tt[4], tt[6] - tt[5], tt[7] - tt[6], t.nboxes, nb0_, nb1_);
   }
 
   // updateflags, tree_routs4.f:217-326
@@ -481,8 +496,10 @@ int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, 
   t.boxsize[lev + 1] = t.boxsize[lev] / 2;
   B.reserve_boxes(t.nboxes + NCH * nref);
   t.lfirst[lev + 1] = t.nboxes;
+  const double bs = t.boxsize[lev + 1];
+#pragma omp parallel for schedule(static) if (nref > 8192)
   for (int box = a; box <= b; box++)
-    if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, t.boxsize[lev + 1]);
+    if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, bs);
   t.nboxes += NCH * nref;
   t.llast[lev + 1] = t.nboxes - 1;
   return nref;
@@ -494,10 +511,14 @@ void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap) {
   t.lfirst.resize(t.nlevels + 1);
   t.llast.resize(t.nlevels + 1);
   Builder B(t);
+  auto T = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  const double q0 = T();
   B.colleagues_all();
+  const double q1 = T();
   B.idmap.resize(t.nboxes);
   for (int k = 0; k < t.nboxes; k++) B.idmap[k] = k;
   if (t.nlevels >= 2) B.fix_lr();
+  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "finish: nb %d colleagues %.4f fix_lr %.4f\n", t.nboxes, q1 - q0, T() - q1);
   idmap.swap(B.idmap);
   const int NCH = t.nch, D = t.dim;
   t.level.resize(t.nboxes);
@@ -548,7 +569,9 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
   for (lev = 0; lev <= nlmax - 1; lev++) {
     const int a = t.lfirst[lev], b = t.llast[lev];
     const int thr = lev < levcut ? ndiv0 : ndiv;
+    const double tr0 = T();
     if (tree_refine_level(t, lev, thr, count, firstchild) == 0) break;
+    if (dbg) fprintf(stderr, "refine_level %d: %.5f nb %d\n", lev, T() - tr0, t.nboxes);
     count.resize(t.nboxes, 0);
     const int* fc = firstchild.data();
     const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0;

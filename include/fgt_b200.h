@@ -85,6 +85,11 @@ int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
  * FGT_TREE_HOST); both give the same tree.  No counterpart in the reference,
  * whose tree is built on the host (pts_tree_build, pts_tree2d4.f:363-590). */
 int fgt_ctx_set_tree(fgt_ctx* ctx, int where);
+/* how many SMs the persistent kernels of the context's plans (created after
+ * the call) size their grids for; 0 (the default) uses every SM.  The
+ * transform server uses half, so that requests arriving while a large one
+ * runs find SMs free.  No counterpart in the reference. */
+int fgt_ctx_set_sm_budget(fgt_ctx* ctx, int sms);
 /* the context used by the Fortran-named entry points (device 0, created on
  * first use) */
 fgt_ctx* fgt_default_ctx(void);

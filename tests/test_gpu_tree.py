@@ -2,7 +2,13 @@
 default) against the host build, which the CPU tests pin to the oracle's
 restatement of pts_tree_build / pts_tree_fix_lr / pts_tree_sort: every
 integer field, the centres and the box sizes must be identical, and
-transforms planned on either tree must give identical results."""
+transforms planned on either tree must give identical results.
+
+The device build has two forms: the exact-key form (one sort of each
+source's child digits, every level a binary search per box; the default for
+trees of at most 31 levels in 2D, 21 in 3D) and the level-by-level
+refinement over all points (deeper trees; FGT_TREE_LEVELWISE=1 selects it
+for any tree).  Both are checked."""
 import numpy as np
 import pytest
 
@@ -29,6 +35,11 @@ def _cases():
     pts = np.c_[g, g[::-1]]
     out.append(("2d_boundaries_dups", 2, 1e-5, 1e-6, pts, pts))
     out.append(("2d_single_point", 2, 1e-4, 1e-6, np.array([[0.3, 0.7]]), np.array([[0.1, 0.2]])))
+    # points exactly on box boundaries and centres at every level
+    grid = np.array(np.meshgrid(np.linspace(0, 1, 257), np.linspace(0, 1, 257))).reshape(2, -1).T.copy()
+    out.append(("2d_grid_exact", 2, 1e-6, 1e-6, grid, grid))
+    g3 = np.array(np.meshgrid(*[np.linspace(0, 1, 33)] * 3)).reshape(3, -1).T.copy()
+    out.append(("3d_grid_exact", 3, 1e-4, 1e-6, g3, g3[::7]))
     return out
 
 
@@ -40,9 +51,12 @@ def ctx(fgt):
     return fgt.Context(0, precision="fp64")
 
 
+@pytest.mark.parametrize("form", ["keys", "levelwise"])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-def test_device_tree_equals_host_tree(case, fgt, ctx):
+def test_device_tree_equals_host_tree(case, form, fgt, ctx, monkeypatch):
     name, dim, delta, eps, src, trg = case
+    if form == "levelwise":
+        monkeypatch.setenv("FGT_TREE_LEVELWISE", "1")
     trg_arg = src if trg is src else trg
     a = fgt.HostTree(dim, delta, eps, src, trg_arg)
     b = fgt.DeviceTree(ctx, dim, delta, eps, src, trg_arg)
