@@ -10,6 +10,11 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
+#include <cstdio>
+#include <cstdlib>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace fgtb {
 
@@ -83,6 +88,9 @@ static void build_tables(HostPlan& H) {
 
 // Flattens the tree into the stage task arrays.
 static void build_tasks(HostPlan& H) {
+  double tq[16];
+  int nq = 0;
+  tq[nq++] = now();
   Params& P = H.P;
   const Tree& t = H.tree;
   const Lists& L = H.lists;
@@ -139,6 +147,7 @@ static void build_tasks(HostPlan& H) {
       }
       H.merge_end[l] = (int)H.merge.size();
     }
+    tq[nq++] = now();
     // (b) mp -> loc at the cut level
     // in box order, the list's boxes with a multipole in list order; tasks
     // and neighbours counted per box, placed by prefix sums, filled in parallel
@@ -180,6 +189,7 @@ static void build_tasks(HostPlan& H) {
         H.m2l[tix[b - a]] = mt;
       }
     }
+    tq[nq++] = now();
     // (b) split, parents at levels nlevstart .. nlevels-1
     for (int l = nls; l <= P.nlevels - 1; l++) {
       H.split_beg[l] = (int)H.split.size();
@@ -220,6 +230,7 @@ static void build_tasks(HostPlan& H) {
       }
     }
   }
+  tq[nq++] = now();
   // flops of the routes taken: Hermite block (2 n P^d) and its separable
   // transform, or the direct exponential sum (8 n nexp); Taylor conversion
   // and evaluation (2 P^d per point) or direct plane-wave evaluation
@@ -272,26 +283,65 @@ static void build_tasks(HostPlan& H) {
     start(H.nloc); for (auto& s : H.split) see(s.dst); rb = c;
     H.shift_bytes[2] = per * (ra + rb);
   }
+  tq[nq++] = now();
+  tq[nq++] = now();
   // (d) near field, target-centric: for every leaf, the ifhung source boxes
   // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
   // box A -> source boxes S with A in list1(S), as CSR in the order of S
-  std::vector<int> ioff(nb + 1, 0), into, icur;
+  // (a transpose of the list1 CSR: the S range is cut into one chunk per
+  // thread, each thread counts and then places its entries through its own
+  // cursors, laid out chunk after chunk, so every segment lists S in
+  // increasing box id whatever the thread count)
+  std::vector<int> ioff(nb + 1, 0), into;
   int nlevend = npl < P.nlevels ? npl : P.nlevels;
-  for (int pass = 0; pass < 2; pass++) {
-    if (pass == 1) {
-      for (int b = 0; b < nb; b++) ioff[b + 1] += ioff[b];
-      into.assign(ioff[nb], 0);
-      icur.assign(ioff.begin(), ioff.end() - 1);
-    }
-    for (int l = 0; l <= nlevend; l++)
-      for (int s = t.lfirst[l]; s <= t.llast[l]; s++) {
-        if (!L.ifhung[s]) continue;
-        for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) {
-          if (pass == 0) ioff[L.l1[k] + 1]++;
-          else into[icur[L.l1[k]]++] = s;
+  const int s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;  // levels 0..nlevend are ids 0..s_hi
+  {
+    int nth = 1;
+#ifdef _OPENMP
+    if (s_hi > 8192) nth = std::max(1, std::min(omp_get_max_threads(), 64));
+#endif
+    std::vector<int> cur((size_t)nth * nb);
+    const int chunk = (s_hi + 1 + nth - 1) / nth;
+#pragma omp parallel num_threads(nth) if (nth > 1)
+    {
+#ifdef _OPENMP
+      const int th = omp_get_thread_num();
+#else
+      const int th = 0;
+#endif
+      int* const c = cur.data() + (size_t)th * nb;
+      std::fill(c, c + nb, 0);
+      const int s0 = th * chunk, s1 = std::min(s_hi + 1, s0 + chunk);
+      for (int s = s0; s < s1; s++)
+        if (L.ifhung[s])
+          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) c[L.l1[k]]++;
+#pragma omp barrier
+#pragma omp for schedule(static)
+      for (int a = 0; a < nb; a++) {
+        int n = 0;
+        for (int q = 0; q < nth; q++) n += cur[(size_t)q * nb + a];
+        ioff[a + 1] = n;
+      }
+#pragma omp single
+      {
+        for (int a = 0; a < nb; a++) ioff[a + 1] += ioff[a];
+        into.assign(ioff[nb], 0);
+      }
+#pragma omp for schedule(static)
+      for (int a = 0; a < nb; a++) {
+        int pos = ioff[a];
+        for (int q = 0; q < nth; q++) {
+          const int n = cur[(size_t)q * nb + a];
+          cur[(size_t)q * nb + a] = pos;
+          pos += n;
         }
       }
+      for (int s = s0; s < s1; s++)
+        if (L.ifhung[s])
+          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[c[L.l1[k]]++] = s;
+    }
   }
+  tq[nq++] = now();
   // per leaf: its source ranges (ancestors' segments, leaf first) once per
   // evaluated point set, and its tasks of <= CH points; counted per leaf,
   // placed by prefix sums in box order, filled in parallel
@@ -311,6 +361,7 @@ static void build_tasks(HostPlan& H) {
       cum_ns[b] = ns_ + (a >= 0 ? cum_ns[a] : 0);
     }
   }
+  tq[nq++] = now();
   std::vector<int> nr(nb, 0);
   std::vector<long long> roff(nb + 1, 0), toff(nb + 1, 0);
 #pragma omp parallel for schedule(static)
@@ -351,6 +402,12 @@ static void build_tasks(HostPlan& H) {
     }
   }
   H.direct_pairs = pairs;
+  tq[nq++] = now();
+  if (getenv("FGT_TREE_TIMING")) {
+    fprintf(stderr, "tasks (dir %zu ranges %zu, near-field csr %d):", H.dir.size(), H.dir_src.size(), ioff[nb]);
+    for (int i = 1; i < nq; i++) fprintf(stderr, " %.4f", tq[i] - tq[i - 1]);
+    fprintf(stderr, "\n");
+  }
   (void)D;
 }
 

@@ -99,9 +99,11 @@ struct Builder {
   double& C(int b, int d) { return t.centers[(size_t)b * D + d]; }
   int& CH(int b, int j) { return t.child[(size_t)b * NCH + j]; }
 
+  // Grows the box arrays to n boxes (the vectors grow their capacity
+  // geometrically; only the new boxes are initialised).
   void reserve_boxes(int n) {
     if ((int)t.level.size() >= n) return;
-    size_t m = std::max<size_t>(n, t.level.size() * 2);
+    const size_t m = n;
     t.level.resize(m, 0);
     t.parent.resize(m, -1);
     t.nchild.resize(m, 0);
@@ -287,24 +289,38 @@ struct Builder {
     tt[0] = T();
     int nlev = t.nlevels;
     std::vector<int> iflag((size_t)t.nboxes * 2, 0);
-    for (int l = nlev; l >= 2; l--) {
-      double dist = 1.05 * (t.boxsize[l - 1] + t.boxsize[l - 2]) / 2.0;
-      for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-        int dad = t.parent[b], gd = t.parent[dad];
+    int* const fl = iflag.data();
+    // Flag pass 1 only ever sets a flag from 0 to 1, so its outcome does not
+    // depend on the order of the boxes: all levels at once, in parallel
+    // (relaxed atomics: several boxes may flag the same colleague).
+    if (nlev >= 2) {
+      const int b0 = t.lfirst[2], b1 = t.llast[nlev];
+#pragma omp parallel for schedule(dynamic, 1024) if (b1 - b0 > 4096)
+      for (int b = b0; b <= b1; b++) {
+        const int l = t.level[b];
+        const double dist = 1.05 * (t.boxsize[l - 1] + t.boxsize[l - 2]) / 2.0;
+        const int dad = t.parent[b], gd = t.parent[dad];
         for (int i = 0; i < t.ncoll[gd]; i++) {
-          int jb = t.coll[(size_t)gd * NCO + i];
-          if (t.nchild[jb] == 0 && iflag[jb] == 0 && touching(jb, dad, dist)) iflag[jb] = 1;
+          const int jb = t.coll[(size_t)gd * NCO + i];
+          if (t.nchild[jb] == 0 && __atomic_load_n(fl + jb, __ATOMIC_RELAXED) == 0 && touching(jb, dad, dist))
+            __atomic_store_n(fl + jb, 1, __ATOMIC_RELAXED);
         }
       }
     }
+    // Pass 2 runs from the finest level up; a level reads its own flags and
+    // only sets flags of the level above from 0 to 2, so each level is one
+    // parallel step.
     for (int l = nlev; l >= 1; l--) {
-      double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+      const double dist = 1.05 * (t.boxsize[l] + t.boxsize[l - 1]) / 2.0;
+#pragma omp parallel for schedule(dynamic, 1024) if (t.llast[l] - t.lfirst[l] > 4096)
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-        if (iflag[b] != 1 && iflag[b] != 2) continue;
-        int dad = t.parent[b];
+        const int f = __atomic_load_n(fl + b, __ATOMIC_RELAXED);
+        if (f != 1 && f != 2) continue;
+        const int dad = t.parent[b];
         for (int i = 0; i < t.ncoll[dad]; i++) {
-          int jb = t.coll[(size_t)dad * NCO + i];
-          if (t.nchild[jb] == 0 && iflag[jb] == 0 && touching(jb, b, dist)) iflag[jb] = 2;
+          const int jb = t.coll[(size_t)dad * NCO + i];
+          if (t.nchild[jb] == 0 && __atomic_load_n(fl + jb, __ATOMIC_RELAXED) == 0 && touching(jb, b, dist))
+            __atomic_store_n(fl + jb, 2, __ATOMIC_RELAXED);
         }
       }
     }
@@ -340,6 +356,7 @@ struct Builder {
       t.ncoll.resize(t.nboxes, 0);
       t.coll.resize((size_t)t.nboxes * NCO, -1);
       double lim = F105 * t.boxsize[l + 1];
+#pragma omp parallel for schedule(static) if (tl[l + 1] - tf[l + 1] > 4096)
       for (int b = tf[l + 1]; b <= tl[l + 1]; b++) {
         int dad = t.parent[b];
         int n = 0;
@@ -366,6 +383,8 @@ struct Builder {
   // updateflags, tree_routs4.f:217-326
   void update_flags(int lev, int a, int b, std::vector<int>& iflag) {
     double dist = 1.05 * (t.boxsize[lev] + t.boxsize[lev + 1]) / 2.0;
+    // each box decides its own flag from its colleagues' children
+#pragma omp parallel for schedule(dynamic, 1024) if (b - a > 4096)
     for (int box = a; box <= b; box++) {
       if (iflag[box] != 3) continue;
       iflag[box] = 0;
@@ -497,7 +516,7 @@ int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, 
   B.reserve_boxes(t.nboxes + NCH * nref);
   t.lfirst[lev + 1] = t.nboxes;
   const double bs = t.boxsize[lev + 1];
-#pragma omp parallel for schedule(static) if (nref > 8192)
+#pragma omp parallel for schedule(static) if (nref > 2048)
   for (int box = a; box <= b; box++)
     if (firstchild[box - a] >= 0) B.make_children(box, firstchild[box - a], lev + 1, bs);
   t.nboxes += NCH * nref;
