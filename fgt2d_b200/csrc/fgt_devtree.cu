@@ -263,6 +263,145 @@ __global__ void k_root_range(int* r0, int* r1, int n) {
   r1[0] = n;
 }
 
+// ---- refinement on the device (exact-key form) ----
+// lev[2 l], lev[2 l + 1]: first and last box of level l (last < first: empty);
+// lev[2 nslot]: the box count.  Box arrays hold the tree as the host builds
+// it (tree_refine_level): level by level, the children of a refined box
+// consecutive, refined boxes in box order.
+__global__ void k_ref_init(int* lev, int nslot, int* r0, int* r1, int* par, int* nchild, int* child, int* level,
+                           double* cen, int nch, int dim, double cx, double cy, double cz, int n, int* ncoll,
+                           int* coll, int nco) {
+  ncoll[0] = 1;
+  coll[0] = 0;
+  for (int q = 1; q < nco; q++) coll[q] = -1;
+  for (int i = 0; i < nslot; i++) {
+    lev[2 * i] = 0;
+    lev[2 * i + 1] = -1;
+  }
+  lev[1] = 0;
+  lev[2 * nslot] = 1;
+  r0[0] = 0;
+  r1[0] = n;
+  par[0] = -1;
+  nchild[0] = 0;
+  level[0] = 0;
+  for (int j = 0; j < nch; j++) child[j] = -1;
+  const double c[3] = {cx, cy, cz};
+  for (int d = 0; d < dim; d++) cen[d] = c[d];
+}
+// flag[i]: box first + i of level l holds more than thr sources
+__global__ void k_ref_flag(const int* __restrict__ lev, int l, const int* __restrict__ r0,
+                           const int* __restrict__ r1, int thr, int* __restrict__ flag) {
+  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    flag[i] = r1[first + i] - r0[first + i] > thr;
+}
+// One block of 1024 threads: exclusive prefix of the flags (the refined
+// boxes' ranks), and the id range of level l + 1.
+__global__ void __launch_bounds__(1024) k_ref_scan(int* __restrict__ lev, int l, int nslot,
+                                                   const int* __restrict__ flag, int* __restrict__ pos, int nch) {
+  __shared__ int part[1024];
+  const int first = lev[2 * l], n = max(0, lev[2 * l + 1] - first + 1);
+  const int per = (n + 1023) / 1024, i0 = min(n, (int)threadIdx.x * per), i1 = min(n, i0 + per);
+  int sum = 0;
+  for (int i = i0; i < i1; i++) sum += flag[i];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int i = i0; i < i1; i++) {
+    pos[i] = run;
+    run += flag[i];
+  }
+  if (threadIdx.x == 1023) {
+    const int nref = part[1023], nb = lev[2 * nslot];
+    if (nref > 0) {
+      lev[2 * (l + 1)] = nb;
+      lev[2 * (l + 1) + 1] = nb + nch * nref - 1;
+      lev[2 * nslot] = nb + nch * nref;
+    }
+  }
+}
+// The children of the refined boxes of level l: structure, centres (the
+// parent's plus or minus h, a quarter of the parent's size, in each
+// dimension) and key ranges; one thread per (box, child).
+__global__ void k_ref_children(const int* __restrict__ lev, int l, const int* __restrict__ flag,
+                               const int* __restrict__ pos, const unsigned long long* __restrict__ key, int shift,
+                               int nch, int dim, double h, int* __restrict__ r0, int* __restrict__ r1,
+                               int* __restrict__ par, int* __restrict__ nchild, int* __restrict__ child,
+                               int* __restrict__ level, double* __restrict__ cen) {
+  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1, c0 = lev[2 * (l + 1)];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)n * nch;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int bi = (int)(i / nch), j = (int)(i - (long long)bi * nch);
+    if (!flag[bi]) continue;
+    const int b = first + bi, c = c0 + nch * pos[bi] + j;
+    if (j == 0) nchild[b] = nch;
+    child[(size_t)b * nch + j] = c;
+    par[c] = b;
+    level[c] = l + 1;
+    nchild[c] = 0;
+    for (int q = 0; q < nch; q++) child[(size_t)c * nch + q] = -1;
+    for (int d = 0; d < dim; d++) cen[(size_t)c * dim + d] = cen[(size_t)b * dim + d] + (((j >> d) & 1) ? h : -h);
+    const int lo = r0[b], hi = r1[b];
+    const int s = digit_lower_bound(key, lo, hi, shift, nch, j);
+    const int e = j == nch - 1 ? hi : digit_lower_bound(key, s, hi, shift, nch, j + 1);
+    r0[c] = s;
+    r1[c] = e;
+  }
+}
+
+// Colleagues of the boxes of level l (computecoll, tree_routs4.f:100-211, as
+// colleagues_box in fgt_tree.cpp): the children of the parent's colleagues
+// whose centres lie within lim of the box's in every dimension, in the
+// parent's colleague order then child order; unused slots -1.
+__global__ void k_ref_colleagues(const int* __restrict__ lev, int l, double lim, int nch, int nco, int dim,
+                                 const int* __restrict__ par, const int* __restrict__ nchild,
+                                 const int* __restrict__ child, const double* __restrict__ cen,
+                                 int* __restrict__ ncoll, int* __restrict__ coll) {
+  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = first + i, dad = par[b];
+    double cb[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) cb[d] = cen[(size_t)b * dim + d];
+    int cnt = 0;
+    for (int q = 0; q < ncoll[dad]; q++) {
+      const int jb = coll[(size_t)dad * nco + q];
+      const int* ch = child + (size_t)jb * nch;
+      if (ch[0] < 0 && nchild[jb] == 0) continue;
+      bool all = true;
+      for (int j = 0; j < nch; j++) all = all && ch[j] >= 0;
+      if (all) {
+        unsigned pass0 = 0u, pass1 = 0u;
+        for (int d = 0; d < dim; d++) {
+          if (fabs(cen[(size_t)ch[0] * dim + d] - cb[d]) <= lim) pass0 |= 1u << d;
+          if (fabs(cen[(size_t)ch[1 << d] * dim + d] - cb[d]) <= lim) pass1 |= 1u << d;
+        }
+        for (int j = 0; j < nch; j++) {
+          const unsigned ok = (pass1 & (unsigned)j) | (pass0 & ~(unsigned)j);
+          if ((ok & ((1u << dim) - 1)) == (1u << dim) - 1) coll[(size_t)b * nco + cnt++] = ch[j];
+        }
+        continue;
+      }
+      for (int j = 0; j < nch; j++) {
+        const int kb = ch[j];
+        if (kb < 0) continue;
+        bool ok = true;
+        for (int d = 0; d < dim; d++)
+          if (!(fabs(cen[(size_t)kb * dim + d] - cb[d]) <= lim)) ok = false;
+        if (ok) coll[(size_t)b * nco + cnt++] = kb;
+      }
+    }
+    for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
+    ncoll[b] = cnt;
+  }
+}
+
 // Device scratch of one build, stream-ordered on the build's stream (no
 // device-wide synchronisation) and freed at the end of the build.
 struct Scratch {
@@ -353,6 +492,24 @@ cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_
   return device_bbox(d_src, ns, d_trg, nt, dim, mn, mx, st);
 }
 
+// Upper bound of the box count of the refinement (per level in *per_level):
+// level l + 1 holds nch children of each box of level l that holds more than
+// thr sources, and at most ns / (thr + 1) boxes can.
+long long key_tree_capacity(const TreeSetup& ts, int dim, int ns, std::vector<long long>* per_level) {
+  const int nch = 1 << dim;
+  std::vector<long long> b(ts.nlmax + 2, 0);
+  b[0] = 1;
+  long long tot = 1;
+  for (int l = 0; l < ts.nlmax && tot < (1LL << 40); l++) {
+    const int thr = l < ts.levcut ? ts.ndiv0 : ts.ndiv;
+    b[l + 1] = nch * std::min<long long>(b[l], (long long)ns / (thr + 1));
+    tot += b[l + 1];
+  }
+  if (per_level) *per_level = b;
+  return tot;
+}
+constexpr long long kKeyTreeMaxBoxes = 1LL << 24;
+
 // The tree from the exact child digits of the sources (k_exact_key), for
 // trees whose depth fits a 64-bit key (31 levels in 2D, 21 in 3D): one sort
 // of the keys, after which every refinement level is a binary search per
@@ -382,58 +539,87 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(S.get(&dtmp, tmp));
     CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, key, skey, wid0, wid, ns, 0, dim * L, st));
   }
-  // per-box ranges in key order, grown with the box count
-  int *r0 = nullptr, *r1 = nullptr;
-  size_t cap = 0;
-  auto grow = [&](size_t need) -> cudaError_t {
-    if (need <= cap) return cudaSuccess;
-    const size_t nc = std::max<size_t>({need, 2 * cap, 4096});
-    int *n0 = nullptr, *n1 = nullptr;
-    CKD(S.get(&n0, nc));
-    CKD(S.get(&n1, nc));
-    if (cap) {
-      CKD(cudaMemcpyAsync(n0, r0, cap * 4, cudaMemcpyDeviceToDevice, st));
-      CKD(cudaMemcpyAsync(n1, r1, cap * 4, cudaMemcpyDeviceToDevice, st));
+  // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563: every
+  // level on the device (flags, the refined boxes' ranks, the children and
+  // their key ranges), no host round trip; the box arrays come back once
+  const int nslot = L + 1;
+  std::vector<long long> bound;
+  const long long cap = key_tree_capacity(ts, dim, ns, &bound);
+  long long maxlev = 1;
+  for (long long v : bound) maxlev = std::max(maxlev, v);
+  int *r0 = nullptr, *r1 = nullptr, *dpar = nullptr, *dnch = nullptr, *dchild = nullptr, *dlevel = nullptr;
+  int *dflag = nullptr, *dpos = nullptr, *dlev = nullptr;
+  double* dcen = nullptr;
+  CKD(S.get(&r0, cap));
+  CKD(S.get(&r1, cap));
+  CKD(S.get(&dpar, cap));
+  CKD(S.get(&dnch, cap));
+  CKD(S.get(&dchild, (size_t)cap * nch));
+  CKD(S.get(&dlevel, cap));
+  CKD(S.get(&dcen, (size_t)cap * dim));
+  CKD(S.get(&dflag, maxlev));
+  CKD(S.get(&dpos, maxlev));
+  CKD(S.get(&dlev, 2 * nslot + 1));
+  const int nco = t.nco;
+  int *dncoll = nullptr, *dcoll = nullptr;
+  CKD(S.get(&dncoll, cap));
+  CKD(S.get(&dcoll, (size_t)cap * nco));
+  k_ref_init<<<1, 1, 0, st>>>(dlev, nslot, r0, r1, dpar, dnch, dchild, dlevel, dcen, nch, dim, ts.cen0[0],
+                              ts.cen0[1], ts.cen0[2], ns, dncoll, dcoll, nco);
+  {
+    double bs = ts.bs0;
+    for (int l = 0; l <= ts.nlmax - 1; l++) {
+      const int thr = l < ts.levcut ? ts.ndiv0 : ts.ndiv;
+      const int g1 = (int)std::max<long long>(1, std::min<long long>((bound[l] + 255) / 256, 1184));
+      const int g2 = (int)std::max<long long>(1, std::min<long long>((bound[l] * nch + 255) / 256, 1184));
+      k_ref_flag<<<g1, 256, 0, st>>>(dlev, l, r0, r1, thr, dflag);
+      k_ref_scan<<<1, 1024, 0, st>>>(dlev, l, nslot, dflag, dpos, nch);
+      bs = bs / 2;  // size of level l + 1, as tree_refine_level
+      k_ref_children<<<g2, 256, 0, st>>>(dlev, l, dflag, dpos, skey, dim * (L - 1 - l), nch, dim, bs / 2, r0, r1,
+                                         dpar, dnch, dchild, dlevel, dcen);
     }
-    r0 = n0;
-    r1 = n1;
-    cap = nc;
-    return cudaSuccess;
-  };
-  CKD(grow(1));
-  k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
-  // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563
-  std::vector<int> count(1, ns), fc;
-  int *d_fc = nullptr, *d_cnt = nullptr;
-  size_t cap_lev = 0, cap_new = 0;
-  int lev;
-  double th = 0;
-  for (lev = 0; lev <= ts.nlmax - 1; lev++) {
-    const int a = t.lfirst[lev], b = t.llast[lev];
-    const int thr = lev < ts.levcut ? ts.ndiv0 : ts.ndiv;
-    const double th0 = now_s();
-    if (tree_refine_level(t, lev, thr, count, fc) == 0) break;
-    th += now_s() - th0;
-    const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0, nlev = b - a + 1;
-    CKD(grow(t.nboxes));
-    if ((size_t)nlev > cap_lev) {
-      cap_lev = (size_t)nlev * 2;
-      CKD(S.get(&d_fc, cap_lev));
+  }
+  // colleagues of every level (the level restriction starts from them)
+  {
+    double bs = ts.bs0;
+    for (int l = 1; l <= ts.nlmax; l++) {
+      bs = bs / 2;
+      const int g = (int)std::max<long long>(1, std::min<long long>((bound[l] + 255) / 256, 1184));
+      k_ref_colleagues<<<g, 256, 0, st>>>(dlev, l, (double)1.05f * bs, nch, nco, dim, dpar, dnch, dchild, dcen,
+                                          dncoll, dcoll);
     }
-    if ((size_t)nnew > cap_new) {
-      cap_new = (size_t)nnew * 2;
-      CKD(S.get(&d_cnt, cap_new));
-    }
-    CKD(upload(d_fc, fc.data(), nlev, st));
-    k_child_ranges<<<(nlev * nch + 255) / 256, 256, 0, st>>>(skey, dim * (L - 1 - lev), nch, a, nlev, d_fc,
-                                                              nullptr, r0, r1, c0, d_cnt);
-    count.resize(t.nboxes, 0);
-    CKD(cudaMemcpyAsync(count.data() + c0, d_cnt, sizeof(int) * nnew, cudaMemcpyDeviceToHost, st));
-    CKD(cudaStreamSynchronize(st));
+  }
+  CKD(cudaGetLastError());
+  std::vector<int> hlev(2 * nslot + 1);
+  CKD(cudaMemcpyAsync(hlev.data(), dlev, sizeof(int) * hlev.size(), cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  const int nbr = hlev[2 * nslot];
+  if (nbr > cap) return cudaErrorLaunchFailure;
+  int lev = 0;
+  while (lev + 1 <= ts.nlmax && hlev[2 * (lev + 1) + 1] >= hlev[2 * (lev + 1)]) lev++;
+  t.nboxes = nbr;
+  t.level.resize(nbr);
+  t.parent.resize(nbr);
+  t.nchild.resize(nbr);
+  t.child.resize((size_t)nbr * nch);
+  t.centers.resize((size_t)nbr * dim);
+  CKD(cudaMemcpyAsync(t.level.data(), dlevel, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.parent.data(), dpar, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.nchild.data(), dnch, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.child.data(), dchild, sizeof(int) * (size_t)nbr * nch, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.centers.data(), dcen, sizeof(double) * (size_t)nbr * dim, cudaMemcpyDeviceToHost, st));
+  t.ncoll.resize(nbr);
+  t.coll.resize((size_t)nbr * nco);
+  CKD(cudaMemcpyAsync(t.ncoll.data(), dncoll, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(t.coll.data(), dcoll, sizeof(int) * (size_t)nbr * nco, cudaMemcpyDeviceToHost, st));
+  for (int l = 0; l <= lev; l++) {
+    t.lfirst[l] = hlev[2 * l];
+    t.llast[l] = hlev[2 * l + 1];
+    if (l > 0) t.boxsize[l] = t.boxsize[l - 1] / 2;
   }
   const double tB = now_s();
   std::vector<int> idmap;
-  tree_finish(t, lev, idmap);
+  tree_finish(t, lev, idmap, true);
   const double tC = now_s();
   std::vector<int> dfs_rank, leaf_of_rank;
   tree_leaf_ranks(t, dfs_rank, leaf_of_rank);
@@ -447,7 +633,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(upload(d_lor, leaf_of_rank.data(), nleaf, st));
   // ranges of the finished tree (the level restriction added boxes and
   // renumbered), level by level from the root
-  CKD(grow(nb));
+  CKD(S.get(&r0, nb));
+  CKD(S.get(&r1, nb));
   k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
   for (int l = 0; l < t.nlevels; l++) {
     const int a = t.lfirst[l], n = t.llast[l] - a + 1;
@@ -494,15 +681,16 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   }
   CKD(cudaStreamSynchronize(st));
   if (dbg)
-    fprintf(stderr, "device tree (keys): refine %.4f (host %.4f, %d levels) lr %.4f ranks+sort_s %.4f sort_t %.4f\n",
-            tB - tA, th, lev, tC - tB, tD - tC, now_s() - tD);
+    fprintf(stderr, "device tree (keys): refine %.4f (%d levels, %d boxes) lr %.4f ranks+sort_s %.4f sort_t %.4f\n",
+            tB - tA, lev, nbr, tC - tB, tD - tC, now_s() - tD);
   return cudaGetLastError();
 }
 
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
                               bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg,
                               cudaStream_t st) {
-  if (ns > 0 && ts.nlmax >= 1 && ts.nlmax <= (dim == 2 ? 31 : 21) && !getenv("FGT_TREE_LEVELWISE"))
+  if (ns > 0 && ts.nlmax >= 1 && ts.nlmax <= (dim == 2 ? 31 : 21) && !getenv("FGT_TREE_LEVELWISE") &&
+      key_tree_capacity(ts, dim, ns, nullptr) <= kKeyTreeMaxBoxes)
     return build_tree_device_keys(t, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st);
   const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   const double tA = now_s();

@@ -524,7 +524,7 @@ int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, 
   return nref;
 }
 
-void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap) {
+void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap, bool have_colleagues) {
   t.nlevels = nlevels;
   t.boxsize.resize(t.nlevels + 1);
   t.lfirst.resize(t.nlevels + 1);
@@ -532,7 +532,7 @@ void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap) {
   Builder B(t);
   auto T = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
   const double q0 = T();
-  B.colleagues_all();
+  if (!have_colleagues) B.colleagues_all();
   const double q1 = T();
   B.idmap.resize(t.nboxes);
   for (int k = 0; k < t.nboxes; k++) B.idmap[k] = k;

@@ -58,14 +58,15 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
 //     (count[box], every box so far) exceeds thr, appending their children;
 //     firstchild[box - lfirst[lev]] receives the first child id or -1.
 //     Returns the number of refined boxes (0 ends the refinement).
-//   tree_finish: closes the refinement at nlevels, computes colleagues and
+//   tree_finish: closes the refinement at nlevels, computes colleagues (unless
+//     have_colleagues: t.ncoll / t.coll already hold them) and
 //     applies the level restriction (pts_tree_fix_lr + reorg); idmap maps a
 //     box id of the refinement to its final id.
 //   tree_leaf_ranks: depth-first rank of the leaves (the pts_tree_sort order).
 //   tree_ranges: per-box point ranges [r0, r1) from the per-leaf counts.
 void tree_init(Tree& t, int dim, double bs0, const double* cen0, int nlmax);
 int tree_refine_level(Tree& t, int lev, int thr, const std::vector<int>& count, std::vector<int>& firstchild);
-void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap);
+void tree_finish(Tree& t, int nlevels, std::vector<int>& idmap, bool have_colleagues = false);
 void tree_leaf_ranks(const Tree& t, std::vector<int>& dfs_rank, std::vector<int>& leaf_of_rank);
 void tree_ranges(const Tree& t, const std::vector<int>& leafcount, const std::vector<int>& leaf_of_rank,
                  std::vector<int>& r0, std::vector<int>& r1);
