@@ -33,6 +33,9 @@ struct fgt_ctx {
   int tree = FGT_TREE_DEVICE;
   int nthreads = 0;
   int sm_budget = 0;  // SMs the persistent kernels of this context's plans size their grids for (0: all)
+  // uploads of a one-shot call's source strengths: they follow the points on
+  // the copy engine while the tree build runs on `stream`
+  cudaStream_t up_stream = nullptr;
   std::mutex mu;
 };
 
@@ -63,6 +66,7 @@ struct fgt_plan {
   const double* pre_q = nullptr;
   const double* pre_rn = nullptr;
   const double* pre_ds = nullptr;
+  cudaEvent_t pre_done = nullptr;  // the strengths' uploads on the context's up_stream
   // recorded after every execute on the stream it used: the frees of
   // fgt_plan_destroy (stream-ordered on the context's stream) wait for it
   cudaEvent_t done = nullptr;
@@ -158,9 +162,20 @@ int alloc_io(fgt_plan* p, int dim, int nd, int ns, int nt, int ifpgh, int ifpght
   cudaStream_t st = p->ctx->stream;
   if (ns > 0) CKS(cudaMemcpyAsync(p->d_src, src_host, n_src * 8, cudaMemcpyHostToDevice, st));
   if (nt > 0 && upload_trg) CKS(cudaMemcpyAsync(p->d_trg, trg_host, n_trg * 8, cudaMemcpyHostToDevice, st));
-  if (ns > 0 && p->pre_q) CKS(cudaMemcpyAsync(p->d_chg, p->pre_q, n_chg * 8, cudaMemcpyHostToDevice, st));
-  if (ns > 0 && p->pre_rn && p->d_rn) CKS(cudaMemcpyAsync(p->d_rn, p->pre_rn, n_rn * 8, cudaMemcpyHostToDevice, st));
-  if (ns > 0 && p->pre_ds && p->d_ds) CKS(cudaMemcpyAsync(p->d_ds, p->pre_ds, n_ds * 8, cudaMemcpyHostToDevice, st));
+  // the strengths go up on the side stream once the points are up, so the
+  // tree build (which needs only the points) does not wait for them; the
+  // execute waits for pre_done
+  if (ns > 0 && (p->pre_q || (p->pre_rn && p->d_rn) || (p->pre_ds && p->d_ds))) {
+    if (!p->ctx->up_stream) CKS(cudaStreamCreateWithFlags(&p->ctx->up_stream, cudaStreamNonBlocking));
+    if (!p->pre_done) CKS(cudaEventCreateWithFlags(&p->pre_done, cudaEventDisableTiming));
+    cudaStream_t us = p->ctx->up_stream;
+    CKS(cudaEventRecord(p->pre_done, st));
+    CKS(cudaStreamWaitEvent(us, p->pre_done, 0));
+    if (p->pre_q) CKS(cudaMemcpyAsync(p->d_chg, p->pre_q, n_chg * 8, cudaMemcpyHostToDevice, us));
+    if (p->pre_rn && p->d_rn) CKS(cudaMemcpyAsync(p->d_rn, p->pre_rn, n_rn * 8, cudaMemcpyHostToDevice, us));
+    if (p->pre_ds && p->d_ds) CKS(cudaMemcpyAsync(p->d_ds, p->pre_ds, n_ds * 8, cudaMemcpyHostToDevice, us));
+    CKS(cudaEventRecord(p->pre_done, us));
+  }
   return FGT_OK;
 }
 
@@ -206,9 +221,11 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   const bool same = targ == sources && nt == ns;
   int st = alloc_io(p, dim, nd, ns, nt, ifpgh, ifpghtarg, 0, sources, targ, !same, ifdipole);
   if (st != FGT_OK) return st;
+  const double tq0 = now_s();
   st = check_finite_device(p, p->d_src, (size_t)ns * dim);
   if (st == FGT_OK && !same) st = check_finite_device(p, p->d_trg, (size_t)nt * dim);
   if (st != FGT_OK) return st;
+  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "plan: points up and checked %.4f\n", now_s() - tq0);
   cudaStream_t s = p->ctx->stream;
   const double* d_trg = same ? p->d_src : p->d_trg;
   int* perms = nullptr;
@@ -232,6 +249,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     std::vector<double> hs((size_t)ns * dim), ht(same ? 0 : (size_t)nt * dim);
     CKS(cudaMemcpyAsync(hs.data(), p->d_src, hs.size() * 8, cudaMemcpyDeviceToHost, s));
     if (!same && nt > 0) CKS(cudaMemcpyAsync(ht.data(), p->d_trg, ht.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (p->pre_done) CKS(cudaStreamWaitEvent(s, p->pre_done, 0));  // the strengths' uploads into d_io
     CKS(cudaStreamSynchronize(s));
     cudaFreeAsync(p->d_io, s);
     p->d_io = nullptr;
@@ -316,6 +334,7 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const doub
   cudaStream_t st = p->ctx->stream;
   CKS(cudaSetDevice(p->ctx->device));
   const size_t ns = P.ns, nt = P.nt, nd = P.nd, nh = P.dim == 2 ? 3 : 6;
+  if (p->pre_done) CKS(cudaStreamWaitEvent(st, p->pre_done, 0));  // strengths uploaded with the points
   Inputs in;
   if (P.ifcharge) {
     if (!charge && ns) return FGT_ERR_BADARG;
@@ -355,6 +374,7 @@ int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const doub
   if (P.ifpghtarg >= 2) CKS(back(host.gradtarg, d.gradtarg, nt * nd * P.dim));
   if (P.ifpghtarg >= 3) CKS(back(host.hesstarg, d.hesstarg, nt * nd * nh));
   CKS(cudaStreamSynchronize(st));
+  if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "exec_host: outputs down %.4f\n", now_s() - tx2);
   return FGT_OK;
 }
 
@@ -395,15 +415,20 @@ int transform_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, int 
     return FGT_OK;
   }
   fgt_plan* plan = nullptr;
+  const double ta = now_s();
   st = plan_create_impl(ctx, dim, nd, delta, eps, ns, sources, nt, targ, ifcharge, ifdipole, ifpgh,
                         ifpghtarg, &plan, ifcharge ? charge : nullptr, ifdipole ? rnormal : nullptr,
                         ifdipole ? dipstr : nullptr);
+  const double tb = now_s();
   if (st == FGT_OK) {
     Outputs h;
     h.pot = pot; h.grad = grad; h.hess = hess;
     h.pottarg = pottarg; h.gradtarg = gradtarg; h.hesstarg = hesstarg;
     st = exec_host(plan, charge, h, rnormal, dipstr);
+    const double tc = now_s();
     fgt_plan_destroy(plan);
+    if (getenv("FGT_TREE_TIMING"))
+      fprintf(stderr, "transform: plan %.4f execute+outputs %.4f destroy %.4f\n", tb - ta, tc - tb, now_s() - tc);
   }
   if (st != FGT_OK) zero();
   return st;
@@ -474,6 +499,7 @@ int fgt_ctx_destroy(fgt_ctx* c) {
   if (c == g_default) return FGT_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->up_stream) cudaStreamDestroy(c->up_stream);
   delete c;
   return FGT_OK;
 }
@@ -614,6 +640,10 @@ int fgt_plan_destroy(fgt_plan* p) {
     // the stream-ordered frees below follow the last execute, on any stream
     cudaStreamWaitEvent(p->ctx->stream, p->done, 0);
     cudaEventDestroy(p->done);
+  }
+  if (p->pre_done) {  // and the strengths' uploads
+    cudaStreamWaitEvent(p->ctx->stream, p->pre_done, 0);
+    cudaEventDestroy(p->pre_done);
   }
   if (p->have_device) {
     p->D.stream = p->ctx->stream;

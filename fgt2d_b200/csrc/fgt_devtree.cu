@@ -24,6 +24,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <initializer_list>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -422,6 +424,87 @@ struct Scratch {
   }
 };
 
+// Pinned staging of the build's transfers of box arrays: copies from or to
+// pageable vectors go through the driver's bounce buffers at a fraction of
+// the link rate.  The stage grows and keeps its old buffers until the thread
+// exits (freeing pinned memory would wait for the whole device).
+struct PinnedStage {
+  char* p = nullptr;
+  size_t cap = 0;
+  std::vector<char*> old;
+  ~PinnedStage() {
+    if (p) cudaFreeHost(p);
+    for (char* q : old) cudaFreeHost(q);
+  }
+  char* get(size_t n) {
+    if (n > cap) {
+      if (p) old.push_back(p);
+      p = nullptr;
+      const size_t want = std::max({n + n / 4, 2 * cap, (size_t)4 << 20});
+      cap = 0;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&p), want, cudaHostAllocPortable) != cudaSuccess) {
+        (void)cudaGetLastError();
+        p = nullptr;
+        return nullptr;
+      }
+      cap = want;
+    }
+    return p;
+  }
+};
+thread_local PinnedStage g_stage;
+
+// One batch of transfers through the stage (sized up front); finish()
+// synchronises the stream and copies the downloads out, after which the
+// stage may be reused.  Without pinned memory the copies go direct.
+struct StagedBatch {
+  cudaStream_t st;
+  char* base = nullptr;
+  size_t used = 0, cap = 0;
+  struct Out {
+    void* dst;
+    size_t off, bytes;
+  };
+  std::vector<Out> outs;
+  StagedBatch(cudaStream_t s, size_t total) : st(s), cap(total) { base = g_stage.get(total); }
+  size_t take(size_t b) {
+    const size_t off = (used + 255) & ~size_t(255);
+    used = off + b;
+    return off;
+  }
+  template <typename T>
+  cudaError_t down(T* dst, const T* dev, size_t n) {
+    const size_t b = n * sizeof(T);
+    if (b == 0) return cudaSuccess;
+    if (!base || ((used + 255) & ~size_t(255)) + b > cap) return cudaMemcpyAsync(dst, dev, b, cudaMemcpyDeviceToHost, st);
+    const size_t off = take(b);
+    outs.push_back({dst, off, b});
+    return cudaMemcpyAsync(base + off, dev, b, cudaMemcpyDeviceToHost, st);
+  }
+  template <typename T>
+  cudaError_t up(T* dev, const T* src, size_t n) {
+    const size_t b = n * sizeof(T);
+    if (b == 0) return cudaSuccess;
+    if (!base || ((used + 255) & ~size_t(255)) + b > cap) return cudaMemcpyAsync(dev, src, b, cudaMemcpyHostToDevice, st);
+    const size_t off = take(b);
+    memcpy(base + off, src, b);
+    return cudaMemcpyAsync(dev, base + off, b, cudaMemcpyHostToDevice, st);
+  }
+  cudaError_t finish() {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+#pragma omp parallel for schedule(dynamic, 1) if (used > (2u << 20))
+    for (long long i = 0; i < (long long)outs.size(); i++) memcpy(outs[i].dst, base + outs[i].off, outs[i].bytes);
+    outs.clear();
+    return cudaSuccess;
+  }
+};
+static size_t staged_bytes(std::initializer_list<size_t> b) {
+  size_t t = 0;
+  for (size_t x : b) t += (x + 255) & ~size_t(255);
+  return t;
+}
+
 template <typename T>
 cudaError_t upload(T* dst, const T* src, size_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
@@ -603,15 +686,20 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   t.nchild.resize(nbr);
   t.child.resize((size_t)nbr * nch);
   t.centers.resize((size_t)nbr * dim);
-  CKD(cudaMemcpyAsync(t.level.data(), dlevel, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.parent.data(), dpar, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.nchild.data(), dnch, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.child.data(), dchild, sizeof(int) * (size_t)nbr * nch, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.centers.data(), dcen, sizeof(double) * (size_t)nbr * dim, cudaMemcpyDeviceToHost, st));
   t.ncoll.resize(nbr);
   t.coll.resize((size_t)nbr * nco);
-  CKD(cudaMemcpyAsync(t.ncoll.data(), dncoll, sizeof(int) * nbr, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.coll.data(), dcoll, sizeof(int) * (size_t)nbr * nco, cudaMemcpyDeviceToHost, st));
+  {
+    const size_t i4 = sizeof(int) * (size_t)nbr;
+    StagedBatch X(st, staged_bytes({i4, i4, i4, i4 * nch, sizeof(double) * (size_t)nbr * dim, i4, i4 * nco}));
+    CKD(X.down(t.level.data(), dlevel, nbr));
+    CKD(X.down(t.parent.data(), dpar, nbr));
+    CKD(X.down(t.nchild.data(), dnch, nbr));
+    CKD(X.down(t.child.data(), dchild, (size_t)nbr * nch));
+    CKD(X.down(t.centers.data(), dcen, (size_t)nbr * dim));
+    CKD(X.down(t.ncoll.data(), dncoll, nbr));
+    CKD(X.down(t.coll.data(), dcoll, (size_t)nbr * nco));
+    CKD(X.finish());
+  }
   for (int l = 0; l <= lev; l++) {
     t.lfirst[l] = hlev[2 * l];
     t.llast[l] = hlev[2 * l + 1];
@@ -628,9 +716,14 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(S.get(&d_nchild, nb));
   CKD(S.get(&d_child, (size_t)nb * nch));
   CKD(S.get(&d_lor, nleaf));
-  CKD(upload(d_nchild, t.nchild.data(), nb, st));
-  CKD(upload(d_child, t.child.data(), (size_t)nb * nch, st));
-  CKD(upload(d_lor, leaf_of_rank.data(), nleaf, st));
+  {
+    StagedBatch X(st, staged_bytes({sizeof(int) * (size_t)nb, sizeof(int) * (size_t)nb * nch,
+                                    sizeof(int) * (size_t)nleaf}));
+    CKD(X.up(d_nchild, t.nchild.data(), nb));
+    CKD(X.up(d_child, t.child.data(), (size_t)nb * nch));
+    CKD(X.up(d_lor, leaf_of_rank.data(), nleaf));
+    CKD(X.finish());
+  }
   // ranges of the finished tree (the level restriction added boxes and
   // renumbered), level by level from the root
   CKD(S.get(&r0, nb));
@@ -644,8 +737,9 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   }
   t.s0.assign(nb, 0);
   t.s1.assign(nb, 0);
-  CKD(cudaMemcpyAsync(t.s0.data(), r0, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
-  CKD(cudaMemcpyAsync(t.s1.data(), r1, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));
+  StagedBatch Xr(st, staged_bytes({sizeof(int) * (size_t)nb, sizeof(int) * (size_t)nb}));
+  CKD(Xr.down(t.s0.data(), r0, nb));
+  CKD(Xr.down(t.s1.data(), r1, nb));
   // final order: leaf rank of each sorted position, to input order, stable sort
   {
     int *lstart = nullptr, *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
@@ -664,9 +758,9 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
   }
   const double tD = now_s();
+  if (same && nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+  CKD(Xr.finish());
   if (same) {
-    if (nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
-    CKD(cudaStreamSynchronize(st));
     t.t0 = t.s0;
     t.t1 = t.s1;
   } else {
@@ -674,8 +768,12 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     double* d_centers = nullptr;
     CKD(S.get(&d_rank, nb));
     CKD(S.get(&d_centers, (size_t)nb * dim));
-    CKD(upload(d_rank, dfs_rank.data(), nb, st));
-    CKD(upload(d_centers, t.centers.data(), (size_t)nb * dim, st));
+    {
+      StagedBatch X(st, staged_bytes({sizeof(int) * (size_t)nb, sizeof(double) * (size_t)nb * dim}));
+      CKD(X.up(d_rank, dfs_rank.data(), nb));
+      CKD(X.up(d_centers, t.centers.data(), (size_t)nb * dim));
+      CKD(X.finish());
+    }
     CKD(sort_points_device(t, d_trg, nt, nullptr, d_nchild, d_child, d_centers, d_rank, nleaf, leaf_of_rank,
                            d_itarg, t.t0, t.t1, st));
   }

@@ -3327,6 +3327,8 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   };
   const double tin = tnow();
+  double tp[8];
+  int np_ = 0;
   D = DevicePlan();
   D.P = H.P;
   const Params& P = H.P;
@@ -3370,6 +3372,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       if (G.p + 1 <= 32 && n > best) { best = n; D.dom_form_group = (int)gi; }
     }
   }
+  tp[np_++] = tnow();
   // 2D Taylor evaluation: one conversion per leaf slot, point chunks of <= 256
   std::vector<ConvTask> conv;
   std::vector<HornerTask> horner;
@@ -3441,6 +3444,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       t = u;
     }
   }
+  tp[np_++] = tnow();
   // padded operand tables of the 2D MMA transforms, one per order group
   std::vector<double> tables;
   if (P.dim == 2 && !P.all_direct) {
@@ -3459,6 +3463,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       G.tab = (long long)tables.size();
       build_conv3_table(H, G.p + 1, tables);
     }
+  tp[np_++] = tnow();
   // merge groups: consecutive tasks with the same destination
   std::vector<MergeGroup> groups;
   D.merge_beg.assign(P.nlevels + 1, 0);
@@ -3473,6 +3478,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     }
     D.merge_end[l] = (int)groups.size();
   }
+  tp[np_++] = tnow();
   // the split tasks still needed: the boxes on the path from the cut level
   // to every evaluation leaf whose conversion does not fuse the split
   std::vector<ShiftTask> split_kept;
@@ -3506,6 +3512,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.direct_pairs = H.direct_pairs;
   D.form_sources = H.form_sources;
   D.eval_points = H.eval_points;
+  tp[np_++] = tnow();
   // 3D: shared-memory paths when the largest order fits, else the scratch path
   std::vector<FormChunk> fchunks;
   std::vector<int> fcbeg;
@@ -3727,6 +3734,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.scratch = reinterpret_cast<double2*>(cur); cur += al((size_t)D.scratch_ctas * D.scratch_per_cta * 16);
   D.uscr = reinterpret_cast<double*>(cur); cur += al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8);
   CK(cudaStreamSynchronize(s));
+  if (getenv("FGT_TREE_TIMING"))
+    fprintf(stderr, "device plan prep parts: sort %.4f conv %.4f tables %.4f merge %.4f split %.4f rest %.4f\n",
+            tp[0] - tin, tp[1] - tp[0], tp[2] - tp[1], tp[3] - tp[2], tp[4] - tp[3], tm0 - tp[4]);
   if (getenv("FGT_TREE_TIMING"))
     fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes); eval tasks: taylor %d "
             "(conversion %d, max order %d) pw %d; form tasks: hermite %d (shared memory %d, max order %d) pw %d\n",
