@@ -3408,6 +3408,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     const int ntay = P.dim == 2 ? D.eval_taylor_n : D.eval3_nsplit;
+    long long nh = 0;
+    for (int t = 0; t < ntay; t++) nh += (ev[t].n + 255) / 256;
+    conv.reserve(ntay);
+    horner.reserve(nh);
     for (int t = 0; t < ntay; t++) {
       const EvalTask& e = ev[t];
       const long long Pn = e.p + 1, E = (Pn + 1) & ~1LL;

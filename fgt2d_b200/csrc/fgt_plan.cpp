@@ -12,6 +12,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -298,9 +299,12 @@ static void build_tasks(HostPlan& H) {
   {
     int nth = 1;
 #ifdef _OPENMP
-    if (s_hi > 8192) nth = std::max(1, std::min(omp_get_max_threads(), 64));
+    if (s_hi > 8192) nth = std::max(1, std::min(omp_get_max_threads(), 8));
 #endif
-    std::vector<int> cur((size_t)nth * nb);
+    // per-thread cursors, left uninitialised here (each thread clears its own)
+    std::unique_ptr<int[]> cur_buf(new int[(size_t)nth * nb]);
+    int* const curp = cur_buf.get();
+    auto cur = [&](size_t i) -> int& { return curp[i]; };
     const int chunk = (s_hi + 1 + nth - 1) / nth;
 #pragma omp parallel num_threads(nth) if (nth > 1)
     {
@@ -309,7 +313,7 @@ static void build_tasks(HostPlan& H) {
 #else
       const int th = 0;
 #endif
-      int* const c = cur.data() + (size_t)th * nb;
+      int* const c = curp + (size_t)th * nb;
       std::fill(c, c + nb, 0);
       const int s0 = th * chunk, s1 = std::min(s_hi + 1, s0 + chunk);
       for (int s = s0; s < s1; s++)
@@ -319,7 +323,7 @@ static void build_tasks(HostPlan& H) {
 #pragma omp for schedule(static)
       for (int a = 0; a < nb; a++) {
         int n = 0;
-        for (int q = 0; q < nth; q++) n += cur[(size_t)q * nb + a];
+        for (int q = 0; q < nth; q++) n += cur((size_t)q * nb + a);
         ioff[a + 1] = n;
       }
 #pragma omp single
@@ -331,8 +335,8 @@ static void build_tasks(HostPlan& H) {
       for (int a = 0; a < nb; a++) {
         int pos = ioff[a];
         for (int q = 0; q < nth; q++) {
-          const int n = cur[(size_t)q * nb + a];
-          cur[(size_t)q * nb + a] = pos;
+          const int n = cur((size_t)q * nb + a);
+          cur((size_t)q * nb + a) = pos;
           pos += n;
         }
       }
