@@ -97,6 +97,7 @@ def lib():
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
     L.fgt_ctx_set_tree.argtypes = [_vp, i]
     L.fgt_ctx_set_sm_budget.argtypes = [_vp, i]
+    L.fgt_ctx_set_scheme.argtypes = [_vp, i]
     L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
     L.fgt_server_set_precision.argtypes = [_vp, i]
     L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
@@ -168,19 +169,26 @@ def _p(a):
 class Context:
     """One CUDA device, its stream and the precision mode."""
 
-    def __init__(self, device=0, precision="auto", host_threads=0, tree="device"):
+    def __init__(self, device=0, precision="auto", host_threads=0, tree="device", scheme="planewave"):
         L = lib()
         h = _vp()
         _check(L.fgt_ctx_create(int(device), ctypes.byref(h)), "fgt_ctx_create")
         self._h = h
         self.set_precision(precision)
         self.set_tree(tree)
+        self.set_scheme(scheme)
         if host_threads:
             L.fgt_ctx_set_host_threads(self._h, int(host_threads))
 
     def set_tree(self, where):
         """Where plans build their tree: "device" (point work on the GPU) or "host"."""
         _check(lib().fgt_ctx_set_tree(self._h, {"device": 0, "host": 1}[where]), "fgt_ctx_set_tree")
+
+    def set_scheme(self, scheme):
+        """The algorithm of plans created afterwards: "planewave" (2d/planewave,
+        3d/planewave) or "nufft" (2d/nufft, 3d/nufft: plane-wave expansions at
+        the cut level only, their NUFFTs as the exact sums)."""
+        _check(lib().fgt_ctx_set_scheme(self._h, {"planewave": 0, "nufft": 1}[scheme]), "fgt_ctx_set_scheme")
 
     def set_sm_budget(self, sms):
         """SMs the persistent kernels of plans created afterwards size their grids for (0: all)."""

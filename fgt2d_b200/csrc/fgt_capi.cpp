@@ -33,6 +33,7 @@ struct fgt_ctx {
   int tree = FGT_TREE_DEVICE;
   int nthreads = 0;
   int sm_budget = 0;  // SMs the persistent kernels of this context's plans size their grids for (0: all)
+  int scheme = FGT_SCHEME_PLANEWAVE;  // the algorithm of the context's plans
   // uploads of a one-shot call's source strengths: they follow the points on
   // the copy engine while the tree build runs on `stream`
   cudaStream_t up_stream = nullptr;
@@ -513,6 +514,11 @@ int fgt_ctx_set_tree(fgt_ctx* c, int where) {
   c->tree = where;
   return FGT_OK;
 }
+int fgt_ctx_set_scheme(fgt_ctx* c, int scheme) {
+  if (!c || (scheme != FGT_SCHEME_PLANEWAVE && scheme != FGT_SCHEME_NUFFT)) return FGT_ERR_BADARG;
+  c->scheme = scheme;
+  return FGT_OK;
+}
 int fgt_ctx_set_sm_budget(fgt_ctx* c, int sms) {
   if (!c || sms < 0) return FGT_ERR_BADARG;
   c->sm_budget = sms;
@@ -603,9 +609,12 @@ int plan_create_impl(fgt_ctx* ctx, int dim, int nd, double delta, double eps, in
   if (st != FGT_OK) return st;
   if (ns == 0) return FGT_ERR_BADARG;
   if (!targ) nt = 0;  // no target array: no targets in the tree either
+  // the NUFFT scheme's 2D form takes charges only
+  if (ctx->scheme == FGT_SCHEME_NUFFT && dim == 2 && ifdipole) return FGT_ERR_UNSUPPORTED;
   std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
   if (!p) return FGT_ERR_NOMEM;
   p->ctx = ctx;
+  p->H.scheme = ctx->scheme;
   p->pre_q = pre_q;
   p->pre_rn = pre_rn;
   p->pre_ds = pre_ds;
@@ -701,6 +710,7 @@ int fgt_plan_create_shard(fgt_ctx* ctx, int dim, int nd, double delta, double ep
   std::unique_ptr<fgt_plan> p(new (std::nothrow) fgt_plan());
   if (!p) return FGT_ERR_NOMEM;
   p->ctx = ctx;
+  p->H.scheme = ctx->scheme;
   p->shard_n = nranks;
   p->shard_r = rank;
   CKS(cudaSetDevice(ctx->device));

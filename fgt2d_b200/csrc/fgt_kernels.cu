@@ -2323,6 +2323,63 @@ __global__ void __launch_bounds__(256) k_form3d_pw(KP k, const FormTask* __restr
     for (int e = threadIdx.x; e < k.nexp; e += blockDim.x) out[e] = make_double2(0.0, 0.0);
 }
 
+// 2D plane-wave expansion of a box formed directly from its sources: the
+// exact sum that the NUFFT scheme computes with a type-1 NUFFT
+// (g2dformpwc_vec, 2d/nufft/src/g2drouts.f:1234-1307),
+//   mp[a + n2 b] = sum_s q_s ws_a ws_b exp(-i (t_a x_s + t_b y_s)),
+// a over the n2 positive x nodes, b over every y node (positive half first,
+// the layout of the plane-wave form and of k_eval2d).  One CTA per (box,
+// density); per chunk of FORM_CH sources the first threads build one
+// source's factor rows each in shared memory (the phases by the recurrence
+// e^{-i t1 x} (e^{-2 i t1 x})^m, the charge folded into the x row), then
+// every thread sums its own coefficients over the chunk.
+__global__ void __launch_bounds__(256) k_form2d_pw(KP k, const FormTask* __restrict__ tasks) {
+  const FormTask T = tasks[blockIdx.x];
+  const int ind = blockIdx.y;
+  const int npw = k.npw, n2 = k.n2, nexp = k.nexp;
+  extern __shared__ double sm[];
+  double2* FX = reinterpret_cast<double2*>(sm);  // [FORM_CH][n2]
+  double2* FY = FX + FORM_CH * n2;               // [FORM_CH][npw]
+  const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
+  double2* out = k.mp + ((size_t)T.slot * k.nd + ind) * nexp;
+  for (int c0 = 0; c0 < T.n; c0 += FORM_CH) {
+    const int m = min(FORM_CH, T.n - c0);
+    __syncthreads();
+    if (threadIdx.x < m) {
+      const int i = T.s0 + c0 + threadIdx.x;
+      const double x = (k.src[2 * i] - cx) * k.dsq, y = (k.src[2 * i + 1] - cy) * k.dsq;
+      const double q = k.chg[(size_t)i * k.nd + ind];
+      double2 ex = cexpi(-k.t1 * x), ey = cexpi(-k.t1 * y);
+      const double2 exx = cmul(ex, ex), eyy = cmul(ey, ey);
+      double2* fx = FX + threadIdx.x * n2;
+      double2* fy = FY + threadIdx.x * npw;
+      for (int mm = 0; mm < n2; mm++) {
+        const double w = k.ws[mm];  // node (2 mm + 1) t1; the weights are even in t
+        fx[mm] = make_double2(ex.x * w * q, ex.y * w * q);
+        const double2 b = make_double2(ey.x * w, ey.y * w);
+        fy[mm] = b;
+        fy[n2 + mm] = make_double2(b.x, -b.y);
+        ex = cmul(ex, exx);
+        ey = cmul(ey, eyy);
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nexp; e += blockDim.x) {
+      const int a = e % n2, b = e / n2;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int t = 0; t < m; t++) acc = cfma(FX[t * n2 + a], FY[t * npw + b], acc);
+      if (c0 == 0) {
+        out[e] = acc;
+      } else {
+        const double2 p = out[e];
+        out[e] = make_double2(p.x + acc.x, p.y + acc.y);
+      }
+    }
+  }
+  if (T.n == 0)  // no sources: a zero expansion
+    for (int e = threadIdx.x; e < nexp; e += blockDim.x) out[e] = make_double2(0.0, 0.0);
+}
+
 // ------------------------------------------------------------ (b) shifts
 // merge: parent = sum over its children of child * W (g2dshiftpw_vec)
 __global__ void k_merge(KP k, const MergeGroup* __restrict__ groups, const ShiftTask* __restrict__ tasks) {
@@ -4028,6 +4085,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       size_t sh = ((size_t)FORM_CH * (2 * P.npw + n2) + 8) * 16;
       CK(cudaFuncSetAttribute(k_form3d_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
       k_form3d_pw<<<dim3(D.form_pw_n, nd), 256, sh, st>>>(k, D.form + D.form_hermite_n);
+      launches++;
+    }
+    if (P.dim == 2 && D.form_pw_n > 0) {  // the NUFFT scheme's direct form
+      const size_t sh = (size_t)FORM_CH * (P.npw + n2) * 16;
+      if (sh > 227 * 1024) return cudaErrorNotSupported;
+      CK(cudaFuncSetAttribute(k_form2d_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+      k_form2d_pw<<<dim3(D.form_pw_n, nd), 256, sh, st>>>(k, D.form + D.form_hermite_n);
       launches++;
     }
     mark(2);

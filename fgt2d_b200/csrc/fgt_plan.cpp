@@ -87,6 +87,134 @@ static void build_tables(HostPlan& H) {
   (void)nch;
 }
 
+// (d) near field, target-centric: for every leaf, the ifhung source boxes
+// whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333);
+// the same in both schemes
+static void build_near_tasks(HostPlan& H) {
+  const Params& P = H.P;
+  const Tree& t = H.tree;
+  const Lists& L = H.lists;
+  const int nb = t.nboxes, npl = P.npwlevel;
+  H.dir.clear();
+  H.dir_src.clear();
+  // box A -> source boxes S with A in list1(S), as CSR in the order of S
+  // (a transpose of the list1 CSR: the S range is cut into one chunk per
+  // thread, each thread counts and then places its entries through its own
+  // cursors, laid out chunk after chunk, so every segment lists S in
+  // increasing box id whatever the thread count)
+  std::vector<int> ioff(nb + 1, 0), into;
+  int nlevend = npl < P.nlevels ? npl : P.nlevels;
+  const int s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;  // levels 0..nlevend are ids 0..s_hi
+  {
+    int nth = 1;
+#ifdef _OPENMP
+    if (s_hi > 8192) nth = std::max(1, std::min(omp_get_max_threads(), 8));
+#endif
+    // per-thread cursors, left uninitialised here (each thread clears its own)
+    std::unique_ptr<int[]> cur_buf(new int[(size_t)nth * nb]);
+    int* const curp = cur_buf.get();
+    auto cur = [&](size_t i) -> int& { return curp[i]; };
+    const int chunk = (s_hi + 1 + nth - 1) / nth;
+#pragma omp parallel num_threads(nth) if (nth > 1)
+    {
+#ifdef _OPENMP
+      const int th = omp_get_thread_num();
+#else
+      const int th = 0;
+#endif
+      int* const c = curp + (size_t)th * nb;
+      std::fill(c, c + nb, 0);
+      const int s0 = th * chunk, s1 = std::min(s_hi + 1, s0 + chunk);
+      for (int s = s0; s < s1; s++)
+        if (L.ifhung[s])
+          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) c[L.l1[k]]++;
+#pragma omp barrier
+#pragma omp for schedule(static)
+      for (int a = 0; a < nb; a++) {
+        int n = 0;
+        for (int q = 0; q < nth; q++) n += cur((size_t)q * nb + a);
+        ioff[a + 1] = n;
+      }
+#pragma omp single
+      {
+        for (int a = 0; a < nb; a++) ioff[a + 1] += ioff[a];
+        into.assign(ioff[nb], 0);
+      }
+#pragma omp for schedule(static)
+      for (int a = 0; a < nb; a++) {
+        int pos = ioff[a];
+        for (int q = 0; q < nth; q++) {
+          const int n = cur((size_t)q * nb + a);
+          cur((size_t)q * nb + a) = pos;
+          pos += n;
+        }
+      }
+      for (int s = s0; s < s1; s++)
+        if (L.ifhung[s])
+          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[c[L.l1[k]]++] = s;
+    }
+  }
+  // per leaf: its source ranges (ancestors' segments, leaf first) once per
+  // evaluated point set, and its tasks of <= CH points; counted per leaf,
+  // placed by prefix sums in box order, filled in parallel
+  const int CH = 32;  // one warp per task
+  const bool sets[2] = {P.ifpgh >= 1, P.ifpghtarg >= 1};
+  // ranges and sources summed down the ancestor chains, level by level
+  std::vector<long long> cum_ns(nb, 0);
+  std::vector<int> cum_r(nb, 0);
+  for (int l = 0; l <= P.nlevels; l++) {
+#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
+    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
+      int r = ioff[b + 1] - ioff[b];
+      long long ns_ = 0;
+      for (int k = ioff[b]; k < ioff[b + 1]; k++) ns_ += t.ns(into[k]);
+      const int a = t.parent[b];
+      cum_r[b] = r + (a >= 0 ? cum_r[a] : 0);
+      cum_ns[b] = ns_ + (a >= 0 ? cum_ns[a] : 0);
+    }
+  }
+  std::vector<int> nr(nb, 0);
+  std::vector<long long> roff(nb + 1, 0), toff(nb + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; b++) {
+    if (t.nchild[b] != 0 || cum_r[b] == 0) continue;
+    const int r = cum_r[b];
+    nr[b] = r;
+    int nset = 0, nt_ = 0;
+    for (int set = 0; set < 2; set++) {
+      const int n = set == 0 ? t.ns(b) : t.nt(b);
+      if (!sets[set] || n == 0) continue;
+      nset++;
+      nt_ += (n + CH - 1) / CH;
+    }
+    roff[b + 1] = (long long)r * nset;
+    toff[b + 1] = nt_;
+  }
+  for (int b = 0; b < nb; b++) {
+    roff[b + 1] += roff[b];
+    toff[b + 1] += toff[b];
+  }
+  H.dir_src.resize(roff[nb]);
+  H.dir.resize(toff[nb]);
+  long long pairs = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs)
+  for (int b = 0; b < nb; b++) {
+    if (nr[b] == 0) continue;
+    long long ro = roff[b], to = toff[b];
+    for (int set = 0; set < 2; set++) {
+      const int n = set == 0 ? t.ns(b) : t.nt(b);
+      if (!sets[set] || n == 0) continue;
+      const int i0 = set == 0 ? t.s0[b] : t.t0[b];
+      const int off = (int)ro;
+      for (int a = b; a >= 0; a = t.parent[a])
+        for (int k = ioff[a]; k < ioff[a + 1]; k++) H.dir_src[ro++] = {t.s0[into[k]], t.ns(into[k])};
+      for (int c = 0; c < n; c += CH) H.dir[to++] = {set, i0 + c, std::min(CH, n - c), off, nr[b]};
+      pairs += cum_ns[b] * n;
+    }
+  }
+  H.direct_pairs = pairs;
+}
+
 // Flattens the tree into the stage task arrays.
 static void build_tasks(HostPlan& H) {
   double tq[16];
@@ -285,134 +413,100 @@ static void build_tasks(HostPlan& H) {
     H.shift_bytes[2] = per * (ra + rb);
   }
   tq[nq++] = now();
-  tq[nq++] = now();
-  // (d) near field, target-centric: for every leaf, the ifhung source boxes
-  // whose list1 holds the leaf or one of its ancestors (fgt2d.f:1287-1333)
-  // box A -> source boxes S with A in list1(S), as CSR in the order of S
-  // (a transpose of the list1 CSR: the S range is cut into one chunk per
-  // thread, each thread counts and then places its entries through its own
-  // cursors, laid out chunk after chunk, so every segment lists S in
-  // increasing box id whatever the thread count)
-  std::vector<int> ioff(nb + 1, 0), into;
-  int nlevend = npl < P.nlevels ? npl : P.nlevels;
-  const int s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;  // levels 0..nlevend are ids 0..s_hi
-  {
-    int nth = 1;
-#ifdef _OPENMP
-    if (s_hi > 8192) nth = std::max(1, std::min(omp_get_max_threads(), 8));
-#endif
-    // per-thread cursors, left uninitialised here (each thread clears its own)
-    std::unique_ptr<int[]> cur_buf(new int[(size_t)nth * nb]);
-    int* const curp = cur_buf.get();
-    auto cur = [&](size_t i) -> int& { return curp[i]; };
-    const int chunk = (s_hi + 1 + nth - 1) / nth;
-#pragma omp parallel num_threads(nth) if (nth > 1)
-    {
-#ifdef _OPENMP
-      const int th = omp_get_thread_num();
-#else
-      const int th = 0;
-#endif
-      int* const c = curp + (size_t)th * nb;
-      std::fill(c, c + nb, 0);
-      const int s0 = th * chunk, s1 = std::min(s_hi + 1, s0 + chunk);
-      for (int s = s0; s < s1; s++)
-        if (L.ifhung[s])
-          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) c[L.l1[k]]++;
-#pragma omp barrier
-#pragma omp for schedule(static)
-      for (int a = 0; a < nb; a++) {
-        int n = 0;
-        for (int q = 0; q < nth; q++) n += cur((size_t)q * nb + a);
-        ioff[a + 1] = n;
-      }
-#pragma omp single
-      {
-        for (int a = 0; a < nb; a++) ioff[a + 1] += ioff[a];
-        into.assign(ioff[nb], 0);
-      }
-#pragma omp for schedule(static)
-      for (int a = 0; a < nb; a++) {
-        int pos = ioff[a];
-        for (int q = 0; q < nth; q++) {
-          const int n = cur((size_t)q * nb + a);
-          cur((size_t)q * nb + a) = pos;
-          pos += n;
-        }
-      }
-      for (int s = s0; s < s1; s++)
-        if (L.ifhung[s])
-          for (int k = L.l1off[s]; k < L.l1off[s + 1]; k++) into[c[L.l1[k]]++] = s;
-    }
-  }
-  tq[nq++] = now();
-  // per leaf: its source ranges (ancestors' segments, leaf first) once per
-  // evaluated point set, and its tasks of <= CH points; counted per leaf,
-  // placed by prefix sums in box order, filled in parallel
-  const int CH = 32;  // one warp per task
-  const bool sets[2] = {P.ifpgh >= 1, P.ifpghtarg >= 1};
-  // ranges and sources summed down the ancestor chains, level by level
-  std::vector<long long> cum_ns(nb, 0);
-  std::vector<int> cum_r(nb, 0);
-  for (int l = 0; l <= P.nlevels; l++) {
-#pragma omp parallel for schedule(static) if (t.llast[l] - t.lfirst[l] > 4096)
-    for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
-      int r = ioff[b + 1] - ioff[b];
-      long long ns_ = 0;
-      for (int k = ioff[b]; k < ioff[b + 1]; k++) ns_ += t.ns(into[k]);
-      const int a = t.parent[b];
-      cum_r[b] = r + (a >= 0 ? cum_r[a] : 0);
-      cum_ns[b] = ns_ + (a >= 0 ? cum_ns[a] : 0);
-    }
-  }
-  tq[nq++] = now();
-  std::vector<int> nr(nb, 0);
-  std::vector<long long> roff(nb + 1, 0), toff(nb + 1, 0);
-#pragma omp parallel for schedule(static)
-  for (int b = 0; b < nb; b++) {
-    if (t.nchild[b] != 0 || cum_r[b] == 0) continue;
-    const int r = cum_r[b];
-    nr[b] = r;
-    int nset = 0, nt_ = 0;
-    for (int set = 0; set < 2; set++) {
-      const int n = set == 0 ? t.ns(b) : t.nt(b);
-      if (!sets[set] || n == 0) continue;
-      nset++;
-      nt_ += (n + CH - 1) / CH;
-    }
-    roff[b + 1] = (long long)r * nset;
-    toff[b + 1] = nt_;
-  }
-  for (int b = 0; b < nb; b++) {
-    roff[b + 1] += roff[b];
-    toff[b + 1] += toff[b];
-  }
-  H.dir_src.resize(roff[nb]);
-  H.dir.resize(toff[nb]);
-  long long pairs = 0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs)
-  for (int b = 0; b < nb; b++) {
-    if (nr[b] == 0) continue;
-    long long ro = roff[b], to = toff[b];
-    for (int set = 0; set < 2; set++) {
-      const int n = set == 0 ? t.ns(b) : t.nt(b);
-      if (!sets[set] || n == 0) continue;
-      const int i0 = set == 0 ? t.s0[b] : t.t0[b];
-      const int off = (int)ro;
-      for (int a = b; a >= 0; a = t.parent[a])
-        for (int k = ioff[a]; k < ioff[a + 1]; k++) H.dir_src[ro++] = {t.s0[into[k]], t.ns(into[k])};
-      for (int c = 0; c < n; c += CH) H.dir[to++] = {set, i0 + c, std::min(CH, n - c), off, nr[b]};
-      pairs += cum_ns[b] * n;
-    }
-  }
-  H.direct_pairs = pairs;
+  build_near_tasks(H);
   tq[nq++] = now();
   if (getenv("FGT_TREE_TIMING")) {
-    fprintf(stderr, "tasks (dir %zu ranges %zu, near-field csr %d):", H.dir.size(), H.dir_src.size(), ioff[nb]);
+    fprintf(stderr, "tasks (dir %zu ranges %zu):", H.dir.size(), H.dir_src.size());
     for (int i = 1; i < nq; i++) fprintf(stderr, " %.4f", tq[i] - tq[i - 1]);
     fprintf(stderr, "\n");
   }
   (void)D;
+}
+
+// The NUFFT scheme (2d/nufft/src/fgt2d.f:695-1060, 3d/nufft/src/fgt3d.f
+// twin): at the cut level (the root level when the cut is above it) a box
+// with more than ndiv sources forms its plane-wave expansion from all its
+// sources (the exact sum of the type-1 NUFFT, route PW), which is also its
+// own local expansion; the boxes with evaluation points add the shifted
+// expansions of their colleagues that have children (listpw of the scheme,
+// which then hold more than ndiv sources) and evaluate the sum at every
+// point of the box (the exact sum of the type-2 NUFFT, route PW) when they
+// have such a colleague or an expansion of their own.  No merge, no split;
+// the near field is the plane-wave scheme's.
+static void build_tasks_nufft(HostPlan& H) {
+  Params& P = H.P;
+  const Tree& t = H.tree;
+  const int nb = t.nboxes, D = P.dim;
+  const int ndiv = D == 2 ? 80 : 100;  // fgt2d.f:162, fgt3d.f:165
+  const int lc = P.nlevstart;
+  H.mp_slot.assign(nb, -1);
+  H.loc_slot.assign(nb, -1);
+  H.nmp = H.nloc = 0;
+  H.form.clear(); H.merge.clear(); H.split.clear(); H.m2l.clear(); H.m2l_nbr.clear();
+  H.eval.clear();
+  H.merge_beg.assign(P.nlevels + 1, 0);
+  H.merge_end.assign(P.nlevels + 1, 0);
+  H.split_beg.assign(P.nlevels + 1, 0);
+  H.split_end.assign(P.nlevels + 1, 0);
+  H.form_sources = H.eval_points = 0;
+  H.form_route_flops = H.eval_route_flops = 0;
+  H.shift_bytes[0] = H.shift_bytes[1] = H.shift_bytes[2] = 0;
+  if (!P.all_direct && lc <= P.nlevels) {
+    const int a0 = t.lfirst[lc], a1 = t.llast[lc];
+    auto big = [&](int b) { return t.ns(b) > ndiv; };
+    auto pw_nbr = [&](int b, int jb) { return jb != b && t.nchild[jb] > 0; };
+    auto npts = [&](int b) { return (P.ifpghtarg > 0 ? t.nt(b) : 0) + (P.ifpgh > 0 ? t.ns(b) : 0); };
+    for (int b = a0; b <= a1; b++)
+      if (big(b)) H.mp_slot[b] = H.nmp++;
+    for (int b = a0; b <= a1; b++) {
+      if (npts(b) <= 0) continue;
+      bool any = big(b);
+      for (int i = 0; i < t.ncoll[b] && !any; i++) any = pw_nbr(b, t.coll[(size_t)b * t.nco + i]);
+      if (any) H.loc_slot[b] = H.nloc++;
+    }
+    // form (fgt2d.f:824-900)
+    for (int b = a0; b <= a1; b++)
+      if (H.mp_slot[b] >= 0) {
+        H.form.push_back({b, t.s0[b], t.ns(b), H.mp_slot[b], 0, ROUTE_PW});
+        H.form_sources += t.ns(b);
+      }
+    // mp -> loc (fgt2d.f:918-958): own expansion plus the colleagues'
+    const double xmin = t.boxsize[lc];
+    for (int b = a0; b <= a1; b++) {
+      if (H.loc_slot[b] < 0) continue;
+      M2LTask mt{H.loc_slot[b], H.mp_slot[b], (int)H.m2l_nbr.size(), 0};
+      for (int i = 0; i < t.ncoll[b]; i++) {
+        const int j = t.coll[(size_t)b * t.nco + i];
+        if (!pw_nbr(b, j) || H.mp_slot[j] < 0) continue;
+        int s = 0, mul = 1;
+        for (int d = 0; d < D; d++) {
+          const int o = (int)std::lround((t.c(b, d) - t.c(j, d)) / xmin);
+          s += (o + 1) * mul;
+          mul *= 3;
+        }
+        H.m2l_nbr.push_back({H.mp_slot[j], s});
+        mt.cnt++;
+      }
+      H.m2l.push_back(mt);
+    }
+    // evaluation at every point of the box (fgt2d.f:973-1047)
+    for (int b = a0; b <= a1; b++) {
+      if (H.loc_slot[b] < 0) continue;
+      for (int set = 1; set >= 0; set--) {
+        if (set == 1 && !(P.ifpghtarg >= 1 && t.nt(b) > 0)) continue;
+        if (set == 0 && !(P.ifpgh >= 1 && t.ns(b) > 0)) continue;
+        const int i0 = set ? t.t0[b] : t.s0[b], n = set ? t.nt(b) : t.ns(b);
+        for (int c = 0; c < n; c += 2048)
+          H.eval.push_back({b, set, i0 + c, std::min(2048, n - c), H.loc_slot[b], 0, ROUTE_PW});
+        H.eval_points += n;
+      }
+    }
+    H.form_route_flops = 8.0 * (double)H.form_sources * P.nexp * P.nd;
+    H.eval_route_flops = 8.0 * (double)H.eval_points * P.nexp * P.nd;
+    const long long per = 16LL * P.nexp * P.nd;
+    H.shift_bytes[1] = per * ((long long)H.nmp + H.nloc);
+  }
+  build_near_tasks(H);
 }
 
 static void finish_plan(HostPlan& H) {
@@ -424,7 +518,8 @@ static void finish_plan(HostPlan& H) {
   double t1 = now();
   H.host_lists_s = t1 - t0;
   if (!P.all_direct) build_tables(H);
-  build_tasks(H);
+  if (P.scheme == 1) build_tasks_nufft(H);
+  else build_tasks(H);
   H.box_centers = t.centers;
   H.host_plan_s = now() - t1;
 }
@@ -453,6 +548,7 @@ bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, 
                 int ifcharge, int ifdipole) {
   Params& P = H.P;
   P = Params();
+  P.scheme = H.scheme;
   P.dim = dim; P.nd = nd; P.delta = delta; P.eps = eps; P.ns = ns; P.nt = nt;
   P.ifpgh = ifpgh; P.ifpghtarg = ifpghtarg;
   P.ifcharge = ifcharge; P.ifdipole = ifdipole;
@@ -466,7 +562,8 @@ bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, 
     P.nlocal0 = nl0 + std::max(ifpgh, ifpghtarg) - 1;
     return false;
   }
-  ts.ndiv0 = dim == 2 ? 10 : 40;
+  // fgt2d.f:158-162 / fgt3d.f:161-165 (3D NUFFT scheme: ndiv0 = 20)
+  ts.ndiv0 = dim == 2 ? 10 : (P.scheme == 1 ? 20 : 40);
   ts.ndiv = dim == 2 ? 80 : 100;
   const int hcap = dim == 2 ? 18 : 15;
   int nlmax = npwlevel + 4, nls = std::max(npwlevel, 0);
@@ -477,6 +574,9 @@ bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, 
     if (nl0 <= hcap) { nlmax = i; break; }
     bsize /= 2;
   }
+  // the NUFFT scheme's tree stops one level below the cut (2d/nufft
+  // fgt2d.f:188, 3d/nufft fgt3d.f:192)
+  if (P.scheme == 1 && npwlevel >= 0) nlmax = npwlevel + 1;
   P.nlmax = nlmax;
   ts.levcut = npwlevel;
   ts.nlmax = nlmax;

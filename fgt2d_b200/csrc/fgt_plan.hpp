@@ -57,11 +57,16 @@ struct Params {
   bool large_delta = false, all_direct = false;
   int nlocal0 = 0;  // large-delta local order
   double cen0[3] = {0, 0, 0};
+  // 0: the plane-wave scheme (2d/planewave, 3d/planewave); 1: the NUFFT
+  // scheme (2d/nufft, 3d/nufft): plane-wave expansions at the cut level
+  // only, formed from and evaluated at every point of their box
+  int scheme = 0;
 };
 
 // Host side of the plan.
 struct HostPlan {
   Params P;
+  int scheme = 0;  // Params.scheme of the next build (set before it)
   Tree tree;
   Lists lists;
   std::vector<int> nlocal;        // per level

@@ -54,6 +54,19 @@ enum {
   FGT_TREE_HOST = 1    /* tree build entirely on the host (OpenMP) */
 };
 
+/* Algorithm of a context's plans (fgt_ctx_set_scheme). */
+enum {
+  /* the plane-wave scheme of 2d/planewave and 3d/planewave (default):
+   * Hermite / plane-wave / Taylor expansions on every level from the cut
+   * level down */
+  FGT_SCHEME_PLANEWAVE = 0,
+  /* the NUFFT scheme of 2d/nufft and 3d/nufft: plane-wave expansions at the
+   * cut level only, formed from and evaluated at every point of a cut-level
+   * box; the reference computes them with type-1 / type-2 NUFFTs (FINUFFT),
+   * this library with the exact sums those approximate.  2D: charges only. */
+  FGT_SCHEME_NUFFT = 1
+};
+
 typedef struct fgt_ctx fgt_ctx;
 typedef struct fgt_plan fgt_plan;
 
@@ -90,6 +103,10 @@ int fgt_ctx_set_tree(fgt_ctx* ctx, int where);
  * transform server uses half, so that requests arriving while a large one
  * runs find SMs free.  No counterpart in the reference. */
 int fgt_ctx_set_sm_budget(fgt_ctx* ctx, int sms);
+/* the algorithm of the plans created after the call (FGT_SCHEME_*): the
+ * reference selects it by building 2d/planewave or 2d/nufft (3D likewise),
+ * whose fgt2d / fgt3d share one signature (2d/nufft/src/fgt2d.f:19-22). */
+int fgt_ctx_set_scheme(fgt_ctx* ctx, int scheme);
 /* the context used by the Fortran-named entry points (device 0, created on
  * first use) */
 fgt_ctx* fgt_default_ctx(void);

@@ -854,6 +854,34 @@ void g2dpweval(int nd, double delta, const double* cent, int npw, const double* 
     }
   }
 }
+// The 2D plane-wave expansion of a box formed directly from its sources:
+// the quantity that g2dformpwc_vec of the NUFFT scheme (2d/nufft/src/
+// g2drouts.f:1234-1307) computes with a type-1 NUFFT (finufft2d1many),
+// here as the exact sum, in this restatement's 2D layout pw(npw/2, npw)
+// (x nodes of the positive half first index, every y node second):
+//   pw(k2, k1) += q ws(k2) ws(k1) exp(-i (ts(k2) x + ts(k1) y)).
+void g2dformpwc(int nd, double delta, const double* src, int ns, const double* chg,
+                const double* cent, int npw, const double* ws, const double* ts, cplx* pw) {
+  cplx eye(0, 1);
+  double dsq = 1.0 / std::sqrt(delta);
+  int n2 = npw / 2;
+  std::vector<cplx> w1(npw + 1), w2(npw + 1);
+  for (int i = 0; i < ns; i++) {
+    double x = (src[2 * i] - cent[0]) * dsq, y = (src[2 * i + 1] - cent[1]) * dsq;
+    for (int j = 1; j <= npw; j++) {
+      w1[j] = ws[j] * std::exp(-eye * ts[j] * x);
+      w2[j] = ws[j] * std::exp(-eye * ts[j] * y);
+    }
+    for (int ind = 0; ind < nd; ind++) {
+      double q = chg[nd * i + ind];
+      cplx* out = pw + (size_t)ind * n2 * npw;
+      for (int k1 = 1; k1 <= npw; k1++) {
+        cplx yq = q * w2[k1];
+        for (int k2 = 1; k2 <= n2; k2++) out[(k2 - 1) + n2 * (k1 - 1)] += yq * w1[k2];
+      }
+    }
+  }
+}
 // g2dformlc_vec, g2drouts.f:621-681 (local accumulated, caller zeroes)
 void g2dformlc(int nd, double delta, const double* src, int ns, const double* chg,
                const double* cent, int p, double* local) {
@@ -1437,12 +1465,21 @@ struct Result {
 
 // fgt2d (fgt2d.f:19-462) + fgt2dmain (fgt2d.f:468-1348) and the 3D twins
 // (fgt3d.f:19-477, 483-1527).  Output arrays are overwritten.
+//
+// nufft = 1 restates the NUFFT scheme of 2d/nufft and 3d/nufft instead
+// (fgt2d.f / fgt3d.f there): the tree stops one level below the cut level
+// (fgt2d.f:188, fgt3d.f:192; 3D ndiv0 = 20, fgt3d.f:161), the boxes of the
+// cut level with more than ndiv sources form their plane-wave expansion
+// from all their sources (type-1 NUFFT there, the exact sum here), the
+// expansions are shifted between cut-level colleagues, evaluated at every
+// point of the cut-level boxes that have one (type-2 NUFFT there, exact
+// here), and the rest is the same direct interaction.
 template <int D>
 int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int ifcharge,
             const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
             int ifpgh, double* pot, double* grad, double* hess,
             int nt, const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
-            double* hesstarg, Result* res) {
+            double* hesstarg, Result* res, int nufft = 0) {
   const int NCH = Tree<D>::NCH;
   const int NH = D == 2 ? 3 : 6;
   if (nd < 1 || !(delta > 0) || !(eps > 0) || ns < 0 || nt < 0) return ORC_BADARG;
@@ -1482,7 +1519,8 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
     return ORC_OK;
   }
 
-  const int ndiv0 = D == 2 ? 10 : 40, ndiv = D == 2 ? 80 : 100, hcap = D == 2 ? 18 : 15;
+  if (nufft && D == 2 && ifdipole) return ORC_UNSUPPORTED;
+  const int ndiv0 = D == 2 ? 10 : (nufft ? 20 : 40), ndiv = D == 2 ? 80 : 100, hcap = D == 2 ? 18 : 15;
   int nlmax = npwlevel + 4;
   int nlevstart = std::max(npwlevel, 0);
   double bsize = bs0 / (double)(1 << nlevstart);
@@ -1492,6 +1530,7 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
     if (nlocal0 <= hcap) { nlmax = i; break; }
     bsize = bsize / 2;
   }
+  if (nufft && npwlevel >= 0) nlmax = npwlevel + 1;
   Tree<D> t;
   std::vector<int> isrc, isrcse, itarg, itargse;
   build_tree<D>(t, sources, ns, targ, nt, ndiv, ndiv0, npwlevel, nlmax, bs0, cen0, isrc, isrcse,
@@ -1555,7 +1594,7 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
   std::vector<int> ifhung(nboxes + 1, 0);
   for (int ilev = 0; ilev <= nlevend; ilev++)
     for (int ibox = t.L(ilev, 0); ibox <= t.L(ilev, 1); ibox++)
-      if (t.nchild[ibox] == 0 && NS(ibox) > 0) ifhung[ibox] = 1;
+      if (t.nchild[ibox] == 0 && NS(ibox) > 0 && (!nufft || NS(ibox) <= ndiv)) ifhung[ibox] = 1;
   std::vector<std::vector<int>> list1;
   if constexpr (D == 2) modified_list1_2d(t, npwlevel, list1);
   else modified_list1_3d(t, npwlevel, list1);
@@ -1657,6 +1696,73 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
       for (int ind = 0; ind < nd; ind++)
         for (size_t j = 0; j < nexp; j++) b[ind * nexp + j] += a[ind * nexp + j] * w[j];
     };
+    if (nufft) {
+      // NUFFT scheme, steps 1-3 at the cut level (the level of the cut when
+      // it is >= 0; the reference leaves npwlevel in {-2, -1} undefined, the
+      // root level is used here)
+      const int lc = nlevstart;
+      const double xmin = t.boxsize[lc];
+      auto big = [&](int b) { return NS(b) > ndiv; };
+      // listpw of the NUFFT scheme: the cut level's colleagues with children
+      // (2d/nufft/src/common/tree_routs4.f:940-953, tree_routs3d.f gt3d_computelistpw)
+      auto lpwn = [&](int ibox) {
+        std::vector<int> v;
+        for (int i = 0; i < t.nnbors[ibox]; i++) {
+          int jbox = t.nbors[(size_t)ibox * Tree<D>::NCO + i];
+          if (jbox != ibox && t.nchild[jbox] > 0) v.push_back(jbox);
+        }
+        return v;
+      };
+      // step 1 (fgt2d.f:824-900 / fgt3d.f:860-960): form, and the copy into
+      // the box's own local expansion
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = t.L(lc, 0); ibox <= t.L(lc, 1); ibox++) {
+        if (!big(ibox)) continue;
+        const double* sp = ssort.data() + (size_t)D * S0(ibox);
+        const double* q = csort.data() + (size_t)nd * S0(ibox);
+        const double* c = &t.centers[(size_t)D * ibox];
+        if (D == 2) {
+          g2dformpwc(nd, delta, sp, NS(ibox), q, c, npw, ws.data(), ts.data(), MP(ibox));
+        } else {
+          if (ifcharge) g3dformpwc(nd, delta, sp, NS(ibox), q, c, npw, ws.data(), ts.data(), MP(ibox));
+          if (ifdipole)
+            g3dformpwd_add(nd, delta, sp, NS(ibox), rsort.data() + (size_t)D * S0(ibox),
+                           dsort.data() + (size_t)nd * S0(ibox), c, npw, ws.data(), ts.data(), MP(ibox));
+        }
+        for (size_t j = 0; j < (size_t)nd * nexp; j++) LO(ibox)[j] += MP(ibox)[j];
+      }
+      // step 2 (fgt2d.f:918-958 / fgt3d.f:990-1030): shifts from the colleagues
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = t.L(lc, 0); ibox <= t.L(lc, 1); ibox++) {
+        int npts = 0;
+        if (ifpghtarg > 0) npts += NT(ibox);
+        if (ifpgh > 0) npts += NS(ibox);
+        if (npts <= 0) continue;
+        for (int jbox : lpwn(ibox)) {
+          if (!big(jbox)) continue;
+          int jx = (int)std::lround((t.c(ibox, 0) - t.c(jbox, 0)) / xmin);
+          int jy = (int)std::lround((t.c(ibox, 1) - t.c(jbox, 1)) / xmin);
+          int jz = D == 3 ? (int)std::lround((t.c(ibox, 2) - t.c(jbox, 2)) / xmin) : -1;
+          shift(MP(jbox), LO(ibox), wsh.data() + nexp * ((jx + 1) + 3 * (jy + 1) + 9 * (jz + 1)));
+        }
+      }
+      // step 3 (fgt2d.f:973-1047 / fgt3d.f:1045-1130): evaluation at every
+      // point of the boxes with a listpw entry or an expansion of their own
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = t.L(lc, 0); ibox <= t.L(lc, 1); ibox++) {
+        if (lpwn(ibox).empty() && !big(ibox)) continue;
+        const double* c = &t.centers[(size_t)D * ibox];
+        const int i0 = T0(ibox), j0 = S0(ibox), nts = NT(ibox), nss = NS(ibox);
+        if (nts > 0 && ifpghtarg >= 1) {
+          if (D == 2) g2dpweval(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 2 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
+          else g3dpweval(nd, delta, c, npw, ts.data(), LO(ibox), tsort.data() + 3 * (size_t)i0, nts, ifpghtarg, PT(i0), GT(i0), HT(i0));
+        }
+        if (nss > 0 && ifpgh >= 1) {
+          if (D == 2) g2dpweval(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 2 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
+          else g3dpweval(nd, delta, c, npw, ts.data(), LO(ibox), ssort.data() + 3 * (size_t)j0, nss, ifpgh, PS(j0), GS(j0), HS(j0));
+        }
+      }
+    } else {
     // step 1: form mp (fgt2d.f:871-959 / fgt3d.f:899-1098)
     for (int ilev = nlevels; ilev >= std::max(npwlevel + 1, 0); ilev--) {
       int p = nlocal[ilev], P = p + 1;
@@ -1808,6 +1914,7 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         }
       }
     }
+    }  // plane-wave scheme
   }
   // step 6: direct (fgt2d.f:1287-1333, cutoff eps/90; fgt3d.f:1466-1512, cutoff eps)
   {
@@ -1963,6 +2070,26 @@ int orc_fgt_full(int dim, int nd, double delta, double eps, int ns, const double
   Result r;
   int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r)
                     : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r);
+  if (info) {
+    info[0] = r.npwlevel; info[1] = r.nlevels; info[2] = r.nboxes; info[3] = r.npw;
+    info[4] = r.nlmax; info[5] = (int)r.nleaf_direct; info[6] = 0; info[7] = 0;
+  }
+  return rc;
+}
+
+// The NUFFT scheme (2d/nufft, 3d/nufft; see fgt_run) with the full argument
+// list of orc_fgt_full.
+int orc_fgt_nufft(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                  int ifcharge, const double* charge, int ifdipole, const double* rnormal,
+                  const double* dipstr, int ifpgh, double* pot, double* grad, double* hess, int nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, int* info, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  Result r;
+  int rc = dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r, 1)
+                    : fgt_run<3>(nd, delta, eps, ns, sources, ifcharge, charge, ifdipole, rnormal, dipstr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, &r, 1);
   if (info) {
     info[0] = r.npwlevel; info[1] = r.nlevels; info[2] = r.nboxes; info[3] = r.npw;
     info[4] = r.nlmax; info[5] = (int)r.nleaf_direct; info[6] = 0; info[7] = 0;

@@ -56,6 +56,8 @@ def lib():
                                    ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
                                    ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                    _dp, _dp, _dp, _ip, ctypes.c_int]
+        L.orc_fgt_nufft.restype = ctypes.c_int
+        L.orc_fgt_nufft.argtypes = L.orc_fgt_full.argtypes
         L.orc_direct_cut.restype = None
         L.orc_direct_cut.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
@@ -159,10 +161,12 @@ def fgt_pgh(dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=
 
 
 def fgt_full(dim, nd, delta, eps, sources, charge=None, targ=None, ifpgh=1, ifpghtarg=0,
-             rnormal=None, dipstr=None, nthreads=0):
+             rnormal=None, dipstr=None, nthreads=0, scheme="planewave"):
     """The restated transform with charges and/or dipoles (``charge`` or
     ``dipstr`` None switches that source kind off): rnormal (ns, dim),
-    dipstr (ns, nd).  Returns the dict of fgt_pgh."""
+    dipstr (ns, nd).  scheme "nufft" restates the NUFFT scheme of 2d/nufft,
+    3d/nufft (its NUFFTs as the exact sums they approximate).  Returns the
+    dict of fgt_pgh."""
     src = _f64(sources)
     ns = src.shape[0]
     ifc, ifd = int(charge is not None), int(dipstr is not None)
@@ -175,9 +179,10 @@ def fgt_full(dim, nd, delta, eps, sources, charge=None, targ=None, ifpgh=1, ifpg
     pot, grad, hess = np.zeros((max(ns, 1), nd)), np.zeros((max(ns, 1), dim, nd)), np.zeros((max(ns, 1), H, nd))
     pt, gt, ht = np.zeros((max(nt, 1), nd)), np.zeros((max(nt, 1), dim, nd)), np.zeros((max(nt, 1), H, nd))
     info = np.zeros(8, dtype=np.int32)
-    rc = lib().orc_fgt_full(dim, nd, float(delta), float(eps), ns, _d(src), ifc, _d(q), ifd, _d(rn),
-                            _d(ds), ifpgh, _d(pot), _d(grad), _d(hess), nt, _d(trg), ifpghtarg,
-                            _d(pt), _d(gt), _d(ht), info.ctypes.data_as(_ip), nthreads)
+    fn = lib().orc_fgt_nufft if scheme == "nufft" else lib().orc_fgt_full
+    rc = fn(dim, nd, float(delta), float(eps), ns, _d(src), ifc, _d(q), ifd, _d(rn),
+            _d(ds), ifpgh, _d(pot), _d(grad), _d(hess), nt, _d(trg), ifpghtarg,
+            _d(pt), _d(gt), _d(ht), info.ctypes.data_as(_ip), nthreads)
     if rc != 0:
         raise RuntimeError(f"oracle fgt returned status {rc}")
     keys = ["npwlevel", "nlevels", "nboxes", "npw", "nlmax", "ndirect_leaves"]
