@@ -89,6 +89,15 @@ PROFILED_TRAFFIC = {
     ("2d_circle_clustered_N1e7_d1e-6_e1e-6", "k_form2d_mma<2>"):
         (216619776 + 16602112, "profiles/form2d_mma_2d_circle_N1e7.md"),
 }
+# The same from a capture of a smaller case of the same distribution, delta
+# and eps (so the same orders): DRAM bytes of the captured launch and its
+# executed flops; a launch's traffic is scaled by its executed flops (the
+# kernel reads each of its sources once, so traffic grows with them).
+PROFILED_TRAFFIC_SCALED = {
+    ("k_form2d_f32", 1e-6, 1e-6): (43087872 + 176384, 596234028.0,
+                                   "profiles/form2d_f32_2d_circle_N2e6.md (N = 2e6 capture, scaled by "
+                                   "the launch's executed flops)"),
+}
 
 
 # ------------------------------------------------------------------ clocks
@@ -435,6 +444,9 @@ def ours_arm(args, w, rank, world, local_rank):
         t_k = sum(dms) / len(dms) / 1e3
         ach = dalg / t_k / 1e12
         traffic, tsrc = PROFILED_TRAFFIC.get((w["name"], dname), (None, None))
+        sc = PROFILED_TRAFFIC_SCALED.get((dname, w["delta"], w["eps"]))
+        if traffic is None and sc is not None and dfl > 0:
+            traffic, tsrc = sc[0] * dfl / sc[1], sc[2]
         roof = {"bound": "tensor", "kernel": dname, "stage": "form", "achieved": ach, "peak": tf,
                 "unit": "TFLOP/s", "frac": ach / tf, "traffic": traffic,
                 "peak_source": f"{peak_src} bf16 dense (burst), MEASURED_PEAKS.json",
