@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -404,6 +405,206 @@ __global__ void k_ref_colleagues(const int* __restrict__ lev, int l, double lim,
   }
 }
 
+// ---- level restriction on the device (pts_tree_fix_lr, pts_tree2d4.f:693-996,
+// as Builder::fix_lr in fgt_tree.cpp) ----
+// Boxes keep their creation ids until the end: the original boxes, then the
+// first pass's new boxes level by level, then the second pass's; every
+// level is at most three contiguous id ranges ("LrRanges"), in the order the
+// host build numbers them after each reorganisation.  The final renumbering
+// and the colleagues of the finished tree follow at the end.
+struct LrRanges {
+  int a[3], b[3];  // ranges [a[i], b[i]] (empty when b < a)
+};
+__device__ __forceinline__ bool lr_touch(const double* __restrict__ cen, int dim, int x, int y, double lim) {
+  for (int d = 0; d < dim; d++)
+    if (!(fabs(cen[(size_t)x * dim + d] - cen[(size_t)y * dim + d]) <= lim)) return false;
+  return true;
+}
+__device__ __forceinline__ int lr_box(const LrRanges& R, int i) {  // i-th box of the concatenated ranges, or -1
+  for (int r = 0; r < 3; r++) {
+    const int n = R.b[r] - R.a[r] + 1;
+    if (n <= 0) continue;
+    if (i < n) return R.a[r] + i;
+    i -= n;
+  }
+  return -1;
+}
+__host__ __device__ __forceinline__ int lr_count(const LrRanges& R) {
+  int n = 0;
+  for (int r = 0; r < 3; r++) n += R.b[r] >= R.a[r] ? R.b[r] - R.a[r] + 1 : 0;
+  return n;
+}
+// first flag pass: a leaf colleague of a grandparent that touches the parent
+// of a box two levels down is flagged 1 (0 -> 1 only, so the order of the
+// boxes does not matter); boxes [b0, b1], dist per level l of the box
+__global__ void k_lr_flag1(int b0, int b1, const int* __restrict__ level, const double* __restrict__ dist1,
+                           const int* __restrict__ par, const int* __restrict__ nchild,
+                           const int* __restrict__ ncoll, const int* __restrict__ coll, int nco,
+                           const double* __restrict__ cen, int dim, int* __restrict__ flag) {
+  for (int b = b0 + blockIdx.x * blockDim.x + threadIdx.x; b <= b1; b += gridDim.x * blockDim.x) {
+    const double dist = dist1[level[b]];
+    const int dad = par[b], gd = par[dad];
+    for (int i = 0; i < ncoll[gd]; i++) {
+      const int jb = coll[(size_t)gd * nco + i];
+      if (nchild[jb] == 0 && flag[jb] == 0 && lr_touch(cen, dim, jb, dad, dist)) atomicCAS(flag + jb, 0, 1);
+    }
+  }
+}
+// second flag pass, one level: a flagged box flags the leaf colleagues of its
+// parent that touch it (0 -> 2)
+__global__ void k_lr_flag2(int b0, int b1, double dist, const int* __restrict__ par,
+                           const int* __restrict__ nchild, const int* __restrict__ ncoll,
+                           const int* __restrict__ coll, int nco, const double* __restrict__ cen, int dim,
+                           int* __restrict__ flag) {
+  for (int b = b0 + blockIdx.x * blockDim.x + threadIdx.x; b <= b1; b += gridDim.x * blockDim.x) {
+    const int f = flag[b];
+    if (f != 1 && f != 2) continue;
+    const int dad = par[b];
+    for (int i = 0; i < ncoll[dad]; i++) {
+      const int jb = coll[(size_t)dad * nco + i];
+      if (nchild[jb] == 0 && flag[jb] == 0 && lr_touch(cen, dim, jb, b, dist)) atomicCAS(flag + jb, 0, 2);
+    }
+  }
+}
+// updateflags (tree_routs4.f:217-326) over the boxes of one level: a box
+// flagged 3 keeps flag 1 when a child of one of its colleagues has children
+// and touches it, else 0
+__global__ void k_lr_update(LrRanges R, double dist, const int* __restrict__ nchild,
+                            const int* __restrict__ child, int nch, const int* __restrict__ ncoll,
+                            const int* __restrict__ coll, int nco, const double* __restrict__ cen, int dim,
+                            int* __restrict__ flag) {
+  const int n = lr_count(R);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int box = lr_box(R, i);
+    if (flag[box] != 3) continue;
+    int f = 0;
+    for (int q = 0; q < ncoll[box] && f == 0; q++) {
+      const int jb = coll[(size_t)box * nco + q];
+      for (int j = 0; j < nch; j++) {
+        const int kb = child[(size_t)jb * nch + j];
+        if (kb >= 0 && nchild[kb] > 0 && lr_touch(cen, dim, kb, box, dist)) {
+          f = 1;
+          break;
+        }
+      }
+    }
+    flag[box] = f;
+  }
+}
+// One block of 1024 threads: rank of every flagged box (flag > 0) among the
+// flagged boxes of the concatenated ranges; *total and, for the first box
+// of each of the nb_mark boxes in mark[], the rank there (rank_at[k]).
+__global__ void __launch_bounds__(1024) k_lr_scan(LrRanges R, const int* __restrict__ flag, int* __restrict__ pos,
+                                                  int* __restrict__ total) {
+  __shared__ int part[1024];
+  const int n = lr_count(R);
+  const int per = (n + 1023) / 1024, i0 = min(n, (int)threadIdx.x * per), i1 = min(n, i0 + per);
+  int sum = 0;
+  for (int i = i0; i < i1; i++) sum += flag[lr_box(R, i)] > 0;
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int i = i0; i < i1; i++) {
+    pos[i] = run;
+    run += flag[lr_box(R, i)] > 0;
+  }
+  if (threadIdx.x == 1023) *total = part[1023];
+}
+// tree_refine_boxes_flag (tree_routs4.f:334-388): the flagged boxes of the
+// concatenated ranges get nch children each, from id base on, in the ranges'
+// order; a child is flagged 3 when its parent's flag is 1.  hsz[l] is a
+// quarter of the size of level l (the children's centre offset).
+__global__ void k_lr_children(LrRanges R, const int* __restrict__ pos, int base, int nch, int dim,
+                              const double* __restrict__ hsz, int* __restrict__ level, int* __restrict__ par,
+                              int* __restrict__ nchild, int* __restrict__ child, double* __restrict__ cen,
+                              int* __restrict__ flag) {
+  const int n = lr_count(R);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * nch;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / nch), j = (int)(t - (long long)i * nch);
+    const int box = lr_box(R, i);
+    const int f = flag[box];
+    if (f <= 0) continue;
+    const int c = base + nch * pos[i] + j;
+    const int l = level[box];
+    if (j == 0) nchild[box] = nch;
+    child[(size_t)box * nch + j] = c;
+    par[c] = box;
+    level[c] = l + 1;
+    nchild[c] = 0;
+    for (int q = 0; q < nch; q++) child[(size_t)c * nch + q] = -1;
+    const double h = hsz[l];
+    for (int d = 0; d < dim; d++) cen[(size_t)c * dim + d] = cen[(size_t)box * dim + d] + (((j >> d) & 1) ? h : -h);
+    flag[c] = f == 1 ? 3 : 0;
+  }
+}
+// colleagues of the boxes of the concatenated ranges from their parents'
+// lists (computecoll; the children of the parent's colleagues within lim, in
+// the parent's colleague order then child order), unused slots -1
+__global__ void k_lr_colleagues(LrRanges R, double lim, int nch, int nco, int dim, const int* __restrict__ par,
+                                const int* __restrict__ child, const double* __restrict__ cen,
+                                int* __restrict__ ncoll, int* __restrict__ coll) {
+  const int n = lr_count(R);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = lr_box(R, i), dad = par[b];
+    int cnt = 0;
+    for (int q = 0; q < ncoll[dad]; q++) {
+      const int jb = coll[(size_t)dad * nco + q];
+      for (int j = 0; j < nch; j++) {
+        const int kb = child[(size_t)jb * nch + j];
+        if (kb >= 0 && lr_touch(cen, dim, kb, b, lim)) coll[(size_t)b * nco + cnt++] = kb;
+      }
+    }
+    for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
+    ncoll[b] = cnt;
+  }
+}
+__global__ void k_lr_gather(const int* __restrict__ src, const int* __restrict__ idx, int n, int* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = src[idx[k]];
+}
+// flags other than 3 back to 0
+__global__ void k_lr_keep3(int n, int* __restrict__ flag) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+    if (flag[b] != 3) flag[b] = 0;
+}
+// final numbering: creation id -> final id from a table of (first creation
+// id, last, first final id) ranges sorted by creation id
+__global__ void k_lr_map(const int* __restrict__ tab, int ntab, int n, int* __restrict__ map) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+    int lo = 0, hi = ntab - 1;  // last range whose first id is <= b
+    while (lo < hi) {
+      const int m = (lo + hi + 1) >> 1;
+      if (tab[3 * m] <= b) lo = m;
+      else hi = m - 1;
+    }
+    map[b] = tab[3 * lo + 2] + (b - tab[3 * lo]);
+  }
+}
+__global__ void k_lr_scatter(int n, const int* __restrict__ map, int nch, int dim, const int* __restrict__ level,
+                             const int* __restrict__ par, const int* __restrict__ nchild,
+                             const int* __restrict__ child, const double* __restrict__ cen, int* __restrict__ level2,
+                             int* __restrict__ par2, int* __restrict__ nchild2, int* __restrict__ child2,
+                             double* __restrict__ cen2) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+    const int f = map[b];
+    level2[f] = level[b];
+    par2[f] = par[b] >= 0 ? map[par[b]] : -1;
+    nchild2[f] = nchild[b];
+    for (int j = 0; j < nch; j++) {
+      const int c = child[(size_t)b * nch + j];
+      child2[(size_t)f * nch + j] = c >= 0 ? map[c] : -1;
+    }
+    for (int d = 0; d < dim; d++) cen2[(size_t)f * dim + d] = cen[(size_t)b * dim + d];
+  }
+}
+
 // Device scratch of one build, stream-ordered on the build's stream (no
 // device-wide synchronisation) and freed at the end of the build.
 struct Scratch {
@@ -680,50 +881,246 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   if (nbr > cap) return cudaErrorLaunchFailure;
   int lev = 0;
   while (lev + 1 <= ts.nlmax && hlev[2 * (lev + 1) + 1] >= hlev[2 * (lev + 1)]) lev++;
-  t.nboxes = nbr;
-  t.level.resize(nbr);
-  t.parent.resize(nbr);
-  t.nchild.resize(nbr);
-  t.child.resize((size_t)nbr * nch);
-  t.centers.resize((size_t)nbr * dim);
-  t.ncoll.resize(nbr);
-  t.coll.resize((size_t)nbr * nco);
+  const double tB = now_s();
+  // level restriction on the device (pts_tree_fix_lr, pts_tree2d4.f:693-996)
+  std::vector<int> lf0(lev + 1), ll0(lev + 1);
+  for (int l = 0; l <= lev; l++) {
+    lf0[l] = hlev[2 * l];
+    ll0[l] = hlev[2 * l + 1];
+  }
+  std::vector<double> bsz(lev + 3);
+  bsz[0] = ts.bs0;
+  for (int l = 1; l < (int)bsz.size(); l++) bsz[l] = bsz[l - 1] / 2;
+  int nbc = nbr;  // boxes so far (creation ids)
+  // LR arrays, growable
+  struct LrA {
+    int *par = nullptr, *nch = nullptr, *child = nullptr, *level = nullptr, *ncoll = nullptr, *coll = nullptr,
+        *flag = nullptr, *pos = nullptr;
+    double* cen = nullptr;
+    size_t cap = 0;
+  } A;
+  auto lr_alloc = [&](LrA& X, size_t c) -> cudaError_t {
+    X.cap = c;
+    CKD(S.get(&X.par, c));
+    CKD(S.get(&X.nch, c));
+    CKD(S.get(&X.child, c * nch));
+    CKD(S.get(&X.level, c));
+    CKD(S.get(&X.ncoll, c));
+    CKD(S.get(&X.coll, c * nco));
+    CKD(S.get(&X.flag, c));
+    CKD(S.get(&X.pos, c));
+    CKD(S.get(&X.cen, c * dim));
+    return cudaSuccess;
+  };
+  auto lr_copy = [&](LrA& X, const int* par_, const int* nch_, const int* child_, const int* level_,
+                     const int* ncoll_, const int* coll_, const int* flag_, const double* cen_, size_t n) -> cudaError_t {
+    auto cp = [&](void* d, const void* s_, size_t b) {
+      return b ? cudaMemcpyAsync(d, s_, b, cudaMemcpyDeviceToDevice, st) : cudaSuccess;
+    };
+    CKD(cp(X.par, par_, 4 * n));
+    CKD(cp(X.nch, nch_, 4 * n));
+    CKD(cp(X.child, child_, 4 * n * nch));
+    CKD(cp(X.level, level_, 4 * n));
+    CKD(cp(X.ncoll, ncoll_, 4 * n));
+    CKD(cp(X.coll, coll_, 4 * n * nco));
+    if (flag_) CKD(cp(X.flag, flag_, 4 * n));
+    CKD(cp(X.cen, cen_, 8 * n * dim));
+    return cudaSuccess;
+  };
+  auto lr_grow = [&](size_t need) -> cudaError_t {
+    if (need <= A.cap) return cudaSuccess;
+    LrA B;
+    CKD(lr_alloc(B, std::max(need, 2 * A.cap)));
+    CKD(lr_copy(B, A.par, A.nch, A.child, A.level, A.ncoll, A.coll, A.flag, A.cen, nbc));
+    A = B;
+    return cudaSuccess;
+  };
+  CKD(lr_alloc(A, (size_t)nbr + std::max<size_t>(nbr / 4, 4096)));
+  CKD(lr_copy(A, dpar, dnch, dchild, dlevel, dncoll, dcoll, nullptr, dcen, nbr));
+  CKD(cudaMemsetAsync(A.flag, 0, sizeof(int) * A.cap, st));
+  // ranges per level: the original boxes, the first pass's, the second's
+  std::vector<LrRanges> RL(lev + 2);
+  for (int l = 0; l <= lev + 1; l++)
+    for (int r = 0; r < 3; r++) {
+      RL[l].a[r] = 0;
+      RL[l].b[r] = -1;
+    }
+  for (int l = 0; l <= lev; l++) {
+    RL[l].a[0] = lf0[l];
+    RL[l].b[0] = ll0[l];
+  }
+  int* d_tot = nullptr;
+  double *d_dist1 = nullptr, *d_hsz = nullptr;
+  CKD(S.get(&d_tot, 64));
+  CKD(S.get(&d_dist1, lev + 3));
+  CKD(S.get(&d_hsz, lev + 3));
+  auto grid_for = [](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 1184)); };
+  if (lev >= 2) {
+    std::vector<double> dist1(lev + 3, 0.0), hsz(lev + 3, 0.0);
+    for (int l = 2; l <= lev; l++) dist1[l] = 1.05 * (bsz[l - 1] + bsz[l - 2]) / 2.0;
+    for (int l = 0; l <= lev; l++) hsz[l] = bsz[l + 1] / 2;
+    CKD(upload(d_dist1, dist1.data(), dist1.size(), st));
+    CKD(upload(d_hsz, hsz.data(), hsz.size(), st));
+    // flag passes
+    k_lr_flag1<<<grid_for(ll0[lev] - lf0[2] + 1), 256, 0, st>>>(lf0[2], ll0[lev], A.level, d_dist1, A.par, A.nch,
+                                                                A.ncoll, A.coll, nco, A.cen, dim, A.flag);
+    for (int l = lev; l >= 1; l--)
+      k_lr_flag2<<<grid_for(ll0[l] - lf0[l] + 1), 256, 0, st>>>(lf0[l], ll0[l], 1.05 * (bsz[l] + bsz[l - 1]) / 2.0,
+                                                                 A.par, A.nch, A.ncoll, A.coll, nco, A.cen, dim,
+                                                                 A.flag);
+    // first refinement pass: flagged boxes of levels 1 .. lev-2, in id order
+    if (lev >= 3) {
+      LrRanges R;
+      for (int r = 0; r < 3; r++) { R.a[r] = 0; R.b[r] = -1; }
+      R.a[0] = lf0[1];
+      R.b[0] = ll0[lev - 2];
+      k_lr_scan<<<1, 1024, 0, st>>>(R, A.flag, A.pos, d_tot);
+      // exclusive ranks at the first box of each level 1 .. lev-2
+      std::vector<int> idx(lev - 2);
+      for (int l = 1; l <= lev - 2; l++) idx[l - 1] = lf0[l] - lf0[1];
+      int* d_idx = nullptr;
+      CKD(S.get(&d_idx, idx.size()));
+      CKD(upload(d_idx, idx.data(), idx.size(), st));
+      k_lr_gather<<<1, 64, 0, st>>>(A.pos, d_idx, (int)idx.size(), d_tot + 1);
+      std::vector<int> rk(lev - 1);
+      CKD(cudaMemcpyAsync(rk.data(), d_tot, sizeof(int) * rk.size(), cudaMemcpyDeviceToHost, st));
+      CKD(cudaStreamSynchronize(st));
+      const int total = rk[0];
+      // rank at level l's first box: rk[l] (l = 1 .. lev-2); level l's flagged boxes: up to the next
+      std::vector<int> at(lev);
+      for (int l = 1; l <= lev - 2; l++) at[l] = rk[l];
+      at[lev - 1] = total;
+      if (total > 0) {
+        CKD(lr_grow((size_t)nbc + (size_t)nch * total));
+        k_lr_children<<<grid_for((long long)lr_count(R) * nch), 256, 0, st>>>(R, A.pos, nbc, nch, dim, d_hsz, A.level,
+                                                                             A.par, A.nch, A.child, A.cen, A.flag);
+        for (int l = 1; l <= lev - 2; l++) {
+          RL[l + 1].a[1] = nbc + nch * at[l];
+          RL[l + 1].b[1] = nbc + nch * at[l + 1] - 1;
+        }
+        nbc += nch * total;
+      }
+    }
+    // colleagues after the first pass (computecoll on that tree)
+    for (int l = 1; l <= lev; l++)
+      k_lr_colleagues<<<grid_for(lr_count(RL[l])), 256, 0, st>>>(RL[l], (double)1.05f * bsz[l], nch, nco, dim, A.par,
+                                                                A.child, A.cen, A.ncoll, A.coll);
+    k_lr_keep3<<<grid_for(nbc), 256, 0, st>>>(nbc, A.flag);
+    // second pass, level by level (updateflags, then refinement in the
+    // order old boxes, this pass's boxes)
+    for (int l = 2; l <= lev - 2; l++) {
+      k_lr_update<<<grid_for(lr_count(RL[l])), 256, 0, st>>>(RL[l], 1.05 * (bsz[l] + bsz[l + 1]) / 2.0, A.nch,
+                                                             A.child, nch, A.ncoll, A.coll, nco, A.cen, dim, A.flag);
+      k_lr_scan<<<1, 1024, 0, st>>>(RL[l], A.flag, A.pos, d_tot);
+      int total = 0;
+      CKD(cudaMemcpyAsync(&total, d_tot, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CKD(cudaStreamSynchronize(st));
+      if (total <= 0) continue;
+      CKD(lr_grow((size_t)nbc + (size_t)nch * total));
+      k_lr_children<<<grid_for((long long)lr_count(RL[l]) * nch), 256, 0, st>>>(RL[l], A.pos, nbc, nch, dim, d_hsz,
+                                                                               A.level, A.par, A.nch, A.child, A.cen,
+                                                                               A.flag);
+      RL[l + 1].a[2] = nbc;
+      RL[l + 1].b[2] = nbc + nch * total - 1;
+      LrRanges Rn;
+      for (int r = 0; r < 3; r++) { Rn.a[r] = 0; Rn.b[r] = -1; }
+      Rn.a[0] = RL[l + 1].a[2];
+      Rn.b[0] = RL[l + 1].b[2];
+      k_lr_colleagues<<<grid_for(nch * total), 256, 0, st>>>(Rn, (double)1.05f * bsz[l + 1], nch, nco, dim, A.par,
+                                                             A.child, A.cen, A.ncoll, A.coll);
+      nbc += nch * total;
+    }
+  }
+  CKD(cudaGetLastError());
+  // final numbering: per level the original boxes, then each pass's
+  std::vector<int> tab, nlevb(lev + 1, 0);
   {
-    const size_t i4 = sizeof(int) * (size_t)nbr;
-    StagedBatch X(st, staged_bytes({i4, i4, i4, i4 * nch, sizeof(double) * (size_t)nbr * dim, i4, i4 * nco}));
-    CKD(X.down(t.level.data(), dlevel, nbr));
-    CKD(X.down(t.parent.data(), dpar, nbr));
-    CKD(X.down(t.nchild.data(), dnch, nbr));
-    CKD(X.down(t.child.data(), dchild, (size_t)nbr * nch));
-    CKD(X.down(t.centers.data(), dcen, (size_t)nbr * dim));
-    CKD(X.down(t.ncoll.data(), dncoll, nbr));
-    CKD(X.down(t.coll.data(), dcoll, (size_t)nbr * nco));
+    std::vector<std::array<int, 3>> rows;
+    int fin = 0;
+    for (int l = 0; l <= lev; l++) {
+      t.lfirst[l] = fin;
+      for (int r = 0; r < 3; r++) {
+        const int a = RL[l].a[r], b = RL[l].b[r];
+        if (b < a) continue;
+        rows.push_back({a, b, fin});
+        fin += b - a + 1;
+      }
+      t.llast[l] = fin - 1;
+    }
+    std::sort(rows.begin(), rows.end());
+    for (auto& r : rows) tab.insert(tab.end(), {r[0], r[1], r[2]});
+    if (fin != nbc) return cudaErrorLaunchFailure;
+  }
+  const int nb = nbc;
+  int *d_tab = nullptr, *d_map = nullptr, *d_nchild = nullptr, *d_child = nullptr, *d_par2 = nullptr,
+      *d_level2 = nullptr, *d_ncoll2 = nullptr, *d_coll2 = nullptr, *d_lev2 = nullptr;
+  double* d_cen2 = nullptr;
+  CKD(S.get(&d_tab, tab.size()));
+  CKD(S.get(&d_map, nb));
+  CKD(S.get(&d_nchild, nb));
+  CKD(S.get(&d_child, (size_t)nb * nch));
+  CKD(S.get(&d_par2, nb));
+  CKD(S.get(&d_level2, nb));
+  CKD(S.get(&d_cen2, (size_t)nb * dim));
+  CKD(S.get(&d_ncoll2, nb));
+  CKD(S.get(&d_coll2, (size_t)nb * nco));
+  CKD(S.get(&d_lev2, 2 * nslot + 1));
+  CKD(upload(d_tab, tab.data(), tab.size(), st));
+  k_lr_map<<<grid_for(nb), 256, 0, st>>>(d_tab, (int)tab.size() / 3, nb, d_map);
+  k_lr_scatter<<<grid_for(nb), 256, 0, st>>>(nb, d_map, nch, dim, A.level, A.par, A.nch, A.child, A.cen, d_level2,
+                                             d_par2, d_nchild, d_child, d_cen2);
+  // colleagues of the finished tree (computecoll), the root's as before
+  {
+    std::vector<int> lv(2 * nslot + 1, 0);
+    for (int l = 0; l < nslot; l++) {
+      lv[2 * l] = 0;
+      lv[2 * l + 1] = -1;
+    }
+    for (int l = 0; l <= lev; l++) {
+      lv[2 * l] = t.lfirst[l];
+      lv[2 * l + 1] = t.llast[l];
+    }
+    lv[2 * nslot] = nb;
+    CKD(upload(d_lev2, lv.data(), lv.size(), st));
+    CKD(cudaMemcpyAsync(d_ncoll2, A.ncoll, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CKD(cudaMemcpyAsync(d_coll2, A.coll, sizeof(int) * nco, cudaMemcpyDeviceToDevice, st));
+    for (int l = 1; l <= lev; l++)
+      k_ref_colleagues<<<grid_for(t.llast[l] - t.lfirst[l] + 1), 256, 0, st>>>(
+          d_lev2, l, (double)1.05f * bsz[l], nch, nco, dim, d_par2, d_nchild, d_child, d_cen2, d_ncoll2, d_coll2);
+  }
+  CKD(cudaGetLastError());
+  t.nboxes = nb;
+  t.nlevels = lev;
+  t.level.resize(nb);
+  t.parent.resize(nb);
+  t.nchild.resize(nb);
+  t.child.resize((size_t)nb * nch);
+  t.centers.resize((size_t)nb * dim);
+  t.ncoll.resize(nb);
+  t.coll.resize((size_t)nb * nco);
+  {
+    const size_t i4 = sizeof(int) * (size_t)nb;
+    StagedBatch X(st, staged_bytes({i4, i4, i4, i4 * nch, sizeof(double) * (size_t)nb * dim, i4, i4 * nco}));
+    CKD(X.down(t.level.data(), d_level2, nb));
+    CKD(X.down(t.parent.data(), d_par2, nb));
+    CKD(X.down(t.nchild.data(), d_nchild, nb));
+    CKD(X.down(t.child.data(), d_child, (size_t)nb * nch));
+    CKD(X.down(t.centers.data(), d_cen2, (size_t)nb * dim));
+    CKD(X.down(t.ncoll.data(), d_ncoll2, nb));
+    CKD(X.down(t.coll.data(), d_coll2, (size_t)nb * nco));
     CKD(X.finish());
   }
-  for (int l = 0; l <= lev; l++) {
-    t.lfirst[l] = hlev[2 * l];
-    t.llast[l] = hlev[2 * l + 1];
-    if (l > 0) t.boxsize[l] = t.boxsize[l - 1] / 2;
-  }
-  const double tB = now_s();
-  std::vector<int> idmap;
-  tree_finish(t, lev, idmap, true);
+  for (int l = 1; l <= lev; l++) t.boxsize[l] = bsz[l];
+  t.boxsize.resize(lev + 1);
+  t.lfirst.resize(lev + 1);
+  t.llast.resize(lev + 1);
   const double tC = now_s();
   std::vector<int> dfs_rank, leaf_of_rank;
   tree_leaf_ranks(t, dfs_rank, leaf_of_rank);
-  const int nb = t.nboxes, nleaf = (int)leaf_of_rank.size();
-  int *d_nchild = nullptr, *d_child = nullptr, *d_lor = nullptr;
-  CKD(S.get(&d_nchild, nb));
-  CKD(S.get(&d_child, (size_t)nb * nch));
+  const int nleaf = (int)leaf_of_rank.size();
+  int* d_lor = nullptr;
   CKD(S.get(&d_lor, nleaf));
-  {
-    StagedBatch X(st, staged_bytes({sizeof(int) * (size_t)nb, sizeof(int) * (size_t)nb * nch,
-                                    sizeof(int) * (size_t)nleaf}));
-    CKD(X.up(d_nchild, t.nchild.data(), nb));
-    CKD(X.up(d_child, t.child.data(), (size_t)nb * nch));
-    CKD(X.up(d_lor, leaf_of_rank.data(), nleaf));
-    CKD(X.finish());
-  }
+  CKD(upload(d_lor, leaf_of_rank.data(), nleaf, st));
   // ranges of the finished tree (the level restriction added boxes and
   // renumbered), level by level from the root
   CKD(S.get(&r0, nb));
