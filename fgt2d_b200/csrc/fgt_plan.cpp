@@ -12,7 +12,9 @@
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
+#include <exception>
 #include <memory>
+#include <thread>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -232,7 +234,7 @@ static void build_tasks(HostPlan& H) {
   H.loc_slot.assign(nb, -1);
   H.nmp = H.nloc = 0;
   H.form.clear(); H.merge.clear(); H.split.clear(); H.m2l.clear(); H.m2l_nbr.clear();
-  H.eval.clear(); H.dir.clear(); H.dir_src.clear();
+  H.eval.clear();
   H.merge_beg.assign(P.nlevels + 1, 0);
   H.merge_end.assign(P.nlevels + 1, 0);
   H.split_beg.assign(P.nlevels + 1, 0);
@@ -413,10 +415,8 @@ static void build_tasks(HostPlan& H) {
     H.shift_bytes[2] = per * (ra + rb);
   }
   tq[nq++] = now();
-  build_near_tasks(H);
-  tq[nq++] = now();
   if (getenv("FGT_TREE_TIMING")) {
-    fprintf(stderr, "tasks (dir %zu ranges %zu):", H.dir.size(), H.dir_src.size());
+    fprintf(stderr, "far-field tasks:");
     for (int i = 1; i < nq; i++) fprintf(stderr, " %.4f", tq[i] - tq[i - 1]);
     fprintf(stderr, "\n");
   }
@@ -506,7 +506,6 @@ static void build_tasks_nufft(HostPlan& H) {
     const long long per = 16LL * P.nexp * P.nd;
     H.shift_bytes[1] = per * ((long long)H.nmp + H.nloc);
   }
-  build_near_tasks(H);
 }
 
 static void finish_plan(HostPlan& H) {
@@ -518,8 +517,30 @@ static void finish_plan(HostPlan& H) {
   double t1 = now();
   H.host_lists_s = t1 - t0;
   if (!P.all_direct) build_tables(H);
-  if (P.scheme == 1) build_tasks_nufft(H);
-  else build_tasks(H);
+  // the near-field tasks (list1 side) and the far-field tasks (slots, form,
+  // shifts, evaluation) read the tree and lists and write disjoint fields of
+  // H: built concurrently
+  std::exception_ptr near_err;
+  std::thread near([&H, &near_err] {
+    try {
+      const double a = now();
+      build_near_tasks(H);
+      if (getenv("FGT_TREE_TIMING"))
+        fprintf(stderr, "near-field tasks: %.4f (dir %zu ranges %zu)\n", now() - a, H.dir.size(), H.dir_src.size());
+    } catch (...) {
+      near_err = std::current_exception();
+    }
+  });
+  std::exception_ptr far_err;
+  try {
+    if (P.scheme == 1) build_tasks_nufft(H);
+    else build_tasks(H);
+  } catch (...) {
+    far_err = std::current_exception();
+  }
+  near.join();
+  if (far_err) std::rethrow_exception(far_err);
+  if (near_err) std::rethrow_exception(near_err);
   H.box_centers = t.centers;
   H.host_plan_s = now() - t1;
 }
