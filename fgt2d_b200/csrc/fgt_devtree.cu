@@ -691,6 +691,16 @@ struct StagedBatch {
     memcpy(base + off, src, b);
     return cudaMemcpyAsync(dev, base + off, b, cudaMemcpyHostToDevice, st);
   }
+  // the same once `ev` (recorded after the downloads) has completed, while
+  // the stream goes on with later work
+  cudaError_t finish_at(cudaEvent_t ev) {
+    cudaError_t e = cudaEventSynchronize(ev);
+    if (e != cudaSuccess) return e;
+#pragma omp parallel for schedule(dynamic, 1) if (used > (2u << 20))
+    for (long long i = 0; i < (long long)outs.size(); i++) memcpy(outs[i].dst, base + outs[i].off, outs[i].bytes);
+    outs.clear();
+    return cudaSuccess;
+  }
   cudaError_t finish() {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
@@ -1137,6 +1147,16 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   StagedBatch Xr(st, staged_bytes({sizeof(int) * (size_t)nb, sizeof(int) * (size_t)nb}));
   CKD(Xr.down(t.s0.data(), r0, nb));
   CKD(Xr.down(t.s1.data(), r1, nb));
+  // the host needs the ranges next; the point order (below) is read only by
+  // the device plan, later on the same stream
+  struct Ev {
+    cudaEvent_t e = nullptr;
+    ~Ev() {
+      if (e) cudaEventDestroy(e);
+    }
+  } ranges_done;
+  CKD(cudaEventCreateWithFlags(&ranges_done.e, cudaEventDisableTiming));
+  CKD(cudaEventRecord(ranges_done.e, st));
   // final order: leaf rank of each sorted position, to input order, stable sort
   {
     int *lstart = nullptr, *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
@@ -1156,7 +1176,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   }
   const double tD = now_s();
   if (same && nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
-  CKD(Xr.finish());
+  CKD(Xr.finish_at(ranges_done.e));
   if (same) {
     t.t0 = t.s0;
     t.t1 = t.s1;
@@ -1174,7 +1194,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(sort_points_device(t, d_trg, nt, nullptr, d_nchild, d_child, d_centers, d_rank, nleaf, leaf_of_rank,
                            d_itarg, t.t0, t.t1, st));
   }
-  CKD(cudaStreamSynchronize(st));
+  if (dbg) CKD(cudaStreamSynchronize(st));
   if (dbg)
     fprintf(stderr, "device tree (keys): refine %.4f (%d levels, %d boxes) lr %.4f ranks+sort_s %.4f sort_t %.4f\n",
             tB - tA, lev, nbr, tC - tB, tD - tC, now_s() - tD);
