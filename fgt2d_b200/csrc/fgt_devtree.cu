@@ -387,7 +387,7 @@ __global__ void k_ref_colleagues(const int* __restrict__ lev, int l, double lim,
         }
         for (int j = 0; j < nch; j++) {
           const unsigned ok = (pass1 & (unsigned)j) | (pass0 & ~(unsigned)j);
-          if ((ok & ((1u << dim) - 1)) == (1u << dim) - 1) coll[(size_t)b * nco + cnt++] = ch[j];
+          if ((ok & ((1u << dim) - 1)) == (1u << dim) - 1 && cnt < nco) coll[(size_t)b * nco + cnt++] = ch[j];
         }
         continue;
       }
@@ -397,7 +397,7 @@ __global__ void k_ref_colleagues(const int* __restrict__ lev, int l, double lim,
         bool ok = true;
         for (int d = 0; d < dim; d++)
           if (!(fabs(cen[(size_t)kb * dim + d] - cb[d]) <= lim)) ok = false;
-        if (ok) coll[(size_t)b * nco + cnt++] = kb;
+        if (ok && cnt < nco) coll[(size_t)b * nco + cnt++] = kb;
       }
     }
     for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(1024) k_lr_scan(LrRanges R, const int* __restr
 __global__ void k_lr_children(LrRanges R, const int* __restrict__ pos, int base, int nch, int dim,
                               const double* __restrict__ hsz, int* __restrict__ level, int* __restrict__ par,
                               int* __restrict__ nchild, int* __restrict__ child, double* __restrict__ cen,
-                              int* __restrict__ flag) {
+                              int* __restrict__ flag, int cap, int* __restrict__ err) {
   const int n = lr_count(R);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * nch;
        t += (long long)gridDim.x * blockDim.x) {
@@ -532,6 +532,10 @@ __global__ void k_lr_children(LrRanges R, const int* __restrict__ pos, int base,
     const int f = flag[box];
     if (f <= 0) continue;
     const int c = base + nch * pos[i] + j;
+    if (c < base || c >= cap) {  // a rank out of the counted range: recorded, not written
+      atomicExch(err, 1);
+      continue;
+    }
     const int l = level[box];
     if (j == 0) nchild[box] = nch;
     child[(size_t)box * nch + j] = c;
@@ -558,7 +562,7 @@ __global__ void k_lr_colleagues(LrRanges R, double lim, int nch, int nco, int di
       const int jb = coll[(size_t)dad * nco + q];
       for (int j = 0; j < nch; j++) {
         const int kb = child[(size_t)jb * nch + j];
-        if (kb >= 0 && lr_touch(cen, dim, kb, b, lim)) coll[(size_t)b * nco + cnt++] = kb;
+        if (kb >= 0 && cnt < nco && lr_touch(cen, dim, kb, b, lim)) coll[(size_t)b * nco + cnt++] = kb;
       }
     }
     for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
@@ -923,7 +927,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     return cudaSuccess;
   };
   auto lr_copy = [&](LrA& X, const int* par_, const int* nch_, const int* child_, const int* level_,
-                     const int* ncoll_, const int* coll_, const int* flag_, const double* cen_, size_t n) -> cudaError_t {
+                     const int* ncoll_, const int* coll_, const int* flag_, const double* cen_, size_t n,
+                     const int* pos_ = nullptr) -> cudaError_t {
     auto cp = [&](void* d, const void* s_, size_t b) {
       return b ? cudaMemcpyAsync(d, s_, b, cudaMemcpyDeviceToDevice, st) : cudaSuccess;
     };
@@ -934,6 +939,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(cp(X.ncoll, ncoll_, 4 * n));
     CKD(cp(X.coll, coll_, 4 * n * nco));
     if (flag_) CKD(cp(X.flag, flag_, 4 * n));
+    if (pos_) CKD(cp(X.pos, pos_, 4 * n));
     CKD(cp(X.cen, cen_, 8 * n * dim));
     return cudaSuccess;
   };
@@ -941,7 +947,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     if (need <= A.cap) return cudaSuccess;
     LrA B;
     CKD(lr_alloc(B, std::max(need, 2 * A.cap)));
-    CKD(lr_copy(B, A.par, A.nch, A.child, A.level, A.ncoll, A.coll, A.flag, A.cen, nbc));
+    // the ranks of the scan that precedes every growth are copied too
+    CKD(lr_copy(B, A.par, A.nch, A.child, A.level, A.ncoll, A.coll, A.flag, A.cen, nbc, A.pos));
     A = B;
     return cudaSuccess;
   };
@@ -962,6 +969,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   int* d_tot = nullptr;
   double *d_dist1 = nullptr, *d_hsz = nullptr;
   CKD(S.get(&d_tot, 64));
+  CKD(cudaMemsetAsync(d_tot, 0, 64 * sizeof(int), st));
   CKD(S.get(&d_dist1, lev + 3));
   CKD(S.get(&d_hsz, lev + 3));
   auto grid_for = [](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 1184)); };
@@ -1003,7 +1011,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
       if (total > 0) {
         CKD(lr_grow((size_t)nbc + (size_t)nch * total));
         k_lr_children<<<grid_for((long long)lr_count(R) * nch), 256, 0, st>>>(R, A.pos, nbc, nch, dim, d_hsz, A.level,
-                                                                             A.par, A.nch, A.child, A.cen, A.flag);
+                                                                             A.par, A.nch, A.child, A.cen, A.flag,
+                                                                             nbc + nch * total, d_tot + 60);
         for (int l = 1; l <= lev - 2; l++) {
           RL[l + 1].a[1] = nbc + nch * at[l];
           RL[l + 1].b[1] = nbc + nch * at[l + 1] - 1;
@@ -1029,7 +1038,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
       CKD(lr_grow((size_t)nbc + (size_t)nch * total));
       k_lr_children<<<grid_for((long long)lr_count(RL[l]) * nch), 256, 0, st>>>(RL[l], A.pos, nbc, nch, dim, d_hsz,
                                                                                A.level, A.par, A.nch, A.child, A.cen,
-                                                                               A.flag);
+                                                                               A.flag, nbc + nch * total, d_tot + 60);
       RL[l + 1].a[2] = nbc;
       RL[l + 1].b[2] = nbc + nch * total - 1;
       LrRanges Rn;
@@ -1042,6 +1051,12 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     }
   }
   CKD(cudaGetLastError());
+  {
+    int lr_err = 0;
+    CKD(cudaMemcpyAsync(&lr_err, d_tot + 60, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CKD(cudaStreamSynchronize(st));
+    if (lr_err) return cudaErrorLaunchFailure;
+  }
   // final numbering: per level the original boxes, then each pass's
   std::vector<int> tab, nlevb(lev + 1, 0);
   {
