@@ -12,9 +12,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
-#include <exception>
 #include <memory>
-#include <thread>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -517,30 +515,12 @@ static void finish_plan(HostPlan& H) {
   double t1 = now();
   H.host_lists_s = t1 - t0;
   if (!P.all_direct) build_tables(H);
-  // the near-field tasks (list1 side) and the far-field tasks (slots, form,
-  // shifts, evaluation) read the tree and lists and write disjoint fields of
-  // H: built concurrently
-  std::exception_ptr near_err;
-  std::thread near([&H, &near_err] {
-    try {
-      const double a = now();
-      build_near_tasks(H);
-      if (getenv("FGT_TREE_TIMING"))
-        fprintf(stderr, "near-field tasks: %.4f (dir %zu ranges %zu)\n", now() - a, H.dir.size(), H.dir_src.size());
-    } catch (...) {
-      near_err = std::current_exception();
-    }
-  });
-  std::exception_ptr far_err;
-  try {
-    if (P.scheme == 1) build_tasks_nufft(H);
-    else build_tasks(H);
-  } catch (...) {
-    far_err = std::current_exception();
-  }
-  near.join();
-  if (far_err) std::rethrow_exception(far_err);
-  if (near_err) std::rethrow_exception(near_err);
+  if (P.scheme == 1) build_tasks_nufft(H);
+  else build_tasks(H);
+  const double tn = now();
+  build_near_tasks(H);
+  if (getenv("FGT_TREE_TIMING"))
+    fprintf(stderr, "near-field tasks: %.4f (dir %zu ranges %zu)\n", now() - tn, H.dir.size(), H.dir_src.size());
   H.box_centers = t.centers;
   H.host_plan_s = now() - t1;
 }
