@@ -239,6 +239,11 @@ static void build_tasks(HostPlan& H) {
   H.split_end.assign(P.nlevels + 1, 0);
   H.form_sources = H.eval_points = 0;
   if (!P.all_direct) {
+    // capacities from the box count (untouched until filled)
+    H.form.reserve(nb);
+    H.merge.reserve(nb);
+    H.split.reserve(nb);
+    H.eval.reserve((size_t)nb + (size_t)(P.ns + P.nt) / 2048 + 16);
     for (int l = nls; l <= P.nlevels; l++)
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
         bool leaf = t.nchild[b] == 0;
