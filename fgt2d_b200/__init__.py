@@ -98,6 +98,7 @@ def lib():
     L.fgt_ctx_set_tree.argtypes = [_vp, i]
     L.fgt_ctx_set_sm_budget.argtypes = [_vp, i]
     L.fgt_ctx_set_scheme.argtypes = [_vp, i]
+    L.fgt_plan_expansion.argtypes = [_vp, i, i, ctypes.POINTER(ctypes.c_double)]
     L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
     L.fgt_server_set_precision.argtypes = [_vp, i]
     L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
@@ -342,6 +343,19 @@ class Plan:
                                                 _p(o["gradtarg"]), _p(o["hesstarg"])),
                "fgt_plan_execute_host_full")
         return o
+
+    def expansion(self, which, box):
+        """The box's multipole ("mp") or local ("loc") plane-wave expansion
+        after the last execute, complex (nd, nexp) in the reference's layout;
+        None when the plan holds no such expansion for the box."""
+        inf = self.info()
+        out = np.zeros(2 * self.nd * inf["nexp"])
+        st = lib().fgt_plan_expansion(self._h, {"mp": 0, "loc": 1}[which], int(box),
+                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if st == 1:
+            return None
+        _check(st, "fgt_plan_expansion")
+        return (out[0::2] + 1j * out[1::2]).reshape(self.nd, inf["nexp"])
 
     def info(self):
         inf = PlanInfo()

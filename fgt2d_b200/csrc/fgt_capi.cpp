@@ -951,6 +951,22 @@ int fgt_plan_profile_device(fgt_plan* p, const double* s, const double* q, const
   return FGT_OK;
 }
 
+int fgt_plan_expansion(fgt_plan* p, int which, int box, double* out) {
+  if (!p || !out || (which != 0 && which != 1)) return FGT_ERR_BADARG;
+  if (!p->have_device) return FGT_ERR_UNSUPPORTED;  // large-delta and all-direct plans hold none
+  const HostPlan& H = p->H;
+  if (box < 0 || box >= H.tree.nboxes) return FGT_ERR_BADARG;
+  const std::vector<int>& slots = which == 0 ? H.mp_slot : H.loc_slot;
+  if ((int)slots.size() <= box || slots[box] < 0) return FGT_ERR_BADARG;
+  const double2* pool = which == 0 ? p->D.mp : p->D.loc;
+  const size_t per = (size_t)H.P.nd * H.P.nexp;
+  CKS(cudaSetDevice(p->ctx->device));
+  if (p->done) CKS(cudaEventSynchronize(p->done));
+  CKS(cudaMemcpyAsync(out, pool + (size_t)slots[box] * per, per * 16, cudaMemcpyDeviceToHost, p->ctx->stream));
+  CKS(cudaStreamSynchronize(p->ctx->stream));
+  return FGT_OK;
+}
+
 int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
   if (!p || !o) return FGT_ERR_BADARG;
   memset(o, 0, sizeof(*o));

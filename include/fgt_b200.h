@@ -235,6 +235,16 @@ int fgt_plan_execute_device_full(fgt_plan* plan, const double* d_charge, const d
 int fgt_plan_profile_device(fgt_plan* plan, const double* d_sources, const double* d_charge,
                             const double* d_targ, double* d_pot, double* d_pottarg, float* ms8);
 int fgt_plan_get_info(const fgt_plan* plan, fgt_plan_info* info);
+/* The plane-wave expansion of one box after the last execute (which = 0:
+ * its multipole expansion, formed or merged; 1: its local expansion at the
+ * cut level after mp -> loc, or below it after the split), copied into
+ * out[2 * nd * nexp] (complex, re/im interleaved) in the reference's layout
+ * (2D pw(npw/2, npw, nd), 3D pw(npw, npw, npw/2, nd) with its node
+ * orders, fgt2d.f:1518-1610 / fgt3d.f).  box is 0-based in the tree's
+ * numbering (the reference's box - 1).  FGT_ERR_BADARG when the box holds
+ * no such expansion (this library allocates them only where the transform
+ * reads them).  For checking intermediate stages against the reference. */
+int fgt_plan_expansion(fgt_plan* plan, int which, int box, double* out);
 /* One execute with CUDA events around the plan's dominant tensor-core launch
  * (the Hermite-block MMA kernel of the form order group with the most
  * sources) on the context's stream: its device time (ms), the flops it

@@ -1463,6 +1463,17 @@ struct Result {
   long long nleaf_direct = 0;
 };
 
+// Expansions of chosen boxes (0-based ids) copied out after the shifts of
+// the plane-wave scheme (multipole after merge, local after split), for the
+// intermediate-stage comparison with the product.
+struct Probe {
+  int nbox = 0;
+  const int* boxes = nullptr;
+  cplx* mp = nullptr;  // [nbox][nd * nexp]
+  cplx* lo = nullptr;
+  int* has = nullptr;  // [nbox]: 1 when the box has expansions (levels >= the cut)
+};
+
 // fgt2d (fgt2d.f:19-462) + fgt2dmain (fgt2d.f:468-1348) and the 3D twins
 // (fgt3d.f:19-477, 483-1527).  Output arrays are overwritten.
 //
@@ -1479,7 +1490,7 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
             const double* charge, int ifdipole, const double* rnormal, const double* dipstr,
             int ifpgh, double* pot, double* grad, double* hess,
             int nt, const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
-            double* hesstarg, Result* res, int nufft = 0) {
+            double* hesstarg, Result* res, int nufft = 0, Probe* probe = nullptr) {
   const int NCH = Tree<D>::NCH;
   const int NH = D == 2 ? 3 : 6;
   if (nd < 1 || !(delta > 0) || !(eps > 0) || ns < 0 || nt < 0) return ORC_BADARG;
@@ -1870,6 +1881,15 @@ int fgt_run(int nd, double delta, double eps, int ns, const double* sources, int
         }
       }
     }
+    if (probe)
+      for (int i = 0; i < probe->nbox; i++) {
+        const int b = probe->boxes[i] + 1;
+        const bool ok = b >= 1 && b <= nboxes && iaddr[2 * b] >= 0;
+        probe->has[i] = ok;
+        if (!ok) continue;
+        std::copy(MP(b), MP(b) + (size_t)nd * nexp, probe->mp + (size_t)i * nd * nexp);
+        std::copy(LO(b), LO(b) + (size_t)nd * nexp, probe->lo + (size_t)i * nd * nexp);
+      }
     // step 5: evaluate (fgt2d.f:1141-1271 / fgt3d.f:1283-1446)
     for (int ilev = nlevstart; ilev <= nlevels; ilev++) {
       int p = nlocal[ilev], P = p + 1;
@@ -2075,6 +2095,33 @@ int orc_fgt_full(int dim, int nd, double delta, double eps, int ns, const double
     info[4] = r.nlmax; info[5] = (int)r.nleaf_direct; info[6] = 0; info[7] = 0;
   }
   return rc;
+}
+
+// The plane-wave scheme's expansions of chosen boxes (0-based ids): mp and
+// lo receive nd * nexp complex values (re, im) per box after the shifts,
+// has[i] = 1 where the box carries expansions (levels >= the cut).
+int orc_fgt_expansions(int dim, int nd, double delta, double eps, int ns, const double* sources,
+                       const double* charge, int nt, const double* targ, int ifpgh, int ifpghtarg, int nbox,
+                       const int* boxes, double* mp, double* lo, int* has, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  Probe pr;
+  pr.nbox = nbox;
+  pr.boxes = boxes;
+  pr.mp = reinterpret_cast<cplx*>(mp);
+  pr.lo = reinterpret_cast<cplx*>(lo);
+  pr.has = has;
+  for (int i = 0; i < nbox; i++) has[i] = 0;
+  const int NH = dim == 2 ? 3 : 6;
+  std::vector<double> pot((size_t)nd * std::max(ns, 1)), pt((size_t)nd * std::max(nt, 1));
+  std::vector<double> g((size_t)nd * dim * std::max(ns, 1)), h((size_t)nd * NH * std::max(ns, 1));
+  std::vector<double> gt((size_t)nd * dim * std::max(nt, 1)), ht((size_t)nd * NH * std::max(nt, 1));
+  Result r;
+  return dim == 2 ? fgt_run<2>(nd, delta, eps, ns, sources, 1, charge, 0, nullptr, nullptr, ifpgh, pot.data(),
+                               g.data(), h.data(), nt, targ, ifpghtarg, pt.data(), gt.data(), ht.data(), &r, 0, &pr)
+                  : fgt_run<3>(nd, delta, eps, ns, sources, 1, charge, 0, nullptr, nullptr, ifpgh, pot.data(),
+                               g.data(), h.data(), nt, targ, ifpghtarg, pt.data(), gt.data(), ht.data(), &r, 0, &pr);
 }
 
 // The NUFFT scheme (2d/nufft, 3d/nufft; see fgt_run) with the full argument

@@ -56,6 +56,10 @@ def lib():
                                    ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp,
                                    ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                    _dp, _dp, _dp, _ip, ctypes.c_int]
+        L.orc_fgt_expansions.restype = ctypes.c_int
+        L.orc_fgt_expansions.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _ip, ctypes.c_int]
         L.orc_fgt_nufft.restype = ctypes.c_int
         L.orc_fgt_nufft.argtypes = L.orc_fgt_full.argtypes
         L.orc_direct_cut.restype = None
@@ -192,6 +196,26 @@ def fgt_full(dim, nd, delta, eps, sources, charge=None, targ=None, ifpgh=1, ifpg
             "gradtarg": gt[:nt] if ifpghtarg >= 2 else None,
             "hesstarg": ht[:nt] if ifpghtarg >= 3 else None,
             "info": {k: int(info[i]) for i, k in enumerate(keys)}}
+
+
+def expansions(dim, nd, delta, eps, sources, charge, targ, ifpgh, ifpghtarg, boxes, nexp, nthreads=0):
+    """The restated transform's plane-wave expansions of ``boxes`` (0-based)
+    after the shifts: (mp, loc, has) with mp/loc complex (nbox, nd, nexp)."""
+    src = _f64(sources)
+    ns = src.shape[0]
+    q = _f64(charge).reshape(ns, nd)
+    trg = _f64(targ) if targ is not None else np.zeros((0, dim))
+    bx = np.ascontiguousarray(boxes, dtype=np.int32)
+    mp = np.zeros(2 * len(bx) * nd * nexp)
+    lo = np.zeros(2 * len(bx) * nd * nexp)
+    has = np.zeros(len(bx), dtype=np.int32)
+    rc = lib().orc_fgt_expansions(dim, nd, float(delta), float(eps), ns, _d(src), _d(q), trg.shape[0], _d(trg),
+                                  ifpgh, ifpghtarg, len(bx), bx.ctypes.data_as(_ip), _d(mp), _d(lo),
+                                  has.ctypes.data_as(_ip), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle expansions returned status {rc}")
+    c = lambda a: (a[0::2] + 1j * a[1::2]).reshape(len(bx), nd, nexp)
+    return c(mp), c(lo), has.astype(bool)
 
 
 def direct_full(dim, nd, delta, sources, targ, charge=None, rnormal=None, dipstr=None, pgh=3,
