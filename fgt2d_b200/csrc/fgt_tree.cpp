@@ -588,9 +588,7 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
   for (lev = 0; lev <= nlmax - 1; lev++) {
     const int a = t.lfirst[lev], b = t.llast[lev];
     const int thr = lev < levcut ? ndiv0 : ndiv;
-    const double tr0 = T();
     if (tree_refine_level(t, lev, thr, count, firstchild) == 0) break;
-    if (dbg) fprintf(stderr, "refine_level %d: %.5f nb %d\n", lev, T() - tr0, t.nboxes);
     count.resize(t.nboxes, 0);
     const int* fc = firstchild.data();
     const int c0 = t.lfirst[lev + 1], nnew = t.nboxes - c0;
