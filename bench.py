@@ -338,7 +338,7 @@ def ours_arm(args, w, rank, world, local_rank):
 
     # plan (tree + lists + device tasks), built once; the context's precision
     # selects the form at each execute
-    ctx = F.Context(dev, precision="mixed")
+    ctx = F.Context(dev, precision="mixed", scheme=args.scheme)
     t0 = time.perf_counter()
     plan = F.Plan(ctx, dim, nd, w["delta"], w["eps"], w["src"], w["trg"], w["ifpgh"],
                   w["ifpghtarg"])
@@ -511,7 +511,7 @@ def ours_arm(args, w, rank, world, local_rank):
         plan.close()
         del d_src, d_chg, d_trg, d_pot, d_pt
         torch.cuda.empty_cache()
-        secondary = secondary_workload("cfg3", dev, max(3, min(args.steps, 5)), 3)
+        secondary = secondary_workload("cfg3", dev, max(3, min(args.steps, 5)), 3, args.scheme)
     ms_mixed, ms_fp64 = results["mixed"], results["fp64"]
     line = {
         "metric": METRIC,
@@ -541,12 +541,13 @@ def ours_arm(args, w, rank, world, local_rank):
         "cpu_baseline": cpu_base,
         "clocks": clocks,
         "secondary": secondary,
+        "scheme": args.scheme,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def secondary_workload(name, dev, steps, warmup):
+def secondary_workload(name, dev, steps, warmup, scheme="planewave"):
     """Device time of both forms on a second workload (the 3D blobs case by
     default) with inputs in HBM, per-stage times and the error of the timed
     outputs against the FP64 direct sum at 1e4 sampled points: reported
@@ -555,7 +556,7 @@ def secondary_workload(name, dev, steps, warmup):
     import fgt2d_b200 as F
     w = make_workload(name, 1234 + 2)
     nd = w["nd"]
-    ctx = F.Context(dev, precision="mixed")
+    ctx = F.Context(dev, precision="mixed", scheme=scheme)
     plan = F.Plan(ctx, w["dim"], nd, w["delta"], w["eps"], w["src"], w["trg"], w["ifpgh"], w["ifpghtarg"])
     d_src = torch.from_numpy(np.ascontiguousarray(w["src"])).to(f"cuda:{dev}")
     d_chg = torch.from_numpy(np.ascontiguousarray(w["chg"]).reshape(-1, nd)).to(f"cuda:{dev}")
@@ -687,6 +688,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-errors", action="store_true", help="skip the sampled direct-sum errors")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 3D blobs line beside the headline")
+    ap.add_argument("--scheme", default="planewave", choices=["planewave", "nufft"],
+                    help="algorithm of the timed plans: the plane-wave scheme (default) or the NUFFT scheme")
     ap.add_argument("--requests", type=int, default=4096, help="serving workload: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: arrivals per second")
     ap.add_argument("--workers", type=int, default=8, help="serving workload: server worker streams")
