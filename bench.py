@@ -622,7 +622,8 @@ def serving_arm(args):
     nmax = int(ns.max())
     base = {2: rng.random((nmax, 2)), 3: rng.random((nmax, 3))}
     chg = rng.random(nmax)
-    srv = F.Server(0, max_bytes=args.server_bytes, workers=args.workers, precision="auto")
+    srv = F.Server(0, max_bytes=args.server_bytes, workers=args.workers, precision="auto",
+                   sm_budget=args.server_sm_budget)
     # warm-up: one small request of each dimension (module load, first launches)
     for d in (2, 3):
         srv.wait(srv.submit(d, 1, 1e-3, 1e-6, base[d][:2000], chg[:2000]))
@@ -667,7 +668,8 @@ def serving_arm(args):
         "failures": [[int(k), int(status[k]), int(dims[k]), int(ns[k]), float(deltas[k]), float(epss[k])]
                      for k in np.flatnonzero(~ok)[:8]],
         "points_per_s": pts / span, "span_s": span,
-        "arrival_rate_per_s": rate, "workers": args.workers, "peak_device_bytes": st["peak_bytes"],
+        "arrival_rate_per_s": rate, "workers": args.workers, "sm_budget": args.server_sm_budget,
+        "peak_device_bytes": st["peak_bytes"],
         "budget_device_bytes": st["budget_bytes"], "data": "synthetic (seeded numpy)",
         "config": {"workload": "serving stream: Poisson arrivals, dim in {2,3}, N log-uniform [1e3,1e6] "
                                "(sources = targets, uniform), charges U[0,1), delta log-uniform [1e-6,1e-1], "
@@ -694,6 +696,8 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: arrivals per second")
     ap.add_argument("--workers", type=int, default=8, help="serving workload: server worker streams")
     ap.add_argument("--server-bytes", type=int, default=0, help="serving workload: device budget (0: 80%% free)")
+    ap.add_argument("--server-sm-budget", type=int, default=0,
+                    help="serving workload: SMs a request's persistent kernels use (0: all)")
     args = ap.parse_args()
     if args.workload == "serving":
         return serving_arm(args)

@@ -101,6 +101,7 @@ def lib():
     L.fgt_plan_expansion.argtypes = [_vp, i, i, ctypes.POINTER(ctypes.c_double)]
     L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
     L.fgt_server_set_precision.argtypes = [_vp, i]
+    L.fgt_server_set_sm_budget.argtypes = [_vp, i]
     L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
     L.fgt_server_wait.argtypes = [_vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]
     L.fgt_server_stats_get.argtypes = [_vp, ctypes.POINTER(ServerStats)]
@@ -484,7 +485,7 @@ class Server:
     """Transform server on one device (continuous batching of independent
     requests over worker streams, admission by device-memory footprint)."""
 
-    def __init__(self, device=0, max_bytes=0, workers=4, precision="auto"):
+    def __init__(self, device=0, max_bytes=0, workers=4, precision="auto", sm_budget=0):
         L = lib()
         h = _vp()
         _check(L.fgt_server_create(int(device), int(max_bytes), int(workers), ctypes.byref(h)),
@@ -492,6 +493,7 @@ class Server:
         self._h = h
         p = _PREC[precision] if isinstance(precision, str) else int(precision)
         _check(L.fgt_server_set_precision(h, p), "fgt_server_set_precision")
+        _check(L.fgt_server_set_sm_budget(h, int(sm_budget)), "fgt_server_set_sm_budget")
         self._live = {}
 
     def submit(self, dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0,

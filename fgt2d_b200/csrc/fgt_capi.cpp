@@ -1564,13 +1564,6 @@ int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_
     S->ctxs.push_back(c);
   }
   {
-    // a request's persistent kernels use at most half of the SMs, so that
-    // the requests arriving meanwhile find SMs free at once
-    int sms = 148;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess)
-      for (fgt_ctx* c : S->ctxs) c->sm_budget = std::max(1, sms / 2);
-  }
-  {
     // reserve the budget in the device's stream-ordered pool once (it keeps
     // freed memory), so that a request's plan is carved from memory the pool
     // already holds instead of growing it (mapping tens of GB) inside the
@@ -1609,6 +1602,15 @@ int fgt_server_set_precision(fgt_server* s, int precision) {
   if (!s) return FGT_ERR_BADARG;
   for (fgt_ctx* c : s->ctxs) {
     int st = fgt_ctx_set_precision(c, precision);
+    if (st != FGT_OK) return st;
+  }
+  return FGT_OK;
+}
+
+int fgt_server_set_sm_budget(fgt_server* s, int sms) {
+  if (!s || sms < 0) return FGT_ERR_BADARG;
+  for (fgt_ctx* c : s->ctxs) {
+    int st = fgt_ctx_set_sm_budget(c, sms);
     if (st != FGT_OK) return st;
   }
   return FGT_OK;

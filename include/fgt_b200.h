@@ -99,9 +99,9 @@ int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
  * whose tree is built on the host (pts_tree_build, pts_tree2d4.f:363-590). */
 int fgt_ctx_set_tree(fgt_ctx* ctx, int where);
 /* how many SMs the persistent kernels of the context's plans (created after
- * the call) size their grids for; 0 (the default) uses every SM.  The
- * transform server uses half, so that requests arriving while a large one
- * runs find SMs free.  No counterpart in the reference. */
+ * the call) size their grids for; 0 (the default) uses every SM.  A smaller
+ * budget leaves SMs free for work that arrives while a large transform runs
+ * (fgt_server_set_sm_budget).  No counterpart in the reference. */
 int fgt_ctx_set_sm_budget(fgt_ctx* ctx, int sms);
 /* the algorithm of the plans created after the call (FGT_SCHEME_*): the
  * reference selects it by building 2d/planewave or 2d/nufft (3D likewise),
@@ -363,6 +363,9 @@ typedef struct fgt_server_stats {
 } fgt_server_stats;
 int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_server** out);
 int fgt_server_set_precision(fgt_server* server, int precision);
+/* SMs the persistent kernels of the requests planned afterwards size their
+ * grids for (0, the default: every SM); see fgt_ctx_set_sm_budget. */
+int fgt_server_set_sm_budget(fgt_server* server, int sms);
 int fgt_server_submit(fgt_server* server, const fgt_request* request, long long* id);
 /* blocks until request id completes; returns its status (and frees its id) */
 int fgt_server_wait(fgt_server* server, long long id, double* latency_s);
