@@ -97,6 +97,8 @@ static void build_near_tasks(HostPlan& H) {
   const int nb = t.nboxes, npl = P.npwlevel;
   H.dir.clear();
   H.dir_src.clear();
+  double tn[6];
+  tn[0] = now();
   // box A -> source boxes S with A in list1(S), as CSR in the order of S
   // (a transpose of the list1 CSR: the S range is cut into one chunk per
   // thread, each thread counts and then places its entries through its own
@@ -160,6 +162,7 @@ static void build_near_tasks(HostPlan& H) {
   const int CH = 32;  // one warp per task
   const bool sets[2] = {P.ifpgh >= 1, P.ifpghtarg >= 1};
   // ranges and sources summed down the ancestor chains, level by level
+  tn[1] = now();
   std::vector<long long> cum_ns(nb, 0);
   std::vector<int> cum_r(nb, 0);
   for (int l = 0; l <= P.nlevels; l++) {
@@ -173,6 +176,7 @@ static void build_near_tasks(HostPlan& H) {
       cum_ns[b] = ns_ + (a >= 0 ? cum_ns[a] : 0);
     }
   }
+  tn[2] = now();
   std::vector<int> nr(nb, 0);
   std::vector<long long> roff(nb + 1, 0), toff(nb + 1, 0);
 #pragma omp parallel for schedule(static)
@@ -197,6 +201,7 @@ static void build_near_tasks(HostPlan& H) {
   H.dir_src.resize(roff[nb]);
   H.dir.resize(toff[nb]);
   long long pairs = 0;
+  tn[3] = now();
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs)
   for (int b = 0; b < nb; b++) {
     if (nr[b] == 0) continue;
@@ -213,6 +218,9 @@ static void build_near_tasks(HostPlan& H) {
     }
   }
   H.direct_pairs = pairs;
+  if (getenv("FGT_TREE_TIMING"))
+    fprintf(stderr, "near-field parts: csr %.4f cum %.4f offsets %.4f fill %.4f\n", tn[1] - tn[0], tn[2] - tn[1],
+            tn[3] - tn[2], now() - tn[3]);
 }
 
 // Flattens the tree into the stage task arrays.
