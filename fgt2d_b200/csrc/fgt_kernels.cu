@@ -3236,16 +3236,16 @@ __global__ void __launch_bounds__(128) k_probe_dmma(double* out, int iters) {
 }
 
 // ------------------------------------------------------------ host helpers
-template <typename T>
-cudaError_t put(char*& cur, T*& dst, const std::vector<T>& v, cudaStream_t s) {
+template <typename T, typename A>
+cudaError_t put(char*& cur, T*& dst, const std::vector<T, A>& v, cudaStream_t s) {
   dst = reinterpret_cast<T*>(cur);
   size_t b = (v.size() * sizeof(T) + 255) & ~size_t(255);
   cur += b;
   if (v.empty()) return cudaSuccess;
   return cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
-template <typename T>
-size_t bytes_of(const std::vector<T>& v) {
+template <typename T, typename A>
+size_t bytes_of(const std::vector<T, A>& v) {
   return (v.size() * sizeof(T) + 255) & ~size_t(255);
 }
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
@@ -3262,8 +3262,8 @@ struct Staged {
   };
   std::vector<Item> items;
   size_t span = 0;
-  template <typename T>
-  void add(char*& cur, T*& dst, const std::vector<T>& v) {
+  template <typename T, typename A>
+  void add(char*& cur, T*& dst, const std::vector<T, A>& v) {
     dst = reinterpret_cast<T*>(cur);
     const size_t b = v.size() * sizeof(T);
     if (b) items.push_back({span, b, v.data()});

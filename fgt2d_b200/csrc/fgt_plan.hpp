@@ -4,11 +4,16 @@
 #pragma once
 #include <cstdint>
 #include <cstddef>
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "fgt_tree.hpp"
 
 namespace fgtb {
+
 
 enum Route { ROUTE_HERMITE = 0, ROUTE_PW = 1, ROUTE_TAYLOR = 0 };
 
@@ -80,7 +85,7 @@ struct HostPlan {
   int nms = 1;
   int nmp = 0, nloc = 0;
   std::vector<int> mp_slot, loc_slot;  // per box, -1 when absent
-  std::vector<double> box_centers;     // dim per box
+  uvector<double> box_centers;         // dim per box
   // tasks
   std::vector<FormTask> form;
   // merge / split tasks of parents at level l: [beg[l], end[l])
@@ -91,8 +96,8 @@ struct HostPlan {
   std::vector<M2LTask> m2l;
   std::vector<M2LNbr> m2l_nbr;
   std::vector<EvalTask> eval;
-  std::vector<DirTask> dir;
-  std::vector<SrcRange> dir_src;
+  uvector<DirTask> dir;
+  uvector<SrcRange> dir_src;
   // statistics
   long long direct_pairs = 0;
   long long form_sources = 0, eval_points = 0;

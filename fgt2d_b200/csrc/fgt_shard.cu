@@ -197,8 +197,8 @@ int shard_filter(HostPlan& H, int nranks, int rank, ShardInfo& S) {
       ls[s].swap(a2);
       lb[s].swap(b2);
     }
-    std::vector<DirTask> d;
-    std::vector<SrcRange> r;
+    uvector<DirTask> d;
+    uvector<SrcRange> r;
     for (const DirTask& x : H.dir) {
       const int s = x.set ? 1 : 0;
       const auto it = std::upper_bound(ls[s].begin(), ls[s].end(), x.i0);

@@ -131,7 +131,7 @@ struct Builder {
   // sibling on the same side of d, so the test is made once per side and
   // dimension (child 0 and child 2^d) and a child passes when its sides do;
   // a box with a missing child takes the test child by child.
-  void colleagues_box(int b, double lim, std::vector<int>& nc, std::vector<int>& co) {
+  void colleagues_box(int b, double lim, uvector<int>& nc, uvector<int>& co) {
     int dad = t.parent[b];
     int n = 0;
     for (int i = 0; i < nc[dad]; i++) {
@@ -178,7 +178,7 @@ struct Builder {
   void colleagues_after_pass(int nold) {
     const int nb = t.nboxes;
     const std::vector<int>& map = last_map;
-    std::vector<int> nc(nb, 0), co((size_t)nb * NCO, -1);
+    uvector<int> nc(nb, 0), co((size_t)nb * NCO, -1);
     std::vector<char> fresh(nb, 1), mark(nb, 0), refd(nb, 0);
 #pragma omp parallel for schedule(static) if (nold > 16384)
     for (int o = 0; o < nold; o++) {

@@ -9,9 +9,35 @@
 // is box k+1 there.
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace fgtb {
+
+// Allocator whose resize leaves new elements default-initialised (no
+// zeroing), for arrays that are filled right after sizing (box arrays read
+// back from the device, task arrays).
+template <class T, class A = std::allocator<T>>
+struct default_init_allocator : A {
+  using A::A;
+  template <class U>
+  struct rebind {
+    using other = default_init_allocator<U, typename std::allocator_traits<A>::template rebind_alloc<U>>;
+  };
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... Args>
+  void construct(U* p, Args&&... args) {
+    std::allocator_traits<A>::construct(static_cast<A&>(*this), p, std::forward<Args>(args)...);
+  }
+};
+template <class T>
+using uvector = std::vector<T, default_init_allocator<T>>;
 
 struct Tree {
   int dim = 2, nch = 4, nco = 9;
@@ -19,10 +45,10 @@ struct Tree {
   int npwlevel = 0;
   double bs0 = 0, cen0[3] = {0, 0, 0};
   std::vector<int> lfirst, llast;          // boxes of level l: [lfirst[l], llast[l]]
-  std::vector<int> level, parent, nchild;  // per box
-  std::vector<int> child;                  // nch per box, -1 when absent
-  std::vector<int> ncoll, coll;            // colleagues (self included), nco per box
-  std::vector<double> centers;             // dim per box
+  uvector<int> level, parent, nchild;  // per box
+  uvector<int> child;                  // nch per box, -1 when absent
+  uvector<int> ncoll, coll;            // colleagues (self included), nco per box
+  uvector<double> centers;             // dim per box
   std::vector<double> boxsize;             // per level
   // sorted order: position -> original index (0-based)
   std::vector<int> isrc, itarg;
