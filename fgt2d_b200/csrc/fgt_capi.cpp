@@ -237,6 +237,9 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     ~Free() { cudaFreeAsync(q, st); }
   } fr{perms, s};
   int *d_isrc = perms, *d_itarg = perms + ns + 1;
+  // an unsharded plan builds its near-field task arrays on the GPU; a shard
+  // filters them on the host
+  p->H.defer_near = p->shard_n <= 1;
   try {
     CKS(build_plan_device(p->H, dim, nd, delta, eps, ns, p->d_src, nt, d_trg, same, ifpgh, ifpghtarg,
                           d_isrc, d_itarg, s, ifcharge, ifdipole));
@@ -258,6 +261,21 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   }
   if (same && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, p->d_src, (size_t)nt * dim * 8, cudaMemcpyDeviceToDevice, s));
   if (shard_filter(p->H, p->shard_n, p->shard_r, p->shard) != 0) return FGT_ERR_BADARG;
+  if (p->H.defer_near && p->H.tree.nboxes > 0) {
+    const double tn = now_s();
+    const cudaError_t e = build_near_tasks_device(p->H, s);
+    if (e != cudaSuccess) {
+      device_near_free(p->H, s);
+      return cuda_status(e);
+    }
+    p->H.host_plan_s += now_s() - tn;
+    if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "near-field tasks (device): %.4f\n", now_s() - tn);
+  }
+  struct NearFree {
+    HostPlan& h;
+    cudaStream_t st;
+    ~NearFree() { device_near_free(h, st); }  // copied into the plan's arena, or abandoned
+  } nf{p->H, s};
   if (admit) {
     size_t bytes = 0;
     DevicePlan probe;
@@ -975,7 +993,7 @@ int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
   o->npwlevel = P.npwlevel; o->nlevels = P.nlevels; o->nboxes = p->H.tree.nboxes;
   o->npw = P.npw; o->nexp = P.nexp; o->nlmax = P.nlmax;
   o->nform = (int)p->H.form.size(); o->neval = (int)p->H.eval.size();
-  o->ndirect_tasks = (int)p->H.dir.size(); o->nmp = p->H.nmp; o->nloc = p->H.nloc;
+  o->ndirect_tasks = p->have_device ? p->D.ndir : (int)p->H.dir.size(); o->nmp = p->H.nmp; o->nloc = p->H.nloc;
   o->direct_pairs = p->H.direct_pairs; o->form_sources = p->H.form_sources;
   o->eval_points = p->H.eval_points;
   o->device_bytes = (long long)(p->D.bytes + p->io_bytes);

@@ -192,6 +192,11 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
                               bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st);
 // Bounding box (per-dimension min / max) of device point arrays.
+// The near-field task arrays of a built host plan on the GPU (H.dnear,
+// H.direct_pairs), in the order of the host's build; device_near_free
+// releases them (after device_plan_create has copied them).
+cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st);
+void device_near_free(HostPlan& H, cudaStream_t st);
 cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim,
                                    double* mn, double* mx, cudaStream_t st);
 cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,

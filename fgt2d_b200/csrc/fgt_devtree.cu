@@ -30,6 +30,7 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "fgt_device.hpp"
 #include "fgt_plan.hpp"
@@ -607,6 +608,81 @@ __global__ void k_lr_scatter(int n, const int* __restrict__ map, int nch, int di
     }
     for (int d = 0; d < dim; d++) cen2[(size_t)f * dim + d] = cen[(size_t)b * dim + d];
   }
+}
+
+// ---- near-field task arrays on the device (the host's build_near_tasks) ----
+// (A, S) pairs of the list1 entries of the near-field source boxes S (levels
+// 0 .. the cut, ids 0 .. s_hi), in S-major order
+__global__ void k_near_count(int s_hi, const unsigned char* __restrict__ ifhung, const int* __restrict__ l1off,
+                             int* __restrict__ cnt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s <= s_hi) cnt[s] = ifhung[s] ? l1off[s + 1] - l1off[s] : 0;
+}
+__global__ void k_near_pairs(int s_hi, const unsigned char* __restrict__ ifhung, const int* __restrict__ l1off,
+                             const int* __restrict__ l1, const int* __restrict__ pfx, int* __restrict__ keyA,
+                             int* __restrict__ valS, int* __restrict__ cntA) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > s_hi || !ifhung[s]) return;
+  int q = pfx[s];
+  for (int k = l1off[s]; k < l1off[s + 1]; k++, q++) {
+    keyA[q] = l1[k];
+    valS[q] = s;
+    atomicAdd(cntA + l1[k], 1);
+  }
+}
+// sources and ranges summed down the ancestor chains, one level
+__global__ void k_near_cum(int a, int n, const int* __restrict__ parent, const int* __restrict__ ioff,
+                           const int* __restrict__ into, const int* __restrict__ s0, const int* __restrict__ s1,
+                           int* __restrict__ cum_r, long long* __restrict__ cum_ns) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = a + i, p = parent[b];
+  long long ns = 0;
+  for (int k = ioff[b]; k < ioff[b + 1]; k++) ns += s1[into[k]] - s0[into[k]];
+  cum_r[b] = ioff[b + 1] - ioff[b] + (p >= 0 ? cum_r[p] : 0);
+  cum_ns[b] = ns + (p >= 0 ? cum_ns[p] : 0);
+}
+// per leaf: its ranges (cum_r per evaluated set) and tasks (<= 32 points)
+__global__ void k_near_sizes(int nb, const int* __restrict__ nchild, const int* __restrict__ cum_r,
+                             const int* __restrict__ s0, const int* __restrict__ s1, const int* __restrict__ t0,
+                             const int* __restrict__ t1, int set0, int set1, long long* __restrict__ rcnt,
+                             long long* __restrict__ tcnt) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  long long r = 0, tk = 0;
+  if (nchild[b] == 0 && cum_r[b] > 0) {
+    const int n0 = s1[b] - s0[b], n1 = t1[b] - t0[b];
+    if (set0 && n0 > 0) { r += cum_r[b]; tk += (n0 + 31) / 32; }
+    if (set1 && n1 > 0) { r += cum_r[b]; tk += (n1 + 31) / 32; }
+  }
+  rcnt[b] = r;
+  tcnt[b] = tk;
+}
+__global__ void k_near_fill(int nb, const int* __restrict__ nchild, const int* __restrict__ parent,
+                            const int* __restrict__ cum_r, const long long* __restrict__ cum_ns,
+                            const int* __restrict__ ioff, const int* __restrict__ into, const int* __restrict__ s0,
+                            const int* __restrict__ s1, const int* __restrict__ t0, const int* __restrict__ t1,
+                            int set0, int set1, const long long* __restrict__ roff, const long long* __restrict__ toff,
+                            DirTask* __restrict__ dir, SrcRange* __restrict__ src,
+                            unsigned long long* __restrict__ pairs) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || nchild[b] != 0 || cum_r[b] == 0) return;
+  long long ro = roff[b], to = toff[b];
+  unsigned long long pr = 0;
+  for (int set = 0; set < 2; set++) {
+    const int n = set == 0 ? s1[b] - s0[b] : t1[b] - t0[b];
+    if (!(set == 0 ? set0 : set1) || n == 0) continue;
+    const int i0 = set == 0 ? s0[b] : t0[b];
+    const int off = (int)ro;
+    for (int a = b; a >= 0; a = parent[a])
+      for (int k = ioff[a]; k < ioff[a + 1]; k++) {
+        const int sb = into[k];
+        src[ro++] = SrcRange{s0[sb], s1[sb] - s0[sb]};
+      }
+    for (int c = 0; c < n; c += 32) dir[to++] = DirTask{set, i0 + c, min(32, n - c), off, cum_r[b]};
+    pr += (unsigned long long)cum_ns[b] * (unsigned long long)n;
+  }
+  if (pr) atomicAdd(pairs, pr);
 }
 
 // Device scratch of one build, stream-ordered on the build's stream (no
@@ -1349,6 +1425,154 @@ cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double
   H.host_tree_s = now_s() - tstart;
   plan_end(H);
   return cudaSuccess;
+}
+
+
+// The near-field task arrays of a built host plan on the GPU, in the order of
+// the host's build_near_tasks (fgt_plan.cpp): for every leaf, its source
+// ranges (the ifhung source boxes whose list1 holds the leaf or one of its
+// ancestors, leaf first, each box's sources in increasing box id) once per
+// evaluated point set, and its tasks of <= 32 points, leaves in box order.
+// The transpose of list1 is a stable radix sort of the (A, S) pairs by A.
+cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
+  const Params& P = H.P;
+  const Tree& t = H.tree;
+  const Lists& L = H.lists;
+  const int nb = t.nboxes, npl = P.npwlevel;
+  const int nlevend = npl < P.nlevels ? npl : P.nlevels;
+  const int s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;
+  const int set0 = P.ifpgh >= 1, set1 = P.ifpghtarg >= 1;
+  Scratch S(st);
+  const int ne = L.l1off.empty() ? 0 : L.l1off[nb];
+  int *d_l1off = nullptr, *d_l1 = nullptr, *d_par = nullptr, *d_nch = nullptr, *d_s0 = nullptr, *d_s1 = nullptr,
+      *d_t0 = nullptr, *d_t1 = nullptr;
+  unsigned char* d_hung = nullptr;
+  CKD(S.get(&d_l1off, nb + 1));
+  CKD(S.get(&d_l1, ne));
+  CKD(S.get(&d_par, nb));
+  CKD(S.get(&d_nch, nb));
+  CKD(S.get(&d_s0, nb));
+  CKD(S.get(&d_s1, nb));
+  CKD(S.get(&d_t0, nb));
+  CKD(S.get(&d_t1, nb));
+  CKD(S.get(&d_hung, nb));
+  {
+    const size_t i4 = sizeof(int) * (size_t)nb;
+    StagedBatch X(st, staged_bytes({i4 + 4, sizeof(int) * (size_t)ne, i4, i4, i4, i4, i4, i4, (size_t)nb}));
+    CKD(X.up(d_l1off, L.l1off.data(), (size_t)nb + 1));
+    CKD(X.up(d_l1, L.l1.data(), (size_t)ne));
+    CKD(X.up(d_par, t.parent.data(), nb));
+    CKD(X.up(d_nch, t.nchild.data(), nb));
+    CKD(X.up(d_s0, t.s0.data(), nb));
+    CKD(X.up(d_s1, t.s1.data(), nb));
+    CKD(X.up(d_t0, t.t0.data(), nb));
+    CKD(X.up(d_t1, t.t1.data(), nb));
+    CKD(X.up(d_hung, L.ifhung.data(), nb));
+    // the stage is reused below only after this batch's copies (finish)
+    CKD(X.finish());
+  }
+  // (A, S) pairs, stable sort by A: into[] = the S of each A in increasing id
+  int *d_cnt = nullptr, *d_pfx = nullptr, *d_keyA = nullptr, *d_valS = nullptr, *d_keyA2 = nullptr,
+      *d_into = nullptr, *d_cntA = nullptr, *d_ioff = nullptr;
+  const int nsrcbox = s_hi + 1;
+  CKD(S.get(&d_cnt, nsrcbox + 1));
+  CKD(S.get(&d_pfx, nsrcbox + 1));
+  CKD(S.get(&d_cntA, nb + 1));
+  CKD(S.get(&d_ioff, nb + 1));
+  CKD(cudaMemsetAsync(d_cntA, 0, sizeof(int) * (nb + 1), st));
+  int npairs = 0;
+  if (nsrcbox > 0) {
+    k_near_count<<<(nsrcbox + 255) / 256, 256, 0, st>>>(s_hi, d_hung, d_l1off, d_cnt);
+    CKD(cudaMemsetAsync(d_cnt + nsrcbox, 0, sizeof(int), st));
+    size_t tmp = 0;
+    CKD(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cnt, d_pfx, nsrcbox + 1, st));
+    char* dt = nullptr;
+    CKD(S.get(&dt, tmp));
+    CKD(cub::DeviceScan::ExclusiveSum(dt, tmp, d_cnt, d_pfx, nsrcbox + 1, st));
+    CKD(cudaMemcpyAsync(&npairs, d_pfx + nsrcbox, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CKD(cudaStreamSynchronize(st));
+  }
+  CKD(S.get(&d_keyA, npairs));
+  CKD(S.get(&d_valS, npairs));
+  CKD(S.get(&d_keyA2, npairs));
+  CKD(S.get(&d_into, npairs));
+  if (npairs > 0) {
+    k_near_pairs<<<(nsrcbox + 255) / 256, 256, 0, st>>>(s_hi, d_hung, d_l1off, d_l1, d_pfx, d_keyA, d_valS, d_cntA);
+    int bits = 1;
+    while ((1 << bits) < nb) bits++;
+    size_t tmp = 0;
+    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d_keyA, d_keyA2, d_valS, d_into, npairs, 0, bits, st));
+    char* dt = nullptr;
+    CKD(S.get(&dt, tmp));
+    CKD(cub::DeviceRadixSort::SortPairs(dt, tmp, d_keyA, d_keyA2, d_valS, d_into, npairs, 0, bits, st));
+  }
+  {
+    size_t tmp = 0;
+    CKD(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cntA, d_ioff, nb + 1, st));
+    char* dt = nullptr;
+    CKD(S.get(&dt, tmp));
+    CKD(cub::DeviceScan::ExclusiveSum(dt, tmp, d_cntA, d_ioff, nb + 1, st));
+  }
+  // sums down the ancestor chains, level by level
+  int* d_cumr = nullptr;
+  long long* d_cumns = nullptr;
+  CKD(S.get(&d_cumr, nb));
+  CKD(S.get(&d_cumns, nb));
+  for (int l = 0; l <= P.nlevels; l++) {
+    const int a = t.lfirst[l], n = t.llast[l] - a + 1;
+    if (n > 0)
+      k_near_cum<<<(n + 255) / 256, 256, 0, st>>>(a, n, d_par, d_ioff, d_into, d_s0, d_s1, d_cumr, d_cumns);
+  }
+  // sizes, offsets (in box order), totals
+  long long *d_rc = nullptr, *d_tc = nullptr, *d_roff = nullptr, *d_toff = nullptr;
+  unsigned long long* d_pairs = nullptr;
+  CKD(S.get(&d_rc, nb + 1));
+  CKD(S.get(&d_tc, nb + 1));
+  CKD(S.get(&d_roff, nb + 1));
+  CKD(S.get(&d_toff, nb + 1));
+  CKD(S.get(&d_pairs, 1));
+  k_near_sizes<<<(nb + 255) / 256, 256, 0, st>>>(nb, d_nch, d_cumr, d_s0, d_s1, d_t0, d_t1, set0, set1, d_rc, d_tc);
+  CKD(cudaMemsetAsync(d_rc + nb, 0, sizeof(long long), st));
+  CKD(cudaMemsetAsync(d_tc + nb, 0, sizeof(long long), st));
+  CKD(cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), st));
+  {
+    size_t tmp = 0, tmp2 = 0;
+    CKD(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_rc, d_roff, nb + 1, st));
+    CKD(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d_tc, d_toff, nb + 1, st));
+    char* dt = nullptr;
+    CKD(S.get(&dt, std::max(tmp, tmp2)));
+    CKD(cub::DeviceScan::ExclusiveSum(dt, tmp, d_rc, d_roff, nb + 1, st));
+    CKD(cub::DeviceScan::ExclusiveSum(dt, tmp2, d_tc, d_toff, nb + 1, st));
+  }
+  long long tot[2] = {0, 0};
+  CKD(cudaMemcpyAsync(&tot[0], d_roff + nb, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CKD(cudaMemcpyAsync(&tot[1], d_toff + nb, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  // the output arrays outlive this build (until the plan copies them)
+  HostPlan::DevNear& out = H.dnear;
+  const size_t bd = ((size_t)tot[1] * sizeof(DirTask) + 255) & ~size_t(255);
+  const size_t bs = (size_t)tot[0] * sizeof(SrcRange);
+  void* mem = nullptr;
+  CKD(cudaMallocAsync(&mem, std::max<size_t>(bd + bs, 256), st));
+  out.mem = mem;
+  out.dir = reinterpret_cast<DirTask*>(mem);
+  out.src = reinterpret_cast<SrcRange*>(static_cast<char*>(mem) + bd);
+  out.ndir = tot[1];
+  out.nsrc = tot[0];
+  k_near_fill<<<(nb + 255) / 256, 256, 0, st>>>(nb, d_nch, d_par, d_cumr, d_cumns, d_ioff, d_into, d_s0, d_s1, d_t0,
+                                                d_t1, set0, set1, d_roff, d_toff, out.dir, out.src, d_pairs);
+  unsigned long long pairs = 0;
+  CKD(cudaMemcpyAsync(&pairs, d_pairs, sizeof(pairs), cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  H.direct_pairs = (long long)pairs;
+  H.dir.clear();
+  H.dir_src.clear();
+  return cudaGetLastError();
+}
+
+void device_near_free(HostPlan& H, cudaStream_t st) {
+  if (H.dnear.mem) cudaFreeAsync(H.dnear.mem, st);
+  H.dnear = HostPlan::DevNear();
 }
 
 }  // namespace fgtb

@@ -3567,7 +3567,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     }
   }
   D.nm2l = (int)H.m2l.size();
-  D.ndir = (int)H.dir.size();
+  D.ndir = (int)(H.dnear.mem ? H.dnear.ndir : (long long)H.dir.size());
   D.nmp = H.nmp;
   D.nloc = H.nloc;
   D.direct_pairs = H.direct_pairs;
@@ -3671,6 +3671,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
                  al((size_t)(std::max(P.ntermmax, 1) + 2) * 8) + al(32 * 8) +
                  bytes_of(form) + bytes_of(groups) + bytes_of(H.merge) + bytes_of(split_kept) +
                  bytes_of(H.m2l) + bytes_of(H.m2l_nbr) + bytes_of(ev) + bytes_of(H.dir) +
+                 al((size_t)H.dnear.ndir * sizeof(DirTask)) + al((size_t)H.dnear.nsrc * sizeof(SrcRange)) +
                  bytes_of(H.dir_src) + al((size_t)H.nmp * nd * P.nexp * 16) +
                  al((size_t)H.nloc * nd * P.nexp * 16) + al(ns * dim * 8) + al(ns * nd * 8) +
                  al(nt * dim * 8) + al(ns * nd * out_comps(dim, P.ifpgh) * 8) +
@@ -3767,8 +3768,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     st.add(cur, D.m2l, H.m2l);
     st.add(cur, D.m2l_nbr, H.m2l_nbr);
     st.add(cur, D.eval, ev);
-    st.add(cur, D.dir, H.dir);
-    st.add(cur, D.dir_src, H.dir_src);
+    if (!H.dnear.mem) {  // else built on the device: copied after this block
+      st.add(cur, D.dir, H.dir);
+      st.add(cur, D.dir_src, H.dir_src);
+    }
     st.add(cur, D.fchunks, fchunks);
     st.add(cur, D.fcbeg, fcbeg);
     st.add(cur, D.form_hoff, form_hoff);
@@ -3776,6 +3779,17 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     st.add(cur, D.conv, conv);
     st.add(cur, D.horner, horner);
     CK(st.upload(b0, s));
+  }
+  if (H.dnear.mem) {
+    D.dir = reinterpret_cast<DirTask*>(cur);
+    cur += al((size_t)H.dnear.ndir * sizeof(DirTask));
+    D.dir_src = reinterpret_cast<SrcRange*>(cur);
+    cur += al((size_t)H.dnear.nsrc * sizeof(SrcRange));
+    if (H.dnear.ndir)
+      CK(cudaMemcpyAsync(D.dir, H.dnear.dir, (size_t)H.dnear.ndir * sizeof(DirTask), cudaMemcpyDeviceToDevice, s));
+    if (H.dnear.nsrc)
+      CK(cudaMemcpyAsync(D.dir_src, H.dnear.src, (size_t)H.dnear.nsrc * sizeof(SrcRange), cudaMemcpyDeviceToDevice,
+                         s));
   }
   D.lo = reinterpret_cast<double*>(cur); cur += al(lo_doubles * 8);
   D.hbuf = reinterpret_cast<double*>(cur); cur += al(hbuf_doubles * 8);

@@ -531,7 +531,7 @@ static void finish_plan(HostPlan& H) {
   if (P.scheme == 1) build_tasks_nufft(H);
   else build_tasks(H);
   const double tn = now();
-  build_near_tasks(H);
+  if (!H.defer_near) build_near_tasks(H);
   if (getenv("FGT_TREE_TIMING"))
     fprintf(stderr, "near-field tasks: %.4f (dir %zu ranges %zu)\n", now() - tn, H.dir.size(), H.dir_src.size());
   H.box_centers = t.centers;

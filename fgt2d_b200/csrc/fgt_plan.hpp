@@ -98,6 +98,16 @@ struct HostPlan {
   std::vector<EvalTask> eval;
   uvector<DirTask> dir;
   uvector<SrcRange> dir_src;
+  // The near-field arrays built on the GPU instead (build_near_tasks_device;
+  // dir / dir_src then stay empty): one stream-ordered allocation, copied
+  // into the plan's arena and released by the plan's creation.
+  struct DevNear {
+    DirTask* dir = nullptr;
+    SrcRange* src = nullptr;
+    long long ndir = 0, nsrc = 0;
+    void* mem = nullptr;
+  } dnear;
+  bool defer_near = false;  // finish_plan leaves the near-field arrays to the device build
   // statistics
   long long direct_pairs = 0;
   long long form_sources = 0, eval_points = 0;
