@@ -56,34 +56,63 @@ __device__ __forceinline__ int child_slot_d(const double* x, const double* c, in
 }
 
 // Per-block minimum and maximum of each coordinate (blockDim = 256);
-// part[6 block + d] = min, part[6 block + 3 + d] = max.
-__global__ void __launch_bounds__(256) k_bbox(const double* __restrict__ x, int n, int dim,
-                                              double* __restrict__ part) {
-  __shared__ double smn[3][256], smx[3][256];
-  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
-    for (int d = 0; d < dim; d++) {
-      const double v = x[(size_t)dim * i + d];
-      mn[d] = fmin(mn[d], v);
-      mx[d] = fmax(mx[d], v);
+// part[6 block + d] = min, part[6 block + 3 + d] = max.  Four points per
+// thread and step, so that several loads are in flight.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_bbox(const double* __restrict__ x, int n, double* __restrict__ part) {
+  __shared__ double smn[DIM][8], smx[DIM][8];
+  double mn[DIM], mx[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    mn[d] = INFINITY;
+    mx[d] = -INFINITY;
+  }
+  const long long tot = (long long)n * DIM, stride = (long long)gridDim.x * 256 * 4;
+  for (long long e = ((long long)blockIdx.x * 256 * 4 + threadIdx.x); e < tot; e += stride) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const long long q = e + (long long)u * 256;
+      v[u] = q < tot ? x[q] : NAN;
     }
-  for (int d = 0; d < 3; d++) {
-    smn[d][threadIdx.x] = mn[d];
-    smx[d][threadIdx.x] = mx[d];
-  }
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      for (int d = 0; d < 3; d++) {
-        smn[d][threadIdx.x] = fmin(smn[d][threadIdx.x], smn[d][threadIdx.x + s]);
-        smx[d][threadIdx.x] = fmax(smx[d][threadIdx.x], smx[d][threadIdx.x + s]);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const long long q = e + (long long)u * 256;
+      if (q < tot) {
+        const int d = (int)(q % DIM);
+#pragma unroll
+        for (int dd = 0; dd < DIM; dd++)
+          if (d == dd) {
+            mn[dd] = fmin(mn[dd], v[u]);
+            mx[dd] = fmax(mx[dd], v[u]);
+          }
       }
-    __syncthreads();
+    }
   }
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+    for (int off = 16; off > 0; off >>= 1) {
+      mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], off));
+      mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], off));
+    }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      smn[d][w] = mn[d];
+      smx[d][w] = mx[d];
+    }
+  __syncthreads();
   if (threadIdx.x == 0)
     for (int d = 0; d < 3; d++) {
-      part[6 * blockIdx.x + d] = smn[d][0];
-      part[6 * blockIdx.x + 3 + d] = smx[d][0];
+      double lo = INFINITY, hi = -INFINITY;
+      if (d < DIM)
+        for (int k = 0; k < 8; k++) {
+          lo = fmin(lo, smn[d][k]);
+          hi = fmax(hi, smx[d][k]);
+        }
+      part[6 * blockIdx.x + d] = lo;
+      part[6 * blockIdx.x + 3 + d] = hi;
     }
 }
 
@@ -182,85 +211,108 @@ __global__ void __launch_bounds__(256) k_locate(const double* __restrict__ x, in
 // centre < 0 as sort_pts_to_children), packed most significant level first.
 // Every box the refinement can create is a contiguous range of these keys in
 // sorted order, and sorted order is the depth-first order of the leaves.
-__global__ void __launch_bounds__(256) k_exact_key(const double* __restrict__ x, int n, int dim, double cx,
-                                                   double cy, double cz, double bs0, int L,
+template <int DIM>
+__global__ void __launch_bounds__(256) k_exact_key(const double* __restrict__ x, int n, double cx, double cy,
+                                                   double cz, double bs0, int L,
                                                    unsigned long long* __restrict__ key, int* __restrict__ id) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double p[3] = {0, 0, 0}, c[3] = {cx, cy, cz};
-  for (int d = 0; d < dim; d++) p[d] = x[(size_t)dim * i + d];
+  double p[DIM], c[DIM];
+  const double c3[3] = {cx, cy, cz};
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    p[d] = x[(size_t)DIM * i + d];
+    c[d] = c3[d];
+  }
   double bs = bs0;
   unsigned long long k = 0;
   for (int l = 0; l < L; l++) {
     int j = 0;
-    for (int d = 0; d < dim; d++)
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
       if (!(p[d] - c[d] < 0)) j |= 1 << d;
-    k = (k << dim) | (unsigned long long)j;
+    k = (k << DIM) | (unsigned long long)j;
     bs = bs / 2;  // size of the child level
     const double h = bs / 2;
-    for (int d = 0; d < dim; d++) c[d] = c[d] + (((j >> d) & 1) ? h : -h);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) c[d] = c[d] + (((j >> d) & 1) ? h : -h);
   }
   key[i] = k;
   id[i] = i;
 }
 
-// First position in [lo, hi) whose digit (key >> shift) & (nch - 1) is >= v;
-// the digits are nondecreasing there (the range is one box of the level
-// above the digit).
-__device__ __forceinline__ int digit_lower_bound(const unsigned long long* __restrict__ key, int lo, int hi,
-                                                 int shift, int nch, int v) {
-  while (lo < hi) {
-    const int m = (lo + hi) >> 1;
-    if ((int)((key[m] >> shift) & (unsigned long long)(nch - 1)) < v) lo = m + 1;
-    else hi = m;
+// First position in [lo, hi) whose digit (key >> shift) & (nch - 1) is >= v,
+// found by one warp: every round the 32 lanes probe 32 increasing positions
+// of the remaining range and a ballot keeps the interval between the last
+// probe below v and the first at or above it (the digits are nondecreasing
+// there: the range is one box of the level above the digit), so a range of
+// n keys takes about log32(n) rounds of independent loads.  Called by all 32
+// lanes with the same arguments; every lane returns the position.
+__device__ __forceinline__ int warp_digit_lower_bound(const unsigned long long* __restrict__ key, int lo, int hi,
+                                                      int shift, int nch, int v) {
+  const int lane = threadIdx.x & 31;
+  int a = lo, b = hi;  // positions < a are below v; position b is at or above v (or b == hi)
+  for (int round = 0; round < 8 && b - a > 32; round++) {
+    const long long span = b - a;
+    const int p = a + (int)(span * lane / 32);  // lane 0 probes a; a < p < b otherwise
+    const bool below = (int)((key[p] >> shift) & (unsigned long long)(nch - 1)) < v;
+    const int c = __popc(__ballot_sync(0xffffffffu, below));  // lanes 0 .. c-1 are below
+    const int pa = __shfl_sync(0xffffffffu, p, (c + 31) & 31);
+    const int pb = __shfl_sync(0xffffffffu, p, c & 31);
+    if (c == 0) return a;
+    b = c < 32 ? pb : b;
+    a = pa + 1;
   }
-  return lo;
+  const int p = a + lane;
+  const bool below = p < b && (int)((key[p] >> shift) & (unsigned long long)(nch - 1)) < v;
+  return a + __popc(__ballot_sync(0xffffffffu, below));
 }
 
-// Ranges of the children of the boxes [a, a + nlev) of one level, from the
-// parents' ranges: one thread per (box, child).  With fc (refinement), the
-// children of box a + i are fc[i] + j (fc[i] < 0: not refined) and their
-// source counts go to cnt[child - c0]; with child (the finished tree), they
-// are child[box * nch + j].
-__global__ void __launch_bounds__(256) k_child_ranges(const unsigned long long* __restrict__ key, int shift,
-                                                      int nch, int a, int nlev, const int* __restrict__ fc,
-                                                      const int* __restrict__ child, int* __restrict__ r0,
-                                                      int* __restrict__ r1, int c0, int* __restrict__ cnt) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nlev * nch) return;
-  const int i = t / nch, j = t - i * nch, box = a + i;
-  const int c = fc ? (fc[i] >= 0 ? fc[i] + j : -1) : child[(size_t)box * nch + j];
-  if (c < 0) return;
-  const int lo = r0[box], hi = r1[box];
-  const int s = digit_lower_bound(key, lo, hi, shift, nch, j);
-  const int e = j == nch - 1 ? hi : digit_lower_bound(key, s, hi, shift, nch, j + 1);
-  r0[c] = s;
-  r1[c] = e;
-  if (cnt) cnt[c - c0] = e - s;
+// Key ranges of the children of the boxes [a, a + nlev) of one level of the
+// finished tree (child[box * NCH + j]), from the parents' ranges: one warp
+// per (box, digit v = 1 .. NCH-1) finds where the children's digit reaches
+// v; child v - 1 ends and child v starts there, child 0 starts at the
+// parent's start and child NCH-1 ends at its end.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_child_bounds(const unsigned long long* __restrict__ key, int shift, int a,
+                                                      int nlev, const int* __restrict__ child, int* __restrict__ r0,
+                                                      int* __restrict__ r1) {
+  constexpr int NCH = 1 << DIM;
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const long long nw = (long long)nlev * (NCH - 1);
+  for (long long w = (long long)blockIdx.x * wpb + (threadIdx.x >> 5); w < nw; w += (long long)gridDim.x * wpb) {
+    const int i = (int)(w / (NCH - 1)), v = (int)(w - (long long)i * (NCH - 1)) + 1, box = a + i;
+    const int* ch = child + (size_t)box * NCH;
+    const int cprev = ch[v - 1], cv = ch[v];
+    if (cprev < 0 && cv < 0) continue;  // (warp-uniform)
+    const int lo = r0[box], hi = r1[box];
+    const int bnd = warp_digit_lower_bound(key, lo, hi, shift, NCH, v);
+    if (lane == 0) {
+      if (cprev >= 0) r1[cprev] = bnd;
+      if (cv >= 0) r0[cv] = bnd;
+      if (v == 1 && cprev >= 0) r0[cprev] = lo;
+      if (v == NCH - 1 && cv >= 0) r1[cv] = hi;
+    }
+  }
 }
 
-// Sort key of the final point order: the depth-first rank of the leaf that
-// holds sorted position k (leaf ranges start at lstart[rank], ascending),
-// scattered to the point's input index, with the input index as the value
-// (a stable sort on the rank keeps the input order inside a leaf).
-__global__ void __launch_bounds__(256) k_position_rank(const int* __restrict__ lstart, int nleaf,
-                                                       const int* __restrict__ wid, int n, int* __restrict__ rk,
+// Sort key of the final point order: the depth-first rank r of the leaf
+// whose key range [r0, r1) holds sorted position k, scattered to the
+// point's input index, with the input index as the value (a stable sort on
+// the rank keeps the input order inside a leaf).  One warp per leaf; the
+// leaves' ranges tile the sorted positions.
+__global__ void __launch_bounds__(256) k_position_rank(const int* __restrict__ r0, const int* __restrict__ r1,
+                                                       const int* __restrict__ leaf_of_rank, int nleaf,
+                                                       const int* __restrict__ wid, int* __restrict__ rk,
                                                        int* __restrict__ idx) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  int lo = 0, hi = nleaf;  // last leaf whose start is <= k
-  while (hi - lo > 1) {
-    const int m = (lo + hi) >> 1;
-    if (lstart[m] <= k) lo = m;
-    else hi = m;
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nleaf; r += gridDim.x * wpb) {
+    const int leaf = leaf_of_rank[r], lo = r0[leaf], hi = r1[leaf];
+    for (int k = lo + lane; k < hi; k += 32) {
+      rk[wid[k]] = r;
+      idx[k] = k;
+    }
   }
-  rk[wid[k]] = lo;
-  idx[k] = k;
-}
-__global__ void k_leaf_starts(const int* __restrict__ r0, const int* __restrict__ leaf_of_rank, int nleaf,
-                              int* __restrict__ lstart) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nleaf) lstart[r] = r0[leaf_of_rank[r]];
 }
 __global__ void k_root_range(int* r0, int* r1, int n) {
   r0[0] = 0;
@@ -293,117 +345,253 @@ __global__ void k_ref_init(int* lev, int nslot, int* r0, int* r1, int* par, int*
   const double c[3] = {cx, cy, cz};
   for (int d = 0; d < dim; d++) cen[d] = c[d];
 }
-// flag[i]: box first + i of level l holds more than thr sources
-__global__ void k_ref_flag(const int* __restrict__ lev, int l, const int* __restrict__ r0,
-                           const int* __restrict__ r1, int thr, int* __restrict__ flag) {
-  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    flag[i] = r1[first + i] - r0[first + i] > thr;
-}
-// One block of 1024 threads: exclusive prefix of the flags (the refined
-// boxes' ranks), and the id range of level l + 1.
-__global__ void __launch_bounds__(1024) k_ref_scan(int* __restrict__ lev, int l, int nslot,
-                                                   const int* __restrict__ flag, int* __restrict__ pos, int nch) {
-  __shared__ int part[1024];
-  const int first = lev[2 * l], n = max(0, lev[2 * l + 1] - first + 1);
-  const int per = (n + 1023) / 1024, i0 = min(n, (int)threadIdx.x * per), i1 = min(n, i0 + per);
-  int sum = 0;
-  for (int i = i0; i < i1; i++) sum += flag[i];
-  part[threadIdx.x] = sum;
+// ---- multi-block exclusive scans of 0/1 flags (blockDim 256) ----
+// Block k of G handles the items [k chunk, min(n, (k + 1) chunk)), chunk =
+// ceil(n / G): a counting pass writes each block's count to part[k], one
+// block scans part[] (k_scan_top), and a ranking pass adds each block's
+// offset to the block-wide prefix of its items.
+__device__ __forceinline__ int block_reduce256(int v, int* sw) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane == 0) sw[w] = v;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  int t = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) t += sw[k];
+  __syncthreads();
+  return t;
+}
+// exclusive prefix of v over the block; *total the block's sum
+__device__ __forceinline__ int block_excl_scan256(int v, int* sw, int& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int x = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += x;
   }
-  int run = part[threadIdx.x] - sum;
+  if (lane == 31) sw[w] = incl;
+  __syncthreads();
+  int before = 0, t = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int x = sw[k];
+    before += k < w ? x : 0;
+    t += x;
+  }
+  __syncthreads();
+  total = t;
+  return before + incl - v;
+}
+// exclusive scan of part[0, G) in place (G <= 4096, one block of 1024);
+// the sum goes to *total, and with lev (the refinement) it makes the id
+// range of level l + 1: nch children per flagged box after the current boxes
+__global__ void __launch_bounds__(1024) k_scan_top(int* __restrict__ part, int G, int* __restrict__ total,
+                                                   int* __restrict__ lev, int l, int nslot, int nch) {
+  __shared__ int sw[32];
+  const int per = (G + 1023) / 1024, i0 = min(G, (int)threadIdx.x * per), i1 = min(G, i0 + per);
+  int v = 0;
+  for (int i = i0; i < i1; i++) v += part[i];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int x = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += x;
+  }
+  if (lane == 31) sw[w] = incl;
+  __syncthreads();
+  int before = 0, t = 0;
+  for (int k = 0; k < 32; k++) {
+    before += k < w ? sw[k] : 0;
+    t += sw[k];
+  }
+  int run = before + incl - v;
   for (int i = i0; i < i1; i++) {
-    pos[i] = run;
-    run += flag[i];
+    const int x = part[i];
+    part[i] = run;
+    run += x;
   }
-  if (threadIdx.x == 1023) {
-    const int nref = part[1023], nb = lev[2 * nslot];
-    if (nref > 0) {
+  if (threadIdx.x == 0) {
+    if (total) *total = t;
+    if (lev && t > 0) {
+      const int nb = lev[2 * nslot];
       lev[2 * (l + 1)] = nb;
-      lev[2 * (l + 1) + 1] = nb + nch * nref - 1;
-      lev[2 * nslot] = nb + nch * nref;
+      lev[2 * (l + 1) + 1] = nb + nch * t - 1;
+      lev[2 * nslot] = nb + nch * t;
     }
   }
 }
+// refinement, level l: flag[i] = box first + i holds more than thr sources;
+// part[block] = the block's count
+__global__ void __launch_bounds__(256) k_ref_count(const int* __restrict__ lev, int l, const int* __restrict__ r0,
+                                                   const int* __restrict__ r1, int thr, int* __restrict__ flag,
+                                                   int* __restrict__ part) {
+  __shared__ int sw[8];
+  const int first = lev[2 * l], n = max(0, lev[2 * l + 1] - first + 1);
+  const int chunk = (n + gridDim.x - 1) / gridDim.x, i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  int c = 0;
+  for (int i = i0 + threadIdx.x; i < i1; i += 256) {
+    const int f = r1[first + i] - r0[first + i] > thr;
+    flag[i] = f;
+    c += f;
+  }
+  c = block_reduce256(c, sw);
+  if (threadIdx.x == 0) part[blockIdx.x] = c;
+}
+// pos[i] = the rank of flagged box first + i among the level's flagged boxes
+__global__ void __launch_bounds__(256) k_ref_rank(const int* __restrict__ lev, int l, const int* __restrict__ flag,
+                                                  const int* __restrict__ part, int* __restrict__ pos) {
+  __shared__ int sw[8];
+  const int first = lev[2 * l], n = max(0, lev[2 * l + 1] - first + 1);
+  const int chunk = (n + gridDim.x - 1) / gridDim.x, i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  int carry = part[blockIdx.x];
+  for (int base = i0; base < i1; base += 256) {  // (block-uniform)
+    const int i = base + threadIdx.x;
+    const int v = i < i1 ? flag[i] : 0;
+    int tot;
+    const int ex = block_excl_scan256(v, sw, tot);
+    if (i < i1) pos[i] = carry + ex;
+    carry += tot;
+  }
+}
+// blocks of a flag scan over n items (at most 4096, 2048 items or more each)
+static int scan_blocks(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 2047) / 2048, 1184)); }
+
 // The children of the refined boxes of level l: structure, centres (the
 // parent's plus or minus h, a quarter of the parent's size, in each
-// dimension) and key ranges; one thread per (box, child).
-__global__ void k_ref_children(const int* __restrict__ lev, int l, const int* __restrict__ flag,
-                               const int* __restrict__ pos, const unsigned long long* __restrict__ key, int shift,
-                               int nch, int dim, double h, int* __restrict__ r0, int* __restrict__ r1,
-                               int* __restrict__ par, int* __restrict__ nchild, int* __restrict__ child,
-                               int* __restrict__ level, double* __restrict__ cen) {
+// dimension) and key ranges.  One warp per (refined box, digit v = 1 ..
+// NCH-1): the warp finds where the children's digit reaches v
+// (warp_digit_lower_bound), lane 0 writes child v - 1 (and lane 1 child
+// NCH-1 for the last digit).
+template <int DIM>
+__device__ __forceinline__ void ref_child(int b, int c, int j, int l, double h, int* __restrict__ par,
+                                          int* __restrict__ nchild, int* __restrict__ child, int* __restrict__ level,
+                                          double* __restrict__ cen) {
+  constexpr int NCH = 1 << DIM;
+  child[(size_t)b * NCH + j] = c;
+  par[c] = b;
+  level[c] = l + 1;
+  nchild[c] = 0;
+#pragma unroll
+  for (int q = 0; q < NCH; q++) child[(size_t)c * NCH + q] = -1;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) cen[(size_t)c * DIM + d] = cen[(size_t)b * DIM + d] + (((j >> d) & 1) ? h : -h);
+}
+template <int DIM>
+__global__ void __launch_bounds__(256) k_ref_children(const int* __restrict__ lev, int l,
+                                                      const int* __restrict__ flag, const int* __restrict__ pos,
+                                                      const unsigned long long* __restrict__ key, int shift, double h,
+                                                      int* __restrict__ r0, int* __restrict__ r1,
+                                                      int* __restrict__ par, int* __restrict__ nchild,
+                                                      int* __restrict__ child, int* __restrict__ level,
+                                                      double* __restrict__ cen) {
+  constexpr int NCH = 1 << DIM;
   const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1, c0 = lev[2 * (l + 1)];
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)n * nch;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int bi = (int)(i / nch), j = (int)(i - (long long)bi * nch);
-    if (!flag[bi]) continue;
-    const int b = first + bi, c = c0 + nch * pos[bi] + j;
-    if (j == 0) nchild[b] = nch;
-    child[(size_t)b * nch + j] = c;
-    par[c] = b;
-    level[c] = l + 1;
-    nchild[c] = 0;
-    for (int q = 0; q < nch; q++) child[(size_t)c * nch + q] = -1;
-    for (int d = 0; d < dim; d++) cen[(size_t)c * dim + d] = cen[(size_t)b * dim + d] + (((j >> d) & 1) ? h : -h);
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const long long nw = (long long)n * (NCH - 1);
+  for (long long w = (long long)blockIdx.x * wpb + (threadIdx.x >> 5); w < nw; w += (long long)gridDim.x * wpb) {
+    const int bi = (int)(w / (NCH - 1)), v = (int)(w - (long long)bi * (NCH - 1)) + 1;
+    if (!flag[bi]) continue;  // (warp-uniform)
+    const int b = first + bi, cb = c0 + NCH * pos[bi];
     const int lo = r0[b], hi = r1[b];
-    const int s = digit_lower_bound(key, lo, hi, shift, nch, j);
-    const int e = j == nch - 1 ? hi : digit_lower_bound(key, s, hi, shift, nch, j + 1);
-    r0[c] = s;
-    r1[c] = e;
+    const int bnd = warp_digit_lower_bound(key, lo, hi, shift, NCH, v);
+    if (lane == 0) {
+      ref_child<DIM>(b, cb + v - 1, v - 1, l, h, par, nchild, child, level, cen);
+      r1[cb + v - 1] = bnd;
+      r0[cb + v] = bnd;
+      if (v == 1) {
+        r0[cb] = lo;
+        nchild[b] = NCH;
+      }
+    } else if (lane == 1 && v == NCH - 1) {
+      ref_child<DIM>(b, cb + NCH - 1, NCH - 1, l, h, par, nchild, child, level, cen);
+      r1[cb + NCH - 1] = hi;
+    }
   }
 }
 
-// Colleagues of the boxes of level l (computecoll, tree_routs4.f:100-211, as
-// colleagues_box in fgt_tree.cpp): the children of the parent's colleagues
-// whose centres lie within lim of the box's in every dimension, in the
-// parent's colleague order then child order; unused slots -1.
-__global__ void k_ref_colleagues(const int* __restrict__ lev, int l, double lim, int nch, int nco, int dim,
-                                 const int* __restrict__ par, const int* __restrict__ nchild,
-                                 const int* __restrict__ child, const double* __restrict__ cen,
-                                 int* __restrict__ ncoll, int* __restrict__ coll) {
-  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int b = first + i, dad = par[b];
-    double cb[3] = {0, 0, 0};
-    for (int d = 0; d < dim; d++) cb[d] = cen[(size_t)b * dim + d];
-    int cnt = 0;
-    for (int q = 0; q < ncoll[dad]; q++) {
-      const int jb = coll[(size_t)dad * nco + q];
-      const int* ch = child + (size_t)jb * nch;
-      if (ch[0] < 0 && nchild[jb] == 0) continue;
-      bool all = true;
-      for (int j = 0; j < nch; j++) all = all && ch[j] >= 0;
-      if (all) {
-        unsigned pass0 = 0u, pass1 = 0u;
-        for (int d = 0; d < dim; d++) {
-          if (fabs(cen[(size_t)ch[0] * dim + d] - cb[d]) <= lim) pass0 |= 1u << d;
-          if (fabs(cen[(size_t)ch[1 << d] * dim + d] - cb[d]) <= lim) pass1 |= 1u << d;
-        }
-        for (int j = 0; j < nch; j++) {
-          const unsigned ok = (pass1 & (unsigned)j) | (pass0 & ~(unsigned)j);
-          if ((ok & ((1u << dim) - 1)) == (1u << dim) - 1 && cnt < nco) coll[(size_t)b * nco + cnt++] = ch[j];
-        }
-        continue;
+// Colleagues of box b (computecoll, tree_routs4.f:100-211, as colleagues_box
+// in fgt_tree.cpp): the children of the parent's colleagues whose centres lie
+// within lim of the box's in every dimension, in the parent's colleague
+// order then child order; unused slots -1.  One warp per box: lane q tests
+// the children of the parent's colleague q (nco <= 32), and a prefix sum of
+// the lanes' counts places them.  When a colleague has all its children,
+// child j's coordinate d is that of child 0 or child 2^d (bit d of j), so
+// two centres per dimension decide all of them.
+template <int DIM>
+__device__ __forceinline__ void colleagues_warp(int b, double lim, int nco, const int* __restrict__ par,
+                                                const int* __restrict__ child, const double* __restrict__ cen,
+                                                int* __restrict__ ncoll, int* __restrict__ coll) {
+  constexpr int NCH = 1 << DIM;
+  const int lane = threadIdx.x & 31;
+  const int dad = par[b];
+  const int nc = ncoll[dad];
+  double cb[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) cb[d] = cen[(size_t)b * DIM + d];
+  int ch[NCH];
+  unsigned mask = 0;
+  const int jb = lane < nc ? coll[(size_t)dad * nco + lane] : -1;
+  if (jb >= 0) {
+    bool all = true;
+#pragma unroll
+    for (int j = 0; j < NCH; j++) {
+      ch[j] = child[(size_t)jb * NCH + j];
+      all = all && ch[j] >= 0;
+    }
+    if (all) {
+      unsigned pass0 = 0u, pass1 = 0u;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        if (fabs(cen[(size_t)ch[0] * DIM + d] - cb[d]) <= lim) pass0 |= 1u << d;
+        if (fabs(cen[(size_t)ch[1 << d] * DIM + d] - cb[d]) <= lim) pass1 |= 1u << d;
       }
-      for (int j = 0; j < nch; j++) {
-        const int kb = ch[j];
-        if (kb < 0) continue;
+#pragma unroll
+      for (int j = 0; j < NCH; j++) {
+        const unsigned ok = (pass1 & (unsigned)j) | (pass0 & ~(unsigned)j);
+        if ((ok & (NCH - 1u)) == NCH - 1u) mask |= 1u << j;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < NCH; j++) {
+        if (ch[j] < 0) continue;
         bool ok = true;
-        for (int d = 0; d < dim; d++)
-          if (!(fabs(cen[(size_t)kb * dim + d] - cb[d]) <= lim)) ok = false;
-        if (ok && cnt < nco) coll[(size_t)b * nco + cnt++] = kb;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) ok = ok && fabs(cen[(size_t)ch[j] * DIM + d] - cb[d]) <= lim;
+        if (ok) mask |= 1u << j;
       }
     }
-    for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
-    ncoll[b] = cnt;
   }
+  const int cnt = __popc(mask);
+  int incl = cnt;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  int o = incl - cnt;
+#pragma unroll
+  for (int j = 0; j < NCH; j++)
+    if ((mask >> j) & 1u) {
+      if (o < nco) coll[(size_t)b * nco + o] = ch[j];
+      o++;
+    }
+  const int kept = min(total, nco);
+  for (int q = kept + lane; q < nco; q += 32) coll[(size_t)b * nco + q] = -1;
+  if (lane == 0) ncoll[b] = kept;
+}
+// the boxes of level l (ids from lev)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_ref_colleagues(const int* __restrict__ lev, int l, double lim, int nco,
+                                                        const int* __restrict__ par, const int* __restrict__ child,
+                                                        const double* __restrict__ cen, int* __restrict__ ncoll,
+                                                        int* __restrict__ coll) {
+  const int first = lev[2 * l], n = lev[2 * l + 1] - first + 1, wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n; w += gridDim.x * wpb)
+    colleagues_warp<DIM>(first + w, lim, nco, par, child, cen, ncoll, coll);
 }
 
 // ---- level restriction on the device (pts_tree_fix_lr, pts_tree2d4.f:693-996,
@@ -492,30 +680,32 @@ __global__ void k_lr_update(LrRanges R, double dist, const int* __restrict__ nch
     flag[box] = f;
   }
 }
-// One block of 1024 threads: rank of every flagged box (flag > 0) among the
-// flagged boxes of the concatenated ranges; *total and, for the first box
-// of each of the nb_mark boxes in mark[], the rank there (rank_at[k]).
-__global__ void __launch_bounds__(1024) k_lr_scan(LrRanges R, const int* __restrict__ flag, int* __restrict__ pos,
-                                                  int* __restrict__ total) {
-  __shared__ int part[1024];
+// Rank of every flagged box (flag > 0) among the flagged boxes of the
+// concatenated ranges, by the multi-block scan above: per-block counts,
+// k_scan_top (the total to *total), ranks pos[i] by position i.
+__global__ void __launch_bounds__(256) k_lr_count(LrRanges R, const int* __restrict__ flag, int* __restrict__ part) {
+  __shared__ int sw[8];
   const int n = lr_count(R);
-  const int per = (n + 1023) / 1024, i0 = min(n, (int)threadIdx.x * per), i1 = min(n, i0 + per);
-  int sum = 0;
-  for (int i = i0; i < i1; i++) sum += flag[lr_box(R, i)] > 0;
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  const int chunk = (n + gridDim.x - 1) / gridDim.x, i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  int c = 0;
+  for (int i = i0 + threadIdx.x; i < i1; i += 256) c += flag[lr_box(R, i)] > 0;
+  c = block_reduce256(c, sw);
+  if (threadIdx.x == 0) part[blockIdx.x] = c;
+}
+__global__ void __launch_bounds__(256) k_lr_rank(LrRanges R, const int* __restrict__ flag,
+                                                 const int* __restrict__ part, int* __restrict__ pos) {
+  __shared__ int sw[8];
+  const int n = lr_count(R);
+  const int chunk = (n + gridDim.x - 1) / gridDim.x, i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  int carry = part[blockIdx.x];
+  for (int base = i0; base < i1; base += 256) {  // (block-uniform)
+    const int i = base + threadIdx.x;
+    const int v = i < i1 ? (flag[lr_box(R, i)] > 0) : 0;
+    int tot;
+    const int ex = block_excl_scan256(v, sw, tot);
+    if (i < i1) pos[i] = carry + ex;
+    carry += tot;
   }
-  int run = part[threadIdx.x] - sum;
-  for (int i = i0; i < i1; i++) {
-    pos[i] = run;
-    run += flag[lr_box(R, i)] > 0;
-  }
-  if (threadIdx.x == 1023) *total = part[1023];
 }
 // tree_refine_boxes_flag (tree_routs4.f:334-388): the flagged boxes of the
 // concatenated ranges get nch children each, from id base on, in the ranges'
@@ -549,26 +739,14 @@ __global__ void k_lr_children(LrRanges R, const int* __restrict__ pos, int base,
     flag[c] = f == 1 ? 3 : 0;
   }
 }
-// colleagues of the boxes of the concatenated ranges from their parents'
-// lists (computecoll; the children of the parent's colleagues within lim, in
-// the parent's colleague order then child order), unused slots -1
-__global__ void k_lr_colleagues(LrRanges R, double lim, int nch, int nco, int dim, const int* __restrict__ par,
-                                const int* __restrict__ child, const double* __restrict__ cen,
-                                int* __restrict__ ncoll, int* __restrict__ coll) {
-  const int n = lr_count(R);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int b = lr_box(R, i), dad = par[b];
-    int cnt = 0;
-    for (int q = 0; q < ncoll[dad]; q++) {
-      const int jb = coll[(size_t)dad * nco + q];
-      for (int j = 0; j < nch; j++) {
-        const int kb = child[(size_t)jb * nch + j];
-        if (kb >= 0 && cnt < nco && lr_touch(cen, dim, kb, b, lim)) coll[(size_t)b * nco + cnt++] = kb;
-      }
-    }
-    for (int q = cnt; q < nco; q++) coll[(size_t)b * nco + q] = -1;
-    ncoll[b] = cnt;
-  }
+// colleagues of the boxes of the concatenated ranges (colleagues_warp)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_lr_colleagues(LrRanges R, double lim, int nco, const int* __restrict__ par,
+                                                       const int* __restrict__ child, const double* __restrict__ cen,
+                                                       int* __restrict__ ncoll, int* __restrict__ coll) {
+  const int n = lr_count(R), wpb = blockDim.x >> 5;
+  for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n; w += gridDim.x * wpb)
+    colleagues_warp<DIM>(lr_box(R, w), lim, nco, par, child, cen, ncoll, coll);
 }
 __global__ void k_lr_gather(const int* __restrict__ src, const int* __restrict__ idx, int n, int* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -790,6 +968,9 @@ struct StagedBatch {
     return cudaSuccess;
   }
 };
+// blocks of 256 threads for one warp per item (the kernels stride beyond)
+static int grid_warps(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 7) / 8, 2368)); }
+
 static size_t staged_bytes(std::initializer_list<size_t> b) {
   size_t t = 0;
   for (size_t x : b) t += (x + 255) & ~size_t(255);
@@ -805,11 +986,16 @@ cudaError_t upload(T* dst, const T* src, size_t n, cudaStream_t st) {
 cudaError_t device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim, double* mn,
                         double* mx, cudaStream_t st) {
   Scratch S(st);
-  const int nb = 296;
+  const int nb = 592;
   double* part = nullptr;
   CKD(S.get(&part, (size_t)12 * nb));
-  k_bbox<<<nb, 256, 0, st>>>(d_src, ns, dim, part);
-  k_bbox<<<nb, 256, 0, st>>>(d_trg, nt, dim, part + 6 * nb);
+  if (dim == 2) {
+    k_bbox<2><<<nb, 256, 0, st>>>(d_src, ns, part);
+    k_bbox<2><<<nb, 256, 0, st>>>(d_trg, nt, part + 6 * nb);
+  } else {
+    k_bbox<3><<<nb, 256, 0, st>>>(d_src, ns, part);
+    k_bbox<3><<<nb, 256, 0, st>>>(d_trg, nt, part + 6 * nb);
+  }
   std::vector<double> h((size_t)12 * nb);
   CKD(cudaMemcpyAsync(h.data(), part, h.size() * 8, cudaMemcpyDeviceToHost, st));
   CKD(cudaStreamSynchronize(st));
@@ -904,8 +1090,12 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(S.get(&skey, ns));
   CKD(S.get(&wid0, ns));
   CKD(S.get(&wid, ns));
-  k_exact_key<<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, dim, ts.cen0[0], ts.cen0[1], ts.cen0[2], ts.bs0, L, key,
-                                                wid0);
+  if (dim == 2)
+    k_exact_key<2><<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, ts.cen0[0], ts.cen0[1], ts.cen0[2], ts.bs0, L, key,
+                                                     wid0);
+  else
+    k_exact_key<3><<<(ns + 255) / 256, 256, 0, st>>>(d_src, ns, ts.cen0[0], ts.cen0[1], ts.cen0[2], ts.bs0, L, key,
+                                                     wid0);
   {
     size_t tmp = 0;
     CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, wid0, wid, ns, 0, dim * L, st));
@@ -934,6 +1124,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(S.get(&dflag, maxlev));
   CKD(S.get(&dpos, maxlev));
   CKD(S.get(&dlev, 2 * nslot + 1));
+  int* dpart = nullptr;
+  CKD(S.get(&dpart, 1184));
   const int nco = t.nco;
   int *dncoll = nullptr, *dcoll = nullptr;
   CKD(S.get(&dncoll, cap));
@@ -944,13 +1136,18 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     double bs = ts.bs0;
     for (int l = 0; l <= ts.nlmax - 1; l++) {
       const int thr = l < ts.levcut ? ts.ndiv0 : ts.ndiv;
-      const int g1 = (int)std::max<long long>(1, std::min<long long>((bound[l] + 255) / 256, 1184));
-      const int g2 = (int)std::max<long long>(1, std::min<long long>((bound[l] * nch + 255) / 256, 1184));
-      k_ref_flag<<<g1, 256, 0, st>>>(dlev, l, r0, r1, thr, dflag);
-      k_ref_scan<<<1, 1024, 0, st>>>(dlev, l, nslot, dflag, dpos, nch);
+      const int g1 = scan_blocks(bound[l]);
+      k_ref_count<<<g1, 256, 0, st>>>(dlev, l, r0, r1, thr, dflag, dpart);
+      k_scan_top<<<1, 1024, 0, st>>>(dpart, g1, nullptr, dlev, l, nslot, nch);
+      k_ref_rank<<<g1, 256, 0, st>>>(dlev, l, dflag, dpart, dpos);
       bs = bs / 2;  // size of level l + 1, as tree_refine_level
-      k_ref_children<<<g2, 256, 0, st>>>(dlev, l, dflag, dpos, skey, dim * (L - 1 - l), nch, dim, bs / 2, r0, r1,
-                                         dpar, dnch, dchild, dlevel, dcen);
+      const int g2 = grid_warps(bound[l] * (nch - 1));
+      if (dim == 2)
+        k_ref_children<2><<<g2, 256, 0, st>>>(dlev, l, dflag, dpos, skey, dim * (L - 1 - l), bs / 2, r0, r1, dpar,
+                                              dnch, dchild, dlevel, dcen);
+      else
+        k_ref_children<3><<<g2, 256, 0, st>>>(dlev, l, dflag, dpos, skey, dim * (L - 1 - l), bs / 2, r0, r1, dpar,
+                                              dnch, dchild, dlevel, dcen);
     }
   }
   // colleagues of every level (the level restriction starts from them)
@@ -958,9 +1155,11 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     double bs = ts.bs0;
     for (int l = 1; l <= ts.nlmax; l++) {
       bs = bs / 2;
-      const int g = (int)std::max<long long>(1, std::min<long long>((bound[l] + 255) / 256, 1184));
-      k_ref_colleagues<<<g, 256, 0, st>>>(dlev, l, (double)1.05f * bs, nch, nco, dim, dpar, dnch, dchild, dcen,
-                                          dncoll, dcoll);
+      const int g = grid_warps(bound[l]);
+      if (dim == 2)
+        k_ref_colleagues<2><<<g, 256, 0, st>>>(dlev, l, (double)1.05f * bs, nco, dpar, dchild, dcen, dncoll, dcoll);
+      else
+        k_ref_colleagues<3><<<g, 256, 0, st>>>(dlev, l, (double)1.05f * bs, nco, dpar, dchild, dcen, dncoll, dcoll);
     }
   }
   CKD(cudaGetLastError());
@@ -1049,6 +1248,20 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(S.get(&d_dist1, lev + 3));
   CKD(S.get(&d_hsz, lev + 3));
   auto grid_for = [](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 1184)); };
+  int* d_part = nullptr;
+  CKD(S.get(&d_part, 1184));
+  // ranks of the flagged boxes of R into A.pos, their number to d_tot[0]
+  auto lr_scan = [&](const LrRanges& R) {
+    const int g = scan_blocks(lr_count(R));
+    k_lr_count<<<g, 256, 0, st>>>(R, A.flag, d_part);
+    k_scan_top<<<1, 1024, 0, st>>>(d_part, g, d_tot, nullptr, 0, 0, 0);
+    k_lr_rank<<<g, 256, 0, st>>>(R, A.flag, d_part, A.pos);
+  };
+  auto lr_colleagues = [&](const LrRanges& R, double lim) {
+    const int g = grid_warps(lr_count(R));
+    if (dim == 2) k_lr_colleagues<2><<<g, 256, 0, st>>>(R, lim, nco, A.par, A.child, A.cen, A.ncoll, A.coll);
+    else k_lr_colleagues<3><<<g, 256, 0, st>>>(R, lim, nco, A.par, A.child, A.cen, A.ncoll, A.coll);
+  };
   if (lev >= 2) {
     std::vector<double> dist1(lev + 3, 0.0), hsz(lev + 3, 0.0);
     for (int l = 2; l <= lev; l++) dist1[l] = 1.05 * (bsz[l - 1] + bsz[l - 2]) / 2.0;
@@ -1068,7 +1281,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
       for (int r = 0; r < 3; r++) { R.a[r] = 0; R.b[r] = -1; }
       R.a[0] = lf0[1];
       R.b[0] = ll0[lev - 2];
-      k_lr_scan<<<1, 1024, 0, st>>>(R, A.flag, A.pos, d_tot);
+      lr_scan(R);
       // exclusive ranks at the first box of each level 1 .. lev-2
       std::vector<int> idx(lev - 2);
       for (int l = 1; l <= lev - 2; l++) idx[l - 1] = lf0[l] - lf0[1];
@@ -1098,15 +1311,14 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     }
     // colleagues after the first pass (computecoll on that tree)
     for (int l = 1; l <= lev; l++)
-      k_lr_colleagues<<<grid_for(lr_count(RL[l])), 256, 0, st>>>(RL[l], (double)1.05f * bsz[l], nch, nco, dim, A.par,
-                                                                A.child, A.cen, A.ncoll, A.coll);
+      lr_colleagues(RL[l], (double)1.05f * bsz[l]);
     k_lr_keep3<<<grid_for(nbc), 256, 0, st>>>(nbc, A.flag);
     // second pass, level by level (updateflags, then refinement in the
     // order old boxes, this pass's boxes)
     for (int l = 2; l <= lev - 2; l++) {
       k_lr_update<<<grid_for(lr_count(RL[l])), 256, 0, st>>>(RL[l], 1.05 * (bsz[l] + bsz[l + 1]) / 2.0, A.nch,
                                                              A.child, nch, A.ncoll, A.coll, nco, A.cen, dim, A.flag);
-      k_lr_scan<<<1, 1024, 0, st>>>(RL[l], A.flag, A.pos, d_tot);
+      lr_scan(RL[l]);
       int total = 0;
       CKD(cudaMemcpyAsync(&total, d_tot, sizeof(int), cudaMemcpyDeviceToHost, st));
       CKD(cudaStreamSynchronize(st));
@@ -1121,8 +1333,7 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
       for (int r = 0; r < 3; r++) { Rn.a[r] = 0; Rn.b[r] = -1; }
       Rn.a[0] = RL[l + 1].a[2];
       Rn.b[0] = RL[l + 1].b[2];
-      k_lr_colleagues<<<grid_for(nch * total), 256, 0, st>>>(Rn, (double)1.05f * bsz[l + 1], nch, nco, dim, A.par,
-                                                             A.child, A.cen, A.ncoll, A.coll);
+      lr_colleagues(Rn, (double)1.05f * bsz[l + 1]);
       nbc += nch * total;
     }
   }
@@ -1185,9 +1396,15 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(upload(d_lev2, lv.data(), lv.size(), st));
     CKD(cudaMemcpyAsync(d_ncoll2, A.ncoll, sizeof(int), cudaMemcpyDeviceToDevice, st));
     CKD(cudaMemcpyAsync(d_coll2, A.coll, sizeof(int) * nco, cudaMemcpyDeviceToDevice, st));
-    for (int l = 1; l <= lev; l++)
-      k_ref_colleagues<<<grid_for(t.llast[l] - t.lfirst[l] + 1), 256, 0, st>>>(
-          d_lev2, l, (double)1.05f * bsz[l], nch, nco, dim, d_par2, d_nchild, d_child, d_cen2, d_ncoll2, d_coll2);
+    for (int l = 1; l <= lev; l++) {
+      const int g = grid_warps(t.llast[l] - t.lfirst[l] + 1);
+      if (dim == 2)
+        k_ref_colleagues<2><<<g, 256, 0, st>>>(d_lev2, l, (double)1.05f * bsz[l], nco, d_par2, d_child, d_cen2,
+                                               d_ncoll2, d_coll2);
+      else
+        k_ref_colleagues<3><<<g, 256, 0, st>>>(d_lev2, l, (double)1.05f * bsz[l], nco, d_par2, d_child, d_cen2,
+                                               d_ncoll2, d_coll2);
+    }
   }
   CKD(cudaGetLastError());
   t.nboxes = nb;
@@ -1229,9 +1446,10 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
   for (int l = 0; l < t.nlevels; l++) {
     const int a = t.lfirst[l], n = t.llast[l] - a + 1;
-    if (n > 0)
-      k_child_ranges<<<(n * nch + 255) / 256, 256, 0, st>>>(skey, dim * (L - 1 - l), nch, a, n, nullptr, d_child,
-                                                            r0, r1, 0, nullptr);
+    if (n <= 0) continue;
+    const int g = grid_warps((long long)n * (nch - 1));
+    if (dim == 2) k_child_bounds<2><<<g, 256, 0, st>>>(skey, dim * (L - 1 - l), a, n, d_child, r0, r1);
+    else k_child_bounds<3><<<g, 256, 0, st>>>(skey, dim * (L - 1 - l), a, n, d_child, r0, r1);
   }
   t.s0.assign(nb, 0);
   t.s1.assign(nb, 0);
@@ -1250,13 +1468,11 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(cudaEventRecord(ranges_done.e, st));
   // final order: leaf rank of each sorted position, to input order, stable sort
   {
-    int *lstart = nullptr, *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
-    CKD(S.get(&lstart, nleaf));
+    int *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
     CKD(S.get(&rk, ns));
     CKD(S.get(&rk2, ns));
     CKD(S.get(&idx, ns));
-    k_leaf_starts<<<(nleaf + 255) / 256, 256, 0, st>>>(r0, d_lor, nleaf, lstart);
-    k_position_rank<<<(ns + 255) / 256, 256, 0, st>>>(lstart, nleaf, wid, ns, rk, idx);
+    k_position_rank<<<grid_warps(nleaf), 256, 0, st>>>(r0, r1, d_lor, nleaf, wid, rk, idx);
     int bits = 1;
     while ((1 << bits) < nleaf) bits++;
     size_t tmp = 0;
