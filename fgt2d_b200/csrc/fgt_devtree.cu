@@ -788,6 +788,98 @@ __global__ void k_lr_scatter(int n, const int* __restrict__ map, int nch, int di
   }
 }
 
+// ---- modified list1 on the device (build_list1 in fgt_tree.cpp:
+// tree_routs4.f:715-879 in 2D, tree_routs3d.f:511-619 in 3D) ----
+// list(X) = [the symmetric entries b, in increasing id | X's own entries in
+// its loop order]; own entries are written by X's thread, symmetric ones
+// through per-box atomic cursors and then sorted (a handful per box).
+struct L1Tree {
+  const int *level, *par, *nchild, *child, *ncoll, *coll;
+  const double* cen;
+  const double* bsz;  // box size per level
+  int nch, nco, dim, npw;
+};
+template <class Own, class Sym>
+__device__ __forceinline__ void l1_visit(const L1Tree& T, int b, Own&& own, Sym&& sym) {
+  if (T.nchild[b] != 0) return;
+  const int l = T.level[b];
+  for (int i = 0; i < T.ncoll[b]; i++) {
+    const int jb = T.coll[(size_t)b * T.nco + i];
+    if (l >= T.npw || T.nchild[jb] == 0) {
+      own(jb);
+      continue;
+    }
+    const double dist = 1.05 * (T.bsz[l] + T.bsz[l + 1]) / 2.0;
+    for (int j = 0; j < T.nch; j++) {
+      const int kb = T.child[(size_t)jb * T.nch + j];
+      if (kb < 0) continue;
+      bool near = true;
+      for (int d = 0; d < T.dim; d++)
+        if (!(fabs(T.cen[(size_t)kb * T.dim + d] - T.cen[(size_t)b * T.dim + d]) < dist)) near = false;
+      if (near) {
+        own(kb);
+        if (T.dim == 2) sym(kb);
+      }
+    }
+  }
+  if (T.dim == 3) {  // coarser leaf neighbours: the parent's leaf colleagues
+    const int dad = T.par[b];
+    const double dist = 1.05 * (T.bsz[l] + T.bsz[l - 1]) / 2.0;
+    for (int i = 0; i < T.ncoll[dad]; i++) {
+      const int jb = T.coll[(size_t)dad * T.nco + i];
+      if (T.nchild[jb] != 0) continue;
+      bool near = true;
+      for (int d = 0; d < T.dim; d++)
+        if (!(fabs(T.cen[(size_t)jb * T.dim + d] - T.cen[(size_t)b * T.dim + d]) < dist)) near = false;
+      if (near) own(jb);
+    }
+  }
+}
+// counts over the visited boxes [b_lo, b_hi]; a leaf root lists itself
+__global__ void k_l1_count(L1Tree T, int b_lo, int b_hi, int* __restrict__ nown, int* __restrict__ nsym) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && T.nchild[0] == 0) nown[0] = 1;
+  for (int b = b_lo + blockIdx.x * blockDim.x + threadIdx.x; b <= b_hi; b += gridDim.x * blockDim.x) {
+    int n = 0;
+    l1_visit(T, b, [&](int) { n++; }, [&](int kb) { atomicAdd(nsym + kb, 1); });
+    nown[b] = n;
+  }
+}
+__global__ void k_l1_sum(int nb, const int* __restrict__ nown, const int* __restrict__ nsym, int* __restrict__ cnt) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += gridDim.x * blockDim.x)
+    cnt[b] = b < nb ? nown[b] + nsym[b] : 0;
+}
+__global__ void k_l1_fill(L1Tree T, int b_lo, int b_hi, const int* __restrict__ l1off, const int* __restrict__ nsym,
+                          int* __restrict__ scur, int* __restrict__ l1) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && T.nchild[0] == 0) l1[l1off[0] + nsym[0]] = 0;
+  for (int b = b_lo + blockIdx.x * blockDim.x + threadIdx.x; b <= b_hi; b += gridDim.x * blockDim.x) {
+    int pos = l1off[b] + nsym[b];
+    l1_visit(T, b, [&](int v) { l1[pos++] = v; }, [&](int kb) { l1[atomicAdd(scur + kb, 1)] = b; });
+  }
+}
+// the symmetric block of every list in increasing id (insertion sort)
+__global__ void k_l1_sortsym(int nb, const int* __restrict__ l1off, const int* __restrict__ nsym,
+                             int* __restrict__ l1) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    int* a = l1 + l1off[b];
+    const int n = nsym[b];
+    for (int i = 1; i < n; i++) {
+      const int v = a[i];
+      int j = i - 1;
+      while (j >= 0 && a[j] > v) {
+        a[j + 1] = a[j];
+        j--;
+      }
+      a[j + 1] = v;
+    }
+  }
+}
+// ifhung: the leaves with sources at levels 0 .. the cut (ids 0 .. s_hi)
+__global__ void k_l1_hung(int s_hi, const int* __restrict__ nchild, const int* __restrict__ s0,
+                          const int* __restrict__ s1, unsigned char* __restrict__ hung) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= s_hi; b += gridDim.x * blockDim.x)
+    hung[b] = nchild[b] == 0 && s1[b] - s0[b] > 0;
+}
+
 // ---- near-field task arrays on the device (the host's build_near_tasks) ----
 // (A, S) pairs of the list1 entries of the near-field source boxes S (levels
 // 0 .. the cut, ids 0 .. s_hi), in S-major order
@@ -1658,35 +1750,77 @@ cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
   const int nlevend = npl < P.nlevels ? npl : P.nlevels;
   const int s_hi = nlevend >= 0 ? t.llast[nlevend] : -1;
   const int set0 = P.ifpgh >= 1, set1 = P.ifpghtarg >= 1;
+  (void)L;
   Scratch S(st);
-  const int ne = L.l1off.empty() ? 0 : L.l1off[nb];
-  int *d_l1off = nullptr, *d_l1 = nullptr, *d_par = nullptr, *d_nch = nullptr, *d_s0 = nullptr, *d_s1 = nullptr,
-      *d_t0 = nullptr, *d_t1 = nullptr;
+  const int nch = t.nch, nco = t.nco, dim = t.dim, nlv = (int)t.boxsize.size();
+  int *d_par = nullptr, *d_nch = nullptr, *d_s0 = nullptr, *d_s1 = nullptr, *d_t0 = nullptr, *d_t1 = nullptr,
+      *d_level = nullptr, *d_child = nullptr, *d_ncoll = nullptr, *d_coll = nullptr;
+  double *d_cen = nullptr, *d_bsz = nullptr;
   unsigned char* d_hung = nullptr;
-  CKD(S.get(&d_l1off, nb + 1));
-  CKD(S.get(&d_l1, ne));
   CKD(S.get(&d_par, nb));
   CKD(S.get(&d_nch, nb));
   CKD(S.get(&d_s0, nb));
   CKD(S.get(&d_s1, nb));
   CKD(S.get(&d_t0, nb));
   CKD(S.get(&d_t1, nb));
+  CKD(S.get(&d_level, nb));
+  CKD(S.get(&d_child, (size_t)nb * nch));
+  CKD(S.get(&d_ncoll, nb));
+  CKD(S.get(&d_coll, (size_t)nb * nco));
+  CKD(S.get(&d_cen, (size_t)nb * dim));
+  CKD(S.get(&d_bsz, nlv + 1));
   CKD(S.get(&d_hung, nb));
   {
     const size_t i4 = sizeof(int) * (size_t)nb;
-    StagedBatch X(st, staged_bytes({i4 + 4, sizeof(int) * (size_t)ne, i4, i4, i4, i4, i4, i4, (size_t)nb}));
-    CKD(X.up(d_l1off, L.l1off.data(), (size_t)nb + 1));
-    CKD(X.up(d_l1, L.l1.data(), (size_t)ne));
+    StagedBatch X(st, staged_bytes({i4, i4, i4, i4, i4, i4, i4, i4 * nch, i4, i4 * nco, 8 * (size_t)nb * dim,
+                                    8 * (size_t)nlv}));
     CKD(X.up(d_par, t.parent.data(), nb));
     CKD(X.up(d_nch, t.nchild.data(), nb));
     CKD(X.up(d_s0, t.s0.data(), nb));
     CKD(X.up(d_s1, t.s1.data(), nb));
     CKD(X.up(d_t0, t.t0.data(), nb));
     CKD(X.up(d_t1, t.t1.data(), nb));
-    CKD(X.up(d_hung, L.ifhung.data(), nb));
+    CKD(X.up(d_level, t.level.data(), nb));
+    CKD(X.up(d_child, t.child.data(), (size_t)nb * nch));
+    CKD(X.up(d_ncoll, t.ncoll.data(), nb));
+    CKD(X.up(d_coll, t.coll.data(), (size_t)nb * nco));
+    CKD(X.up(d_cen, t.centers.data(), (size_t)nb * dim));
+    CKD(X.up(d_bsz, t.boxsize.data(), nlv));
     // the stage is reused below only after this batch's copies (finish)
     CKD(X.finish());
   }
+  // list1 of the boxes at levels 1 .. min(nlevels, cut) and the ifhung flags
+  const int lmax = std::min(t.nlevels, nlevend);
+  const int b_hi = lmax >= 1 ? t.llast[lmax] : -1, b_lo = t.nlevels >= 1 ? t.lfirst[1] : 1;
+  int *d_nown = nullptr, *d_nsym = nullptr, *d_l1cnt = nullptr, *d_l1off = nullptr, *d_l1 = nullptr,
+      *d_scur = nullptr;
+  CKD(S.get(&d_nown, nb));
+  CKD(S.get(&d_nsym, nb));
+  CKD(S.get(&d_l1cnt, nb + 1));
+  CKD(S.get(&d_l1off, nb + 1));
+  CKD(S.get(&d_scur, nb));
+  CKD(cudaMemsetAsync(d_nown, 0, sizeof(int) * nb, st));
+  CKD(cudaMemsetAsync(d_nsym, 0, sizeof(int) * nb, st));
+  L1Tree LT{d_level, d_par, d_nch, d_child, d_ncoll, d_coll, d_cen, d_bsz, nch, nco, dim, npl};
+  const int gv = (int)std::max<long long>(1, std::min<long long>(((long long)b_hi - b_lo + 1 + 255) / 256, 1184));
+  const int gb = (int)std::max<long long>(1, std::min<long long>(((long long)nb + 1 + 255) / 256, 1184));
+  k_l1_count<<<gv, 256, 0, st>>>(LT, b_lo, b_hi, d_nown, d_nsym);
+  k_l1_sum<<<gb, 256, 0, st>>>(nb, d_nown, d_nsym, d_l1cnt);
+  {
+    size_t tmp = 0;
+    CKD(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_l1cnt, d_l1off, nb + 1, st));
+    char* dt = nullptr;
+    CKD(S.get(&dt, tmp));
+    CKD(cub::DeviceScan::ExclusiveSum(dt, tmp, d_l1cnt, d_l1off, nb + 1, st));
+  }
+  int ne = 0;
+  CKD(cudaMemcpyAsync(&ne, d_l1off + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKD(cudaStreamSynchronize(st));
+  CKD(S.get(&d_l1, std::max(ne, 1)));
+  CKD(cudaMemcpyAsync(d_scur, d_l1off, sizeof(int) * nb, cudaMemcpyDeviceToDevice, st));
+  k_l1_fill<<<gv, 256, 0, st>>>(LT, b_lo, b_hi, d_l1off, d_nsym, d_scur, d_l1);
+  if (dim == 2) k_l1_sortsym<<<gb, 256, 0, st>>>(nb, d_l1off, d_nsym, d_l1);
+  if (s_hi >= 0) k_l1_hung<<<(s_hi + 256) / 256, 256, 0, st>>>(s_hi, d_nch, d_s0, d_s1, d_hung);
   // (A, S) pairs, stable sort by A: into[] = the S of each A in increasing id
   int *d_cnt = nullptr, *d_pfx = nullptr, *d_keyA = nullptr, *d_valS = nullptr, *d_keyA2 = nullptr,
       *d_into = nullptr, *d_cntA = nullptr, *d_ioff = nullptr;

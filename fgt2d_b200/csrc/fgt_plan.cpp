@@ -524,7 +524,7 @@ static void finish_plan(HostPlan& H) {
   Tree& t = H.tree;
   double t0 = now();
   t.npwlevel = P.npwlevel;
-  build_lists(t, H.lists);
+  build_lists(t, H.lists, !H.defer_near);
   double t1 = now();
   H.host_lists_s = t1 - t0;
   if (!P.all_direct) build_tables(H);

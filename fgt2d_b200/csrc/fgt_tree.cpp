@@ -632,10 +632,23 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
   if (dbg) fprintf(stderr, "tree: refine %.3f lr %.3f dfs %.3f sort_s %.3f sort_t %.3f\n", tB - tA, tC - tB, tD - tC, tE - tD, tF - tE);
 }
 
-void build_lists(const Tree& t, Lists& L) {
+static void build_list1(const Tree& t, Lists& L, int nb, int NCO, int NCH, int D, int npw, int nlevend);
+static void build_pw_lists(const Tree& t, Lists& L, int nb, int NCO, int D, int npw);
+
+void build_lists(const Tree& t, Lists& L, bool near) {
   int nb = t.nboxes, NCO = t.nco, NCH = t.nch, D = t.dim;
   int npw = t.npwlevel;
   int nlevend = npw < t.nlevels ? npw : t.nlevels;
+  if (near) build_list1(t, L, nb, NCO, NCH, D, npw, nlevend);
+  else {
+    L.ifhung.clear();
+    L.l1off.clear();
+    L.l1.clear();
+  }
+  build_pw_lists(t, L, nb, NCO, D, npw);
+}
+
+static void build_list1(const Tree& t, Lists& L, int nb, int NCO, int NCH, int D, int npw, int nlevend) {
   L.ifhung.assign(nb, 0);
   for (int l = 0; l <= nlevend; l++)
     for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
@@ -718,7 +731,9 @@ void build_lists(const Tree& t, Lists& L) {
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++)
     if (nsym[b] > 1) std::sort(L.l1.begin() + L.l1off[b], L.l1.begin() + L.l1off[b] + nsym[b]);
+}
 
+static void build_pw_lists(const Tree& t, Lists& L, int nb, int NCO, int D, int npw) {
   // plane-wave lists: the plan reads only the cut level's lists (mp -> loc;
   // merge and split take the children from the tree), so only those are
   // built: the colleagues other than the box itself (3D: the non-leaf ones),

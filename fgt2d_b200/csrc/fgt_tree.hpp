@@ -107,7 +107,9 @@ struct Lists {
   std::vector<int> pwoff, pw;
   std::vector<uint8_t> ifhung, iflocal;
 };
-void build_lists(const Tree& t, Lists& L);
+// near = false skips list1 and ifhung (a plan that builds its near-field
+// tasks on the GPU makes them there)
+void build_lists(const Tree& t, Lists& L, bool near = true);
 
 // Recomputes colleagues (computecoll) on a tree given from outside.
 void compute_colleagues(Tree& t);
