@@ -240,6 +240,11 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   // an unsharded plan builds its near-field task arrays on the GPU; a shard
   // filters them on the host
   p->H.defer_near = p->shard_n <= 1;
+  struct NearFree {
+    HostPlan& h;
+    cudaStream_t st;
+    ~NearFree() { device_near_free(h, st); }  // copied into the plan's arena, or abandoned
+  } nf{p->H, s};
   try {
     CKS(build_plan_device(p->H, dim, nd, delta, eps, ns, p->d_src, nt, d_trg, same, ifpgh, ifpghtarg,
                           d_isrc, d_itarg, s, ifcharge, ifdipole));
@@ -271,11 +276,6 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
     p->H.host_plan_s += now_s() - tn;
     if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "near-field tasks (device): %.4f\n", now_s() - tn);
   }
-  struct NearFree {
-    HostPlan& h;
-    cudaStream_t st;
-    ~NearFree() { device_near_free(h, st); }  // copied into the plan's arena, or abandoned
-  } nf{p->H, s};
   if (admit) {
     size_t bytes = 0;
     DevicePlan probe;

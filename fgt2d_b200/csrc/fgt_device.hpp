@@ -188,15 +188,20 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
 // Tree and plan with the point work of the tree build on the GPU
 // (fgt_devtree.cu).  d_src (ns, dim) and d_trg (nt, dim) are device arrays in
 // the caller's order (same: targets are the sources); the permutations
-// (position -> input index) are written to d_isrc / d_itarg.
+// (position -> input index) are written to d_isrc / d_itarg.  With keep, the
+// exact-key form leaves the finished tree's box arrays on the device there
+// (keep->mem non-null; the caller frees it on the stream).
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
-                              bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st);
-// Bounding box (per-dimension min / max) of device point arrays.
+                              bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st,
+                              HostPlan::DevTree* keep = nullptr);
 // The near-field task arrays of a built host plan on the GPU (H.dnear,
-// H.direct_pairs), in the order of the host's build; device_near_free
-// releases them (after device_plan_create has copied them).
+// H.direct_pairs), in the order of the host's build, with list1 built there
+// too (from H.dtree when the tree build left it, else from the host tree);
+// device_near_free releases them and H.dtree (after device_plan_create has
+// copied them).
 cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st);
 void device_near_free(HostPlan& H, cudaStream_t st);
+// Bounding box (per-dimension min / max) of device point arrays.
 cudaError_t build_plan_device_bbox(const double* d_src, int ns, const double* d_trg, int nt, int dim,
                                    double* mn, double* mx, cudaStream_t st);
 cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double eps, int ns,

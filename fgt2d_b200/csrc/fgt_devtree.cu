@@ -31,6 +31,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include "fgt_device.hpp"
 #include "fgt_plan.hpp"
@@ -296,22 +297,16 @@ __global__ void __launch_bounds__(256) k_child_bounds(const unsigned long long* 
   }
 }
 
-// Sort key of the final point order: the depth-first rank r of the leaf
-// whose key range [r0, r1) holds sorted position k, scattered to the
-// point's input index, with the input index as the value (a stable sort on
-// the rank keeps the input order inside a leaf).  One warp per leaf; the
-// leaves' ranges tile the sorted positions.
-__global__ void __launch_bounds__(256) k_position_rank(const int* __restrict__ r0, const int* __restrict__ r1,
-                                                       const int* __restrict__ leaf_of_rank, int nleaf,
-                                                       const int* __restrict__ wid, int* __restrict__ rk,
-                                                       int* __restrict__ idx) {
-  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nleaf; r += gridDim.x * wpb) {
-    const int leaf = leaf_of_rank[r], lo = r0[leaf], hi = r1[leaf];
-    for (int k = lo + lane; k < hi; k += 32) {
-      rk[wid[k]] = r;
-      idx[k] = k;
-    }
+// Key ranges [lb, le) of the leaves in depth-first order (the segments of
+// the final point order: input order inside each leaf, as pts_tree_sort)
+__global__ void k_leaf_bounds(const int* __restrict__ r0, const int* __restrict__ r1,
+                              const int* __restrict__ leaf_of_rank, int nleaf, int* __restrict__ lb,
+                              int* __restrict__ le) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nleaf) {
+    const int leaf = leaf_of_rank[r];
+    lb[r] = r0[leaf];
+    le[r] = r1[leaf];
   }
 }
 __global__ void k_root_range(int* r0, int* r1, int n) {
@@ -1170,7 +1165,8 @@ constexpr long long kKeyTreeMaxBoxes = 1LL << 24;
 // over the points per level, and the same tree, ranges and permutations as
 // the per-level refinement below.
 cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
-                                   bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st) {
+                                   bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg, cudaStream_t st,
+                                   HostPlan::DevTree* keep) {
   const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   const double tA = now_s();
   tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
@@ -1459,16 +1455,46 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   int *d_tab = nullptr, *d_map = nullptr, *d_nchild = nullptr, *d_child = nullptr, *d_par2 = nullptr,
       *d_level2 = nullptr, *d_ncoll2 = nullptr, *d_coll2 = nullptr, *d_lev2 = nullptr;
   double* d_cen2 = nullptr;
+  int *fr0 = nullptr, *fr1 = nullptr;  // the finished tree's key ranges
   CKD(S.get(&d_tab, tab.size()));
   CKD(S.get(&d_map, nb));
-  CKD(S.get(&d_nchild, nb));
-  CKD(S.get(&d_child, (size_t)nb * nch));
-  CKD(S.get(&d_par2, nb));
-  CKD(S.get(&d_level2, nb));
-  CKD(S.get(&d_cen2, (size_t)nb * dim));
-  CKD(S.get(&d_ncoll2, nb));
-  CKD(S.get(&d_coll2, (size_t)nb * nco));
   CKD(S.get(&d_lev2, 2 * nslot + 1));
+  if (keep) {  // one allocation that outlives this build
+    const size_t ib = (((size_t)nb * 4) + 255) & ~size_t(255);
+    const size_t bytes = ib * (7 + (size_t)nch + nco) + ((((size_t)nb * dim * 8) + 255) & ~size_t(255));
+    char* m = nullptr;
+    CKD(cudaMallocAsync(reinterpret_cast<void**>(&m), bytes, st));
+    keep->mem = m;
+    auto take = [&](size_t b) { char* p = m; m += (b + 255) & ~size_t(255); return p; };
+    d_level2 = reinterpret_cast<int*>(take((size_t)nb * 4));
+    d_par2 = reinterpret_cast<int*>(take((size_t)nb * 4));
+    d_nchild = reinterpret_cast<int*>(take((size_t)nb * 4));
+    d_ncoll2 = reinterpret_cast<int*>(take((size_t)nb * 4));
+    fr0 = reinterpret_cast<int*>(take((size_t)nb * 4));
+    fr1 = reinterpret_cast<int*>(take((size_t)nb * 4));
+    d_child = reinterpret_cast<int*>(take((size_t)nb * 4 * nch));
+    d_coll2 = reinterpret_cast<int*>(take((size_t)nb * 4 * nco));
+    d_cen2 = reinterpret_cast<double*>(take((size_t)nb * 8 * dim));
+    keep->level = d_level2;
+    keep->parent = d_par2;
+    keep->nchild = d_nchild;
+    keep->child = d_child;
+    keep->ncoll = d_ncoll2;
+    keep->coll = d_coll2;
+    keep->centers = d_cen2;
+    keep->s0 = fr0;
+    keep->s1 = fr1;
+  } else {
+    CKD(S.get(&d_nchild, nb));
+    CKD(S.get(&d_child, (size_t)nb * nch));
+    CKD(S.get(&d_par2, nb));
+    CKD(S.get(&d_level2, nb));
+    CKD(S.get(&d_cen2, (size_t)nb * dim));
+    CKD(S.get(&d_ncoll2, nb));
+    CKD(S.get(&d_coll2, (size_t)nb * nco));
+    CKD(S.get(&fr0, nb));
+    CKD(S.get(&fr1, nb));
+  }
   CKD(upload(d_tab, tab.data(), tab.size(), st));
   k_lr_map<<<grid_for(nb), 256, 0, st>>>(d_tab, (int)tab.size() / 3, nb, d_map);
   k_lr_scatter<<<grid_for(nb), 256, 0, st>>>(nb, d_map, nch, dim, A.level, A.par, A.nch, A.child, A.cen, d_level2,
@@ -1533,8 +1559,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(upload(d_lor, leaf_of_rank.data(), nleaf, st));
   // ranges of the finished tree (the level restriction added boxes and
   // renumbered), level by level from the root
-  CKD(S.get(&r0, nb));
-  CKD(S.get(&r1, nb));
+  r0 = fr0;
+  r1 = fr1;
   k_root_range<<<1, 1, 0, st>>>(r0, r1, ns);
   for (int l = 0; l < t.nlevels; l++) {
     const int a = t.lfirst[l], n = t.llast[l] - a + 1;
@@ -1558,20 +1584,18 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   } ranges_done;
   CKD(cudaEventCreateWithFlags(&ranges_done.e, cudaEventDisableTiming));
   CKD(cudaEventRecord(ranges_done.e, st));
-  // final order: leaf rank of each sorted position, to input order, stable sort
+  // final order: the input indices of every leaf's key range in increasing
+  // order (the leaves tile the sorted positions, in depth-first order)
   {
-    int *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
-    CKD(S.get(&rk, ns));
-    CKD(S.get(&rk2, ns));
-    CKD(S.get(&idx, ns));
-    k_position_rank<<<grid_warps(nleaf), 256, 0, st>>>(r0, r1, d_lor, nleaf, wid, rk, idx);
-    int bits = 1;
-    while ((1 << bits) < nleaf) bits++;
+    int *lb = nullptr, *le = nullptr;
+    CKD(S.get(&lb, nleaf));
+    CKD(S.get(&le, nleaf));
+    k_leaf_bounds<<<(nleaf + 255) / 256, 256, 0, st>>>(r0, r1, d_lor, nleaf, lb, le);
     size_t tmp = 0;
-    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
+    CKD(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, wid, d_isrc, ns, nleaf, lb, le, st));
     char* dtmp = nullptr;
     CKD(S.get(&dtmp, tmp));
-    CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
+    CKD(cub::DeviceSegmentedSort::SortKeys(dtmp, tmp, wid, d_isrc, ns, nleaf, lb, le, st));
   }
   const double tD = now_s();
   if (same && nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
@@ -1602,10 +1626,10 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
 
 cudaError_t build_tree_device(Tree& t, int dim, const double* d_src, int ns, const double* d_trg, int nt,
                               bool same, const TreeSetup& ts, int* d_isrc, int* d_itarg,
-                              cudaStream_t st) {
+                              cudaStream_t st, HostPlan::DevTree* keep) {
   if (ns > 0 && ts.nlmax >= 1 && ts.nlmax <= (dim == 2 ? 31 : 21) && !getenv("FGT_TREE_LEVELWISE") &&
       key_tree_capacity(ts, dim, ns, nullptr) <= kKeyTreeMaxBoxes)
-    return build_tree_device_keys(t, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st);
+    return build_tree_device_keys(t, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st, keep);
   const bool dbg = getenv("FGT_TREE_TIMING") != nullptr;
   const double tA = now_s();
   tree_init(t, dim, ts.bs0, ts.cen0, ts.nlmax);
@@ -1729,7 +1753,8 @@ cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double
     H.host_tree_s = now_s() - tstart;
     return cudaSuccess;
   }
-  CKD(build_tree_device(H.tree, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st));
+  CKD(build_tree_device(H.tree, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st,
+                        H.defer_near ? &H.dtree : nullptr));
   H.host_tree_s = now_s() - tstart;
   plan_end(H);
   return cudaSuccess;
@@ -1757,20 +1782,49 @@ cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
       *d_level = nullptr, *d_child = nullptr, *d_ncoll = nullptr, *d_coll = nullptr;
   double *d_cen = nullptr, *d_bsz = nullptr;
   unsigned char* d_hung = nullptr;
-  CKD(S.get(&d_par, nb));
-  CKD(S.get(&d_nch, nb));
-  CKD(S.get(&d_s0, nb));
-  CKD(S.get(&d_s1, nb));
-  CKD(S.get(&d_t0, nb));
-  CKD(S.get(&d_t1, nb));
-  CKD(S.get(&d_level, nb));
-  CKD(S.get(&d_child, (size_t)nb * nch));
-  CKD(S.get(&d_ncoll, nb));
-  CKD(S.get(&d_coll, (size_t)nb * nco));
-  CKD(S.get(&d_cen, (size_t)nb * dim));
   CKD(S.get(&d_bsz, nlv + 1));
   CKD(S.get(&d_hung, nb));
-  {
+  const HostPlan::DevTree& K = H.dtree;
+  const bool tsame = t.t0.size() == t.s0.size() && t.t1.size() == t.s1.size() &&
+                     std::memcmp(t.t0.data(), t.s0.data(), sizeof(int) * nb) == 0 &&
+                     std::memcmp(t.t1.data(), t.s1.data(), sizeof(int) * nb) == 0;
+  if (K.mem) {  // the tree build's arrays, still on the device
+    d_par = K.parent;
+    d_nch = K.nchild;
+    d_s0 = K.s0;
+    d_s1 = K.s1;
+    d_level = K.level;
+    d_child = K.child;
+    d_ncoll = K.ncoll;
+    d_coll = K.coll;
+    d_cen = K.centers;
+    if (tsame) {
+      d_t0 = d_s0;
+      d_t1 = d_s1;
+    } else {
+      CKD(S.get(&d_t0, nb));
+      CKD(S.get(&d_t1, nb));
+    }
+    StagedBatch X(st, staged_bytes({8 * (size_t)nlv, tsame ? 0 : sizeof(int) * (size_t)nb,
+                                    tsame ? 0 : sizeof(int) * (size_t)nb}));
+    CKD(X.up(d_bsz, t.boxsize.data(), nlv));
+    if (!tsame) {
+      CKD(X.up(d_t0, t.t0.data(), nb));
+      CKD(X.up(d_t1, t.t1.data(), nb));
+    }
+    CKD(X.finish());
+  } else {
+    CKD(S.get(&d_par, nb));
+    CKD(S.get(&d_nch, nb));
+    CKD(S.get(&d_s0, nb));
+    CKD(S.get(&d_s1, nb));
+    CKD(S.get(&d_t0, nb));
+    CKD(S.get(&d_t1, nb));
+    CKD(S.get(&d_level, nb));
+    CKD(S.get(&d_child, (size_t)nb * nch));
+    CKD(S.get(&d_ncoll, nb));
+    CKD(S.get(&d_coll, (size_t)nb * nco));
+    CKD(S.get(&d_cen, (size_t)nb * dim));
     const size_t i4 = sizeof(int) * (size_t)nb;
     StagedBatch X(st, staged_bytes({i4, i4, i4, i4, i4, i4, i4, i4 * nch, i4, i4 * nco, 8 * (size_t)nb * dim,
                                     8 * (size_t)nlv}));
@@ -1922,7 +1976,9 @@ cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
 
 void device_near_free(HostPlan& H, cudaStream_t st) {
   if (H.dnear.mem) cudaFreeAsync(H.dnear.mem, st);
+  if (H.dtree.mem) cudaFreeAsync(H.dtree.mem, st);
   H.dnear = HostPlan::DevNear();
+  H.dtree = HostPlan::DevTree();
 }
 
 }  // namespace fgtb

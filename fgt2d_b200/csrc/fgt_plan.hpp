@@ -108,6 +108,15 @@ struct HostPlan {
     void* mem = nullptr;
   } dnear;
   bool defer_near = false;  // finish_plan leaves the near-field arrays to the device build
+  // The finished tree's box arrays as the device build left them (final ids;
+  // kept for the near-field build when defer_near, else empty): one
+  // stream-ordered allocation, released with dnear.
+  struct DevTree {
+    int *level = nullptr, *parent = nullptr, *nchild = nullptr, *child = nullptr, *ncoll = nullptr,
+        *coll = nullptr, *s0 = nullptr, *s1 = nullptr;
+    double* centers = nullptr;
+    void* mem = nullptr;
+  } dtree;
   // statistics
   long long direct_pairs = 0;
   long long form_sources = 0, eval_points = 0;
