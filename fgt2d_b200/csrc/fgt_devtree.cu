@@ -1191,6 +1191,8 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     CKD(S.get(&dtmp, tmp));
     CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, key, skey, wid0, wid, ns, 0, dim * L, st));
   }
+  if (dbg) CKD(cudaStreamSynchronize(st));
+  const double tK = now_s();
   // refinement on source counts (idivflag = 0), pts_tree2d4.f:495-563: every
   // level on the device (flags, the refined boxes' ranks, the children and
   // their key ranges), no host round trip; the box arrays come back once
@@ -1619,8 +1621,10 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   }
   if (dbg) CKD(cudaStreamSynchronize(st));
   if (dbg)
-    fprintf(stderr, "device tree (keys): refine %.4f (%d levels, %d boxes) lr %.4f ranks+sort_s %.4f sort_t %.4f\n",
-            tB - tA, lev, nbr, tC - tB, tD - tC, now_s() - tD);
+    fprintf(stderr,
+            "device tree (keys): keys+sort %.4f refine %.4f (%d levels, %d boxes) lr %.4f ranks+sort_s %.4f "
+            "sort_t %.4f\n",
+            tK - tA, tB - tK, lev, nbr, tC - tB, tD - tC, now_s() - tD);
   return cudaGetLastError();
 }
 
@@ -1971,6 +1975,10 @@ cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
   H.direct_pairs = (long long)pairs;
   H.dir.clear();
   H.dir_src.clear();
+  if (H.dtree.mem) {  // the tree arrays are not read after this (stream-ordered release)
+    CKD(cudaFreeAsync(H.dtree.mem, st));
+    H.dtree = HostPlan::DevTree();
+  }
   return cudaGetLastError();
 }
 

@@ -6,8 +6,6 @@
 // near field are unchanged around them.
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
 #include "fgt_kcommon.cuh"
 
 namespace fgtb {
@@ -191,178 +189,109 @@ __global__ void __launch_bounds__(128) k_eval2d_horner_f32(KP k, const HornerTas
 // holds four targets as two packed pairs, so every subtraction, square and
 // accumulation serves two targets; a staged source is kept in shared memory
 // with each value twice, (s, s), ready as the other operand of a pair.
-//
-// Every warp runs a persistent loop over the tasks w, w + W, ... (W warps in
-// the grid) as a two-stage pipeline: while one task's sources are staged and
-// summed, the next task's targets and first source ranges and the descriptor
-// after it are already in flight, so a task exposes one memory latency (its
-// sources) instead of the chain descriptor -> targets and ranges -> sources
-// -> output.  The outputs are added with one atomic add per (target,
-// density): each target belongs to one task, so this is the same single
-// rounded addition as a read-modify-write.
-template <int DIM>
-struct DirTargets {
-  float2 th[2][DIM], tl[2][DIM];  // targets (4 tt, 4 tt + 1) and (4 tt + 2, 4 tt + 3): (hi, lo) pairs
-};
-__device__ __forceinline__ int dir_group(int n) {  // lanes per group of four targets
-  const int ngr = (n + 3) / 4;
-  int g = 1;
-  while (g * 2 * ngr <= 32) g *= 2;
-  return g;
-}
-template <int DIM>
-__device__ __forceinline__ void dir_load_targets(const KP& k, const DirTask& T, int lane, DirTargets<DIM>& X) {
-  const float* fp = T.set ? k.ftrg : k.fsrc;
-  const int tt = lane / dir_group(T.n);
-#pragma unroll
-  for (int p = 0; p < 2; p++) {
-    const int i0 = min(tt * 4 + 2 * p, T.n - 1), i1 = min(tt * 4 + 2 * p + 1, T.n - 1);
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      X.th[p][d] = make_float2(fp[(size_t)2 * DIM * (T.i0 + i0) + 2 * d], fp[(size_t)2 * DIM * (T.i0 + i1) + 2 * d]);
-      X.tl[p][d] = make_float2(fp[(size_t)2 * DIM * (T.i0 + i0) + 2 * d + 1],
-                               fp[(size_t)2 * DIM * (T.i0 + i1) + 2 * d + 1]);
-    }
-  }
-}
-__device__ __forceinline__ SrcRange dir_load_range(const SrcRange* __restrict__ ranges, const DirTask& T, int rc,
-                                                   int lane) {
-  SrcRange R{0, 0};
-  if (lane < min(32, T.cnt - rc)) R = ranges[T.off + rc + lane];
-  return R;
-}
-// the chunk of (at most 32) ranges whose entries the lanes hold
-__device__ __forceinline__ RangeChunk dir_chunk(const SrcRange& R, int nr, int lane) {
-  RangeChunk C;
-  C.nr = nr;
-  C.s0 = R.s0;
-  int inc = R.n;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(FULL_MASK, inc, o);
-    if (lane >= o) inc += v;
-  }
-  C.excl = inc - R.n;
-  C.tot = __shfl_sync(FULL_MASK, inc, 31);
-  return C;
-}
-
 template <int DIM>
 __global__ void __launch_bounds__(128) k_direct_mixed_x2(KP k, const DirTask* __restrict__ tasks, int ntask,
                                                          const SrcRange* __restrict__ ranges, float amax) {
   constexpr int CAP = 128;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 4 + warp;
   __shared__ float2 fsm[4][(2 * DIM + 1) * CAP];
-  const int W = gridDim.x * 4;
-  int w = blockIdx.x * 4 + warp;
   if (w >= ntask) return;  // whole warp leaves; no block-wide barrier below
+  const DirTask T = tasks[w];
   const int ind = blockIdx.y;
-  float2* sh = fsm[warp];       // [DIM][CAP] (hi, hi)
-  float2* sl = sh + DIM * CAP;  // [DIM][CAP] (lo, lo)
-  float2* sq = sl + DIM * CAP;  // [CAP] (q, q)
-  DirTask T = tasks[w];
-  DirTargets<DIM> X;
-  dir_load_targets<DIM>(k, T, lane, X);
-  SrcRange R = dir_load_range(ranges, T, 0, lane);
-  bool has_next = w + W < ntask;
-  DirTask Tn = has_next ? tasks[w + W] : T;
-  for (;;) {
-    // the next task's targets and first ranges, and the descriptor after it
-    DirTargets<DIM> Xn;
-    SrcRange Rn{0, 0};
-    const bool has_nn = w + 2 * W < ntask;
-    DirTask Tnn = Tn;
-    if (has_next) {
-      dir_load_targets<DIM>(k, Tn, lane, Xn);
-      Rn = dir_load_range(ranges, Tn, 0, lane);
-      if (has_nn) Tnn = tasks[w + 2 * W];
+  float2* sh = fsm[warp];          // [DIM][CAP] (hi, hi)
+  float2* sl = sh + DIM * CAP;     // [DIM][CAP] (lo, lo)
+  float2* sq = sl + DIM * CAP;     // [CAP] (q, q)
+  const int ngr = (T.n + 3) / 4;
+  int g = 1;
+  while (g * 2 * ngr <= 32) g *= 2;
+  const int tt = lane / g, sub = lane - tt * g;
+  const bool act = tt < ngr;
+  double* out = T.set ? k.pottarg : k.pot;
+  const int nc = T.set ? k.nc_t : k.nc_s;
+  const float* fp = T.set ? k.ftrg : k.fsrc;
+  float2 th[2][DIM], tl[2][DIM];  // targets (4 tt, 4 tt + 1) and (4 tt + 2, 4 tt + 3)
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    const int i0 = min(tt * 4 + 2 * p, T.n - 1), i1 = min(tt * 4 + 2 * p + 1, T.n - 1);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      th[p][d] = make_float2(fp[(size_t)2 * DIM * (T.i0 + i0) + 2 * d], fp[(size_t)2 * DIM * (T.i0 + i1) + 2 * d]);
+      tl[p][d] = make_float2(fp[(size_t)2 * DIM * (T.i0 + i0) + 2 * d + 1],
+                             fp[(size_t)2 * DIM * (T.i0 + i1) + 2 * d + 1]);
     }
-    const int ngr = (T.n + 3) / 4, g = dir_group(T.n);
-    const int tt = lane / g, sub = lane - tt * g;
-    const bool act = tt < ngr;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int rc = 0; rc < T.cnt; rc += 32) {
-      if (rc > 0) R = dir_load_range(ranges, T, rc, lane);
-      const RangeChunk C = dir_chunk(R, min(32, T.cnt - rc), lane);
-      for (int b0 = 0; b0 < C.tot; b0 += CAP) {
-        const int m = min(CAP, C.tot - b0);
-        int js[CAP / 32];
+  }
+  for (int rc = 0; rc < T.cnt; rc += 32) {
+    const RangeChunk C = load_range_chunk(ranges, T.off, T.cnt, rc, lane);
+    for (int b0 = 0; b0 < C.tot; b0 += CAP) {
+      const int m = min(CAP, C.tot - b0);
+      int js[CAP / 32];
 #pragma unroll
-        for (int u = 0; u < CAP / 32; u++) js[u] = range_slot_source(C, b0 + lane + 32 * u);
-        __syncwarp();
+      for (int u = 0; u < CAP / 32; u++) js[u] = range_slot_source(C, b0 + lane + 32 * u);
+      __syncwarp();
 #pragma unroll
-        for (int u = 0; u < CAP / 32; u++) {
-          const int t = lane + 32 * u;
-          if (t < m) {
-            const int j = js[u];
+      for (int u = 0; u < CAP / 32; u++) {
+        const int t = lane + 32 * u;
+        if (t < m) {
+          const int j = js[u];
 #pragma unroll
-            for (int d = 0; d < DIM; d++) {
-              const float2 hl = reinterpret_cast<const float2*>(k.fsrc)[(size_t)DIM * j + d];
-              sh[d * CAP + t] = make_float2(hl.x, hl.x);
-              sl[d * CAP + t] = make_float2(hl.y, hl.y);
-            }
-            const float q = (float)k.chg[(size_t)j * k.nd + ind];
-            sq[t] = make_float2(q, q);
+          for (int d = 0; d < DIM; d++) {
+            const float2 hl = reinterpret_cast<const float2*>(k.fsrc)[(size_t)DIM * j + d];
+            sh[d * CAP + t] = make_float2(hl.x, hl.x);
+            sl[d * CAP + t] = make_float2(hl.y, hl.y);
           }
+          const float q = (float)k.chg[(size_t)j * k.nd + ind];
+          sq[t] = make_float2(q, q);
         }
-        __syncwarp();
-        if (act) {
-          for (int t = sub; t < m; t += 4 * g) {
-            float2 part[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      }
+      __syncwarp();
+      if (act) {
+        for (int t = sub; t < m; t += 4 * g) {
+          float2 part[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-              const int tu = t + u * g;
-              if (tu < m) {
-                float2 sH[DIM], sL[DIM];
+          for (int u = 0; u < 4; u++) {
+            const int tu = t + u * g;
+            if (tu < m) {
+              float2 sH[DIM], sL[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) {
-                  sH[d] = sh[d * CAP + tu];
-                  sL[d] = sl[d * CAP + tu];
+              for (int d = 0; d < DIM; d++) {
+                sH[d] = sh[d * CAP + tu];
+                sL[d] = sl[d * CAP + tu];
+              }
+              const float2 q2 = sq[tu];
+#pragma unroll
+              for (int p = 0; p < 2; p++) {
+                float2 dd = fadd2(fsub2(th[p][0], sH[0]), fsub2(tl[p][0], sL[0]));
+                float2 a = fmul2(dd, dd);
+#pragma unroll
+                for (int d = 1; d < DIM; d++) {
+                  dd = fadd2(fsub2(th[p][d], sH[d]), fsub2(tl[p][d], sL[d]));
+                  a = ffma2(dd, dd, a);
                 }
-                const float2 q2 = sq[tu];
-#pragma unroll
-                for (int p = 0; p < 2; p++) {
-                  float2 dd = fadd2(fsub2(X.th[p][0], sH[0]), fsub2(X.tl[p][0], sL[0]));
-                  float2 a = fmul2(dd, dd);
-#pragma unroll
-                  for (int d = 1; d < DIM; d++) {
-                    dd = fadd2(fsub2(X.th[p][d], sH[d]), fsub2(X.tl[p][d], sL[d]));
-                    a = ffma2(dd, dd, a);
-                  }
-                  const float2 e = make_float2(a.x < amax ? ex2_approx(-a.x) : 0.f,
-                                               a.y < amax ? ex2_approx(-a.y) : 0.f);
-                  part[p] = ffma2(e, q2, part[p]);
-                }
+                const float2 e = make_float2(a.x < amax ? ex2_approx(-a.x) : 0.f,
+                                             a.y < amax ? ex2_approx(-a.y) : 0.f);
+                part[p] = ffma2(e, q2, part[p]);
               }
             }
-            acc[0] += (double)part[0].x;
-            acc[1] += (double)part[0].y;
-            acc[2] += (double)part[1].x;
-            acc[3] += (double)part[1].y;
           }
+          acc[0] += (double)part[0].x;
+          acc[1] += (double)part[0].y;
+          acc[2] += (double)part[1].x;
+          acc[3] += (double)part[1].y;
         }
-        __syncwarp();  // the staging rows are rewritten by the next batch
       }
     }
+  }
 #pragma unroll
-    for (int v = 0; v < 4; v++)
-      for (int o2 = 1; o2 < g; o2 <<= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o2);
-    if (act && sub == 0) {
-      double* out = T.set ? k.pottarg : k.pot;
-      const int nc = T.set ? k.nc_t : k.nc_s;
+  for (int v = 0; v < 4; v++)
+    for (int o2 = 1; o2 < g; o2 <<= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o2);
+  if (act && sub == 0) {
 #pragma unroll
-      for (int v = 0; v < 4; v++) {
-        const int it = tt * 4 + v;
-        if (it < T.n) atomicAdd(out + ((size_t)(T.i0 + it) * nc) * k.nd + ind, acc[v]);
-      }
+    for (int v = 0; v < 4; v++) {
+      const int it = tt * 4 + v;
+      if (it < T.n) out[((size_t)(T.i0 + it) * nc) * k.nd + ind] += acc[v];
     }
-    if (!has_next) break;
-    w += W;
-    T = Tn;
-    X = Xn;
-    R = Rn;
-    Tn = Tnn;
-    has_next = has_nn;
   }
 }
 
@@ -371,14 +300,7 @@ __global__ void __launch_bounds__(128) k_direct_mixed_x2(KP k, const DirTask* __
 cudaError_t launch_direct_mixed_x2(const KP& k, const DirTask* tasks, int ntask, int nd,
                                    const SrcRange* ranges, float amax, cudaStream_t st) {
   if (ntask <= 0) return cudaSuccess;
-  // persistent warps: as many CTAs as fit on the device at once
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (k.dim == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_direct_mixed_x2<2>, 128, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_direct_mixed_x2<3>, 128, 0);
-  const int resident = std::max(1, sms * std::max(per_sm, 1) / std::max(nd, 1));
-  const dim3 g(std::min((ntask + 3) / 4, resident), nd);
+  const dim3 g((ntask + 3) / 4, nd);
   if (k.dim == 2) k_direct_mixed_x2<2><<<g, 128, 0, st>>>(k, tasks, ntask, ranges, amax);
   else k_direct_mixed_x2<3><<<g, 128, 0, st>>>(k, tasks, ntask, ranges, amax);
   return cudaGetLastError();

@@ -230,12 +230,30 @@ static void build_tasks(HostPlan& H) {
   tq[nq++] = now();
   Params& P = H.P;
   const Tree& t = H.tree;
-  const Lists& L = H.lists;
-  int nb = t.nboxes, D = P.dim, nch = t.nch;
+  int nb = t.nboxes, D = P.dim, nch = t.nch, nco = t.nco;
   int npl = P.npwlevel, nls = P.nlevstart;
   auto relevant = [&](int b) {
     return (P.ifpghtarg > 0 ? t.nt(b) : 0) + (P.ifpgh > 0 ? t.ns(b) : 0);
   };
+  // the plane-wave list of a cut-level box (gt2d_computelistpw_slow /
+  // gt3d_computelistpw): its colleagues other than itself, in 3D the
+  // non-leaf ones, in colleague order
+  auto pw_keep = [&](int b, int jb) { return jb != b && (D == 2 || t.nchild[jb] > 0); };
+  // iflocal (fgt2d.f:790-814): a cut-level leaf with a non-leaf colleague
+  std::vector<uint8_t> ifl;
+  if (npl >= 0 && npl <= P.nlevels) {
+    const int a = t.lfirst[npl], z = t.llast[npl];
+    ifl.assign(z - a + 1, 0);
+#pragma omp parallel for schedule(static) if (z - a > 4096)
+    for (int b = a; b <= z; b++)
+      if (t.nchild[b] == 0)
+        for (int i = 0; i < t.ncoll[b]; i++)
+          if (t.nchild[t.coll[(size_t)b * nco + i]] > 0) {
+            ifl[b - a] = 1;
+            break;
+          }
+  }
+  auto iflocal = [&](int b) { return ifl[b - t.lfirst[npl]] != 0; };  // b at the cut level
   H.mp_slot.assign(nb, -1);
   H.loc_slot.assign(nb, -1);
   H.nmp = H.nloc = 0;
@@ -256,7 +274,7 @@ static void build_tasks(HostPlan& H) {
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
         bool leaf = t.nchild[b] == 0;
         if (t.ns(b) > 0 && !(leaf && l == npl)) H.mp_slot[b] = H.nmp++;
-        if (relevant(b) > 0 && !(leaf && l == npl && !L.iflocal[b])) H.loc_slot[b] = H.nloc++;
+        if (relevant(b) > 0 && !(leaf && l == npl && !iflocal(b))) H.loc_slot[b] = H.nloc++;
       }
     // (a) form, levels nlevels .. max(npwlevel+1, 0) (fgt2d.f:871)
     for (int l = P.nlevels; l >= std::max(npl + 1, 0); l--) {
@@ -301,7 +319,10 @@ static void build_tasks(HostPlan& H) {
       for (int b = a; b <= z; b++) {
         if (H.loc_slot[b] < 0) continue;
         int n = 0;
-        for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) n += H.mp_slot[L.pw[k]] >= 0;
+        for (int i = 0; i < t.ncoll[b]; i++) {
+          const int j = t.coll[(size_t)b * nco + i];
+          n += pw_keep(b, j) && H.mp_slot[j] >= 0;
+        }
         tix[b - a + 1] = 1;
         nix[b - a + 1] = n;
       }
@@ -316,9 +337,9 @@ static void build_tasks(HostPlan& H) {
         if (H.loc_slot[b] < 0) continue;
         int q = nix[b - a];
         M2LTask mt{H.loc_slot[b], H.mp_slot[b], q, 0};
-        for (int k = L.pwoff[b]; k < L.pwoff[b + 1]; k++) {
-          int j = L.pw[k];
-          if (H.mp_slot[j] < 0) continue;
+        for (int i = 0; i < t.ncoll[b]; i++) {
+          const int j = t.coll[(size_t)b * nco + i];
+          if (!pw_keep(b, j) || H.mp_slot[j] < 0) continue;
           int s = 0, mul = 1;
           for (int d = 0; d < D; d++) {
             int o = (int)std::lround((t.c(b, d) - t.c(j, d)) / xmin);
@@ -355,7 +376,7 @@ static void build_tasks(HostPlan& H) {
       }
       for (int b = t.lfirst[l]; b <= t.llast[l]; b++) {
         if (t.nchild[b] != 0 || H.loc_slot[b] < 0) continue;
-        if (l == npl && !L.iflocal[b]) continue;
+        if (l == npl && !iflocal(b)) continue;
         int route = pw ? ROUTE_PW : ROUTE_TAYLOR;
         if (D == 3 && pw && t.ns(b) + t.nt(b) >= 1000000) route = ROUTE_TAYLOR;
         // big leaves are cut into chunks so that no CTA serialises a
@@ -524,7 +545,8 @@ static void finish_plan(HostPlan& H) {
   Tree& t = H.tree;
   double t0 = now();
   t.npwlevel = P.npwlevel;
-  build_lists(t, H.lists, !H.defer_near);
+  if (H.defer_near) H.lists = Lists();  // list1 is built on the device with the near-field tasks
+  else build_lists(t, H.lists);
   double t1 = now();
   H.host_lists_s = t1 - t0;
   if (!P.all_direct) build_tables(H);

@@ -110,7 +110,8 @@ struct HostPlan {
   bool defer_near = false;  // finish_plan leaves the near-field arrays to the device build
   // The finished tree's box arrays as the device build left them (final ids;
   // kept for the near-field build when defer_near, else empty): one
-  // stream-ordered allocation, released with dnear.
+  // stream-ordered allocation, released by the near-field build (or with
+  // dnear when the plan's creation stops before it).
   struct DevTree {
     int *level = nullptr, *parent = nullptr, *nchild = nullptr, *child = nullptr, *ncoll = nullptr,
         *coll = nullptr, *s0 = nullptr, *s1 = nullptr;

@@ -632,23 +632,10 @@ void build_tree(Tree& t, int dim, const double* src, int ns, const double* trg, 
   if (dbg) fprintf(stderr, "tree: refine %.3f lr %.3f dfs %.3f sort_s %.3f sort_t %.3f\n", tB - tA, tC - tB, tD - tC, tE - tD, tF - tE);
 }
 
-static void build_list1(const Tree& t, Lists& L, int nb, int NCO, int NCH, int D, int npw, int nlevend);
-static void build_pw_lists(const Tree& t, Lists& L, int nb, int NCO, int D, int npw);
-
-void build_lists(const Tree& t, Lists& L, bool near) {
+void build_lists(const Tree& t, Lists& L) {
   int nb = t.nboxes, NCO = t.nco, NCH = t.nch, D = t.dim;
   int npw = t.npwlevel;
   int nlevend = npw < t.nlevels ? npw : t.nlevels;
-  if (near) build_list1(t, L, nb, NCO, NCH, D, npw, nlevend);
-  else {
-    L.ifhung.clear();
-    L.l1off.clear();
-    L.l1.clear();
-  }
-  build_pw_lists(t, L, nb, NCO, D, npw);
-}
-
-static void build_list1(const Tree& t, Lists& L, int nb, int NCO, int NCH, int D, int npw, int nlevend) {
   L.ifhung.assign(nb, 0);
   for (int l = 0; l <= nlevend; l++)
     for (int b = t.lfirst[l]; b <= t.llast[l]; b++)
@@ -731,45 +718,6 @@ static void build_list1(const Tree& t, Lists& L, int nb, int NCO, int NCH, int D
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < nb; b++)
     if (nsym[b] > 1) std::sort(L.l1.begin() + L.l1off[b], L.l1.begin() + L.l1off[b] + nsym[b]);
-}
-
-static void build_pw_lists(const Tree& t, Lists& L, int nb, int NCO, int D, int npw) {
-  // plane-wave lists: the plan reads only the cut level's lists (mp -> loc;
-  // merge and split take the children from the tree), so only those are
-  // built: the colleagues other than the box itself (3D: the non-leaf ones),
-  // counted and filled in parallel in colleague order
-  L.pwoff.assign(nb + 1, 0);
-  if (npw >= 0 && npw <= t.nlevels) {
-    const int a = t.lfirst[npw], z = t.llast[npw];
-    auto keep = [&](int b, int jb) { return jb != b && (D == 2 || t.nchild[jb] > 0); };
-#pragma omp parallel for schedule(static) if (z - a > 4096)
-    for (int b = a; b <= z; b++) {
-      int n = 0;
-      for (int i = 0; i < t.ncoll[b]; i++) n += keep(b, t.coll[(size_t)b * NCO + i]);
-      L.pwoff[b + 1] = n;
-    }
-    for (int b = a; b <= z; b++) L.pwoff[b + 1] += L.pwoff[b];
-    for (int b = z + 1; b < nb; b++) L.pwoff[b + 1] = L.pwoff[z + 1];
-    L.pw.assign(L.pwoff[nb], 0);
-#pragma omp parallel for schedule(static) if (z - a > 4096)
-    for (int b = a; b <= z; b++) {
-      int q = L.pwoff[b];
-      for (int i = 0; i < t.ncoll[b]; i++) {
-        const int jb = t.coll[(size_t)b * NCO + i];
-        if (keep(b, jb)) L.pw[q++] = jb;
-      }
-    }
-  } else {
-    L.pw.clear();
-  }
-
-  // iflocal: cut-level leaves with a non-leaf colleague (fgt2d.f:790-814)
-  L.iflocal.assign(nb, 0);
-  if (npw >= 0 && npw <= t.nlevels)
-    for (int b = t.lfirst[npw]; b <= t.llast[npw]; b++)
-      if (t.nchild[b] == 0)
-        for (int i = 0; i < t.ncoll[b]; i++)
-          if (t.nchild[t.coll[(size_t)b * NCO + i]] > 0) { L.iflocal[b] = 1; break; }
 }
 
 }  // namespace fgtb

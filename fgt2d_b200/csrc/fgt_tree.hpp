@@ -100,16 +100,13 @@ void tree_ranges(const Tree& t, const std::vector<int>& leafcount, const std::ve
 // Interaction lists used by the transform (fgt2dmain / fgt3dmain set-up).
 struct Lists {
   // modified list1 as CSR over boxes (compute_modified_list1); filled for
-  // the boxes at levels <= the cut, the only ones whose lists are read
+  // the boxes at levels <= the cut, the only ones whose lists are read.
+  // (The plane-wave lists of the cut level are the colleagues filtered
+  // where the far-field tasks are built.)
   std::vector<int> l1off, l1;
-  // plane-wave list (gt2d_computelistpw_slow / gt3d_computelistpw), CSR;
-  // filled at the cut level, the only level the plan reads
-  std::vector<int> pwoff, pw;
-  std::vector<uint8_t> ifhung, iflocal;
+  std::vector<uint8_t> ifhung;
 };
-// near = false skips list1 and ifhung (a plan that builds its near-field
-// tasks on the GPU makes them there)
-void build_lists(const Tree& t, Lists& L, bool near = true);
+void build_lists(const Tree& t, Lists& L);
 
 // Recomputes colleagues (computecoll) on a tree given from outside.
 void compute_colleagues(Tree& t);
