@@ -623,7 +623,7 @@ def serving_arm(args):
     base = {2: rng.random((nmax, 2)), 3: rng.random((nmax, 3))}
     chg = rng.random(nmax)
     srv = F.Server(0, max_bytes=args.server_bytes, workers=args.workers, precision="auto",
-                   sm_budget=args.server_sm_budget)
+                   sm_budget=args.server_sm_budget, grid_yield=args.server_grid_yield)
     # warm-up: one small request of each dimension (module load, first launches)
     for d in (2, 3):
         srv.wait(srv.submit(d, 1, 1e-3, 1e-6, base[d][:2000], chg[:2000]))
@@ -668,7 +668,7 @@ def serving_arm(args):
         "failures": [[int(k), int(status[k]), int(dims[k]), int(ns[k]), float(deltas[k]), float(epss[k])]
                      for k in np.flatnonzero(~ok)[:8]],
         "points_per_s": pts / span, "span_s": span,
-        "arrival_rate_per_s": rate, "workers": args.workers, "sm_budget": args.server_sm_budget,
+        "arrival_rate_per_s": rate, "workers": args.workers, "sm_budget": args.server_sm_budget, "grid_yield": args.server_grid_yield,
         "peak_device_bytes": st["peak_bytes"],
         "budget_device_bytes": st["budget_bytes"], "data": "synthetic (seeded numpy)",
         "config": {"workload": "serving stream: Poisson arrivals, dim in {2,3}, N log-uniform [1e3,1e6] "
@@ -698,6 +698,8 @@ def main():
     ap.add_argument("--server-bytes", type=int, default=0, help="serving workload: device budget (0: 80%% free)")
     ap.add_argument("--server-sm-budget", type=int, default=0,
                     help="serving workload: SMs a request's persistent kernels use (0: all)")
+    ap.add_argument("--server-grid-yield", action="store_true",
+                    help="serving workload: one CTA per task instead of persistent CTAs")
     args = ap.parse_args()
     if args.workload == "serving":
         return serving_arm(args)

@@ -97,11 +97,13 @@ def lib():
     L.fgt_ctx_set_host_threads.argtypes = [_vp, i]
     L.fgt_ctx_set_tree.argtypes = [_vp, i]
     L.fgt_ctx_set_sm_budget.argtypes = [_vp, i]
+    L.fgt_ctx_set_grid_yield.argtypes = [_vp, i]
     L.fgt_ctx_set_scheme.argtypes = [_vp, i]
     L.fgt_plan_expansion.argtypes = [_vp, i, i, ctypes.POINTER(ctypes.c_double)]
     L.fgt_server_create.argtypes = [i, ctypes.c_longlong, i, ctypes.POINTER(_vp)]
     L.fgt_server_set_precision.argtypes = [_vp, i]
     L.fgt_server_set_sm_budget.argtypes = [_vp, i]
+    L.fgt_server_set_grid_yield.argtypes = [_vp, i]
     L.fgt_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
     L.fgt_server_wait.argtypes = [_vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)]
     L.fgt_server_stats_get.argtypes = [_vp, ctypes.POINTER(ServerStats)]
@@ -195,6 +197,10 @@ class Context:
     def set_sm_budget(self, sms):
         """SMs the persistent kernels of plans created afterwards size their grids for (0: all)."""
         _check(lib().fgt_ctx_set_sm_budget(self._h, int(sms)), "fgt_ctx_set_sm_budget")
+
+    def set_grid_yield(self, on):
+        """One CTA per task instead of persistent CTAs (plans created afterwards)."""
+        _check(lib().fgt_ctx_set_grid_yield(self._h, int(bool(on))), "fgt_ctx_set_grid_yield")
 
     def set_precision(self, precision):
         p = _PREC[precision] if isinstance(precision, str) else int(precision)
@@ -485,7 +491,7 @@ class Server:
     """Transform server on one device (continuous batching of independent
     requests over worker streams, admission by device-memory footprint)."""
 
-    def __init__(self, device=0, max_bytes=0, workers=4, precision="auto", sm_budget=0):
+    def __init__(self, device=0, max_bytes=0, workers=4, precision="auto", sm_budget=0, grid_yield=False):
         L = lib()
         h = _vp()
         _check(L.fgt_server_create(int(device), int(max_bytes), int(workers), ctypes.byref(h)),
@@ -494,6 +500,7 @@ class Server:
         p = _PREC[precision] if isinstance(precision, str) else int(precision)
         _check(L.fgt_server_set_precision(h, p), "fgt_server_set_precision")
         _check(L.fgt_server_set_sm_budget(h, int(sm_budget)), "fgt_server_set_sm_budget")
+        _check(L.fgt_server_set_grid_yield(h, int(bool(grid_yield))), "fgt_server_set_grid_yield")
         self._live = {}
 
     def submit(self, dim, nd, delta, eps, sources, charge, targ=None, ifpgh=1, ifpghtarg=0,

@@ -33,6 +33,7 @@ struct fgt_ctx {
   int tree = FGT_TREE_DEVICE;
   int nthreads = 0;
   int sm_budget = 0;  // SMs the persistent kernels of this context's plans size their grids for (0: all)
+  bool yield_grids = false;  // one CTA per task where a kernel allows it (DevicePlan::yield_grids)
   int scheme = FGT_SCHEME_PLANEWAVE;  // the algorithm of the context's plans
   // uploads of a one-shot call's source strengths: they follow the points on
   // the copy engine while the tree build runs on `stream`
@@ -204,6 +205,7 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
     CKS(device_plan_create(p->H, p->D));
     p->have_device = true;
     p->D.persist_sms = p->ctx->sm_budget;
+  p->D.yield_grids = p->ctx->yield_grids;
     CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, st));
   }
   return FGT_OK;
@@ -286,6 +288,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   CKS(device_plan_create(p->H, p->D, d_isrc, d_itarg, s));
   p->have_device = true;
   p->D.persist_sms = p->ctx->sm_budget;
+  p->D.yield_grids = p->ctx->yield_grids;
   CKS(device_plan_set_points(p->D, p->d_src, p->d_trg, s));
   CKS(cudaStreamSynchronize(s));
   if (getenv("FGT_TREE_TIMING"))
@@ -540,6 +543,11 @@ int fgt_ctx_set_scheme(fgt_ctx* c, int scheme) {
 int fgt_ctx_set_sm_budget(fgt_ctx* c, int sms) {
   if (!c || sms < 0) return FGT_ERR_BADARG;
   c->sm_budget = sms;
+  return FGT_OK;
+}
+int fgt_ctx_set_grid_yield(fgt_ctx* c, int on) {
+  if (!c) return FGT_ERR_BADARG;
+  c->yield_grids = on != 0;
   return FGT_OK;
 }
 int fgt_ctx_set_host_threads(fgt_ctx* c, int nthreads) {
@@ -1629,6 +1637,15 @@ int fgt_server_set_sm_budget(fgt_server* s, int sms) {
   if (!s || sms < 0) return FGT_ERR_BADARG;
   for (fgt_ctx* c : s->ctxs) {
     int st = fgt_ctx_set_sm_budget(c, sms);
+    if (st != FGT_OK) return st;
+  }
+  return FGT_OK;
+}
+
+int fgt_server_set_grid_yield(fgt_server* s, int on) {
+  if (!s) return FGT_ERR_BADARG;
+  for (fgt_ctx* c : s->ctxs) {
+    int st = fgt_ctx_set_grid_yield(c, on);
     if (st != FGT_OK) return st;
   }
   return FGT_OK;

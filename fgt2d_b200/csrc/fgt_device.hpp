@@ -168,6 +168,14 @@ struct DevicePlan {
   // to the requests that arrive while they run
   int persist_sms = 0;
   int psm() const { return persist_sms > 0 && persist_sms < sm_count ? persist_sms : sm_count; }
+  // One CTA per task instead of persistent CTAs, in the kernels whose CTAs
+  // hold no per-CTA scratch: CTAs of other streams (a server's small
+  // requests, on higher-priority streams) are then scheduled as soon as any
+  // CTA of this plan finishes, not after the whole launch.
+  bool yield_grids = false;
+  int pgrid(int ntask, int per_sm) const {
+    return yield_grids ? ntask : (ntask < psm() * per_sm ? ntask : psm() * per_sm);
+  }
   // statistics copied from the host plan
   long long direct_pairs = 0, form_sources = 0, eval_points = 0;
   long long launches = 0;

@@ -31,7 +31,6 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
-#include <cub/device/device_segmented_sort.cuh>
 
 #include "fgt_device.hpp"
 #include "fgt_plan.hpp"
@@ -297,16 +296,24 @@ __global__ void __launch_bounds__(256) k_child_bounds(const unsigned long long* 
   }
 }
 
-// Key ranges [lb, le) of the leaves in depth-first order (the segments of
-// the final point order: input order inside each leaf, as pts_tree_sort)
-__global__ void k_leaf_bounds(const int* __restrict__ r0, const int* __restrict__ r1,
-                              const int* __restrict__ leaf_of_rank, int nleaf, int* __restrict__ lb,
-                              int* __restrict__ le) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nleaf) {
-    const int leaf = leaf_of_rank[r];
-    lb[r] = r0[leaf];
-    le[r] = r1[leaf];
+// Sort key of the final point order: the depth-first rank r of the leaf
+// whose key range [r0, r1) holds sorted position k, scattered to the
+// point's input index, with the input index as the value (a stable sort on
+// the rank keeps the input order inside a leaf).  One warp per leaf; the
+// leaves' ranges tile the sorted positions.  (A segmented sort of each
+// leaf's input indices is slower: the leaves of clustered inputs hold
+// thousands of points, and large segments are sorted one block each.)
+__global__ void __launch_bounds__(256) k_position_rank(const int* __restrict__ r0, const int* __restrict__ r1,
+                                                       const int* __restrict__ leaf_of_rank, int nleaf,
+                                                       const int* __restrict__ wid, int* __restrict__ rk,
+                                                       int* __restrict__ idx) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < nleaf; r += gridDim.x * wpb) {
+    const int leaf = leaf_of_rank[r], lo = r0[leaf], hi = r1[leaf];
+    for (int k = lo + lane; k < hi; k += 32) {
+      rk[wid[k]] = r;
+      idx[k] = k;
+    }
   }
 }
 __global__ void k_root_range(int* r0, int* r1, int n) {
@@ -1586,18 +1593,20 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   } ranges_done;
   CKD(cudaEventCreateWithFlags(&ranges_done.e, cudaEventDisableTiming));
   CKD(cudaEventRecord(ranges_done.e, st));
-  // final order: the input indices of every leaf's key range in increasing
-  // order (the leaves tile the sorted positions, in depth-first order)
+  // final order: leaf rank of each sorted position, to input order, stable sort
   {
-    int *lb = nullptr, *le = nullptr;
-    CKD(S.get(&lb, nleaf));
-    CKD(S.get(&le, nleaf));
-    k_leaf_bounds<<<(nleaf + 255) / 256, 256, 0, st>>>(r0, r1, d_lor, nleaf, lb, le);
+    int *rk = nullptr, *rk2 = nullptr, *idx = nullptr;
+    CKD(S.get(&rk, ns));
+    CKD(S.get(&rk2, ns));
+    CKD(S.get(&idx, ns));
+    k_position_rank<<<grid_warps(nleaf), 256, 0, st>>>(r0, r1, d_lor, nleaf, wid, rk, idx);
+    int bits = 1;
+    while ((1 << bits) < nleaf) bits++;
     size_t tmp = 0;
-    CKD(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, wid, d_isrc, ns, nleaf, lb, le, st));
+    CKD(cub::DeviceRadixSort::SortPairs(nullptr, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
     char* dtmp = nullptr;
     CKD(S.get(&dtmp, tmp));
-    CKD(cub::DeviceSegmentedSort::SortKeys(dtmp, tmp, wid, d_isrc, ns, nleaf, lb, le, st));
+    CKD(cub::DeviceRadixSort::SortPairs(dtmp, tmp, rk, rk2, idx, d_isrc, ns, 0, bits, st));
   }
   const double tD = now_s();
   if (same && nt > 0) CKD(cudaMemcpyAsync(d_itarg, d_isrc, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));

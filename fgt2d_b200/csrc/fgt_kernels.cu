@@ -4055,7 +4055,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const FormTask* ft = D.form + G.beg;
         const int* cb = D.fcbeg + G.beg;
         // persistent CTAs: as many as fit on the SMs at once
-        const dim3 pg(std::min(ntk, D.psm() * (ks * mt <= 4 && 2 * (sh + 1024) <= 228 * 1024 ? 2 : 1)), nd);
+        const dim3 pg(D.pgrid(ntk, ks * mt <= 4 && 2 * (sh + 1024) <= 228 * 1024 ? 2 : 1), nd);
         if (ks <= 4 && mt <= 4 && sh <= 227 * 1024) {
           switch (4 * (ks - 1) + mt - 1) {
 #define H2PW_CASE(KS_, MT_)                                                                        \
@@ -4212,7 +4212,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const int n2 = P.npw / 2, ksm = (n2 + 3) / 4;
         const size_t shm = C3Dims(Pn, P.npw).total * 8;
         if (Pn <= 16 && ksm <= 8 && shm <= 227 * 1024) {
-          const dim3 pg(std::min(nt, D.psm() * (2 * (shm + 1024) <= 228 * 1024 ? 2 : 1)), nd);
+          const dim3 pg(D.pgrid(nt, 2 * (shm + 1024) <= 228 * 1024 ? 2 : 1), nd);
           switch (ksm) {
 #define CONV3M_CASE(N)                                                                            \
   case N:                                                                                         \
@@ -4231,7 +4231,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         while (gs2 > 1 && C3Dims2(Pn, P.npw, gs2).total * 8 > 227 * 1024) gs2 >>= 1;
         const size_t shm2 = C3Dims2(Pn, P.npw, gs2).total * 8;
         if (Pn > 16 && Pn <= 32 && ksm <= 8 && shm2 <= 227 * 1024) {
-          const dim3 pg(std::min(nt, D.psm()), nd);
+          const dim3 pg(D.pgrid(nt, 1), nd);
           switch (ksm) {
 #define CONV3M2_CASE(N)                                                                           \
   case N:                                                                                         \

@@ -103,6 +103,12 @@ int fgt_ctx_set_tree(fgt_ctx* ctx, int where);
  * budget leaves SMs free for work that arrives while a large transform runs
  * (fgt_server_set_sm_budget).  No counterpart in the reference. */
 int fgt_ctx_set_sm_budget(fgt_ctx* ctx, int sms);
+/* on != 0: the context's plans (created after the call) launch one CTA per
+ * task, instead of persistent CTAs, in the kernels that allow it, so that a
+ * large transform's launches let work on other (higher-priority) streams
+ * onto the SMs as soon as any of their CTAs finish.  Default off.  No
+ * counterpart in the reference. */
+int fgt_ctx_set_grid_yield(fgt_ctx* ctx, int on);
 /* the algorithm of the plans created after the call (FGT_SCHEME_*): the
  * reference selects it by building 2d/planewave or 2d/nufft (3D likewise),
  * whose fgt2d / fgt3d share one signature (2d/nufft/src/fgt2d.f:19-22). */
@@ -366,6 +372,8 @@ int fgt_server_set_precision(fgt_server* server, int precision);
 /* SMs the persistent kernels of the requests planned afterwards size their
  * grids for (0, the default: every SM); see fgt_ctx_set_sm_budget. */
 int fgt_server_set_sm_budget(fgt_server* server, int sms);
+/* fgt_ctx_set_grid_yield for the requests planned afterwards */
+int fgt_server_set_grid_yield(fgt_server* server, int on);
 int fgt_server_submit(fgt_server* server, const fgt_request* request, long long* id);
 /* blocks until request id completes; returns its status (and frees its id) */
 int fgt_server_wait(fgt_server* server, long long id, double* latency_s);
