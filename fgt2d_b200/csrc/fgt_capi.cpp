@@ -1499,8 +1499,17 @@ int server_run(fgt_server* S, fgt_ctx* ctx, const fgt_request& r) {
   return st;
 }
 
+// points of a request (sources and targets it carries)
+long long job_points(const fgt_server::Job* J) { return (long long)J->r.ns + (J->r.targ ? J->r.nt : 0); }
+
 void server_worker(fgt_server* S, int w) {
   fgt_ctx* ctx = S->ctxs[w];
+  // the first quarter of the workers (at least one when there are two or
+  // more) take only small requests, so that those never wait on the host for
+  // a worker that holds a large one
+  const int nsmall = S->ctxs.size() >= 2 ? std::max<int>(1, (int)S->ctxs.size() / 4) : 0;
+  const bool small_only = w < nsmall;
+  auto takeable = [&](const fgt_server::Job* J) { return !small_only || job_points(J) <= kServerSmall; };
   // the workers share the host cores: each builds its host-side plan parts
   // with its share of them
   omp_set_num_threads(std::max(1, omp_get_num_procs() / (int)S->ctxs.size()));
@@ -1508,13 +1517,20 @@ void server_worker(fgt_server* S, int w) {
     fgt_server::Job* J = nullptr;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_q.wait(lk, [&] { return S->stop || !S->queue.empty(); });
-      if (S->queue.empty()) return;  // stop requested and nothing left
+      auto any = [&] {
+        for (const fgt_server::Job* J : S->queue)
+          if (takeable(J)) return true;
+        return false;
+      };
+      S->cv_q.wait(lk, [&] { return S->stop || any(); });
+      if (!any()) return;  // stop requested and nothing left for this worker
       const double t = now_s();
       size_t pick = 0;
-      for (size_t k = 1; k < S->queue.size(); k++) {
+      while (!takeable(S->queue[pick])) pick++;
+      for (size_t k = pick + 1; k < S->queue.size(); k++) {
         const fgt_server::Job* a = S->queue[k];
         const fgt_server::Job* b = S->queue[pick];
+        if (!takeable(a)) continue;
         const bool a_old = t - a->t_sub > kServerAgeS, b_old = t - b->t_sub > kServerAgeS;
         if (a_old != b_old ? a_old
                            : (a_old ? a->t_sub < b->t_sub
@@ -1528,7 +1544,7 @@ void server_worker(fgt_server* S, int w) {
     }
     // small requests run on the worker's high-priority stream
     const cudaStream_t base = ctx->stream;
-    const bool on_hi = (long long)J->r.ns + (J->r.targ ? J->r.nt : 0) <= kServerSmall && S->hi[w];
+    const bool on_hi = job_points(J) <= kServerSmall && S->hi[w];
     if (on_hi) ctx->stream = S->hi[w];
     int st = server_run(S, ctx, J->r);
     for (int retry = 0; st == FGT_ERR_NOMEM && retry < 50; retry++) {
@@ -1668,7 +1684,7 @@ int fgt_server_submit(fgt_server* s, const fgt_request* req, long long* id) {
   s->queue.push_back(J);
   s->submitted++;
   *id = J->id;
-  s->cv_q.notify_one();
+  s->cv_q.notify_all();  // a worker that takes only small requests may not take this one
   return FGT_OK;
 }
 

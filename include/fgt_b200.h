@@ -330,7 +330,9 @@ int fgt_host_tree_destroy(fgt_host_tree* t);
  * device accepts transforms of any dimension, size, delta and eps as they
  * arrive and runs them on worker threads, each with its own stream, so
  * requests that arrive while others are on the GPU overlap with them.  The
- * smallest pending request goes first (the oldest once it has waited 50 ms).
+ * smallest pending request goes first (the oldest once it has waited 50 ms);
+ * a quarter of the workers (at least one of two or more) take only requests
+ * of at most 1e5 points, and those run on high-priority streams.
  * Device memory is admitted by footprint: a quarter of max_device_bytes for
  * the requests' point arrays and tree scratch, the rest for their plans,
  * whose exact size is known before allocation; a request that does not fit
