@@ -1561,6 +1561,10 @@ void server_worker(fgt_server* S, int w) {
       st = server_run(S, ctx, J->r);
     }
     ctx->stream = base;
+    if (st == FGT_ERR_CUDA)  // an internal failure: say which
+      fprintf(stderr, "fgt server: request %lld (dim %d, %d + %d points, delta %g, eps %g) failed: CUDA error %d (%s)\n",
+              J->id, J->r.dim, J->r.ns, J->r.targ ? J->r.nt : 0, J->r.delta, J->r.eps, g_last_cuda,
+              cudaGetErrorName((cudaError_t)g_last_cuda));
     {
       std::lock_guard<std::mutex> lk(S->mu);
       S->running--;

@@ -1134,7 +1134,10 @@ cudaError_t sort_points_device(const Tree& t, const double* d_x, int n, const in
   CKD(cudaMemcpyAsync(lc.data(), cnt, sizeof(int) * nleaf, cudaMemcpyDeviceToHost, st));
   CKD(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKD(cudaStreamSynchronize(st));
-  if (herr) return cudaErrorLaunchFailure;
+  if (herr) {
+    fprintf(stderr, "fgt device tree: a point did not reach a leaf (%d points)\n", n);
+    return cudaErrorLaunchFailure;
+  }
   tree_ranges(t, lc, leaf_of_rank, r0, r1);
   return cudaGetLastError();
 }
@@ -1264,7 +1267,11 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
   CKD(cudaMemcpyAsync(hlev.data(), dlev, sizeof(int) * hlev.size(), cudaMemcpyDeviceToHost, st));
   CKD(cudaStreamSynchronize(st));
   const int nbr = hlev[2 * nslot];
-  if (nbr > cap) return cudaErrorLaunchFailure;
+  if (nbr > cap) {
+    fprintf(stderr, "fgt device tree: %d boxes exceed the capacity %lld (%d sources, %d levels)\n", nbr, cap, ns,
+            ts.nlmax);
+    return cudaErrorLaunchFailure;
+  }
   int lev = 0;
   while (lev + 1 <= ts.nlmax && hlev[2 * (lev + 1) + 1] >= hlev[2 * (lev + 1)]) lev++;
   const double tB = now_s();
@@ -1439,7 +1446,10 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     int lr_err = 0;
     CKD(cudaMemcpyAsync(&lr_err, d_tot + 60, sizeof(int), cudaMemcpyDeviceToHost, st));
     CKD(cudaStreamSynchronize(st));
-    if (lr_err) return cudaErrorLaunchFailure;
+    if (lr_err) {
+      fprintf(stderr, "fgt device tree: level restriction child id out of range (%d boxes, %d sources)\n", nbc, ns);
+      return cudaErrorLaunchFailure;
+    }
   }
   // final numbering: per level the original boxes, then each pass's
   std::vector<int> tab, nlevb(lev + 1, 0);
@@ -1458,7 +1468,10 @@ cudaError_t build_tree_device_keys(Tree& t, int dim, const double* d_src, int ns
     }
     std::sort(rows.begin(), rows.end());
     for (auto& r : rows) tab.insert(tab.end(), {r[0], r[1], r[2]});
-    if (fin != nbc) return cudaErrorLaunchFailure;
+    if (fin != nbc) {
+      fprintf(stderr, "fgt device tree: renumbering covers %d of %d boxes (%d sources)\n", fin, nbc, ns);
+      return cudaErrorLaunchFailure;
+    }
   }
   const int nb = nbc;
   int *d_tab = nullptr, *d_map = nullptr, *d_nchild = nullptr, *d_child = nullptr, *d_par2 = nullptr,

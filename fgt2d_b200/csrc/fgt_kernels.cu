@@ -1166,10 +1166,14 @@ void build_conv_table(const HostPlan& H, int Pn, std::vector<double>& out) {
     }
 }
 
+// With f32, each coefficient is stored as the FP32 pair (c, c) in its FP64
+// slot instead (the layout k_eval2d_horner_f32 reads: a row's float4 m holds
+// (c_2m, c_2m, c_2m+1, c_2m+1)), so the mixed evaluation needs no
+// conversion pass of its own.
 template <int KS>  // pass A depth in steps of 4: KS = ceil(n2 / 4)
 __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __restrict__ tasks, int ntask,
                                                      double* __restrict__ lo_all,
-                                                     const double* __restrict__ tab) {
+                                                     const double* __restrict__ tab, int f32) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int t = blockIdx.x * nw + warp;
   if (t >= ntask) return;  // no CTA-wide barrier in this kernel
@@ -1224,17 +1228,22 @@ __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __res
   __syncwarp();
   // pass B: 2 Re(i^k1 ...) = 2 {x, -y, -x, y}[k1 mod 4]
   double* out = lo_all + T.off + (size_t)ind * Pn * E;
+  float2* out2 = reinterpret_cast<float2*>(out);
+  auto put = [&](int e, double v) {
+    if (f32) out2[e] = make_float2((float)v, (float)v);
+    else out[e] = v;
+  };
   warp_gemm<true>(AE, Z.ldA2, BE, Z.ldB2, AO, BO, Z.M2 / 8, Z.N2 / 8, KS,  // A through L1
                   [&](int i, int k2, double e0, double e1, double o0, double o1) {
                     const double se = (i & 1) ? -2.0 : 2.0, so = -se;
                     const int ke = 2 * i, ko = 2 * i + 1;
                     if (ke < Pn) {
-                      if (k2 < E) out[ke * E + k2] = se * e0;
-                      if (k2 + 1 < E) out[ke * E + k2 + 1] = se * e1;
+                      if (k2 < E) put(ke * E + k2, se * e0);
+                      if (k2 + 1 < E) put(ke * E + k2 + 1, se * e1);
                     }
                     if (ko < Pn) {
-                      if (k2 < E) out[ko * E + k2] = so * o0;
-                      if (k2 + 1 < E) out[ko * E + k2 + 1] = so * o1;
+                      if (k2 < E) put(ko * E + k2, so * o0);
+                      if (k2 + 1 < E) put(ko * E + k2 + 1, so * o1);
                     }
                   });
 }
@@ -4142,11 +4151,13 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const size_t sh = (size_t)nw * Z.warp * 8;
         if (sh > 227 * 1024) return cudaErrorNotSupported;
         const dim3 cg((nt + nw - 1) / nw, nd);
+        // the blocks the mixed evaluation reads (the condition of its launch below)
+        const int f32 = mixed_ac && pgh == 1 && (Pn + 1) / 2 <= 16;
         switch (Z.K1 / 4) {
 #define CONV_CASE(N)                                                                              \
   case N:                                                                                         \
     CK(cudaFuncSetAttribute(k_pw2taylor2d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
-    k_pw2taylor2d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab);     \
+    k_pw2taylor2d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab, f32);  \
     break;
           CONV_CASE(1) CONV_CASE(2) CONV_CASE(3) CONV_CASE(4) CONV_CASE(5) CONV_CASE(6)
           CONV_CASE(7) CONV_CASE(8) CONV_CASE(9) CONV_CASE(10) CONV_CASE(11) CONV_CASE(12)
