@@ -3959,10 +3959,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
   do {                                                                                            \
     const size_t sh = (size_t)4 * 2 * (8 * NT) * 36 * 8;                                          \
     if (P.ifdipole) {                                                                             \
-      CK(cudaFuncSetAttribute(k_form2d_mma<NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      CK(smem_limit(k_form2d_mma<NT, true>)); \
       k_form2d_mma<NT, true><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);             \
     } else {                                                                                      \
-      CK(cudaFuncSetAttribute(k_form2d_mma<NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      CK(smem_limit(k_form2d_mma<NT, false>)); \
       k_form2d_mma<NT, false><<<g, 128, sh, st>>>(k, tk, D.form_hoff + G.beg, D.hbuf);            \
     }                                                                                             \
   } while (0)
@@ -3987,7 +3987,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (Z.Kq / 4) {
 #define H2PW_CASE(N)                                                                              \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_h2pw2d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh2)); \
+    CK(smem_limit(k_h2pw2d<N>)); \
     k_h2pw2d<N><<<hg, 128, sh2, st>>>(k, tk, nt, D.form_hoff + G.beg, D.hbuf, D.tables + G.tab);  \
     break;
             H2PW_CASE(1) H2PW_CASE(2) H2PW_CASE(3) H2PW_CASE(4) H2PW_CASE(5) H2PW_CASE(6)
@@ -4001,7 +4001,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           if (tpd * tpd > 256) return cudaErrorNotSupported;
           const int ch = Pp <= 32 ? 128 : 64;
           size_t sh = ((size_t)2 * ch * Pp + 4096 + 2 * (size_t)Pn * n2) * 8;
-          CK(cudaFuncSetAttribute(k_form2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+          CK(smem_limit(k_form2d));
           k_form2d<<<g, 256, sh, st>>>(k, tk, D.isq, ch);
         }
         launches++;
@@ -4032,10 +4032,10 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
 #define FORM3_CASE(N)                                                                             \
   case N:                                                                                         \
     if (P.ifdipole) {                                                                             \
-      CK(cudaFuncSetAttribute(k_form3d_mma<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      CK(smem_limit(k_form3d_mma<N, true>)); \
       k_form3d_mma<N, true><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                   \
     } else {                                                                                      \
-      CK(cudaFuncSetAttribute(k_form3d_mma<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+      CK(smem_limit(k_form3d_mma<N, false>)); \
       k_form3d_mma<N, false><<<fg, 256, sh, st>>>(k, D.form, ch, D.hbuf, D.isq);                  \
     }                                                                                             \
     break;
@@ -4069,7 +4069,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (4 * (ks - 1) + mt - 1) {
 #define H2PW_CASE(KS_, MT_)                                                                        \
   case 4 * (KS_ - 1) + MT_ - 1:                                                                    \
-    CK(cudaFuncSetAttribute(k_form3d_h2pw_mma<KS_, MT_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    CK(smem_limit(k_form3d_h2pw_mma<KS_, MT_>)); \
     k_form3d_h2pw_mma<KS_, MT_><<<pg, 256, sh, st>>>(k, ft, ntk, cb, D.fchunks, D.hbuf, pf);       \
     break;
             H2PW_CASE(1, 1) H2PW_CASE(1, 2) H2PW_CASE(1, 3) H2PW_CASE(1, 4)
@@ -4081,7 +4081,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           }
         } else {
           const size_t shb = form3_simt_smem(Pn, P.npw);
-          CK(cudaFuncSetAttribute(k_form3d_h2pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
+          CK(smem_limit(k_form3d_h2pw));
           k_form3d_h2pw<<<hg, 512, shb, st>>>(k, ft, cb, D.fchunks, D.hbuf);
         }
         launches++;
@@ -4096,24 +4096,24 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       if (Pn > 32 || sh > 227 * 1024) return cudaErrorNotSupported;
       int grid = std::min(D.scratch_ctas, 2 * D.psm());
       if (Pn <= 16) {
-        CK(cudaFuncSetAttribute(k_form3d_hermite<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+        CK(smem_limit(k_form3d_hermite<16>));
         k_form3d_hermite<16><<<grid, 256, sh, st>>>(k, ft, nft, D.scratch, D.scratch_per_cta, D.isq);
       } else {
-        CK(cudaFuncSetAttribute(k_form3d_hermite<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+        CK(smem_limit(k_form3d_hermite<32>));
         k_form3d_hermite<32><<<grid, 256, sh, st>>>(k, ft, nft, D.scratch, D.scratch_per_cta, D.isq);
       }
       launches++;
     }
     if (P.dim == 3 && D.form_pw_n > 0) {
       size_t sh = ((size_t)FORM_CH * (2 * P.npw + n2) + 8) * 16;
-      CK(cudaFuncSetAttribute(k_form3d_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+      CK(smem_limit(k_form3d_pw));
       k_form3d_pw<<<dim3(D.form_pw_n, nd), 256, sh, st>>>(k, D.form + D.form_hermite_n);
       launches++;
     }
     if (P.dim == 2 && D.form_pw_n > 0) {  // the NUFFT scheme's direct form
       const size_t sh = (size_t)FORM_CH * (P.npw + n2) * 16;
       if (sh > 227 * 1024) return cudaErrorNotSupported;
-      CK(cudaFuncSetAttribute(k_form2d_pw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+      CK(smem_limit(k_form2d_pw));
       k_form2d_pw<<<dim3(D.form_pw_n, nd), 256, sh, st>>>(k, D.form + D.form_hermite_n);
       launches++;
     }
@@ -4156,7 +4156,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         switch (Z.K1 / 4) {
 #define CONV_CASE(N)                                                                              \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_pw2taylor2d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    CK(smem_limit(k_pw2taylor2d<N>)); \
     k_pw2taylor2d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab, f32);  \
     break;
           CONV_CASE(1) CONV_CASE(2) CONV_CASE(3) CONV_CASE(4) CONV_CASE(5) CONV_CASE(6)
@@ -4183,7 +4183,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (np2) {
 #define HORNER_CASE(N)                                                                            \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_eval2d_horner<N, PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    CK(smem_limit(k_eval2d_horner<N, PG>)); \
     k_eval2d_horner<N, PG><<<g, 128, sh, st>>>(k, tk, D.lo);                                      \
     break;
             HORNER_CASE(1) HORNER_CASE(2) HORNER_CASE(3) HORNER_CASE(4) HORNER_CASE(5) HORNER_CASE(6)
@@ -4194,7 +4194,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
             HORNER_CASE(31) HORNER_CASE(32)
 #undef HORNER_CASE
             default:
-              CK(cudaFuncSetAttribute(k_eval2d_horner_any<PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+              CK(smem_limit(k_eval2d_horner_any<PG>));
               k_eval2d_horner_any<PG><<<g, 128, sh, st>>>(k, tk, D.lo);
           }
           return cudaSuccess;
@@ -4227,7 +4227,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (ksm) {
 #define CONV3M_CASE(N)                                                                            \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_pw2taylor3d_mma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm)); \
+    CK(smem_limit(k_pw2taylor3d_mma<N>)); \
     k_pw2taylor3d_mma<N><<<pg, 256, shm, st>>>(k, D.conv + G.beg, nt, D.lo);                      \
     break;
             CONV3M_CASE(1) CONV3M_CASE(2) CONV3M_CASE(3) CONV3M_CASE(4)
@@ -4246,7 +4246,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (ksm) {
 #define CONV3M2_CASE(N)                                                                           \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_pw2taylor3d_mma2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm2)); \
+    CK(smem_limit(k_pw2taylor3d_mma2<N>)); \
     k_pw2taylor3d_mma2<N><<<pg, 256, shm2, st>>>(k, D.conv + G.beg, nt, D.lo, gs2);               \
     break;
             CONV3M2_CASE(1) CONV3M2_CASE(2) CONV3M2_CASE(3) CONV3M2_CASE(4)
@@ -4260,7 +4260,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         switch ((P.npw + 3) / 4) {
 #define CONV3_CASE(N)                                                                             \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_pw2taylor3d<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    CK(smem_limit(k_pw2taylor3d<N>)); \
     k_pw2taylor3d<N><<<cg, 32 * nw, sh, st>>>(k, D.conv + G.beg, nt, D.lo, D.tables + G.tab,      \
                                               D.uscr, D.uscr_per_cta);                            \
     break;
@@ -4289,7 +4289,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
           switch (np2) {
 #define HORNER3_CASE(N)                                                                           \
   case N:                                                                                         \
-    CK(cudaFuncSetAttribute(k_eval3d_horner<N, PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    CK(smem_limit(k_eval3d_horner<N, PG>)); \
     k_eval3d_horner<N, PG><<<g, 128, sh, st>>>(k, tk, D.lo);                                      \
     break;
             HORNER3_CASE(1) HORNER3_CASE(2) HORNER3_CASE(3) HORNER3_CASE(4) HORNER3_CASE(5)
@@ -4311,14 +4311,14 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
     const size_t sh_sep = ((size_t)(2 * P.npw + P.npw / 2) * SEP_NPB + 256 * 4) * 16 +
                           (size_t)(D.eval_pmax + 1) * P.npw * 8;
     if (nbig > 0 && pgh == 1) {
-      CK(cudaFuncSetAttribute(k_eval3d_sep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh_sep));
+      CK(smem_limit(k_eval3d_sep<true>));
       k_eval3d_sep<true><<<dim3(nbig, nd), 256, sh_sep, st>>>(k, D.eval + D.eval3_nsplit);
       launches++;
     } else if (nbig > 0 && D.eval3_smem) {
       {
           const cudaError_t e_pgh = with_pgh(pgh, [&](auto G) -> cudaError_t {
         constexpr int PG = decltype(G)::value;
-        CK(cudaFuncSetAttribute(k_eval3d_taylor_smem<PG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.eval3_sh));
+        CK(smem_limit(k_eval3d_taylor_smem<PG>));
         k_eval3d_taylor_smem<PG><<<dim3(nbig, nd), 512, D.eval3_sh, st>>>(k, D.eval + D.eval3_nsplit);
         return cudaSuccess;
       });
@@ -4337,7 +4337,7 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
       launches++;
     }
     if (P.dim == 3 && D.eval_pw_n > 0 && pgh == 1) {
-      CK(cudaFuncSetAttribute(k_eval3d_sep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh_sep));
+      CK(smem_limit(k_eval3d_sep<false>));
       k_eval3d_sep<false><<<dim3(D.eval_pw_n, nd), 256, sh_sep, st>>>(k, D.eval + D.eval_taylor_n);
       launches++;
     } else if (P.dim == 3 && D.eval_pw_n > 0) {
@@ -4469,8 +4469,8 @@ cudaError_t large_delta_execute(const Params& P, const double* src, const Inputs
   size_t sh = 3 * FORM_CH * Pn * 8;
   if (sh > 227 * 1024) return cudaErrorNotSupported;
   if (sh > 48 * 1024) {
-    CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-    CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    CK(smem_limit(k_ld_form<2>));
+    CK(smem_limit(k_ld_form<3>));
   }
   // deterministic: per-CTA partial blocks after the local block, summed in
   // CTA order; otherwise atomic accumulation (last-bit order dependence)
@@ -4542,8 +4542,8 @@ cudaError_t large_delta_noalloc(const Params& P, const double* src, const double
   // the source staging of the local-expansion kernel grows with the order
   const int sh = (int)(3 * FORM_CH * Pn * 8);
   if (sh > 48 * 1024) {
-    CK(cudaFuncSetAttribute(k_ld_form<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
-    CK(cudaFuncSetAttribute(k_ld_form<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
+    CK(smem_limit(k_ld_form<2>));
+    CK(smem_limit(k_ld_form<3>));
   }
   // large_delta_execute clears the local expansion (work[0..nd*nent)) on the
   // stream before accumulating into it; the centre goes by value in the

@@ -133,35 +133,39 @@ __global__ void __launch_bounds__(128) k_form2d_f32(KP k, const FormTask* __rest
 // a chunk of <= 256 points of one leaf, two points per thread.  The leaf's
 // Taylor block comes from k_pw2taylor2d already in FP32, each coefficient as
 // the pair (c, c) (row k: float4 m = (c_2m, c_2m, c_2m+1, c_2m+1)), and is
-// read straight from global memory: every thread of the CTA reads the same
-// rows, so they are served from L1 after the first warp, with no staging,
-// barrier or conversion.  Each row's polynomial in x runs in FP32 (Pn FMAs),
-// the outer polynomial in y and the output in FP64.
+// copied to shared memory as it is (no conversion).  Each row's polynomial
+// in x runs in FP32 (Pn FMAs), the outer polynomial in y and the output in
+// FP64.  (Reading the rows straight from global memory, every thread the
+// same addresses, made the evaluation 1.7x slower than staging them.)
 template <int NP2>
 __global__ void __launch_bounds__(128) k_eval2d_horner_f32(KP k, const HornerTask* __restrict__ tasks,
                                                            const double* __restrict__ lo_all) {
   const HornerTask T = tasks[blockIdx.x];
   const int ind = blockIdx.y, Pn = T.p + 1;
-  const int ta = threadIdx.x, tb = threadIdx.x + 128;
-  if (ta >= T.n) return;
-  const bool two = tb < T.n;
+  extern __shared__ float4 lf[];  // [Pn][NP2]
   const double* pts = T.set ? k.trg : k.src;
   double* out = T.set ? k.pottarg : k.pot;
   const int nc = T.set ? k.nc_t : k.nc_s;
   const double cx = k.centers[2 * T.box], cy = k.centers[2 * T.box + 1];
-  const double2 pa = reinterpret_cast<const double2*>(pts)[T.i0 + ta];
-  const double2 pb = reinterpret_cast<const double2*>(pts)[T.i0 + (two ? tb : ta)];
-  const float4* lf = reinterpret_cast<const float4*>(lo_all + T.off + (size_t)ind * Pn * 2 * NP2);
+  const int ta = threadIdx.x, tb = threadIdx.x + 128;
+  const bool one = ta < T.n, two = tb < T.n;
+  // the points are loaded before the block, so both loads are in flight together
+  const double2 pa = reinterpret_cast<const double2*>(pts)[T.i0 + (one ? ta : 0)];
+  const double2 pb = reinterpret_cast<const double2*>(pts)[T.i0 + (two ? tb : 0)];
+  const float4* src = reinterpret_cast<const float4*>(lo_all + T.off + (size_t)ind * Pn * 2 * NP2);
+  for (int e = threadIdx.x; e < Pn * NP2; e += blockDim.x) lf[e] = src[e];
+  __syncthreads();
+  if (!one) return;
   const float2 x01 = make_float2((float)((pa.x - cx) * k.dsq), (float)((pb.x - cx) * k.dsq));
   const double y0 = (pa.y - cy) * k.dsq, y1 = (pb.y - cy) * k.dsq;
   double r0 = 0.0, r1 = 0.0;
   for (int k1 = Pn - 1; k1 >= 0; k1--) {
     const float4* rw = lf + k1 * NP2;
-    const float4 ct = __ldg(rw + NP2 - 1);
+    const float4 ct = rw[NP2 - 1];
     float2 s = ffma2(make_float2(ct.z, ct.w), x01, make_float2(ct.x, ct.y));
 #pragma unroll
     for (int m = NP2 - 2; m >= 0; m--) {
-      const float4 c = __ldg(rw + m);
+      const float4 c = rw[m];
       s = ffma2(s, x01, make_float2(c.z, c.w));
       s = ffma2(s, x01, make_float2(c.x, c.y));
     }
@@ -311,11 +315,12 @@ cudaError_t launch_eval2d_horner_f32(const KP& k, const HornerTask* tasks, int n
                                      const double* lo, cudaStream_t st) {
   if (ntask <= 0) return cudaSuccess;
   const int np2 = (Pn + 1) / 2;
+  const size_t sh = (size_t)Pn * np2 * sizeof(float4);
   const dim3 g(ntask, nd);
   switch (np2) {
 #define HF32_CASE(N)                                                   \
   case N:                                                              \
-    k_eval2d_horner_f32<N><<<g, 128, 0, st>>>(k, tasks, lo);           \
+    k_eval2d_horner_f32<N><<<g, 128, sh, st>>>(k, tasks, lo);          \
     break;
     HF32_CASE(1) HF32_CASE(2) HF32_CASE(3) HF32_CASE(4) HF32_CASE(5) HF32_CASE(6) HF32_CASE(7)
     HF32_CASE(8) HF32_CASE(9) HF32_CASE(10) HF32_CASE(11) HF32_CASE(12) HF32_CASE(13) HF32_CASE(14)

@@ -499,7 +499,7 @@ cudaError_t launch_form3d_tc(const KP& k, const FormTask* tasks, const FormChunk
 #define F3TC_CASE(P_)                                                                                  \
   case P_: {                                                                                           \
     const int sh = Form3Dims<P_>::SMEM + 1024;                                                         \
-    CK(cudaFuncSetAttribute(k_form3d_tc<P_>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));       \
+    CK(smem_limit(k_form3d_tc<P_>));       \
     k_form3d_tc<P_><<<g, Form3Dims<P_>::NT, sh, st>>>(k, tasks, chunks, hbuf, isq);                    \
     break;                                                                                             \
   }
@@ -523,7 +523,7 @@ cudaError_t launch_eval3d_tc(const KP& k, const HornerTask* tasks, int ntask, in
     /* TMEM: PER_SM CTAs hold their columns on one SM at a time; the shared memory request keeps */       \
     /* more CTAs off the SM instead of waiting in tcgen05.alloc */                                        \
     const int sh = std::max(D::SMEM + 1024, (228 * 1024) / (D::PER_SM + 1) + 1024);                      \
-    CK(cudaFuncSetAttribute(k_eval3d_tc<P_>, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));         \
+    CK(smem_limit(k_eval3d_tc<P_>));         \
     k_eval3d_tc<P_><<<g, 128, sh, st>>>(k, tasks, lo);                                                   \
     break;                                                                                               \
   }
@@ -562,7 +562,7 @@ cudaError_t tc_selftest(int N, double* max_rel_err) {
   CK(cudaMemcpy(dA, A.data(), A.size() * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dB, B.data(), B.size() * 4, cudaMemcpyHostToDevice));
   const int sh = 3 * 4096 + 3 * N * 32 + 1024;
-  CK(cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, sh));
+  CK(smem_limit(k_tc_selftest));
   k_tc_selftest<<<1, 128, sh>>>(dA, dB, N, dD);
   CK(cudaGetLastError());
   CK(cudaDeviceSynchronize());
