@@ -268,7 +268,7 @@ int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double e
   }
   if (same && nt > 0) CKS(cudaMemcpyAsync(p->d_trg, p->d_src, (size_t)nt * dim * 8, cudaMemcpyDeviceToDevice, s));
   if (shard_filter(p->H, p->shard_n, p->shard_r, p->shard) != 0) return FGT_ERR_BADARG;
-  if (p->H.defer_near && p->H.tree.nboxes > 0) {
+  if (p->H.defer_near && p->H.tree.nboxes > 0 && !p->H.near_built) {
     const double tn = now_s();
     const cudaError_t e = build_near_tasks_device(p->H, s);
     if (e != cudaSuccess) {

@@ -1782,6 +1782,26 @@ cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double
   CKD(build_tree_device(H.tree, dim, d_src, ns, d_trg, nt, same, ts, d_isrc, d_itarg, st,
                         H.defer_near ? &H.dtree : nullptr));
   H.host_tree_s = now_s() - tstart;
+  if (H.defer_near && H.dtree.mem) {
+    // the near-field arrays on the GPU, driven from a second host thread
+    // beside the host's far-field tasks (its kernels go to the same stream;
+    // this thread makes no CUDA call meanwhile)
+    int dev = 0;
+    CKD(cudaGetDevice(&dev));
+    cudaError_t near_err = cudaSuccess;
+    plan_end(H, [&] {
+      try {
+        const double tn = now_s();
+        near_err = cudaSetDevice(dev);
+        if (near_err == cudaSuccess) near_err = build_near_tasks_device(H, st);
+        if (getenv("FGT_TREE_TIMING")) fprintf(stderr, "near-field tasks (device, beside): %.4f\n", now_s() - tn);
+      } catch (const std::bad_alloc&) {
+        near_err = cudaErrorMemoryAllocation;
+      }
+    });
+    H.near_built = true;
+    return near_err;
+  }
   plan_end(H);
   return cudaSuccess;
 }
@@ -1831,14 +1851,13 @@ cudaError_t build_near_tasks_device(HostPlan& H, cudaStream_t st) {
       CKD(S.get(&d_t0, nb));
       CKD(S.get(&d_t1, nb));
     }
-    StagedBatch X(st, staged_bytes({8 * (size_t)nlv, tsame ? 0 : sizeof(int) * (size_t)nb,
-                                    tsame ? 0 : sizeof(int) * (size_t)nb}));
-    CKD(X.up(d_bsz, t.boxsize.data(), nlv));
+    // small copies, straight from the host arrays (this may run on a thread
+    // of its own, whose pinned stage would be allocated for the one call)
+    CKD(upload(d_bsz, t.boxsize.data(), nlv, st));
     if (!tsame) {
-      CKD(X.up(d_t0, t.t0.data(), nb));
-      CKD(X.up(d_t1, t.t1.data(), nb));
+      CKD(upload(d_t0, t.t0.data(), nb, st));
+      CKD(upload(d_t1, t.t1.data(), nb, st));
     }
-    CKD(X.finish());
   } else {
     CKD(S.get(&d_par, nb));
     CKD(S.get(&d_nch, nb));

@@ -296,15 +296,23 @@ __device__ void horner3_rt(const double* lo, int ld, int Pn, double x, double y,
 // ------------------------------------------------------------ (d) near field: source ranges
 // A near-field task's sources are a list of ranges; a warp reads up to 32
 // ranges at a time and maps slots of their concatenation to source indices.
-// Raises a kernel's dynamic shared-memory limit to the opt-in maximum of
-// sm_100 (227 KB); every launch then asks for its own size below it.
-// Setting each launch's own size instead would let concurrent plans (a
-// server's worker threads) lower the limit under one another's launches,
-// which then fail with an invalid-argument error.
-constexpr int kMaxDynSmem = 227 * 1024;
+// Raises a kernel's dynamic shared-memory limit to the most the device
+// allows beside the kernel's static shared memory; every launch then asks
+// for its own size below it.  Setting each launch's own size instead would
+// let concurrent plans (a server's worker threads) lower the limit under one
+// another's launches, which then fail with an invalid-argument error.  The
+// limit only ever rises, so concurrent calls agree.
 template <typename K>
 cudaError_t smem_limit(K* kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  const int lim = optin - (int)fa.sharedSizeBytes;
+  if (fa.maxDynamicSharedSizeBytes >= lim) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 struct RangeChunk {

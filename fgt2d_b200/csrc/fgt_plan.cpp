@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
+#include <thread>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -621,7 +622,7 @@ bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, 
   return true;
 }
 
-void plan_end(HostPlan& H) {
+void plan_end(HostPlan& H, const std::function<void()>& beside) {
   Params& P = H.P;
   const int dim = P.dim;
   Tree& t = H.tree;
@@ -641,7 +642,18 @@ void plan_end(HostPlan& H) {
   double pweps = nadd > 2 ? P.eps / 100 : P.eps;
   pwterms(2 * t.bs0 / std::pow(2.0, nls), P.delta, pweps, &P.pmax, &P.npw);
   P.nexp = dim == 2 ? P.npw * P.npw / 2 : P.npw * P.npw * P.npw / 2;
-  finish_plan(H);
+  if (!beside) {
+    finish_plan(H);
+    return;
+  }
+  std::thread th(beside);
+  try {
+    finish_plan(H);
+  } catch (...) {
+    th.join();
+    throw;
+  }
+  th.join();
 }
 
 int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,

@@ -4,6 +4,7 @@
 #pragma once
 #include <cstdint>
 #include <cstddef>
+#include <functional>
 #include <memory>
 #include <new>
 #include <type_traits>
@@ -108,6 +109,7 @@ struct HostPlan {
     void* mem = nullptr;
   } dnear;
   bool defer_near = false;  // finish_plan leaves the near-field arrays to the device build
+  bool near_built = false;  // the device build has run (beside the host tasks)
   // The finished tree's box arrays as the device build left them (final ids;
   // kept for the near-field build when defer_near, else empty): one
   // stream-ordered allocation, released by the near-field build (or with
@@ -130,7 +132,10 @@ struct HostPlan {
 // and the tree whose point work runs on the GPU):
 //   plan_begin: parameters from the bounding-box results; false for the
 //     large-delta path (no tree).  ts receives the tree-build settings.
-//   plan_end: expansion lengths, tables and tasks once H.tree is complete.
+//   plan_end: expansion lengths, tables and tasks once H.tree is complete;
+//     beside (if given) runs on a second thread while the tables and tasks
+//     are built, after the parameters it may read are final (the device
+//     build of the near-field tasks, which reads H.P and H.tree only).
 struct TreeSetup {
   int ndiv = 0, ndiv0 = 0, levcut = 0, nlmax = 0;
   double bs0 = 0, cen0[3] = {0, 0, 0};
@@ -138,7 +143,7 @@ struct TreeSetup {
 bool plan_begin(HostPlan& H, int dim, int nd, double delta, double eps, int ns, int nt, int ifpgh,
                 int ifpghtarg, int npwlevel, double bs0, const double* cen0, TreeSetup& ts,
                 int ifcharge = 1, int ifdipole = 0);
-void plan_end(HostPlan& H);
+void plan_end(HostPlan& H, const std::function<void()>& beside = nullptr);
 
 int build_host_plan(HostPlan& H, int dim, int nd, double delta, double eps, int ns,
                     const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
