@@ -113,6 +113,23 @@ __global__ void k_all_finite(const double* __restrict__ x, size_t n, int* __rest
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     if (!isfinite(x[i])) *bad = 1;
 }
+// qs[i] = q[perm[i]] for one density (the charges of every execute): four
+// independent random reads in flight per thread
+__global__ void __launch_bounds__(256) k_gather1(const double* __restrict__ q, const int* __restrict__ perm, int n,
+                                                 double* __restrict__ qs) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 4 * stride) {
+    int p[4];
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) p[u] = i + u * stride < n ? perm[i + u * stride] : -1;
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = p[u] >= 0 ? q[p[u]] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (p[u] >= 0) qs[i + u * stride] = v[u];
+  }
+}
 // inv[perm[i]] = i
 __global__ void k_invperm(const int* __restrict__ perm, int n, int* __restrict__ inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -3403,6 +3420,9 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   int dev = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev));
+  double tq[8];
+  int nq = 0;
+  tq[nq++] = tnow();
   // order form and eval tasks by route so each kernel gets a contiguous range
   // (then by order; stable)
   const std::vector<FormTask> form = route_order_sort(H.form);
@@ -3417,6 +3437,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     (e.route == ROUTE_PW ? D.eval_pw_n : D.eval_taylor_n)++;
     if (e.route == ROUTE_TAYLOR) D.eval_pmax = std::max(D.eval_pmax, e.p);
   }
+  tq[nq++] = tnow();
   // launch groups of equal order among the Hermite form / Taylor eval tasks
   for (int t = 0; t < D.form_hermite_n;) {
     int u = t;
@@ -3471,6 +3492,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   };
   const int lcut = std::max(P.npwlevel, 0);
   std::vector<uint8_t> fused_leaf(H.tree.nboxes, 0);
+  tq[nq++] = tnow();
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
     std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     const int ntay = P.dim == 2 ? D.eval_taylor_n : D.eval3_nsplit;
@@ -3500,6 +3522,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
       for (int c = 0; c < e.n; c += 256)
         horner.push_back({e.box, e.set, e.i0 + c, std::min(256, e.n - c), e.p, slot_off[e.slot]});
     }
+    tq[nq++] = tnow();
     // conv and horner are in order of p (the Taylor tasks are sorted by p)
     for (size_t t = 0; t < conv.size();) {
       size_t u = t;
@@ -3819,8 +3842,10 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   D.uscr = reinterpret_cast<double*>(cur); cur += al((size_t)D.conv3_ctas * nd * D.uscr_per_cta * 8);
   CK(cudaStreamSynchronize(s));
   if (getenv("FGT_TREE_TIMING"))
-    fprintf(stderr, "device plan prep parts: sort %.4f conv %.4f tables %.4f merge %.4f split %.4f rest %.4f\n",
-            tp[0] - tin, tp[1] - tp[0], tp[2] - tp[1], tp[3] - tp[2], tp[4] - tp[3], tm0 - tp[4]);
+    fprintf(stderr, "device plan prep parts: sort %.4f conv %.4f tables %.4f merge %.4f split %.4f rest %.4f"
+            " (device %.4f route sorts %.4f groups %.4f conv loop %.4f)\n",
+            tp[0] - tin, tp[1] - tp[0], tp[2] - tp[1], tp[3] - tp[2], tp[4] - tp[3], tm0 - tp[4], tq[0] - tin,
+            tq[1] - tq[0], tq[2] - tq[1], nq > 3 ? tq[3] - tq[2] : 0.0);
   if (getenv("FGT_TREE_TIMING"))
     fprintf(stderr, "device plan: prep %.4f malloc %.4f upload %.4f (%zu bytes); eval tasks: taylor %d "
             "(conversion %d, max order %d) pw %d; form tasks: hermite %d (shared memory %d, max order %d) pw %d\n",
@@ -3930,7 +3955,8 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
   // charges into tree order (coordinates were sorted once, at plan set-up)
   const int gb = std::max(1, std::min(8 * D.sm_count, (std::max(P.ns, P.nt) + 255) / 256));
   if (ph1 && P.ns > 0 && P.ifcharge) {
-    k_gather_pts<<<gb, 256, 0, st>>>(nullptr, in.charge, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
+    if (nd == 1) k_gather1<<<gb, 256, 0, st>>>(in.charge, D.isrc, P.ns, D.csort);
+    else k_gather_pts<<<gb, 256, 0, st>>>(nullptr, in.charge, nullptr, D.csort, D.isrc, P.ns, P.dim, nd, 0);
     launches++;
   }
   if (ph1 && P.ns > 0 && P.ifdipole) {  // directions and strengths of the dipoles
@@ -4390,7 +4416,9 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
   auto unsort = [&](const double* in, const int* inv, int n, int nc, double* pot, double* grad,
                     double* hess) {
     if (pot) {
-      k_unsort<<<gb, 256, 0, st>>>(in, pot, inv, n, nc * nd, 0, nd);
+      // one density, one component per point: the same random gather
+      if (nd == 1 && nc == 1) k_gather1<<<gb, 256, 0, st>>>(in, inv, n, pot);
+      else k_unsort<<<gb, 256, 0, st>>>(in, pot, inv, n, nc * nd, 0, nd);
       launches++;
     }
     if (nc > 1 && grad) {
