@@ -125,6 +125,25 @@ def test_reference_test_inputs_3d(fgt, oracle):
     assert oracle.derr(opot, pot) <= FP64_TOL
 
 
+@pytest.mark.parametrize("dim,nsrc", [(2, 1_000_000), (3, 300_000)])
+def test_reference_test_inputs_full_size(fgt, oracle, dim, nsrc):
+    """The reference drivers' own runs at their own sizes (test_fgt2d.f:52-145:
+    1e6 sources and targets, eps = 5e-11; test_fgt3d.f:32-125: 3e5, eps =
+    1e-6; potentials at the sources), checked as they check: the relative l2
+    error at the first 20 sources against the direct sum
+    (test_fgt2d.f:161-174, 204-225), and here at 1000 more sampled sources."""
+    gen = oracle.reference_test_inputs_2d if dim == 2 else oracle.reference_test_inputs_3d
+    src, q, trg, delta, eps = gen(nsrc)
+    run = fgt.fgt2d if dim == 2 else fgt.fgt3d
+    pot, _ = run(1, delta, eps, src, q, trg, 1, 0, ctx=fgt.Context(0, "fp64"))
+    ex = oracle.direct(dim, 1, delta, src, q, src[:20])
+    e20 = oracle.derr(ex, pot[:20])
+    idx = np.random.default_rng(5).choice(nsrc, 1000, replace=False)
+    es = oracle.derr(oracle.direct(dim, 1, delta, src, q, src[idx]), pot[idx])
+    print(f"{dim}D reference run, {nsrc} sources, eps {eps:g}: first 20 {e20:.2e}, 1000 sampled {es:.2e}")
+    assert e20 <= 10 * eps and es <= 10 * eps
+
+
 def test_edge_cases(fgt, oracle):
     ctx = fgt.Context(0, "fp64")
     # one source, one target: a root box far below the Gaussian width takes
