@@ -3364,13 +3364,29 @@ size_t form3_simt_smem(int Pn_, int npw) {
 // small integers), linear in the number of tasks.
 template <typename Task>
 std::vector<Task> route_order_sort(const std::vector<Task>& in) {
+  // the tasks come level by level, so runs of one key are long: count and
+  // place whole runs (a per-task counter increment is a dependency chain
+  // through one memory cell when most tasks share a key)
+  auto key = [](const Task& t) { return 4096 * t.route + t.p; };
+  std::vector<std::pair<size_t, size_t>> runs;  // [begin, end)
   int kmax = 0;
-  for (const Task& t : in) kmax = std::max(kmax, 4096 * t.route + t.p);
-  std::vector<int> cnt((size_t)kmax + 2, 0);
-  for (const Task& t : in) cnt[4096 * t.route + t.p + 1]++;
+  for (size_t i = 0; i < in.size();) {
+    size_t j = i + 1;
+    const int k = key(in[i]);
+    while (j < in.size() && key(in[j]) == k) j++;
+    runs.push_back({i, j});
+    kmax = std::max(kmax, k);
+    i = j;
+  }
+  std::vector<size_t> cnt((size_t)kmax + 2, 0);
+  for (const auto& r : runs) cnt[key(in[r.first]) + 1] += r.second - r.first;
   for (size_t i = 1; i < cnt.size(); i++) cnt[i] += cnt[i - 1];
   std::vector<Task> out(in.size());
-  for (const Task& t : in) out[cnt[4096 * t.route + t.p]++] = t;
+  for (const auto& r : runs) {
+    size_t& at = cnt[key(in[r.first])];
+    std::copy(in.begin() + r.first, in.begin() + r.second, out.begin() + at);
+    at += r.second - r.first;
+  }
   return out;
 }
 // Whether the 3D Hermite form of order Pn runs on the shared-memory kernels:
@@ -3494,30 +3510,76 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   std::vector<uint8_t> fused_leaf(H.tree.nboxes, 0);
   tq[nq++] = tnow();
   if ((P.dim == 2 || D.eval3_split) && !P.all_direct) {
-    std::vector<long long> slot_off(std::max(H.nloc, 1), -1);
     const int ntay = P.dim == 2 ? D.eval_taylor_n : D.eval3_nsplit;
-    long long nh = 0;
-    for (int t = 0; t < ntay; t++) nh += (ev[t].n + 255) / 256;
-    conv.reserve(ntay);
-    horner.reserve(nh);
-    for (int t = 0; t < ntay; t++) {
-      const EvalTask& e = ev[t];
+    // the conversion of leaf slot s, made by its first task: (ConvTask, the
+    // fused split), the same for either way of filling below
+    auto make_conv = [&](const EvalTask& e, long long off) {
+      const long long Pn = e.p + 1;
+      ConvTask ct{e.slot, e.p, off};
+      if (conv3_fusable((int)Pn) && H.tree.level[e.box] > lcut) {
+        int a = e.box;
+        while (H.tree.level[a] > lcut) a = H.tree.parent[a];
+        if (a >= 0 && H.loc_slot[a] >= 0) {
+          ct.slot = H.loc_slot[a];
+          ct.fused = 1;
+          for (int d = 0; d < P.dim; d++) ct.sh[d] = (H.tree.c(e.box, d) - H.tree.c(a, d)) * P.dsq;
+          fused_leaf[e.box] = 1;
+        }
+      }
+      return ct;
+    };
+    auto lo_size = [&](const EvalTask& e) {
       const long long Pn = e.p + 1, E = (Pn + 1) & ~1LL;
+      return (size_t)(P.nd * Pn * E * (P.dim == 3 ? Pn : 1));
+    };
+    // The tasks of one leaf are consecutive (the builder emits them leaf by
+    // leaf and the route sort is stable): then every slot's first task starts
+    // a run, the conversions and chunk lists are laid out by prefix sums and
+    // filled in parallel.  Otherwise the serial loop below does the same.
+    std::vector<int> cidx(ntay + 1, 0);
+    std::vector<long long> hidx(ntay + 1, 0);
+    bool runs = true;
+    {
+      std::vector<uint8_t> seen(std::max(H.nloc, 1), 0);
+      for (int t = 0; t < ntay; t++) {
+        const bool first = t == 0 || ev[t].slot != ev[t - 1].slot;
+        if (first) {
+          if (seen[ev[t].slot]) runs = false;
+          seen[ev[t].slot] = 1;
+        }
+        cidx[t + 1] = cidx[t] + first;
+        hidx[t + 1] = hidx[t] + (ev[t].n + 255) / 256;
+      }
+    }
+    if (runs) {
+      const int ncv = cidx[ntay];
+      std::vector<long long> coff(ncv + 1, 0);
+      for (int t = 0; t < ntay; t++)
+        if (cidx[t + 1] != cidx[t]) coff[cidx[t] + 1] = (long long)lo_size(ev[t]);
+      for (int c = 0; c < ncv; c++) coff[c + 1] += coff[c];
+      lo_doubles = (size_t)coff[ncv];
+      conv.resize(ncv);
+      horner.resize(hidx[ntay]);
+#pragma omp parallel for schedule(static) if (ntay > 4096)
+      for (int t = 0; t < ntay; t++) {
+        const EvalTask& e = ev[t];
+        const int c = cidx[t + 1] - 1;  // this task's slot's conversion
+        if (cidx[t + 1] != cidx[t]) conv[c] = make_conv(e, coff[c]);
+        long long h = hidx[t];
+        for (int k = 0; k < e.n; k += 256) horner[h++] = {e.box, e.set, e.i0 + k, std::min(256, e.n - k), e.p, coff[c]};
+      }
+    }
+    std::vector<long long> slot_off(runs ? 1 : std::max(H.nloc, 1), -1);
+    if (!runs) {
+      conv.reserve(ntay);
+      horner.reserve(hidx[ntay]);
+    }
+    for (int t = 0; t < ntay && !runs; t++) {
+      const EvalTask& e = ev[t];
       if (slot_off[e.slot] < 0) {
         slot_off[e.slot] = (long long)lo_doubles;
-        ConvTask ct{e.slot, e.p, (long long)lo_doubles};
-        if (conv3_fusable((int)Pn) && H.tree.level[e.box] > lcut) {
-          int a = e.box;
-          while (H.tree.level[a] > lcut) a = H.tree.parent[a];
-          if (a >= 0 && H.loc_slot[a] >= 0) {
-            ct.slot = H.loc_slot[a];
-            ct.fused = 1;
-            for (int d = 0; d < P.dim; d++) ct.sh[d] = (H.tree.c(e.box, d) - H.tree.c(a, d)) * P.dsq;
-            fused_leaf[e.box] = 1;
-          }
-        }
-        conv.push_back(ct);
-        lo_doubles += (size_t)(P.nd * Pn * E * (P.dim == 3 ? Pn : 1));
+        conv.push_back(make_conv(e, (long long)lo_doubles));
+        lo_doubles += lo_size(e);
       }
       for (int c = 0; c < e.n; c += 256)
         horner.push_back({e.box, e.set, e.i0 + c, std::min(256, e.n - c), e.p, slot_off[e.slot]});
