@@ -1768,6 +1768,7 @@ cudaError_t build_plan_device(HostPlan& H, int dim, int nd, double delta, double
                               int ifpghtarg, int* d_isrc, int* d_itarg, cudaStream_t st,
                               int ifcharge, int ifdipole) {
   const double tstart = now_s();
+  H.same_points = same;
   double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
   CKD(device_bbox(d_src, ns, d_trg, same ? 0 : nt, dim, mn, mx, st));
   int npwlevel;

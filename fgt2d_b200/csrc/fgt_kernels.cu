@@ -3788,73 +3788,29 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   const double tm1 = tnow();
   char* cur = D.base;
   cudaStream_t s = pst;
-  CK(put(cur, D.centers, H.box_centers, s));
-  CK(put(cur, D.h2x, H.h2x, s));
-  CK(put(cur, D.x2l, H.x2l, s));
+  // Everything that goes up from the host, laid out in the arena as it
+  // comes, goes in one copy from a pinned mirror of that range (filled by the
+  // host threads); no pageable copy (each would wait for the stream) and no
+  // synchronisation here: the kernels below follow the copy on the stream.
+  std::vector<double2> ww(H.ww.size() / 2), w1(H.w1.size() / 2);
+  memcpy(ww.data(), H.ww.data(), H.ww.size() * 8);
+  memcpy(w1.data(), H.w1.data(), H.w1.size() * 8);
+  std::vector<double> isq(std::max(P.ntermmax, 1) + 2, 0.0);
+  for (size_t j = 1; j < isq.size(); j++) isq[j] = 1.0 / std::sqrt((double)j);
+  std::vector<double> cfac(32);
+  cfac[0] = 1.0;
+  for (int j = 1; j < 32; j++) cfac[j] = cfac[j - 1] / std::sqrt((double)j);
+  double2 *d_ww = nullptr, *d_w1 = nullptr;
   {
-    // translation tables formed on the device from their 1D factors
-    std::vector<double2> ww(H.ww.size() / 2), w1(H.w1.size() / 2);
-    memcpy(ww.data(), H.ww.data(), H.ww.size() * 8);
-    memcpy(w1.data(), H.w1.data(), H.w1.size() * 8);
-    double2 *d_ww = nullptr, *d_w1 = nullptr;
-    CK(put(cur, d_ww, ww, s));
-    CK(put(cur, d_w1, w1, s));
-    D.wms = reinterpret_cast<double2*>(cur); cur += al(n_wms * 16);
-    D.wsh = reinterpret_cast<double2*>(cur); cur += al(n_wsh * 16);
-    if (n_wms > 0) {
-      const long long tot = (long long)(n_wms + n_wsh);
-      const int blocks = (int)std::min<long long>((tot + 255) / 256, (long long)D.sm_count * 16);
-      k_shift_tables<<<blocks, 256, 0, s>>>(P.dim, P.npw, P.nexp, P.nlevels, std::max(P.nlevstart, 0), H.nms,
-                                            d_ww, d_w1, D.wms, D.wsh);
-      CK(cudaGetLastError());
-    }
-    CK(cudaStreamSynchronize(s));
-  }
-  if (d_isrc) {
-    // permutations built on the device (fgt_devtree.cu): copy, invert there
-    auto carve = [&](int*& dst, size_t n) {
-      dst = reinterpret_cast<int*>(cur);
-      cur += al(n * 4);
-    };
-    carve(D.isrc, P.ns);
-    carve(D.itarg, P.nt);
-    carve(D.isrc_inv, P.ns);
-    carve(D.itarg_inv, P.nt);
-    if (P.ns > 0) {
-      CK(cudaMemcpyAsync(D.isrc, d_isrc, (size_t)P.ns * 4, cudaMemcpyDeviceToDevice, pst));
-      k_invperm<<<(P.ns + 255) / 256, 256, 0, pst>>>(D.isrc, P.ns, D.isrc_inv);
-    }
-    if (P.nt > 0) {
-      CK(cudaMemcpyAsync(D.itarg, d_itarg, (size_t)P.nt * 4, cudaMemcpyDeviceToDevice, pst));
-      k_invperm<<<(P.nt + 255) / 256, 256, 0, pst>>>(D.itarg, P.nt, D.itarg_inv);
-    }
-    CK(cudaStreamSynchronize(pst));
-  } else {
-    CK(put(cur, D.isrc, H.tree.isrc, s));
-    CK(put(cur, D.itarg, H.tree.itarg, s));
-    std::vector<int> inv(H.tree.isrc.size());
-    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.isrc[i]] = (int)i;
-    CK(put(cur, D.isrc_inv, inv, s));
-    CK(cudaStreamSynchronize(s));
-    inv.assign(H.tree.itarg.size(), 0);
-    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.itarg[i]] = (int)i;
-    CK(put(cur, D.itarg_inv, inv, s));
-  }
-  {
-    std::vector<double> isq(std::max(P.ntermmax, 1) + 2, 0.0);
-    for (size_t j = 1; j < isq.size(); j++) isq[j] = 1.0 / std::sqrt((double)j);
-    CK(put(cur, D.isq, isq, s));
-    std::vector<double> cfac(32);
-    cfac[0] = 1.0;
-    for (int j = 1; j < 32; j++) cfac[j] = cfac[j - 1] / std::sqrt((double)j);
-    CK(put(cur, D.cfac, cfac, s));
-    CK(cudaStreamSynchronize(s));
-  }
-  {
-    // the task arrays, laid out in the arena as they come, go up in one copy
-    // from a pinned mirror of that range (filled by the host threads)
     char* const b0 = cur;
     Staged st;
+    st.add(cur, D.centers, H.box_centers);
+    st.add(cur, D.h2x, H.h2x);
+    st.add(cur, D.x2l, H.x2l);
+    st.add(cur, d_ww, ww);
+    st.add(cur, d_w1, w1);
+    st.add(cur, D.isq, isq);
+    st.add(cur, D.cfac, cfac);
     st.add(cur, D.form, form);
     st.add(cur, D.mgroups, groups);
     st.add(cur, D.merge, H.merge);
@@ -3873,6 +3829,52 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     st.add(cur, D.conv, conv);
     st.add(cur, D.horner, horner);
     CK(st.upload(b0, s));
+  }
+  // translation tables formed on the device from their 1D factors
+  D.wms = reinterpret_cast<double2*>(cur); cur += al(n_wms * 16);
+  D.wsh = reinterpret_cast<double2*>(cur); cur += al(n_wsh * 16);
+  if (n_wms > 0) {
+    const long long tot = (long long)(n_wms + n_wsh);
+    const int blocks = (int)std::min<long long>((tot + 255) / 256, (long long)D.sm_count * 16);
+    k_shift_tables<<<blocks, 256, 0, s>>>(P.dim, P.npw, P.nexp, P.nlevels, std::max(P.nlevstart, 0), H.nms,
+                                          d_ww, d_w1, D.wms, D.wsh);
+    CK(cudaGetLastError());
+  }
+  if (d_isrc) {
+    // permutations built on the device (fgt_devtree.cu): copy, invert there;
+    // targets that are the sources share the sources' arrays
+    auto carve = [&](int*& dst, size_t n) {
+      dst = reinterpret_cast<int*>(cur);
+      cur += al(n * 4);
+    };
+    const bool same = H.same_points && P.nt == P.ns;
+    carve(D.isrc, P.ns);
+    carve(D.isrc_inv, P.ns);
+    if (same) {
+      D.itarg = D.isrc;
+      D.itarg_inv = D.isrc_inv;
+    } else {
+      carve(D.itarg, P.nt);
+      carve(D.itarg_inv, P.nt);
+    }
+    if (P.ns > 0) {
+      CK(cudaMemcpyAsync(D.isrc, d_isrc, (size_t)P.ns * 4, cudaMemcpyDeviceToDevice, pst));
+      k_invperm<<<(P.ns + 255) / 256, 256, 0, pst>>>(D.isrc, P.ns, D.isrc_inv);
+    }
+    if (P.nt > 0 && !same) {
+      CK(cudaMemcpyAsync(D.itarg, d_itarg, (size_t)P.nt * 4, cudaMemcpyDeviceToDevice, pst));
+      k_invperm<<<(P.nt + 255) / 256, 256, 0, pst>>>(D.itarg, P.nt, D.itarg_inv);
+    }
+  } else {
+    CK(put(cur, D.isrc, H.tree.isrc, s));
+    CK(put(cur, D.itarg, H.tree.itarg, s));
+    std::vector<int> inv(H.tree.isrc.size());
+    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.isrc[i]] = (int)i;
+    CK(put(cur, D.isrc_inv, inv, s));
+    CK(cudaStreamSynchronize(s));
+    inv.assign(H.tree.itarg.size(), 0);
+    for (size_t i = 0; i < inv.size(); i++) inv[H.tree.itarg[i]] = (int)i;
+    CK(put(cur, D.itarg_inv, inv, s));
   }
   if (H.dnear.mem) {
     D.dir = reinterpret_cast<DirTask*>(cur);

@@ -110,6 +110,7 @@ struct HostPlan {
   } dnear;
   bool defer_near = false;  // finish_plan leaves the near-field arrays to the device build
   bool near_built = false;  // the device build has run (beside the host tasks)
+  bool same_points = false;  // the targets are the sources (their permutations agree)
   // The finished tree's box arrays as the device build left them (final ids;
   // kept for the near-field build when defer_near, else empty): one
   // stream-ordered allocation, released by the near-field build (or with

@@ -404,7 +404,7 @@ int fgt_server_destroy(fgt_server* server);
  * holds until the process exits; nd * (nlocal+1)^dim larger than that returns
  * FGT_ERR_SCRATCH.  All calls share the array: calls that overlap on the GPU
  * race.  The first call on a device looks up the array's device address
- * (set-up); make that first call before any stream capture. */
+ * (a one-time set-up). */
 #define FGT_NOALLOC_MAX_DOUBLES 65536
 int fgt_large_delta_noalloc(int dim, int nd, double delta, int ns, const double* sources,
                             const double* charge, int nlocal, const double* center, int ifpgh,
