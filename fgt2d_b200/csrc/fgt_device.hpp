@@ -53,11 +53,11 @@ struct OrderGroup {
 struct ConvTask {
   int slot, p;
   long long off;
-  // split fused into the conversion (3D): slot is then the cut-level
-  // ancestor's local expansion and sh the leaf centre minus the ancestor's,
-  // scaled by 1/sqrt(delta); the conversion multiplies the ancestor's
-  // coefficients by exp(i (t_m3 sh0 + t_m2 sh1 + t_m1 sh2)), the product of
-  // the split factors from the ancestor down to the leaf
+  // split fused into the conversion: slot is then the cut-level ancestor's
+  // local expansion and sh the leaf centre minus the ancestor's, scaled by
+  // 1/sqrt(delta); the conversion multiplies the ancestor's coefficients by
+  // exp(i t . sh) (3D: t_m3 sh0 + t_m2 sh1 + t_m1 sh2; 2D: t_j2 sh0 + t_J
+  // sh1), the product of the split factors from the ancestor to the leaf
   int fused = 0;
   double sh[3] = {0, 0, 0};
 };

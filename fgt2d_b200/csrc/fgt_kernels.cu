@@ -1160,7 +1160,7 @@ struct ConvDims {
     ldA2 = mma_lda(K1);
     ldB2 = mma_ldb(N2);
     tab = M1 * ldX + 2 * M2 * ldA2;
-    warp = 2 * K1 * ldB2;
+    warp = 2 * K1 * ldB2 + 2 * (n2 + npw);  // be, bo, the fused split's phases (double2 [n2 + npw])
   }
 };
 constexpr int CONV_MAXKS = 12;  // largest pass A depth in steps of 4: n2 <= 48
@@ -1204,6 +1204,8 @@ __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __res
   const double* AO = AE + Z.M2 * Z.ldA2;  // [M2][ldA2]
   double* BE = s1 + warp * Z.warp;        // [K1][ldB2]: be[j1][k2]
   double* BO = BE + Z.K1 * Z.ldB2;        // [K1][ldB2]: bo[j1][k2]
+  double2* PHX = reinterpret_cast<double2*>(BO + Z.K1 * Z.ldB2);  // fused split: [n2] x phases, then
+  double2* PHY = PHX + n2;                                         // [npw] y phases
   // rows of be / bo that pass A does not write
   for (int rr = Z.N1 / 4; rr < Z.K1; rr++)
     for (int c = lane; c < Z.ldB2; c += 32) {
@@ -1213,6 +1215,18 @@ __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __res
   const int ind = blockIdx.y;
   const double* Ld = reinterpret_cast<const double*>(k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp);
   const int r = lane >> 2, c = lane & 3;
+  // the split fused (T.fused: T.slot is the cut-level ancestor's expansion):
+  // the leaf's coefficient (j2, J) is the ancestor's times
+  // exp(i (t_j2 sh0 + t_J sh1)), t_m = x2l[1][m] the nodes, sh the leaf
+  // centre minus the ancestor's over sqrt(delta)
+  if (T.fused) {
+    for (int m = lane; m < n2 + k.npw; m += 32) {
+      double sn, cs;
+      sincos(k.x2l[k.npw + (m < n2 ? m : m - n2)] * T.sh[m < n2 ? 0 : 1], &sn, &cs);
+      PHX[m] = make_double2(cs, sn);
+    }
+    __syncwarp();
+  }
   // pass A: B[j2][n], n = 4 j1 + {re, im of L[.][j1], re, im of L[.][j1 + n2]},
   // read straight from the leaf's expansion (it stays in L1 across the tiles).
   // The accumulator pair of lane (r, c) in tile (mt, nt) is row k2 = 8 mt + r,
@@ -1223,9 +1237,23 @@ __global__ void __launch_bounds__(128) k_pw2taylor2d(KP k, const ConvTask* __res
     {
       const int j1 = 2 * nt + (r >> 2), q = r & 3;
       const bool ok = j1 < n2;
-      const double* bp = Ld + 2 * (c + n2 * (j1 + (q >> 1) * n2)) + (q & 1);
+      const int J = j1 + (q >> 1) * n2;  // the y node of this lane's column
+      const double* bp = Ld + 2 * (c + n2 * J) + (q & 1);
+      if (T.fused) {
 #pragma unroll
-      for (int ks = 0; ks < KS; ks++) bk[ks] = (ok && 4 * ks + c < n2) ? __ldg(bp + 8 * ks) : 0.0;
+        for (int ks = 0; ks < KS; ks++) {
+          const int j2 = 4 * ks + c;
+          bk[ks] = 0.0;
+          if (ok && j2 < n2) {
+            const double2 L = __ldg(reinterpret_cast<const double2*>(Ld) + j2 + n2 * J);
+            const double2 v = cmul_rn(L, cmul_rn(PHX[j2], PHY[J]));
+            bk[ks] = (q & 1) ? v.y : v.x;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int ks = 0; ks < KS; ks++) bk[ks] = (ok && 4 * ks + c < n2) ? __ldg(bp + 8 * ks) : 0.0;
+      }
     }
     for (int mt = 0; mt < Z.M1 / 8; mt++) {
       const double* ap = XA + (8 * mt + r) * Z.ldX + c;
@@ -3494,12 +3522,15 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
   }
   D.eval3_split = D.eval3_nsplit > 0;
   const int split_pmax = D.eval3_split ? ev[D.eval3_nsplit - 1].p : -1;
-  // 3D: the split is fused into the conversion kernels that stage the
-  // expansion in shared memory (orders <= 32): they read the cut-level
-  // ancestor's local expansion and apply the leaf's phases (ConvTask.sh)
-  auto conv3_fusable = [&](int Pn) {
+  // The split is fused into the conversion kernels (2D: all; 3D: those that
+  // stage the expansion in shared memory, orders <= 32): they read the
+  // cut-level ancestor's local expansion and apply the leaf's phases
+  // (ConvTask.sh)
+  // 2D: every conversion (k_pw2taylor2d) applies the fused split itself
+  auto conv_fusable = [&](int Pn) {
+    if (P.dim == 2) return true;
     const int ksm = (P.npw / 2 + 3) / 4;
-    if (P.dim != 3 || ksm > 8) return false;
+    if (ksm > 8) return false;
     if (Pn <= 16) return C3Dims(Pn, P.npw).total * 8 <= 227 * 1024;
     if (Pn > 32) return false;
     int gs2 = 4;
@@ -3516,7 +3547,7 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
     auto make_conv = [&](const EvalTask& e, long long off) {
       const long long Pn = e.p + 1;
       ConvTask ct{e.slot, e.p, off};
-      if (conv3_fusable((int)Pn) && H.tree.level[e.box] > lcut) {
+      if (conv_fusable((int)Pn) && H.tree.level[e.box] > lcut) {
         int a = e.box;
         while (H.tree.level[a] > lcut) a = H.tree.parent[a];
         if (a >= 0 && H.loc_slot[a] >= 0) {
