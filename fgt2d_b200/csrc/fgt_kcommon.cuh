@@ -359,10 +359,6 @@ cudaError_t launch_form2d_f32(const KP& k, const FormTask* tasks, int ntask, int
 // Mixed near field of potentials (charges) on the packed FP32 pipe.
 cudaError_t launch_direct_mixed_x2(const KP& k, const DirTask* tasks, int ntask, int nd,
                                    const SrcRange* ranges, float amax, cudaStream_t st);
-// 2D PW -> Taylor conversion in FP32 (Pn <= 32, npw <= 64) for the leaves of
-// one order group, written as the FP32 pairs k_eval2d_horner_f32 reads.
-cudaError_t launch_pw2taylor2d_f32(const KP& k, const ConvTask* tasks, int ntask, int nd, int Pn, double* lo,
-                                   cudaStream_t st);
 // 2D Taylor evaluation of potentials in FP32 (Pn <= 32) for the point chunks
 // of one order group, added into the sorted outputs; the group's Taylor
 // blocks must have been written in FP32 pairs (k_pw2taylor2d with f32).

@@ -4274,11 +4274,6 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const dim3 cg((nt + nw - 1) / nw, nd);
         // the blocks the mixed evaluation reads (the condition of its launch below)
         const int f32 = mixed_ac && pgh == 1 && (Pn + 1) / 2 <= 16;
-        if (f32 && P.npw <= 64) {  // converted in FP32 as well
-          CK(launch_pw2taylor2d_f32(k, D.conv + G.beg, nt, nd, Pn, D.lo, st));
-          launches++;
-          continue;
-        }
         switch (Z.K1 / 4) {
 #define CONV_CASE(N)                                                                              \
   case N:                                                                                         \

@@ -128,100 +128,6 @@ __global__ void __launch_bounds__(128) k_form2d_f32(KP k, const FormTask* __rest
   }
 }
 
-// ------------------------------------------------------------ (c) PW -> Taylor, 2D, FP32
-// The mixed form's conversion of a leaf's plane-wave expansion into its
-// Taylor block (g2dpw2local_real_vec, g2drouts.f:1417-1540), the two passes
-// of k_pw2taylor2d in FP32 on the CUDA cores, one warp per leaf:
-//     lx[k2][J] = i^k2 sum_{j2 < n2} x2l[k2][j2] L[j2 + n2 J]            (pass A)
-//     lo[2i][k2]   =  s_i 2 sum_{j1 < n2} x2l[2i][j1]   Re(lx[k2][j1] + lx[k2][j1 + n2])
-//     lo[2i+1][k2] = -s_i 2 sum_{j1 < n2} x2l[2i+1][j1] Im(lx[k2][j1] - lx[k2][j1 + n2])
-// with s_i = (-1)^i (pass B).  Lane J of pass A holds the Pn sums of column
-// J; lane (k2, parity) of pass B the sums of one column and row parity.  The
-// leaf's expansion is staged in FP32 (the fused split's phases applied in
-// FP64 first), x2l in FP32 for the whole CTA (one order per launch).  The
-// block is written as FP32 pairs (c, c) in the FP64 slots, the layout
-// k_eval2d_horner_f32 reads; the padding column of an odd order is zero.
-template <int PNB>  // Pn <= PNB
-__global__ void __launch_bounds__(128) k_pw2taylor2d_f32(KP k, const ConvTask* __restrict__ tasks, int ntask,
-                                                         double* __restrict__ lo_all, int Pn) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int npw = k.npw, n2 = k.n2, E = (Pn + 1) & ~1;
-  extern __shared__ double2 f2s_d[];
-  double2* PH = f2s_d + (size_t)warp * (n2 + npw);  // fused split: x phases [n2], y phases [npw]
-  float* X = reinterpret_cast<float*>(f2s_d + 4 * (n2 + npw));  // [Pn][n2]: x2l[k][j], j < n2
-  float2* Lw = reinterpret_cast<float2*>(X + ((Pn * n2 + 3) & ~3)) + (size_t)warp * (n2 * npw + PNB * npw);
-  float2* LX = Lw + n2 * npw;  // [Pn][npw]
-  for (int e = threadIdx.x; e < Pn * n2; e += blockDim.x) X[e] = (float)k.x2l[(size_t)(e / n2) * npw + e % n2];
-  __syncthreads();  // the only CTA-wide barrier: before any warp leaves
-  const int t = blockIdx.x * 4 + warp;
-  if (t >= ntask) return;
-  const ConvTask T = tasks[t];
-  const int ind = blockIdx.y;
-  const double2* Ld = k.loc + ((size_t)T.slot * k.nd + ind) * k.nexp;
-  // the leaf's expansion, with the fused split's phases exp(i (t_j2 sh0 + t_J sh1))
-  if (T.fused) {
-    for (int m = lane; m < n2 + npw; m += 32) {
-      double sn, cs;
-      sincos(k.x2l[npw + (m < n2 ? m : m - n2)] * T.sh[m < n2 ? 0 : 1], &sn, &cs);
-      PH[m] = make_double2(cs, sn);
-    }
-    __syncwarp();
-  }
-  for (int e = lane; e < n2 * npw; e += 32) {
-    double2 v = __ldg(Ld + e);
-    if (T.fused) {
-      const double2 px = PH[e % n2], py = PH[n2 + e / n2];
-      const double2 ph = make_double2(px.x * py.x - px.y * py.y, px.x * py.y + px.y * py.x);
-      v = make_double2(v.x * ph.x - v.y * ph.y, v.x * ph.y + v.y * ph.x);
-    }
-    Lw[e] = make_float2((float)v.x, (float)v.y);
-  }
-  __syncwarp();
-  // pass A
-  for (int J = lane; J < npw; J += 32) {
-    float2 acc[PNB];
-#pragma unroll
-    for (int q = 0; q < PNB; q++) acc[q] = make_float2(0.f, 0.f);
-    for (int j2 = 0; j2 < n2; j2++) {
-      const float2 l = Lw[j2 + n2 * J];
-#pragma unroll
-      for (int q = 0; q < PNB; q++)
-        if (q < Pn) {
-          const float x = X[q * n2 + j2];
-          acc[q].x = fmaf(x, l.x, acc[q].x);
-          acc[q].y = fmaf(x, l.y, acc[q].y);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < PNB; q++)
-      if (q < Pn) {  // times i^q
-        const float a = (q & 1) ? -acc[q].y : acc[q].x, b = (q & 1) ? acc[q].x : acc[q].y;
-        LX[q * npw + J] = (q & 2) ? make_float2(-a, -b) : make_float2(a, b);
-      }
-  }
-  __syncwarp();
-  // pass B
-  float2* out = reinterpret_cast<float2*>(lo_all + T.off + (size_t)ind * Pn * E);
-  for (int w = lane; w < 2 * E; w += 32) {
-    const int k2 = w >> 1, par = w & 1;
-    if (k2 >= Pn) {  // the zero padding column of an odd order
-      for (int k1 = par; k1 < Pn; k1 += 2) out[k1 * E + k2] = make_float2(0.f, 0.f);
-      continue;
-    }
-    for (int k1 = par; k1 < Pn; k1 += 2) {
-      float sum = 0.f;
-      for (int j1 = 0; j1 < n2; j1++) {
-        const float2 a = LX[k2 * npw + j1], b = LX[k2 * npw + j1 + n2];
-        const float v = par ? a.y - b.y : a.x + b.x;
-        sum = fmaf(X[k1 * n2 + j1], v, sum);
-      }
-      const int i = k1 >> 1;
-      const float sg = ((i & 1) ? -2.f : 2.f) * (par ? -1.f : 1.f);
-      out[k1 * E + k2] = make_float2(sg * sum, sg * sum);
-    }
-  }
-}
-
 // ------------------------------------------------------------ (c) eval, 2D Taylor, FP32
 // pot += sum_k y^k sum_j L[k][j] x^j (g2dlevalp_vec, g2drouts.f:847-900) for
 // a chunk of <= 256 points of one leaf, two points per thread.  The leaf's
@@ -402,24 +308,6 @@ cudaError_t launch_form2d_f32(const KP& k, const FormTask* tasks, int ntask, int
                               const long long* hoff, double* hbuf, int Pn, cudaStream_t st) {
   if (Pn > 16 || ntask <= 0) return Pn > 16 ? cudaErrorInvalidValue : cudaSuccess;
   k_form2d_f32<<<dim3(ntask, nd), 128, 0, st>>>(k, tasks, hoff, hbuf);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_pw2taylor2d_f32(const KP& k, const ConvTask* tasks, int ntask, int nd, int Pn, double* lo,
-                                   cudaStream_t st) {
-  if (ntask <= 0) return cudaSuccess;
-  if (Pn > 32 || k.npw > 64) return cudaErrorNotSupported;
-  const int PNB = Pn <= 16 ? 16 : 32;
-  const size_t sh = sizeof(double2) * 4 * ((size_t)k.n2 + k.npw) +
-                    sizeof(float) * (((size_t)Pn * k.n2 + 3) & ~(size_t)3) +
-                    sizeof(float2) * 4 * ((size_t)k.n2 * k.npw + (size_t)PNB * k.npw);
-  if (sh > 48 * 1024) {
-    cudaError_t e = PNB == 16 ? smem_limit(k_pw2taylor2d_f32<16>) : smem_limit(k_pw2taylor2d_f32<32>);
-    if (e != cudaSuccess) return e;
-  }
-  const dim3 g((ntask + 3) / 4, nd);
-  if (PNB == 16) k_pw2taylor2d_f32<16><<<g, 128, sh, st>>>(k, tasks, ntask, lo, Pn);
-  else k_pw2taylor2d_f32<32><<<g, 128, sh, st>>>(k, tasks, ntask, lo, Pn);
   return cudaGetLastError();
 }
 
