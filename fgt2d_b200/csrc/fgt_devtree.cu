@@ -1169,8 +1169,8 @@ constexpr long long kKeyTreeMaxBoxes = 1LL << 24;
 
 // The tree from the exact child digits of the sources (k_exact_key), for
 // trees whose depth fits a 64-bit key (31 levels in 2D, 21 in 3D): one sort
-// of the keys, after which every refinement level is a binary search per
-// (refined box, child) inside the parent's range, and the final point order
+// of the keys, after which every refinement level is a warp search per
+// (refined box, child digit) inside the parent's range, and the final point order
 // is the key order with the input order restored inside each leaf.  No pass
 // over the points per level, and the same tree, ranges and permutations as
 // the per-level refinement below.

@@ -5,7 +5,7 @@ integer field, the centres and the box sizes must be identical, and
 transforms planned on either tree must give identical results.
 
 The device build has two forms: the exact-key form (one sort of each
-source's child digits, every level a binary search per box; the default for
+source's child digits, every level a search of each box's key range; the default for
 trees of at most 31 levels in 2D, 21 in 3D) and the level-by-level
 refinement over all points (deeper trees; FGT_TREE_LEVELWISE=1 selects it
 for any tree).  Both are checked."""

@@ -34,7 +34,7 @@ def _device_tree(src, dim, T):
         level.append(lev); par.append(box); nchild.append(0); child.append([-1] * nch)
         cen.append(np.array([cen[box][d] + (h if (j >> d) & 1 else -h) for d in range(dim)]))
 
-    for l in range(L):  # k_ref_flag / k_ref_scan / k_ref_children
+    for l in range(L):  # k_ref_count / k_scan_top / k_ref_rank, k_ref_children
         thr = ndiv0 if l < levcut else ndiv
         shift, h, first = np.uint64(dim * (L - 1 - l)), bsz[l + 1] / 2, len(level)
         for box in range(lfirst[l], llast[l] + 1):

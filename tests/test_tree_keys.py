@@ -6,7 +6,7 @@ Steps restated: every source descends from the root for nlmax levels with
 the tree's centre arithmetic, its child digits packed most significant level
 first (k_exact_key); one sort of the keys; the range of every box of the
 finished tree from its parent's range by the digit of its level
-(k_child_ranges); the final order restores the input order inside each leaf
+(k_child_bounds); the final order restores the input order inside each leaf
 (k_position_rank + the stable sort).  Every box range and the source
 permutation must equal the host tree's, including on grids whose points lie
 exactly on box boundaries and centres."""
