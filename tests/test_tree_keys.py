@@ -84,3 +84,36 @@ def test_exact_key_tree_equals_host_tree(fgt, case):
     for b in np.where(ichild[:, 0] < 0)[0]:
         perm[r0[b]:r1[b]] = np.sort(perm[r0[b]:r1[b]])
     assert np.array_equal(perm, T["isrc"] - 1)
+
+
+def _warp_digit_lower_bound(dig, a, b, v):
+    """warp_digit_lower_bound (fgt_devtree.cu) lane by lane: each round the 32
+    lanes probe a + floor(span * lane / 32), a ballot counts the probes whose
+    digit is below v (a prefix of the lanes, the digits being sorted), and the
+    range narrows to the gap after the last of them; <= 32 keys are probed
+    one per lane."""
+    for _ in range(8):
+        if b - a <= 32:
+            break
+        span = b - a
+        p = [a + span * lane // 32 for lane in range(32)]
+        below = [dig[q] < v for q in p]
+        c = sum(below)
+        assert below == [True] * c + [False] * (32 - c)
+        if c == 0:
+            return a
+        a, b = p[c - 1] + 1, (p[c] if c < 32 else b)
+    assert b - a <= 32
+    return a + sum(1 for lane in range(32) if a + lane < b and dig[a + lane] < v)
+
+
+def test_warp_digit_search_matches_lower_bound():
+    rng = np.random.default_rng(17)
+    for n in [1, 2, 31, 32, 33, 64, 65, 1000, 4097, 100_000]:
+        for nch in (4, 8):
+            for _ in range(3):
+                dig = np.sort(rng.integers(0, nch, n))
+                if rng.random() < 0.3:  # runs of one digit, empty digits
+                    dig = np.sort(rng.choice([0, nch - 1], n))
+                for v in range(1, nch):
+                    assert _warp_digit_lower_bound(dig, 0, n, v) == np.searchsorted(dig, v, "left")
