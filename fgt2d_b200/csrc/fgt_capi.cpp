@@ -1010,6 +1010,7 @@ int fgt_plan_get_info(const fgt_plan* p, fgt_plan_info* o) {
   o->large_delta = P.large_delta; o->all_direct = P.all_direct;
   o->kernel_launches = p->last_launches;
   for (int i = 0; i < 3; i++) o->shift_bytes[i] = p->H.shift_bytes[i];
+  if (p->have_device) o->shift_bytes[2] = p->D.split_bytes;  // the splits that run
   o->form_route_flops = p->H.form_route_flops;
   o->eval_route_flops = p->H.eval_route_flops;
   double npwd = std::pow((double)P.npw, P.dim);

@@ -179,6 +179,10 @@ struct DevicePlan {
   // statistics copied from the host plan
   long long direct_pairs = 0, form_sources = 0, eval_points = 0;
   long long launches = 0;
+  // algorithmic bytes of the split tasks that run (the others are fused into
+  // the conversion): each distinct expansion read or written once, 16 B per
+  // complex coefficient
+  long long split_bytes = 0;
 };
 
 // Makes freed stream-ordered allocations stay in the current device's default

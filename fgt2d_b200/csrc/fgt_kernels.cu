@@ -3690,6 +3690,13 @@ cudaError_t device_plan_create(const HostPlan& H, DevicePlan& D, const int* d_is
         if (need[loc_box[H.split[i].dst]]) split_kept.push_back(H.split[i]);
       D.split_end[l] = (int)split_kept.size();
     }
+    std::vector<uint8_t> rd(std::max(H.nloc, 1), 0), wr(std::max(H.nloc, 1), 0);
+    long long nrw = 0;
+    for (const ShiftTask& x : split_kept) {
+      nrw += !rd[x.src] + !wr[x.dst];
+      rd[x.src] = wr[x.dst] = 1;
+    }
+    D.split_bytes = 16LL * P.nexp * P.nd * nrw;
   }
   D.nm2l = (int)H.m2l.size();
   D.ndir = (int)(H.dnear.mem ? H.dnear.ndir : (long long)H.dir.size());

@@ -80,8 +80,10 @@ typedef struct fgt_plan_info {
   int large_delta, all_direct;
   int kernel_launches;
   /* algorithmic work per execute: stage (b) bytes counting each distinct
-   * expansion once (merge, mp->loc, split), stage (a)/(c) flops as
-   * 4 * points * npw^dim, stage (d) source-target pairs */
+   * expansion once (merge, mp->loc, split; the split's counts only the
+   * split tasks that run, the rest being fused into the conversion to
+   * Taylor form), stage (a)/(c) flops as 4 * points * npw^dim, stage (d)
+   * source-target pairs */
   long long shift_bytes[3];
   double form_flops, eval_flops;
   /* flops of the routes actually taken (Hermite/Taylor or plane wave),
