@@ -217,10 +217,24 @@ int plan_device(fgt_plan* p, const double* src_host, const double* trg_host) {
 // admit (optional) is called with the device bytes of the plan proper once
 // the tree is built and before they are allocated; it may block, and a
 // status other than FGT_OK abandons the plan.
+// The OpenMP team of a plan's host work: the context's setting, else half
+// the cores and at most 8.  On the 16-core benchmark host the full team lost
+// time to threads descheduled at its barriers (the drop-in call 12.2-16 ms
+// with 16 threads, 11.4-12.0 ms with 8).  The calling thread's setting comes
+// back when the guard ends.
+struct OmpTeam {
+  int old;
+  explicit OmpTeam(const fgt_ctx* c) : old(omp_get_max_threads()) {
+    omp_set_num_threads(c && c->nthreads > 0 ? c->nthreads : std::max(1, std::min(8, omp_get_num_procs() / 2)));
+  }
+  ~OmpTeam() { omp_set_num_threads(old); }
+};
+
 int plan_create_device_tree(fgt_plan* p, int dim, int nd, double delta, double eps, int ns,
                             const double* sources, int nt, const double* targ, int ifpgh, int ifpghtarg,
                             const std::function<int(size_t)>* admit = nullptr, int ifcharge = 1,
                             int ifdipole = 0) {
+  OmpTeam team(p->ctx);
   const bool same = targ == sources && nt == ns;
   int st = alloc_io(p, dim, nd, ns, nt, ifpgh, ifpghtarg, 0, sources, targ, !same, ifdipole);
   if (st != FGT_OK) return st;
@@ -352,6 +366,7 @@ int run_device(fgt_plan* p, const Inputs& in, const Outputs& o, cudaStream_t st,
 // computes back to the non-null host arrays of `host`.
 int exec_host(fgt_plan* p, const double* charge, const Outputs& host, const double* rnormal = nullptr,
               const double* dipstr = nullptr) {
+  OmpTeam team(p->ctx);
   const Params& P = p->H.P;
   cudaStream_t st = p->ctx->stream;
   CKS(cudaSetDevice(p->ctx->device));
@@ -1608,6 +1623,7 @@ int fgt_server_create(int device, long long max_device_bytes, int nworkers, fgt_
       for (fgt_ctx* x : S->ctxs) fgt_ctx_destroy(x);
       return st;
     }
+    c->nthreads = std::max(1, omp_get_num_procs() / nworkers);  // the workers share the host cores
     S->ctxs.push_back(c);
   }
   {

@@ -95,6 +95,10 @@ typedef struct fgt_plan_info {
 int fgt_ctx_create(int device, fgt_ctx** out);
 int fgt_ctx_destroy(fgt_ctx* ctx);
 int fgt_ctx_set_precision(fgt_ctx* ctx, int precision);
+/* OpenMP threads of the host parts of the context's plans (tree, lists,
+ * task arrays, staging copies); 0 (the default) uses half the cores, at most
+ * 8 (a server's contexts: the cores divided among its workers).  The calling
+ * thread's own OpenMP setting is restored when each call returns. */
 int fgt_ctx_set_host_threads(fgt_ctx* ctx, int nthreads);
 /* where plans built with this context build their tree (FGT_TREE_DEVICE or
  * FGT_TREE_HOST); both give the same tree.  No counterpart in the reference,
