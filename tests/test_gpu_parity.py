@@ -3,7 +3,7 @@ and against the FP64 direct sum, through the C ABI.
 
 Bars (relative l2, the reference test's ``derr``):
   * FP64 plain form vs oracle: <= 1e-12       (same routes, rounding-level)
-  * mixed form vs oracle:      <= eps          (north-star parity bar)
+  * mixed form vs oracle:      <= eps          (the floating-point parity bar)
   * both forms vs direct sum:  <= 10 * eps     (the reference's own accuracy)
 """
 import zlib
