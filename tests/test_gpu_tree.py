@@ -73,9 +73,19 @@ def test_device_tree_equals_host_tree(case, form, fgt, ctx, monkeypatch):
 
 @pytest.mark.parametrize("dim,n,delta,eps", [(2, 200000, 1e-6, 1e-6), (2, 60000, 1e-4, 1e-9),
                                              (3, 100000, 1e-3, 1e-6), (2, 500, 10.0, 1e-6)])
-def test_plans_on_either_tree_agree(fgt, dim, n, delta, eps):
+@pytest.mark.parametrize("form", ["keys", "levelwise"])
+@pytest.mark.parametrize("targets", ["separate", "sources"])
+def test_plans_on_either_tree_agree(fgt, dim, n, delta, eps, form, targets, monkeypatch):
+    """Transforms planned on the device tree (either form; the level-by-level
+    form leaves no tree arrays on the device, so the near-field build uploads
+    them) and on the host tree, bitwise; targets apart from the sources, or
+    the sources themselves (one permutation serves both)."""
+    if form == "levelwise":
+        monkeypatch.setenv("FGT_TREE_LEVELWISE", "1")
     rng = np.random.default_rng(n + dim)
     src, trg, q = rng.random((n, dim)), rng.random((n // 2, dim)), rng.standard_normal(n)
+    if targets == "sources":
+        trg = src
     cd = fgt.Context(0, precision="fp64", tree="device")
     ch = fgt.Context(0, precision="fp64", tree="host")
     pd, ptd = fgt.transform(dim, 1, delta, eps, src, q, trg, 1, 1, ctx=cd)
