@@ -410,7 +410,7 @@ def ours_arm(args, w, rank, world, local_rank):
         out_h["pot"] = torch.zeros((w["src"].shape[0], nd), dtype=torch.float64).pin_memory().numpy()
     if w["ifpghtarg"]:
         out_h["pottarg"] = torch.zeros((w["trg"].shape[0], nd), dtype=torch.float64).pin_memory().numpy()
-    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 5))
     ctx.set_precision("mixed")
     e2e_s = float("nan")
     if e2e_steps:
