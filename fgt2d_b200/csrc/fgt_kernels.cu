@@ -4144,7 +4144,12 @@ cudaError_t device_plan_execute(DevicePlan& D, const Inputs& in, const Outputs& 
         const size_t sh = ((size_t)8 * mt + 2 * Pn) * 68 * 8;
         const dim3 fg(G.end - G.beg, nd);
         const FormChunk* ch = D.fchunks + G.beg;
-        if (mixed_ac && form3d_tc_supported(Pn)) {
+        // The tcgen05 Hermite blocks (BF16 x 3) only on request: building
+        // their Pn^2 split operand rows per source costs more than the FP64
+        // DMMA kernel's whole block (3D blobs, Pn = 14: form 4.2 vs 3.45 ms),
+        // so the mixed form keeps the FP64 blocks by default.
+        const bool tc_form = getenv("FGT_FORM3D_TC") != nullptr;
+        if (mixed_ac && tc_form && form3d_tc_supported(Pn)) {
           // mixed form: the Hermite blocks as BF16 x 3 tensor-core products
           CK(launch_form3d_tc(k, D.form, ch, G.end - G.beg, nd, Pn, D.hbuf, D.isq, st));
           if (dom) {

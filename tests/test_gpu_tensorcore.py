@@ -3,9 +3,10 @@
 * The BF16 x 3 compensated tile (three exact BF16 pieces per operand, the six
   piece products of order <= 2 accumulated in FP32 in TMEM) against an FP64
   product: FP32-level agreement for every N the kernels use.
-* The mixed 3D form (tcgen05 Hermite blocks and Taylor evaluation, FP32 near
-  field) against the FP64 form on the same inputs: the difference is rounding
-  of FP32 size (~1e-7), well below eps, and no bounded wait of a tensor-core
+* The mixed 3D form (tcgen05 Taylor evaluation, FP32 near field; the
+  tcgen05 Hermite blocks too with FGT_FORM3D_TC set, else the FP64 blocks)
+  against the FP64 form on the same inputs: the difference is rounding of
+  FP32 size (~1e-7), well below eps, and no bounded wait of a tensor-core
   kernel gave up.
 """
 import ctypes
@@ -26,7 +27,10 @@ def test_bf16x3_tile_matches_fp64(fgt, n):
 
 
 @pytest.mark.parametrize("delta,n", [(1e-3, 60000), (1e-2, 30000)])
-def test_mixed_3d_eval_matches_fp64(fgt, oracle, delta, n):
+@pytest.mark.parametrize("tc_form", [False, True])
+def test_mixed_3d_eval_matches_fp64(fgt, oracle, delta, n, tc_form, monkeypatch):
+    if tc_form:
+        monkeypatch.setenv("FGT_FORM3D_TC", "1")
     rng = np.random.default_rng(77)
     src = rng.random((n, 3))
     trg = rng.random((n // 2, 3))
